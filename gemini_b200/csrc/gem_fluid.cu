@@ -1,0 +1,605 @@
+// Host side of libgemini_b200: device grid/work objects, kernel launchers and the
+// device-resident C ABI declared in include/gem_fluid.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gem_fluid.h"
+#include "gem_kernels.cuh"
+
+using namespace gemk;
+
+extern "C" void gem_capi_bind_grid(gem_grid* g);
+extern "C" void gem_capi_forget_grid(gem_grid* g);
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define GEM_CUDA(call)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return set_err(GEM_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                     __FILE__, __LINE__);                                                 \
+  } while (0)
+
+#define GEM_LAUNCHED(name)                                                                    \
+  do {                                                                                        \
+    cudaError_t e_ = cudaGetLastError();                                                      \
+    if (e_ != cudaSuccess) return set_err(GEM_ECUDA, "launch of %s failed: %s", name, cudaGetErrorString(e_)); \
+  } while (0)
+
+int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+unsigned grid_for(long long n, int threads, int per_sm = 8) {
+  long long b = (n + threads - 1) / threads;
+  const long long cap = (long long)num_sms() * per_sm;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+struct gem_grid {
+  GridDev dev;
+  int lnull;
+  std::vector<void*> allocs;
+};
+
+struct gem_work {
+  int lx1, lx2, lx3;
+  double *vs1i, *vs2i, *vs3i, *nn, *Tn, *dt;
+  unsigned long long* acc;  // 32 slots: CFL maxima / counters
+  long long nf1, nf2, nf3;
+  // device staging of the host blocks for gem_fluid_adv_host
+  double *F, *A, *E;
+  size_t nF, nA, nE;
+};
+
+namespace {
+
+int dev_copy(const double* h, size_t n, const double** out, std::vector<void*>& allocs) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess)
+    return set_err(GEM_ENOMEM, "cudaMalloc of %zu doubles failed", n);
+  allocs.push_back(p);
+  GEM_CUDA(cudaMemcpy(p, h, n * sizeof(double), cudaMemcpyHostToDevice));
+  *out = static_cast<const double*>(p);
+  return GEM_OK;
+}
+
+int check_grid(const gem_grid* g) {
+  if (!g) return set_err(GEM_EINVAL, "null grid");
+  return GEM_OK;
+}
+
+Blocks blocks(const gem_grid* g, double* F, double* A) {
+  Blocks b;
+  b.F = F;
+  b.A = A;
+  b.ng = g->dev.d.ng;
+  return b;
+}
+
+// fused step requirements shared by several launchers
+int check_step(const gem_grid* g) {
+  const Dims& d = g->dev.d;
+  if (d.lx1 < 4) return set_err(GEM_EINVAL, "lx1=%d: the x1 boundary and diffusion stencils need lx1 >= 4", d.lx1);
+  if (g->dev.flagper && d.lx3 < 2) return set_err(GEM_EINVAL, "periodic x3 needs lx3 >= 2 (lx3=%d)", d.lx3);
+  return GEM_OK;
+}
+
+template <int DIM, bool FUSED>
+int launch_sweep_t(const gem_grid* g, SweepArgs a, int nsp, cudaStream_t st) {
+  const Dims& d = g->dev.d;
+  const int lxa = (DIM == 1) ? d.lx2 : d.lx1;
+  const int lxb = (DIM == 3) ? d.lx2 : d.lx3;
+  dim3 block(32, nsp);
+  dim3 grid((lxa + 31) / 32, lxb);
+  if (g->dev.unit)
+    k_sweep<DIM, true, FUSED><<<grid, block, 0, st>>>(a);
+  else
+    k_sweep<DIM, false, FUSED><<<grid, block, 0, st>>>(a);
+  GEM_LAUNCHED("k_sweep");
+  return GEM_OK;
+}
+
+int launch_sweep(const gem_grid* g, int dim, bool fused, SweepArgs a, int nsp, cudaStream_t st) {
+  if (fused) {
+    if (dim == 1) return launch_sweep_t<1, true>(g, a, nsp, st);
+    if (dim == 2) return launch_sweep_t<2, true>(g, a, nsp, st);
+    return launch_sweep_t<3, true>(g, a, nsp, st);
+  }
+  if (dim == 1) return launch_sweep_t<1, false>(g, a, nsp, st);
+  if (dim == 2) return launch_sweep_t<2, false>(g, a, nsp, st);
+  return launch_sweep_t<3, false>(g, a, nsp, st);
+}
+
+int launch_ghost_fill(const gem_grid* g, Blocks B, const double* vs1i, int lsp, bool fused,
+                      cudaStream_t st) {
+  const Dims& d = g->dev.d;
+  const GridDev& G = g->dev;
+  const long long ncol = (long long)(d.lx2 + 4) * (d.lx3 + 4) * lsp;
+  const long long nrow2 = (long long)(d.lx1 + 4) * (d.lx3 + 4) * lsp;
+  const long long nrow3 = (long long)(d.lx1 + 4) * (d.lx2 + 4) * lsp;
+  if (fused) {
+    k_ghost_x1<true><<<grid_for(ncol, 128), 128, 0, st>>>(G, B, vs1i, lsp);
+    k_ghost_x2<true><<<grid_for(nrow2, 128), 128, 0, st>>>(G, B, lsp);
+    if (G.flagper)
+      k_ghost_x3<true, true><<<grid_for(nrow3, 128), 128, 0, st>>>(G, B, lsp);
+    else
+      k_ghost_x3<true, false><<<grid_for(nrow3, 128), 128, 0, st>>>(G, B, lsp);
+  } else {
+    k_ghost_x1<false><<<grid_for(ncol, 128), 128, 0, st>>>(G, B, vs1i, lsp);
+    k_ghost_x2<false><<<grid_for(nrow2, 128), 128, 0, st>>>(G, B, lsp);
+    if (!G.flagper) k_ghost_x3<false, false><<<grid_for(nrow3, 128), 128, 0, st>>>(G, B, lsp);
+  }
+  GEM_LAUNCHED("ghost fill");
+  return GEM_OK;
+}
+
+int launch_diffusion(const gem_grid* g, DiffArgs a, cudaStream_t st) {
+  const Dims& d = g->dev.d;
+  const int M = std::max(2, (d.lx1 + 31) / 32);
+  const size_t per_warp = (size_t)DNA * M * 32 * sizeof(double);
+  int wpb = (int)std::min<size_t>(4, (227 * 1024) / per_warp);
+  if (wpb < 1) return set_err(GEM_EINVAL, "lx1=%d too long for the on-chip column solver", d.lx1);
+  a.M = M;
+  const size_t smem = per_warp * wpb;
+  const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
+  long long nblk = (ncs + wpb - 1) / wpb;
+  int per_sm = 0;
+  if (g->dev.unit) {
+    GEM_CUDA(cudaFuncSetAttribute(k_diffusion<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion<true>, 32 * wpb, smem));
+  } else {
+    GEM_CUDA(cudaFuncSetAttribute(k_diffusion<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion<false>, 32 * wpb, smem));
+  }
+  if (per_sm < 1) per_sm = 1;
+  const long long cap = (long long)num_sms() * per_sm;
+  if (nblk > cap) nblk = cap;
+  if (g->dev.unit)
+    k_diffusion<true><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
+  else
+    k_diffusion<false><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
+  GEM_LAUNCHED("k_diffusion");
+  return GEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gem_last_error(void) { return g_err.c_str(); }
+int gem_version(void) { return 1; }
+
+int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
+  if (!desc || !out) return set_err(GEM_EINVAL, "null argument");
+  *out = nullptr;
+  const int lx1 = desc->lx1, lx2 = desc->lx2, lx3 = desc->lx3;
+  if (lx1 < 1 || lx2 < 1 || lx3 < 1) return set_err(GEM_EINVAL, "grid sizes must be positive");
+  if (desc->gridflag < 0 || desc->gridflag > 2) return set_err(GEM_EINVAL, "gridflag must be 0, 1 or 2");
+  gem_grid* g = new gem_grid();
+  GridDev& G = g->dev;
+  G.d = make_dims(lx1, lx2, lx3);
+  G.gridflag = desc->gridflag;
+  G.flagper = desc->flagper ? 1 : 0;
+  G.unit = desc->unit_metrics ? 1 : 0;
+  const size_t ng = (size_t)G.d.ng;
+  int rc = GEM_OK;
+  auto cp = [&](const double* h, size_t n, const double** o) {
+    if (rc != GEM_OK) return;
+    if (!h) {
+      rc = set_err(GEM_EINVAL, "missing grid array");
+      return;
+    }
+    rc = dev_copy(h, n, o, g->allocs);
+  };
+  cp(desc->dx1, lx1 + 3, &G.dx1);
+  cp(desc->dx1i, lx1, &G.dx1i);
+  cp(desc->dx2, lx2 + 3, &G.dx2);
+  cp(desc->dx2i, lx2, &G.dx2i);
+  cp(desc->dx3, lx3 + 3, &G.dx3);
+  cp(desc->dx3i, lx3, &G.dx3i);
+  cp(desc->h1, ng, &G.h1);
+  cp(desc->h2, ng, &G.h2);
+  cp(desc->h3, ng, &G.h3);
+  const size_t n1 = (size_t)(lx1 + 1) * lx2 * lx3, n2 = (size_t)lx1 * (lx2 + 1) * lx3,
+               n3 = (size_t)lx1 * lx2 * (lx3 + 1);
+  cp(desc->h1x1i, n1, &G.h1x1i);
+  cp(desc->h2x1i, n1, &G.h2x1i);
+  cp(desc->h3x1i, n1, &G.h3x1i);
+  cp(desc->h1x2i, n2, &G.h1x2i);
+  cp(desc->h2x2i, n2, &G.h2x2i);
+  cp(desc->h3x2i, n2, &G.h3x2i);
+  cp(desc->h1x3i, n3, &G.h1x3i);
+  cp(desc->h2x3i, n3, &G.h2x3i);
+  cp(desc->h3x3i, n3, &G.h3x3i);
+  g->lnull = 0;
+  G.has_null = 0;
+  G.nullpts = nullptr;
+  if (rc == GEM_OK && desc->nullpts) {
+    const size_t nc = (size_t)lx1 * lx2 * lx3;
+    for (size_t k = 0; k < nc; ++k) g->lnull += desc->nullpts[k] ? 1 : 0;
+    if (g->lnull > 0) {
+      void* p = nullptr;
+      if (cudaMalloc(&p, nc) != cudaSuccess) {
+        rc = set_err(GEM_ENOMEM, "cudaMalloc for nullpts failed");
+      } else {
+        g->allocs.push_back(p);
+        if (cudaMemcpy(p, desc->nullpts, nc, cudaMemcpyHostToDevice) != cudaSuccess)
+          rc = set_err(GEM_ECUDA, "copy of nullpts failed");
+        G.nullpts = static_cast<const unsigned char*>(p);
+        G.has_null = 1;
+      }
+    }
+  }
+  if (rc != GEM_OK) {
+    gem_grid_destroy(g);
+    return rc;
+  }
+  *out = g;
+  gem_capi_bind_grid(g);  // the grid sizes the size-less *_C entry points use
+  return GEM_OK;
+}
+
+int gem_grid_destroy(gem_grid* g) {
+  if (!g) return GEM_OK;
+  gem_capi_forget_grid(g);
+  for (void* p : g->allocs) cudaFree(p);
+  delete g;
+  return GEM_OK;
+}
+
+int gem_grid_dims(const gem_grid* g, int* lx1, int* lx2, int* lx3) {
+  if (check_grid(g)) return GEM_EINVAL;
+  if (lx1) *lx1 = g->dev.d.lx1;
+  if (lx2) *lx2 = g->dev.d.lx2;
+  if (lx3) *lx3 = g->dev.d.lx3;
+  return GEM_OK;
+}
+
+int gem_work_create(const gem_grid* g, gem_work** out) {
+  if (check_grid(g) || !out) return set_err(GEM_EINVAL, "null argument");
+  *out = nullptr;
+  const Dims& d = g->dev.d;
+  gem_work* w = new gem_work();
+  std::memset(w, 0, sizeof(*w));
+  w->lx1 = d.lx1;
+  w->lx2 = d.lx2;
+  w->lx3 = d.lx3;
+  w->nf1 = (long long)(d.lx1 + 1) * d.lx2 * d.lx3;
+  w->nf2 = (long long)d.lx1 * (d.lx2 + 1) * d.lx3;
+  w->nf3 = (long long)d.lx1 * d.lx2 * (d.lx3 + 1);
+  const long long nc = (long long)d.lx1 * d.lx2 * d.lx3;
+  struct A {
+    void** p;
+    size_t bytes;
+  } al[] = {{(void**)&w->vs1i, sizeof(double) * w->nf1 * LSP},
+            {(void**)&w->vs2i, sizeof(double) * w->nf2 * LSP},
+            {(void**)&w->vs3i, sizeof(double) * w->nf3 * LSP},
+            {(void**)&w->nn, sizeof(double) * nc * 3},
+            {(void**)&w->Tn, sizeof(double) * nc},
+            {(void**)&w->dt, sizeof(double) * 4},
+            {(void**)&w->acc, sizeof(unsigned long long) * 32}};
+  for (auto& a : al) {
+    if (cudaMalloc(a.p, a.bytes) != cudaSuccess) {
+      gem_work_destroy(w);
+      return set_err(GEM_ENOMEM, "cudaMalloc of %zu bytes for the work object failed", a.bytes);
+    }
+    // libgemini.f90:288-291: interface velocities start at zero
+    if (cudaMemset(*a.p, 0, a.bytes) != cudaSuccess) {
+      gem_work_destroy(w);
+      return set_err(GEM_ECUDA, "cudaMemset failed");
+    }
+  }
+  *out = w;
+  return GEM_OK;
+}
+
+int gem_work_destroy(gem_work* w) {
+  if (!w) return GEM_OK;
+  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  delete w;
+  return GEM_OK;
+}
+
+int gem_work_set_neutrals(gem_work* w, const double* nn, const double* Tn) {
+  if (!w || !nn || !Tn) return set_err(GEM_EINVAL, "null argument");
+  const size_t nc = (size_t)w->lx1 * w->lx2 * w->lx3;
+  GEM_CUDA(cudaMemcpy(w->nn, nn, nc * 3 * sizeof(double), cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy(w->Tn, Tn, nc * sizeof(double), cudaMemcpyHostToDevice));
+  return GEM_OK;
+}
+
+int gem_work_interface_vels(gem_work* w, int which, double* host, int dir) {
+  if (!w || !host || which < 1 || which > 3) return set_err(GEM_EINVAL, "bad argument");
+  double* p = which == 1 ? w->vs1i : which == 2 ? w->vs2i : w->vs3i;
+  const long long n = (which == 1 ? w->nf1 : which == 2 ? w->nf2 : w->nf3) * LSP;
+  if (dir == 0)
+    GEM_CUDA(cudaMemcpy(p, host, n * sizeof(double), cudaMemcpyHostToDevice));
+  else
+    GEM_CUDA(cudaMemcpy(host, p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return GEM_OK;
+}
+
+double* gem_work_array(gem_work* w, int which) {
+  if (!w) return nullptr;
+  switch (which) {
+    case 1: return w->vs1i;
+    case 2: return w->vs2i;
+    case 3: return w->vs3i;
+    case 4: return w->nn;
+    case 5: return w->Tn;
+    default: return nullptr;
+  }
+}
+
+double* gem_work_dt(gem_work* w) { return w ? w->dt : nullptr; }
+
+// ---- conversions ---------------------------------------------------------------------
+#define ELEMWISE(name, kern, Fp, Ap)                                                   \
+  int name(const gem_grid* g, Fp fluidvars, Ap fluidauxvars, void* stream) {           \
+    if (check_grid(g) || !fluidvars || !fluidauxvars) return set_err(GEM_EINVAL, "null argument"); \
+    Blocks B = blocks(g, const_cast<double*>(fluidvars), const_cast<double*>(fluidauxvars)); \
+    kern<<<grid_for(g->dev.d.ng, 256), 256, 0, S(stream)>>>(B);                        \
+    GEM_LAUNCHED(#kern);                                                               \
+    return GEM_OK;                                                                     \
+  }
+ELEMWISE(gem_v12rhov1_dev, k_v12rhov1, const double*, double*)
+ELEMWISE(gem_T2rhoe_dev, k_T2rhoe, const double*, double*)
+ELEMWISE(gem_rhov12v1_dev, k_rhov12v1, double*, const double*)
+ELEMWISE(gem_rhoe2T_dev, k_rhoe2T, double*, const double*)
+#undef ELEMWISE
+
+int gem_set_global_boundaries_allspec_dev(const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                                          const gem_work* w, int lsp, void* stream) {
+  if (check_grid(g) || !fluidvars || !fluidauxvars || !w) return set_err(GEM_EINVAL, "null argument");
+  if (lsp < 1 || lsp > LSP) return set_err(GEM_EINVAL, "number of global boundaries must be in 1..%d", LSP);
+  if (g->dev.d.lx1 < 3) return set_err(GEM_EINVAL, "lx1 must be >= 3 for the x1 boundary extrapolation");
+  return launch_ghost_fill(g, blocks(g, fluidvars, fluidauxvars), w->vs1i, lsp, false, S(stream));
+}
+
+int gem_halo_fluidvars_dev(const gem_grid* g, double* fluidvars, double* fluidauxvars, void* stream) {
+  if (check_grid(g) || !fluidvars || !fluidauxvars) return set_err(GEM_EINVAL, "null argument");
+  if (!g->dev.flagper) return GEM_OK;
+  if (g->dev.d.lx3 < 2) return set_err(GEM_EINVAL, "periodic x3 needs lx3 >= 2");
+  const long long n = (long long)(g->dev.d.lx1 + 4) * g->dev.d.lx2 * LSP;
+  k_halo_wrap<<<grid_for(n, 128), 128, 0, S(stream)>>>(g->dev, blocks(g, fluidvars, fluidauxvars), 1);
+  GEM_LAUNCHED("k_halo_wrap");
+  return GEM_OK;
+}
+
+int gem_halo_allparams_dev(const gem_grid* g, double* fluidvars, double* fluidauxvars, void* stream) {
+  if (check_grid(g) || !fluidvars || !fluidauxvars) return set_err(GEM_EINVAL, "null argument");
+  if (!g->dev.flagper) return GEM_OK;
+  if (g->dev.d.lx3 < 2) return set_err(GEM_EINVAL, "periodic x3 needs lx3 >= 2");
+  const long long n = (long long)(g->dev.d.lx1 + 4) * g->dev.d.lx2 * LSP;
+  k_halo_wrap<<<grid_for(n, 128), 128, 0, S(stream)>>>(g->dev, blocks(g, fluidvars, fluidauxvars), 0);
+  GEM_LAUNCHED("k_halo_wrap");
+  return GEM_OK;
+}
+
+int gem_interface_vels_allspec_dev(const gem_grid* g, const double* fluidvars, gem_work* w, int lsp,
+                                   void* stream) {
+  if (check_grid(g) || !fluidvars || !w) return set_err(GEM_EINVAL, "null argument");
+  if (lsp < 1 || lsp > LSP) return set_err(GEM_EINVAL, "number of interface vels must be in 1..%d", LSP);
+  const Dims& d = g->dev.d;
+  const long long n = (nf1(d) + nf2(d) + nf3(d)) * lsp;
+  k_interface_vels<<<grid_for(n, 256), 256, 0, S(stream)>>>(g->dev, blocks(g, const_cast<double*>(fluidvars), nullptr),
+                                                          w->vs1i, w->vs2i, w->vs3i, lsp);
+  GEM_LAUNCHED("k_interface_vels");
+  return GEM_OK;
+}
+
+int gem_sweep_allspec_dev(const gem_grid* g, int dim, int which, double* fluidvars, double* fluidauxvars,
+                          const gem_work* w, const double* dt, void* stream) {
+  if (check_grid(g) || !fluidvars || !fluidauxvars || !w || !dt) return set_err(GEM_EINVAL, "null argument");
+  if (dim < 1 || dim > 3 || which < 0 || which > 2) return set_err(GEM_EINVAL, "dim must be 1..3, which 0..2");
+  SweepArgs a;
+  a.G = g->dev;
+  a.B = blocks(g, fluidvars, fluidauxvars);
+  a.vsi = dim == 1 ? w->vs1i : dim == 2 ? w->vs2i : w->vs3i;
+  a.vs1i = nullptr;
+  a.dtp = dt;
+  a.which = which;
+  const int nsp = (which == 2) ? LSP : LSP - 1;  // multifluid.f90:55,63,71
+  return launch_sweep(g, dim, false, a, nsp, S(stream));
+}
+
+int gem_clean_param_dev(const gem_grid* g, int iparm, double* fluidvars, void* stream) {
+  if (check_grid(g) || !fluidvars) return set_err(GEM_EINVAL, "null argument");
+  if (iparm < 1 || iparm > 3) return set_err(GEM_EINVAL, "non-standard parameter selected in clean_params");
+  const long long ng = g->dev.d.ng;
+  double* param = fluidvars + (iparm == 1 ? 0 : iparm == 2 ? LSP : 4 * LSP) * ng;
+  k_clean_elementwise<<<grid_for(ng, 256), 256, 0, S(stream)>>>(g->dev, param, iparm);
+  GEM_LAUNCHED("k_clean_elementwise");
+  if (iparm == 2 && g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1)) {
+    const long long n = (long long)g->dev.d.lx2 * g->dev.d.lx3 * LSP;
+    k_clean_vel_edges<<<grid_for(n, 128), 128, 0, S(stream)>>>(g->dev, param);
+    GEM_LAUNCHED("k_clean_vel_edges");
+  }
+  return GEM_OK;
+}
+
+int gem_energy_diffusion_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars,
+                             const double* electrovars, const gem_work* w, const double* dt, void* stream) {
+  if (!cfg || check_grid(g) || !fluidvars || !electrovars || !w || !dt) return set_err(GEM_EINVAL, "null argument");
+  if (cfg->diffsolvetype != 1 && cfg->diffsolvetype != 2)
+    return set_err(GEM_EINVAL, "Unsupported diffusion solver type/mode: %d. Should be either 1 or 2.", cfg->diffsolvetype);
+  if (g->dev.d.lx1 < 4) return set_err(GEM_EINVAL, "diffusion needs lx1 >= 4");
+  DiffArgs a;
+  a.G = g->dev;
+  a.B = blocks(g, fluidvars, nullptr);
+  a.J1 = electrovars + 3 * g->dev.d.ng;
+  a.nn = w->nn;
+  a.Tn = w->Tn;
+  a.dtp = dt;
+  a.Teinf = cfg->Teinf;
+  a.solver = cfg->diffsolvetype;
+  a.fused = 0;
+  int rc = launch_diffusion(g, a, S(stream));
+  if (rc) return rc;
+  k_diffusion_ghost_floor<<<grid_for(g->dev.d.ng, 256), 256, 0, S(stream)>>>(g->dev, a.B);
+  GEM_LAUNCHED("k_diffusion_ghost_floor");
+  return GEM_OK;
+}
+
+int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem_work* w, double* dt_out,
+                    void* stream) {
+  if (check_grid(g) || !fluidvars || !w || !dt_out) return set_err(GEM_EINVAL, "null argument");
+  cudaStream_t st = S(stream);
+  GEM_CUDA(cudaMemsetAsync(w->acc, 0, 3 * LSP * sizeof(unsigned long long), st));
+  Blocks B = blocks(g, const_cast<double*>(fluidvars), nullptr);
+  const unsigned nb = grid_for(nci(g->dev.d), 256, 4);
+  if (g->dev.unit)
+    k_dt_reduce<true><<<nb, 256, 0, st>>>(g->dev, B, w->acc, nullptr, 0);
+  else
+    k_dt_reduce<false><<<nb, 256, 0, st>>>(g->dev, B, w->acc, nullptr, 0);
+  GEM_LAUNCHED("k_dt_reduce");
+  k_dt_finalize<<<1, 32, 0, st>>>(w->acc, tcfl, dt_out);
+  GEM_LAUNCHED("k_dt_finalize");
+  return GEM_OK;
+}
+
+int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, const double* dt,
+                   double* maxcfl_out, void* stream) {
+  if (check_grid(g) || !fluidvars || !w || !dt || !maxcfl_out) return set_err(GEM_EINVAL, "null argument");
+  cudaStream_t st = S(stream);
+  GEM_CUDA(cudaMemsetAsync(w->acc + 24, 0, sizeof(unsigned long long), st));
+  Blocks B = blocks(g, const_cast<double*>(fluidvars), nullptr);
+  const unsigned nb = grid_for(nci(g->dev.d), 256, 4);
+  if (g->dev.unit)
+    k_dt_reduce<true><<<nb, 256, 0, st>>>(g->dev, B, w->acc + 24, dt, 1);
+  else
+    k_dt_reduce<false><<<nb, 256, 0, st>>>(g->dev, B, w->acc + 24, dt, 1);
+  GEM_LAUNCHED("k_dt_reduce");
+  k_maxcfl_finalize<<<1, 32, 0, st>>>(w->acc + 24, maxcfl_out);
+  GEM_LAUNCHED("k_maxcfl_finalize");
+  return GEM_OK;
+}
+
+int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                      const double* electrovars, gem_work* w, const double* dt, void* stream) {
+  if (!cfg || check_grid(g) || !fluidvars || !fluidauxvars || !electrovars || !w || !dt)
+    return set_err(GEM_EINVAL, "null argument");
+  if (cfg->diffsolvetype != 1 && cfg->diffsolvetype != 2)
+    return set_err(GEM_EINVAL, "Unsupported diffusion solver type/mode: %d. Should be either 1 or 2.", cfg->diffsolvetype);
+  int rc = check_step(g);
+  if (rc) return rc;
+  cudaStream_t st = S(stream);
+  Blocks B = blocks(g, fluidvars, fluidauxvars);
+  // v12rhov1 + T2rhoe + set_global_boundaries + halo_fluidvars (the interior conversions
+  // are folded into the x3 sweep)
+  rc = launch_ghost_fill(g, B, w->vs1i, LSP, true, st);
+  if (rc) return rc;
+  SweepArgs a;
+  a.G = g->dev;
+  a.B = B;
+  a.vsi = nullptr;
+  a.vs1i = w->vs1i;
+  a.dtp = dt;
+  a.which = 0;
+  if ((rc = launch_sweep(g, 3, true, a, LSP, st))) return rc;
+  if ((rc = launch_sweep(g, 1, true, a, LSP, st))) return rc;
+  if ((rc = launch_sweep(g, 2, true, a, LSP, st))) return rc;
+  k_ghost_epilogue<<<grid_for(g->dev.d.ng, 256), 256, 0, st>>>(g->dev, B);
+  GEM_LAUNCHED("k_ghost_epilogue");
+  if (g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1)) {
+    const long long n = (long long)g->dev.d.lx2 * g->dev.d.lx3 * LSP;
+    k_clean_vel_edges<<<grid_for(n, 128), 128, 0, st>>>(g->dev, fluidvars + LSP * g->dev.d.ng);
+    GEM_LAUNCHED("k_clean_vel_edges");
+  }
+  DiffArgs d;
+  d.G = g->dev;
+  d.B = B;
+  d.J1 = electrovars + 3 * g->dev.d.ng;
+  d.nn = w->nn;
+  d.Tn = w->Tn;
+  d.dtp = dt;
+  d.Teinf = cfg->Teinf;
+  d.solver = cfg->diffsolvetype;
+  d.fused = 1;
+  return launch_diffusion(g, d, st);
+}
+
+int gem_fluid_adv_host(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                       const double* electrovars, gem_work* w, double* dt_inout, void* stream) {
+  if (!cfg || check_grid(g) || !fluidvars || !fluidauxvars || !electrovars || !w || !dt_inout)
+    return set_err(GEM_EINVAL, "null argument");
+  const size_t ng = (size_t)g->dev.d.ng;
+  const size_t nF = ng * 5 * LSP, nA = ng * (2 * LSP + 9), nE = ng * 7;
+  if (!w->F) {
+    if (cudaMalloc(&w->F, nF * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&w->A, nA * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&w->E, nE * sizeof(double)) != cudaSuccess)
+      return set_err(GEM_ENOMEM, "device staging allocation failed");
+    w->nF = nF;
+    w->nA = nA;
+    w->nE = nE;
+  }
+  cudaStream_t st = S(stream);
+  GEM_CUDA(cudaMemcpyAsync(w->F, fluidvars, nF * sizeof(double), cudaMemcpyHostToDevice, st));
+  GEM_CUDA(cudaMemcpyAsync(w->A, fluidauxvars, nA * sizeof(double), cudaMemcpyHostToDevice, st));
+  GEM_CUDA(cudaMemcpyAsync(w->E, electrovars, nE * sizeof(double), cudaMemcpyHostToDevice, st));
+  int rc;
+  if (*dt_inout < 0) {
+    if ((rc = gem_dt_calc_dev(g, cfg->tcfl, w->F, w, w->dt, stream))) return rc;
+  } else {
+    GEM_CUDA(cudaMemcpyAsync(w->dt, dt_inout, sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  if ((rc = gem_fluid_adv_dev(cfg, g, w->F, w->A, w->E, w, w->dt, stream))) return rc;
+  GEM_CUDA(cudaMemcpyAsync(fluidvars, w->F, nF * sizeof(double), cudaMemcpyDeviceToHost, st));
+  GEM_CUDA(cudaMemcpyAsync(fluidauxvars, w->A, nA * sizeof(double), cudaMemcpyDeviceToHost, st));
+  GEM_CUDA(cudaMemcpyAsync(dt_inout, w->dt, sizeof(double), cudaMemcpyDeviceToHost, st));
+  GEM_CUDA(cudaStreamSynchronize(st));
+  return GEM_OK;
+}
+
+int gem_check_finite(const gem_grid* g, const double* fluidvars, gem_work* w, long long* count, void* stream) {
+  if (check_grid(g) || !fluidvars || !w || !count) return set_err(GEM_EINVAL, "null argument");
+  cudaStream_t st = S(stream);
+  GEM_CUDA(cudaMemsetAsync(w->acc + 28, 0, sizeof(unsigned long long), st));
+  k_count_nonfinite<<<grid_for(nci(g->dev.d), 256, 4), 256, 0, st>>>(
+      g->dev, blocks(g, const_cast<double*>(fluidvars), nullptr), w->acc + 28);
+  GEM_LAUNCHED("k_count_nonfinite");
+  unsigned long long c = 0;
+  GEM_CUDA(cudaMemcpyAsync(&c, w->acc + 28, sizeof(c), cudaMemcpyDeviceToHost, st));
+  GEM_CUDA(cudaStreamSynchronize(st));
+  *count = (long long)c;
+  return c ? GEM_ENONFINITE : GEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,145 @@
+/* gem_fluid.h -- device-resident C ABI of the B200 fluid-advance library (libgemini_b200.so).
+ *
+ * This is the path GEMINI3D calls for the multifluid advection sweeps and the
+ * field-aligned heat diffusion.  The entry points below take DEVICE pointers to the
+ * reference's own memory blocks (same Fortran layout, see below), an explicit stream, and
+ * return an int status (no error stop, no host synchronisation unless stated).  The
+ * host-pointer entry points with the reference's names and signatures are declared in
+ * gemini3d_fluid.h.
+ *
+ * Memory-block layout (libgemini.f90:401-417, 462-519), Fortran order, x1 fastest,
+ * 2 ghost cells per side, lsp = 7 (6 ions + electrons):
+ *   fluidvars    (lx1+4, lx2+4, lx3+4, 5*lsp)   ns | vs1 | vs2 | vs3 | Ts
+ *   fluidauxvars (lx1+4, lx2+4, lx3+4, 2*lsp+9) rhovs1 | rhoes | 9 MHD scalars (untouched)
+ *   electrovars  (lx1+4, lx2+4, lx3+4, 7)       E1 E2 E3 J1 J2 J3 Phi (J1 read)
+ * Work arrays carried in gem_work (libgemini.f90:92-129, 284-291):
+ *   vs1i (lx1+1,lx2,lx3,lsp), vs2i (lx1,lx2+1,lx3,lsp), vs3i (lx1,lx2,lx3+1,lsp)
+ *   nn (lx1,lx2,lx3,3) = n(O), n(N2), n(O2);  Tn (lx1,lx2,lx3)
+ * All values are IEEE binary64.  Streams are passed as void* (a cudaStream_t; NULL is
+ * the legacy default stream).
+ */
+#ifndef GEM_FLUID_H
+#define GEM_FLUID_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define GEM_OK 0
+#define GEM_EINVAL 1      /* bad argument or unsupported size */
+#define GEM_ENONFINITE 2  /* non-finite values detected (gem_check_finite) */
+#define GEM_ETIMEOUT 3    /* a bounded device wait gave up */
+#define GEM_ECUDA 4       /* CUDA runtime error; see gem_last_error() */
+#define GEM_ENOMEM 5      /* device allocation failed */
+
+typedef struct gem_grid gem_grid; /* device copy of a curvmesh (meshobj.f90:49-154) */
+typedef struct gem_work gem_work; /* interface velocities, neutrals, dt and scratch */
+
+/* Host description of a grid; every array is copied to the device by gem_grid_create.
+ * Replaces read_grid_C / set_gridpointer_dyntype (libgemini_c.f90:63-82): the grid
+ * object the *_C entry points receive as xC is a gem_grid*. */
+typedef struct gem_grid_desc {
+  int lx1, lx2, lx3;
+  int gridflag; /* 0 closed dipole, 1 open inverted, 2 non-inverted (meshobj.f90:549-570) */
+  int flagper;  /* x3 periodic (meshobj.f90:324-335) */
+  const double *dx1, *dx1i, *dx2, *dx2i, *dx3, *dx3i; /* dx: l+3 values (0:l+2), dxi: l */
+  const double *h1, *h2, *h3;                          /* ghosted (lx1+4)(lx2+4)(lx3+4) */
+  const double *h1x1i, *h2x1i, *h3x1i;                 /* (lx1+1, lx2, lx3) */
+  const double *h1x2i, *h2x2i, *h3x2i;                 /* (lx1, lx2+1, lx3) */
+  const double *h1x3i, *h2x3i, *h3x3i;                 /* (lx1, lx2, lx3+1) */
+  const unsigned char* nullpts;                        /* (lx1, lx2, lx3) or NULL */
+  int unit_metrics; /* 1 if every metric factor is exactly 1 (Cartesian); the kernels then
+                       skip the metric loads -- results are identical */
+} gem_grid_desc;
+
+/* Plain-value run parameters (gemini_cfg fields read on this path, config_nml.f90). */
+typedef struct gem_cfg {
+  double Teinf;      /* exospheric electron temperature for the top Dirichlet BC */
+  int diffsolvetype; /* 1 backward Euler, 2 TRBDF2 */
+  double tcfl;       /* target CFL number for dt_calc */
+  int flagglow;      /* non-zero: dt_select_C also clips dt at the GLOW output time */
+} gem_cfg;
+
+const char* gem_last_error(void); /* thread-local message for the last non-zero status */
+int gem_version(void);
+
+/* grid and work objects (allocate device memory; synchronous) */
+int gem_grid_create(const gem_grid_desc* desc, gem_grid** out);
+int gem_grid_destroy(gem_grid* g);
+int gem_grid_dims(const gem_grid* g, int* lx1, int* lx2, int* lx3);
+int gem_work_create(const gem_grid* g, gem_work** out);
+int gem_work_destroy(gem_work* w);
+/* copy neutral inputs (host pointers; nn (lx1,lx2,lx3,3), Tn (lx1,lx2,lx3)) */
+int gem_work_set_neutrals(gem_work* w, const double* nn, const double* Tn);
+/* host<->device copies of vs1i|vs2i|vs3i (which: 1,2,3); dir 0 host->device, 1 device->host */
+int gem_work_interface_vels(gem_work* w, int which, double* host, int dir);
+/* device pointer of the work array vs{which}i (which 1..3), of nn (4) or Tn (5) */
+double* gem_work_array(gem_work* w, int which);
+/* device pointer of the 1-element dt slot inside the work object */
+double* gem_work_dt(gem_work* w);
+
+/* ---- individual reference routines, device-resident ------------------------------ */
+/* multifluid.f90:179-233 conversions over the full ghosted arrays, all species */
+int gem_v12rhov1_dev(const gem_grid* g, const double* fluidvars, double* fluidauxvars, void* stream);
+int gem_T2rhoe_dev(const gem_grid* g, const double* fluidvars, double* fluidauxvars, void* stream);
+int gem_rhov12v1_dev(const gem_grid* g, double* fluidvars, const double* fluidauxvars, void* stream);
+int gem_rhoe2T_dev(const gem_grid* g, double* fluidvars, const double* fluidauxvars, void* stream);
+/* advec.f90:21-149 (single resident grid: every boundary is global) */
+int gem_set_global_boundaries_allspec_dev(const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                                          const gem_work* w, int lsp, void* stream);
+/* multifluid_mpi.f90:12-41 on one grid: only the x3 periodic self-wrap (mpihalo.f90:147-151) */
+int gem_halo_fluidvars_dev(const gem_grid* g, double* fluidvars, double* fluidauxvars, void* stream);
+int gem_halo_allparams_dev(const gem_grid* g, double* fluidvars, double* fluidauxvars, void* stream);
+/* advec.f90:155-229 */
+int gem_interface_vels_allspec_dev(const gem_grid* g, const double* fluidvars, gem_work* w, int lsp,
+                                   void* stream);
+/* advec.f90:233-381 via multifluid.f90:49-126: dim 1..3; which 0 mass (ns, 1..6),
+ * 1 momentum (rhovs1, 1..6, frank 1), 2 energy (rhoes, 1..7); dt is a device pointer */
+int gem_sweep_allspec_dev(const gem_grid* g, int dim, int which, double* fluidvars,
+                          double* fluidauxvars, const gem_work* w, const double* dt, void* stream);
+/* multifluid.f90:553-688; iparm 1 density, 2 velocity, 3 temperature */
+int gem_clean_param_dev(const gem_grid* g, int iparm, double* fluidvars, void* stream);
+/* multifluid.f90:309-342 with collisions.f90:162-199 and diffusion.f90:24-152.  The
+ * tridiagonal systems are eliminated without pivoting and the Dirichlet rows are exact
+ * (LAPACK's partial pivoting on those identity rows adds rounding of up to ~1e-9 relative
+ * in stiff columns).  Ghost cells: the x1 layers 0 and lx1+1 receive the Dirichlet
+ * values, then max(T,100) over every cell. */
+int gem_energy_diffusion_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars,
+                             const double* electrovars, const gem_work* w, const double* dt,
+                             void* stream);
+/* temporal_mpi.f90:86-167 dt_calc and the 1e-6 floor of dt_comm; writes *dt_out (device) */
+int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem_work* w,
+                    double* dt_out, void* stream);
+/* temporal.f90:12-49 cflcalc; writes *maxcfl_out (device) */
+int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, const double* dt,
+                   double* maxcfl_out, void* stream);
+
+/* ---- the fused fluid advance --------------------------------------------------------
+ * One call = the advection + diffusion subset of fluid_adv (app/main.f90:280-355,
+ * libgemini.cpp:155-210) with compression and sources excluded:
+ *   v12rhov1, T2rhoe, set_global_boundaries, halo, interface_vels, sweep3, sweep1, halo,
+ *   sweep2, rhov12v1, clean_param(1), clean_param(2), rhoe2T, clean_param(3),
+ *   energy_diffusion, clean_param(3), T2rhoe.
+ * Asynchronous on `stream`; dt is a device pointer (e.g. written by gem_dt_calc_dev).  Of
+ * the work arrays only the x1 boundary faces of vs1i are kept current (the only part read
+ * by the next step); gem_interface_vels_allspec_dev fills all faces. */
+int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                      const double* electrovars, gem_work* w, const double* dt, void* stream);
+
+/* The same step through host buffers: copies the three blocks to the device, runs
+ * gem_dt_calc_dev (if dt_inout < 0, else uses *dt_inout) and gem_fluid_adv_dev, copies the
+ * blocks back and synchronises.  Device staging buffers are allocated on first use and
+ * kept in the work object. */
+int gem_fluid_adv_host(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                       const double* electrovars, gem_work* w, double* dt_inout, void* stream);
+
+/* number of non-finite values in the interior of ns, vs1 and Ts (blocks until done) */
+int gem_check_finite(const gem_grid* g, const double* fluidvars, gem_work* w, long long* count,
+                     void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GEM_FLUID_H */

@@ -1,0 +1,76 @@
+"""Host-side logic without a GPU: grid/state generators and the C ABI library surface."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from gemini_b200 import _lib, build
+from gemini_b200 import grid as G
+from gemini_b200 import state as S
+
+
+def test_coord_diffs_definition():
+    x = np.cumsum(np.random.default_rng(0).uniform(1, 2, 14))
+    dx, xi, dxi = G.coord_diffs(x)
+    lx = x.size - 4
+    assert dx.size == lx + 3 and xi.size == lx + 1 and dxi.size == lx
+    assert np.array_equal(dx, x[1:] - x[:-1])
+    assert np.array_equal(xi, 0.5 * (x[1:lx + 2] + x[2:lx + 3]))
+
+
+def test_cartesian_grid():
+    g = G.cartesian_grid(12, 5, 4)
+    assert g.gridflag == 2 and g.unit_metrics and g.lnull == 0
+    assert g.h1.shape == (16, 9, 8) and g.h1.flags.f_contiguous
+    assert g.h2x1i.shape == (13, 5, 4) and g.h3x2i.shape == (12, 6, 4) and g.h1x3i.shape == (12, 5, 5)
+    gi = G.cartesian_grid(12, 5, 4, inverted=True)
+    assert gi.gridflag == 1
+
+
+def test_dipole_grid():
+    g = G.dipole_grid(48, 6, 4)
+    assert g.gridflag == 0 and g.lnull == 0
+    assert (g.h1 > 0).all() and (g.h2 > 0).all() and (g.h3 > 0).all()
+    alt = g.alt[2:-2, 2:-2, 2:-2]
+    assert alt.min() >= 80e3 - 1 and abs(alt[0, 0, 0] - 90e3) < 1.0
+    # metric factors do not depend on x3
+    assert np.array_equal(g.h1[:, :, 0], g.h1[:, :, -1])
+    gn = G.dipole_grid(48, 6, 4, q_extent=0.5)
+    assert gn.lnull > 0
+
+
+def test_dipole_rtheta_roundtrip():
+    q = np.array([-0.3, 0.0, 0.2])
+    p = np.array([1.5, 2.0, 3.0])
+    r, th = G.dipole_rtheta(q, p)
+    qq = (G.RE / r) ** 2 * np.cos(th)
+    pp = r / G.RE / np.sin(th) ** 2
+    assert np.allclose(qq, q, atol=1e-14) and np.allclose(pp, p, rtol=1e-14)
+
+
+def test_state_generator():
+    g = G.cartesian_grid(20, 4, 3)
+    st = S.init_state(g, seed=1)
+    ns = st.ns
+    assert (ns[..., :6] >= 1e6).all()
+    assert np.array_equal(ns[..., 6], ns[..., :6].sum(axis=-1))
+    assert (st.Ts >= 100).all()
+    assert st.nn.shape == (20, 4, 3, 3) and st.Tn.shape == (20, 4, 3)
+    st2 = S.init_state(g, seed=1)
+    assert np.array_equal(st.fluidvars, st2.fluidvars)
+
+
+def test_library_builds_and_exports_header_symbols():
+    """The C-ABI library loads without a GPU and exports every function include/*.h declares."""
+    try:
+        build.build()
+    except RuntimeError as e:  # no nvcc in this environment
+        if not os.path.exists(build.LIB):
+            pytest.skip(str(e))
+    L = ctypes.CDLL(build.LIB)
+    names = _lib.header_symbols()
+    assert len(names) > 40
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert _lib.lib().gem_version() >= 1
