@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the FP64 fluid advance (advection sweeps + TRBDF2 diffusion) on B200.
+
+Workload: the dipole grid 384 x 192 x 192 x 7 species (L-shells 1.2-3.0, MLON span 10 deg,
+seeded +-20 % lognormal perturbations), one step = dt_calc at CFL 0.5 followed by the fused
+fluid advance (v12rhov1 ... T2rhoe without compression / sources).  Metric: cell-species
+updates per second, lx1*lx2*lx3*7*steps / time / 1e9.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 runs under torchrun, one replica per GPU (the path has no data exchange:
+weak scaling); the time is the max over ranks.  --impl reference times the reference's
+algorithm on the host CPU (the C++ restatement of the Fortran, all host threads).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(kind="dipole", lx1=384, lx2=192, lx3=192, Lmin=1.2, Lmax=3.0, mlon_span_deg=10.0,
+                perturb=0.2, seed=1)
+METRIC = "fluid Gcell-species-steps/s"
+UNIT = "Gcell-species-steps/s"
+LSP = 7
+PHASES = ["dt_calc", "ghost_fill", "sweep_x3", "sweep_x1", "sweep_x2_epilogue", "ghost_epilogue", "diffusion"]
+
+
+def algorithmic_doubles_per_cell(unit_metrics: bool) -> dict:
+    """Minimum HBM traffic of each phase per interior cell, in 8-byte words: every input the
+    phase needs read once and every output written once.  A sweep reads 3 cell + 3 face
+    metric factors, dt_calc and the diffusion 3 cell factors; none on a unit-metric grid."""
+    ms = 0 if unit_metrics else 6
+    m3 = 0 if unit_metrics else 3
+    return {
+        "dt_calc": 28 + m3,                  # in: Ts, vs1, vs2, vs3 (7 species each)
+        "ghost_fill": 0,                     # boundary layers only
+        "sweep_x3": 28 + ms + 20,            # in: ns, vs1, Ts, vs3 (7); out: ns (6), rhovs1, rhoes (7)
+        "sweep_x1": 26 + ms + 19,            # in: ns, rhovs1 (6), rhoes, vs1 (7); out: the 19 swept
+        "sweep_x2_epilogue": 26 + ms + 27,   # in: ns, rhovs1 (6), rhoes, vs2 (7); out: ns, vs1, Ts (7), rhovs1 (6)
+        "ghost_epilogue": 0,                 # ghost cells only
+        "diffusion": 18 + m3 + 14,           # in: Ts, ns (7), nn (3), J1; out: Ts, rhoes (7)
+    }
+
+
+def build_problem(lx1, lx2, lx3, seed, perturb, kind="dipole"):
+    from gemini_b200 import grid as G
+    from gemini_b200 import state as S
+    if kind == "dipole":
+        g = G.dipole_grid(lx1, lx2, lx3, Lmin=WORKLOAD["Lmin"], Lmax=WORKLOAD["Lmax"],
+                          mlon_span_deg=WORKLOAD["mlon_span_deg"])
+    else:
+        g = G.cartesian_grid(lx1, lx2, lx3)
+    st = S.init_state(g, seed=seed, perturb=perturb)
+    return g, st
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv") \
+            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/gemini_b200_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001 -- no nvidia-smi
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:  # noqa: BLE001
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(lx1, lx2, lx3, target_seconds=12.0):
+    """The oracle (C++ restatement of the reference Fortran) on the host cores, all threads,
+    on an x3 slab of the workload grid; returns (cell-species-steps/s, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # checker/baseline only
+    threads = os.cpu_count() or 1
+    O.set_num_threads(threads)
+    slab = 4
+    while True:
+        g, st = build_problem(lx1, lx2, slab, WORKLOAD["seed"], WORKLOAD["perturb"])
+        t0 = time.perf_counter()
+        dt, _ = O.dt_calc(g, st, 0.5)
+        O.fluid_adv(g, st, dt)
+        el = time.perf_counter() - t0
+        if el * 2 > target_seconds or slab >= lx3:
+            break
+        slab = min(lx3, max(slab * 2, int(slab * target_seconds / max(el, 1e-3) / 2)))
+    nsteps = max(1, int(target_seconds / max(el, 1e-3)) - 1)
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        dt, _ = O.dt_calc(g, st, 0.5)
+        O.fluid_adv(g, st, dt)
+    el = time.perf_counter() - t0
+    value = lx1 * lx2 * slab * LSP * nsteps / el / 1e9
+    sample = (f"{nsteps} step(s) of dt_calc + fluid advance on a {lx1}x{lx2}x{slab} x3-slab of the "
+              f"{lx1}x{lx2}x{lx3} dipole workload, {threads} OpenMP threads, {el:.1f} s")
+    return value, threads, sample
+
+
+def dist_setup(n):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference algorithm on the host CPU (rank 0 only)."""
+    if rank != 0:
+        return None
+    w = WORKLOAD
+    vals = []
+    info = None
+    for _ in range(args.warmup):
+        cpu_baseline(w["lx1"], w["lx2"], w["lx3"], target_seconds=2.0)
+    for _ in range(args.steps):
+        v, threads, sample = cpu_baseline(w["lx1"], w["lx2"], w["lx3"], target_seconds=args.cpu_seconds)
+        vals.append(v)
+        info = (threads, sample)
+    value = float(np.median(vals))
+    threads, sample = info
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def config_dict(world):
+    w = WORKLOAD
+    return {"workload": f"plain FP64 dipole {w['lx1']}x{w['lx2']}x{w['lx3']} x 7 species, "
+                        "dt_calc (CFL 0.5) + fused fluid advance (advection sweeps x3,x1,x2 + TRBDF2 diffusion)",
+            "lx1": w["lx1"], "lx2": w["lx2"], "lx3": w["lx3"], "species": LSP, "grid": "closed dipole",
+            "L_shells": [w["Lmin"], w["Lmax"]], "mlon_span_deg": w["mlon_span_deg"], "perturb": w["perturb"],
+            "diffsolvetype": 2, "tcfl": 0.5, "parallelism": f"replicas x{world}",
+            "l2": "state ~7 GB per replica, larger than L2 (no flush between steps)"}
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    from gemini_b200 import _lib
+    from gemini_b200 import fluid as F
+
+    w = WORKLOAD
+    g, st = build_problem(w["lx1"], w["lx2"], w["lx3"], w["seed"] + rank, w["perturb"])
+    dg = F.DeviceGrid(g)
+    ds = F.DeviceState.from_host(dg, st.copy())
+    cfg = F.FluidCfg(st.Teinf, 2, 0.5)
+    stream = torch.cuda.current_stream()
+    L = _lib.lib()
+    ccfg = cfg.c()
+    import ctypes
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    gh = dg.handle
+    Fp, Ap, Ep = (ctypes.c_void_p(t.data_ptr()) for t in (ds.fluidvars, ds.fluidauxvars, ds.electrovars))
+    dtp = ctypes.c_void_p(ds.dt.data_ptr())
+
+    def step():
+        _lib.check(L.gem_dt_calc_dev(gh, 0.5, Fp, ds.work, dtp, sptr))
+        _lib.check(L.gem_fluid_adv_dev(ctypes.byref(ccfg), gh, Fp, Ap, Ep, ds.work, dtp, sptr))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    _lib.check(L.gem_work_phase_timing(ds.work, args.steps))
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(args.steps):
+        step()
+    end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = start.elapsed_time(end)
+    phase = np.zeros(8)
+    nph, nst = ctypes.c_int(0), ctypes.c_int(0)
+    _lib.check(L.gem_work_phase_times(ds.work, phase.ctypes.data_as(_lib._D), 8, ctypes.byref(nph),
+                                      ctypes.byref(nst)))
+    _lib.check(L.gem_work_phase_timing(ds.work, 0))
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    nonfinite = F.check_finite(ds)
+    cells = w["lx1"] * w["lx2"] * w["lx3"]
+    value = world * cells * LSP * args.steps / (ms_max / 1e3) / 1e9
+
+    # roofline of the dominant phase (algorithmic bytes / mean duration)
+    unit = g.unit_metrics
+    alg = algorithmic_doubles_per_cell(unit)
+    phase_ms = {PHASES[i]: float(phase[i]) for i in range(len(PHASES))}
+    dom = max((p for p in PHASES if alg.get(p, 0) > 0), key=lambda p: phase_ms[p])
+    alg_bytes = alg[dom] * 8 * cells
+    achieved = alg_bytes / (phase_ms[dom] / 1e3) / 1e9
+    peak, peak_src = measured_hbm_peak()
+    step_bytes = sum(alg[p] for p in PHASES) * 8 * cells
+    step_achieved = step_bytes / (ms_max / args.steps / 1e3) / 1e9
+    survey_bytes = 8 * (162 + (0 if unit else 21)) * cells
+
+    # end to end through the host-buffer entry point (state copied in and out each step)
+    e2e = None
+    if args.e2e_steps > 0:
+        h = st.copy()
+        pin = {}
+        for name in ("fluidvars", "fluidauxvars", "electrovars"):
+            a = getattr(h, name)
+            tpin = torch.from_numpy(a.ravel(order="K")).pin_memory()
+            pin[name] = tpin
+        dtv = ctypes.c_double(-1.0)
+        ptrs = [ctypes.c_void_p(pin[n].data_ptr()) for n in ("fluidvars", "fluidauxvars", "electrovars")]
+        for _ in range(1):
+            dtv.value = -1.0
+            _lib.check(L.gem_fluid_adv_host(ctypes.byref(ccfg), gh, *ptrs, ds.work, ctypes.byref(dtv), sptr))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_start.record(stream)
+        for _ in range(args.e2e_steps):
+            dtv.value = -1.0
+            _lib.check(L.gem_fluid_adv_host(ctypes.byref(ccfg), gh, *ptrs, ds.work, ctypes.byref(dtv), sptr))
+        e_end.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ems = e_start.elapsed_time(e_end)
+        te = torch.tensor([ems], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        ems = float(te.item())
+        ng = (w["lx1"] + 4) * (w["lx2"] + 4) * (w["lx3"] + 4)
+        h2d = ng * 8 * (5 * LSP + 2 * LSP + 9 + 7)
+        d2h = ng * 8 * (5 * LSP + 2 * LSP + 9) + 8
+        e2e = {"value": world * cells * LSP * args.e2e_steps / (ems / 1e3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "api": "gem_fluid_adv_host (host blocks, pinned)", "steps": args.e2e_steps,
+               "wall_s": wall}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, threads, sample = cpu_baseline(w["lx1"], w["lx2"], w["lx3"], args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+
+    launches_per_step = 2 + 3 + 3 + 1 + (1 if g.lnull > 0 else 0) + 1
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(world),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "step_achieved_GBs": step_achieved, "step_frac": step_achieved / peak,
+                     "step_algorithmic_bytes": step_bytes,
+                     "survey_algorithmic_bytes_per_step": survey_bytes,
+                     "survey_frac": survey_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak},
+        "phases_ms": phase_ms,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clocks,
+        "gpu_launches": launches_per_step * args.steps,
+        "nonfinite": nonfinite,
+    }
+    ds.close()
+    dg.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        line = run_reference(args, world, rank)
+        if line is not None:
+            print(json.dumps(line))
+        return
+    world, rank, local = dist_setup(args.gpus)
+    line = run_b200(args, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -70,6 +70,9 @@ _SIGS = [
     ("gem_fluid_adv_dev", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("gem_fluid_adv_host", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _D, _VP]),
     ("gem_check_finite", ctypes.c_int, [_VP, _VP, _VP, ctypes.POINTER(ctypes.c_longlong), _VP]),
+    ("gem_work_phase_timing", ctypes.c_int, [_VP, ctypes.c_int]),
+    ("gem_work_phase_times", ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]),
     ("gem_capi_bind_grid", None, [_VP]),
     ("gem_capi_set_error_mode", None, [ctypes.c_int]),
     ("gem_capi_last_status", ctypes.c_int, []),

@@ -75,7 +75,21 @@ struct gem_grid {
   std::vector<void*> allocs;
 };
 
+// Per-step CUDA events at the phase boundaries of dt_calc + the fused step (optional):
+// E0 dt_calc E1 ghost fill E2 sweep x3 E3 sweep x1 E4 sweep x2 E5 ghost epilogue E6
+// diffusion E7
+constexpr int NPHASE = 7;
+struct PhaseTimer {
+  int cap = 0;
+  long long step = 0;
+  std::vector<cudaEvent_t> ev;  // cap * (NPHASE + 1)
+  void record(int k, cudaStream_t st) {
+    if (cap > 0) cudaEventRecord(ev[(size_t)(step % cap) * (NPHASE + 1) + k], st);
+  }
+};
+
 struct gem_work {
+  PhaseTimer timer;
   int lx1, lx2, lx3;
   double *vs1i, *vs2i, *vs3i, *nn, *Tn, *dt;
   unsigned long long* acc;  // 32 slots: CFL maxima / counters
@@ -294,7 +308,10 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
   *out = nullptr;
   const Dims& d = g->dev.d;
   gem_work* w = new gem_work();
-  std::memset(w, 0, sizeof(*w));
+  w->vs1i = w->vs2i = w->vs3i = w->nn = w->Tn = w->dt = nullptr;
+  w->acc = nullptr;
+  w->F = w->A = w->E = nullptr;
+  w->nF = w->nA = w->nE = 0;
   w->lx1 = d.lx1;
   w->lx2 = d.lx2;
   w->lx3 = d.lx3;
@@ -329,6 +346,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
 
 int gem_work_destroy(gem_work* w) {
   if (!w) return GEM_OK;
+  for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);
   void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E};
   for (void* p : ps)
     if (p) cudaFree(p);
@@ -481,6 +499,7 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
                     void* stream) {
   if (check_grid(g) || !fluidvars || !w || !dt_out) return set_err(GEM_EINVAL, "null argument");
   cudaStream_t st = S(stream);
+  w->timer.record(0, st);
   GEM_CUDA(cudaMemsetAsync(w->acc, 0, 3 * LSP * sizeof(unsigned long long), st));
   Blocks B = blocks(g, const_cast<double*>(fluidvars), nullptr);
   const unsigned nb = grid_for(nci(g->dev.d), 256, 4);
@@ -491,6 +510,7 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
   GEM_LAUNCHED("k_dt_reduce");
   k_dt_finalize<<<1, 32, 0, st>>>(w->acc, tcfl, dt_out);
   GEM_LAUNCHED("k_dt_finalize");
+  w->timer.record(1, st);
   return GEM_OK;
 }
 
@@ -521,10 +541,12 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
   if (rc) return rc;
   cudaStream_t st = S(stream);
   Blocks B = blocks(g, fluidvars, fluidauxvars);
+  w->timer.record(1, st);
   // v12rhov1 + T2rhoe + set_global_boundaries + halo_fluidvars (the interior conversions
   // are folded into the x3 sweep)
   rc = launch_ghost_fill(g, B, w->vs1i, LSP, true, st);
   if (rc) return rc;
+  w->timer.record(2, st);
   SweepArgs a;
   a.G = g->dev;
   a.B = B;
@@ -533,8 +555,11 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
   a.dtp = dt;
   a.which = 0;
   if ((rc = launch_sweep(g, 3, true, a, LSP, st))) return rc;
+  w->timer.record(3, st);
   if ((rc = launch_sweep(g, 1, true, a, LSP, st))) return rc;
+  w->timer.record(4, st);
   if ((rc = launch_sweep(g, 2, true, a, LSP, st))) return rc;
+  w->timer.record(5, st);
   k_ghost_epilogue<<<grid_for(g->dev.d.ng, 256), 256, 0, st>>>(g->dev, B);
   GEM_LAUNCHED("k_ghost_epilogue");
   if (g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1)) {
@@ -552,7 +577,46 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
   d.Teinf = cfg->Teinf;
   d.solver = cfg->diffsolvetype;
   d.fused = 1;
-  return launch_diffusion(g, d, st);
+  w->timer.record(6, st);
+  rc = launch_diffusion(g, d, st);
+  if (rc) return rc;
+  w->timer.record(7, st);
+  if (w->timer.cap > 0) w->timer.step++;
+  return GEM_OK;
+}
+
+int gem_work_phase_timing(gem_work* w, int max_steps) {
+  if (!w || max_steps < 0) return set_err(GEM_EINVAL, "bad argument");
+  for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);
+  w->timer.ev.clear();
+  w->timer.cap = 0;
+  w->timer.step = 0;
+  if (max_steps == 0) return GEM_OK;
+  w->timer.ev.resize((size_t)max_steps * (NPHASE + 1));
+  for (auto& e : w->timer.ev) GEM_CUDA(cudaEventCreate(&e));
+  w->timer.cap = max_steps;
+  return GEM_OK;
+}
+
+int gem_work_phase_times(gem_work* w, double* ms, int nphase_max, int* nphase, int* nsteps) {
+  if (!w || !ms) return set_err(GEM_EINVAL, "bad argument");
+  const int ns = (int)std::min<long long>(w->timer.step, w->timer.cap);
+  const int np = std::min(nphase_max, NPHASE);
+  for (int p = 0; p < np; ++p) ms[p] = 0.0;
+  for (int k = 0; k < ns; ++k) {
+    const cudaEvent_t* e = &w->timer.ev[(size_t)k * (NPHASE + 1)];
+    GEM_CUDA(cudaEventSynchronize(e[NPHASE]));
+    for (int p = 0; p < np; ++p) {
+      float t = 0.f;
+      GEM_CUDA(cudaEventElapsedTime(&t, e[p], e[p + 1]));
+      ms[p] += t;
+    }
+  }
+  for (int p = 0; p < np; ++p) ms[p] = ns ? ms[p] / ns : 0.0;
+  if (nphase) *nphase = np;
+  if (nsteps) *nsteps = ns;
+  w->timer.step = 0;
+  return GEM_OK;
 }
 
 int gem_fluid_adv_host(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,

@@ -918,12 +918,20 @@ __global__ void k_ghost_epilogue(GridDev G, Blocks B) {
 // ======================================================================================
 // 7. Field-aligned heat diffusion (multifluid.f90:309-342; collisions.f90:162-199;
 //    diffusion.f90:24-152; PDEparabolic.f90:19-346).  One warp per (x1 column, species).
-//    Lane l owns the M contiguous cells 1+l*M .. l*M+M of the column.  Each tridiagonal
-//    system (TR half step, then BDF2; or one backward-Euler step) is solved by the
-//    partition method: every lane eliminates its block down and up in shared memory, the
-//    64-row interface system (2 rows per lane) is solved by parallel cyclic reduction with
-//    warp shuffles, and the block interiors are back-substituted.  The Dirichlet rows are
-//    identity rows, so the boundary values are exact.
+//    Lane l owns the M contiguous cells 1+l*M .. l*M+M of the column.
+//
+//    Coefficients: lambda, beta, C, D, B, Dh and every band entry / right-hand side are
+//    formed with the reference's operation order (PDEparabolic.f90:59-136, 150-210), so the
+//    banded system is bit-identical to the one the reference hands to dgbsv (T**(5/2) is the
+//    correctly rounded value; see pow25).
+//    Solve: each tridiagonal system is eliminated by the partition method -- every lane
+//    eliminates its block down and up in shared memory, the 64-row interface system (2 rows
+//    per lane) is solved by parallel cyclic reduction with warp shuffles, and the block
+//    interiors are back-substituted -- followed by one step of iterative refinement with a
+//    compensated (TwoSum/TwoProd) residual.  The Dirichlet rows are identity rows, so the
+//    boundary values are exact.  The result is the solution of the reference's discrete
+//    system to ~1e-15 relative; the TR half step of a stiff column (Crank-Nicolson part)
+//    amplifies plain double-precision solve error to ~1e-12, which the refinement removes.
 // ======================================================================================
 struct DiffArgs {
   GridDev G;
@@ -938,8 +946,10 @@ struct DiffArgs {
   int fused;   // 1: clean_param(3) + T2rhoe folded into the store
 };
 
-constexpr int DA_T = 0, DA_LO = 1, DA_UP = 2, DA_S = 3, DA_SS = 4, DA_IB = 5, DA_TT = 6, DA_R = 7;
-constexpr int DNA = 8;
+// shared-memory arrays per warp: inputs (T and the per-row conduction/advection factors),
+// the refinement copy, and the partition solver's four work arrays
+constexpr int DA_T = 0, DA_QP = 1, DA_QM = 2, DA_BQ = 3, DA_X = 4, DA_SS = 5, DA_IB = 6, DA_TT = 7, DA_R = 8;
+constexpr int DNA = 9;
 
 struct WarpMem {
   double* p;
@@ -949,7 +959,21 @@ struct WarpMem {
   }
 };
 
-// identity row (outside the system)
+// x**2.5 as x*x*sqrt(x) in double-double (fma for the exact product errors), rounded once:
+// correctly rounded except in vanishingly rare near-halfway cases.  The CPU checker
+// evaluates the same expression.
+__device__ __forceinline__ double pow25(double x) {
+  if (!(x > 0.0)) return pow(x, 2.5);
+  const double s = sqrt(x);
+  const double es = __fma_rn(-s, s, x);
+  const double sl = es / (2.0 * s);
+  const double x2 = x * x;
+  const double x2l = __fma_rn(x, x, -x2);
+  const double p = x2 * s;
+  const double pl = __fma_rn(x2, s, -p);
+  return p + (pl + (x2 * sl + x2l * s));
+}
+
 struct Row4 {
   double A, B, C, R;
 };
@@ -971,7 +995,7 @@ __device__ __forceinline__ Row4 shfl_up_row(const Row4& r, int delta, int lane) 
   o.B = __shfl_up_sync(0xffffffffu, r.B, delta);
   o.C = __shfl_up_sync(0xffffffffu, r.C, delta);
   o.R = __shfl_up_sync(0xffffffffu, r.R, delta);
-  if (lane < delta) o = Row4{0.0, 1.0, 0.0, 0.0};
+  if (lane < delta) o = Row4{0.0, 1.0, 0.0, 0.0};  // outside the system: identity row
   return o;
 }
 __device__ __forceinline__ Row4 shfl_down_row(const Row4& r, int delta, int lane) {
@@ -984,8 +1008,9 @@ __device__ __forceinline__ Row4 shfl_down_row(const Row4& r, int delta, int lane
   return o;
 }
 
-// Solve the lane-blocked system whose row k (of this lane) is produced by rowf(k, a,b,c,r).
-// The solution of row k is left in W.at(DA_R, k, lane).
+// Solve the lane-blocked system whose row k (of this lane) is rowf(k, a,b,c,r); rowf is
+// called for k = 1..M-1 (ascending) and then k = 0, and may read W.at(DA_R, k, lane) for
+// row k before this function overwrites it.  The solution of row k ends in DA_R.
 template <class RowF>
 __device__ void partition_solve(const WarpMem& W, int M, int lane, RowF rowf) {
   double a, b, c, r;
@@ -1032,7 +1057,6 @@ __device__ void partition_solve(const WarpMem& W, int M, int lane, RowF rowf) {
   }
   // parallel cyclic reduction on the 64 interface rows (z_{2l} = lo, z_{2l+1} = hi)
   {
-    // stride 1
     const Row4 prev_lo = shfl_up_row(hi, 1, lane);
     const Row4 next_hi = shfl_down_row(lo, 1, lane);
     const Row4 lo0 = lo, hi0 = hi;
@@ -1057,6 +1081,51 @@ __device__ void partition_solve(const WarpMem& W, int M, int lane, RowF rowf) {
   W.at(DA_R, M - 1, lane) = xl;
 }
 
+// exact-error accumulation for the refinement residual r - (a xm + b x + c xp)
+__device__ __forceinline__ double residual3(double r, double a, double xm, double b, double x, double c, double xp) {
+  const double p1 = a * xm, e1 = __fma_rn(a, xm, -p1);
+  const double p2 = b * x, e2 = __fma_rn(b, x, -p2);
+  const double p3 = c * xp, e3 = __fma_rn(c, xp, -p3);
+  double s = r, comp = 0.0;
+  const double v[3] = {-p1, -p2, -p3};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {  // TwoSum
+    const double t = s + v[q];
+    const double bp = t - s;
+    comp += (s - (t - bp)) + (v[q] - bp);
+    s = t;
+  }
+  return s + (comp - (e1 + e2 + e3));
+}
+
+// Solve with one refinement step; the solution ends in DA_R.
+template <class RowF>
+__device__ void refined_solve(const WarpMem& W, int M, int lane, RowF rowf) {
+  partition_solve(W, M, lane, rowf);
+  __syncwarp();
+  for (int k = 0; k < M; ++k) W.at(DA_X, k, lane) = W.at(DA_R, k, lane);
+  __syncwarp();
+  const double xprev = __shfl_up_sync(0xffffffffu, W.at(DA_X, M - 1, lane), 1);
+  const double xnext = __shfl_down_sync(0xffffffffu, W.at(DA_X, 0, lane), 1);
+  for (int k = 0; k < M; ++k) {
+    double a, b, c, r;
+    rowf(k, a, b, c, r);
+    const double xm = (k > 0) ? W.at(DA_X, k - 1, lane) : xprev;
+    const double xp = (k < M - 1) ? W.at(DA_X, k + 1, lane) : xnext;
+    W.at(DA_R, k, lane) = residual3(r, a, xm, b, W.at(DA_X, k, lane), c, xp);
+  }
+  __syncwarp();
+  auto rowres = [&](int k, double& a, double& b, double& c, double& r) {
+    double rr;
+    rowf(k, a, b, c, rr);
+    r = W.at(DA_R, k, lane);
+  };
+  partition_solve(W, M, lane, rowres);
+  __syncwarp();
+  for (int k = 0; k < M; ++k) W.at(DA_R, k, lane) = W.at(DA_X, k, lane) + W.at(DA_R, k, lane);
+  __syncwarp();
+}
+
 template <bool UNIT>
 __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
   extern __shared__ double smem[];
@@ -1075,11 +1144,11 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
     const int s = (int)(cs % LSP);
     const long long col = cs / LSP;
     const int i2 = (int)(col % d.lx2) + 1, i3 = (int)(col / d.lx2) + 1;
-    const double* Tcol = P.B.Ts(s) + gi(d, 0, i2, i3);  // Tcol[i] = T(i)
-    const double* ncol = P.B.ns(s) + gi(d, 0, i2, i3);
-    const long long m0 = gi(d, 0, i2, i3);
+    const long long m0 = gi(d, 0, i2, i3);  // m0 + i = cell (i, i2, i3)
+    const double* Tcol = P.B.Ts(s) + m0;
+    const double* ncol = P.B.ns(s) + m0;
     const double c0 = (c_gammas[s] - 1.0) / KB;
-    // ---- per-cell coefficients (thermal_conduct + diffusion_prep), into shared memory
+    // ---- thermal_conduct + diffusion_prep per cell: C -> DA_SS, D -> DA_IB, B -> DA_TT
     for (int k = 0; k < M; ++k) {
       const int i = 1 + lane * M + k;
       double T = 0.0, Cc = 0.0, Dc = 0.0, Bc = 0.0;
@@ -1088,16 +1157,15 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
         const double nv = ncol[i];
         const double h1v = ldm<UNIT>(G.h1, m0 + i), h2v = ldm<UNIT>(G.h2, m0 + i),
                      h3v = ldm<UNIT>(G.h3, m0 + i);
-        const double sq = sqrt(T);
-        const double T25 = T * T * sq;  // T**(5/2)
+        const double T25 = pow25(T);
         double lam;
         if (s < LSP - 1) {
           lam = c_tcoef[s] * T25;
         } else {
           const long long q = ci(d, i, i2, i3);
           const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
-          const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
-                           n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
+          const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sqrt(T) * (1 - 1.21e-4 * T) +
+                           n3 * 2.2e-16 * (1 + 3.6e-2 * sqrt(T));
           lam = ELCHRG * 100 * 7.7e5 * T25 / (1 + 3.22e4 * (T * T) / nv * X);
           Bc = 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i];  // beta (collisions.f90:197)
         }
@@ -1111,33 +1179,29 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
       W.at(DA_TT, k, lane) = Bc;
     }
     __syncwarp();
-    // ---- row coefficients lo, up, S (TR form: M(ll+4), M(ll+2), and the two conduction
-    // terms of the diagonal without the 1/2)
+    // ---- per-row conduction factors qm = C*Dh(i)/dx1i/dx1(i), qp = C*Dh(i+1)/dx1i/dx1(i+1)
+    // and advection factor bq = B/(dx1(i+1)+dx1(i)) (PDEparabolic.f90:70-80)
     const double Dprev = __shfl_up_sync(0xffffffffu, W.at(DA_IB, M - 1, lane), 1);
     const double Dnext = __shfl_down_sync(0xffffffffu, W.at(DA_IB, 0, lane), 1);
     for (int k = 0; k < M; ++k) {
       const int i = 1 + lane * M + k;
-      double lo = 0.0, up = 0.0, S = 0.0;
+      double qp = 0.0, qm = 0.0, bq = 0.0;
       if (i >= 2 && i <= n - 1) {
         const double Dm = (k > 0) ? W.at(DA_IB, k - 1, lane) : Dprev;
         const double Dc = W.at(DA_IB, k, lane);
         const double Dp = (k < M - 1) ? W.at(DA_IB, k + 1, lane) : Dnext;
-        const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);
-        const double Cc = W.at(DA_SS, k, lane), Bc = W.at(DA_TT, k, lane);
+        const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);  // PDEparabolic.f90:49
+        const double Cc = W.at(DA_SS, k, lane);
         const double dxm = __ldg(G.dx1 + i), dxp = __ldg(G.dx1 + i + 1), dxi = __ldg(G.dx1i + i - 1);
-        const double gm = Cc * Dhm / dxi / dxm;
-        const double gp = Cc * Dhp / dxi / dxp;
-        const double adv = Bc / (dxp + dxm);
-        lo = (-gm + adv) * 0.5;
-        up = (-gp - adv) * 0.5;
-        S = gp + gm;
+        qm = Cc * Dhm / dxi / dxm;
+        qp = Cc * Dhp / dxi / dxp;
+        bq = W.at(DA_TT, k, lane) / (dxp + dxm);
       }
-      W.at(DA_LO, k, lane) = lo;
-      W.at(DA_UP, k, lane) = up;
-      W.at(DA_S, k, lane) = S;
+      W.at(DA_QP, k, lane) = qp;
+      W.at(DA_QM, k, lane) = qm;
+      W.at(DA_BQ, k, lane) = bq;
     }
     __syncwarp();
-    // neighbour temperatures across lane blocks
     const double Tprev = __shfl_up_sync(0xffffffffu, W.at(DA_T, M - 1, lane), 1);
     const double Tnext = __shfl_down_sync(0xffffffffu, W.at(DA_T, 0, lane), 1);
     // Dirichlet values (diffusion.f90:54-79)
@@ -1153,67 +1217,64 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
       if (k >= M) return Tnext;
       return W.at(DA_T, k, lane);
     };
-    const double idt = 1.0 / dt;
+    // identity rows: Dirichlet rows 1 and lx1 (PDEparabolic.f90:59-63, 131-136) and padding
+    auto ident = [&](int i, double& a, double& b, double& c, double& r) -> bool {
+      if (i == 1) { a = 0; b = 1; c = 0; r = tmin; return true; }
+      if (i == n) { a = 0; b = 1; c = 0; r = tmax; return true; }
+      if (i > n) { a = 0; b = 1; c = 0; r = 0; return true; }
+      return false;
+    };
     if (P.solver == 2) {
-      const double two_dt = 1.0 / (dt / 2);
-      // TR half step
+      // TR half step (PDEparabolic.f90:66-127), A = E = 0
+      const double tr_d = 1 / (dt / 2);
       auto rowTR = [&](int k, double& a, double& b, double& c, double& r) {
         const int i = 1 + lane * M + k;
-        if (i == 1) { a = 0; b = 1; c = 0; r = tmin; return; }
-        if (i == n) { a = 0; b = 1; c = 0; r = tmax; return; }
-        if (i > n) { a = 0; b = 1; c = 0; r = 0; return; }
-        const double lo = W.at(DA_LO, k, lane), up = W.at(DA_UP, k, lane), S = W.at(DA_S, k, lane);
+        if (ident(i, a, b, c, r)) return;
+        const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
         const double Tc = W.at(DA_T, k, lane);
-        a = lo;
-        c = up;
-        b = two_dt + S * 0.5;
-        r = Tc * two_dt - lo * Tat(k - 1) - (S * 0.5) * Tc - up * Tat(k + 1);
+        a = -(qm / 2) + bq / 2;
+        b = tr_d + qp / 2 + qm / 2;
+        c = -(qp / 2) - bq / 2;
+        const double Pd = qp / 2 + qm / 2;
+        r = Tc / (dt / 2) - a * Tat(k - 1) - Pd * Tc - c * Tat(k + 1);
       };
-      partition_solve(W, M, lane, rowTR);
-      __syncwarp();
-      // BDF2 step; the TR solution sits in DA_R and is read before being overwritten
-      const double three_dt = 1.0 / (dt / 3);
-      auto rowBDF = [&](int k, double& a, double& b, double& c, double& r) {
-        const int i = 1 + lane * M + k;
-        if (i == 1) { a = 0; b = 1; c = 0; r = tmin; return; }
-        if (i == n) { a = 0; b = 1; c = 0; r = tmax; return; }
-        if (i > n) { a = 0; b = 1; c = 0; r = 0; return; }
-        const double lo = W.at(DA_LO, k, lane), up = W.at(DA_UP, k, lane), S = W.at(DA_S, k, lane);
-        a = 2 * lo;
-        c = 2 * up;
-        b = three_dt + S;
-        r = -1 / 3.0 * W.at(DA_T, k, lane) * three_dt + 4 / 3.0 * W.at(DA_R, k, lane) * three_dt;
-      };
-      // the BDF2 right-hand side needs TR at row k; keep a copy before the solve reuses DA_R
+      refined_solve(W, M, lane, rowTR);
+      // BDF2 right-hand side (PDEparabolic.f90:167-202) into DA_T; T is not needed after
       for (int k = 0; k < M; ++k) {
-        double a, b, c, r;
-        rowBDF(k, a, b, c, r);
-        W.at(DA_T, k, lane) = r;  // T is no longer needed: hold the BDF2 right-hand side
+        const int i = 1 + lane * M + k;
+        double r;
+        if (i == 1) r = tmin;
+        else if (i == n) r = tmax;
+        else if (i > n) r = 0;
+        else r = -(1 / 3.0 * W.at(DA_T, k, lane) / (dt / 3)) + 4 / 3.0 * W.at(DA_R, k, lane) / (dt / 3);
+        W.at(DA_T, k, lane) = r;
       }
       __syncwarp();
-      auto rowBDF2 = [&](int k, double& a, double& b, double& c, double& r) {
+      const double bdf_d = 1 / (dt / 3);
+      auto rowBDF = [&](int k, double& a, double& b, double& c, double& r) {
         const int i = 1 + lane * M + k;
         r = W.at(DA_T, k, lane);
         if (i == 1 || i >= n) { a = 0; b = 1; c = 0; return; }
-        a = 2 * W.at(DA_LO, k, lane);
-        c = 2 * W.at(DA_UP, k, lane);
-        b = three_dt + W.at(DA_S, k, lane);
+        const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
+        a = -qm + bq;
+        b = bdf_d + qp + qm;
+        c = -qp - bq;
       };
-      partition_solve(W, M, lane, rowBDF2);
+      refined_solve(W, M, lane, rowBDF);
     } else {
+      // backward Euler (PDEparabolic.f90:250-319)
+      const double be_d = 1 / dt;
       auto rowBE = [&](int k, double& a, double& b, double& c, double& r) {
         const int i = 1 + lane * M + k;
-        if (i == 1) { a = 0; b = 1; c = 0; r = tmin; return; }
-        if (i == n) { a = 0; b = 1; c = 0; r = tmax; return; }
-        if (i > n) { a = 0; b = 1; c = 0; r = 0; return; }
-        a = 2 * W.at(DA_LO, k, lane);
-        c = 2 * W.at(DA_UP, k, lane);
-        b = idt + W.at(DA_S, k, lane);
-        r = W.at(DA_T, k, lane) * idt;
+        if (ident(i, a, b, c, r)) return;
+        const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
+        a = -qm + bq;
+        b = be_d + qp + qm;
+        c = -qp - bq;
+        r = W.at(DA_T, k, lane) / dt;
       };
-      partition_solve(W, M, lane, rowBE);
+      refined_solve(W, M, lane, rowBE);
     }
-    __syncwarp();
     // ---- store: max(T,100) (multifluid.f90:340); fused: clean_param(3) and T2rhoe
     double* Tout = P.B.Ts(s) + m0;
     for (int k = 0; k < M; ++k) {

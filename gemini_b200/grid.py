@@ -130,7 +130,10 @@ def cartesian_grid(lx1: int, lx2: int, lx3: int, *, zmin: float = 80e3, zmax: fl
         return lo + d * np.arange(-2, lx + 2, dtype=np.float64)
 
     z = axis(lx1, zmin, zmax)
-    x1 = z[::-1].copy() if inverted else z
+    # the x1 coordinate always increases with the index; an inverted grid has the highest
+    # altitude at x1 index 1 (GEMINI's gridflag 1)
+    x1 = z
+    alt1 = z[::-1].copy() if inverted else z
     x2 = axis(lx2, -x2span / 2, x2span / 2)
     x3 = axis(lx3, -x3span / 2, x3span / 2)
     dx1, _, dx1i = coord_diffs(x1)
@@ -138,7 +141,7 @@ def cartesian_grid(lx1: int, lx2: int, lx3: int, *, zmin: float = 80e3, zmax: fl
     dx3, _, dx3i = coord_diffs(x3)
     g = (lx1 + 4, lx2 + 4, lx3 + 4)
     ones = lambda s: np.ones(s, dtype=np.float64, order="F")
-    alt = np.asfortranarray(np.broadcast_to(x1[:, None, None], g).copy())
+    alt = np.asfortranarray(np.broadcast_to(alt1[:, None, None], g).copy())
     nullpts = np.asfortranarray(alt[2:lx1 + 2, 2:lx2 + 2, 2:lx3 + 2] < 80e3)
     grid = Grid(lx1, lx2, lx3, _gridflag(alt, lx1), int(flagper), "cartesian",
                 x1, x2, x3, dx1, dx1i, dx2, dx2i, dx3, dx3i,

@@ -134,6 +134,15 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
 int gem_fluid_adv_host(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
                        const double* electrovars, gem_work* w, double* dt_inout, void* stream);
 
+/* Optional per-phase timing of gem_dt_calc_dev + gem_fluid_adv_dev with CUDA events
+ * recorded on the launching stream (no synchronisation inside the step).  Phases:
+ * 0 dt_calc, 1 ghost fill, 2 x3 sweep, 3 x1 sweep, 4 x2 sweep + epilogue, 5 ghost-cell
+ * epilogue, 6 diffusion.  gem_work_phase_timing(w, n) keeps events for up to n steps
+ * (0 turns it off); gem_work_phase_times waits for them, returns the mean milliseconds per
+ * step of each phase and restarts the count. */
+int gem_work_phase_timing(gem_work* w, int max_steps);
+int gem_work_phase_times(gem_work* w, double* ms, int nphase_max, int* nphase, int* nsteps);
+
 /* number of non-finite values in the interior of ns, vs1 and Ts (blocks until done) */
 int gem_check_finite(const gem_grid* g, const double* fluidvars, gem_work* w, long long* count,
                      void* stream);

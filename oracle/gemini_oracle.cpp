@@ -709,6 +709,27 @@ namespace {
 // the reference disagree by that much).
 int g_diff_solver = 0;
 
+// T**(5/2) (collisions.f90:187,189).  Mode 0: the C library pow, as the Fortran calls it
+// (glibc's pow is not correctly rounded everywhere: ~1 in 1200 arguments in 1e2..4e4 differ
+// by 1 ulp from the correctly rounded value).  Mode 1: x^2 * sqrt(x) evaluated in
+// double-double with fma and rounded once -- the correctly rounded value except in
+// vanishingly rare near-halfway cases; the GPU kernels evaluate the same expression.
+int g_pow_mode = 0;
+
+double pow25_dd(double x) {
+  if (!(x > 0.0)) return std::pow(x, 2.5);
+  const double s = std::sqrt(x);
+  const double es = std::fma(-s, s, x);   // x - s*s exactly
+  const double sl = es / (2.0 * s);       // sqrt(x) ~ s + sl
+  const double x2 = x * x;
+  const double x2l = std::fma(x, x, -x2); // x*x = x2 + x2l exactly
+  const double p = x2 * s;
+  const double pl = std::fma(x2, s, -p);  // x2*s = p + pl exactly
+  return p + (pl + (x2 * sl + x2l * s));
+}
+
+inline double pow25(double x) { return g_pow_mode == 1 ? pow25_dd(x) : std::pow(x, 2.5); }
+
 // Tridiagonal band matrix in dgbsv storage (ldab 7, kl=ku=2; only the diagonal and the
 // first sub/super diagonals are non-zero), solved by Thomas in long double.
 void band_solve_extended(int n, const double* M, double* b) {
@@ -916,14 +937,14 @@ int ora_energy_diffusion(const ora_grid* G, const double* ns, double* Ts, const 
           const long long k = X.c(i1, i2, i3), q = X.g(i1, i2, i3);
           const double t = T[q];
           if (s < LSP - 1) {
-            lam[k] = K.thermal_coeff[s] * std::pow(t, 2.5);
+            lam[k] = K.thermal_coeff[s] * pow25(t);
             beta[k] = 0.0;
           } else {
             const double n1 = nn[k], n2 = nn[nc + k], n3 = nn[2 * nc + k];
             const double X3 = n1 * 1.1e-16 * (1 + 5.7e-4 * t) +
                               n2 * 2.82e-17 * std::sqrt(t) * (1 - 1.21e-4 * t) +
                               n3 * 2.2e-16 * (1 + 3.6e-2 * std::sqrt(t));
-            lam[k] = elchrg * 100 * 7.7e5 * std::pow(t, 2.5) / (1 + 3.22e4 * (t * t) / n[q] * X3);
+            lam[k] = elchrg * 100 * 7.7e5 * pow25(t) / (1 + 3.22e4 * (t * t) / n[q] * X3);
             beta[k] = 5.0 / 2 * kB / elchrg * J1[q];
           }
           // diffusion_prep (A = E = 0)
@@ -1057,6 +1078,8 @@ int ora_fluid_adv(const ora_grid* G, double* fluidvars, double* fluidauxvars, co
 }
 
 void ora_set_diffusion_solver(int mode) { g_diff_solver = mode; }
+void ora_set_pow_mode(int mode) { g_pow_mode = mode; }
+double ora_pow25(double x) { return pow25(x); }
 
 int ora_num_threads(void) {
 #ifdef _OPENMP

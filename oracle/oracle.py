@@ -78,6 +78,10 @@ def lib():
         L.ora_fluid_adv.restype = ctypes.c_int
         L.ora_constants.argtypes = [_D, _D, _D, _D]
         L.ora_num_threads.restype = ctypes.c_int
+        L.ora_set_diffusion_solver.argtypes = [ctypes.c_int]
+        L.ora_set_pow_mode.argtypes = [ctypes.c_int]
+        L.ora_pow25.argtypes = [ctypes.c_double]
+        L.ora_pow25.restype = ctypes.c_double
         L.ora_set_num_threads.argtypes = [ctypes.c_int]
         L.ora_advec1D_MC_curv.argtypes = [_D, _D, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, _D]
         _lib = L
@@ -108,6 +112,25 @@ class _GridHandle:
     @property
     def ref(self):
         return ctypes.byref(self.s)
+
+
+def set_diffusion_solver(mode: int) -> None:
+    """0: LAPACK dgbsv restated (default); 1: extended-precision solve of the same system."""
+    lib().ora_set_diffusion_solver(int(mode))
+
+
+def set_pow_mode(mode: int) -> None:
+    """0: libm pow(T, 2.5) as the Fortran calls it (default); 1: correctly rounded T**2.5."""
+    lib().ora_set_pow_mode(int(mode))
+
+
+def set_exact_dependencies(on: bool) -> None:
+    set_diffusion_solver(1 if on else 0)
+    set_pow_mode(1 if on else 0)
+
+
+def pow25(x: float) -> float:
+    return float(lib().ora_pow25(float(x)))
 
 
 def set_num_threads(n: int) -> None:

@@ -1,6 +1,5 @@
 """The CPU oracle pinned to the reference's own tests and to LAPACK, plus oracle-side
 properties (no GPU needed)."""
-import ctypes
 import json
 import os
 
@@ -107,14 +106,12 @@ def test_extended_solver_vs_lapack_spread():
     st = S.init_state(g, seed=4, perturb=0.2)
     a, b = st.copy(), st.copy()
     dt, _ = O.dt_calc(g, st, 0.5)
-    L = O.lib()
-    L.ora_set_diffusion_solver.argtypes = [ctypes.c_int]
     try:
-        L.ora_set_diffusion_solver(0)
+        O.set_diffusion_solver(0)
         O.energy_diffusion(g, a, dt)
-        L.ora_set_diffusion_solver(1)
+        O.set_diffusion_solver(1)
         O.energy_diffusion(g, b, dt)
     finally:
-        L.ora_set_diffusion_solver(0)
+        O.set_diffusion_solver(0)
     rel = np.max(np.abs(a.Ts - b.Ts) / b.Ts)
     assert rel < 1e-8
