@@ -123,33 +123,49 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(lx1, lx2, lx3, target_seconds=12.0):
+class CpuSample:
     """The oracle (C++ restatement of the reference Fortran) on the host cores, all threads,
-    on an x3 slab of the workload grid; returns (cell-species-steps/s, description)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O  # checker/baseline only
-    threads = os.cpu_count() or 1
-    O.set_num_threads(threads)
-    slab = 4
-    while True:
-        g, st = build_problem(lx1, lx2, slab, WORKLOAD["seed"], WORKLOAD["perturb"])
+    on an x3 slab of the workload grid sized so one step takes about `step_seconds`."""
+
+    def __init__(self, lx1, lx2, lx3, step_seconds=4.0):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O  # checker / CPU baseline only
+        self.O = O
+        self.threads = os.cpu_count() or 1
+        O.set_num_threads(self.threads)
+        self.lx1, self.lx2, self.lx3 = lx1, lx2, lx3
+        slab, el = 2, None
+        while True:
+            g, st = build_problem(lx1, lx2, slab, WORKLOAD["seed"], WORKLOAD["perturb"])
+            el = self._one(g, st)
+            if el * 1.5 > step_seconds or slab >= lx3:
+                break
+            slab = min(lx3, max(slab * 2, int(slab * step_seconds / max(el, 1e-3))))
+        self.g, self.st, self.slab = g, st, slab
+
+    def _one(self, g, st):
         t0 = time.perf_counter()
-        dt, _ = O.dt_calc(g, st, 0.5)
-        O.fluid_adv(g, st, dt)
-        el = time.perf_counter() - t0
-        if el * 2 > target_seconds or slab >= lx3:
-            break
-        slab = min(lx3, max(slab * 2, int(slab * target_seconds / max(el, 1e-3) / 2)))
-    nsteps = max(1, int(target_seconds / max(el, 1e-3)) - 1)
+        dt, _ = self.O.dt_calc(g, st, 0.5)
+        self.O.fluid_adv(g, st, dt)
+        return time.perf_counter() - t0
+
+    def step(self) -> float:
+        """One timed oracle step; returns cell-species-steps/s."""
+        el = self._one(self.g, self.st)
+        return self.lx1 * self.lx2 * self.slab * LSP / el / 1e9
+
+    def describe(self, nsteps, seconds):
+        return (f"{nsteps} step(s) of dt_calc + fluid advance on a {self.lx1}x{self.lx2}x{self.slab} x3-slab "
+                f"of the {self.lx1}x{self.lx2}x{self.lx3} dipole workload, {self.threads} OpenMP threads, "
+                f"{seconds:.1f} s")
+
+
+def cpu_baseline(lx1, lx2, lx3, target_seconds=15.0):
+    cs = CpuSample(lx1, lx2, lx3, step_seconds=target_seconds / 4)
     t0 = time.perf_counter()
-    for _ in range(nsteps):
-        dt, _ = O.dt_calc(g, st, 0.5)
-        O.fluid_adv(g, st, dt)
+    vals = [cs.step() for _ in range(3)]
     el = time.perf_counter() - t0
-    value = lx1 * lx2 * slab * LSP * nsteps / el / 1e9
-    sample = (f"{nsteps} step(s) of dt_calc + fluid advance on a {lx1}x{lx2}x{slab} x3-slab of the "
-              f"{lx1}x{lx2}x{lx3} dipole workload, {threads} OpenMP threads, {el:.1f} s")
-    return value, threads, sample
+    return float(np.median(vals)), cs.threads, cs.describe(3, el)
 
 
 def dist_setup(n):
@@ -169,26 +185,27 @@ def dist_setup(n):
 
 
 def run_reference(args, world, rank):
-    """--impl reference: the reference algorithm on the host CPU (rank 0 only)."""
+    """--impl reference: the reference algorithm on the host CPU (rank 0 only).  Each step is
+    one oracle step on a bounded x3-slab of the workload grid."""
     if rank != 0:
         return None
     w = WORKLOAD
-    vals = []
-    info = None
+    per_step = min(args.cpu_seconds / 3, 150.0 / max(args.steps + args.warmup, 1))
+    cs = CpuSample(w["lx1"], w["lx2"], w["lx3"], step_seconds=per_step)
     for _ in range(args.warmup):
-        cpu_baseline(w["lx1"], w["lx2"], w["lx3"], target_seconds=2.0)
-    for _ in range(args.steps):
-        v, threads, sample = cpu_baseline(w["lx1"], w["lx2"], w["lx3"], target_seconds=args.cpu_seconds)
-        vals.append(v)
-        info = (threads, sample)
+        cs.step()
+    t0 = time.perf_counter()
+    vals = [cs.step() for _ in range(args.steps)]
+    el = time.perf_counter() - t0
     value = float(np.median(vals))
-    threads, sample = info
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * w["lx1"] * w["lx2"] * w["lx3"] * LSP / (value * 1e9),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_dict(world),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cs.threads, "kind": "port",
+                         "sample": cs.describe(args.steps, el)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
@@ -352,7 +369,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--lx", type=int, nargs=3, default=None, metavar=("LX1", "LX2", "LX3"),
+                    help="override the grid size (profiling runs on a smaller case)")
     args = ap.parse_args()
+    if args.lx:
+        WORKLOAD.update(lx1=args.lx[0], lx2=args.lx[1], lx3=args.lx[2])
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))

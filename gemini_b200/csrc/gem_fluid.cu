@@ -135,15 +135,24 @@ int check_step(const gem_grid* g) {
 template <int DIM, bool FUSED>
 int launch_sweep_t(const gem_grid* g, SweepArgs a, int nsp, cudaStream_t st) {
   const Dims& d = g->dev.d;
-  const int lxa = (DIM == 1) ? d.lx2 : d.lx1;
-  const int lxb = (DIM == 3) ? d.lx2 : d.lx3;
   dim3 block(32, nsp);
-  dim3 grid((lxa + 31) / 32, lxb);
+  if (DIM == 1) {
+    // one warp per (x1 column, species)
+    dim3 grid(d.lx2, d.lx3);
+    if (g->dev.unit)
+      k_sweep_x1<true, FUSED><<<grid, block, 0, st>>>(a);
+    else
+      k_sweep_x1<false, FUSED><<<grid, block, 0, st>>>(a);
+    GEM_LAUNCHED("k_sweep_x1");
+    return GEM_OK;
+  }
+  // one thread per (x2 or x3 line, species), 32 adjacent x1 per warp
+  dim3 grid((d.lx1 + 31) / 32, (DIM == 3) ? d.lx2 : d.lx3);
   if (g->dev.unit)
-    k_sweep<DIM, true, FUSED><<<grid, block, 0, st>>>(a);
+    k_sweep_march<DIM == 3 ? 3 : 2, true, FUSED><<<grid, block, 0, st>>>(a);
   else
-    k_sweep<DIM, false, FUSED><<<grid, block, 0, st>>>(a);
-  GEM_LAUNCHED("k_sweep");
+    k_sweep_march<DIM == 3 ? 3 : 2, false, FUSED><<<grid, block, 0, st>>>(a);
+  GEM_LAUNCHED("k_sweep_march");
   return GEM_OK;
 }
 
@@ -231,6 +240,7 @@ int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
   G.unit = desc->unit_metrics ? 1 : 0;
   const size_t ng = (size_t)G.d.ng;
   int rc = GEM_OK;
+  G.c3 = G.d.s3;
   auto cp = [&](const double* h, size_t n, const double** o) {
     if (rc != GEM_OK) return;
     if (!h) {
@@ -239,26 +249,106 @@ int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
     }
     rc = dev_copy(h, n, o, g->allocs);
   };
-  cp(desc->dx1, lx1 + 3, &G.dx1);
-  cp(desc->dx1i, lx1, &G.dx1i);
-  cp(desc->dx2, lx2 + 3, &G.dx2);
-  cp(desc->dx2i, lx2, &G.dx2i);
-  cp(desc->dx3, lx3 + 3, &G.dx3);
-  cp(desc->dx3i, lx3, &G.dx3i);
-  cp(desc->h1, ng, &G.h1);
-  cp(desc->h2, ng, &G.h2);
-  cp(desc->h3, ng, &G.h3);
   const size_t n1 = (size_t)(lx1 + 1) * lx2 * lx3, n2 = (size_t)lx1 * (lx2 + 1) * lx3,
                n3 = (size_t)lx1 * lx2 * (lx3 + 1);
-  cp(desc->h1x1i, n1, &G.h1x1i);
-  cp(desc->h2x1i, n1, &G.h2x1i);
-  cp(desc->h3x1i, n1, &G.h3x1i);
-  cp(desc->h1x2i, n2, &G.h1x2i);
-  cp(desc->h2x2i, n2, &G.h2x2i);
-  cp(desc->h3x2i, n2, &G.h3x2i);
-  cp(desc->h1x3i, n3, &G.h1x3i);
-  cp(desc->h2x3i, n3, &G.h2x3i);
-  cp(desc->h3x3i, n3, &G.h3x3i);
+  const double* need[] = {desc->dx1, desc->dx1i, desc->dx2, desc->dx2i, desc->dx3, desc->dx3i,
+                          desc->h1, desc->h2, desc->h3, desc->h1x1i, desc->h2x1i, desc->h3x1i,
+                          desc->h1x2i, desc->h2x2i, desc->h3x2i, desc->h1x3i, desc->h2x3i, desc->h3x3i};
+  for (const double* p : need)
+    if (!p) rc = set_err(GEM_EINVAL, "missing grid array");
+  // 1-D tables per direction: dx, dx(j)+dx(j+1), dxi and their reciprocals
+  const double* dxs_in[3] = {desc->dx1, desc->dx2, desc->dx3};
+  const double* dxi_in[3] = {desc->dx1i, desc->dx2i, desc->dx3i};
+  const int lxs[3] = {lx1, lx2, lx3};
+  for (int dd = 0; dd < 3 && rc == GEM_OK; ++dd) {
+    const int l = lxs[dd];
+    std::vector<double> dx(dxs_in[dd], dxs_in[dd] + l + 3), ydx(l + 3), dxs(l + 2), ydxs(l + 2),
+        dxi(dxi_in[dd], dxi_in[dd] + l), ydxi(l);
+    for (int j = 0; j < l + 3; ++j) ydx[j] = 1.0 / dx[j];
+    for (int j = 0; j < l + 2; ++j) {
+      dxs[j] = dx[j] + dx[j + 1];
+      ydxs[j] = 1.0 / dxs[j];
+    }
+    for (int j = 0; j < l; ++j) ydxi[j] = 1.0 / dxi[j];
+    Line1D& L = G.L[dd];
+    cp(dx.data(), dx.size(), &L.dx);
+    cp(ydx.data(), ydx.size(), &L.ydx);
+    cp(dxs.data(), dxs.size(), &L.dxs);
+    cp(ydxs.data(), ydxs.size(), &L.ydxs);
+    cp(dxi.data(), dxi.size(), &L.dxi);
+    cp(ydxi.data(), ydxi.size(), &L.ydxi);
+  }
+  // Metric tables.  When no metric factor varies along x3 (checked bit for bit over the
+  // interior x3 range, the only one the kernels read), one x3 slice is stored and the x3
+  // strides are 0, so the tables of a large grid stay resident in L2.
+  const long long s2 = G.d.s2, s3 = G.d.s3;
+  bool inv = lx3 > 1 && rc == GEM_OK && !G.unit;
+  auto same_x3 = [&](const double* a, long long t3, long long inner, int i3lo, int i3hi) {
+    for (int i3 = i3lo + 1; i3 <= i3hi; ++i3)
+      if (std::memcmp(a + t3 * (i3 - i3lo), a, sizeof(double) * inner) != 0) return false;
+    return true;
+  };
+  if (inv) {
+    const long long inner_c = s2 * (lx2 + 4);
+    for (const double* h : {desc->h1, desc->h2, desc->h3}) inv = inv && same_x3(h + s3 * 2, s3, inner_c, 1, lx3);
+    const long long in1 = (long long)(lx1 + 1) * lx2, in2 = (long long)lx1 * (lx2 + 1), in3 = (long long)lx1 * lx2;
+    for (const double* f : {desc->h1x1i, desc->h2x1i, desc->h3x1i}) inv = inv && same_x3(f, in1, in1, 1, lx3);
+    for (const double* f : {desc->h1x2i, desc->h2x2i, desc->h3x2i}) inv = inv && same_x3(f, in2, in2, 1, lx3);
+    for (const double* f : {desc->h1x3i, desc->h2x3i, desc->h3x3i}) inv = inv && same_x3(f, in3, in3, 1, lx3 + 1);
+  }
+  G.c3 = inv ? 0 : s3;
+  if (rc == GEM_OK && !G.unit) {
+    // cell tables (ghosted layout; one slice at ghosted x3 index 2 when invariant)
+    const size_t ncell = inv ? (size_t)(s2 * (lx2 + 4)) : ng;
+    const size_t off = inv ? (size_t)(s3 * 2) : 0;
+    std::vector<double> h1(desc->h1 + off, desc->h1 + off + ncell), h2(desc->h2 + off, desc->h2 + off + ncell),
+        h3(desc->h3 + off, desc->h3 + off + ncell), a0(ncell), a1(ncell), y0(ncell), y1(ncell), yh1(ncell);
+    for (size_t k = 0; k < ncell; ++k) {
+      a0[k] = h1[k] * h2[k] * h3[k];          // advec.f90:312 (frank 0)
+      a1[k] = h1[k] * h1[k] * h2[k] * h3[k];  // advec.f90:310 (frank 1)
+      y0[k] = 1.0 / a0[k];
+      y1[k] = 1.0 / a1[k];
+      yh1[k] = 1.0 / h1[k];
+    }
+    cp(h1.data(), ncell, &G.h1);
+    cp(h2.data(), ncell, &G.h2);
+    cp(h3.data(), ncell, &G.h3);
+    cp(yh1.data(), ncell, &G.yh1);
+    cp(a0.data(), ncell, &G.ha1_0);
+    cp(a1.data(), ncell, &G.ha1_1);
+    cp(y0.data(), ncell, &G.yha1_0);
+    cp(y1.data(), ncell, &G.yha1_1);
+    // face tables: sweep x1 uses h2x1i*h3x1i and h1x1i, x2 h1x2i*h3x2i and h2x2i, x3
+    // h1x3i*h2x3i and h3x3i (advec.f90:302-304, 333-340, 369-376)
+    struct Fam {
+      const double *ha, *hb, *hc;
+      long long e1, e2, e3;  // extents
+    } fam[3] = {{desc->h2x1i, desc->h3x1i, desc->h1x1i, lx1 + 1, lx2, lx3},
+                {desc->h1x2i, desc->h3x2i, desc->h2x2i, lx1, lx2 + 1, lx3},
+                {desc->h1x3i, desc->h2x3i, desc->h3x3i, lx1, lx2, lx3 + 1}};
+    for (int dd = 0; dd < 3 && rc == GEM_OK; ++dd) {
+      const Fam& f = fam[dd];
+      const size_t nfc = inv ? (size_t)(f.e1 * f.e2) : (size_t)(f.e1 * f.e2 * f.e3);
+      std::vector<double> p0(nfc), p1(nfc), hc(f.hc, f.hc + nfc), yhc(nfc);
+      for (size_t k = 0; k < nfc; ++k) {
+        p0[k] = f.ha[k] * f.hb[k];
+        p1[k] = f.ha[k] * f.ha[k] * f.hb[k];
+        yhc[k] = 1.0 / hc[k];
+      }
+      FaceTab& T = G.F[dd];
+      T.t1 = 1;
+      T.t2 = f.e1;
+      T.t3 = inv ? 0 : f.e1 * f.e2;
+      cp(p0.data(), nfc, &T.ha2i0);
+      cp(p1.data(), nfc, &T.ha2i1);
+      cp(hc.data(), nfc, &T.hc);
+      cp(yhc.data(), nfc, &T.yhc);
+    }
+  } else if (rc == GEM_OK) {
+    // unit metrics: the kernels read no metric table
+    G.h1 = G.h2 = G.h3 = G.yh1 = G.ha1_0 = G.ha1_1 = G.yha1_0 = G.yha1_1 = nullptr;
+    for (int dd = 0; dd < 3; ++dd) G.F[dd] = FaceTab{nullptr, nullptr, nullptr, nullptr, 1, 0, 0};
+  }
   g->lnull = 0;
   G.has_null = 0;
   G.nullpts = nullptr;
@@ -504,9 +594,9 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
   Blocks B = blocks(g, const_cast<double*>(fluidvars), nullptr);
   const unsigned nb = grid_for(nci(g->dev.d), 256, 4);
   if (g->dev.unit)
-    k_dt_reduce<true><<<nb, 256, 0, st>>>(g->dev, B, w->acc, nullptr, 0);
+    k_dt_reduce<true, 0><<<nb, 256, 0, st>>>(g->dev, B, w->acc, nullptr);
   else
-    k_dt_reduce<false><<<nb, 256, 0, st>>>(g->dev, B, w->acc, nullptr, 0);
+    k_dt_reduce<false, 0><<<nb, 256, 0, st>>>(g->dev, B, w->acc, nullptr);
   GEM_LAUNCHED("k_dt_reduce");
   k_dt_finalize<<<1, 32, 0, st>>>(w->acc, tcfl, dt_out);
   GEM_LAUNCHED("k_dt_finalize");
@@ -522,9 +612,9 @@ int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, cons
   Blocks B = blocks(g, const_cast<double*>(fluidvars), nullptr);
   const unsigned nb = grid_for(nci(g->dev.d), 256, 4);
   if (g->dev.unit)
-    k_dt_reduce<true><<<nb, 256, 0, st>>>(g->dev, B, w->acc + 24, dt, 1);
+    k_dt_reduce<true, 1><<<nb, 256, 0, st>>>(g->dev, B, w->acc + 24, dt);
   else
-    k_dt_reduce<false><<<nb, 256, 0, st>>>(g->dev, B, w->acc + 24, dt, 1);
+    k_dt_reduce<false, 1><<<nb, 256, 0, st>>>(g->dev, B, w->acc + 24, dt);
   GEM_LAUNCHED("k_dt_reduce");
   k_maxcfl_finalize<<<1, 32, 0, st>>>(w->acc + 24, maxcfl_out);
   GEM_LAUNCHED("k_maxcfl_finalize");

@@ -29,6 +29,10 @@ constexpr double MINDENSDIV = 1.0e-5;
 // phys_consts.in.f90:43-53; collisions.f90:51-53 (default-REAL literals widened)
 __constant__ double c_ms[LSP] = {16.0 * AMU, 30.0 * AMU, 28.0 * AMU, 32.0 * AMU,
                                  14.0 * AMU, 1.0 * AMU,  5.485799090e-4 * AMU};
+// correctly rounded reciprocals of the masses (constant-folded in IEEE double)
+__constant__ double c_yms[LSP] = {1.0 / (16.0 * AMU), 1.0 / (30.0 * AMU), 1.0 / (28.0 * AMU),
+                                  1.0 / (32.0 * AMU), 1.0 / (14.0 * AMU), 1.0 / (1.0 * AMU),
+                                  1.0 / (5.485799090e-4 * AMU)};
 __constant__ double c_qs[LSP] = {1.0 * ELCHRG, 1.0 * ELCHRG, 1.0 * ELCHRG, 1.0 * ELCHRG,
                                  1.0 * ELCHRG, 1.0 * ELCHRG, -1.0 * ELCHRG};
 __constant__ double c_gammas[LSP] = {5.0 / 3, 7.0 / 5, 7.0 / 5, 7.0 / 5, 5.0 / 3, 5.0 / 3, 5.0 / 3};
@@ -75,22 +79,61 @@ __device__ __forceinline__ long long f3i(const Dims& d, int i1, int i2, int i3) 
 }
 __host__ __device__ __forceinline__ long long nf3(const Dims& d) { return (long long)d.lx1 * d.lx2 * (d.lx3 + 1); }
 
+// 1-D tables of one sweep direction (meshobj.f90:356-389 differences and their correctly
+// rounded reciprocals, for the exact reciprocal-corrected division mdiv below)
+struct Line1D {
+  const double *dx, *ydx;    // dx(j), j = 0..l+2, at [j]
+  const double *dxs, *ydxs;  // dx(j) + dx(j+1), j = 0..l+1, at [j]
+  const double *dxi, *ydxi;  // dxi(j), j = 1..l, at [j-1]
+};
+
+// face tables of one sweep direction: ha2i for frank 0 and 1, the advected-direction metric
+// h1i and its reciprocal (advec.f90:302-304, 333-340, 369-376).  Face (i1,i2,i3) of the
+// family is at (i1-1)*t1 + (i2-1)*t2 + (i3-1)*t3.
+struct FaceTab {
+  const double *ha2i0, *ha2i1, *hc, *yhc;
+  long long t1, t2, t3;
+};
+
 struct GridDev {
   Dims d;
   int gridflag, flagper, unit, has_null;
-  const double *dx1, *dx1i, *dx2, *dx2i, *dx3, *dx3i;
-  const double *h1, *h2, *h3;
-  const double *h1x1i, *h2x1i, *h3x1i;
-  const double *h1x2i, *h2x2i, *h3x2i;
-  const double *h1x3i, *h2x3i, *h3x3i;
+  long long c3;  // x3 stride of the cell metric tables: d.s3, or 0 when they do not vary in x3
+  Line1D L[3];
+  const double *h1, *h2, *h3, *yh1;               // cell metric factors (ghosted), 1/h1
+  const double *ha1_0, *ha1_1, *yha1_0, *yha1_1;  // h1*h2*h3, h1*h1*h2*h3 and reciprocals
+  FaceTab F[3];
   const unsigned char* nullpts;
 };
+
+// cell metric index (ghosted indices; x3 stride 0 for x3-invariant metrics)
+__device__ __forceinline__ long long cmi(const GridDev& G, int i1, int i2, int i3) {
+  return (long long)(i1 + 1) + G.d.s2 * (i2 + 1) + G.c3 * (i3 + 1);
+}
+__device__ __forceinline__ long long fmi(const FaceTab& F, int i1, int i2, int i3) {
+  return (long long)(i1 - 1) * F.t1 + (long long)(i2 - 1) * F.t2 + (long long)(i3 - 1) * F.t3;
+}
 
 // Metric loads; UNIT grids return exactly 1 (products with 1 are exact, results match).
 template <bool UNIT>
 __device__ __forceinline__ double ldm(const double* p, long long k) {
   if (UNIT) return 1.0;
   return __ldg(p + k);
+}
+
+// a/b from y = RN(1/b) with one exact correction (Markstein): q0 = a*y, r = a - b*q0 (exact
+// with fma), q = RN(q0 + r*y) equals the IEEE quotient RN(a/b) whenever |a|, |q0| and |y|
+// lie in (2^-900, 2^900); outside that range the IEEE division is used.  Bit-identical to
+// a/b, at the cost of a multiply and two fma.
+__device__ __noinline__ double slow_div(double a, double b) { return a / b; }
+__device__ __forceinline__ double mdiv(double a, double b, double y) {
+  const double q0 = a * y;
+  const double r = __fma_rn(-q0, b, a);
+  const double q1 = __fma_rn(r, y, q0);
+  const double aq = fabs(q0), aa = fabs(a), ay = fabs(y);
+  if (aq > 0x1p-900 && aq < 0x1p900 && aa > 0x1p-900 && aa < 0x1p900 && ay > 0x1p-900 && ay < 0x1p900)
+    return q1;
+  return slow_div(a, b);
 }
 
 __device__ __forceinline__ bool is_null(const GridDev& G, int i1, int i2, int i3) {
@@ -124,67 +167,6 @@ struct Blocks {
 __device__ __forceinline__ double conv_rv(double n, double v1, int s) { return n * c_ms[s] * v1; }
 __device__ __forceinline__ double conv_re(double n, double T, int s) {
   return n * KB * T / (c_gammas[s] - 1);
-}
-
-// ======================================================================================
-// 1. MC-limited line update, streamed along the line (advec.f90:384-435)
-// ======================================================================================
-// Running state of one field while marching j = 0..lx+1:
-//   fp = f(j-1), fc = f(j), ls = lslope, slp = slope(j-1), php = phi(j-1)
-struct FieldRun {
-  double fp, fc, ls, slp, php;
-};
-
-__device__ __forceinline__ void run_init(FieldRun& r, double fm1, double f0, double dx0) {
-  r.fp = fm1;
-  r.fc = f0;
-  r.ls = (f0 - fm1) / dx0;
-  r.slp = 0.0;
-  r.php = 0.0;
-}
-
-// Face quantities shared by the fields of one species at face j:
-//   v = v1i(j), hv = 0.5*v, qp = dx(j) + v/h1i(j)*dt, qm = dx(j) - v/h1i(j)*dt
-struct Face {
-  double v, hv, qp, qm;
-};
-
-__device__ __forceinline__ Face make_face(double v, double h1i, double dxj, double dt) {
-  Face f;
-  f.v = v;
-  f.hv = 0.5 * v;
-  const double q = v / h1i * dt;
-  f.qp = dxj + q;
-  f.qm = dxj - q;
-  return f;
-}
-
-// March step j for one field, fn = f(j+1).  When j >= 2, `out` receives the updated value
-// of cell j-1 and the function returns true.
-__device__ __forceinline__ bool run_step(FieldRun& r, int j, double fn, double dxc, double dxn,
-                                         const Face& F, double ha2_j, double ha2_jm1, double dt,
-                                         double dxi_jm1, double ha1_jm1, double& out) {
-  const double rs = (fn - r.fc) / dxn;
-  const double cs = (fn - r.fp) / (dxc + dxn);
-  const double sl = minmod(cs, minmod(2 * r.ls, 2 * rs));
-  r.ls = rs;
-  bool have = false;
-  if (j >= 1) {
-    double ph;
-    if (F.v < 0)
-      ph = r.fc * F.v - F.hv * F.qp * sl;
-    else
-      ph = r.fp * F.v + F.hv * F.qm * r.slp;
-    if (j >= 2) {
-      out = r.fp - dt * (ha2_j * ph - ha2_jm1 * r.php) / dxi_jm1 / ha1_jm1;
-      have = true;
-    }
-    r.php = ph;
-  }
-  r.slp = sl;
-  r.fp = r.fc;
-  r.fc = fn;
-  return have;
 }
 
 // ======================================================================================
@@ -579,19 +561,24 @@ __global__ void k_interface_vels(GridDev G, Blocks B, double* vs1i, double* vs2i
 }
 
 // ======================================================================================
-// 6. The advection sweeps.  One thread per (line, species); a warp covers 32 adjacent
-//    lines (adjacent x1 for the x2/x3 sweeps, so every load is a 256-byte coalesced row;
-//    adjacent x2 for the x1 sweep, which relies on L1 sector reuse along the column).
-//    Each thread marches along its line with the running state of its fields in
-//    registers and writes cell j-1 in place once cell j+1 has been read.
+// 6. The advection sweeps (advec.f90:233-435 through multifluid.f90:49-126).
 //
+//    Divisions use mdiv with correctly rounded reciprocals of the grid divisors (1-D tables
+//    and per-cell/per-face metric tables), so every update is bit-identical to the
+//    reference's a/b chain.  Two kernels:
+//      k_sweep_march<DIM=2|3>: one thread per (x2 or x3 line, species), a warp covering 32
+//        adjacent x1 -- every load is a coalesced 256-byte row; the thread marches along its
+//        line with the running state of its fields in registers, prefetching the values of
+//        step j+2 while computing step j, and writes cell j-1 in place.
+//      k_sweep_x1: one warp per (x1 column, species), lanes along the contiguous x1, the
+//        column processed in chunks of 32 cells with neighbours exchanged by shuffles.
 //    Standalone (FUSED=false): one field set (which: 0 ns, 1 rhovs1 (frank 1), 2 rhoes),
-//    interface velocities from the work arrays, ghosts from memory (multifluid.f90:49-126).
-//    Fused x3 (DIM 3): v12rhov1/T2rhoe folded in, x3 ghosts and vs3i formed on the fly.
-//    Fused x1 (DIM 1): vs1i formed on the fly (boundary faces stored for the next step),
-//    the halo_allparams wrap of the swept values written directly.
-//    Fused x2 (DIM 2): rhov12v1, clean_param(1,2,3) element parts and rhoe2T applied to
-//    each finished cell (species exchanged through shared memory).
+//    interface velocities from the work arrays, ghosts from memory.
+//    Fused x3: v12rhov1/T2rhoe folded in, x3 ghosts and vs3i formed on the fly.
+//    Fused x1: vs1i formed on the fly (boundary faces stored for the next step), the
+//    halo_allparams self-wrap of the swept values written directly.
+//    Fused x2: rhov12v1, clean_param(1,2,3) element parts and rhoe2T applied to each
+//    finished cell (species exchanged through shared memory).
 // ======================================================================================
 struct SweepArgs {
   GridDev G;
@@ -602,63 +589,87 @@ struct SweepArgs {
   int which;  // standalone field set
 };
 
-template <int DIM>
-struct LineGeo {
-  int lx;
-  long long base, stride;
-  const double *dx, *dxi;
+// Running state of one field while marching j = 0..lx+1 along a line:
+//   fp = f(j-1), fc = f(j), ls = lslope, slp = slope(j-1), php = phi(j-1)
+struct FieldRun {
+  double fp, fc, ls, slp, php;
 };
 
-// Face metric index (for face j of the line) and cell metric index
-template <int DIM>
-__device__ __forceinline__ long long face_idx(const Dims& d, int a, int b, int j);
-template <>
-__device__ __forceinline__ long long face_idx<3>(const Dims& d, int a, int b, int j) {
-  return f3i(d, a, b, j);
-}
-template <>
-__device__ __forceinline__ long long face_idx<2>(const Dims& d, int a, int b, int j) {
-  return f2i(d, a, j, b);
-}
-template <>
-__device__ __forceinline__ long long face_idx<1>(const Dims& d, int a, int b, int j) {
-  return f1i(d, j, a, b);
+// Face quantities shared by the fields of one species at face j:
+//   v = v1i(j), hv = 0.5*v, qp = dx(j) + v/h1i(j)*dt, qm = dx(j) - v/h1i(j)*dt
+struct Face {
+  double v, hv, qp, qm;
+};
+
+__device__ __forceinline__ Face make_face(double v, double hc, double yhc, double dxj, double dt) {
+  Face f;
+  f.v = v;
+  f.hv = 0.5 * v;
+  const double q = mdiv(v, hc, yhc) * dt;
+  f.qp = dxj + q;
+  f.qm = dxj - q;
+  return f;
 }
 
+// slope(j) (advec.f90:407-414): needs f(j-1), f(j), f(j+1) and lslope = rslope(j-1)
+__device__ __forceinline__ double mc_slope(double fm, double f0, double fpl, double ls, const Line1D& L,
+                                           int j, double& rs) {
+  rs = mdiv(fpl - f0, __ldg(L.dx + j + 1), __ldg(L.ydx + j + 1));
+  const double cs = mdiv(fpl - fm, __ldg(L.dxs + j), __ldg(L.ydxs + j));
+  return minmod(cs, minmod(2 * ls, 2 * rs));
+}
+
+// phi(j) (advec.f90:418-424)
+__device__ __forceinline__ double mc_phi(double fjm1, double fj, double sljm1, double slj, const Face& F) {
+  if (F.v < 0) return fj * F.v - F.hv * F.qp * slj;
+  return fjm1 * F.v + F.hv * F.qm * sljm1;
+}
+
+// updated cell value (advec.f90:427): f - dt*(Pr - Pl)/dxi/ha1 with P = ha2i*phi
+__device__ __forceinline__ double mc_update(double f, double Pr, double Pl, double dt, double dxi, double ydxi,
+                                            double ha1, double yha1) {
+  return f - mdiv(mdiv(dt * (Pr - Pl), dxi, ydxi), ha1, yha1);
+}
+
+template <bool UNIT>
+__device__ __forceinline__ void cell_metric(const GridDev& G, long long k, int frank, double& ha1, double& yha1) {
+  if (UNIT) {
+    ha1 = 1.0;
+    yha1 = 1.0;
+  } else if (frank == 0) {
+    ha1 = __ldg(G.ha1_0 + k);
+    yha1 = __ldg(G.yha1_0 + k);
+  } else {
+    ha1 = __ldg(G.ha1_1 + k);
+    yha1 = __ldg(G.yha1_1 + k);
+  }
+}
+
+// ---- x2 / x3 sweeps ---------------------------------------------------------------------
 template <int DIM, bool UNIT, bool FUSED>
-__global__ void __launch_bounds__(224) k_sweep(SweepArgs P) {
+__global__ void __launch_bounds__(224, 2) k_sweep_march(SweepArgs P) {
   const GridDev& G = P.G;
   const Dims d = G.d;
   const Blocks& B = P.B;
   const double dt = *P.dtp;
   const int s = threadIdx.y;
-  // line coordinates (a, b): DIM3 (i1,i2), DIM2 (i1,i3), DIM1 (i2,i3)
-  const int lxa = (DIM == 1) ? d.lx2 : d.lx1;
+  const Line1D& L = G.L[DIM - 1];
+  const FaceTab& FT = G.F[DIM - 1];
+  // line coordinates: DIM3 (i1, i2), DIM2 (i1, i3)
   const int a = blockIdx.x * 32 + threadIdx.x + 1;
   const int b = blockIdx.y + 1;
-  const bool valid = a <= lxa;
-  const int aa = valid ? a : lxa;  // clamp for address arithmetic of idle lanes
-  int lx;
-  long long stride, base;
-  const double *dx, *dxi;
-  if (DIM == 3) {
-    lx = d.lx3; stride = d.s3; base = gi(d, aa, b, 0) - d.s3; dx = G.dx3; dxi = G.dx3i;
-  } else if (DIM == 2) {
-    lx = d.lx2; stride = d.s2; base = gi(d, aa, 0, b) - d.s2; dx = G.dx2; dxi = G.dx2i;
-  } else {
-    lx = d.lx1; stride = 1; base = gi(d, 0, aa, b) - 1; dx = G.dx1; dxi = G.dx1i;
-  }
-  // cell (line index j) -> ghosted offset base + (j+1)*stride
+  const bool valid = a <= d.lx1;
+  const int aa = valid ? a : d.lx1;  // idle lanes read a valid line
+  const int lx = (DIM == 3) ? d.lx3 : d.lx2;
+  const long long stride = (DIM == 3) ? d.s3 : d.s2;
+  const long long base = (DIM == 3) ? gi(d, aa, b, 0) - d.s3 : gi(d, aa, 0, b) - d.s2;
   auto cell = [&](int j) -> long long { return base + (long long)(j + 1) * stride; };
-  const double* h1 = G.h1;
-  const double* h2 = G.h2;
-  const double* h3 = G.h3;
-  const double *hfa, *hfb, *hfc;  // face metrics: ha2i = hfa*hfb (frank 0), hfa*hfa*hfb (1); h1i = hfc
-  if (DIM == 3) { hfa = G.h1x3i; hfb = G.h2x3i; hfc = G.h3x3i; }
-  else if (DIM == 2) { hfa = G.h1x2i; hfb = G.h3x2i; hfc = G.h2x2i; }
-  else { hfa = G.h2x1i; hfb = G.h3x1i; hfc = G.h1x1i; }
+  auto cmet = [&](int j) -> long long { return (DIM == 3) ? cmi(G, aa, b, j) : cmi(G, aa, j, b); };
+  auto fmet = [&](int j) -> long long { return (DIM == 3) ? fmi(FT, aa, b, j) : fmi(FT, aa, j, b); };
+  auto fvel = [&](int j) -> long long {  // face j in the work arrays (full 3-D layout)
+    return (DIM == 3) ? f3i(d, aa, b, j) : f2i(d, aa, j, b);
+  };
 
-  // ---- field set
   int nf;
   double* fld[3];
   int frank[3];
@@ -666,7 +677,7 @@ __global__ void __launch_bounds__(224) k_sweep(SweepArgs P) {
     if (s < LSP - 1) {
       nf = 3;
       fld[0] = B.ns(s); fld[1] = B.rv(s); fld[2] = B.re(s);
-      frank[0] = 0; frank[1] = (DIM == 1) ? 0 : 1; frank[2] = 0;
+      frank[0] = 0; frank[1] = 1; frank[2] = 0;
     } else {
       nf = 1;
       fld[0] = B.re(s); fld[1] = fld[0]; fld[2] = fld[0];
@@ -676,46 +687,55 @@ __global__ void __launch_bounds__(224) k_sweep(SweepArgs P) {
     nf = 1;
     fld[0] = (P.which == 0) ? B.ns(s) : (P.which == 1) ? B.rv(s) : B.re(s);
     fld[1] = fld[0]; fld[2] = fld[0];
-    frank[0] = (P.which == 1 && DIM != 1) ? 1 : 0; frank[1] = frank[0]; frank[2] = frank[0];
+    frank[0] = (P.which == 1) ? 1 : 0; frank[1] = frank[0]; frank[2] = frank[0];
   }
-  // field value at line index j (FUSED x3: converted and with on-the-fly x3 ghosts)
   const bool per = G.flagper != 0;
-  auto map3 = [&](int j) -> int {
+  auto map3 = [&](int j) -> int {  // x3 ghosts after set_global_boundaries / the self-wrap
     if (j >= 1 && j <= lx) return j;
     if (per) return (j < 1) ? j + lx : j - lx;
     return (j < 1) ? 1 : lx;
   };
-  auto fval = [&](int f, int j) -> double {
+  // raw loads of line index j (FUSED x3 converts ns, vs1, Ts into the three fields)
+  struct Raw {
+    double x[3];
+  };
+  auto load_raw = [&](int j) -> Raw {
+    Raw r;
     if (FUSED && DIM == 3) {
       const long long k = cell(map3(j));
+      r.x[0] = B.ns(s)[k];
+      r.x[1] = (s < LSP - 1) ? B.vs1(s)[k] : 0.0;
+      r.x[2] = B.Ts(s)[k];
+    } else {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) r.x[f] = (f < nf) ? fld[f][cell(j)] : 0.0;
+    }
+    return r;
+  };
+  auto fields_of = [&](const Raw& r, double* out) {
+    if (FUSED && DIM == 3) {
       if (s < LSP - 1) {
-        if (f == 0) return B.ns(s)[k];
-        if (f == 1) return conv_rv(B.ns(s)[k], B.vs1(s)[k], s);
+        out[0] = r.x[0];
+        out[1] = conv_rv(r.x[0], r.x[1], s);
+        out[2] = conv_re(r.x[0], r.x[2], s);
+      } else {
+        out[0] = conv_re(r.x[0], r.x[2], s);
+        out[1] = out[0];
+        out[2] = out[0];
       }
-      return conv_re(B.ns(s)[k], B.Ts(s)[k], s);
+    } else {
+      out[0] = r.x[0]; out[1] = r.x[1]; out[2] = r.x[2];
     }
-    return fld[f][cell(j)];
   };
-  // cell-centred velocity for on-the-fly faces
-  auto vcell = [&](int j) -> double {
+  auto vcell = [&](int j) -> double {  // cell velocity for on-the-fly faces (fused)
     if (DIM == 3) return B.vs3(s)[cell(map3(j))];
-    if (DIM == 2) {
-      const int jj = (j < 1) ? 1 : (j > lx ? lx : j);
-      return B.vs2(s)[cell(jj)];
-    }
-    return B.vs1(s)[cell(j)];
-  };
-  auto mcell = [&](int j, int fr) -> double {  // ha1 at cell j
-    if (UNIT) return 1.0;
-    const long long k = cell(j);
-    const double x1 = __ldg(h1 + k);
-    if (fr == 0) return x1 * __ldg(h2 + k) * __ldg(h3 + k);
-    return x1 * x1 * __ldg(h2 + k) * __ldg(h3 + k);
+    const int jj = (j < 1) ? 1 : (j > lx ? lx : j);
+    return B.vs2(s)[cell(jj)];
   };
 
   if (lx <= 1) {
-    // advec1D_MC_curv passes a single-cell line through unchanged; the fused x3 sweep
-    // still materialises the converted momentum/energy densities.
+    // advec1D_MC_curv passes a single-cell line through; the fused x3 sweep still
+    // materialises the converted momentum/energy densities
     if (FUSED && DIM == 3 && valid) {
       const long long k = cell(1);
       B.rv(s)[k] = conv_rv(B.ns(s)[k], B.vs1(s)[k], s);
@@ -724,98 +744,110 @@ __global__ void __launch_bounds__(224) k_sweep(SweepArgs P) {
     return;
   }
 
-  // periodic fused x3: cache the pre-sweep values that the tail of the line wraps to
-  double wrapv[3][2];
+  // periodic fused x3: keep the pre-sweep values the tail of the line wraps to
+  double wrap1[3], wrap2[3];
   if (FUSED && DIM == 3 && per) {
-#pragma unroll
-    for (int f = 0; f < 3; ++f)
-      if (f < nf) {
-        wrapv[f][0] = fval(f, 1);
-        wrapv[f][1] = fval(f, 2);
-      }
+    fields_of(load_raw(1), wrap1);
+    fields_of(load_raw(2), wrap2);
   }
   FieldRun run[3];
-  const double dx0 = __ldg(dx + 0);
+  {
+    double fm1[3], f0[3];
+    fields_of(load_raw(-1), fm1);
+    fields_of(load_raw(0), f0);
+    const double dx0 = __ldg(L.dx);
 #pragma unroll
-  for (int f = 0; f < 3; ++f)
-    if (f < nf) run_init(run[f], fval(f, -1), fval(f, 0), dx0);
-
-  // fused x1: velocities at the two boundary faces (advec.f90:170-196)
-  double v_first = 0.0, v_lastprev = 0.0;
-  if (FUSED && DIM == 1) {
-    const double vc1 = vcell(1), vc2 = vcell(2);
-    v_first = (G.gridflag == 1) ? fmin_f(0.5 * (vc1 + vc2), 0.0) : vc1;
+    for (int f = 0; f < 3; ++f) {
+      run[f].fp = fm1[f];
+      run[f].fc = f0[f];
+      run[f].ls = mdiv(f0[f] - fm1[f], dx0, __ldg(L.ydx));
+      run[f].slp = 0.0;
+      run[f].php = 0.0;
+    }
   }
-  double vprev = (FUSED && DIM != 1) ? vcell(0) : 0.0;  // cell velocity j-1 for faces
   double ha2prev0 = 0.0, ha2prev1 = 0.0;
-  double dxc = dx0;
+  // prefetch pipeline: raw values of f(j+1) (next) and f(j+2) (next2); fused cell
+  // velocities v(j) (vq) and v(j+1) (vq1); vprev = v(j-1)
+  Raw next = load_raw(1), next2 = load_raw(2);
+  double vprev = 0.0, vq = 0.0, vq1 = 0.0;
+  if (FUSED) {
+    vq = vcell(0);
+    vq1 = vcell(1);
+  }
 
   for (int j = 0; j <= lx + 1; ++j) {
-    const double dxn = __ldg(dx + j + 1);
-    // face j
+    // values of this step
+    double fn[3];
+    if (FUSED && DIM == 3 && j + 1 > lx) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) fn[f] = per ? ((j + 1 == lx + 1) ? wrap1[f] : wrap2[f]) : run[f].fc;
+    } else {
+      fields_of(next, fn);
+    }
+    const double vc = vq;  // v(j)
+    // issue the loads two steps ahead
+    next = next2;
+    if (j + 3 <= lx + 2) next2 = load_raw(j + 3);
+    if (FUSED) {
+      vq = vq1;
+      if (j + 2 <= lx + 1) vq1 = vcell(j + 2);
+    }
+
     Face F = {0.0, 0.0, 0.0, 0.0};
     double ha2j0 = 0.0, ha2j1 = 0.0;
     if (j >= 1) {
       double v;
       if (!FUSED) {
-        v = P.vsi[(long long)s * ((DIM == 3) ? nf3(d) : (DIM == 2) ? nf2(d) : nf1(d)) +
-                  face_idx<DIM>(d, aa, b, j)];
-      } else if (DIM == 1) {
-        if (j == 1) {
-          v = v_first;
-        } else if (j <= lx) {
-          v = 0.5 * (vcell(j - 1) + vcell(j));
-        } else {
-          v = (G.gridflag == 0 || G.gridflag == 1) ? vcell(lx) : fmax_f(v_lastprev, 0.0);
-        }
-        v_lastprev = v;
-        if (valid && (j == 1 || j == lx + 1))
-          P.vs1i[(long long)s * nf1(d) + f1i(d, j, aa, b)] = v;
+        v = P.vsi[(long long)s * ((DIM == 3) ? nf3(d) : nf2(d)) + fvel(j)];
       } else {
-        const double vc = vcell(j);
         v = 0.5 * (vprev + vc);
         vprev = vc;
       }
-      const long long fk = face_idx<DIM>(d, aa, b, j);
-      const double hc = ldm<UNIT>(hfc, fk);
-      F = make_face(v, hc, dxc, dt);
-      if (!UNIT) {
-        const double ha = __ldg(hfa + fk), hb = __ldg(hfb + fk);
-        ha2j0 = ha * hb;
-        ha2j1 = ha * ha * hb;
+      const long long fk = fmet(j);
+      const double dxc = __ldg(L.dx + j);
+      if (UNIT) {
+        F = make_face(v, 1.0, 1.0, dxc, dt);
+        ha2j0 = ha2j1 = 1.0;
       } else {
-        ha2j0 = 1.0;
-        ha2j1 = 1.0;
+        F = make_face(v, __ldg(FT.hc + fk), __ldg(FT.yhc + fk), dxc, dt);
+        ha2j0 = __ldg(FT.ha2i0 + fk);
+        ha2j1 = __ldg(FT.ha2i1 + fk);
       }
+    } else if (FUSED) {
+      vprev = vc;
     }
-    double dxi_jm1 = 0.0, ha1_0 = 1.0, ha1_1 = 1.0;
+    double ha1_0 = 1.0, yha1_0 = 1.0, ha1_1 = 1.0, yha1_1 = 1.0, dxi = 0.0, ydxi = 0.0;
     if (j >= 2) {
-      dxi_jm1 = __ldg(dxi + (j - 2));
-      ha1_0 = mcell(j - 1, 0);
-      if (frank[1] == 1 || frank[0] == 1) ha1_1 = mcell(j - 1, 1);
+      dxi = __ldg(L.dxi + j - 2);
+      ydxi = __ldg(L.ydxi + j - 2);
+      const long long ck = cmet(j - 1);
+      cell_metric<UNIT>(G, ck, 0, ha1_0, yha1_0);
+      if (frank[0] == 1 || frank[1] == 1) cell_metric<UNIT>(G, ck, 1, ha1_1, yha1_1);
     }
     double outv[3];
-    bool have = false;
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
       if (f < nf) {
-        double fn;
-        if (FUSED && DIM == 3) {
-          if (j + 1 <= lx) fn = fval(f, j + 1);
-          else if (per) fn = wrapv[f][j + 1 - lx - 1];
-          else fn = run[f].fc;  // f(lx+1) = f(lx+2) = f(lx)
-        } else {
-          fn = fld[f][cell(j + 1)];
+        FieldRun& r = run[f];
+        double rs;
+        const double sl = mc_slope(r.fp, r.fc, fn[f], r.ls, L, j, rs);
+        r.ls = rs;
+        if (j >= 1) {
+          const double ph = mc_phi(r.fp, r.fc, r.slp, sl, F);
+          const bool fr = frank[f] == 1;
+          if (j >= 2)
+            outv[f] = mc_update(r.fp, (fr ? ha2j1 : ha2j0) * ph, (fr ? ha2prev1 : ha2prev0) * r.php, dt, dxi, ydxi,
+                                fr ? ha1_1 : ha1_0, fr ? yha1_1 : yha1_0);
+          r.php = ph;
         }
-        const bool fr1 = frank[f] == 1;
-        have = run_step(run[f], j, fn, dxc, dxn, F, fr1 ? ha2j1 : ha2j0, fr1 ? ha2prev1 : ha2prev0,
-                        dt, dxi_jm1, fr1 ? ha1_1 : ha1_0, outv[f]);
+        r.slp = sl;
+        r.fp = r.fc;
+        r.fc = fn[f];
       }
     }
     ha2prev0 = ha2j0;
     ha2prev1 = ha2j1;
-    dxc = dxn;
-    if (!have) continue;
+    if (j < 2) continue;
     const int c = j - 1;  // finished cell
     const long long kc = cell(c);
     if constexpr (!(FUSED && DIM == 2)) {
@@ -825,20 +857,6 @@ __global__ void __launch_bounds__(224) k_sweep(SweepArgs P) {
           if (f < nf) fld[f][kc] = outv[f];
         if (FUSED && DIM == 3 && s == LSP - 1)  // unswept electron momentum density
           B.rv(s)[kc] = conv_rv(B.ns(s)[kc], B.vs1(s)[kc], s);
-        if (FUSED && DIM == 1 && per) {
-          // halo_allparams self-wrap of the updated column (mpihalo.f90:147-151)
-          const int i3 = b;
-          int tg[2] = {0, 0};
-          int ntg = 0;
-          if (i3 >= d.lx3 - 1) tg[ntg++] = i3 - d.lx3;
-          if (i3 <= 2) tg[ntg++] = i3 + d.lx3;
-          for (int q = 0; q < ntg; ++q) {
-            const long long kw = gi(d, c, aa, tg[q]);
-#pragma unroll
-            for (int f = 0; f < 3; ++f)
-              if (f < nf) fld[f][kw] = outv[f];
-          }
-        }
       }
     } else {
       // ---- fused x2 epilogue: rhov12v1 (multifluid.f90:218-233), clean_param(1),
@@ -885,6 +903,143 @@ __global__ void __launch_bounds__(224) k_sweep(SweepArgs P) {
         }
       }
     }
+  }
+}
+
+// ---- x1 sweep: lanes along the column ------------------------------------------------------
+// Lane l of chunk c handles position p = 32c + l - 1... the chunk covers p = 32c .. 32c+31 over
+// p = 0 .. lx1+1: the slope at cell p, the flux P(p) = ha2i(p)*phi(p) at face p, and the update
+// of cell p-1 (which needs P(p) and P(p-1)).  Values crossing the chunk edge (slope(p-1),
+// P(p-1)) are carried from lane 31 of the previous chunk.
+template <bool UNIT, bool FUSED>
+__global__ void __launch_bounds__(224) k_sweep_x1(SweepArgs P) {
+  const GridDev& G = P.G;
+  const Dims d = G.d;
+  const Blocks& B = P.B;
+  const double dt = *P.dtp;
+  const int s = threadIdx.y;
+  const int lane = threadIdx.x;
+  const int i2 = blockIdx.x + 1, i3 = blockIdx.y + 1;
+  const int n = d.lx1;
+  const Line1D& L = G.L[0];
+  const FaceTab& FT = G.F[0];
+  const long long col = gi(d, 0, i2, i3);  // cell i at col + i
+  int nf;
+  double* fld[3];
+  if (FUSED) {
+    if (s < LSP - 1) {
+      nf = 3;
+      fld[0] = B.ns(s); fld[1] = B.rv(s); fld[2] = B.re(s);
+    } else {
+      nf = 1;
+      fld[0] = B.re(s); fld[1] = fld[0]; fld[2] = fld[0];
+    }
+  } else {
+    nf = 1;
+    fld[0] = (P.which == 0) ? B.ns(s) : (P.which == 1) ? B.rv(s) : B.re(s);
+    fld[1] = fld[0]; fld[2] = fld[0];
+  }
+  const double* V1 = B.vs1(s) + col;
+  // fused: velocities of the two boundary faces (advec.f90:170-196)
+  double vface1 = 0.0, vfaceN = 0.0;
+  if (FUSED) {
+    const double v1 = V1[1], v2 = V1[2], vn1 = V1[n - 1], vn = V1[n];
+    vface1 = (G.gridflag == 1) ? fmin_f(0.5 * (v1 + v2), 0.0) : v1;
+    vfaceN = (G.gridflag == 0 || G.gridflag == 1) ? vn : fmax_f(0.5 * (vn1 + vn), 0.0);
+    if (lane == 0) {
+      P.vs1i[(long long)s * nf1(d) + f1i(d, 1, i2, i3)] = vface1;
+      P.vs1i[(long long)s * nf1(d) + f1i(d, n + 1, i2, i3)] = vfaceN;
+    }
+  }
+  double carry_sl[3] = {0.0, 0.0, 0.0}, carry_P[3] = {0.0, 0.0, 0.0};
+  const int nchunk = (n + 2 + 31) / 32;
+  for (int c = 0; c < nchunk; ++c) {
+    const int p = 32 * c + lane;  // 0 .. n+1 when active
+    const bool act = p <= n + 1;
+    const int pc = act ? p : n + 1;  // clamped for loads
+    // face p velocity (p >= 1)
+    double v = 0.0;
+    if (FUSED) {
+      const double vcur = V1[(pc >= 1 && pc <= n) ? pc : 1];
+      double vleft = __shfl_up_sync(0xffffffffu, vcur, 1);
+      if (lane == 0) vleft = V1[(pc - 1 >= 1) ? pc - 1 : 1];
+      if (pc == 1) v = vface1;
+      else if (pc == n + 1) v = vfaceN;
+      else v = 0.5 * (vleft + vcur);
+    } else {
+      v = P.vsi[(long long)s * nf1(d) + f1i(d, (pc >= 1) ? pc : 1, i2, i3)];
+    }
+    Face F = {0.0, 0.0, 0.0, 0.0};
+    double ha2 = 1.0;
+    const int pf = (pc >= 1) ? pc : 1;
+    const double dxc = __ldg(L.dx + pc), ydxc = __ldg(L.ydx + pc);
+    const double dxn = __ldg(L.dx + pc + 1), ydxn = __ldg(L.ydx + pc + 1);
+    const double dxs = __ldg(L.dxs + pc), ydxs = __ldg(L.ydxs + pc);
+    {
+      if (UNIT) {
+        F = make_face(v, 1.0, 1.0, dxc, dt);
+      } else {
+        const long long fk = fmi(FT, pf, i2, i3);
+        F = make_face(v, __ldg(FT.hc + fk), __ldg(FT.yhc + fk), dxc, dt);
+        ha2 = __ldg(FT.ha2i0 + fk);
+      }
+    }
+    // cell p-1 metrics for the update
+    const int q = pc - 1;  // updated cell
+    double ha1 = 1.0, yha1 = 1.0, dxi = 1.0, ydxi = 1.0;
+    if (q >= 1 && q <= n) {
+      dxi = __ldg(L.dxi + q - 1);
+      ydxi = __ldg(L.ydxi + q - 1);
+      cell_metric<UNIT>(G, cmi(G, q, i2, i3), 0, ha1, yha1);
+    }
+    double outv[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      if (f < nf) {
+        const double* fc = fld[f] + col;
+        const double f0 = fc[pc];
+        const double fpl = fc[pc + 1];
+        double fm = __shfl_up_sync(0xffffffffu, f0, 1);
+        if (lane == 0) fm = fc[pc - 1];
+        // slope(p) (advec.f90:407-414) with lslope = rslope(p-1) from the lane below
+        const double rs = mdiv(fpl - f0, dxn, ydxn);
+        double ls = __shfl_up_sync(0xffffffffu, rs, 1);
+        if (lane == 0) ls = mdiv(f0 - fm, dxc, ydxc);
+        const double cs = mdiv(fpl - fm, dxs, ydxs);
+        const double sl = minmod(cs, minmod(2 * ls, 2 * rs));
+        double slm = __shfl_up_sync(0xffffffffu, sl, 1);
+        if (lane == 0) slm = carry_sl[f];
+        const double ph = mc_phi(fm, f0, slm, sl, F);
+        const double Pp = ha2 * ph;
+        double Pm = __shfl_up_sync(0xffffffffu, Pp, 1);
+        if (lane == 0) Pm = carry_P[f];
+        outv[f] = mc_update(fm, Pp, Pm, dt, dxi, ydxi, ha1, yha1);
+        carry_sl[f] = __shfl_sync(0xffffffffu, sl, 31);
+        carry_P[f] = __shfl_sync(0xffffffffu, Pp, 31);
+      }
+    }
+    if (act && q >= 1 && q <= n) {
+      const long long kq = col + q;
+#pragma unroll
+      for (int f = 0; f < 3; ++f)
+        if (f < nf) fld[f][kq] = outv[f];
+      if (FUSED && G.flagper) {
+        // halo_allparams self-wrap of the updated column (mpihalo.f90:147-151)
+        if (i3 >= d.lx3 - 1) {
+          const long long kw = gi(d, q, i2, i3 - d.lx3);
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+            if (f < nf) fld[f][kw] = outv[f];
+        }
+        if (i3 <= 2) {
+          const long long kw = gi(d, q, i2, i3 + d.lx3);
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+            if (f < nf) fld[f][kw] = outv[f];
+        }
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -947,8 +1102,8 @@ struct DiffArgs {
 };
 
 // shared-memory arrays per warp: inputs (T and the per-row conduction/advection factors),
-// the refinement copy, and the partition solver's four work arrays
-constexpr int DA_T = 0, DA_QP = 1, DA_QM = 2, DA_BQ = 3, DA_X = 4, DA_SS = 5, DA_IB = 6, DA_TT = 7, DA_R = 8;
+// the stage right-hand side / residual, the solution, and the factorisation (IB, SS, TT)
+constexpr int DA_T = 0, DA_QP = 1, DA_QM = 2, DA_BQ = 3, DA_RHS = 4, DA_SS = 5, DA_IB = 6, DA_TT = 7, DA_R = 8;
 constexpr int DNA = 9;
 
 struct WarpMem {
@@ -974,111 +1129,150 @@ __device__ __forceinline__ double pow25(double x) {
   return p + (pl + (x2 * sl + x2l * s));
 }
 
-struct Row4 {
-  double A, B, C, R;
+// Lane-blocked tridiagonal solver.  Row k of this lane's block (global row 32-lane block
+// order: lane l owns rows l*M .. l*M+M-1) couples x_{k-1}, x_k, x_{k+1}.
+//
+// Factorisation (matrix only, once per stage):
+//   1. block elimination: rows 1..M-1 eliminated downward with row 1 as pivot start, which
+//      leaves fill-in SS in the column of the block's first unknown x0; then rows M-3..1
+//      upward, leaving fill-in TT in the column of the block's last unknown xl.  Row 0
+//      then eliminates x1 (multiplier g0).  What remains per lane is two interface rows,
+//      lo (row 0: prev xl, x0, xl) and hi (row M-1: x0, xl, next x0).
+//   2. odd-even reduction: hi loses x0 (own lo, multiplier e1) and the next lane's x0
+//      (next lo, e2), leaving a 32-row tridiagonal system in the xl of the lanes.
+//   3. parallel cyclic reduction of that system over 5 shuffle levels (multipliers k1, k2).
+// Every multiplier stays in shared memory (IB, SS, TT per row) or registers (IfaceLU), so
+// a solve for a new right-hand side replays only the vector updates.
+struct IfaceLU {
+  double loA, loB, loC, g0;
+  double e1, e2;
+  double k1[5], k2[5];
+  double hiB;
 };
 
-__device__ __forceinline__ void pcr_update(Row4& r, const Row4& p, const Row4& n) {
-  const double k1 = r.A / p.B;
-  const double k2 = r.C / n.B;
-  Row4 o;
-  o.A = -k1 * p.A;
-  o.C = -k2 * n.C;
-  o.B = r.B - k1 * p.C - k2 * n.A;
-  o.R = r.R - k1 * p.R - k2 * n.R;
-  r = o;
-}
-
-__device__ __forceinline__ Row4 shfl_up_row(const Row4& r, int delta, int lane) {
-  Row4 o;
-  o.A = __shfl_up_sync(0xffffffffu, r.A, delta);
-  o.B = __shfl_up_sync(0xffffffffu, r.B, delta);
-  o.C = __shfl_up_sync(0xffffffffu, r.C, delta);
-  o.R = __shfl_up_sync(0xffffffffu, r.R, delta);
-  if (lane < delta) o = Row4{0.0, 1.0, 0.0, 0.0};  // outside the system: identity row
-  return o;
-}
-__device__ __forceinline__ Row4 shfl_down_row(const Row4& r, int delta, int lane) {
-  Row4 o;
-  o.A = __shfl_down_sync(0xffffffffu, r.A, delta);
-  o.B = __shfl_down_sync(0xffffffffu, r.B, delta);
-  o.C = __shfl_down_sync(0xffffffffu, r.C, delta);
-  o.R = __shfl_down_sync(0xffffffffu, r.R, delta);
-  if (lane + delta > 31) o = Row4{0.0, 1.0, 0.0, 0.0};
-  return o;
-}
-
-// Solve the lane-blocked system whose row k (of this lane) is rowf(k, a,b,c,r); rowf is
-// called for k = 1..M-1 (ascending) and then k = 0, and may read W.at(DA_R, k, lane) for
-// row k before this function overwrites it.  The solution of row k ends in DA_R.
-template <class RowF>
-__device__ void partition_solve(const WarpMem& W, int M, int lane, RowF rowf) {
-  double a, b, c, r;
-  // downward elimination, rows 1..M-1, fill-in in the column of the block's first unknown
-  rowf(1, a, b, c, r);
-  double s_prev = a, b_prev = b, r_prev = r, c_prev = c;
-  double ib_prev = 1.0 / b;
+template <class RowM>
+__device__ __forceinline__ void band_factor(const WarpMem& W, int M, int lane, RowM rowm, IfaceLU& F) {
+  double a, b, c;
+  rowm(1, a, b, c);
+  double s_prev = a, c_prev = c, bp = b, ib_prev = 1.0 / b;
   W.at(DA_SS, 1, lane) = s_prev;
   W.at(DA_IB, 1, lane) = ib_prev;
-  W.at(DA_R, 1, lane) = r_prev;
   W.at(DA_TT, 1, lane) = c;
   for (int k = 2; k < M; ++k) {
-    rowf(k, a, b, c, r);
+    rowm(k, a, b, c);
     const double f = a * ib_prev;
     const double sk = -f * s_prev;
     const double bk = b - f * c_prev;
-    const double rk = r - f * r_prev;
     const double ibk = 1.0 / bk;
     W.at(DA_SS, k, lane) = sk;
     W.at(DA_IB, k, lane) = ibk;
-    W.at(DA_R, k, lane) = rk;
     W.at(DA_TT, k, lane) = c;
     s_prev = sk;
-    ib_prev = ibk;
-    r_prev = rk;
     c_prev = c;
-    b_prev = bk;
+    bp = bk;
+    ib_prev = ibk;
   }
-  Row4 hi = {s_prev, b_prev, c_prev, r_prev};  // row M-1 -> interface row z_{2l+1}
-  // upward elimination, rows M-3..1, fill-in in the column of the block's last unknown
+  const double hiA = s_prev, hiC = c_prev;
+  double hiB = bp;
   for (int k = M - 3; k >= 1; --k) {
     const double g = W.at(DA_TT, k, lane) * W.at(DA_IB, k + 1, lane);
     W.at(DA_SS, k, lane) = W.at(DA_SS, k, lane) - g * W.at(DA_SS, k + 1, lane);
     W.at(DA_TT, k, lane) = -g * W.at(DA_TT, k + 1, lane);
-    W.at(DA_R, k, lane) = W.at(DA_R, k, lane) - g * W.at(DA_R, k + 1, lane);
   }
-  rowf(0, a, b, c, r);
-  Row4 lo;
+  rowm(0, a, b, c);
   if (M >= 3) {
-    const double g = c * W.at(DA_IB, 1, lane);
-    lo = Row4{a, b - g * W.at(DA_SS, 1, lane), -g * W.at(DA_TT, 1, lane), r - g * W.at(DA_R, 1, lane)};
+    F.g0 = c * W.at(DA_IB, 1, lane);
+    F.loA = a;
+    F.loB = b - F.g0 * W.at(DA_SS, 1, lane);
+    F.loC = -F.g0 * W.at(DA_TT, 1, lane);
   } else {
-    lo = Row4{a, b, c, r};
+    F.g0 = 0.0;
+    F.loA = a;
+    F.loB = b;
+    F.loC = c;
   }
-  // parallel cyclic reduction on the 64 interface rows (z_{2l} = lo, z_{2l+1} = hi)
-  {
-    const Row4 prev_lo = shfl_up_row(hi, 1, lane);
-    const Row4 next_hi = shfl_down_row(lo, 1, lane);
-    const Row4 lo0 = lo, hi0 = hi;
-    pcr_update(lo, prev_lo, hi0);
-    pcr_update(hi, lo0, next_hi);
+  // odd-even reduction onto the hi rows; the row below lane 31 is an identity row
+  double nA = __shfl_down_sync(0xffffffffu, F.loA, 1);
+  double nB = __shfl_down_sync(0xffffffffu, F.loB, 1);
+  double nC = __shfl_down_sync(0xffffffffu, F.loC, 1);
+  if (lane == 31) {
+    nA = 0.0;
+    nB = 1.0;
+    nC = 0.0;
   }
+  F.e1 = hiA / F.loB;
+  double A = -F.e1 * F.loA, B = hiB - F.e1 * F.loC, C = hiC;
+  F.e2 = C / nB;
+  B = B - F.e2 * nA;
+  C = -F.e2 * nC;
 #pragma unroll
-  for (int sh = 1; sh <= 16; sh <<= 1) {
-    const Row4 pl = shfl_up_row(lo, sh, lane), nl = shfl_down_row(lo, sh, lane);
-    const Row4 ph = shfl_up_row(hi, sh, lane), nh = shfl_down_row(hi, sh, lane);
-    pcr_update(lo, pl, nl);
-    pcr_update(hi, ph, nh);
+  for (int lv = 0; lv < 5; ++lv) {
+    const int sh = 1 << lv;
+    double pA = __shfl_up_sync(0xffffffffu, A, sh), pB = __shfl_up_sync(0xffffffffu, B, sh),
+           pC = __shfl_up_sync(0xffffffffu, C, sh);
+    double qA = __shfl_down_sync(0xffffffffu, A, sh), qB = __shfl_down_sync(0xffffffffu, B, sh),
+           qC = __shfl_down_sync(0xffffffffu, C, sh);
+    if (lane < sh) {
+      pA = 0.0;
+      pB = 1.0;
+      pC = 0.0;
+    }
+    if (lane + sh > 31) {
+      qA = 0.0;
+      qB = 1.0;
+      qC = 0.0;
+    }
+    const double k1 = A / pB, k2 = C / qB;
+    F.k1[lv] = k1;
+    F.k2[lv] = k2;
+    const double nA2 = -k1 * pA, nC2 = -k2 * qC;
+    B = B - k1 * pC - k2 * qA;
+    A = nA2;
+    C = nC2;
   }
-  const double x0 = lo.R / lo.B;
-  const double xl = hi.R / hi.B;
-  for (int k = 1; k <= M - 2; ++k) {
-    const double xk =
-        (W.at(DA_R, k, lane) - W.at(DA_SS, k, lane) * x0 - W.at(DA_TT, k, lane) * xl) * W.at(DA_IB, k, lane);
-    W.at(DA_R, k, lane) = xk;
+  F.hiB = B;
+}
+
+// Solve for the right-hand side in array ARR (in place: the solution replaces it).
+template <class RowM>
+__device__ __forceinline__ void band_solve(const WarpMem& W, int M, int lane, RowM rowm, const IfaceLU& F,
+                                           int ARR) {
+  double a, b, c;
+  double rp = W.at(ARR, 1, lane);
+  for (int k = 2; k < M; ++k) {
+    rowm(k, a, b, c);
+    rp = W.at(ARR, k, lane) - a * W.at(DA_IB, k - 1, lane) * rp;
+    W.at(ARR, k, lane) = rp;
   }
-  W.at(DA_R, 0, lane) = x0;
-  W.at(DA_R, M - 1, lane) = xl;
+  const double hiR = rp;
+  double rn = (M >= 3) ? W.at(ARR, M - 2, lane) : 0.0;
+  for (int k = M - 3; k >= 1; --k) {
+    rowm(k, a, b, c);
+    rn = W.at(ARR, k, lane) - c * W.at(DA_IB, k + 1, lane) * rn;
+    W.at(ARR, k, lane) = rn;
+  }
+  const double loR = (M >= 3) ? W.at(ARR, 0, lane) - F.g0 * W.at(ARR, 1, lane) : W.at(ARR, 0, lane);
+  double nR = __shfl_down_sync(0xffffffffu, loR, 1);
+  if (lane == 31) nR = 0.0;
+  double R = hiR - F.e1 * loR;
+  R = R - F.e2 * nR;
+#pragma unroll
+  for (int lv = 0; lv < 5; ++lv) {
+    const int sh = 1 << lv;
+    double pR = __shfl_up_sync(0xffffffffu, R, sh), qR = __shfl_down_sync(0xffffffffu, R, sh);
+    if (lane < sh) pR = 0.0;
+    if (lane + sh > 31) qR = 0.0;
+    R = R - F.k1[lv] * pR - F.k2[lv] * qR;
+  }
+  const double xl = R / F.hiB;
+  double xlp = __shfl_up_sync(0xffffffffu, xl, 1);
+  if (lane == 0) xlp = 0.0;
+  const double x0 = (loR - F.loA * xlp - F.loC * xl) / F.loB;
+  for (int k = 1; k <= M - 2; ++k)
+    W.at(ARR, k, lane) =
+        (W.at(ARR, k, lane) - W.at(DA_SS, k, lane) * x0 - W.at(DA_TT, k, lane) * xl) * W.at(DA_IB, k, lane);
+  W.at(ARR, 0, lane) = x0;
+  W.at(ARR, M - 1, lane) = xl;
 }
 
 // exact-error accumulation for the refinement residual r - (a xm + b x + c xp)
@@ -1098,31 +1292,28 @@ __device__ __forceinline__ double residual3(double r, double a, double xm, doubl
   return s + (comp - (e1 + e2 + e3));
 }
 
-// Solve with one refinement step; the solution ends in DA_R.
-template <class RowF>
-__device__ void refined_solve(const WarpMem& W, int M, int lane, RowF rowf) {
-  partition_solve(W, M, lane, rowf);
+// Solve the stage system (matrix rowm, right-hand side in DA_RHS) with one step of
+// iterative refinement; the solution ends in DA_R, DA_RHS is consumed.
+template <class RowM>
+__device__ void refined_solve(const WarpMem& W, int M, int lane, RowM rowm) {
+  IfaceLU F;
+  band_factor(W, M, lane, rowm, F);
+  for (int k = 0; k < M; ++k) W.at(DA_R, k, lane) = W.at(DA_RHS, k, lane);
+  band_solve(W, M, lane, rowm, F, DA_R);
   __syncwarp();
-  for (int k = 0; k < M; ++k) W.at(DA_X, k, lane) = W.at(DA_R, k, lane);
-  __syncwarp();
-  const double xprev = __shfl_up_sync(0xffffffffu, W.at(DA_X, M - 1, lane), 1);
-  const double xnext = __shfl_down_sync(0xffffffffu, W.at(DA_X, 0, lane), 1);
+  const double xprev = __shfl_up_sync(0xffffffffu, W.at(DA_R, M - 1, lane), 1);
+  const double xnext = __shfl_down_sync(0xffffffffu, W.at(DA_R, 0, lane), 1);
+  double xm = xprev, xc = W.at(DA_R, 0, lane);
   for (int k = 0; k < M; ++k) {
-    double a, b, c, r;
-    rowf(k, a, b, c, r);
-    const double xm = (k > 0) ? W.at(DA_X, k - 1, lane) : xprev;
-    const double xp = (k < M - 1) ? W.at(DA_X, k + 1, lane) : xnext;
-    W.at(DA_R, k, lane) = residual3(r, a, xm, b, W.at(DA_X, k, lane), c, xp);
+    double a, b, c;
+    rowm(k, a, b, c);
+    const double xp = (k < M - 1) ? W.at(DA_R, k + 1, lane) : xnext;
+    W.at(DA_RHS, k, lane) = residual3(W.at(DA_RHS, k, lane), a, xm, b, xc, c, xp);
+    xm = xc;
+    xc = xp;
   }
-  __syncwarp();
-  auto rowres = [&](int k, double& a, double& b, double& c, double& r) {
-    double rr;
-    rowf(k, a, b, c, rr);
-    r = W.at(DA_R, k, lane);
-  };
-  partition_solve(W, M, lane, rowres);
-  __syncwarp();
-  for (int k = 0; k < M; ++k) W.at(DA_R, k, lane) = W.at(DA_X, k, lane) + W.at(DA_R, k, lane);
+  band_solve(W, M, lane, rowm, F, DA_RHS);
+  for (int k = 0; k < M; ++k) W.at(DA_R, k, lane) = W.at(DA_R, k, lane) + W.at(DA_RHS, k, lane);
   __syncwarp();
 }
 
@@ -1155,8 +1346,11 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
       if (i <= n) {
         T = Tcol[i];
         const double nv = ncol[i];
-        const double h1v = ldm<UNIT>(G.h1, m0 + i), h2v = ldm<UNIT>(G.h2, m0 + i),
-                     h3v = ldm<UNIT>(G.h3, m0 + i);
+        const long long mk = cmi(G, i, i2, i3);
+        const double h1v = ldm<UNIT>(G.h1, mk), h2v = ldm<UNIT>(G.h2, mk), h3v = ldm<UNIT>(G.h3, mk);
+        const double yh1 = ldm<UNIT>(G.yh1, mk);
+        double ha1v = 1.0, yha1v = 1.0;
+        cell_metric<UNIT>(G, mk, 0, ha1v, yha1v);  // h1*h2*h3
         const double T25 = pow25(T);
         double lam;
         if (s < LSP - 1) {
@@ -1169,9 +1363,9 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
           lam = ELCHRG * 100 * 7.7e5 * T25 / (1 + 3.22e4 * (T * T) / nv * X);
           Bc = 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i];  // beta (collisions.f90:197)
         }
-        Cc = c0 / fmax_f(nv, MINDENSDIV) / (h1v * h2v * h3v);
-        Dc = lam * h2v * h3v / h1v;
-        Bc = (s < LSP - 1) ? 0.0 : Cc * Bc / h1v;
+        Cc = mdiv(c0 / fmax_f(nv, MINDENSDIV), ha1v, yha1v);
+        Dc = mdiv(lam * h2v * h3v, h1v, yh1);
+        Bc = (s < LSP - 1) ? 0.0 : mdiv(Cc * Bc, h1v, yh1);
       }
       W.at(DA_T, k, lane) = T;
       W.at(DA_SS, k, lane) = Cc;
@@ -1192,10 +1386,11 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
         const double Dp = (k < M - 1) ? W.at(DA_IB, k + 1, lane) : Dnext;
         const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);  // PDEparabolic.f90:49
         const double Cc = W.at(DA_SS, k, lane);
-        const double dxm = __ldg(G.dx1 + i), dxp = __ldg(G.dx1 + i + 1), dxi = __ldg(G.dx1i + i - 1);
-        qm = Cc * Dhm / dxi / dxm;
-        qp = Cc * Dhp / dxi / dxp;
-        bq = W.at(DA_TT, k, lane) / (dxp + dxm);
+        const Line1D& L1 = G.L[0];
+        const double dxi = __ldg(L1.dxi + i - 1), ydxi = __ldg(L1.ydxi + i - 1);
+        qm = mdiv(mdiv(Cc * Dhm, dxi, ydxi), __ldg(L1.dx + i), __ldg(L1.ydx + i));
+        qp = mdiv(mdiv(Cc * Dhp, dxi, ydxi), __ldg(L1.dx + i + 1), __ldg(L1.ydx + i + 1));
+        bq = mdiv(W.at(DA_TT, k, lane), __ldg(L1.dxs + i), __ldg(L1.ydxs + i));  // dx1(i+1)+dx1(i)
       }
       W.at(DA_QP, k, lane) = qp;
       W.at(DA_QM, k, lane) = qm;
@@ -1218,60 +1413,77 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
       return W.at(DA_T, k, lane);
     };
     // identity rows: Dirichlet rows 1 and lx1 (PDEparabolic.f90:59-63, 131-136) and padding
-    auto ident = [&](int i, double& a, double& b, double& c, double& r) -> bool {
-      if (i == 1) { a = 0; b = 1; c = 0; r = tmin; return true; }
-      if (i == n) { a = 0; b = 1; c = 0; r = tmax; return true; }
-      if (i > n) { a = 0; b = 1; c = 0; r = 0; return true; }
-      return false;
-    };
+    // Dirichlet rows i = 1 and i = n and the padding rows past n are identity rows
+    auto ident_rhs = [&](int i) -> double { return (i == 1) ? tmin : (i == n) ? tmax : 0.0; };
     if (P.solver == 2) {
       // TR half step (PDEparabolic.f90:66-127), A = E = 0
-      const double tr_d = 1 / (dt / 2);
-      auto rowTR = [&](int k, double& a, double& b, double& c, double& r) {
+      const double dt2 = dt / 2, ydt2 = 1 / (dt / 2);  // 1/(dt/2) is also the diagonal term
+      auto rowTR = [&](int k, double& a, double& b, double& c) {
         const int i = 1 + lane * M + k;
-        if (ident(i, a, b, c, r)) return;
+        if (i == 1 || i >= n) {
+          a = 0; b = 1; c = 0;
+          return;
+        }
         const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
-        const double Tc = W.at(DA_T, k, lane);
         a = -(qm / 2) + bq / 2;
-        b = tr_d + qp / 2 + qm / 2;
+        b = ydt2 + qp / 2 + qm / 2;
         c = -(qp / 2) - bq / 2;
-        const double Pd = qp / 2 + qm / 2;
-        r = Tc / (dt / 2) - a * Tat(k - 1) - Pd * Tc - c * Tat(k + 1);
       };
-      refined_solve(W, M, lane, rowTR);
-      // BDF2 right-hand side (PDEparabolic.f90:167-202) into DA_T; T is not needed after
       for (int k = 0; k < M; ++k) {
         const int i = 1 + lane * M + k;
         double r;
-        if (i == 1) r = tmin;
-        else if (i == n) r = tmax;
-        else if (i > n) r = 0;
-        else r = -(1 / 3.0 * W.at(DA_T, k, lane) / (dt / 3)) + 4 / 3.0 * W.at(DA_R, k, lane) / (dt / 3);
-        W.at(DA_T, k, lane) = r;
+        if (i == 1 || i >= n) {
+          r = ident_rhs(i);
+        } else {
+          const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
+          const double a = -(qm / 2) + bq / 2, c = -(qp / 2) - bq / 2;
+          const double Tc = W.at(DA_T, k, lane);
+          const double Pd = qp / 2 + qm / 2;
+          r = mdiv(Tc, dt2, ydt2) - a * Tat(k - 1) - Pd * Tc - c * Tat(k + 1);
+        }
+        W.at(DA_RHS, k, lane) = r;
       }
-      __syncwarp();
-      const double bdf_d = 1 / (dt / 3);
-      auto rowBDF = [&](int k, double& a, double& b, double& c, double& r) {
+      refined_solve(W, M, lane, rowTR);
+      // BDF2 step (PDEparabolic.f90:167-202) from T and the TR solution
+      const double dt3 = dt / 3, ydt3 = 1 / (dt / 3);
+      for (int k = 0; k < M; ++k) {
         const int i = 1 + lane * M + k;
-        r = W.at(DA_T, k, lane);
-        if (i == 1 || i >= n) { a = 0; b = 1; c = 0; return; }
+        double r;
+        if (i == 1 || i >= n)
+          r = ident_rhs(i);
+        else
+          r = -mdiv(1 / 3.0 * W.at(DA_T, k, lane), dt3, ydt3) + mdiv(4 / 3.0 * W.at(DA_R, k, lane), dt3, ydt3);
+        W.at(DA_RHS, k, lane) = r;
+      }
+      auto rowBDF = [&](int k, double& a, double& b, double& c) {
+        const int i = 1 + lane * M + k;
+        if (i == 1 || i >= n) {
+          a = 0; b = 1; c = 0;
+          return;
+        }
         const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
         a = -qm + bq;
-        b = bdf_d + qp + qm;
+        b = ydt3 + qp + qm;
         c = -qp - bq;
       };
       refined_solve(W, M, lane, rowBDF);
     } else {
       // backward Euler (PDEparabolic.f90:250-319)
-      const double be_d = 1 / dt;
-      auto rowBE = [&](int k, double& a, double& b, double& c, double& r) {
+      const double ydt = 1 / dt;
+      for (int k = 0; k < M; ++k) {
         const int i = 1 + lane * M + k;
-        if (ident(i, a, b, c, r)) return;
+        W.at(DA_RHS, k, lane) = (i == 1 || i >= n) ? ident_rhs(i) : mdiv(W.at(DA_T, k, lane), dt, ydt);
+      }
+      auto rowBE = [&](int k, double& a, double& b, double& c) {
+        const int i = 1 + lane * M + k;
+        if (i == 1 || i >= n) {
+          a = 0; b = 1; c = 0;
+          return;
+        }
         const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
         a = -qm + bq;
-        b = be_d + qp + qm;
+        b = ydt + qp + qm;
         c = -qp - bq;
-        r = W.at(DA_T, k, lane) / dt;
       };
       refined_solve(W, M, lane, rowBE);
     }
@@ -1317,41 +1529,49 @@ __global__ void k_diffusion_ghost_floor(GridDev G, Blocks B) {
 // Rates are >= 0, so their IEEE bit patterns order like unsigned integers and the block
 // maxima combine with 64-bit atomicMax; max is exact, so the result is independent of the
 // reduction order and equals the reference's sequential loop.
-template <bool UNIT>
-__global__ void k_dt_reduce(GridDev G, Blocks B, unsigned long long* acc /*3*LSP*/, const double* dtp,
-                            int mode /*0 gridrates, 1 maxcfl*/) {
+template <bool UNIT, int MODE /*0 gridrates, 1 maxcfl*/>
+__global__ void __launch_bounds__(256, 2) k_dt_reduce(GridDev G, Blocks B, unsigned long long* acc /*3*LSP*/,
+                                                   const double* dtp) {
   const Dims d = G.d;
-  const long long nc = nci(d);
   double g1[LSP], g2[LSP], g3[LSP];
 #pragma unroll
   for (int s = 0; s < LSP; ++s) g1[s] = g2[s] = g3[s] = 0.0;
-  const double dtv = (mode == 1) ? *dtp : 0.0;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nc;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int i1 = (int)(q % d.lx1) + 1;
-    const long long r = q / d.lx1;
-    const int i2 = (int)(r % d.lx2) + 1, i3 = (int)(r / d.lx2) + 1;
+  const double dtv = (MODE == 1) ? *dtp : 0.0;
+  // warps stride over the x1 rows (i2, i3); lanes run along x1
+  const int nrow = d.lx2 * d.lx3;
+  const int lane = threadIdx.x & 31;
+  const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int row = wid; row < nrow; row += nw)
+  for (int i1 = lane + 1; i1 <= d.lx1; i1 += 32) {
+    const int i2 = row % d.lx2 + 1, i3 = row / d.lx2 + 1;
     const long long k = gi(d, i1, i2, i3);
-    const double dl1 = __ldg(G.dx1i + i1 - 1) * ldm<UNIT>(G.h1, k);
-    const double dl2 = __ldg(G.dx2i + i2 - 1) * ldm<UNIT>(G.h2, k);
-    const double dl3 = __ldg(G.dx3i + i3 - 1) * ldm<UNIT>(G.h3, k);
+    const long long mk = cmi(G, i1, i2, i3);
+    // dl = dxi*h (multifluid.f90:764-770); each is divided into 7 (or 14) rates, so one
+    // IEEE reciprocal per direction turns those into exact mdiv quotients
+    const double dl1 = __ldg(G.L[0].dxi + i1 - 1) * ldm<UNIT>(G.h1, mk);
+    const double dl2 = __ldg(G.L[1].dxi + i2 - 1) * ldm<UNIT>(G.h2, mk);
+    const double dl3 = __ldg(G.L[2].dxi + i3 - 1) * ldm<UNIT>(G.h3, mk);
+    const double y1 = 1.0 / dl1, y2 = 1.0 / dl2, y3 = 1.0 / dl3;
     const double Te = B.Ts(LSP - 1)[k];
 #pragma unroll
     for (int s = 0; s < LSP; ++s) {
       double vsnd = 0.0;
-      if (s < LSP - 1) vsnd = sqrt(KB * B.Ts(s)[k] / c_ms[s] + 5.0 / 3.0 * KB * Te / c_ms[s]);
-      if (mode == 0) {
-        g1[s] = fmax_f((vsnd + fabs(B.vs1(s)[k])) / dl1, g1[s]);
-        g2[s] = fmax_f(fabs(B.vs2(s)[k]) / dl2, g2[s]);
-        g3[s] = fmax_f(fabs(B.vs3(s)[k]) / dl3, g3[s]);
+      if (s < LSP - 1)
+        vsnd = sqrt(mdiv(KB * B.Ts(s)[k], c_ms[s], c_yms[s]) + mdiv(5.0 / 3.0 * KB * Te, c_ms[s], c_yms[s]));
+      if (MODE == 0) {
+        g1[s] = fmax_f(mdiv(vsnd + fabs(B.vs1(s)[k]), dl1, y1), g1[s]);
+        g2[s] = fmax_f(mdiv(fabs(B.vs2(s)[k]), dl2, y2), g2[s]);
+        g3[s] = fmax_f(mdiv(fabs(B.vs3(s)[k]), dl3, y3), g3[s]);
       } else {
-        g1[0] = fmax_f(dtv * (vsnd + fabs(B.vs1(s)[k])) / dl1, g1[0]);
-        g1[0] = fmax_f(dtv * fabs(B.vs2(s)[k]) / dl2, g1[0]);
-        g1[0] = fmax_f(dtv * fabs(B.vs3(s)[k]) / dl3, g1[0]);
+        g1[0] = fmax_f(mdiv(dtv * (vsnd + fabs(B.vs1(s)[k])), dl1, y1), g1[0]);
+        g1[0] = fmax_f(mdiv(dtv * fabs(B.vs2(s)[k]), dl2, y2), g1[0]);
+        g1[0] = fmax_f(mdiv(dtv * fabs(B.vs3(s)[k]), dl3, y3), g1[0]);
       }
     }
   }
-  const int nslot = (mode == 0) ? 3 * LSP : 1;
+  constexpr int nslot = (MODE == 0) ? 3 * LSP : 1;
+#pragma unroll
   for (int q = 0; q < nslot; ++q) {
     double v = (q < LSP) ? g1[q] : (q < 2 * LSP) ? g2[q - LSP] : g3[q - 2 * LSP];
     for (int o = 16; o > 0; o >>= 1) v = fmax_f(v, __shfl_down_sync(0xffffffffu, v, o));
