@@ -314,6 +314,36 @@ int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
     cp(h2.data(), ncell, &G.h2);
     cp(h3.data(), ncell, &G.h3);
     cp(yh1.data(), ncell, &G.yh1);
+    // dx{d}i*h{d} (multifluid.f90:764-770) and reciprocals; x1 ghosts are never read
+    {
+      const long long ncol = (long long)ncell / (lx1 + 4);  // (i2, i3) rows in the table
+      std::vector<double> dl(ncell), ydl(ncell);
+      const std::vector<double>* hs[3] = {&h1, &h2, &h3};
+      // with one stored x3 slice, dx3i*h3 is tabulated only when dx3i is uniform
+      bool dx3_uniform = true;
+      for (int j = 1; j < lx3; ++j) dx3_uniform = dx3_uniform && desc->dx3i[j] == desc->dx3i[0];
+      G.dl3_tab = (!inv || dx3_uniform) ? 1 : 0;
+      for (int dd = 0; dd < 3 && rc == GEM_OK; ++dd) {
+        if (dd == 2 && !G.dl3_tab) {
+          G.dl[2] = G.ydl[2] = nullptr;
+          break;
+        }
+        for (long long r = 0; r < ncol; ++r) {
+          const int i2 = (int)(r % (lx2 + 4)) - 1, i3 = inv ? 1 : (int)(r / (lx2 + 4)) - 1;
+          for (int i1 = -1; i1 <= lx1 + 2; ++i1) {
+            const size_t k = (size_t)(i1 + 1) + (size_t)r * (lx1 + 4);
+            const int ii = (dd == 0) ? i1 : (dd == 1) ? i2 : i3;
+            const int li = lxs[dd];
+            double v = 0.0;
+            if (ii >= 1 && ii <= li) v = dxi_in[dd][ii - 1] * (*hs[dd])[k];
+            dl[k] = v;
+            ydl[k] = 1.0 / v;
+          }
+        }
+        cp(dl.data(), ncell, &G.dl[dd]);
+        cp(ydl.data(), ncell, &G.ydl[dd]);
+      }
+    }
     cp(a0.data(), ncell, &G.ha1_0);
     cp(a1.data(), ncell, &G.ha1_1);
     cp(y0.data(), ncell, &G.yha1_0);
@@ -347,6 +377,7 @@ int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
   } else if (rc == GEM_OK) {
     // unit metrics: the kernels read no metric table
     G.h1 = G.h2 = G.h3 = G.yh1 = G.ha1_0 = G.ha1_1 = G.yha1_0 = G.yha1_1 = nullptr;
+    for (int dd = 0; dd < 3; ++dd) G.dl[dd] = G.ydl[dd] = nullptr;
     for (int dd = 0; dd < 3; ++dd) G.F[dd] = FaceTab{nullptr, nullptr, nullptr, nullptr, 1, 0, 0};
   }
   g->lnull = 0;
@@ -592,11 +623,11 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
   w->timer.record(0, st);
   GEM_CUDA(cudaMemsetAsync(w->acc, 0, 3 * LSP * sizeof(unsigned long long), st));
   Blocks B = blocks(g, const_cast<double*>(fluidvars), nullptr);
-  const unsigned nb = grid_for(nci(g->dev.d), 256, 4);
+  const unsigned nb = (unsigned)std::min<long long>((long long)g->dev.d.lx2 * g->dev.d.lx3, (long long)num_sms() * 8);
   if (g->dev.unit)
-    k_dt_reduce<true, 0><<<nb, 256, 0, st>>>(g->dev, B, w->acc, nullptr);
+    k_dt_reduce<true, 0><<<nb, dim3(32, LSP), 0, st>>>(g->dev, B, w->acc, nullptr);
   else
-    k_dt_reduce<false, 0><<<nb, 256, 0, st>>>(g->dev, B, w->acc, nullptr);
+    k_dt_reduce<false, 0><<<nb, dim3(32, LSP), 0, st>>>(g->dev, B, w->acc, nullptr);
   GEM_LAUNCHED("k_dt_reduce");
   k_dt_finalize<<<1, 32, 0, st>>>(w->acc, tcfl, dt_out);
   GEM_LAUNCHED("k_dt_finalize");
@@ -610,11 +641,11 @@ int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, cons
   cudaStream_t st = S(stream);
   GEM_CUDA(cudaMemsetAsync(w->acc + 24, 0, sizeof(unsigned long long), st));
   Blocks B = blocks(g, const_cast<double*>(fluidvars), nullptr);
-  const unsigned nb = grid_for(nci(g->dev.d), 256, 4);
+  const unsigned nb = (unsigned)std::min<long long>((long long)g->dev.d.lx2 * g->dev.d.lx3, (long long)num_sms() * 8);
   if (g->dev.unit)
-    k_dt_reduce<true, 1><<<nb, 256, 0, st>>>(g->dev, B, w->acc + 24, dt);
+    k_dt_reduce<true, 1><<<nb, dim3(32, LSP), 0, st>>>(g->dev, B, w->acc + 24, dt);
   else
-    k_dt_reduce<false, 1><<<nb, 256, 0, st>>>(g->dev, B, w->acc + 24, dt);
+    k_dt_reduce<false, 1><<<nb, dim3(32, LSP), 0, st>>>(g->dev, B, w->acc + 24, dt);
   GEM_LAUNCHED("k_dt_reduce");
   k_maxcfl_finalize<<<1, 32, 0, st>>>(w->acc + 24, maxcfl_out);
   GEM_LAUNCHED("k_maxcfl_finalize");

@@ -102,6 +102,8 @@ struct GridDev {
   Line1D L[3];
   const double *h1, *h2, *h3, *yh1;               // cell metric factors (ghosted), 1/h1
   const double *ha1_0, *ha1_1, *yha1_0, *yha1_1;  // h1*h2*h3, h1*h1*h2*h3 and reciprocals
+  const double *dl[3], *ydl[3];                   // dx{d}i*h{d} per cell and reciprocals
+  int dl3_tab;                                    // dl[2]/ydl[2] present (else formed in the kernel)
   FaceTab F[3];
   const unsigned char* nullpts;
 };
@@ -121,19 +123,34 @@ __device__ __forceinline__ double ldm(const double* p, long long k) {
   return __ldg(p + k);
 }
 
-// a/b from y = RN(1/b) with one exact correction (Markstein): q0 = a*y, r = a - b*q0 (exact
-// with fma), q = RN(q0 + r*y) equals the IEEE quotient RN(a/b) whenever |a|, |q0| and |y|
-// lie in (2^-900, 2^900); outside that range the IEEE division is used.  Bit-identical to
-// a/b, at the cost of a multiply and two fma.
+// a/b from y = RN(1/b) with one exact correction (Markstein's theorem): q0 = RN(a*y),
+// r = a - b*q0 (exact with fma), q = RN(q0 + r*y) equals the IEEE quotient RN(a/b) as long
+// as nothing over- or underflows, which |a| in (2^-500, 2^500) and |y| in [2^-400, 2^400]
+// guarantee (q0 and the remainder stay normal).  Both ranges are tested on the exponent
+// bits (integer pipe).  A zero numerator returns q0 = a*y, the correctly signed zero of
+// a/b; anything else out of range takes the IEEE division.
 __device__ __noinline__ double slow_div(double a, double b) { return a / b; }
 __device__ __forceinline__ double mdiv(double a, double b, double y) {
   const double q0 = a * y;
   const double r = __fma_rn(-q0, b, a);
   const double q1 = __fma_rn(r, y, q0);
-  const double aq = fabs(q0), aa = fabs(a), ay = fabs(y);
-  if (aq > 0x1p-900 && aq < 0x1p900 && aa > 0x1p-900 && aa < 0x1p900 && ay > 0x1p-900 && ay < 0x1p900)
-    return q1;
+  const unsigned ha = (unsigned)__double2hiint(a) & 0x7fffffffu;
+  const unsigned hy = (unsigned)__double2hiint(y) & 0x7fffffffu;
+  if ((ha - (523u << 20) < (1000u << 20)) & (hy - (623u << 20) < (800u << 20))) return q1;
+  if (a == 0.0 && (hy - (623u << 20) < (800u << 20))) return q0;
   return slow_div(a, b);
+}
+
+// mdiv without the fallback: clears ok when the quotient must be recomputed as a/b
+__device__ __forceinline__ double mdiv_try(double a, double b, double y, bool& ok) {
+  const double q0 = a * y;
+  const double r = __fma_rn(-q0, b, a);
+  const double q1 = __fma_rn(r, y, q0);
+  const unsigned ha = (unsigned)__double2hiint(a) & 0x7fffffffu;
+  const unsigned hy = (unsigned)__double2hiint(y) & 0x7fffffffu;
+  const bool zero = a == 0.0;
+  ok = ok && (hy - (623u << 20) < (800u << 20)) && ((ha - (523u << 20) < (1000u << 20)) || zero);
+  return zero ? q0 : q1;
 }
 
 __device__ __forceinline__ bool is_null(const GridDev& G, int i1, int i2, int i3) {
@@ -1106,13 +1123,31 @@ struct DiffArgs {
 constexpr int DA_T = 0, DA_QP = 1, DA_QM = 2, DA_BQ = 3, DA_RHS = 4, DA_SS = 5, DA_IB = 6, DA_TT = 7, DA_R = 8;
 constexpr int DNA = 9;
 
+// Row-interleaved layout: the DNA arrays of row k of every lane sit together, so one
+// pointer per row serves every array with an immediate offset:
+//   warp base + (k*DNA + arr)*32 + lane
 struct WarpMem {
-  double* p;
-  int M;
-  __device__ __forceinline__ double& at(int arr, int k, int lane) const {
-    return p[((long long)arr * M + k) * 32 + lane];
-  }
+  double* wb;  // warp base
+  double* b;   // warp base + lane
+  __device__ __forceinline__ double& at(int arr, int k) const { return b[(k * DNA + arr) * 32]; }
+  __device__ __forceinline__ double& at_lane(int arr, int k, int l) const { return wb[(k * DNA + arr) * 32 + l]; }
 };
+
+// 1/b to about one ulp for the solver's pivots and elimination multipliers (not for the
+// discretisation coefficients, which stay IEEE): two Newton-Raphson steps y <- y + y(1-by)
+// from the PTX hardware approximation rcp.approx.ftz.f64.  Zero, infinite and
+// out-of-range pivots take the IEEE reciprocal.
+__device__ __forceinline__ double rcp_nr(double b) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  const unsigned hb = (unsigned)__double2hiint(b) & 0x7fffffffu;
+  if (hb - (123u << 20) < (1800u << 20)) return y;  // 2^-900 < |b| < 2^900
+  return 1.0 / b;
+}
 
 // x**2.5 as x*x*sqrt(x) in double-double (fma for the exact product errors), rounded once:
 // correctly rounded except in vanishingly rare near-halfway cases.  The CPU checker
@@ -1147,26 +1182,26 @@ struct IfaceLU {
   double loA, loB, loC, g0;
   double e1, e2;
   double k1[5], k2[5];
-  double hiB;
+  double iloB, ihiB;  // reciprocal pivots of the lo row and of the reduced hi row
 };
 
 template <class RowM>
 __device__ __forceinline__ void band_factor(const WarpMem& W, int M, int lane, RowM rowm, IfaceLU& F) {
   double a, b, c;
   rowm(1, a, b, c);
-  double s_prev = a, c_prev = c, bp = b, ib_prev = 1.0 / b;
-  W.at(DA_SS, 1, lane) = s_prev;
-  W.at(DA_IB, 1, lane) = ib_prev;
-  W.at(DA_TT, 1, lane) = c;
+  double s_prev = a, c_prev = c, bp = b, ib_prev = rcp_nr(b);
+  W.at(DA_SS, 1) = s_prev;
+  W.at(DA_IB, 1) = ib_prev;
+  W.at(DA_TT, 1) = c;
   for (int k = 2; k < M; ++k) {
     rowm(k, a, b, c);
     const double f = a * ib_prev;
     const double sk = -f * s_prev;
     const double bk = b - f * c_prev;
-    const double ibk = 1.0 / bk;
-    W.at(DA_SS, k, lane) = sk;
-    W.at(DA_IB, k, lane) = ibk;
-    W.at(DA_TT, k, lane) = c;
+    const double ibk = rcp_nr(bk);
+    W.at(DA_SS, k) = sk;
+    W.at(DA_IB, k) = ibk;
+    W.at(DA_TT, k) = c;
     s_prev = sk;
     c_prev = c;
     bp = bk;
@@ -1175,16 +1210,16 @@ __device__ __forceinline__ void band_factor(const WarpMem& W, int M, int lane, R
   const double hiA = s_prev, hiC = c_prev;
   double hiB = bp;
   for (int k = M - 3; k >= 1; --k) {
-    const double g = W.at(DA_TT, k, lane) * W.at(DA_IB, k + 1, lane);
-    W.at(DA_SS, k, lane) = W.at(DA_SS, k, lane) - g * W.at(DA_SS, k + 1, lane);
-    W.at(DA_TT, k, lane) = -g * W.at(DA_TT, k + 1, lane);
+    const double g = W.at(DA_TT, k) * W.at(DA_IB, k + 1);
+    W.at(DA_SS, k) = W.at(DA_SS, k) - g * W.at(DA_SS, k + 1);
+    W.at(DA_TT, k) = -g * W.at(DA_TT, k + 1);
   }
   rowm(0, a, b, c);
   if (M >= 3) {
-    F.g0 = c * W.at(DA_IB, 1, lane);
+    F.g0 = c * W.at(DA_IB, 1);
     F.loA = a;
-    F.loB = b - F.g0 * W.at(DA_SS, 1, lane);
-    F.loC = -F.g0 * W.at(DA_TT, 1, lane);
+    F.loB = b - F.g0 * W.at(DA_SS, 1);
+    F.loC = -F.g0 * W.at(DA_TT, 1);
   } else {
     F.g0 = 0.0;
     F.loA = a;
@@ -1200,9 +1235,10 @@ __device__ __forceinline__ void band_factor(const WarpMem& W, int M, int lane, R
     nB = 1.0;
     nC = 0.0;
   }
-  F.e1 = hiA / F.loB;
+  F.iloB = rcp_nr(F.loB);
+  F.e1 = hiA * F.iloB;
   double A = -F.e1 * F.loA, B = hiB - F.e1 * F.loC, C = hiC;
-  F.e2 = C / nB;
+  F.e2 = C * rcp_nr(nB);
   B = B - F.e2 * nA;
   C = -F.e2 * nC;
 #pragma unroll
@@ -1222,7 +1258,7 @@ __device__ __forceinline__ void band_factor(const WarpMem& W, int M, int lane, R
       qB = 1.0;
       qC = 0.0;
     }
-    const double k1 = A / pB, k2 = C / qB;
+    const double k1 = A * rcp_nr(pB), k2 = C * rcp_nr(qB);
     F.k1[lv] = k1;
     F.k2[lv] = k2;
     const double nA2 = -k1 * pA, nC2 = -k2 * qC;
@@ -1230,7 +1266,7 @@ __device__ __forceinline__ void band_factor(const WarpMem& W, int M, int lane, R
     A = nA2;
     C = nC2;
   }
-  F.hiB = B;
+  F.ihiB = rcp_nr(B);
 }
 
 // Solve for the right-hand side in array ARR (in place: the solution replaces it).
@@ -1238,20 +1274,20 @@ template <class RowM>
 __device__ __forceinline__ void band_solve(const WarpMem& W, int M, int lane, RowM rowm, const IfaceLU& F,
                                            int ARR) {
   double a, b, c;
-  double rp = W.at(ARR, 1, lane);
+  double rp = W.at(ARR, 1);
   for (int k = 2; k < M; ++k) {
     rowm(k, a, b, c);
-    rp = W.at(ARR, k, lane) - a * W.at(DA_IB, k - 1, lane) * rp;
-    W.at(ARR, k, lane) = rp;
+    rp = W.at(ARR, k) - a * W.at(DA_IB, k - 1) * rp;
+    W.at(ARR, k) = rp;
   }
   const double hiR = rp;
-  double rn = (M >= 3) ? W.at(ARR, M - 2, lane) : 0.0;
+  double rn = (M >= 3) ? W.at(ARR, M - 2) : 0.0;
   for (int k = M - 3; k >= 1; --k) {
     rowm(k, a, b, c);
-    rn = W.at(ARR, k, lane) - c * W.at(DA_IB, k + 1, lane) * rn;
-    W.at(ARR, k, lane) = rn;
+    rn = W.at(ARR, k) - c * W.at(DA_IB, k + 1) * rn;
+    W.at(ARR, k) = rn;
   }
-  const double loR = (M >= 3) ? W.at(ARR, 0, lane) - F.g0 * W.at(ARR, 1, lane) : W.at(ARR, 0, lane);
+  const double loR = (M >= 3) ? W.at(ARR, 0) - F.g0 * W.at(ARR, 1) : W.at(ARR, 0);
   double nR = __shfl_down_sync(0xffffffffu, loR, 1);
   if (lane == 31) nR = 0.0;
   double R = hiR - F.e1 * loR;
@@ -1264,15 +1300,15 @@ __device__ __forceinline__ void band_solve(const WarpMem& W, int M, int lane, Ro
     if (lane + sh > 31) qR = 0.0;
     R = R - F.k1[lv] * pR - F.k2[lv] * qR;
   }
-  const double xl = R / F.hiB;
+  const double xl = R * F.ihiB;
   double xlp = __shfl_up_sync(0xffffffffu, xl, 1);
   if (lane == 0) xlp = 0.0;
-  const double x0 = (loR - F.loA * xlp - F.loC * xl) / F.loB;
+  const double x0 = (loR - F.loA * xlp - F.loC * xl) * F.iloB;
   for (int k = 1; k <= M - 2; ++k)
-    W.at(ARR, k, lane) =
-        (W.at(ARR, k, lane) - W.at(DA_SS, k, lane) * x0 - W.at(DA_TT, k, lane) * xl) * W.at(DA_IB, k, lane);
-  W.at(ARR, 0, lane) = x0;
-  W.at(ARR, M - 1, lane) = xl;
+    W.at(ARR, k) =
+        (W.at(ARR, k) - W.at(DA_SS, k) * x0 - W.at(DA_TT, k) * xl) * W.at(DA_IB, k);
+  W.at(ARR, 0) = x0;
+  W.at(ARR, M - 1) = xl;
 }
 
 // exact-error accumulation for the refinement residual r - (a xm + b x + c xp)
@@ -1298,22 +1334,22 @@ template <class RowM>
 __device__ void refined_solve(const WarpMem& W, int M, int lane, RowM rowm) {
   IfaceLU F;
   band_factor(W, M, lane, rowm, F);
-  for (int k = 0; k < M; ++k) W.at(DA_R, k, lane) = W.at(DA_RHS, k, lane);
+  for (int k = 0; k < M; ++k) W.at(DA_R, k) = W.at(DA_RHS, k);
   band_solve(W, M, lane, rowm, F, DA_R);
   __syncwarp();
-  const double xprev = __shfl_up_sync(0xffffffffu, W.at(DA_R, M - 1, lane), 1);
-  const double xnext = __shfl_down_sync(0xffffffffu, W.at(DA_R, 0, lane), 1);
-  double xm = xprev, xc = W.at(DA_R, 0, lane);
+  const double xprev = __shfl_up_sync(0xffffffffu, W.at(DA_R, M - 1), 1);
+  const double xnext = __shfl_down_sync(0xffffffffu, W.at(DA_R, 0), 1);
+  double xm = xprev, xc = W.at(DA_R, 0);
   for (int k = 0; k < M; ++k) {
     double a, b, c;
     rowm(k, a, b, c);
-    const double xp = (k < M - 1) ? W.at(DA_R, k + 1, lane) : xnext;
-    W.at(DA_RHS, k, lane) = residual3(W.at(DA_RHS, k, lane), a, xm, b, xc, c, xp);
+    const double xp = (k < M - 1) ? W.at(DA_R, k + 1) : xnext;
+    W.at(DA_RHS, k) = residual3(W.at(DA_RHS, k), a, xm, b, xc, c, xp);
     xm = xc;
     xc = xp;
   }
   band_solve(W, M, lane, rowm, F, DA_RHS);
-  for (int k = 0; k < M; ++k) W.at(DA_R, k, lane) = W.at(DA_R, k, lane) + W.at(DA_RHS, k, lane);
+  for (int k = 0; k < M; ++k) W.at(DA_R, k) = W.at(DA_R, k) + W.at(DA_RHS, k);
   __syncwarp();
 }
 
@@ -1325,28 +1361,34 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int M = P.M;
-  WarpMem W{smem + (long long)warp * DNA * M * 32, M};
+  WarpMem W{smem + warp * DNA * M * 32, smem + warp * DNA * M * 32 + lane};
   const int n = d.lx1;
   const double dt = *P.dtp;
   const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
   const long long nc = nci(d);
   const int wpb = blockDim.x >> 5;
+  // coalesced pass: row index idx = 32c + lane lives in the slot (lane idx/M, row idx%M)
+  const int lp0 = lane / M, kp0 = lane - lp0 * M, q32 = 32 / M, r32 = 32 - q32 * M;
   for (long long cs = (long long)blockIdx.x * wpb + warp; cs < ncs; cs += (long long)gridDim.x * wpb) {
     const int s = (int)(cs % LSP);
-    const long long col = cs / LSP;
-    const int i2 = (int)(col % d.lx2) + 1, i3 = (int)(col / d.lx2) + 1;
+    const int col = (int)(cs / LSP);
+    const int i2 = col % d.lx2 + 1, i3 = col / d.lx2 + 1;
     const long long m0 = gi(d, 0, i2, i3);  // m0 + i = cell (i, i2, i3)
+    const long long mm0 = cmi(G, 0, i2, i3);
+    const long long q0 = ci(d, 1, i2, i3) - 1;  // q0 + i: (i, i2, i3) in the interior-only arrays
     const double* Tcol = P.B.Ts(s) + m0;
     const double* ncol = P.B.ns(s) + m0;
     const double c0 = (c_gammas[s] - 1.0) / KB;
-    // ---- thermal_conduct + diffusion_prep per cell: C -> DA_SS, D -> DA_IB, B -> DA_TT
-    for (int k = 0; k < M; ++k) {
-      const int i = 1 + lane * M + k;
+    // ---- thermal_conduct + diffusion_prep per cell (collisions.f90:162-199,
+    // diffusion.f90:24-52): C -> DA_SS, D -> DA_IB, B -> DA_TT, read coalesced along x1
+    int lp = lp0, kp = kp0;
+    for (int c = 0; c < M; ++c) {
+      const int i = 1 + 32 * c + lane;
       double T = 0.0, Cc = 0.0, Dc = 0.0, Bc = 0.0;
       if (i <= n) {
         T = Tcol[i];
         const double nv = ncol[i];
-        const long long mk = cmi(G, i, i2, i3);
+        const long long mk = mm0 + i;
         const double h1v = ldm<UNIT>(G.h1, mk), h2v = ldm<UNIT>(G.h2, mk), h3v = ldm<UNIT>(G.h3, mk);
         const double yh1 = ldm<UNIT>(G.yh1, mk);
         double ha1v = 1.0, yha1v = 1.0;
@@ -1356,7 +1398,7 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
         if (s < LSP - 1) {
           lam = c_tcoef[s] * T25;
         } else {
-          const long long q = ci(d, i, i2, i3);
+          const long long q = q0 + i;
           const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
           const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sqrt(T) * (1 - 1.21e-4 * T) +
                            n3 * 2.2e-16 * (1 + 3.6e-2 * sqrt(T));
@@ -1367,38 +1409,44 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
         Dc = mdiv(lam * h2v * h3v, h1v, yh1);
         Bc = (s < LSP - 1) ? 0.0 : mdiv(Cc * Bc, h1v, yh1);
       }
-      W.at(DA_T, k, lane) = T;
-      W.at(DA_SS, k, lane) = Cc;
-      W.at(DA_IB, k, lane) = Dc;
-      W.at(DA_TT, k, lane) = Bc;
+      W.at_lane(DA_T, kp, lp) = T;
+      W.at_lane(DA_SS, kp, lp) = Cc;
+      W.at_lane(DA_IB, kp, lp) = Dc;
+      W.at_lane(DA_TT, kp, lp) = Bc;
+      kp += r32;
+      lp += q32;
+      if (kp >= M) {
+        kp -= M;
+        ++lp;
+      }
     }
     __syncwarp();
     // ---- per-row conduction factors qm = C*Dh(i)/dx1i/dx1(i), qp = C*Dh(i+1)/dx1i/dx1(i+1)
     // and advection factor bq = B/(dx1(i+1)+dx1(i)) (PDEparabolic.f90:70-80)
-    const double Dprev = __shfl_up_sync(0xffffffffu, W.at(DA_IB, M - 1, lane), 1);
-    const double Dnext = __shfl_down_sync(0xffffffffu, W.at(DA_IB, 0, lane), 1);
+    const double Dprev = __shfl_up_sync(0xffffffffu, W.at(DA_IB, M - 1), 1);
+    const double Dnext = __shfl_down_sync(0xffffffffu, W.at(DA_IB, 0), 1);
     for (int k = 0; k < M; ++k) {
       const int i = 1 + lane * M + k;
       double qp = 0.0, qm = 0.0, bq = 0.0;
       if (i >= 2 && i <= n - 1) {
-        const double Dm = (k > 0) ? W.at(DA_IB, k - 1, lane) : Dprev;
-        const double Dc = W.at(DA_IB, k, lane);
-        const double Dp = (k < M - 1) ? W.at(DA_IB, k + 1, lane) : Dnext;
+        const double Dm = (k > 0) ? W.at(DA_IB, k - 1) : Dprev;
+        const double Dc = W.at(DA_IB, k);
+        const double Dp = (k < M - 1) ? W.at(DA_IB, k + 1) : Dnext;
         const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);  // PDEparabolic.f90:49
-        const double Cc = W.at(DA_SS, k, lane);
+        const double Cc = W.at(DA_SS, k);
         const Line1D& L1 = G.L[0];
         const double dxi = __ldg(L1.dxi + i - 1), ydxi = __ldg(L1.ydxi + i - 1);
         qm = mdiv(mdiv(Cc * Dhm, dxi, ydxi), __ldg(L1.dx + i), __ldg(L1.ydx + i));
         qp = mdiv(mdiv(Cc * Dhp, dxi, ydxi), __ldg(L1.dx + i + 1), __ldg(L1.ydx + i + 1));
-        bq = mdiv(W.at(DA_TT, k, lane), __ldg(L1.dxs + i), __ldg(L1.ydxs + i));  // dx1(i+1)+dx1(i)
+        bq = mdiv(W.at(DA_TT, k), __ldg(L1.dxs + i), __ldg(L1.ydxs + i));  // dx1(i+1)+dx1(i)
       }
-      W.at(DA_QP, k, lane) = qp;
-      W.at(DA_QM, k, lane) = qm;
-      W.at(DA_BQ, k, lane) = bq;
+      W.at(DA_QP, k) = qp;
+      W.at(DA_QM, k) = qm;
+      W.at(DA_BQ, k) = bq;
     }
     __syncwarp();
-    const double Tprev = __shfl_up_sync(0xffffffffu, W.at(DA_T, M - 1, lane), 1);
-    const double Tnext = __shfl_down_sync(0xffffffffu, W.at(DA_T, 0, lane), 1);
+    const double Tprev = __shfl_up_sync(0xffffffffu, W.at(DA_T, M - 1), 1);
+    const double Tnext = __shfl_down_sync(0xffffffffu, W.at(DA_T, 0), 1);
     // Dirichlet values (diffusion.f90:54-79)
     double tmin, tmax;
     {
@@ -1410,7 +1458,7 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
     auto Tat = [&](int k) -> double {
       if (k < 0) return Tprev;
       if (k >= M) return Tnext;
-      return W.at(DA_T, k, lane);
+      return W.at(DA_T, k);
     };
     // identity rows: Dirichlet rows 1 and lx1 (PDEparabolic.f90:59-63, 131-136) and padding
     // Dirichlet rows i = 1 and i = n and the padding rows past n are identity rows
@@ -1424,7 +1472,7 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
           a = 0; b = 1; c = 0;
           return;
         }
-        const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
+        const double qp = W.at(DA_QP, k), qm = W.at(DA_QM, k), bq = W.at(DA_BQ, k);
         a = -(qm / 2) + bq / 2;
         b = ydt2 + qp / 2 + qm / 2;
         c = -(qp / 2) - bq / 2;
@@ -1435,13 +1483,13 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
         if (i == 1 || i >= n) {
           r = ident_rhs(i);
         } else {
-          const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
+          const double qp = W.at(DA_QP, k), qm = W.at(DA_QM, k), bq = W.at(DA_BQ, k);
           const double a = -(qm / 2) + bq / 2, c = -(qp / 2) - bq / 2;
-          const double Tc = W.at(DA_T, k, lane);
+          const double Tc = W.at(DA_T, k);
           const double Pd = qp / 2 + qm / 2;
           r = mdiv(Tc, dt2, ydt2) - a * Tat(k - 1) - Pd * Tc - c * Tat(k + 1);
         }
-        W.at(DA_RHS, k, lane) = r;
+        W.at(DA_RHS, k) = r;
       }
       refined_solve(W, M, lane, rowTR);
       // BDF2 step (PDEparabolic.f90:167-202) from T and the TR solution
@@ -1452,8 +1500,8 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
         if (i == 1 || i >= n)
           r = ident_rhs(i);
         else
-          r = -mdiv(1 / 3.0 * W.at(DA_T, k, lane), dt3, ydt3) + mdiv(4 / 3.0 * W.at(DA_R, k, lane), dt3, ydt3);
-        W.at(DA_RHS, k, lane) = r;
+          r = -mdiv(1 / 3.0 * W.at(DA_T, k), dt3, ydt3) + mdiv(4 / 3.0 * W.at(DA_R, k), dt3, ydt3);
+        W.at(DA_RHS, k) = r;
       }
       auto rowBDF = [&](int k, double& a, double& b, double& c) {
         const int i = 1 + lane * M + k;
@@ -1461,7 +1509,7 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
           a = 0; b = 1; c = 0;
           return;
         }
-        const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
+        const double qp = W.at(DA_QP, k), qm = W.at(DA_QM, k), bq = W.at(DA_BQ, k);
         a = -qm + bq;
         b = ydt3 + qp + qm;
         c = -qp - bq;
@@ -1472,7 +1520,7 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
       const double ydt = 1 / dt;
       for (int k = 0; k < M; ++k) {
         const int i = 1 + lane * M + k;
-        W.at(DA_RHS, k, lane) = (i == 1 || i >= n) ? ident_rhs(i) : mdiv(W.at(DA_T, k, lane), dt, ydt);
+        W.at(DA_RHS, k) = (i == 1 || i >= n) ? ident_rhs(i) : mdiv(W.at(DA_T, k), dt, ydt);
       }
       auto rowBE = [&](int k, double& a, double& b, double& c) {
         const int i = 1 + lane * M + k;
@@ -1480,7 +1528,7 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
           a = 0; b = 1; c = 0;
           return;
         }
-        const double qp = W.at(DA_QP, k, lane), qm = W.at(DA_QM, k, lane), bq = W.at(DA_BQ, k, lane);
+        const double qp = W.at(DA_QP, k), qm = W.at(DA_QM, k), bq = W.at(DA_BQ, k);
         a = -qm + bq;
         b = ydt + qp + qm;
         c = -qp - bq;
@@ -1492,7 +1540,7 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
     for (int k = 0; k < M; ++k) {
       const int i = 1 + lane * M + k;
       if (i > n) break;
-      double T = fmax_f(W.at(DA_R, k, lane), 100.0);
+      double T = fmax_f(W.at(DA_R, k), 100.0);
       if (P.fused) {
         if (is_null(G, i, i2, i3)) T = 100;
         Tout[i] = T;
@@ -1529,53 +1577,105 @@ __global__ void k_diffusion_ghost_floor(GridDev G, Blocks B) {
 // Rates are >= 0, so their IEEE bit patterns order like unsigned integers and the block
 // maxima combine with 64-bit atomicMax; max is exact, so the result is independent of the
 // reduction order and equals the reference's sequential loop.
+// Block (32, LSP): threadIdx.y is the species, lanes run along x1, blocks stride over the
+// x1 rows (i2, i3).  Each thread keeps the three running maxima of its species.
 template <bool UNIT, int MODE /*0 gridrates, 1 maxcfl*/>
-__global__ void __launch_bounds__(256, 2) k_dt_reduce(GridDev G, Blocks B, unsigned long long* acc /*3*LSP*/,
-                                                   const double* dtp) {
+__global__ void __launch_bounds__(32 * LSP, 4) k_dt_reduce(GridDev G, Blocks B, unsigned long long* acc /*3*LSP*/,
+                                                        const double* dtp) {
   const Dims d = G.d;
-  double g1[LSP], g2[LSP], g3[LSP];
-#pragma unroll
-  for (int s = 0; s < LSP; ++s) g1[s] = g2[s] = g3[s] = 0.0;
+  const int s = threadIdx.y;
+  const int lane = threadIdx.x;
+  double g1 = 0.0, g2 = 0.0, g3 = 0.0;
   const double dtv = (MODE == 1) ? *dtp : 0.0;
-  // warps stride over the x1 rows (i2, i3); lanes run along x1
   const int nrow = d.lx2 * d.lx3;
-  const int lane = threadIdx.x & 31;
-  const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
-  for (int row = wid; row < nrow; row += nw)
-  for (int i1 = lane + 1; i1 <= d.lx1; i1 += 32) {
+  const double* Tsp = B.Ts(s);
+  const double* Tep = B.Ts(LSP - 1);
+  const double* v1p = B.vs1(s);
+  const double* v2p = B.vs2(s);
+  const double* v3p = B.vs3(s);
+  const double ms = c_ms[s], yms = c_yms[s];
+  for (int row = blockIdx.x; row < nrow; row += gridDim.x) {
     const int i2 = row % d.lx2 + 1, i3 = row / d.lx2 + 1;
-    const long long k = gi(d, i1, i2, i3);
-    const long long mk = cmi(G, i1, i2, i3);
-    // dl = dxi*h (multifluid.f90:764-770); each is divided into 7 (or 14) rates, so one
-    // IEEE reciprocal per direction turns those into exact mdiv quotients
-    const double dl1 = __ldg(G.L[0].dxi + i1 - 1) * ldm<UNIT>(G.h1, mk);
-    const double dl2 = __ldg(G.L[1].dxi + i2 - 1) * ldm<UNIT>(G.h2, mk);
-    const double dl3 = __ldg(G.L[2].dxi + i3 - 1) * ldm<UNIT>(G.h3, mk);
-    const double y1 = 1.0 / dl1, y2 = 1.0 / dl2, y3 = 1.0 / dl3;
-    const double Te = B.Ts(LSP - 1)[k];
-#pragma unroll
-    for (int s = 0; s < LSP; ++s) {
-      double vsnd = 0.0;
-      if (s < LSP - 1)
-        vsnd = sqrt(mdiv(KB * B.Ts(s)[k], c_ms[s], c_yms[s]) + mdiv(5.0 / 3.0 * KB * Te, c_ms[s], c_yms[s]));
-      if (MODE == 0) {
-        g1[s] = fmax_f(mdiv(vsnd + fabs(B.vs1(s)[k]), dl1, y1), g1[s]);
-        g2[s] = fmax_f(mdiv(fabs(B.vs2(s)[k]), dl2, y2), g2[s]);
-        g3[s] = fmax_f(mdiv(fabs(B.vs3(s)[k]), dl3, y3), g3[s]);
+    const long long k0 = gi(d, 0, i2, i3);
+    const long long m0 = cmi(G, 0, i2, i3);
+    const double dx2i = __ldg(G.L[1].dxi + i2 - 1), ydx2i = __ldg(G.L[1].ydxi + i2 - 1);
+    const double dx3i = __ldg(G.L[2].dxi + i3 - 1), ydx3i = __ldg(G.L[2].ydxi + i3 - 1);
+#pragma unroll 2
+    for (int i1 = lane + 1; i1 <= d.lx1; i1 += 32) {
+      const long long k = k0 + i1;
+      // dl = dxi*h (multifluid.f90:764-770), tabulated per cell with its reciprocal
+      double dl1, y1, dl2, y2, dl3, y3;
+      if (UNIT) {
+        dl1 = __ldg(G.L[0].dxi + i1 - 1);
+        y1 = __ldg(G.L[0].ydxi + i1 - 1);
+        dl2 = dx2i;
+        y2 = ydx2i;
+        dl3 = dx3i;
+        y3 = ydx3i;
       } else {
-        g1[0] = fmax_f(mdiv(dtv * (vsnd + fabs(B.vs1(s)[k])), dl1, y1), g1[0]);
-        g1[0] = fmax_f(mdiv(dtv * fabs(B.vs2(s)[k]), dl2, y2), g1[0]);
-        g1[0] = fmax_f(mdiv(dtv * fabs(B.vs3(s)[k]), dl3, y3), g1[0]);
+        const long long mk = m0 + i1;
+        dl1 = __ldg(G.dl[0] + mk);
+        y1 = __ldg(G.ydl[0] + mk);
+        dl2 = __ldg(G.dl[1] + mk);
+        y2 = __ldg(G.ydl[1] + mk);
+        if (G.dl3_tab) {
+          dl3 = __ldg(G.dl[2] + mk);
+          y3 = __ldg(G.ydl[2] + mk);
+        } else {
+          dl3 = dx3i * __ldg(G.h3 + mk);
+          y3 = 1.0 / dl3;
+        }
+      }
+      const double T = Tsp[k], Te = Tep[k], v1 = v1p[k], v2 = v2p[k], v3 = v3p[k];
+      bool ok = true;
+      double vsnd = 0.0;
+      if (s < LSP - 1) vsnd = sqrt(mdiv_try(KB * T, ms, yms, ok) + mdiv_try(5.0 / 3.0 * KB * Te, ms, yms, ok));
+      double r1, r2, r3;
+      if (MODE == 0) {
+        r1 = mdiv_try(vsnd + fabs(v1), dl1, y1, ok);
+        r2 = mdiv_try(fabs(v2), dl2, y2, ok);
+        r3 = mdiv_try(fabs(v3), dl3, y3, ok);
+      } else {
+        r1 = mdiv_try(dtv * (vsnd + fabs(v1)), dl1, y1, ok);
+        r2 = mdiv_try(dtv * fabs(v2), dl2, y2, ok);
+        r3 = mdiv_try(dtv * fabs(v3), dl3, y3, ok);
+      }
+      if (!ok) {  // rare: a quotient outside the exact fast range
+        vsnd = 0.0;
+        if (s < LSP - 1) vsnd = sqrt(slow_div(KB * T, ms) + slow_div(5.0 / 3.0 * KB * Te, ms));
+        const double a1 = (MODE == 0) ? vsnd + fabs(v1) : dtv * (vsnd + fabs(v1));
+        const double a2 = (MODE == 0) ? fabs(v2) : dtv * fabs(v2);
+        const double a3 = (MODE == 0) ? fabs(v3) : dtv * fabs(v3);
+        r1 = slow_div(a1, dl1);
+        r2 = slow_div(a2, dl2);
+        r3 = slow_div(a3, dl3);
+      }
+      if (MODE == 0) {
+        g1 = fmax_f(r1, g1);
+        g2 = fmax_f(r2, g2);
+        g3 = fmax_f(r3, g3);
+      } else {
+        g1 = fmax_f(r1, g1);
+        g1 = fmax_f(r2, g1);
+        g1 = fmax_f(r3, g1);
       }
     }
   }
-  constexpr int nslot = (MODE == 0) ? 3 * LSP : 1;
-#pragma unroll
-  for (int q = 0; q < nslot; ++q) {
-    double v = (q < LSP) ? g1[q] : (q < 2 * LSP) ? g2[q - LSP] : g3[q - 2 * LSP];
-    for (int o = 16; o > 0; o >>= 1) v = fmax_f(v, __shfl_down_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(acc + q, (unsigned long long)__double_as_longlong(v));
+  for (int o = 16; o > 0; o >>= 1) {
+    g1 = fmax_f(g1, __shfl_down_sync(0xffffffffu, g1, o));
+    if (MODE == 0) {
+      g2 = fmax_f(g2, __shfl_down_sync(0xffffffffu, g2, o));
+      g3 = fmax_f(g3, __shfl_down_sync(0xffffffffu, g3, o));
+    }
+  }
+  if (lane == 0) {
+    if (MODE == 0) {
+      atomicMax(acc + s, (unsigned long long)__double_as_longlong(g1));
+      atomicMax(acc + LSP + s, (unsigned long long)__double_as_longlong(g2));
+      atomicMax(acc + 2 * LSP + s, (unsigned long long)__double_as_longlong(g3));
+    } else {
+      atomicMax(acc, (unsigned long long)__double_as_longlong(g1));
+    }
   }
 }
 
