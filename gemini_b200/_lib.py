@@ -67,6 +67,7 @@ _SIGS = [
     ("gem_energy_diffusion_dev", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _VP]),
     ("gem_dt_calc_dev", ctypes.c_int, [_VP, ctypes.c_double, _VP, _VP, _VP, _VP]),
     ("gem_maxcfl_dev", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
+    ("gem_dt_calc_noalloc_dev", ctypes.c_int, [_VP, ctypes.c_double, _VP, _VP, _VP]),
     ("gem_fluid_adv_dev", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("gem_fluid_adv_host", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _D, _VP]),
     ("gem_check_finite", ctypes.c_int, [_VP, _VP, _VP, ctypes.POINTER(ctypes.c_longlong), _VP]),

@@ -221,6 +221,14 @@ int launch_diffusion(const gem_grid* g, DiffArgs a, cudaStream_t st) {
 
 }  // namespace
 
+// Static scratch of gem_dt_calc_noalloc_dev: 3*LSP partial maxima per x3 plane.
+static __device__ __align__(256) double g_dt_noalloc_part[GEM_DT_NOALLOC_MAX_PLANES * 3 * LSP];
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_part_ptr[kNoallocMaxDevices] = {};
+}  // namespace
+
 extern "C" {
 
 const char* gem_last_error(void) { return g_err.c_str(); }
@@ -632,6 +640,49 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
   k_dt_finalize<<<1, 32, 0, st>>>(w->acc, tcfl, dt_out);
   GEM_LAUNCHED("k_dt_finalize");
   w->timer.record(1, st);
+  return GEM_OK;
+}
+
+// dt_calc variant that allocates nothing: its scratch (per-x3-plane partial maxima) is
+// the file-scope device array below, whose address is resolved once per device.
+int gem_dt_calc_noalloc_dev(const gem_grid* g, double tcfl, const double* fluidvars, double* dt_out,
+                            void* stream) {
+  if (check_grid(g) || !fluidvars || !dt_out) return set_err(GEM_EINVAL, "null argument");
+  const Dims& d = g->dev.d;
+  if (d.lx3 > GEM_DT_NOALLOC_MAX_PLANES)
+    return set_err(GEM_EINVAL,
+                   "gem_dt_calc_noalloc_dev: lx3=%d x3 planes exceed its static scratch of %d planes "
+                   "(use gem_dt_calc_dev)",
+                   d.lx3, GEM_DT_NOALLOC_MAX_PLANES);
+  int dev = 0;
+  GEM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocMaxDevices)
+    return set_err(GEM_EINVAL, "gem_dt_calc_noalloc_dev: device ordinal %d out of range", dev);
+  double* part = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    part = g_noalloc_part_ptr[dev];
+    if (!part) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_dt_noalloc_part);
+      if (e != cudaSuccess || !p)
+        return set_err(GEM_ECUDA, "cudaGetSymbolAddress of the no-alloc dt scratch failed: %s",
+                       cudaGetErrorString(e));
+      part = static_cast<double*>(p);
+      g_noalloc_part_ptr[dev] = part;
+    }
+  }
+  // every partial slot that the finalize reads is written by the reduce: nothing in the
+  // scratch has to start at zero
+  cudaStream_t st = S(stream);
+  Blocks B = blocks(g, const_cast<double*>(fluidvars), nullptr);
+  if (g->dev.unit)
+    k_dt_reduce_planes<true><<<d.lx3, dim3(32, LSP), 0, st>>>(g->dev, B, part);
+  else
+    k_dt_reduce_planes<false><<<d.lx3, dim3(32, LSP), 0, st>>>(g->dev, B, part);
+  GEM_LAUNCHED("k_dt_reduce_planes");
+  k_dt_finalize_planes<<<1, 32, 0, st>>>(part, d.lx3, tcfl, dt_out);
+  GEM_LAUNCHED("k_dt_finalize_planes");
   return GEM_OK;
 }
 

@@ -1679,6 +1679,60 @@ __global__ void __launch_bounds__(32 * LSP, 4) k_dt_reduce(GridDev G, Blocks B, 
   }
 }
 
+// Per-x3-plane partial maxima of the dt rates (block i3 covers the plane's x1 rows):
+// part[(i3-1)*3*LSP + slot], slot as in k_dt_reduce.  Every slot of every plane is written.
+template <bool UNIT>
+__global__ void __launch_bounds__(32 * LSP) k_dt_reduce_planes(GridDev G, Blocks B, double* part) {
+  const Dims d = G.d;
+  const int s = threadIdx.y;
+  const int lane = threadIdx.x;
+  const int i3 = blockIdx.x + 1;
+  double g1 = 0.0, g2 = 0.0, g3 = 0.0;
+  const double ms = c_ms[s];
+  const double dx3i = __ldg(G.L[2].dxi + i3 - 1);
+  for (int i2 = 1; i2 <= d.lx2; ++i2) {
+    const long long k0 = gi(d, 0, i2, i3);
+    const long long m0 = cmi(G, 0, i2, i3);
+    const double dx2i = __ldg(G.L[1].dxi + i2 - 1);
+    for (int i1 = lane + 1; i1 <= d.lx1; i1 += 32) {
+      const long long k = k0 + i1;
+      const double dl1 = __ldg(G.L[0].dxi + i1 - 1) * ldm<UNIT>(G.h1, m0 + i1);
+      const double dl2 = dx2i * ldm<UNIT>(G.h2, m0 + i1);
+      const double dl3 = dx3i * ldm<UNIT>(G.h3, m0 + i1);
+      double vsnd = 0.0;
+      if (s < LSP - 1) vsnd = sqrt(KB * B.Ts(s)[k] / ms + 5.0 / 3.0 * KB * B.Ts(LSP - 1)[k] / ms);
+      g1 = fmax_f((vsnd + fabs(B.vs1(s)[k])) / dl1, g1);
+      g2 = fmax_f(fabs(B.vs2(s)[k]) / dl2, g2);
+      g3 = fmax_f(fabs(B.vs3(s)[k]) / dl3, g3);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    g1 = fmax_f(g1, __shfl_down_sync(0xffffffffu, g1, o));
+    g2 = fmax_f(g2, __shfl_down_sync(0xffffffffu, g2, o));
+    g3 = fmax_f(g3, __shfl_down_sync(0xffffffffu, g3, o));
+  }
+  if (lane == 0) {
+    double* p = part + (long long)(i3 - 1) * 3 * LSP;
+    p[s] = g1;
+    p[LSP + s] = g2;
+    p[2 * LSP + s] = g3;
+  }
+}
+
+// max over the planes per slot, then the k_dt_finalize formula (one warp)
+__global__ void k_dt_finalize_planes(const double* part, int nplane, double tcfl, double* dt_out) {
+  const int lane = threadIdx.x;
+  double m = 0.0;
+  for (int q = 0; q < 3 * LSP; ++q) {
+    double g = 0.0;
+    for (int p = lane; p < nplane; p += 32) g = fmax_f(part[(long long)p * 3 * LSP + q], g);
+    for (int o = 16; o > 0; o >>= 1) g = fmax_f(g, __shfl_xor_sync(0xffffffffu, g, o));
+    const double inv = 1.0 / fmax_f(g, 1e-10);
+    if (q == 0 || inv < m) m = inv;
+  }
+  if (lane == 0) *dt_out = fmax_f(tcfl * m, 1e-6);
+}
+
 __global__ void k_dt_finalize(const unsigned long long* acc, double tcfl, double* dt_out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double m = 0.0;

@@ -115,6 +115,21 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
 int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, const double* dt,
                    double* maxcfl_out, void* stream);
 
+/* No counterpart in the reference.  dt_calc (the same result as gem_dt_calc_dev) for callers
+ * that cannot allocate device memory or hold a gem_work (for example code that runs inside
+ * a pool-managed or already-captured context): it calls no allocator.  Its scratch is a
+ * static device array of GEM_DT_NOALLOC_MAX_PLANES * 21 doubles (344 KiB) holding one set of
+ * partial maxima per x3 plane; grids with lx3 > GEM_DT_NOALLOC_MAX_PLANES are rejected with
+ * GEM_EINVAL.  The first call on each device, made with that device current, resolves the
+ * scratch address (cudaGetSymbolAddress), which may initialise the module: make it before
+ * any stream capture.  Nothing in the scratch has to start at zero (every partial slot read
+ * is written in the same call).  All calls on one device share the one scratch array, so
+ * calls whose executions overlap (on different streams or host threads) race: serialise
+ * them. */
+#define GEM_DT_NOALLOC_MAX_PLANES 2048
+int gem_dt_calc_noalloc_dev(const gem_grid* g, double tcfl, const double* fluidvars, double* dt_out,
+                            void* stream);
+
 /* ---- the fused fluid advance --------------------------------------------------------
  * One call = the advection + diffusion subset of fluid_adv (app/main.f90:280-355,
  * libgemini.cpp:155-210) with compression and sources excluded:
