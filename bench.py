@@ -51,6 +51,19 @@ def algorithmic_doubles_per_cell(unit_metrics: bool) -> dict:
     }
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per interior cell and launch,
+# from one ncu --set full capture of each phase's kernel on the 384x48x32 dipole case
+# (profiles/kernels_ncu_full_dipole384x48x32.md); traffic scales with the cells processed,
+# so the full-size figure is this times the cell count.  Re-measure when a kernel changes.
+NCU_TRAFFIC_BYTES_PER_CELL = {
+    "dt_calc": 142.37e6 / 589824,
+    "sweep_x3": 196.78e6 / 589824,
+    "sweep_x1": 163.58e6 / 589824,
+    "sweep_x2_epilogue": 215.91e6 / 589824,
+    "diffusion": 103.81e6 / 589824,
+}
+
+
 def build_problem(lx1, lx2, lx3, seed, perturb, kind="dipole"):
     from gemini_b200 import grid as G
     from gemini_b200 import state as S
@@ -342,7 +355,11 @@ def run_b200(args, world, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_dict(world),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                     "frac": achieved / peak,
+                     "traffic": (NCU_TRAFFIC_BYTES_PER_CELL[dom] * cells
+                                 if (not unit and dom in NCU_TRAFFIC_BYTES_PER_CELL) else None),
+                     "traffic_source": "ncu dram bytes of the 384x48x32 dipole launch, scaled by cells",
+                     "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "step_achieved_GBs": step_achieved, "step_frac": step_achieved / peak,
                      "step_algorithmic_bytes": step_bytes,

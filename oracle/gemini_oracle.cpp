@@ -1097,4 +1097,62 @@ void ora_set_num_threads(int n) {
 #endif
 }
 
+
+// Checker for the device's exact division (test infrastructure): with y = RN(1/b),
+// q0 = RN(a*y), r = fma(-q0, b, a), q = fma(r, y, q0) must equal RN(a/b) whenever the
+// device's guard accepts (|a| in [2^-500, 2^500), |y| in [2^-400, 2^400)); a zero
+// numerator returns q0.  Random operands over the guarded range plus near-representable
+// quotients (a = RN(b*q) for random q), which are the hard cases of the correction.
+// Returns the number of mismatches; *checked receives the number of guarded cases.
+long long ora_markstein_mismatches(long long n, unsigned long long seed, long long* checked) {
+  unsigned long long st = seed * 0x9E3779B97F4A7C15ull + 1;
+  auto next = [&]() {
+    st ^= st << 13;
+    st ^= st >> 7;
+    st ^= st << 17;
+    return st;
+  };
+  auto rnd = [&](int emin, int emax) {
+    const unsigned long long m = (next() >> 11) | (1ull << 52);  // 53-bit significand
+    const int e = emin + (int)(next() % (unsigned long long)(emax - emin + 1));
+    const double v = std::ldexp((double)m, e - 52);
+    return (next() & 1) ? -v : v;
+  };
+  auto guard = [](double a, double y) {
+    const double aa = std::fabs(a), ay = std::fabs(y);
+    return aa >= std::ldexp(1.0, -500) && aa < std::ldexp(1.0, 500) && ay >= std::ldexp(1.0, -400) &&
+           ay < std::ldexp(1.0, 400);
+  };
+  long long bad = 0, cnt = 0;
+  for (long long i = 0; i < n; ++i) {
+    const double b = rnd(-399, 399);
+    double a;
+    if (i % 3 == 0) {
+      a = rnd(-499, 499);
+    } else {
+      const double q = rnd(-60, 60);
+      a = b * q;  // a/b lands next to a representable quotient
+      if (i % 3 == 2) a = std::nextafter(a, (next() & 1) ? 1e308 : -1e308);
+    }
+    if (i % 1000 == 0) a = (i % 2000 == 0) ? 0.0 : -0.0;
+    const double y = 1.0 / b;
+    const double q0 = a * y;
+    const double r = std::fma(-q0, b, a);
+    const double q1 = std::fma(r, y, q0);
+    double q;
+    if (guard(a, y)) {
+      q = q1;
+    } else if (a == 0.0 && std::fabs(y) >= std::ldexp(1.0, -400) && std::fabs(y) < std::ldexp(1.0, 400)) {
+      q = q0;
+    } else {
+      continue;
+    }
+    ++cnt;
+    const double ref = a / b;
+    if (std::memcmp(&q, &ref, sizeof(double)) != 0) ++bad;
+  }
+  if (checked) *checked = cnt;
+  return bad;
+}
+
 }  // extern "C"

@@ -133,6 +133,17 @@ def pow25(x: float) -> float:
     return float(lib().ora_pow25(float(x)))
 
 
+def markstein_mismatches(n: int, seed: int = 1) -> tuple[int, int]:
+    """(mismatches, guarded cases) of the device's reciprocal-corrected division vs a/b."""
+    L = lib()
+    f = L.ora_markstein_mismatches
+    f.restype = ctypes.c_longlong
+    f.argtypes = [ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_longlong)]
+    cnt = ctypes.c_longlong(0)
+    bad = f(int(n), int(seed), ctypes.byref(cnt))
+    return int(bad), int(cnt.value)
+
+
 def set_num_threads(n: int) -> None:
     lib().ora_set_num_threads(int(n))
 
