@@ -74,6 +74,13 @@ _SIGS = [
     ("gem_work_phase_timing", ctypes.c_int, [_VP, ctypes.c_int]),
     ("gem_work_phase_times", ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int)]),
+    ("gem_batch_create", ctypes.c_int, [ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(_VP)]),
+    ("gem_batch_destroy", ctypes.c_int, [_VP]),
+    ("gem_batch_size", ctypes.c_int, [_VP]),
+    ("gem_batch_set_param", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    ("gem_batch_step", ctypes.c_int, [_VP, _VP]),
+    ("gem_batch_dts", ctypes.c_int, [_VP, _D]),
+    ("gem_batch_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]),
     ("gem_capi_bind_grid", None, [_VP]),
     ("gem_capi_set_error_mode", None, [ctypes.c_int]),
     ("gem_capi_last_status", ctypes.c_int, []),

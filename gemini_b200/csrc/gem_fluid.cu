@@ -197,6 +197,7 @@ int launch_diffusion(const gem_grid* g, DiffArgs a, cudaStream_t st) {
   int wpb = (int)std::min<size_t>(4, (227 * 1024) / per_warp);
   if (wpb < 1) return set_err(GEM_EINVAL, "lx1=%d too long for the on-chip column solver", d.lx1);
   a.M = M;
+  a.Mslot = M;
   const size_t smem = per_warp * wpb;
   const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
   long long nblk = (ncs + wpb - 1) / wpb;
@@ -839,3 +840,5 @@ int gem_check_finite(const gem_grid* g, const double* fluidvars, gem_work* w, lo
 }
 
 }  // extern "C"
+
+#include "gem_batch.cuh"

@@ -79,6 +79,12 @@ __device__ __forceinline__ long long f3i(const Dims& d, int i1, int i2, int i3) 
 }
 __host__ __device__ __forceinline__ long long nf3(const Dims& d) { return (long long)d.lx1 * d.lx2 * (d.lx3 + 1); }
 
+// Block coordinate of a kernel body: the launch's own blockIdx / gridDim for the plain
+// kernels, or the (block, per-instance grid extent) of a work item for the batched ones.
+struct VB {
+  int bx, by, gx;
+};
+
 // 1-D tables of one sweep direction (meshobj.f90:356-389 differences and their correctly
 // rounded reciprocals, for the exact reciprocal-corrected division mdiv below)
 struct Line1D {
@@ -275,11 +281,11 @@ __global__ void k_clean_elementwise(GridDev G, double* param, int iparm) {
 
 // clean_param(2) border fix along field lines (multifluid.f90:614-654), one thread per
 // (column, species).  The null-point scan reproduces the reference's loop bounds exactly.
-__global__ void k_clean_vel_edges(GridDev G, double* vs1) {
+__device__ __forceinline__ void b_clean_vel_edges(const GridDev& G, double* vs1, const VB vb) {
   const Dims d = G.d;
   const long long ncol = (long long)d.lx2 * d.lx3;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncol * LSP;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = vb.bx * (long long)blockDim.x + threadIdx.x; t < ncol * LSP;
+       t += (long long)vb.gx * blockDim.x) {
     const int s = (int)(t / ncol);
     const long long c = t - s * ncol;
     const int i2 = (int)(c % d.lx2) + 1, i3 = (int)(c / d.lx2) + 1;
@@ -298,6 +304,11 @@ __global__ void k_clean_vel_edges(GridDev G, double* vs1) {
     }
   }
 }
+
+__global__ void k_clean_vel_edges(GridDev G, double* vs1) {
+  b_clean_vel_edges(G, vs1, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
 
 // ======================================================================================
 // 4. Global-boundary ghost fill (advec.f90:21-149) and the single-grid halo
@@ -331,12 +342,12 @@ struct GhostSrc {
 // interior momentum/energy values are also materialised for ghost columns (pass B/C read
 // them), interior columns keep them implicit.
 template <bool CONV>
-__global__ void k_ghost_x1(GridDev G, Blocks B, const double* __restrict__ vs1i, int lsp) {
+__device__ __forceinline__ void b_ghost_x1(const GridDev& G, const Blocks& B, const double* __restrict__ vs1i, int lsp, const VB vb) {
   const Dims d = G.d;
   const int n2 = d.lx2 + 4, n3 = d.lx3 + 4;
   const long long ncol = (long long)n2 * n3;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncol * lsp;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = vb.bx * (long long)blockDim.x + threadIdx.x; t < ncol * lsp;
+       t += (long long)vb.gx * blockDim.x) {
     const int s = (int)(t / ncol);
     const long long c = t - s * ncol;
     const int j2 = (int)(c % n2) - 1, j3 = (int)(c / n2) - 1;
@@ -408,15 +419,21 @@ __global__ void k_ghost_x1(GridDev G, Blocks B, const double* __restrict__ vs1i,
   }
 }
 
+template <bool CONV>
+__global__ void k_ghost_x1(GridDev G, Blocks B, const double* __restrict__ vs1i, int lsp) {
+  b_ghost_x1<CONV>(G, B, vs1i, lsp, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
+
 // Pass B (advec.f90:83-104): x2 ghost rows := edge rows, for vs2, ns, rhovs1, rhoes, every
 // x1 (incl. ghosts) and every x3 (incl. ghosts).  One thread per (i1, i3, species).
 template <bool CONV>
-__global__ void k_ghost_x2(GridDev G, Blocks B, int lsp) {
+__device__ __forceinline__ void b_ghost_x2(const GridDev& G, const Blocks& B, int lsp, const VB vb) {
   const Dims d = G.d;
   const int n1 = d.lx1 + 4, n3 = d.lx3 + 4;
   const long long nrow = (long long)n1 * n3;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nrow * lsp;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = vb.bx * (long long)blockDim.x + threadIdx.x; t < nrow * lsp;
+       t += (long long)vb.gx * blockDim.x) {
     const int s = (int)(t / nrow);
     const long long c = t - s * nrow;
     const int i1 = (int)(c % n1) - 1, i3 = (int)(c / n1) - 1;
@@ -442,17 +459,23 @@ __global__ void k_ghost_x2(GridDev G, Blocks B, int lsp) {
   }
 }
 
+template <bool CONV>
+__global__ void k_ghost_x2(GridDev G, Blocks B, int lsp) {
+  b_ghost_x2<CONV>(G, B, lsp, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
+
 // Pass C.  Non-periodic (advec.f90:107-132): x3 ghost slabs := edge slabs for vs3, ns,
 // rhovs1, rhoes over every x1 and x2.  Periodic with WRAP (the halo_fluidvars self-wrap,
 // mpihalo.f90:147-151, lhalo = 2): rows 1:lx2, every x1, for ns, rhovs1, rhoes, vs2, vs3.
 // One thread per (i1, i2, species).
 template <bool CONV, bool WRAP>
-__global__ void k_ghost_x3(GridDev G, Blocks B, int lsp) {
+__device__ __forceinline__ void b_ghost_x3(const GridDev& G, const Blocks& B, int lsp, const VB vb) {
   const Dims d = G.d;
   const int n1 = d.lx1 + 4, n2 = d.lx2 + 4;
   const long long nrow = (long long)n1 * n2;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nrow * lsp;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = vb.bx * (long long)blockDim.x + threadIdx.x; t < nrow * lsp;
+       t += (long long)vb.gx * blockDim.x) {
     const int s = (int)(t / nrow);
     const long long c = t - s * nrow;
     const int i1 = (int)(c % n1) - 1, i2 = (int)(c / n1) - 1;
@@ -495,6 +518,12 @@ __global__ void k_ghost_x3(GridDev G, Blocks B, int lsp) {
     }
   }
 }
+
+template <bool CONV, bool WRAP>
+__global__ void k_ghost_x3(GridDev G, Blocks B, int lsp) {
+  b_ghost_x3<CONV, WRAP>(G, B, lsp, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
 
 // Halo wrap only (standalone halo_allparams / halo_fluidvars): rows 1:lx2, all x1.
 __global__ void k_halo_wrap(GridDev G, Blocks B, int with_v23) {
@@ -603,7 +632,8 @@ struct SweepArgs {
   const double* vsi;  // standalone: vs{dim}i (all species)
   double* vs1i;       // fused x1: boundary faces written here
   const double* dtp;
-  int which;  // standalone field set
+  double* dtp_w;  // writable alias of dtp (batched dt finalize); unused by the sweeps
+  int which;      // standalone field set
 };
 
 // Running state of one field while marching j = 0..lx+1 along a line:
@@ -664,7 +694,7 @@ __device__ __forceinline__ void cell_metric(const GridDev& G, long long k, int f
 
 // ---- x2 / x3 sweeps ---------------------------------------------------------------------
 template <int DIM, bool UNIT, bool FUSED>
-__global__ void __launch_bounds__(224, 2) k_sweep_march(SweepArgs P) {
+__device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
   const GridDev& G = P.G;
   const Dims d = G.d;
   const Blocks& B = P.B;
@@ -673,8 +703,8 @@ __global__ void __launch_bounds__(224, 2) k_sweep_march(SweepArgs P) {
   const Line1D& L = G.L[DIM - 1];
   const FaceTab& FT = G.F[DIM - 1];
   // line coordinates: DIM3 (i1, i2), DIM2 (i1, i3)
-  const int a = blockIdx.x * 32 + threadIdx.x + 1;
-  const int b = blockIdx.y + 1;
+  const int a = vb.bx * 32 + threadIdx.x + 1;
+  const int b = vb.by + 1;
   const bool valid = a <= d.lx1;
   const int aa = valid ? a : d.lx1;  // idle lanes read a valid line
   const int lx = (DIM == 3) ? d.lx3 : d.lx2;
@@ -923,20 +953,26 @@ __global__ void __launch_bounds__(224, 2) k_sweep_march(SweepArgs P) {
   }
 }
 
+template <int DIM, bool UNIT, bool FUSED>
+__global__ void __launch_bounds__(224, 2) k_sweep_march(SweepArgs P) {
+  b_sweep_march<DIM, UNIT, FUSED>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
+
 // ---- x1 sweep: lanes along the column ------------------------------------------------------
 // Lane l of chunk c handles position p = 32c + l - 1... the chunk covers p = 32c .. 32c+31 over
 // p = 0 .. lx1+1: the slope at cell p, the flux P(p) = ha2i(p)*phi(p) at face p, and the update
 // of cell p-1 (which needs P(p) and P(p-1)).  Values crossing the chunk edge (slope(p-1),
 // P(p-1)) are carried from lane 31 of the previous chunk.
 template <bool UNIT, bool FUSED>
-__global__ void __launch_bounds__(224) k_sweep_x1(SweepArgs P) {
+__device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
   const GridDev& G = P.G;
   const Dims d = G.d;
   const Blocks& B = P.B;
   const double dt = *P.dtp;
   const int s = threadIdx.y;
   const int lane = threadIdx.x;
-  const int i2 = blockIdx.x + 1, i3 = blockIdx.y + 1;
+  const int i2 = vb.bx + 1, i3 = vb.by + 1;
   const int n = d.lx1;
   const Line1D& L = G.L[0];
   const FaceTab& FT = G.F[0];
@@ -1060,13 +1096,19 @@ __global__ void __launch_bounds__(224) k_sweep_x1(SweepArgs P) {
   }
 }
 
+template <bool UNIT, bool FUSED>
+__global__ void __launch_bounds__(224) k_sweep_x1(SweepArgs P) {
+  b_sweep_x1<UNIT, FUSED>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
+
 // Fused step: the same epilogue for every ghost cell (rhov12v1 on the ghost values, then
 // clean_param(1) sets density ghosts to mindensdiv and clean_param(3) temperature ghosts to
 // 100; T2rhoe of those constants gives the final energy-density ghosts).
-__global__ void k_ghost_epilogue(GridDev G, Blocks B) {
+__device__ __forceinline__ void b_ghost_epilogue(const GridDev& G, const Blocks& B, const VB vb) {
   const Dims d = G.d;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < d.ng;
-       k += (long long)gridDim.x * blockDim.x) {
+  for (long long k = vb.bx * (long long)blockDim.x + threadIdx.x; k < d.ng;
+       k += (long long)vb.gx * blockDim.x) {
     int i1, i2, i3;
     decode_cell(d, k, i1, i2, i3);
     if (!is_ghost(d, i1, i2, i3)) continue;
@@ -1086,6 +1128,11 @@ __global__ void k_ghost_epilogue(GridDev G, Blocks B) {
     }
   }
 }
+
+__global__ void k_ghost_epilogue(GridDev G, Blocks B) {
+  b_ghost_epilogue(G, B, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
 
 // ======================================================================================
 // 7. Field-aligned heat diffusion (multifluid.f90:309-342; collisions.f90:162-199;
@@ -1115,6 +1162,7 @@ struct DiffArgs {
   double Teinf;
   int solver;  // 1 backward Euler, 2 TRBDF2
   int M;       // rows per lane
+  int Mslot;   // rows per lane that each warp's shared-memory slot is sized for (>= M)
   int fused;   // 1: clean_param(3) + T2rhoe folded into the store
 };
 
@@ -1354,14 +1402,14 @@ __device__ void refined_solve(const WarpMem& W, int M, int lane, RowM rowm) {
 }
 
 template <bool UNIT>
-__global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
+__device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
   extern __shared__ double smem[];
   const GridDev& G = P.G;
   const Dims d = G.d;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int M = P.M;
-  WarpMem W{smem + warp * DNA * M * 32, smem + warp * DNA * M * 32 + lane};
+  WarpMem W{smem + warp * DNA * P.Mslot * 32, smem + warp * DNA * P.Mslot * 32 + lane};
   const int n = d.lx1;
   const double dt = *P.dtp;
   const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
@@ -1369,7 +1417,7 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
   const int wpb = blockDim.x >> 5;
   // coalesced pass: row index idx = 32c + lane lives in the slot (lane idx/M, row idx%M)
   const int lp0 = lane / M, kp0 = lane - lp0 * M, q32 = 32 / M, r32 = 32 - q32 * M;
-  for (long long cs = (long long)blockIdx.x * wpb + warp; cs < ncs; cs += (long long)gridDim.x * wpb) {
+  for (long long cs = (long long)vb.bx * wpb + warp; cs < ncs; cs += (long long)vb.gx * wpb) {
     const int s = (int)(cs % LSP);
     const int col = (int)(cs / LSP);
     const int i2 = col % d.lx2 + 1, i3 = col / d.lx2 + 1;
@@ -1557,6 +1605,12 @@ __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
   }
 }
 
+template <bool UNIT>
+__global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
+  b_diffusion<UNIT>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
+
 // standalone energy_diffusion: max(T,100) on the ghost cells other than the x1 BC layers
 __global__ void k_diffusion_ghost_floor(GridDev G, Blocks B) {
   const Dims d = G.d;
@@ -1580,8 +1634,8 @@ __global__ void k_diffusion_ghost_floor(GridDev G, Blocks B) {
 // Block (32, LSP): threadIdx.y is the species, lanes run along x1, blocks stride over the
 // x1 rows (i2, i3).  Each thread keeps the three running maxima of its species.
 template <bool UNIT, int MODE /*0 gridrates, 1 maxcfl*/>
-__global__ void __launch_bounds__(32 * LSP, 4) k_dt_reduce(GridDev G, Blocks B, unsigned long long* acc /*3*LSP*/,
-                                                        const double* dtp) {
+__device__ __forceinline__ void b_dt_reduce(const GridDev& G, const Blocks& B, unsigned long long* acc /*3*LSP*/,
+                                                        const double* dtp, const VB vb) {
   const Dims d = G.d;
   const int s = threadIdx.y;
   const int lane = threadIdx.x;
@@ -1594,7 +1648,7 @@ __global__ void __launch_bounds__(32 * LSP, 4) k_dt_reduce(GridDev G, Blocks B, 
   const double* v2p = B.vs2(s);
   const double* v3p = B.vs3(s);
   const double ms = c_ms[s], yms = c_yms[s];
-  for (int row = blockIdx.x; row < nrow; row += gridDim.x) {
+  for (int row = vb.bx; row < nrow; row += vb.gx) {
     const int i2 = row % d.lx2 + 1, i3 = row / d.lx2 + 1;
     const long long k0 = gi(d, 0, i2, i3);
     const long long m0 = cmi(G, 0, i2, i3);
@@ -1678,6 +1732,13 @@ __global__ void __launch_bounds__(32 * LSP, 4) k_dt_reduce(GridDev G, Blocks B, 
     }
   }
 }
+
+template <bool UNIT, int MODE /*0 gridrates, 1 maxcfl*/>
+__global__ void __launch_bounds__(32 * LSP, 4) k_dt_reduce(GridDev G, Blocks B, unsigned long long* acc /*3*LSP*/,
+                                                        const double* dtp) {
+  b_dt_reduce<UNIT, MODE>(G, B, acc, dtp, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
 
 // Per-x3-plane partial maxima of the dt rates (block i3 covers the plane's x1 rows):
 // part[(i3-1)*3*LSP + slot], slot as in k_dt_reduce.  Every slot of every plane is written.

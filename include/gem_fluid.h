@@ -130,6 +130,32 @@ int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, cons
 int gem_dt_calc_noalloc_dev(const gem_grid* g, double tcfl, const double* fluidvars, double* dt_out,
                             void* stream);
 
+/* ---- batched instances ---------------------------------------------------------------
+ * No counterpart in the reference (which runs one simulation per MPI job): n independent
+ * simulations, each with its own grid, work object, state blocks (device) and gem_cfg,
+ * advanced together.  One gem_batch_step = gem_dt_calc_dev(cfg.tcfl) + gem_fluid_adv_dev
+ * for every instance, with the same results bit for bit.  Each phase of the step is one
+ * persistent launch over an (instance, block) work list, largest instances first, and the
+ * step's launches are captured once into a CUDA graph that later calls replay (on any
+ * stream).  Each instance's dt is computed into its work object's dt slot (gem_work_dt).
+ * The batch keeps pointers to the objects it was given: they must outlive it and must not
+ * move.  Tuning parameters (gem_batch_set_param) rebuild the work lists and the graph. */
+typedef struct gem_batch gem_batch;
+#define GEM_BATCH_USE_GRAPH 0  /* 1 (default): capture the step into a CUDA graph */
+#define GEM_BATCH_DIFF_WARPS 1 /* warps (columns) per diffusion block, 1..4 */
+#define GEM_BATCH_GRID_PCT 2   /* persistent grid size, % of the occupancy limit (10..400) */
+int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works, double* const* fluidvars,
+                     double* const* fluidauxvars, const double* const* electrovars, const gem_cfg* cfgs,
+                     gem_batch** out);
+int gem_batch_destroy(gem_batch* b);
+int gem_batch_size(const gem_batch* b);
+int gem_batch_set_param(gem_batch* b, int param, int value);
+int gem_batch_step(gem_batch* b, void* stream);
+/* per-instance dt of the last step (synchronous device->host copies) */
+int gem_batch_dts(const gem_batch* b, double* host_dt);
+/* launches per step and (instance, block) work items per step */
+int gem_batch_info(const gem_batch* b, int* launches_per_step, long long* items_per_step);
+
 /* ---- the fused fluid advance --------------------------------------------------------
  * One call = the advection + diffusion subset of fluid_adv (app/main.f90:280-355,
  * libgemini.cpp:155-210) with compression and sources excluded:
