@@ -377,6 +377,89 @@ def run_b200(args, world, rank, local):
     return line
 
 
+BATCHED = dict(instances=64, seed=2024, perturb=0.2)
+
+
+def run_batched(args, world, rank):
+    """The uneven-instance batch: instances sharded across ranks by cost, each rank's shard
+    advanced by gem_batch_step (graph replay), timed over args.batch_steps steps; then the
+    same instances as sequential plain solves (dt_calc + fluid_adv one after another)."""
+    import torch
+    import torch.distributed as dist
+
+    from gemini_b200 import batch as BT
+    from gemini_b200 import fluid as F
+    from gemini_b200 import workloads as WL
+
+    specs = WL.batched_specs(BATCHED["instances"], BATCHED["seed"])
+    mine = WL.shard(specs, world, rank)
+    insts = []
+    for i in mine:
+        g = WL.make_grid(specs[i])
+        dg = F.DeviceGrid(g)
+        ds = WL.device_state(dg, g, specs[i].seed, BATCHED["perturb"])
+        insts.append((dg, ds, F.FluidCfg(ds.Teinf)))
+    torch.cuda.synchronize()
+    b = BT.Batch(insts)
+    stream = torch.cuda.current_stream()
+    from gemini_b200 import autotune as AT
+    tuned = AT.tune(b, steps=2)
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms_b = timed(b.step, args.batch_steps)
+
+    def sequential():
+        for dg, ds, cfg in insts:
+            BT.plain_step(dg, ds, cfg)
+
+    ms_s = timed(sequential, max(1, args.batch_steps // 2))
+    seq_steps = max(1, args.batch_steps // 2)
+    total_cells = sum(s.cells for s in specs)
+    my_cells = sum(specs[i].cells for i in mine)
+    cells_t = torch.tensor([float(my_cells)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(cells_t)
+    launches, items = b.info()
+    fin = [F.check_finite(ds) for _, ds, _ in insts]
+    out = {
+        "workload": f"{len(specs)} instances, lx1~U{{64..512}}, lx2,lx3~U{{16..128}}, Cartesian/dipole 50/50, "
+                    f"seeded per instance, {total_cells} cells in total",
+        "value": float(cells_t.item()) * LSP * args.batch_steps / (ms_b / 1e3) / 1e9,
+        "unit": UNIT, "ms_per_step": ms_b / args.batch_steps, "steps": args.batch_steps,
+        "sequential_plain_value": float(cells_t.item()) * LSP * seq_steps / (ms_s / 1e3) / 1e9,
+        "sequential_plain_ms_per_step": ms_s / seq_steps,
+        "launches_per_step": launches, "work_items_per_step": items,
+        "graph": "one CUDA graph per step (replayed)", "instances_on_rank0": len(mine),
+        "autotune": {"params": {("grid_pct" if k == 2 else "diff_warps" if k == 1 else str(k)): v
+                                for k, v in tuned["params"].items()},
+                     "cached": tuned["cached"],
+                     "trials_ms": [round(t["ms_per_step"], 3) for t in tuned["trials"]]},
+        "sharding": "longest-processing-time over cells x species, no collective on the data path",
+        "nonfinite_cells": int(sum(fin)),
+    }
+    b.close()
+    for dg, ds, _ in insts:
+        ds.close()
+        dg.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,6 +469,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched instances")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-instance measurement")
     ap.add_argument("--lx", type=int, nargs=3, default=None, metavar=("LX1", "LX2", "LX3"),
                     help="override the grid size (profiling runs on a smaller case)")
     args = ap.parse_args()
@@ -400,6 +485,10 @@ def main():
         return
     world, rank, local = dist_setup(args.gpus)
     line = run_b200(args, world, rank, local)
+    if not args.no_batched and not args.lx:
+        import torch
+        torch.cuda.empty_cache()
+        line["batched"] = run_batched(args, world, rank)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -14,8 +14,16 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libgemini_b200.so")
 SOURCES = ["gem_fluid.cu", "gem_capi_ref.cpp"]
-HEADERS = ["gem_kernels.cuh", os.path.join("..", "..", "include", "gem_fluid.h"),
-           os.path.join("..", "..", "include", "gemini3d_fluid.h")]
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+
+def _headers() -> list[str]:
+    """Every header the library build reads (csrc/*.cuh, *.h and include/*.h)."""
+    out = []
+    for d in (CSRC, INCLUDE):
+        if os.path.isdir(d):
+            out += [os.path.join(d, f) for f in sorted(os.listdir(d)) if f.endswith((".cuh", ".h"))]
+    return out
 
 # -fmad=false: no contraction of a*b+c, so the advection and its ghost/epilogue arithmetic
 # round exactly like the reference's (gfortran on x86-64 emits no FMA without -march).
@@ -34,8 +42,7 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    for f in SOURCES + HEADERS:
-        p = os.path.join(CSRC, f)
+    for p in [os.path.join(CSRC, f) for f in SOURCES] + _headers():
         if os.path.exists(p) and os.path.getmtime(p) > t:
             return True
     return False

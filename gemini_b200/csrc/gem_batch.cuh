@@ -22,15 +22,12 @@ struct InstDev {
 // work item: instance, block x, block y, the instance's own grid x extent
 using Item = int4;
 
+template <bool UNIT>
 __global__ void __launch_bounds__(32 * LSP, 4) kb_dt_reduce(const InstDev* __restrict__ inst, const Item* __restrict__ it, int n) {
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
     const Item q = it[w];
     const InstDev& I = inst[q.x];
-    const VB vb{q.y, q.z, q.w};
-    if (I.sw.G.unit)
-      b_dt_reduce<true, 0>(I.sw.G, I.sw.B, I.acc, nullptr, vb);
-    else
-      b_dt_reduce<false, 0>(I.sw.G, I.sw.B, I.acc, nullptr, vb);
+    b_dt_reduce<UNIT, 0>(I.sw.G, I.sw.B, I.acc, nullptr, VB{q.y, q.z, q.w});
   }
 }
 
@@ -80,29 +77,22 @@ __global__ void __launch_bounds__(128) kb_ghost_x3(const InstDev* __restrict__ i
   }
 }
 
-template <int DIM>
+template <int DIM, bool UNIT>
 __global__ void __launch_bounds__(224, 2) kb_sweep_march(const InstDev* __restrict__ inst, const Item* __restrict__ it, int n) {
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
     const Item q = it[w];
     const InstDev& I = inst[q.x];
-    const VB vb{q.y, q.z, q.w};
-    if (I.sw.G.unit)
-      b_sweep_march<DIM, true, true>(I.sw, vb);
-    else
-      b_sweep_march<DIM, false, true>(I.sw, vb);
+    b_sweep_march<DIM, UNIT, true>(I.sw, VB{q.y, q.z, q.w});
     if (DIM == 2) __syncthreads();  // the epilogue's shared buffers are reused by the next item
   }
 }
 
+template <bool UNIT>
 __global__ void __launch_bounds__(224) kb_sweep_x1(const InstDev* __restrict__ inst, const Item* __restrict__ it, int n) {
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
     const Item q = it[w];
     const InstDev& I = inst[q.x];
-    const VB vb{q.y, q.z, q.w};
-    if (I.sw.G.unit)
-      b_sweep_x1<true, true>(I.sw, vb);
-    else
-      b_sweep_x1<false, true>(I.sw, vb);
+    b_sweep_x1<UNIT, true>(I.sw, VB{q.y, q.z, q.w});
   }
 }
 
@@ -122,14 +112,16 @@ __global__ void __launch_bounds__(128) kb_clean_vel_edges(const InstDev* __restr
   }
 }
 
-__global__ void __launch_bounds__(128) kb_diffusion(const InstDev* __restrict__ inst, const Item* __restrict__ it, int n) {
+// one launch per (metric variant, rows-per-lane bucket); every instance of the launch
+// uses the bucket's slot size Mslot (>= its own M)
+template <bool UNIT>
+__global__ void __launch_bounds__(128) kb_diffusion(const InstDev* __restrict__ inst, const Item* __restrict__ it, int n,
+                                                   int Mslot) {
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
     const Item q = it[w];
     const InstDev& I = inst[q.x];
-    if (I.df.G.unit)
-      b_diffusion<true>(I.df, VB{q.y, q.z, q.w});
-    else
-      b_diffusion<false>(I.df, VB{q.y, q.z, q.w});
+    (void)Mslot;  // I.df.Mslot holds the instance's bucket slot size (set on the host)
+    b_diffusion<UNIT>(I.df, VB{q.y, q.z, q.w});
   }
 }
 
@@ -140,14 +132,20 @@ __global__ void __launch_bounds__(128) kb_diffusion(const InstDev* __restrict__ 
 // ---------------------------------------------------------------------------------------
 namespace {
 
-enum BatchPhase {
-  BP_DT = 0, BP_GX1, BP_GX2, BP_GX3, BP_SW3, BP_SW1, BP_SW2, BP_EPI, BP_CVE, BP_DIFF, BP_N
+// One launch of the batched step: a phase, its variant (metric variant; for the diffusion
+// also the rows-per-lane bucket) and the work items of the instances it covers.
+enum BatchKernel {
+  BK_DT = 0, BK_GX1, BK_GX2, BK_GX3, BK_SW3, BK_SW1, BK_SW2, BK_EPI, BK_CVE, BK_DIFF, BK_N
 };
 
-struct PhaseList {
+struct BatchLaunch {
+  int kernel = 0;
+  int unit = 0;
+  int Mslot = 0, wpb = 0;  // diffusion only
+  size_t smem = 0;
+  int grid = 0;
   std::vector<Item> items;
   Item* d_items = nullptr;
-  int grid = 0;  // persistent blocks
 };
 
 }  // namespace
@@ -157,9 +155,8 @@ struct gem_batch {
   std::vector<const gem_grid*> grids;
   std::vector<gem_work*> works;
   InstDev* d_inst = nullptr;
-  PhaseList ph[BP_N];
-  int Mmax = 2, wpb = 4;
-  size_t diff_smem = 0;
+  std::vector<BatchLaunch> launches;  // in step order
+  int wpb_max = 4;
   int per_sm_scale = 100;  // percent of the occupancy-limited persistent grid
   cudaStream_t cap_stream = nullptr;
   cudaGraph_t graph = nullptr;
@@ -169,78 +166,132 @@ struct gem_batch {
 
 namespace {
 
-// per-instance block counts of each phase, as the plain launchers size them
-void instance_items(const gem_grid* g, int idx, int wpb, std::vector<Item>* out) {
-  const Dims& d = g->dev.d;
-  auto add1 = [&](int ph, long long nb) {
-    for (long long b = 0; b < nb; ++b) out[ph].push_back(make_int4(idx, (int)b, 0, (int)nb));
-  };
-  add1(BP_DT, std::min<long long>((long long)d.lx2 * d.lx3, (long long)num_sms() * 8));
-  add1(BP_GX1, grid_for((long long)(d.lx2 + 4) * (d.lx3 + 4) * LSP, 128));
-  add1(BP_GX2, grid_for((long long)(d.lx1 + 4) * (d.lx3 + 4) * LSP, 128));
-  add1(BP_GX3, grid_for((long long)(d.lx1 + 4) * (d.lx2 + 4) * LSP, 128));
-  const int gx13 = (d.lx1 + 31) / 32;
-  for (int by = 0; by < d.lx2; ++by)
-    for (int bx = 0; bx < gx13; ++bx) out[BP_SW3].push_back(make_int4(idx, bx, by, gx13));
-  for (int by = 0; by < d.lx3; ++by)
-    for (int bx = 0; bx < d.lx2; ++bx) out[BP_SW1].push_back(make_int4(idx, bx, by, d.lx2));
-  for (int by = 0; by < d.lx3; ++by)
-    for (int bx = 0; bx < gx13; ++bx) out[BP_SW2].push_back(make_int4(idx, bx, by, gx13));
-  add1(BP_EPI, grid_for(d.ng, 256));
-  if (g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1))
-    add1(BP_CVE, grid_for((long long)d.lx2 * d.lx3 * LSP, 128));
-  const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
-  add1(BP_DIFF, std::min<long long>((ncs + wpb - 1) / wpb, (long long)num_sms() * 2));
+int diff_M(const gem_grid* g) { return std::max(2, (g->dev.d.lx1 + 31) / 32); }
+// rows-per-lane buckets: instances share a launch (and a slot size) within a bucket
+int diff_bucket_M(int M) { return M <= 4 ? 4 : M <= 8 ? 8 : M <= 12 ? 12 : M <= 16 ? 16 : ((M + 7) / 8) * 8; }
+
+void add_items(BatchLaunch& L, int idx, long long nbx, int nby = 1) {
+  for (int by = 0; by < nby; ++by)
+    for (long long bx = 0; bx < nbx; ++bx) L.items.push_back(make_int4(idx, (int)bx, by, (int)nbx));
 }
 
 template <class K>
-int persistent_grid(K kernel, int threads, size_t smem, size_t nitems, int scale_pct, int* out) {
+int occupancy_grid(K kernel, int threads, size_t smem, size_t nitems, int scale_pct, int* out) {
+  if (scale_pct == 0) {  // one block per work item: the hardware scheduler balances
+    *out = (int)std::max<size_t>(1, nitems);
+    return GEM_OK;
+  }
   int per_sm = 0;
   GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
   if (per_sm < 1) per_sm = 1;
   long long g = (long long)num_sms() * per_sm * scale_pct / 100;
-  if (g < 1) g = 1;
-  if (g > (long long)nitems) g = (long long)nitems;
-  *out = (int)std::max<long long>(g, 1);
+  g = std::max<long long>(1, std::min<long long>(g, (long long)nitems));
+  *out = (int)g;
   return GEM_OK;
 }
 
+int launch_grid(gem_batch* b, BatchLaunch& L) {
+  const size_t n = L.items.size();
+  const int sc = b->per_sm_scale;
+  const bool u = L.unit != 0;
+  switch (L.kernel) {
+    case BK_DT: return u ? occupancy_grid(kb_dt_reduce<true>, 32 * LSP, 0, n, sc, &L.grid)
+                         : occupancy_grid(kb_dt_reduce<false>, 32 * LSP, 0, n, sc, &L.grid);
+    case BK_GX1: return occupancy_grid(kb_ghost_x1, 128, 0, n, sc, &L.grid);
+    case BK_GX2: return occupancy_grid(kb_ghost_x2, 128, 0, n, sc, &L.grid);
+    case BK_GX3: return occupancy_grid(kb_ghost_x3, 128, 0, n, sc, &L.grid);
+    case BK_SW3: return u ? occupancy_grid(kb_sweep_march<3, true>, 32 * LSP, 0, n, sc, &L.grid)
+                          : occupancy_grid(kb_sweep_march<3, false>, 32 * LSP, 0, n, sc, &L.grid);
+    case BK_SW1: return u ? occupancy_grid(kb_sweep_x1<true>, 32 * LSP, 0, n, sc, &L.grid)
+                          : occupancy_grid(kb_sweep_x1<false>, 32 * LSP, 0, n, sc, &L.grid);
+    case BK_SW2: return u ? occupancy_grid(kb_sweep_march<2, true>, 32 * LSP, 0, n, sc, &L.grid)
+                          : occupancy_grid(kb_sweep_march<2, false>, 32 * LSP, 0, n, sc, &L.grid);
+    case BK_EPI: return occupancy_grid(kb_ghost_epilogue, 256, 0, n, sc, &L.grid);
+    case BK_CVE: return occupancy_grid(kb_clean_vel_edges, 128, 0, n, sc, &L.grid);
+    case BK_DIFF:
+      // the dynamic shared-memory limit was raised to the largest bucket's size beforehand
+      return u ? occupancy_grid(kb_diffusion<true>, 32 * L.wpb, L.smem, n, sc, &L.grid)
+               : occupancy_grid(kb_diffusion<false>, 32 * L.wpb, L.smem, n, sc, &L.grid);
+  }
+  return set_err(GEM_EINVAL, "unknown batched kernel %d", L.kernel);
+}
+
 int batch_build_lists(gem_batch* b) {
-  std::vector<Item> lists[BP_N];
+  for (auto& L : b->launches)
+    if (L.d_items) cudaFree(L.d_items);
+  b->launches.clear();
   // largest instances first, so the long items start early
   std::vector<int> order(b->n);
   for (int i = 0; i < b->n; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return b->grids[x]->dev.d.ng > b->grids[y]->dev.d.ng;
-  });
-  for (int i : order) instance_items(b->grids[i], i, b->wpb, lists);
-  for (int p = 0; p < BP_N; ++p) {
-    PhaseList& L = b->ph[p];
-    if (L.d_items) cudaFree(L.d_items);
-    L.d_items = nullptr;
-    L.items = lists[p];
-    if (!L.items.empty()) {
-      if (cudaMalloc(&L.d_items, L.items.size() * sizeof(Item)) != cudaSuccess)
-        return set_err(GEM_ENOMEM, "cudaMalloc of a batch work list failed");
-      GEM_CUDA(cudaMemcpy(L.d_items, L.items.data(), L.items.size() * sizeof(Item), cudaMemcpyHostToDevice));
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return b->grids[x]->dev.d.ng > b->grids[y]->dev.d.ng; });
+  auto launch_for = [&](int kernel, int unit, int Mslot = 0) -> BatchLaunch& {
+    for (auto& L : b->launches)
+      if (L.kernel == kernel && L.unit == unit && L.Mslot == Mslot) return L;
+    BatchLaunch L;
+    L.kernel = kernel;
+    L.unit = unit;
+    L.Mslot = Mslot;
+    b->launches.push_back(L);
+    return b->launches.back();
+  };
+  // create the launches in step order (variants of one phase next to each other)
+  for (int k = 0; k < BK_N; ++k) {
+    for (int u = 1; u >= 0; --u) {
+      for (int i : order) {
+        const gem_grid* g = b->grids[i];
+        const Dims& d = g->dev.d;
+        const bool unit = g->dev.unit != 0;
+        const bool variant = (k == BK_DT || k == BK_SW3 || k == BK_SW1 || k == BK_SW2 || k == BK_DIFF);
+        if (variant && unit != (u == 1)) continue;
+        if (!variant && u == 0) continue;  // unsplit phases: once
+        const int gx13 = (d.lx1 + 31) / 32;
+        switch (k) {
+          case BK_DT:
+            add_items(launch_for(k, u), i, std::min<long long>((long long)d.lx2 * d.lx3, (long long)num_sms() * 8));
+            break;
+          case BK_GX1: add_items(launch_for(k, 0), i, grid_for((long long)(d.lx2 + 4) * (d.lx3 + 4) * LSP, 128)); break;
+          case BK_GX2: add_items(launch_for(k, 0), i, grid_for((long long)(d.lx1 + 4) * (d.lx3 + 4) * LSP, 128)); break;
+          case BK_GX3: add_items(launch_for(k, 0), i, grid_for((long long)(d.lx1 + 4) * (d.lx2 + 4) * LSP, 128)); break;
+          case BK_SW3: add_items(launch_for(k, u), i, gx13, d.lx2); break;
+          case BK_SW1: add_items(launch_for(k, u), i, d.lx2, d.lx3); break;
+          case BK_SW2: add_items(launch_for(k, u), i, gx13, d.lx3); break;
+          case BK_EPI: add_items(launch_for(k, 0), i, grid_for(d.ng, 256)); break;
+          case BK_CVE:
+            if (g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1))
+              add_items(launch_for(k, 0), i, grid_for((long long)d.lx2 * d.lx3 * LSP, 128));
+            break;
+          case BK_DIFF: {
+            const int Ms = diff_bucket_M(diff_M(g));
+            BatchLaunch& L = launch_for(k, u, Ms);
+            const size_t per_warp = (size_t)DNA * Ms * 32 * sizeof(double);
+            L.wpb = (int)std::max<size_t>(1, std::min<size_t>((size_t)b->wpb_max, (227 * 1024) / per_warp));
+            L.smem = per_warp * L.wpb;
+            const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
+            add_items(L, i, std::min<long long>((ncs + L.wpb - 1) / L.wpb, (long long)num_sms() * 2));
+            break;
+          }
+        }
+      }
     }
   }
-  b->diff_smem = (size_t)DNA * b->Mmax * 32 * sizeof(double) * b->wpb;
-  GEM_CUDA(cudaFuncSetAttribute(kb_diffusion, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->diff_smem));
-  int rc = GEM_OK;
-  const int sc = b->per_sm_scale;
-  if ((rc = persistent_grid(kb_dt_reduce, 32 * LSP, 0, b->ph[BP_DT].items.size(), sc, &b->ph[BP_DT].grid))) return rc;
-  if ((rc = persistent_grid(kb_ghost_x1, 128, 0, b->ph[BP_GX1].items.size(), sc, &b->ph[BP_GX1].grid))) return rc;
-  if ((rc = persistent_grid(kb_ghost_x2, 128, 0, b->ph[BP_GX2].items.size(), sc, &b->ph[BP_GX2].grid))) return rc;
-  if ((rc = persistent_grid(kb_ghost_x3, 128, 0, b->ph[BP_GX3].items.size(), sc, &b->ph[BP_GX3].grid))) return rc;
-  if ((rc = persistent_grid(kb_sweep_march<3>, 32 * LSP, 0, b->ph[BP_SW3].items.size(), sc, &b->ph[BP_SW3].grid))) return rc;
-  if ((rc = persistent_grid(kb_sweep_x1, 32 * LSP, 0, b->ph[BP_SW1].items.size(), sc, &b->ph[BP_SW1].grid))) return rc;
-  if ((rc = persistent_grid(kb_sweep_march<2>, 32 * LSP, 0, b->ph[BP_SW2].items.size(), sc, &b->ph[BP_SW2].grid))) return rc;
-  if ((rc = persistent_grid(kb_ghost_epilogue, 256, 0, b->ph[BP_EPI].items.size(), sc, &b->ph[BP_EPI].grid))) return rc;
-  if ((rc = persistent_grid(kb_clean_vel_edges, 128, 0, std::max<size_t>(1, b->ph[BP_CVE].items.size()), sc,
-                            &b->ph[BP_CVE].grid))) return rc;
-  if ((rc = persistent_grid(kb_diffusion, 32 * b->wpb, b->diff_smem, b->ph[BP_DIFF].items.size(), sc,
-                            &b->ph[BP_DIFF].grid))) return rc;
+  // one function attribute per kernel variant: the largest shared memory of its launches
+  size_t smem_max[2] = {0, 0};
+  for (const auto& L : b->launches)
+    if (L.kernel == BK_DIFF) smem_max[L.unit ? 1 : 0] = std::max(smem_max[L.unit ? 1 : 0], L.smem);
+  if (smem_max[1])
+    GEM_CUDA(cudaFuncSetAttribute(kb_diffusion<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max[1]));
+  if (smem_max[0])
+    GEM_CUDA(cudaFuncSetAttribute(kb_diffusion<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max[0]));
+  for (auto& L : b->launches) {
+    if (L.kernel == BK_DIFF && (size_t)DNA * L.Mslot * 32 * sizeof(double) > 227 * 1024)
+      return set_err(GEM_EINVAL, "lx1 too long for the on-chip column solver (rows per lane %d)", L.Mslot);
+    if (cudaMalloc(&L.d_items, L.items.size() * sizeof(Item)) != cudaSuccess)
+      return set_err(GEM_ENOMEM, "cudaMalloc of a batch work list failed");
+    GEM_CUDA(cudaMemcpy(L.d_items, L.items.data(), L.items.size() * sizeof(Item), cudaMemcpyHostToDevice));
+    const int rc = launch_grid(b, L);
+    if (rc) return rc;
+  }
   return GEM_OK;
 }
 
@@ -251,23 +302,45 @@ void batch_drop_graph(gem_batch* b) {
   b->graph = nullptr;
 }
 
-// the eleven launches of one batched step
 int batch_enqueue(gem_batch* b, cudaStream_t st) {
   const InstDev* I = b->d_inst;
-  auto n = [&](int p) { return (int)b->ph[p].items.size(); };
   kb_zero_acc<<<b->n, 32, 0, st>>>(I, b->n);
-  kb_dt_reduce<<<b->ph[BP_DT].grid, dim3(32, LSP), 0, st>>>(I, b->ph[BP_DT].d_items, n(BP_DT));
-  kb_dt_finalize<<<(b->n + 63) / 64, 64, 0, st>>>(I, b->n);
-  kb_ghost_x1<<<b->ph[BP_GX1].grid, 128, 0, st>>>(I, b->ph[BP_GX1].d_items, n(BP_GX1));
-  kb_ghost_x2<<<b->ph[BP_GX2].grid, 128, 0, st>>>(I, b->ph[BP_GX2].d_items, n(BP_GX2));
-  kb_ghost_x3<<<b->ph[BP_GX3].grid, 128, 0, st>>>(I, b->ph[BP_GX3].d_items, n(BP_GX3));
-  kb_sweep_march<3><<<b->ph[BP_SW3].grid, dim3(32, LSP), 0, st>>>(I, b->ph[BP_SW3].d_items, n(BP_SW3));
-  kb_sweep_x1<<<b->ph[BP_SW1].grid, dim3(32, LSP), 0, st>>>(I, b->ph[BP_SW1].d_items, n(BP_SW1));
-  kb_sweep_march<2><<<b->ph[BP_SW2].grid, dim3(32, LSP), 0, st>>>(I, b->ph[BP_SW2].d_items, n(BP_SW2));
-  kb_ghost_epilogue<<<b->ph[BP_EPI].grid, 256, 0, st>>>(I, b->ph[BP_EPI].d_items, n(BP_EPI));
-  if (n(BP_CVE) > 0)
-    kb_clean_vel_edges<<<b->ph[BP_CVE].grid, 128, 0, st>>>(I, b->ph[BP_CVE].d_items, n(BP_CVE));
-  kb_diffusion<<<b->ph[BP_DIFF].grid, 32 * b->wpb, b->diff_smem, st>>>(I, b->ph[BP_DIFF].d_items, n(BP_DIFF));
+  bool finalized = false;
+  for (const auto& L : b->launches) {
+    const int n = (int)L.items.size();
+    const bool u = L.unit != 0;
+    if (L.kernel != BK_DT && !finalized) {
+      kb_dt_finalize<<<(b->n + 63) / 64, 64, 0, st>>>(I, b->n);
+      finalized = true;
+    }
+    switch (L.kernel) {
+      case BK_DT:
+        if (u) kb_dt_reduce<true><<<L.grid, dim3(32, LSP), 0, st>>>(I, L.d_items, n);
+        else kb_dt_reduce<false><<<L.grid, dim3(32, LSP), 0, st>>>(I, L.d_items, n);
+        break;
+      case BK_GX1: kb_ghost_x1<<<L.grid, 128, 0, st>>>(I, L.d_items, n); break;
+      case BK_GX2: kb_ghost_x2<<<L.grid, 128, 0, st>>>(I, L.d_items, n); break;
+      case BK_GX3: kb_ghost_x3<<<L.grid, 128, 0, st>>>(I, L.d_items, n); break;
+      case BK_SW3:
+        if (u) kb_sweep_march<3, true><<<L.grid, dim3(32, LSP), 0, st>>>(I, L.d_items, n);
+        else kb_sweep_march<3, false><<<L.grid, dim3(32, LSP), 0, st>>>(I, L.d_items, n);
+        break;
+      case BK_SW1:
+        if (u) kb_sweep_x1<true><<<L.grid, dim3(32, LSP), 0, st>>>(I, L.d_items, n);
+        else kb_sweep_x1<false><<<L.grid, dim3(32, LSP), 0, st>>>(I, L.d_items, n);
+        break;
+      case BK_SW2:
+        if (u) kb_sweep_march<2, true><<<L.grid, dim3(32, LSP), 0, st>>>(I, L.d_items, n);
+        else kb_sweep_march<2, false><<<L.grid, dim3(32, LSP), 0, st>>>(I, L.d_items, n);
+        break;
+      case BK_EPI: kb_ghost_epilogue<<<L.grid, 256, 0, st>>>(I, L.d_items, n); break;
+      case BK_CVE: kb_clean_vel_edges<<<L.grid, 128, 0, st>>>(I, L.d_items, n); break;
+      case BK_DIFF:
+        if (u) kb_diffusion<true><<<L.grid, 32 * L.wpb, L.smem, st>>>(I, L.d_items, n, L.Mslot);
+        else kb_diffusion<false><<<L.grid, 32 * L.wpb, L.smem, st>>>(I, L.d_items, n, L.Mslot);
+        break;
+    }
+  }
   GEM_LAUNCHED("batched step");
   return GEM_OK;
 }
@@ -285,7 +358,6 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
   std::vector<InstDev> h(n);
   gem_batch* b = new gem_batch();
   b->n = n;
-  int Mmax = 2;
   for (int i = 0; i < n; ++i) {
     const gem_grid* g = grids[i];
     gem_work* w = works[i];
@@ -307,8 +379,7 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
       delete b;
       return set_err(GEM_EINVAL, "gem_batch_create: instance %d: work and grid sizes differ", i);
     }
-    const int M = std::max(2, (g->dev.d.lx1 + 31) / 32);
-    Mmax = std::max(Mmax, M);
+    const int M = diff_M(g);
     InstDev& I = h[i];
     std::memset(&I, 0, sizeof(I));
     I.sw.G = g->dev;
@@ -327,19 +398,12 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
     I.df.Teinf = cfgs[i].Teinf;
     I.df.solver = cfgs[i].diffsolvetype;
     I.df.M = M;
+    I.df.Mslot = diff_bucket_M(M);  // the slot size of the instance's diffusion launch
     I.df.fused = 1;
     I.acc = w->acc;
     I.tcfl = cfgs[i].tcfl;
     b->grids.push_back(g);
     b->works.push_back(w);
-  }
-  b->Mmax = Mmax;
-  for (int i = 0; i < n; ++i) h[i].df.Mslot = Mmax;  // one slot size: warps move between instances
-  const size_t per_warp = (size_t)DNA * Mmax * 32 * sizeof(double);
-  b->wpb = (int)std::min<size_t>(4, (227 * 1024) / per_warp);
-  if (b->wpb < 1) {
-    delete b;
-    return set_err(GEM_EINVAL, "gem_batch_create: lx1 too long for the on-chip column solver");
   }
   int rc = GEM_OK;
   if (cudaMalloc(&b->d_inst, sizeof(InstDev) * n) != cudaSuccess) {
@@ -362,8 +426,8 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
 int gem_batch_destroy(gem_batch* b) {
   if (!b) return GEM_OK;
   batch_drop_graph(b);
-  for (int p = 0; p < BP_N; ++p)
-    if (b->ph[p].d_items) cudaFree(b->ph[p].d_items);
+  for (auto& L : b->launches)
+    if (L.d_items) cudaFree(L.d_items);
   if (b->d_inst) cudaFree(b->d_inst);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   delete b;
@@ -379,12 +443,11 @@ int gem_batch_set_param(gem_batch* b, int param, int value) {
     return GEM_OK;
   }
   if (param == GEM_BATCH_DIFF_WARPS) {
-    const size_t per_warp = (size_t)DNA * b->Mmax * 32 * sizeof(double);
-    if (value < 1 || value > 4 || per_warp * value > 227 * 1024)
-      return set_err(GEM_EINVAL, "diffusion warps per block %d: 1..4 within 227 KB of shared memory", value);
-    b->wpb = value;
+    if (value < 1 || value > 4) return set_err(GEM_EINVAL, "diffusion warps per block %d: 1..4", value);
+    b->wpb_max = value;
   } else if (param == GEM_BATCH_GRID_PCT) {
-    if (value < 10 || value > 400) return set_err(GEM_EINVAL, "persistent grid percentage %d: 10..400", value);
+    if (value != 0 && (value < 10 || value > 400))
+      return set_err(GEM_EINVAL, "persistent grid percentage %d: 0 (one block per item) or 10..400", value);
     b->per_sm_scale = value;
   } else {
     return set_err(GEM_EINVAL, "unknown batch parameter %d", param);
@@ -422,13 +485,9 @@ int gem_batch_dts(const gem_batch* b, double* host_dt) {
 
 int gem_batch_info(const gem_batch* b, int* launches_per_step, long long* items_per_step) {
   if (!b) return set_err(GEM_EINVAL, "null batch");
-  int l = 3;  // zero, dt reduce, dt finalize
   long long it = 0;
-  for (int p = 0; p < BP_N; ++p) {
-    it += (long long)b->ph[p].items.size();
-    if (p != BP_DT && !b->ph[p].items.empty()) ++l;
-  }
-  if (launches_per_step) *launches_per_step = l;
+  for (const auto& L : b->launches) it += (long long)L.items.size();
+  if (launches_per_step) *launches_per_step = (int)b->launches.size() + 2;  // + zero, dt finalize
   if (items_per_step) *items_per_step = it;
   return GEM_OK;
 }

@@ -143,7 +143,8 @@ int gem_dt_calc_noalloc_dev(const gem_grid* g, double tcfl, const double* fluidv
 typedef struct gem_batch gem_batch;
 #define GEM_BATCH_USE_GRAPH 0  /* 1 (default): capture the step into a CUDA graph */
 #define GEM_BATCH_DIFF_WARPS 1 /* warps (columns) per diffusion block, 1..4 */
-#define GEM_BATCH_GRID_PCT 2   /* persistent grid size, % of the occupancy limit (10..400) */
+#define GEM_BATCH_GRID_PCT 2   /* persistent grid size, % of the occupancy limit (10..400);
+                                  0: one block per work item (no persistence) */
 int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works, double* const* fluidvars,
                      double* const* fluidauxvars, const double* const* electrovars, const gem_cfg* cfgs,
                      gem_batch** out);

@@ -60,7 +60,8 @@ def test_batch_equals_plain_steps(use_graph):
         assert_identical(dsb.to_host(st), dsp.to_host(st), what=f"batched {name}")
         assert dtb == dtp, name
     launches, items = b.info()
-    assert launches <= 12 and items > len(insts)
+    # zero + finalize + per phase one launch per metric variant (+ diffusion row buckets)
+    assert launches <= 2 + 4 * 2 + 5 + 2 * 5 and items > len(insts)
 
 
 def test_batch_params_do_not_change_results():
@@ -92,3 +93,49 @@ def test_batch_rejects_bad_params():
         b.set_param(BT.DIFF_WARPS, 9)
     with pytest.raises(_lib.GemError):
         b.set_param(99, 1)
+
+
+def test_device_generated_uneven_batch_matches_plain():
+    """Instances generated on the device (the bench's generator) with lx1 spread over
+    several diffusion row buckets (rows per lane 2..17): batched == plain, finite."""
+    import torch
+
+    from gemini_b200 import workloads as WL
+
+    specs = WL.batched_specs(6, seed=11, lx1=(40, 540), lx23=(3, 6))
+    specs = specs + [WL.InstanceSpec("dipole", 530, 4, 3, 99), WL.InstanceSpec("cartesian", 260, 3, 4, 98)]
+
+    def build():
+        out = []
+        for sp in specs:
+            g = WL.make_grid(sp)
+            dg = F.DeviceGrid(g)
+            ds = WL.device_state(dg, g, sp.seed)
+            out.append((dg, ds, F.FluidCfg(ds.Teinf)))
+        return out
+
+    batched, plain = build(), build()
+    b = BT.Batch(batched)
+    for _ in range(2):
+        b.step()
+        for dg, ds, cfg in plain:
+            BT.plain_step(dg, ds, cfg)
+    torch.cuda.synchronize()
+    for (_, db, _), (_, dp, _) in zip(batched, plain):
+        assert torch.equal(db.fluidvars, dp.fluidvars)
+        assert torch.equal(db.fluidauxvars, dp.fluidauxvars)
+        assert F.check_finite(db) == 0
+    assert (b.dts() > 0).all()
+
+
+def test_autotune_picks_and_caches(tmp_path, monkeypatch):
+    from gemini_b200 import autotune as AT
+
+    monkeypatch.setenv("GEMINI_B200_CACHE", str(tmp_path / "tune.json"))
+    insts = _instances()[:3]
+    b = BT.Batch(_device(insts))
+    r = AT.tune(b, steps=1)
+    assert not r["cached"] and len(r["trials"]) == len(AT.CANDIDATES)
+    b2 = BT.Batch(_device(insts))
+    r2 = AT.tune(b2, steps=1)
+    assert r2["cached"] and r2["params"] == r["params"]
