@@ -54,6 +54,7 @@ _SIGS = [
     ("gem_work_interface_vels", ctypes.c_int, [_VP, ctypes.c_int, _VP, ctypes.c_int]),
     ("gem_work_array", _VP, [_VP, ctypes.c_int]),
     ("gem_work_dt", _VP, [_VP]),
+    ("gem_work_set_top_temperature", ctypes.c_int, [_VP, _VP, ctypes.c_int]),
     ("gem_v12rhov1_dev", ctypes.c_int, [_VP, _VP, _VP, _VP]),
     ("gem_T2rhoe_dev", ctypes.c_int, [_VP, _VP, _VP, _VP]),
     ("gem_rhov12v1_dev", ctypes.c_int, [_VP, _VP, _VP, _VP]),

@@ -1,0 +1,236 @@
+"""Differentiable fluid advance: gradients of a loss of the final state with respect to the
+initial ion densities and the per-column top (exospheric) temperature.
+
+``FluidAdvance.apply(n0, Ttop, problem)`` runs ``problem.nsteps`` steps of the CUDA step
+(``gem_fluid_adv_dev``) on a frozen time-step schedule (dt_calc is not differentiated; the
+schedule comes from one plain run of the unperturbed problem), saving the state every
+``problem.checkpoint_every`` steps.  The backward pass recomputes each segment from its
+checkpoint with the CUDA step and pulls the cotangent back one step at a time with the
+step's vector-Jacobian product; the VJP of a step is ``torchstep.step`` differentiated by
+torch.autograd (its energy diffusion optionally replaced by the hand-written CUDA adjoint).
+
+State carried between steps: ns, vs1, Ts (interior; the step rebuilds every ghost cell) and
+the two x1 boundary faces of vs1i (read, one step stale, by set_global_boundaries); vs2,
+vs3, nn, Tn, J1 are inputs of the problem.  Grids without null cells.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from . import fluid as F
+from . import torchstep as TS
+from .state import LSP
+
+
+class _CudaArray:
+    """__cuda_array_interface__ view of a raw device pointer (float64)."""
+
+    def __init__(self, ptr: int, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+class DiffProblem:
+    """One differentiable problem: grid, fixed inputs, dt schedule, scratch device state."""
+
+    def __init__(self, grid, st, nsteps: int, checkpoint_every: int = 5, tcfl: float = 0.5,
+                 diffsolvetype: int = 2, device="cuda"):
+        import torch
+
+        self.grid = grid
+        self.nsteps = int(nsteps)
+        self.k = max(1, int(checkpoint_every))
+        self.diffsolvetype = diffsolvetype
+        self.tg = TS.tgrid(grid, device)
+        self.dg = F.DeviceGrid(grid)
+        self.ds = F.DeviceState.from_host(self.dg, st.copy())
+        self.cfg = F.FluidCfg(st.Teinf, diffsolvetype=diffsolvetype, tcfl=tcfl)
+        X1, X2, X3 = grid.lx1 + 4, grid.lx2 + 4, grid.lx3 + 4
+        self.shape = (5 * LSP, X3, X2, X1)
+        self.base = self.ds.fluidvars.view(self.shape).clone()
+        self.vs2 = self.base[2 * LSP:3 * LSP]
+        self.vs3 = self.base[3 * LSP:4 * LSP]
+        self.nn = torch.from_numpy(np.ascontiguousarray(st.nn.transpose(3, 2, 1, 0))).to(device)
+        self.Tn = torch.from_numpy(np.ascontiguousarray(st.Tn.transpose(2, 1, 0))).to(device)
+        self.J1 = torch.from_numpy(np.ascontiguousarray(st.electrovars[..., 3].transpose(2, 1, 0))).to(device)
+        self.Teinf = float(st.Teinf)
+        self.v1i = torch.as_tensor(_CudaArray(_lib.lib().gem_work_array(self.ds.work, 1),
+                                              (LSP, grid.lx3, grid.lx2, grid.lx1 + 1)), device=device)
+        self.lo0 = self.v1i[..., 0].clone()
+        self.hi0 = self.v1i[..., -1].clone()
+        # the frozen schedule: dt_calc of a plain run from the base state
+        self.dts = []
+        self._load(self.base[0:LSP], self.base[LSP:2 * LSP], self.base[4 * LSP:], self.lo0, self.hi0, None)
+        for _ in range(self.nsteps):
+            dt = F.dt_calc(self.ds, tcfl)
+            self.dts.append(float(dt.item()))
+            F.fluid_adv(self.cfg, self.ds, dt)
+
+    # -- CUDA state plumbing -------------------------------------------------------------
+    def _load(self, ns, vs1, Ts, lo, hi, Ttop):
+        fv = self.ds.fluidvars.view(self.shape)
+        fv.copy_(self.base)
+        fv[0:LSP] = ns
+        fv[LSP:2 * LSP] = vs1
+        fv[4 * LSP:] = Ts
+        self.v1i[..., 0] = lo
+        self.v1i[..., -1] = hi
+        if Ttop is None:
+            _lib.check(_lib.lib().gem_work_set_top_temperature(self.ds.work, None, 0))
+        else:
+            t = Ttop.detach().contiguous()
+            _lib.check(_lib.lib().gem_work_set_top_temperature(self.ds.work, ctypes.c_void_p(t.data_ptr()), 1))
+
+    def _save(self):
+        fv = self.ds.fluidvars.view(self.shape)
+        return (fv[0:LSP].clone(), fv[LSP:2 * LSP].clone(), fv[4 * LSP:].clone(),
+                self.v1i[..., 0].clone(), self.v1i[..., -1].clone())
+
+    def cuda_step(self, j: int) -> None:
+        import torch
+
+        dt = torch.full((1,), self.dts[j], dtype=torch.float64, device=self.ds.fluidvars.device)
+        F.fluid_adv(self.cfg, self.ds, dt)
+
+    def initial_state(self, n0, Ttop=None):
+        """Full-layout initial state with the ion densities n0 (6, lx3, lx2, lx1) in the
+        interior; the electrons are their sum (as in the state generator)."""
+        import torch
+
+        g = self.grid
+        ns = self.base[0:LSP].clone()
+        I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
+        ions = n0
+        e = ions[0]
+        for s in range(1, LSP - 1):
+            e = e + ions[s]
+        inner = torch.cat([ions, e.unsqueeze(0)], 0)
+        ns = ns.clone()
+        ns[(slice(None),) + I] = inner
+        return ns
+
+    def run(self, n0, Ttop=None, keep=False):
+        """CUDA forward from the controls; returns the final (ns, vs1, Ts) tensors and, with
+        keep, the checkpoints {step: state}."""
+        ns = self.initial_state(n0.detach())
+        st = (ns, self.base[LSP:2 * LSP], self.base[4 * LSP:], self.lo0, self.hi0)
+        self._load(*st, Ttop)
+        ckpt = {}
+        for j in range(self.nsteps):
+            if keep and j % self.k == 0:
+                ckpt[j] = self._save()
+            self.cuda_step(j)
+        out = self._save()
+        return out, ckpt
+
+    def step_vjp(self, state, Ttop, j, cot, use_cuda_diffusion_adjoint=False):
+        """Pull the cotangent of the state after step j back to the state before it (and
+        to Ttop).  state / cot: (ns, vs1, Ts, lo, hi)."""
+        import torch
+
+        inp = [t.detach().requires_grad_(True) for t in state]
+        tt = None if Ttop is None else Ttop.detach().requires_grad_(True)
+        with torch.enable_grad():
+            out = TS.step(self.tg, inp[0], inp[1], self.vs2, self.vs3, inp[2], inp[3], inp[4], self.nn,
+                          self.Tn, self.J1, self.dts[j], self.Teinf, tt, self.diffsolvetype)
+            pairs = [(o, c) for o, c in zip(out, cot) if c is not None]
+            wrt = inp + ([tt] if tt is not None else [])
+            grads = torch.autograd.grad([o for o, _ in pairs], wrt, [c for _, c in pairs], allow_unused=True)
+        g_state = [torch.zeros_like(t) if g is None else g for g, t in zip(grads[:5], inp)]
+        g_top = None if tt is None else (torch.zeros_like(tt) if grads[5] is None else grads[5])
+        return g_state, g_top
+
+
+class FluidAdvance:
+    """torch.autograd.Function factory bound to a DiffProblem."""
+
+    @staticmethod
+    def apply(n0, Ttop, problem: DiffProblem):
+        return _Fn.apply(n0, Ttop, problem)
+
+
+def _fn_class():
+    import torch
+
+    class Fn(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, n0, Ttop, problem):
+            (ns, vs1, Ts, lo, hi), ckpt = problem.run(n0, Ttop, keep=True)
+            ctx.problem = problem
+            ctx.ckpt = ckpt
+            ctx.save_for_backward(n0, Ttop)
+            return ns, Ts
+
+        @staticmethod
+        def backward(ctx, g_ns, g_Ts):
+            import torch
+
+            P = ctx.problem
+            n0, Ttop = ctx.saved_tensors
+            zeros = lambda t: torch.zeros_like(t)
+            ns_f = P.base[0:LSP]
+            cot = [g_ns if g_ns is not None else zeros(ns_f), zeros(ns_f),
+                   g_Ts if g_Ts is not None else zeros(ns_f), zeros(P.lo0), zeros(P.hi0)]
+            g_top = torch.zeros_like(Ttop) if Ttop is not None else None
+            starts = sorted(ctx.ckpt)
+            for seg_i in range(len(starts) - 1, -1, -1):
+                j0 = starts[seg_i]
+                j1 = starts[seg_i + 1] if seg_i + 1 < len(starts) else P.nsteps
+                # recompute the states of the segment from its checkpoint
+                P._load(*ctx.ckpt[j0], Ttop)
+                states = [ctx.ckpt[j0]]
+                for j in range(j0, j1 - 1):
+                    P.cuda_step(j)
+                    states.append(P._save())
+                for j in range(j1 - 1, j0 - 1, -1):
+                    cot, gt = P.step_vjp(states[j - j0], Ttop, j, cot)
+                    if gt is not None:
+                        g_top = g_top + gt
+            g = P.grid
+            I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
+            gns = cot[0][(slice(None),) + I]
+            g_n0 = gns[:LSP - 1] + gns[LSP - 1].unsqueeze(0)  # electrons = sum of ions
+            return g_n0, g_top, None
+
+    return Fn
+
+
+class _Lazy:
+    _cls = None
+
+    @classmethod
+    def get(cls):
+        if cls._cls is None:
+            cls._cls = _fn_class()
+        return cls._cls
+
+
+class _FnProxy:
+    @staticmethod
+    def apply(*args):
+        return _Lazy.get().apply(*args)
+
+
+_Fn = _FnProxy
+
+
+def misfit(ns, Ts, target_Te, target_nOp, grid, Te_scale=1000.0, n_scale=1e11):
+    """L2 misfit of the final electron temperature and O+ density (interior)."""
+    I = (slice(2, grid.lx3 + 2), slice(2, grid.lx2 + 2), slice(2, grid.lx1 + 2))
+    dT = (Ts[(LSP - 1,) + I] - target_Te) / Te_scale
+    dn = (ns[(0,) + I] - target_nOp) / n_scale
+    return 0.5 * (dT * dT).mean() + 0.5 * (dn * dn).mean()
+
+
+def torch_reference_loss(problem: DiffProblem, n0, Ttop, target_Te, target_nOp):
+    """The same loss computed by the pure-tensor transcription (autograd end to end)."""
+    P = problem
+    ns = P.initial_state(n0)
+    vs1, Ts, lo, hi = P.base[LSP:2 * LSP], P.base[4 * LSP:], P.lo0, P.hi0
+    for j in range(P.nsteps):
+        ns, vs1, Ts, lo, hi = TS.step(P.tg, ns, vs1, P.vs2, P.vs3, Ts, lo, hi, P.nn, P.Tn, P.J1, P.dts[j],
+                                      P.Teinf, Ttop, P.diffsolvetype)
+    return misfit(ns, Ts, target_Te, target_nOp, P.grid)

@@ -396,6 +396,7 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
     I.df.Tn = w->Tn;
     I.df.dtp = w->dt;
     I.df.Teinf = cfgs[i].Teinf;
+    I.df.Ttop = w->Ttop;
     I.df.solver = cfgs[i].diffsolvetype;
     I.df.M = M;
     I.df.Mslot = diff_bucket_M(M);  // the slot size of the instance's diffusion launch

@@ -92,6 +92,7 @@ struct gem_work {
   PhaseTimer timer;
   int lx1, lx2, lx3;
   double *vs1i, *vs2i, *vs3i, *nn, *Tn, *dt;
+  double* Ttop;             // per-column exospheric temperature (lx2*lx3), or null for Teinf
   unsigned long long* acc;  // 32 slots: CFL maxima / counters
   long long nf1, nf2, nf3;
   // device staging of the host blocks for gem_fluid_adv_host
@@ -440,6 +441,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
   gem_work* w = new gem_work();
   w->vs1i = w->vs2i = w->vs3i = w->nn = w->Tn = w->dt = nullptr;
   w->acc = nullptr;
+  w->Ttop = nullptr;
   w->F = w->A = w->E = nullptr;
   w->nF = w->nA = w->nE = 0;
   w->lx1 = d.lx1;
@@ -477,7 +479,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
 int gem_work_destroy(gem_work* w) {
   if (!w) return GEM_OK;
   for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);
-  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E};
+  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete w;
@@ -516,6 +518,22 @@ double* gem_work_array(gem_work* w, int which) {
 }
 
 double* gem_work_dt(gem_work* w) { return w ? w->dt : nullptr; }
+
+int gem_work_set_top_temperature(gem_work* w, const double* Ttop, int on_device) {
+  if (!w) return set_err(GEM_EINVAL, "null work object");
+  if (!Ttop) {
+    if (w->Ttop) cudaFree(w->Ttop);
+    w->Ttop = nullptr;
+    return GEM_OK;
+  }
+  const size_t n = (size_t)w->lx2 * w->lx3;
+  if (!w->Ttop && cudaMalloc(&w->Ttop, n * sizeof(double)) != cudaSuccess) {
+    w->Ttop = nullptr;
+    return set_err(GEM_ENOMEM, "cudaMalloc of the top-temperature array failed");
+  }
+  GEM_CUDA(cudaMemcpy(w->Ttop, Ttop, n * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+  return GEM_OK;
+}
 
 // ---- conversions ---------------------------------------------------------------------
 #define ELEMWISE(name, kern, Fp, Ap)                                                   \
@@ -616,6 +634,7 @@ int gem_energy_diffusion_dev(const gem_cfg* cfg, const gem_grid* g, double* flui
   a.Tn = w->Tn;
   a.dtp = dt;
   a.Teinf = cfg->Teinf;
+  a.Ttop = w->Ttop;
   a.solver = cfg->diffsolvetype;
   a.fused = 0;
   int rc = launch_diffusion(g, a, S(stream));
@@ -748,6 +767,7 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
   d.Tn = w->Tn;
   d.dtp = dt;
   d.Teinf = cfg->Teinf;
+  d.Ttop = w->Ttop;
   d.solver = cfg->diffsolvetype;
   d.fused = 1;
   w->timer.record(6, st);

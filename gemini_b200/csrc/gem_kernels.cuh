@@ -1160,6 +1160,7 @@ struct DiffArgs {
   const double* Tn;  // (lx1,lx2,lx3)
   const double* dtp;
   double Teinf;
+  const double* Ttop;  // optional per-column (i2 fastest) exospheric temperature, else Teinf
   int solver;  // 1 backward Euler, 2 TRBDF2
   int M;       // rows per lane
   int Mslot;   // rows per lane that each warp's shared-memory slot is sized for (>= M)
@@ -1500,8 +1501,10 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
     {
       const double tn1 = __ldg(P.Tn + ci(d, 1, i2, i3)), tnl = __ldg(P.Tn + ci(d, n, i2, i3));
       if (G.gridflag == 0) { tmin = tn1; tmax = tnl; }
-      else if (G.gridflag == 1) { tmin = P.Teinf; tmax = tnl; }
-      else { tmin = tn1; tmax = P.Teinf; }
+      // the exospheric side: Teinf, or the per-column value when one is set
+      const double tinf = P.Ttop ? __ldg(P.Ttop + (i2 - 1) + (long long)d.lx2 * (i3 - 1)) : P.Teinf;
+      if (G.gridflag == 1) { tmin = tinf; tmax = tnl; }
+      else if (G.gridflag == 2) { tmin = tn1; tmax = tinf; }
     }
     auto Tat = [&](int k) -> double {
       if (k < 0) return Tprev;

@@ -78,6 +78,12 @@ int gem_work_interface_vels(gem_work* w, int which, double* host, int dir);
 double* gem_work_array(gem_work* w, int which);
 /* device pointer of the 1-element dt slot inside the work object */
 double* gem_work_dt(gem_work* w);
+/* Per-column exospheric (top Dirichlet) temperature, lx2*lx3 values with i2 fastest,
+ * replacing cfg->Teinf on the gridflag 1 / 2 boundary (diffusion.f90:67-79) for the steps
+ * that follow; NULL restores the scalar Teinf.  on_device: Ttop is a device pointer.  No
+ * counterpart in the reference (its Teinf is one number); it is the boundary control of
+ * the differentiable path.  A batch reads it when created. */
+int gem_work_set_top_temperature(gem_work* w, const double* Ttop, int on_device);
 
 /* ---- individual reference routines, device-resident ------------------------------ */
 /* multifluid.f90:179-233 conversions over the full ghosted arrays, all species */
