@@ -37,9 +37,10 @@ class DiffProblem:
     """One differentiable problem: grid, fixed inputs, dt schedule, scratch device state."""
 
     def __init__(self, grid, st, nsteps: int, checkpoint_every: int = 5, tcfl: float = 0.5,
-                 diffsolvetype: int = 2, device="cuda"):
+                 diffsolvetype: int = 2, device="cuda", cuda_diffusion_adjoint: bool = True):
         import torch
 
+        self.cuda_diffusion_adjoint = bool(cuda_diffusion_adjoint)
         self.grid = grid
         self.nsteps = int(nsteps)
         self.k = max(1, int(checkpoint_every))
@@ -126,6 +127,65 @@ class DiffProblem:
         out = self._save()
         return out, ckpt
 
+    # -- the energy diffusion with its hand-written CUDA adjoint ----------------------
+    def diffusion_forward(self, n, T, Ttop, j):
+        """gem_energy_diffusion_dev on (n, T): the diffusion output (max(T,100) applied)."""
+        import torch
+
+        fv = torch.zeros(self.shape, dtype=torch.float64, device=n.device)
+        fv[0:LSP] = n
+        fv[4 * LSP:] = T
+        self._set_top(Ttop)
+        dt = torch.full((1,), self.dts[j], dtype=torch.float64, device=n.device)
+        c = self.cfg.c()
+        _lib.check(_lib.lib().gem_energy_diffusion_dev(ctypes.byref(c), self.dg.handle, F._ptr(fv),
+                                                       F._ptr(self.ds.electrovars), self.ds.work, F._ptr(dt),
+                                                       F._stream()))
+        return fv[4 * LSP:].clone()
+
+    def diffusion_vjp(self, n, T, Ttop, j, Ybar):
+        import torch
+
+        g = self.grid
+        self._set_top(Ttop)
+        dt = torch.full((1,), self.dts[j], dtype=torch.float64, device=n.device)
+        n = n.contiguous()
+        T = T.contiguous()
+        Yb = Ybar.contiguous()
+        Tb = torch.zeros_like(T)
+        nb = torch.zeros_like(n)
+        tb = torch.zeros((LSP, g.lx3, g.lx2), dtype=torch.float64, device=n.device)
+        need = int(_lib.lib().gem_diffusion_vjp_scratch_doubles(self.dg.handle))
+        if getattr(self, "_scratch", None) is None or self._scratch.numel() < need:
+            self._scratch = torch.empty(need, dtype=torch.float64, device=n.device)
+        c = self.cfg.c()
+        _lib.check(_lib.lib().gem_diffusion_vjp_dev(ctypes.byref(c), self.dg.handle, F._ptr(T), F._ptr(n),
+                                                    F._ptr(self.ds.electrovars), self.ds.work, F._ptr(dt),
+                                                    F._ptr(Yb), F._ptr(Tb), F._ptr(nb), F._ptr(tb),
+                                                    F._ptr(self._scratch), F._stream()))
+        # ghost cells: out = max(T, 100) except the x1 boundary layers, which hold the
+        # Dirichlet values max(tmin, 100) / max(tmax, 100)
+        ghost = torch.ones_like(T[0], dtype=torch.bool)
+        ghost[2:g.lx3 + 2, 2:g.lx2 + 2, 2:g.lx1 + 2] = False
+        bc = torch.zeros_like(ghost)
+        bc[2:g.lx3 + 2, 2:g.lx2 + 2, 1] = True
+        bc[2:g.lx3 + 2, 2:g.lx2 + 2, g.lx1 + 2] = True
+        pas = ghost & ~bc
+        Tb = Tb + torch.where(pas & (T >= 100.0), Yb, torch.zeros_like(Yb))
+        # the boundary layer on the exospheric side carries max(Ttop, 100)
+        side = {1: 1, 2: g.lx1 + 2}.get(g.gridflag)
+        if side is not None and Ttop is not None:
+            bcv = Ttop.unsqueeze(0).expand(LSP, g.lx3, g.lx2)
+            tb = tb + torch.where(bcv >= 100.0, Yb[:, 2:g.lx3 + 2, 2:g.lx2 + 2, side], torch.zeros_like(bcv))
+        return nb, Tb, tb.sum(0)
+
+    def _set_top(self, Ttop):
+        if Ttop is None:
+            _lib.check(_lib.lib().gem_work_set_top_temperature(self.ds.work, None, 0))
+        else:
+            t = Ttop.detach().contiguous()
+            _lib.check(_lib.lib().gem_work_set_top_temperature(self.ds.work, ctypes.c_void_p(t.data_ptr()), 1))
+
     def step_vjp(self, state, Ttop, j, cot, use_cuda_diffusion_adjoint=False):
         """Pull the cotangent of the state after step j back to the state before it (and
         to Ttop).  state / cot: (ns, vs1, Ts, lo, hi)."""
@@ -133,15 +193,47 @@ class DiffProblem:
 
         inp = [t.detach().requires_grad_(True) for t in state]
         tt = None if Ttop is None else Ttop.detach().requires_grad_(True)
+        diff = None
+        if use_cuda_diffusion_adjoint:
+            P = self
+
+            def diff(n, T, Ttop_):
+                return _diffusion_fn().apply(n, T, Ttop_, P, j)
         with torch.enable_grad():
             out = TS.step(self.tg, inp[0], inp[1], self.vs2, self.vs3, inp[2], inp[3], inp[4], self.nn,
-                          self.Tn, self.J1, self.dts[j], self.Teinf, tt, self.diffsolvetype)
+                          self.Tn, self.J1, self.dts[j], self.Teinf, tt, self.diffsolvetype, diffusion=diff)
             pairs = [(o, c) for o, c in zip(out, cot) if c is not None]
             wrt = inp + ([tt] if tt is not None else [])
             grads = torch.autograd.grad([o for o, _ in pairs], wrt, [c for _, c in pairs], allow_unused=True)
         g_state = [torch.zeros_like(t) if g is None else g for g, t in zip(grads[:5], inp)]
         g_top = None if tt is None else (torch.zeros_like(tt) if grads[5] is None else grads[5])
         return g_state, g_top
+
+
+_DIFF_FN = None
+
+
+def _diffusion_fn():
+    """torch.autograd.Function: CUDA energy diffusion forward, CUDA adjoint backward."""
+    global _DIFF_FN
+    if _DIFF_FN is None:
+        import torch
+
+        class DiffusionFn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, n, T, Ttop, problem, j):
+                ctx.problem, ctx.j = problem, j
+                ctx.save_for_backward(n, T, Ttop)
+                return problem.diffusion_forward(n, T, Ttop, j)
+
+            @staticmethod
+            def backward(ctx, Ybar):
+                n, T, Ttop = ctx.saved_tensors
+                nb, Tb, tb = ctx.problem.diffusion_vjp(n, T, Ttop, ctx.j, Ybar)
+                return nb, Tb, (tb if Ttop is not None else None), None, None
+
+        _DIFF_FN = DiffusionFn
+    return _DIFF_FN
 
 
 class FluidAdvance:
@@ -186,7 +278,7 @@ def _fn_class():
                     P.cuda_step(j)
                     states.append(P._save())
                 for j in range(j1 - 1, j0 - 1, -1):
-                    cot, gt = P.step_vjp(states[j - j0], Ttop, j, cot)
+                    cot, gt = P.step_vjp(states[j - j0], Ttop, j, cot, P.cuda_diffusion_adjoint)
                     if gt is not None:
                         g_top = g_top + gt
             g = P.grid

@@ -663,6 +663,47 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
   return GEM_OK;
 }
 
+// Vector-Jacobian product of the energy diffusion (differentiable path).
+long long gem_diffusion_vjp_scratch_doubles(const gem_grid* g) {
+  if (!g) return -1;
+  const Dims& d = g->dev.d;
+  return (long long)DADJ_N * d.lx1 * d.lx2 * d.lx3 * LSP;
+}
+
+int gem_diffusion_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const double* Ts, const double* ns,
+                          const double* electrovars, const gem_work* w, const double* dt, const double* Ybar,
+                          double* Tbar, double* nbar, double* Ttop_bar, double* scratch, void* stream) {
+  if (!cfg || check_grid(g) || !Ts || !ns || !electrovars || !w || !dt || !Ybar || !Tbar || !nbar || !scratch)
+    return set_err(GEM_EINVAL, "null argument");
+  if (cfg->diffsolvetype != 1 && cfg->diffsolvetype != 2)
+    return set_err(GEM_EINVAL, "Unsupported diffusion solver type/mode: %d. Should be either 1 or 2.", cfg->diffsolvetype);
+  if (g->dev.d.lx1 < 4) return set_err(GEM_EINVAL, "lx1=%d: the diffusion needs lx1 >= 4", g->dev.d.lx1);
+  DiffAdjArgs a;
+  a.G = g->dev;
+  a.T = Ts;
+  a.ns = ns;
+  a.J1 = electrovars + 3 * g->dev.d.ng;
+  a.nn = w->nn;
+  a.Tn = w->Tn;
+  a.Ttop = w->Ttop;
+  a.Teinf = cfg->Teinf;
+  a.dtp = dt;
+  a.solver = cfg->diffsolvetype;
+  a.Ybar = Ybar;
+  a.Tbar = Tbar;
+  a.nbar = nbar;
+  a.Ttop_bar = Ttop_bar;
+  a.scratch = scratch;
+  const long long ncs = (long long)g->dev.d.lx2 * g->dev.d.lx3 * LSP;
+  cudaStream_t st = S(stream);
+  if (g->dev.unit)
+    k_diffusion_vjp<true><<<grid_for(ncs, 128, 16), 128, 0, st>>>(a);
+  else
+    k_diffusion_vjp<false><<<grid_for(ncs, 128, 16), 128, 0, st>>>(a);
+  GEM_LAUNCHED("k_diffusion_vjp");
+  return GEM_OK;
+}
+
 // dt_calc variant that allocates nothing: its scratch (per-x3-plane partial maxima) is
 // the file-scope device array below, whose address is resolved once per device.
 int gem_dt_calc_noalloc_dev(const gem_grid* g, double tcfl, const double* fluidvars, double* dt_out,

@@ -1629,6 +1629,314 @@ __global__ void k_diffusion_ghost_floor(GridDev G, Blocks B) {
 }
 
 // ======================================================================================
+// 7b. Adjoint (vector-Jacobian product) of the energy diffusion, for the differentiable
+//     path.  One thread per (x1 column, species) -- species slowest, so neighbouring threads
+//     hold neighbouring columns -- with per-row work arrays in global scratch laid out
+//     [array][row][thread] (coalesced).  The thread recomputes the forward coefficients and
+//     both stage solutions (Thomas), then runs the transposed solves and chains the
+//     cotangents of the band entries and right-hand sides through q+-, Dh, C, B and the
+//     conductivity lambda(T, n) back to T, n and the exospheric boundary temperature.
+//     Cotangent inputs/outputs are ghosted 7-species blocks; only interior rows are
+//     written (the caller zero-initialises Tbar and nbar).
+// ======================================================================================
+struct DiffAdjArgs {
+  GridDev G;
+  const double* T;     // diffusion input temperature (ghosted, 7 species)
+  const double* ns;    // densities (ghosted, 7 species)
+  const double* J1;    // electrovars(:,:,:,4)
+  const double* nn;    // (lx1,lx2,lx3,3)
+  const double* Tn;    // (lx1,lx2,lx3)
+  const double* Ttop;  // optional per-column exospheric temperature
+  double Teinf;
+  const double* dtp;
+  int solver;
+  const double* Ybar;  // cotangent of the diffusion output (after max(T,100))
+  double* Tbar;
+  double* nbar;
+  double* Ttop_bar;    // optional: (lx2*lx3) per species, species slowest
+  double* scratch;     // DADJ_N * lx1 * (lx2*lx3*7) doubles
+};
+constexpr int DJ_QM = 0, DJ_QP = 1, DJ_BQ = 2, DJ_X = 3, DJ_Y = 4, DJ_CP = 5, DJ_DP = 6, DJ_L2 = 7, DJ_G = 8,
+              DJ_QMB = 9, DJ_QPB = 10, DJ_BQB = 11, DJ_TB = 12;
+constexpr int DADJ_N = 13;
+
+template <bool UNIT>
+__global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
+  const GridDev& G = P.G;
+  const Dims d = G.d;
+  const int n = d.lx1;
+  const long long ncol = (long long)d.lx2 * d.lx3;
+  const long long ncs = ncol * LSP;
+  const double dt = *P.dtp;
+  const Line1D& L1 = G.L[0];
+  for (long long cs = blockIdx.x * (long long)blockDim.x + threadIdx.x; cs < ncs;
+       cs += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(cs / ncol);
+    const long long col = cs - (long long)s * ncol;
+    const int i2 = (int)(col % d.lx2) + 1, i3 = (int)(col / d.lx2) + 1;
+    const long long m0 = gi(d, 0, i2, i3);
+    const long long mm0 = cmi(G, 0, i2, i3);
+    const long long q0 = ci(d, 1, i2, i3) - 1;
+    const long long nc = nci(d);
+    const double* Tc = P.T + (long long)s * d.ng + m0;
+    const double* nsc = P.ns + (long long)s * d.ng + m0;
+    auto S = [&](int arr, int i) -> double& { return P.scratch[((long long)arr * n + (i - 1)) * ncs + cs]; };
+    const double c0 = (c_gammas[s] - 1.0) / KB;
+    // conductivity and its partial derivatives at row i
+    auto lam_d = [&](int i, double& lam, double& dl_dT, double& dl_dn) {
+      const double T = Tc[i];
+      const double T25 = pow25(T);
+      if (s < LSP - 1) {
+        lam = c_tcoef[s] * T25;
+        dl_dT = 2.5 * lam / T;
+        dl_dn = 0.0;
+      } else {
+        const long long q = q0 + i;
+        const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
+        const double sq = sqrt(T);
+        const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
+                         n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
+        const double Xp = n1 * 1.1e-16 * 5.7e-4 + n2 * 2.82e-17 * (0.5 / sq * (1 - 1.21e-4 * T) - 1.21e-4 * sq) +
+                          n3 * 2.2e-16 * 3.6e-2 * 0.5 / sq;
+        const double ne = nsc[i];
+        const double den = 1 + 3.22e4 * (T * T) / ne * X;
+        lam = ELCHRG * 100 * 7.7e5 * T25 / den;
+        const double dden_dT = 3.22e4 * (2 * T * X + T * T * Xp) / ne;
+        dl_dT = lam * (2.5 / T - dden_dT / den);
+        dl_dn = lam * (3.22e4 * T * T * X / (ne * ne)) / den;
+      }
+    };
+    auto coefC = [&](int i, double& C, double& dC_dn) {
+      const double nv = nsc[i];
+      const double ha1 = UNIT ? 1.0 : __ldg(G.ha1_0 + mm0 + i);
+      C = c0 / fmax_f(nv, MINDENSDIV) / ha1;
+      dC_dn = (nv > MINDENSDIV) ? -C / nv : 0.0;
+    };
+    auto h1_ = [&](int i) { return UNIT ? 1.0 : __ldg(G.h1 + mm0 + i); };
+    auto h23 = [&](int i) { return UNIT ? 1.0 : __ldg(G.h2 + mm0 + i) * __ldg(G.h3 + mm0 + i); };
+    auto beta_ = [&](int i) { return (s < LSP - 1) ? 0.0 : 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i]; };
+    auto Dv = [&](int i) {
+      double lam, a, b;
+      lam_d(i, lam, a, b);
+      return lam * h23(i) / h1_(i);
+    };
+    auto Cv = [&](int i) {
+      double C, dc;
+      coefC(i, C, dc);
+      return C;
+    };
+    // ---- forward: q-, q+, bq for rows 2..n-1
+    for (int i = 2; i <= n - 1; ++i) {
+      const double Dm = Dv(i - 1), Dc = Dv(i), Dp = Dv(i + 1);
+      const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);
+      const double C = Cv(i);
+      const double B = C * beta_(i) / h1_(i);
+      const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
+      S(DJ_QM, i) = C * Dhm / dxi / dxm;
+      S(DJ_QP, i) = C * Dhp / dxi / dxp;
+      S(DJ_BQ, i) = B / (dxp + dxm);
+    }
+    double tmin, tmax;
+    {
+      const double tn1 = __ldg(P.Tn + ci(d, 1, i2, i3)), tnl = __ldg(P.Tn + ci(d, n, i2, i3));
+      const double tinf = P.Ttop ? __ldg(P.Ttop + col) : P.Teinf;
+      if (G.gridflag == 0) { tmin = tn1; tmax = tnl; }
+      else if (G.gridflag == 1) { tmin = tinf; tmax = tnl; }
+      else { tmin = tn1; tmax = tinf; }
+    }
+    const bool trbdf = P.solver == 2;
+    const double dA = trbdf ? 1 / (dt / 2) : 1 / dt;  // first-stage diagonal term
+    const double hA = trbdf ? 0.5 : 1.0;              // first-stage scale of the q's
+    // first-stage rows (TR half step, or the backward-Euler step)
+    auto rowA = [&](int i, double& a, double& b, double& c) {
+      if (i == 1 || i == n) { a = 0; b = 1; c = 0; return; }
+      const double qm = S(DJ_QM, i), qp = S(DJ_QP, i), bq = S(DJ_BQ, i);
+      if (trbdf) {
+        a = -(qm / 2) + bq / 2;
+        b = dA + qp / 2 + qm / 2;
+        c = -(qp / 2) - bq / 2;
+      } else {
+        a = -qm + bq;
+        b = dA + qp + qm;
+        c = -qp - bq;
+      }
+    };
+    auto rowB = [&](int i, double& a, double& b, double& c) {  // BDF2 rows
+      if (i == 1 || i == n) { a = 0; b = 1; c = 0; return; }
+      const double qm = S(DJ_QM, i), qp = S(DJ_QP, i), bq = S(DJ_BQ, i);
+      a = -qm + bq;
+      b = 1 / (dt / 3) + qp + qm;
+      c = -qp - bq;
+    };
+    // Thomas solve of rows rowf with right-hand side in array R, solution into array OUT
+    auto thomas = [&](auto rowf, int R, int OUT) {
+      double cp = 0.0, dp = 0.0;
+      for (int i = 1; i <= n; ++i) {
+        double a, b, c;
+        rowf(i, a, b, c);
+        const double den = b - a * cp;
+        cp = c / den;
+        dp = (S(R, i) - a * dp) / den;
+        S(DJ_CP, i) = cp;
+        S(DJ_DP, i) = dp;
+      }
+      double x = 0.0;
+      for (int i = n; i >= 1; --i) {
+        x = S(DJ_DP, i) - S(DJ_CP, i) * x;
+        S(OUT, i) = x;
+      }
+    };
+    // transposed solve: A^T has sub-diagonal c(i-1), diagonal b(i), super-diagonal a(i+1)
+    auto thomasT = [&](auto rowf, int R, int OUT) {
+      double cp = 0.0, dp = 0.0;
+      double a_i, b_i, c_i, a_n, b_n, c_n, c_prev = 0.0;
+      rowf(1, a_i, b_i, c_i);
+      for (int i = 1; i <= n; ++i) {
+        double sup = 0.0;
+        if (i < n) {
+          rowf(i + 1, a_n, b_n, c_n);
+          sup = a_n;
+        }
+        const double sub = (i > 1) ? c_prev : 0.0;
+        const double den = b_i - sub * cp;
+        cp = sup / den;
+        dp = (S(R, i) - sub * dp) / den;
+        S(DJ_CP, i) = cp;
+        S(DJ_DP, i) = dp;
+        c_prev = c_i;
+        if (i < n) { a_i = a_n; b_i = b_n; c_i = c_n; }
+      }
+      double x = 0.0;
+      for (int i = n; i >= 1; --i) {
+        x = S(DJ_DP, i) - S(DJ_CP, i) * x;
+        S(OUT, i) = x;
+      }
+    };
+    // first-stage right-hand side into DJ_G
+    for (int i = 1; i <= n; ++i) {
+      double r;
+      if (i == 1) r = tmin;
+      else if (i == n) r = tmax;
+      else if (trbdf) {
+        double a, b, c;
+        rowA(i, a, b, c);
+        const double qm = S(DJ_QM, i), qp = S(DJ_QP, i);
+        const double Pd = qp / 2 + qm / 2;
+        r = Tc[i] / (dt / 2) - a * Tc[i - 1] - Pd * Tc[i] - c * Tc[i + 1];
+      } else {
+        r = Tc[i] / dt;
+      }
+      S(DJ_G, i) = r;
+    }
+    thomas(rowA, DJ_G, DJ_X);
+    if (trbdf) {
+      for (int i = 1; i <= n; ++i) {
+        double r;
+        if (i == 1) r = tmin;
+        else if (i == n) r = tmax;
+        else r = -(1 / 3.0 * Tc[i] / (dt / 3)) + 4 / 3.0 * S(DJ_X, i) / (dt / 3);
+        S(DJ_G, i) = r;
+      }
+      thomas(rowB, DJ_G, DJ_Y);
+    }
+    const int YOUT = trbdf ? DJ_Y : DJ_X;
+    // ---- adjoint
+    const double* Yb = P.Ybar + (long long)s * d.ng + m0;
+    for (int i = 1; i <= n; ++i) {
+      S(DJ_G, i) = (S(YOUT, i) >= 100.0) ? Yb[i] : 0.0;  // max(T,100)
+      S(DJ_QMB, i) = 0.0;
+      S(DJ_QPB, i) = 0.0;
+      S(DJ_BQB, i) = 0.0;
+      S(DJ_TB, i) = 0.0;
+    }
+    double tminb = 0.0, tmaxb = 0.0;
+    int LA = DJ_L2;  // adjoint of the first stage, in DJ_L2 after the loop below
+    if (trbdf) {
+      thomasT(rowB, DJ_G, DJ_L2);  // lambda2 = A2^-T ybar
+      tminb += S(DJ_L2, 1);
+      tmaxb += S(DJ_L2, n);
+      for (int i = 2; i <= n - 1; ++i) {
+        const double l2 = S(DJ_L2, i);
+        const double ab = -l2 * S(DJ_Y, i - 1), bb = -l2 * S(DJ_Y, i), cb = -l2 * S(DJ_Y, i + 1);
+        S(DJ_QMB, i) += -ab + bb;
+        S(DJ_QPB, i) += bb - cb;
+        S(DJ_BQB, i) += ab - cb;
+        S(DJ_TB, i) += l2 * (-(1 / 3.0) / (dt / 3));
+        S(DJ_G, i) = l2 * ((4 / 3.0) / (dt / 3));  // xbar
+      }
+      S(DJ_G, 1) = 0.0;
+      S(DJ_G, n) = 0.0;
+    }
+    thomasT(rowA, DJ_G, LA);  // lambda1 = A1^-T xbar (or A^-T ybar for backward Euler)
+    tminb += S(LA, 1);
+    tmaxb += S(LA, n);
+    for (int i = 2; i <= n - 1; ++i) {
+      const double l1 = S(LA, i);
+      double a, b, c;
+      rowA(i, a, b, c);
+      const double xm = S(DJ_X, i - 1), xc = S(DJ_X, i), xp = S(DJ_X, i + 1);
+      if (trbdf) {
+        const double qm = S(DJ_QM, i), qp = S(DJ_QP, i);
+        const double Pd = qp / 2 + qm / 2;
+        const double ab = -l1 * (xm + Tc[i - 1]), cb = -l1 * (xp + Tc[i + 1]), bb = -l1 * xc, pb = -l1 * Tc[i];
+        S(DJ_QMB, i) += -ab / 2 + bb / 2 + pb / 2;
+        S(DJ_QPB, i) += -cb / 2 + bb / 2 + pb / 2;
+        S(DJ_BQB, i) += ab / 2 - cb / 2;
+        S(DJ_TB, i) += l1 * (dA - Pd);
+        S(DJ_TB, i - 1) += -l1 * a;
+        S(DJ_TB, i + 1) += -l1 * c;
+      } else {
+        const double ab = -l1 * xm, cb = -l1 * xp, bb = -l1 * xc;
+        S(DJ_QMB, i) += -ab + bb;
+        S(DJ_QPB, i) += bb - cb;
+        S(DJ_BQB, i) += ab - cb;
+        S(DJ_TB, i) += l1 * dA;
+      }
+    }
+    (void)hA;
+    // ---- chain through q-, q+, bq -> C, Dh -> D -> lambda(T, n)
+    double* Tbo = P.Tbar + (long long)s * d.ng + m0;
+    double* nbo = P.nbar + (long long)s * d.ng + m0;
+    for (int i = 1; i <= n; ++i) {
+      double C, dC_dn;
+      coefC(i, C, dC_dn);
+      double Cb = 0.0, Dhb_i = 0.0, Dhb_ip1 = 0.0;
+      if (i >= 2 && i <= n - 1) {
+        const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
+        const double Dm = Dv(i - 1), Dc = Dv(i), Dp = Dv(i + 1);
+        const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);
+        const double qmb = S(DJ_QMB, i), qpb = S(DJ_QPB, i);
+        Cb += qmb * Dhm / (dxi * dxm) + qpb * Dhp / (dxi * dxp);
+        Dhb_i += qmb * C / (dxi * dxm);
+        Dhb_ip1 += qpb * C / (dxi * dxp);
+        const double Bb = S(DJ_BQB, i) / (dxp + dxm);
+        Cb += Bb * beta_(i) / h1_(i);
+      }
+      // Dh(i) also collects q+ of row i-1; Dh(i+1) the q- of row i+1
+      if (i - 1 >= 2 && i - 1 <= n - 1) {
+        const double dxi = __ldg(L1.dxi + i - 2), dxp = __ldg(L1.dx + i);
+        Dhb_i += S(DJ_QPB, i - 1) * Cv(i - 1) / (dxi * dxp);
+      }
+      if (i + 1 >= 2 && i + 1 <= n - 1) {
+        const double dxi = __ldg(L1.dxi + i), dxm = __ldg(L1.dx + i + 1);
+        Dhb_ip1 += S(DJ_QMB, i + 1) * Cv(i + 1) / (dxi * dxm);
+      }
+      // Dh(j) = 0.5*(D(j-1) + D(j)) for j = 2..n: D(i) feeds Dh(i) (i >= 2) and Dh(i+1) (i < n)
+      const double Db = 0.5 * ((i >= 2 ? Dhb_i : 0.0) + (i < n ? Dhb_ip1 : 0.0));
+      double lam, dl_dT, dl_dn;
+      lam_d(i, lam, dl_dT, dl_dn);
+      const double lamb = Db * h23(i) / h1_(i);
+      Tbo[i] = S(DJ_TB, i) + lamb * dl_dT;
+      nbo[i] = Cb * dC_dn + lamb * dl_dn;
+    }
+    if (P.Ttop_bar) {
+      const double tb = (G.gridflag == 1) ? tminb : (G.gridflag == 2) ? tmaxb : 0.0;
+      P.Ttop_bar[cs] = tb;
+    }
+  }
+}
+
+// ======================================================================================
 // 8. CFL time step (temporal_mpi.f90:86-167), max CFL (temporal.f90:12-49), finiteness
 // ======================================================================================
 // Rates are >= 0, so their IEEE bit patterns order like unsigned integers and the block

@@ -150,12 +150,13 @@ def _wrap3(x):
 
 # ---- the step ------------------------------------------------------------------------
 def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf, Ttop=None,
-         diffsolvetype=2):
+         diffsolvetype=2, diffusion=None):
     """One fused step.  ns, vs1, Ts: (7, X3, X2, X1); vs2, vs3 likewise (inputs only);
     v1i_lo / v1i_hi: the x1 boundary faces of vs1i from the previous step, (7, lx3, lx2);
     nn: (3, lx3, lx2, lx1); Tn: (lx3, lx2, lx1); J1: (X3, X2, X1); Ttop: optional per-column
-    top Dirichlet temperature (lx3, lx2) replacing Teinf.  Returns
-    (ns, vs1, Ts, v1i_lo, v1i_hi) after the step."""
+    top Dirichlet temperature (lx3, lx2) replacing Teinf; diffusion: optional replacement of
+    energy_diffusion, called as diffusion(n, T, Ttop) (e.g. a function with a hand-written
+    adjoint).  Returns (ns, vs1, Ts, v1i_lo, v1i_hi) after the step."""
     import torch
 
     lx1, lx2, lx3 = G.lx1, G.lx2, G.lx3
@@ -305,7 +306,10 @@ def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf,
     T = torch.where(ghost, torch.full_like(T, 100.0), T)
 
     # ---- energy diffusion (multifluid.f90:309-342)
-    T = energy_diffusion(G, n, T, J1, nn, Tn, dt, Teinf, Ttop, diffsolvetype)
+    if diffusion is None:
+        T = energy_diffusion(G, n, T, J1, nn, Tn, dt, Teinf, Ttop, diffsolvetype)
+    else:
+        T = diffusion(n, T, Ttop)
     T = torch.where(ghost, torch.full_like(T, 100.0), torch.clamp(T, min=100.0))
     return n, v1, T, v1i[..., 0], v1i[..., -1]
 

@@ -121,6 +121,20 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
 int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, const double* dt,
                    double* maxcfl_out, void* stream);
 
+/* ---- differentiable path (no counterpart in the reference) ------------------------
+ * Vector-Jacobian product of gem_energy_diffusion_dev: given Ybar, the cotangent of the
+ * diffusion's output temperature (ghosted 7-species block; interior rows used, including
+ * the max(T,100) floor), accumulate the cotangents of its inputs into Tbar (temperature),
+ * nbar (densities; both ghosted 7-species blocks, interior rows written, caller zeroes
+ * them) and, if not NULL, Ttop_bar (lx2*lx3 per species, species slowest: the exospheric
+ * boundary value of each column and species).  Ts / ns are the inputs of the forward call;
+ * the kernel recomputes the forward coefficients and both TRBDF2 stages (Thomas), then
+ * solves the transposed systems.  scratch: gem_diffusion_vjp_scratch_doubles(g) doubles. */
+long long gem_diffusion_vjp_scratch_doubles(const gem_grid* g);
+int gem_diffusion_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const double* Ts, const double* ns,
+                          const double* electrovars, const gem_work* w, const double* dt, const double* Ybar,
+                          double* Tbar, double* nbar, double* Ttop_bar, double* scratch, void* stream);
+
 /* No counterpart in the reference.  dt_calc (the same result as gem_dt_calc_dev) for callers
  * that cannot allocate device memory or hold a gem_work (for example code that runs inside
  * a pool-managed or already-captured context): it calls no allocator.  Its scratch is a
