@@ -460,6 +460,65 @@ def run_batched(args, world, rank):
     return out
 
 
+ADJOINT = dict(lx1=128, lx2=64, lx3=64, steps=20, checkpoint_every=5, seed=11)
+
+
+def run_adjoint(args):
+    """Adjoint workload: Cartesian 128x64x64 x 7 species, 20 steps, L2 misfit of the final Te
+    and n_O+ against a seeded target; gradient w.r.t. the initial ion densities and the
+    per-column top temperature.  Reports forward time, forward+backward time and the ratio
+    (device time, CUDA events)."""
+    import torch
+
+    from gemini_b200 import adjoint as AD
+    from gemini_b200 import grid as G
+    from gemini_b200 import state as S
+
+    a = ADJOINT
+    g = G.cartesian_grid(a["lx1"], a["lx2"], a["lx3"])
+    st = S.init_state(g, seed=a["seed"], perturb=0.1)
+    P = AD.DiffProblem(g, st, a["steps"], checkpoint_every=a["checkpoint_every"])
+    I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
+    n0 = P.base[(slice(0, 6),) + I].clone()
+    rng = np.random.default_rng(a["seed"])
+    Ttop = torch.from_numpy(st.Teinf * (1 + 0.05 * rng.uniform(-1, 1, (g.lx3, g.lx2)))).cuda()
+    tT = torch.from_numpy(rng.uniform(1500, 3000, (g.lx3, g.lx2, g.lx1))).cuda()
+    tn = torch.from_numpy(rng.uniform(0.5e10, 5e10, (g.lx3, g.lx2, g.lx1))).cuda()
+    s = torch.cuda.current_stream()
+
+    def fwd():
+        (ns, _, Ts, _, _), _ = P.run(n0, Ttop)
+        return AD.misfit(ns, Ts, tT, tn, g)
+
+    def fwd_bwd():
+        x = n0.clone().requires_grad_(True)
+        t = Ttop.clone().requires_grad_(True)
+        ns, Ts = AD.FluidAdvance.apply(x, t, P)
+        L = AD.misfit(ns, Ts, tT, tn, g)
+        L.backward()
+        return x.grad, t.grad
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_f = timed(fwd, 3)
+    ms_fb = timed(fwd_bwd, 1)
+    return {"workload": f"Cartesian {a['lx1']}x{a['lx2']}x{a['lx3']} x 7 species, {a['steps']} steps, "
+                        f"checkpoint every {a['checkpoint_every']}; loss = L2 misfit of final Te and n_O+",
+            "forward_ms": ms_f, "forward_backward_ms": ms_fb, "adjoint_over_forward": (ms_fb - ms_f) / ms_f,
+            "gradient_wrt": "initial ion densities (6 x cells) and per-column top temperature",
+            "backward": "step VJP: CUDA diffusion adjoint + autograd through the tensor transcription "
+                        "of the advection, boundaries and conversions; CUDA recompute per segment"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -471,6 +530,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched instances")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instance measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--lx", type=int, nargs=3, default=None, metavar=("LX1", "LX2", "LX3"),
                     help="override the grid size (profiling runs on a smaller case)")
     args = ap.parse_args()
@@ -489,6 +549,10 @@ def main():
         import torch
         torch.cuda.empty_cache()
         line["batched"] = run_batched(args, world, rank)
+    if not args.no_adjoint and not args.lx and rank == 0:
+        import torch
+        torch.cuda.empty_cache()
+        line["adjoint"] = run_adjoint(args)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

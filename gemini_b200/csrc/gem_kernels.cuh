@@ -1097,7 +1097,7 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
 }
 
 template <bool UNIT, bool FUSED>
-__global__ void __launch_bounds__(224) k_sweep_x1(SweepArgs P) {
+__global__ void __launch_bounds__(224, 3) k_sweep_x1(SweepArgs P) {
   b_sweep_x1<UNIT, FUSED>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
 }
 
