@@ -515,8 +515,9 @@ def run_adjoint(args):
                         f"checkpoint every {a['checkpoint_every']}; loss = L2 misfit of final Te and n_O+",
             "forward_ms": ms_f, "forward_backward_ms": ms_fb, "adjoint_over_forward": (ms_fb - ms_f) / ms_f,
             "gradient_wrt": "initial ion densities (6 x cells) and per-column top temperature",
-            "backward": "step VJP: CUDA diffusion adjoint + autograd through the tensor transcription "
-                        "of the advection, boundaries and conversions; CUDA recompute per segment"}
+            "backward": "per step: hand-written CUDA adjoints of the 9 field sweeps and of the TRBDF2 "
+                        "diffusion; autograd through the tensor transcription for the boundaries, "
+                        "interface velocities and conversions; CUDA recompute per checkpoint segment"}
 
 
 def main():

@@ -37,10 +37,13 @@ class DiffProblem:
     """One differentiable problem: grid, fixed inputs, dt schedule, scratch device state."""
 
     def __init__(self, grid, st, nsteps: int, checkpoint_every: int = 5, tcfl: float = 0.5,
-                 diffsolvetype: int = 2, device="cuda", cuda_diffusion_adjoint: bool = True):
+                 diffsolvetype: int = 2, device="cuda", cuda_diffusion_adjoint: bool = True,
+                 cuda_sweep_adjoint: bool = True):
         import torch
 
         self.cuda_diffusion_adjoint = bool(cuda_diffusion_adjoint)
+        self.cuda_sweep_adjoint = bool(cuda_sweep_adjoint)
+        self._dtt = {}
         self.grid = grid
         self.nsteps = int(nsteps)
         self.k = max(1, int(checkpoint_every))
@@ -89,6 +92,16 @@ class DiffProblem:
         fv = self.ds.fluidvars.view(self.shape)
         return (fv[0:LSP].clone(), fv[LSP:2 * LSP].clone(), fv[4 * LSP:].clone(),
                 self.v1i[..., 0].clone(), self.v1i[..., -1].clone())
+
+    def dt_tensor(self, j: int):
+        """The step's dt as a cached 1-element device tensor."""
+        import torch
+
+        t = self._dtt.get(j)
+        if t is None:
+            t = torch.full((1,), self.dts[j], dtype=torch.float64, device=self.base.device)
+            self._dtt[j] = t
+        return t
 
     def cuda_step(self, j: int) -> None:
         import torch
@@ -194,14 +207,22 @@ class DiffProblem:
         inp = [t.detach().requires_grad_(True) for t in state]
         tt = None if Ttop is None else Ttop.detach().requires_grad_(True)
         diff = None
+        sweep = None
         if use_cuda_diffusion_adjoint:
             P = self
 
             def diff(n, T, Ttop_):
                 return _diffusion_fn().apply(n, T, Ttop_, P, j)
+
+        if self.cuda_sweep_adjoint:
+            P = self
+
+            def sweep(f, v, dim, frank, nsp):
+                return _sweep_fn().apply(f, v, P, dim, frank, nsp, j)
         with torch.enable_grad():
             out = TS.step(self.tg, inp[0], inp[1], self.vs2, self.vs3, inp[2], inp[3], inp[4], self.nn,
-                          self.Tn, self.J1, self.dts[j], self.Teinf, tt, self.diffsolvetype, diffusion=diff)
+                          self.Tn, self.J1, self.dts[j], self.Teinf, tt, self.diffsolvetype, diffusion=diff,
+                          sweep_impl=sweep)
             pairs = [(o, c) for o, c in zip(out, cot) if c is not None]
             wrt = inp + ([tt] if tt is not None else [])
             grads = torch.autograd.grad([o for o, _ in pairs], wrt, [c for _, c in pairs], allow_unused=True)
@@ -211,6 +232,43 @@ class DiffProblem:
 
 
 _DIFF_FN = None
+_SWEEP_FN = None
+
+
+def _sweep_fn():
+    """torch.autograd.Function: CUDA field sweep forward, CUDA sweep VJP backward."""
+    global _SWEEP_FN
+    if _SWEEP_FN is None:
+        import torch
+
+        class SweepFn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, f, v, problem, dim, frank, nsp, j):
+                f = f.contiguous()
+                v = v.contiguous()
+                out = f.clone()
+                dt = problem.dt_tensor(j)
+                _lib.check(_lib.lib().gem_sweep_field_dev(problem.dg.handle, dim, frank, nsp, F._ptr(out), F._ptr(v),
+                                                          F._ptr(dt), F._stream()))
+                ctx.problem, ctx.dim, ctx.frank, ctx.nsp, ctx.j = problem, dim, frank, nsp, j
+                ctx.save_for_backward(f, v)
+                return out
+
+            @staticmethod
+            def backward(ctx, obar):
+                f, v = ctx.saved_tensors
+                P = ctx.problem
+                obar = obar.contiguous()
+                fbar = obar.clone()
+                vbar = torch.zeros_like(v) if ctx.needs_input_grad[1] else None
+                dt = P.dt_tensor(ctx.j)
+                _lib.check(_lib.lib().gem_sweep_field_vjp_dev(
+                    P.dg.handle, ctx.dim, ctx.frank, ctx.nsp, F._ptr(f), F._ptr(v), F._ptr(dt), F._ptr(obar),
+                    F._ptr(fbar), None if vbar is None else F._ptr(vbar), F._stream()))
+                return fbar, vbar, None, None, None, None, None
+
+        _SWEEP_FN = SweepFn
+    return _SWEEP_FN
 
 
 def _diffusion_fn():

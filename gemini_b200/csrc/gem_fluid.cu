@@ -663,6 +663,60 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
   return GEM_OK;
 }
 
+// One field sweep on a caller-provided field (differentiable path): species 0..nsp-1 of
+// the ghosted block f, face velocities v (reference face layout), frank 0 or 1.
+int gem_sweep_field_dev(const gem_grid* g, int dim, int frank, int nsp, double* f, const double* v,
+                        const double* dt, void* stream) {
+  if (check_grid(g) || !f || !v || !dt) return set_err(GEM_EINVAL, "null argument");
+  if (dim < 1 || dim > 3 || frank < 0 || frank > 1 || nsp < 1 || nsp > LSP)
+    return set_err(GEM_EINVAL, "dim %d / frank %d / nsp %d out of range", dim, frank, nsp);
+  SweepArgs a;
+  a.G = g->dev;
+  Blocks B;
+  B.F = f;  // which 0 reads ns(s) = F + s*ng (frank 0); which 1 reads rv(s) = A + s*ng (frank 1)
+  B.A = f;
+  B.ng = g->dev.d.ng;
+  a.B = B;
+  a.vsi = v;
+  a.vs1i = nullptr;
+  a.dtp = dt;
+  a.dtp_w = nullptr;
+  a.which = (frank == 1 && dim != 1) ? 1 : 0;
+  return launch_sweep(g, dim, false, a, nsp, S(stream));
+}
+
+int gem_sweep_field_vjp_dev(const gem_grid* g, int dim, int frank, int nsp, const double* f, const double* v,
+                            const double* dt, const double* obar, double* fbar, double* vbar, void* stream) {
+  if (check_grid(g) || !f || !v || !dt || !obar || !fbar) return set_err(GEM_EINVAL, "null argument");
+  if (dim < 1 || dim > 3 || frank < 0 || frank > 1 || nsp < 1 || nsp > LSP)
+    return set_err(GEM_EINVAL, "dim %d / frank %d / nsp %d out of range", dim, frank, nsp);
+  SweepVjpArgs a;
+  a.G = g->dev;
+  a.f = f;
+  a.v = v;
+  a.dtp = dt;
+  a.obar = obar;
+  a.fbar = fbar;
+  a.vbar = vbar;
+  a.frank = (dim == 1) ? 0 : frank;
+  a.nsp = nsp;
+  const Dims& d = g->dev.d;
+  const long long nl = (dim == 1) ? (long long)d.lx2 * d.lx3 : (dim == 2) ? (long long)d.lx1 * d.lx3
+                                                                          : (long long)d.lx1 * d.lx2;
+  const unsigned nb = grid_for(nl * nsp, 128, 16);
+  cudaStream_t st = S(stream);
+  const bool u = g->dev.unit != 0;
+  if (dim == 1) {
+    if (u) k_sweep_vjp<1, true><<<nb, 128, 0, st>>>(a); else k_sweep_vjp<1, false><<<nb, 128, 0, st>>>(a);
+  } else if (dim == 2) {
+    if (u) k_sweep_vjp<2, true><<<nb, 128, 0, st>>>(a); else k_sweep_vjp<2, false><<<nb, 128, 0, st>>>(a);
+  } else {
+    if (u) k_sweep_vjp<3, true><<<nb, 128, 0, st>>>(a); else k_sweep_vjp<3, false><<<nb, 128, 0, st>>>(a);
+  }
+  GEM_LAUNCHED("k_sweep_vjp");
+  return GEM_OK;
+}
+
 // Vector-Jacobian product of the energy diffusion (differentiable path).
 long long gem_diffusion_vjp_scratch_doubles(const gem_grid* g) {
   if (!g) return -1;

@@ -1937,6 +1937,135 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
 }
 
 // ======================================================================================
+// 7c. Adjoint (vector-Jacobian product) of one field sweep (advec.f90:384-435 along x1, x2
+//     or x3, species 0..nsp-1), for the differentiable path.  With the limiter and upwind
+//     branches of the forward sweep replayed, the line update is linear in f, and its
+//     transpose is a local stencil: each face's flux cotangent goes to the one or two cells
+//     its phi reads and, through the selected slope (zero, centred, or twice the left or
+//     right difference), to two more cells.  One thread per (line, species), i1 fastest for
+//     the x2/x3 lines.  fbar enters holding the output cotangent (the identity part) and
+//     receives the flux parts; vbar (optional) gets the face-velocity cotangent.
+// ======================================================================================
+struct SweepVjpArgs {
+  GridDev G;
+  const double* f;  // the sweep's input field (ghosted, nsp species blocks)
+  const double* v;  // face velocities (reference face layout, species blocks)
+  const double* dtp;
+  const double* obar;  // cotangent of the output field
+  double* fbar;        // in: a copy of obar; out: the cotangent of f
+  double* vbar;        // optional: cotangent of v (same layout as v)
+  int frank, nsp;
+};
+
+// minmod(a,b) branch: 0 zero, 1 a, 2 b (advec.f90:438-447)
+__device__ __forceinline__ int minmod_branch(double a, double b) {
+  if (a * b <= 0.0) return 0;
+  return (fabs(a) < fabs(b)) ? 1 : 2;
+}
+
+template <int DIM, bool UNIT>
+__global__ void __launch_bounds__(128) k_sweep_vjp(SweepVjpArgs P) {
+  const GridDev& G = P.G;
+  const Dims d = G.d;
+  const double dt = *P.dtp;
+  const int lx = (DIM == 1) ? d.lx1 : (DIM == 2) ? d.lx2 : d.lx3;
+  const int na = (DIM == 1) ? d.lx2 : d.lx1;  // fastest line coordinate
+  const int nb = (DIM == 3) ? d.lx2 : d.lx3;
+  const long long nlines = (long long)na * nb;
+  const long long nthr = nlines * P.nsp;
+  const Line1D& L = G.L[DIM - 1];
+  const FaceTab& FT = G.F[DIM - 1];
+  if (lx <= 1) return;  // single-cell lines pass through
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nthr;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(t / nlines);
+    const long long ln = t - (long long)s * nlines;
+    const int a = (int)(ln % na) + 1, b = (int)(ln / na) + 1;
+    long long base, stride, nfaces;
+    if (DIM == 1) { base = gi(d, 0, a, b) - 1; stride = 1; nfaces = nf1(d); }
+    else if (DIM == 2) { base = gi(d, a, 0, b) - d.s2; stride = d.s2; nfaces = nf2(d); }
+    else { base = gi(d, a, b, 0) - d.s3; stride = d.s3; nfaces = nf3(d); }
+    const long long so = (long long)s * d.ng;
+    auto cell = [&](int j) -> long long { return so + base + (long long)(j + 1) * stride; };
+    auto face = [&](int j) -> long long {
+      const long long k = (DIM == 1) ? f1i(d, j, a, b) : (DIM == 2) ? f2i(d, a, j, b) : f3i(d, a, b, j);
+      return (long long)s * nfaces + k;
+    };
+    auto fmk = [&](int j) -> long long {
+      return (DIM == 1) ? fmi(FT, j, a, b) : (DIM == 2) ? fmi(FT, a, j, b) : fmi(FT, a, b, j);
+    };
+    auto cmk = [&](int j) -> long long {
+      return (DIM == 1) ? cmi(G, j, a, b) : (DIM == 2) ? cmi(G, a, j, b) : cmi(G, a, b, j);
+    };
+    auto F = [&](int j) { return P.f[cell(j)]; };
+    auto kappa = [&](int c) {  // d out(c) / d P(c) = dt / dxi(c) / ha1(c)
+      double ha1 = 1.0;
+      if (!UNIT) ha1 = (P.frank == 1) ? __ldg(G.ha1_1 + cmk(c)) : __ldg(G.ha1_0 + cmk(c));
+      return dt / __ldg(L.dxi + c - 1) / ha1;
+    };
+    // slope(k) with its branch, and the accumulation of a slope cotangent into fbar
+    auto slope = [&](int k, int& code) -> double {
+      const double fm = F(k - 1), f0 = F(k), fp = F(k + 1);
+      const double dxk = __ldg(L.dx + k), dxk1 = __ldg(L.dx + k + 1);
+      const double Ls = (f0 - fm) / dxk, Rs = (fp - f0) / dxk1, Cs = (fp - fm) / (dxk + dxk1);
+      const int inner = minmod_branch(2 * Ls, 2 * Rs);
+      const double m1 = (inner == 0) ? 0.0 : (inner == 1) ? 2 * Ls : 2 * Rs;
+      const int outer = minmod_branch(Cs, m1);
+      // 0 zero, 1 centred, 2 twice left, 3 twice right
+      code = (outer == 0) ? 0 : (outer == 1) ? 1 : (inner == 0) ? 0 : (inner == 1) ? 2 : 3;
+      return (code == 0) ? 0.0 : (code == 1) ? Cs : (code == 2) ? 2 * Ls : 2 * Rs;
+    };
+    auto add_slope_bar = [&](int k, int code, double sb) {
+      if (code == 0 || sb == 0.0) return;
+      const double dxk = __ldg(L.dx + k), dxk1 = __ldg(L.dx + k + 1);
+      if (code == 1) {
+        const double w = sb / (dxk + dxk1);
+        P.fbar[cell(k + 1)] += w;
+        P.fbar[cell(k - 1)] -= w;
+      } else if (code == 2) {
+        const double w = 2 * sb / dxk;
+        P.fbar[cell(k)] += w;
+        P.fbar[cell(k - 1)] -= w;
+      } else {
+        const double w = 2 * sb / dxk1;
+        P.fbar[cell(k + 1)] += w;
+        P.fbar[cell(k)] -= w;
+      }
+    };
+    for (int i = 1; i <= lx + 1; ++i) {
+      double Pb = 0.0;
+      if (i - 1 >= 1) Pb -= kappa(i - 1) * P.obar[cell(i - 1)];
+      if (i <= lx) Pb += kappa(i) * P.obar[cell(i)];
+      double ha2 = 1.0, hc = 1.0;
+      if (!UNIT) {
+        const long long fk = fmk(i);
+        ha2 = (P.frank == 1) ? __ldg(FT.ha2i1 + fk) : __ldg(FT.ha2i0 + fk);
+        hc = __ldg(FT.hc + fk);
+      }
+      const double phib = ha2 * Pb;
+      const double v = P.v[face(i)];
+      const double dxi_ = __ldg(L.dx + i);
+      const double vq = v / hc * dt;
+      double vb;
+      if (v < 0) {
+        int code;
+        const double sl = slope(i, code);
+        P.fbar[cell(i)] += v * phib;
+        add_slope_bar(i, code, -0.5 * v * (dxi_ + vq) * phib);
+        vb = phib * (F(i) - 0.5 * (dxi_ + vq) * sl - 0.5 * v * (dt / hc) * sl);
+      } else {
+        int code;
+        const double sl = slope(i - 1, code);
+        P.fbar[cell(i - 1)] += v * phib;
+        add_slope_bar(i - 1, code, 0.5 * v * (dxi_ - vq) * phib);
+        vb = phib * (F(i - 1) + 0.5 * (dxi_ - vq) * sl - 0.5 * v * (dt / hc) * sl);
+      }
+      if (P.vbar) P.vbar[face(i)] = vb;
+    }
+  }
+}
+
+// ======================================================================================
 // 8. CFL time step (temporal_mpi.f90:86-167), max CFL (temporal.f90:12-49), finiteness
 // ======================================================================================
 // Rates are >= 0, so their IEEE bit patterns order like unsigned integers and the block

@@ -148,15 +148,61 @@ def _wrap3(x):
     return torch.cat([x.narrow(2, 0, 2), newcore, x.narrow(2, X2 - 2, 2)], dim=2)
 
 
+def sweep_field(G: TGrid, f, v, dim, frank, nsp, dt):
+    """sweep{dim}_allspec of species 0..nsp-1 of the ghosted field f (S, X3, X2, X1) with the
+    face velocities v (reference face layout as a tensor); the other species and every
+    ghost cell pass through (advec.f90:283-381)."""
+    import torch
+
+    lx1, lx2, lx3 = G.lx1, G.lx2, G.lx3
+    h1, h2, h3 = G.h
+    hx = G.hx
+
+    def ha1(fr):
+        return (h1 * h1 * h2 * h3) if fr else (h1 * h2 * h3)
+
+    if dim == 1:
+        cell = ha1(0)[2:lx3 + 2, 2:lx2 + 2, :]
+        ha2 = hx[(2, 1)] * hx[(3, 1)]
+        h1i = hx[(1, 1)]
+        core = f[:nsp, 2:lx3 + 2, 2:lx2 + 2, :]
+        out = advec_line(core, v[:nsp], dt, G.dx[0], G.dxi[0], cell, ha2, h1i, lx1, 3)
+        top = f[:nsp]
+        mid = torch.cat([top[:, 2:lx3 + 2, :2], out, top[:, 2:lx3 + 2, lx2 + 2:]], 2)
+        top = torch.cat([top[:, :2], mid, top[:, lx3 + 2:]], 1)
+        return torch.cat([top, f[nsp:]], 0)
+    if dim == 2:
+        cell = ha1(frank)[2:lx3 + 2, :, 2:lx1 + 2]
+        ha2 = (hx[(1, 2)] * hx[(1, 2)] * hx[(3, 2)]) if frank else (hx[(1, 2)] * hx[(3, 2)])
+        h1i = hx[(2, 2)]
+        core = f[:nsp, 2:lx3 + 2, :, 2:lx1 + 2]
+        out = advec_line(core, v[:nsp], dt, G.dx[1], G.dxi[1], cell, ha2, h1i, lx2, 2)
+        top = f[:nsp]
+        mid = torch.cat([top[:, 2:lx3 + 2, :, :2], out, top[:, 2:lx3 + 2, :, lx1 + 2:]], 3)
+        top = torch.cat([top[:, :2], mid, top[:, lx3 + 2:]], 1)
+        return torch.cat([top, f[nsp:]], 0)
+    cell = ha1(frank)[:, 2:lx2 + 2, 2:lx1 + 2]
+    ha2 = (hx[(1, 3)] * hx[(1, 3)] * hx[(2, 3)]) if frank else (hx[(1, 3)] * hx[(2, 3)])
+    h1i = hx[(3, 3)]
+    core = f[:nsp, :, 2:lx2 + 2, 2:lx1 + 2]
+    out = advec_line(core, v[:nsp], dt, G.dx[2], G.dxi[2], cell, ha2, h1i, lx3, 1)
+    top = f[:nsp]
+    mid = torch.cat([top[:, :, 2:lx2 + 2, :2], out, top[:, :, 2:lx2 + 2, lx1 + 2:]], 3)
+    top = torch.cat([top[:, :, :2], mid, top[:, :, lx2 + 2:]], 2)
+    return torch.cat([top, f[nsp:]], 0)
+
+
 # ---- the step ------------------------------------------------------------------------
 def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf, Ttop=None,
-         diffsolvetype=2, diffusion=None):
+         diffsolvetype=2, diffusion=None, sweep_impl=None):
     """One fused step.  ns, vs1, Ts: (7, X3, X2, X1); vs2, vs3 likewise (inputs only);
     v1i_lo / v1i_hi: the x1 boundary faces of vs1i from the previous step, (7, lx3, lx2);
     nn: (3, lx3, lx2, lx1); Tn: (lx3, lx2, lx1); J1: (X3, X2, X1); Ttop: optional per-column
     top Dirichlet temperature (lx3, lx2) replacing Teinf; diffusion: optional replacement of
     energy_diffusion, called as diffusion(n, T, Ttop) (e.g. a function with a hand-written
-    adjoint).  Returns (ns, vs1, Ts, v1i_lo, v1i_hi) after the step."""
+    adjoint); sweep_impl: optional replacement of the field sweeps, called as
+    sweep_impl(f, v, dim, frank, nsp) with the face velocities v of direction dim.  Returns
+    (ns, vs1, Ts, v1i_lo, v1i_hi) after the step."""
     import torch
 
     lx1, lx2, lx3 = G.lx1, G.lx2, G.lx3
@@ -230,44 +276,14 @@ def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf,
     v3c = v3[:, :, 2:lx2 + 2, 2:lx1 + 2]
     v3i = 0.5 * (v3c[:, 1:lx3 + 2] + v3c[:, 2:lx3 + 3])    # (7, lx3+1, lx2, lx1)
 
-    def ha1(frank):
-        return (h1 * h1 * h2 * h3) if frank else (h1 * h2 * h3)
-
-    hx = G.hx
-
     def sweep(f, dim, frank, nsp):
-        """sweep{dim}_allspec of species 0..nsp-1 (the others pass through)."""
-        ax = _axis(dim)
-        if dim == 1:
-            cell = ha1(0)[2:lx3 + 2, 2:lx2 + 2, :]
-            ha2 = hx[(2, 1)] * hx[(3, 1)]
-            h1i = hx[(1, 1)]
-            v = v1i
-            core = f[:nsp, 2:lx3 + 2, 2:lx2 + 2, :]
-            out = advec_line(core, v[:nsp], dt, G.dx[0], G.dxi[0], cell, ha2, h1i, lx1, 3)
-            top = f[:nsp]
-            mid = torch.cat([top[:, 2:lx3 + 2, :2], out, top[:, 2:lx3 + 2, lx2 + 2:]], 2)
-            top = torch.cat([top[:, :2], mid, top[:, lx3 + 2:]], 1)
-            return torch.cat([top, f[nsp:]], 0)
-        if dim == 2:
-            cell = ha1(frank)[2:lx3 + 2, :, 2:lx1 + 2]
-            ha2 = (hx[(1, 2)] * hx[(1, 2)] * hx[(3, 2)]) if frank else (hx[(1, 2)] * hx[(3, 2)])
-            h1i = hx[(2, 2)]
-            core = f[:nsp, 2:lx3 + 2, :, 2:lx1 + 2]
-            out = advec_line(core, v2i[:nsp], dt, G.dx[1], G.dxi[1], cell, ha2, h1i, lx2, 2)
-            top = f[:nsp]
-            mid = torch.cat([top[:, 2:lx3 + 2, :, :2], out, top[:, 2:lx3 + 2, :, lx1 + 2:]], 3)
-            top = torch.cat([top[:, :2], mid, top[:, lx3 + 2:]], 1)
-            return torch.cat([top, f[nsp:]], 0)
-        cell = ha1(frank)[:, 2:lx2 + 2, 2:lx1 + 2]
-        ha2 = (hx[(1, 3)] * hx[(1, 3)] * hx[(2, 3)]) if frank else (hx[(1, 3)] * hx[(2, 3)])
-        h1i = hx[(3, 3)]
-        core = f[:nsp, :, 2:lx2 + 2, 2:lx1 + 2]
-        out = advec_line(core, v3i[:nsp], dt, G.dx[2], G.dxi[2], cell, ha2, h1i, lx3, 1)
-        top = f[:nsp]
-        mid = torch.cat([top[:, :, 2:lx2 + 2, :2], out, top[:, :, 2:lx2 + 2, lx1 + 2:]], 3)
-        top = torch.cat([top[:, :, :2], mid, top[:, :, lx2 + 2:]], 2)
-        return torch.cat([top, f[nsp:]], 0)
+        return sweep_field(G, f, {1: v1i, 2: v2i, 3: v3i}[dim], dim, frank, nsp, dt)
+
+    if sweep_impl is not None:
+        vel = {1: v1i, 2: v2i, 3: v3i}
+
+        def sweep(f, dim, frank, nsp):  # noqa: F811 -- the replacement
+            return sweep_impl(f, vel[dim], dim, frank, nsp)
 
     n = sweep(n, 3, 0, 6)
     rv = sweep(rv, 3, 1, 6)

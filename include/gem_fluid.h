@@ -130,6 +130,16 @@ int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, cons
  * boundary value of each column and species).  Ts / ns are the inputs of the forward call;
  * the kernel recomputes the forward coefficients and both TRBDF2 stages (Thomas), then
  * solves the transposed systems.  scratch: gem_diffusion_vjp_scratch_doubles(g) doubles. */
+/* One field sweep (advec.f90:384-435 along dim, species 0..nsp-1, frank 0/1; x1 sweeps use
+ * frank 0) on a caller-provided ghosted field f (nsp species blocks, updated in place) with
+ * face velocities v in the reference face layout; dt is a device pointer. */
+int gem_sweep_field_dev(const gem_grid* g, int dim, int frank, int nsp, double* f, const double* v,
+                        const double* dt, void* stream);
+/* Its vector-Jacobian product: f is the sweep's input, obar the output cotangent, fbar must
+ * hold a copy of obar on entry and receives the cotangent of f; vbar (optional) receives the
+ * cotangent of v. */
+int gem_sweep_field_vjp_dev(const gem_grid* g, int dim, int frank, int nsp, const double* f, const double* v,
+                            const double* dt, const double* obar, double* fbar, double* vbar, void* stream);
 long long gem_diffusion_vjp_scratch_doubles(const gem_grid* g);
 int gem_diffusion_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const double* Ts, const double* ns,
                           const double* electrovars, const gem_work* w, const double* dt, const double* Ybar,
