@@ -112,6 +112,15 @@ __global__ void __launch_bounds__(128) kb_clean_vel_edges(const InstDev* __restr
   }
 }
 
+template <bool UNIT>
+__global__ void __launch_bounds__(128) kb_diffusion_coef(const InstDev* __restrict__ inst, const Item* __restrict__ it,
+                                                        int n) {
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const Item q = it[w];
+    b_diffusion_coef<UNIT>(inst[q.x].df, VB{q.y, q.z, q.w});
+  }
+}
+
 // one launch per (metric variant, rows-per-lane bucket); every instance of the launch
 // uses the bucket's slot size Mslot (>= its own M)
 template <bool UNIT>
@@ -135,7 +144,7 @@ namespace {
 // One launch of the batched step: a phase, its variant (metric variant; for the diffusion
 // also the rows-per-lane bucket) and the work items of the instances it covers.
 enum BatchKernel {
-  BK_DT = 0, BK_GX1, BK_GX2, BK_GX3, BK_SW3, BK_SW1, BK_SW2, BK_EPI, BK_CVE, BK_DIFF, BK_N
+  BK_DT = 0, BK_GX1, BK_GX2, BK_GX3, BK_SW3, BK_SW1, BK_SW2, BK_EPI, BK_CVE, BK_DCOEF, BK_DIFF, BK_N
 };
 
 struct BatchLaunch {
@@ -208,6 +217,13 @@ int launch_grid(gem_batch* b, BatchLaunch& L) {
                           : occupancy_grid(kb_sweep_march<2, false>, 32 * LSP, 0, n, sc, &L.grid);
     case BK_EPI: return occupancy_grid(kb_ghost_epilogue, 256, 0, n, sc, &L.grid);
     case BK_CVE: return occupancy_grid(kb_clean_vel_edges, 128, 0, n, sc, &L.grid);
+    case BK_DCOEF:
+      if (u) {
+        GEM_CUDA(cudaFuncSetAttribute(kb_diffusion_coef<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+        return occupancy_grid(kb_diffusion_coef<true>, 128, L.smem, n, sc, &L.grid);
+      }
+      GEM_CUDA(cudaFuncSetAttribute(kb_diffusion_coef<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+      return occupancy_grid(kb_diffusion_coef<false>, 128, L.smem, n, sc, &L.grid);
     case BK_DIFF:
       // the dynamic shared-memory limit was raised to the largest bucket's size beforehand
       return u ? occupancy_grid(kb_diffusion<true>, 32 * L.wpb, L.smem, n, sc, &L.grid)
@@ -242,7 +258,8 @@ int batch_build_lists(gem_batch* b) {
         const gem_grid* g = b->grids[i];
         const Dims& d = g->dev.d;
         const bool unit = g->dev.unit != 0;
-        const bool variant = (k == BK_DT || k == BK_SW3 || k == BK_SW1 || k == BK_SW2 || k == BK_DIFF);
+        const bool variant = (k == BK_DT || k == BK_SW3 || k == BK_SW1 || k == BK_SW2 || k == BK_DCOEF ||
+                              k == BK_DIFF);
         if (variant && unit != (u == 1)) continue;
         if (!variant && u == 0) continue;  // unsplit phases: once
         const int gx13 = (d.lx1 + 31) / 32;
@@ -261,6 +278,12 @@ int batch_build_lists(gem_batch* b) {
             if (g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1))
               add_items(launch_for(k, 0), i, grid_for((long long)d.lx2 * d.lx3 * LSP, 128));
             break;
+          case BK_DCOEF: {
+            BatchLaunch& L = launch_for(k, u);
+            L.smem = std::max<size_t>(L.smem, (size_t)3 * d.lx1 * sizeof(double));
+            add_items(L, i, std::min<long long>((long long)d.lx2 * d.lx3 * LSP, (long long)num_sms() * 16));
+            break;
+          }
           case BK_DIFF: {
             const int Ms = diff_bucket_M(diff_M(g));
             BatchLaunch& L = launch_for(k, u, Ms);
@@ -335,6 +358,10 @@ int batch_enqueue(gem_batch* b, cudaStream_t st) {
         break;
       case BK_EPI: kb_ghost_epilogue<<<L.grid, 256, 0, st>>>(I, L.d_items, n); break;
       case BK_CVE: kb_clean_vel_edges<<<L.grid, 128, 0, st>>>(I, L.d_items, n); break;
+      case BK_DCOEF:
+        if (u) kb_diffusion_coef<true><<<L.grid, 128, L.smem, st>>>(I, L.d_items, n);
+        else kb_diffusion_coef<false><<<L.grid, 128, L.smem, st>>>(I, L.d_items, n);
+        break;
       case BK_DIFF:
         if (u) kb_diffusion<true><<<L.grid, 32 * L.wpb, L.smem, st>>>(I, L.d_items, n, L.Mslot);
         else kb_diffusion<false><<<L.grid, 32 * L.wpb, L.smem, st>>>(I, L.d_items, n, L.Mslot);
@@ -397,6 +424,7 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
     I.df.dtp = w->dt;
     I.df.Teinf = cfgs[i].Teinf;
     I.df.Ttop = w->Ttop;
+    I.df.coef = w->dcoef;
     I.df.solver = cfgs[i].diffsolvetype;
     I.df.M = M;
     I.df.Mslot = diff_bucket_M(M);  // the slot size of the instance's diffusion launch

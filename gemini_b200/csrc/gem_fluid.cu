@@ -93,6 +93,7 @@ struct gem_work {
   int lx1, lx2, lx3;
   double *vs1i, *vs2i, *vs3i, *nn, *Tn, *dt;
   double* Ttop;             // per-column exospheric temperature (lx2*lx3), or null for Teinf
+  double* dcoef;            // diffusion coefficients C, D, B per interior cell (DCOEF_N * nc)
   unsigned long long* acc;  // 32 slots: CFL maxima / counters
   long long nf1, nf2, nf3;
   // device staging of the host blocks for gem_fluid_adv_host
@@ -213,6 +214,17 @@ int launch_diffusion(const gem_grid* g, DiffArgs a, cudaStream_t st) {
   if (per_sm < 1) per_sm = 1;
   const long long cap = (long long)num_sms() * per_sm;
   if (nblk > cap) nblk = cap;
+  if (!a.coef) return set_err(GEM_EINVAL, "diffusion without a coefficient buffer");
+  const unsigned nrow = (unsigned)std::min<long long>((long long)d.lx2 * d.lx3 * LSP, (long long)num_sms() * 16);
+  const size_t csm = (size_t)3 * d.lx1 * sizeof(double);
+  if (g->dev.unit) {
+    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_coef<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+    k_diffusion_coef<true><<<nrow, 128, csm, st>>>(a);
+  } else {
+    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_coef<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+    k_diffusion_coef<false><<<nrow, 128, csm, st>>>(a);
+  }
+  GEM_LAUNCHED("k_diffusion_coef");
   if (g->dev.unit)
     k_diffusion<true><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
   else
@@ -442,6 +454,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
   w->vs1i = w->vs2i = w->vs3i = w->nn = w->Tn = w->dt = nullptr;
   w->acc = nullptr;
   w->Ttop = nullptr;
+  w->dcoef = nullptr;
   w->F = w->A = w->E = nullptr;
   w->nF = w->nA = w->nE = 0;
   w->lx1 = d.lx1;
@@ -460,7 +473,8 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
             {(void**)&w->nn, sizeof(double) * nc * 3},
             {(void**)&w->Tn, sizeof(double) * nc},
             {(void**)&w->dt, sizeof(double) * 4},
-            {(void**)&w->acc, sizeof(unsigned long long) * 32}};
+            {(void**)&w->acc, sizeof(unsigned long long) * 32},
+            {(void**)&w->dcoef, sizeof(double) * nc * DCOEF_N}};
   for (auto& a : al) {
     if (cudaMalloc(a.p, a.bytes) != cudaSuccess) {
       gem_work_destroy(w);
@@ -479,7 +493,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
 int gem_work_destroy(gem_work* w) {
   if (!w) return GEM_OK;
   for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);
-  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop};
+  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop, w->dcoef};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete w;
@@ -635,6 +649,7 @@ int gem_energy_diffusion_dev(const gem_cfg* cfg, const gem_grid* g, double* flui
   a.dtp = dt;
   a.Teinf = cfg->Teinf;
   a.Ttop = w->Ttop;
+  a.coef = w->dcoef;
   a.solver = cfg->diffsolvetype;
   a.fused = 0;
   int rc = launch_diffusion(g, a, S(stream));
@@ -863,6 +878,7 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
   d.dtp = dt;
   d.Teinf = cfg->Teinf;
   d.Ttop = w->Ttop;
+  d.coef = w->dcoef;
   d.solver = cfg->diffsolvetype;
   d.fused = 1;
   w->timer.record(6, st);

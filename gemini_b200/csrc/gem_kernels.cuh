@@ -1165,7 +1165,13 @@ struct DiffArgs {
   int M;       // rows per lane
   int Mslot;   // rows per lane that each warp's shared-memory slot is sized for (>= M)
   int fused;   // 1: clean_param(3) + T2rhoe folded into the store
+  double* coef;  // per-cell C (7 species), D (7), B (electrons): written by k_diffusion_coef
 };
+
+// Coefficient scratch layout (interior cells q = ci(i1,i2,i3), nc of them): the per-row
+// conduction factors q-, q+ of species s at coef[s*nc + q], coef[(LSP+s)*nc + q], and the
+// electron advection factor bq at coef[2*LSP*nc + q] (rows 2..lx1-1; rows 1, lx1 hold 0).
+constexpr int DCOEF_N = 2 * LSP + 1;
 
 // shared-memory arrays per warp: inputs (T and the per-row conduction/advection factors),
 // the stage right-hand side / residual, the solution, and the factorisation (IB, SS, TT)
@@ -1402,6 +1408,86 @@ __device__ void refined_solve(const WarpMem& W, int M, int lane, RowM rowm) {
   __syncwarp();
 }
 
+// thermal_conduct + diffusion_prep per cell (collisions.f90:162-199, diffusion.f90:24-52):
+// C = (gamma-1)/kB / max(n,1e-5) / (h1 h2 h3), D = lambda h2 h3 / h1, B = C beta / h1, then the
+// per-row factors of the band matrices (PDEparabolic.f90:70-80) q- = C Dh(i)/dx1i/dx1(i),
+// q+ = C Dh(i+1)/dx1i/dx1(i+1), bq = B/(dx1(i+1)+dx1(i)) with Dh(i) = (D(i-1)+D(i))/2.
+// One block per (i2, i3, species) row at a time, threads along x1 (coalesced, full
+// occupancy); C, D, B of the row in dynamic shared memory (3*lx1 doubles).
+template <bool UNIT>
+__device__ __forceinline__ void b_diffusion_coef(const DiffArgs& P, const VB vb) {
+  extern __shared__ double dsm[];
+  const GridDev& G = P.G;
+  const Dims d = G.d;
+  const int n = d.lx1;
+  double* sC = dsm;
+  double* sD = dsm + n;
+  double* sB = dsm + 2 * n;
+  const long long nc = nci(d);
+  const int ncol = d.lx2 * d.lx3;
+  const int nrow = ncol * LSP;
+  const Line1D& L1 = G.L[0];
+  for (int r = vb.bx; r < nrow; r += vb.gx) {
+    const int s = r / ncol;
+    const int col = r - s * ncol;
+    const int i2 = col % d.lx2 + 1, i3 = col / d.lx2 + 1;
+    const long long m0 = gi(d, 0, i2, i3);
+    const long long mm0 = cmi(G, 0, i2, i3);
+    const long long q0 = ci(d, 1, i2, i3) - 1;
+    const double* Tcol = P.B.Ts(s) + m0;
+    const double* ncol_ = P.B.ns(s) + m0;
+    const double c0 = (c_gammas[s] - 1.0) / KB;
+    for (int i = threadIdx.x + 1; i <= n; i += blockDim.x) {
+      const double T = Tcol[i];
+      const double nv = ncol_[i];
+      const long long mk = mm0 + i;
+      const double h1v = ldm<UNIT>(G.h1, mk), h2v = ldm<UNIT>(G.h2, mk), h3v = ldm<UNIT>(G.h3, mk);
+      const double yh1 = ldm<UNIT>(G.yh1, mk);
+      double ha1v = 1.0, yha1v = 1.0;
+      cell_metric<UNIT>(G, mk, 0, ha1v, yha1v);  // h1*h2*h3
+      const double T25 = pow25(T);
+      double lam, Bc = 0.0;
+      if (s < LSP - 1) {
+        lam = c_tcoef[s] * T25;
+      } else {
+        const long long q = q0 + i;
+        const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
+        const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sqrt(T) * (1 - 1.21e-4 * T) +
+                         n3 * 2.2e-16 * (1 + 3.6e-2 * sqrt(T));
+        lam = ELCHRG * 100 * 7.7e5 * T25 / (1 + 3.22e4 * (T * T) / nv * X);
+        Bc = 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i];  // beta (collisions.f90:197)
+      }
+      const double Cc = mdiv(c0 / fmax_f(nv, MINDENSDIV), ha1v, yha1v);
+      sC[i - 1] = Cc;
+      sD[i - 1] = mdiv(lam * h2v * h3v, h1v, yh1);
+      sB[i - 1] = (s < LSP - 1) ? 0.0 : mdiv(Cc * Bc, h1v, yh1);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x + 1; i <= n; i += blockDim.x) {
+      double qp = 0.0, qm = 0.0, bq = 0.0;
+      if (i >= 2 && i <= n - 1) {
+        const double Dm = sD[i - 2], Dc = sD[i - 1], Dp = sD[i];
+        const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);  // PDEparabolic.f90:49
+        const double Cc = sC[i - 1];
+        const double dxi = __ldg(L1.dxi + i - 1), ydxi = __ldg(L1.ydxi + i - 1);
+        qm = mdiv(mdiv(Cc * Dhm, dxi, ydxi), __ldg(L1.dx + i), __ldg(L1.ydx + i));
+        qp = mdiv(mdiv(Cc * Dhp, dxi, ydxi), __ldg(L1.dx + i + 1), __ldg(L1.ydx + i + 1));
+        bq = mdiv(sB[i - 1], __ldg(L1.dxs + i), __ldg(L1.ydxs + i));  // dx1(i+1)+dx1(i)
+      }
+      const long long q = q0 + i;
+      P.coef[(long long)s * nc + q] = qm;
+      P.coef[(long long)(LSP + s) * nc + q] = qp;
+      if (s == LSP - 1) P.coef[(long long)2 * LSP * nc + q] = bq;
+    }
+    __syncthreads();
+  }
+}
+
+template <bool UNIT>
+__global__ void __launch_bounds__(128) k_diffusion_coef(DiffArgs P) {
+  b_diffusion_coef<UNIT>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
 template <bool UNIT>
 __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
   extern __shared__ double smem[];
@@ -1427,41 +1513,27 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
     const long long q0 = ci(d, 1, i2, i3) - 1;  // q0 + i: (i, i2, i3) in the interior-only arrays
     const double* Tcol = P.B.Ts(s) + m0;
     const double* ncol = P.B.ns(s) + m0;
-    const double c0 = (c_gammas[s] - 1.0) / KB;
-    // ---- thermal_conduct + diffusion_prep per cell (collisions.f90:162-199,
-    // diffusion.f90:24-52): C -> DA_SS, D -> DA_IB, B -> DA_TT, read coalesced along x1
+    // ---- T and the band factors q-, q+, bq (k_diffusion_coef), read along x1
+    // Dirichlet values (diffusion.f90:54-79), loaded early
+    const double tn1 = __ldg(P.Tn + ci(d, 1, i2, i3)), tnl = __ldg(P.Tn + ci(d, n, i2, i3));
+    const double tinf = P.Ttop ? __ldg(P.Ttop + (i2 - 1) + (long long)d.lx2 * (i3 - 1)) : P.Teinf;
     int lp = lp0, kp = kp0;
+    // independent chunks: unrolled so that their loads are in flight together
+#pragma unroll 4
     for (int c = 0; c < M; ++c) {
       const int i = 1 + 32 * c + lane;
-      double T = 0.0, Cc = 0.0, Dc = 0.0, Bc = 0.0;
+      double T = 0.0, qm = 0.0, qp = 0.0, bq = 0.0;
       if (i <= n) {
+        const long long q = q0 + i;
         T = Tcol[i];
-        const double nv = ncol[i];
-        const long long mk = mm0 + i;
-        const double h1v = ldm<UNIT>(G.h1, mk), h2v = ldm<UNIT>(G.h2, mk), h3v = ldm<UNIT>(G.h3, mk);
-        const double yh1 = ldm<UNIT>(G.yh1, mk);
-        double ha1v = 1.0, yha1v = 1.0;
-        cell_metric<UNIT>(G, mk, 0, ha1v, yha1v);  // h1*h2*h3
-        const double T25 = pow25(T);
-        double lam;
-        if (s < LSP - 1) {
-          lam = c_tcoef[s] * T25;
-        } else {
-          const long long q = q0 + i;
-          const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
-          const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sqrt(T) * (1 - 1.21e-4 * T) +
-                           n3 * 2.2e-16 * (1 + 3.6e-2 * sqrt(T));
-          lam = ELCHRG * 100 * 7.7e5 * T25 / (1 + 3.22e4 * (T * T) / nv * X);
-          Bc = 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i];  // beta (collisions.f90:197)
-        }
-        Cc = mdiv(c0 / fmax_f(nv, MINDENSDIV), ha1v, yha1v);
-        Dc = mdiv(lam * h2v * h3v, h1v, yh1);
-        Bc = (s < LSP - 1) ? 0.0 : mdiv(Cc * Bc, h1v, yh1);
+        qm = P.coef[(long long)s * nc + q];
+        qp = P.coef[(long long)(LSP + s) * nc + q];
+        if (s == LSP - 1) bq = P.coef[(long long)2 * LSP * nc + q];
       }
       W.at_lane(DA_T, kp, lp) = T;
-      W.at_lane(DA_SS, kp, lp) = Cc;
-      W.at_lane(DA_IB, kp, lp) = Dc;
-      W.at_lane(DA_TT, kp, lp) = Bc;
+      W.at_lane(DA_QM, kp, lp) = qm;
+      W.at_lane(DA_QP, kp, lp) = qp;
+      W.at_lane(DA_BQ, kp, lp) = bq;
       kp += r32;
       lp += q32;
       if (kp >= M) {
@@ -1470,41 +1542,15 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
       }
     }
     __syncwarp();
-    // ---- per-row conduction factors qm = C*Dh(i)/dx1i/dx1(i), qp = C*Dh(i+1)/dx1i/dx1(i+1)
-    // and advection factor bq = B/(dx1(i+1)+dx1(i)) (PDEparabolic.f90:70-80)
-    const double Dprev = __shfl_up_sync(0xffffffffu, W.at(DA_IB, M - 1), 1);
-    const double Dnext = __shfl_down_sync(0xffffffffu, W.at(DA_IB, 0), 1);
-    for (int k = 0; k < M; ++k) {
-      const int i = 1 + lane * M + k;
-      double qp = 0.0, qm = 0.0, bq = 0.0;
-      if (i >= 2 && i <= n - 1) {
-        const double Dm = (k > 0) ? W.at(DA_IB, k - 1) : Dprev;
-        const double Dc = W.at(DA_IB, k);
-        const double Dp = (k < M - 1) ? W.at(DA_IB, k + 1) : Dnext;
-        const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);  // PDEparabolic.f90:49
-        const double Cc = W.at(DA_SS, k);
-        const Line1D& L1 = G.L[0];
-        const double dxi = __ldg(L1.dxi + i - 1), ydxi = __ldg(L1.ydxi + i - 1);
-        qm = mdiv(mdiv(Cc * Dhm, dxi, ydxi), __ldg(L1.dx + i), __ldg(L1.ydx + i));
-        qp = mdiv(mdiv(Cc * Dhp, dxi, ydxi), __ldg(L1.dx + i + 1), __ldg(L1.ydx + i + 1));
-        bq = mdiv(W.at(DA_TT, k), __ldg(L1.dxs + i), __ldg(L1.ydxs + i));  // dx1(i+1)+dx1(i)
-      }
-      W.at(DA_QP, k) = qp;
-      W.at(DA_QM, k) = qm;
-      W.at(DA_BQ, k) = bq;
-    }
-    __syncwarp();
     const double Tprev = __shfl_up_sync(0xffffffffu, W.at(DA_T, M - 1), 1);
     const double Tnext = __shfl_down_sync(0xffffffffu, W.at(DA_T, 0), 1);
     // Dirichlet values (diffusion.f90:54-79)
     double tmin, tmax;
     {
-      const double tn1 = __ldg(P.Tn + ci(d, 1, i2, i3)), tnl = __ldg(P.Tn + ci(d, n, i2, i3));
-      if (G.gridflag == 0) { tmin = tn1; tmax = tnl; }
       // the exospheric side: Teinf, or the per-column value when one is set
-      const double tinf = P.Ttop ? __ldg(P.Ttop + (i2 - 1) + (long long)d.lx2 * (i3 - 1)) : P.Teinf;
-      if (G.gridflag == 1) { tmin = tinf; tmax = tnl; }
-      else if (G.gridflag == 2) { tmin = tn1; tmax = tinf; }
+      if (G.gridflag == 0) { tmin = tn1; tmax = tnl; }
+      else if (G.gridflag == 1) { tmin = tinf; tmax = tnl; }
+      else { tmin = tn1; tmax = tinf; }
     }
     auto Tat = [&](int k) -> double {
       if (k < 0) return Tprev;
@@ -1587,17 +1633,30 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
       refined_solve(W, M, lane, rowBE);
     }
     // ---- store: max(T,100) (multifluid.f90:340); fused: clean_param(3) and T2rhoe
+    // written along x1 (coalesced): row idx = 32c + lane sits in slot (idx/M, idx%M)
     double* Tout = P.B.Ts(s) + m0;
-    for (int k = 0; k < M; ++k) {
-      const int i = 1 + lane * M + k;
-      if (i > n) break;
-      double T = fmax_f(W.at(DA_R, k), 100.0);
-      if (P.fused) {
-        if (is_null(G, i, i2, i3)) T = 100;
-        Tout[i] = T;
-        P.B.re(s)[m0 + i] = conv_re(ncol[i], T, s);
-      } else {
-        Tout[i] = T;
+    __syncwarp();
+    {
+      int lq = lp0, kq = kp0;
+#pragma unroll 4
+      for (int c = 0; c < M; ++c) {
+        const int i = 1 + 32 * c + lane;
+        if (i <= n) {
+          double T = fmax_f(W.at_lane(DA_R, kq, lq), 100.0);
+          if (P.fused) {
+            if (is_null(G, i, i2, i3)) T = 100;
+            Tout[i] = T;
+            P.B.re(s)[m0 + i] = conv_re(ncol[i], T, s);
+          } else {
+            Tout[i] = T;
+          }
+        }
+        kq += r32;
+        lq += q32;
+        if (kq >= M) {
+          kq -= M;
+          ++lq;
+        }
       }
     }
     if (!P.fused && lane == 0) {
