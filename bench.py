@@ -520,6 +520,61 @@ def run_adjoint(args):
                         "interface velocities and conversions; CUDA recompute per checkpoint segment"}
 
 
+BATCHED_ADJOINT = dict(instances=32, steps=200, checkpoint_every=10, group=8, seed=77)
+
+
+def run_batched_adjoint(args):
+    """Batched + adjoint workload: 32 uneven Cartesian instances (lx1 128-256, lx2, lx3
+    32-128), 200 steps, checkpoint every 10; per-instance gradients of the L2 misfit of the
+    final Te and n_O+ w.r.t. the initial ion densities and the per-column top temperature.
+    Forward: one batched step per time step (graph replay, prescribed time steps)."""
+    import torch
+
+    from gemini_b200 import adjoint as AD
+    from gemini_b200 import grid as G
+    from gemini_b200 import state as S
+
+    a = BATCHED_ADJOINT
+    rng = np.random.default_rng(a["seed"])
+    inst = []
+    for i in range(a["instances"]):
+        g = G.cartesian_grid(int(rng.integers(128, 257)), int(rng.integers(32, 129)), int(rng.integers(32, 129)))
+        inst.append((g, S.init_state(g, seed=a["seed"] * 100 + i, perturb=0.1)))
+    BA = AD.BatchedAdjoint(inst, a["steps"], checkpoint_every=a["checkpoint_every"], group=a["group"])
+    controls, targets = [], []
+    for (g, st), P in zip(inst, BA.problems):
+        I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
+        controls.append((P.base[(slice(0, 6),) + I].clone(),
+                         torch.from_numpy(st.Teinf * (1 + 0.05 * rng.uniform(-1, 1, (g.lx3, g.lx2)))).cuda()))
+        targets.append((torch.from_numpy(rng.uniform(1500, 3000, (g.lx3, g.lx2, g.lx1))).cuda(),
+                        torch.from_numpy(rng.uniform(0.5e10, 5e10, (g.lx3, g.lx2, g.lx1))).cuda()))
+
+    def loss(i, ns, Ts):
+        return AD.misfit(ns, Ts, targets[i][0], targets[i][1], inst[i][0])
+
+    s = torch.cuda.current_stream()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    e[0].record(s)
+    for g0 in range(0, len(inst), a["group"]):
+        idx = list(range(g0, min(g0 + a["group"], len(inst))))
+        BA.forward_group(idx, [controls[i] for i in idx], keep=False)
+    e[1].record(s)
+    e[2].record(s)
+    res = BA.gradients(controls, loss)
+    e[3].record(s)
+    torch.cuda.synchronize()
+    fwd = e[0].elapsed_time(e[1])
+    fb = e[2].elapsed_time(e[3])
+    cells = sum(g.lx1 * g.lx2 * g.lx3 for g, _ in inst)
+    return {"workload": f"{a['instances']} uneven Cartesian instances (lx1 128-256, lx2,lx3 32-128, {cells} cells), "
+                        f"{a['steps']} steps, checkpoint every {a['checkpoint_every']}",
+            "forward_ms": fwd, "forward_backward_ms": fb, "adjoint_over_forward": (fb - fwd) / fwd,
+            "forward_value": cells * 7 * a["steps"] / (fwd / 1e3) / 1e9, "unit": UNIT,
+            "gradients_finite": bool(all(torch.isfinite(gn).all() and torch.isfinite(gt).all() for _, gn, gt in res)),
+            "forward": "groups of 8 instances, one batched step (captured graph, prescribed time steps) per time step"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -532,6 +587,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched instances")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instance measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
+    ap.add_argument("--batched-adjoint", action="store_true",
+                    help="also measure the batched adjoint workload (32 instances x 200 steps; minutes)")
     ap.add_argument("--lx", type=int, nargs=3, default=None, metavar=("LX1", "LX2", "LX3"),
                     help="override the grid size (profiling runs on a smaller case)")
     args = ap.parse_args()
@@ -554,6 +611,10 @@ def main():
         import torch
         torch.cuda.empty_cache()
         line["adjoint"] = run_adjoint(args)
+    if args.batched_adjoint and rank == 0:
+        import torch
+        torch.cuda.empty_cache()
+        line["batched_adjoint"] = run_batched_adjoint(args)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -84,6 +84,7 @@ _SIGS = [
     ("gem_batch_size", ctypes.c_int, [_VP]),
     ("gem_batch_set_param", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     ("gem_batch_step", ctypes.c_int, [_VP, _VP]),
+    ("gem_batch_step_fixed_dt", ctypes.c_int, [_VP, _D, _VP]),
     ("gem_batch_dts", ctypes.c_int, [_VP, _D]),
     ("gem_batch_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]),
     ("gem_capi_bind_grid", None, [_VP]),

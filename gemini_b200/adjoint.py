@@ -302,6 +302,94 @@ class FluidAdvance:
         return _Fn.apply(n0, Ttop, problem)
 
 
+def backward_from_checkpoints(P: "DiffProblem", ckpt, Ttop, g_ns, g_Ts):
+    """Pull the cotangents of the final (ns, Ts) back to (n0, Ttop): segment by segment from
+    the checkpoints {step: state}, recomputing each segment with the CUDA step."""
+    import torch
+
+    zeros = lambda t: torch.zeros_like(t)
+    ns_f = P.base[0:LSP]
+    cot = [g_ns if g_ns is not None else zeros(ns_f), zeros(ns_f),
+           g_Ts if g_Ts is not None else zeros(ns_f), zeros(P.lo0), zeros(P.hi0)]
+    g_top = torch.zeros_like(Ttop) if Ttop is not None else None
+    starts = sorted(ckpt)
+    for seg_i in range(len(starts) - 1, -1, -1):
+        j0 = starts[seg_i]
+        j1 = starts[seg_i + 1] if seg_i + 1 < len(starts) else P.nsteps
+        P._load(*ckpt[j0], Ttop)
+        states = [ckpt[j0]]
+        for j in range(j0, j1 - 1):
+            P.cuda_step(j)
+            states.append(P._save())
+        for j in range(j1 - 1, j0 - 1, -1):
+            cot, gt = P.step_vjp(states[j - j0], Ttop, j, cot, P.cuda_diffusion_adjoint)
+            if gt is not None:
+                g_top = g_top + gt
+    g = P.grid
+    I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
+    gns = cot[0][(slice(None),) + I]
+    g_n0 = gns[:LSP - 1] + gns[LSP - 1].unsqueeze(0)  # electrons = sum of ions
+    return g_n0, g_top
+
+
+class BatchedAdjoint:
+    """Per-instance gradients for many independent instances (uneven sizes).
+
+    Instances are processed in groups: a group's forward pass is one batched step per time
+    step (gem_batch_step_fixed_dt: every instance on its own frozen schedule, all phases as
+    one replayed CUDA graph), with each instance's state saved every k steps; then each
+    instance's cotangent is pulled back from its checkpoints (recompute + step VJPs).  The
+    group size bounds the checkpoint memory."""
+
+    def __init__(self, instances, nsteps: int, checkpoint_every: int = 10, group: int = 8, **problem_kw):
+        self.problems = [DiffProblem(g, st, nsteps, checkpoint_every=checkpoint_every, **problem_kw)
+                         for g, st in instances]
+        self.nsteps = int(nsteps)
+        self.k = max(1, int(checkpoint_every))
+        self.group = max(1, int(group))
+
+    def forward_group(self, idx, controls, keep=True):
+        """Batched forward of the instances idx from their controls [(n0, Ttop)]; returns the
+        final states and the checkpoints of each."""
+        from . import batch as BT
+
+        Ps = [self.problems[i] for i in idx]
+        for P, (n0, Ttop) in zip(Ps, controls):
+            ns = P.initial_state(n0.detach())
+            P._load(ns, P.base[LSP:2 * LSP], P.base[4 * LSP:], P.lo0, P.hi0, Ttop)
+        b = BT.Batch([(P.dg, P.ds, P.cfg) for P in Ps])
+        ckpts = [dict() for _ in Ps]
+        for j in range(self.nsteps):
+            if keep and j % self.k == 0:
+                for c, P in zip(ckpts, Ps):
+                    c[j] = P._save()
+            b.step_fixed_dt([P.dts[j] for P in Ps])
+        finals = [P._save() for P in Ps]
+        b.close()
+        return finals, ckpts
+
+    def gradients(self, controls, loss_fn):
+        """controls: [(n0, Ttop)] per instance; loss_fn(i, ns, Ts) -> scalar tensor.
+        Returns [(loss, g_n0, g_Ttop)] per instance."""
+        import torch
+
+        out = [None] * len(self.problems)
+        for g0 in range(0, len(self.problems), self.group):
+            idx = list(range(g0, min(g0 + self.group, len(self.problems))))
+            finals, ckpts = self.forward_group(idx, [controls[i] for i in idx])
+            for i, fin, ck in zip(idx, finals, ckpts):
+                ns = fin[0].detach().requires_grad_(True)
+                Ts = fin[2].detach().requires_grad_(True)
+                L = loss_fn(i, ns, Ts)
+                gns, gTs = torch.autograd.grad(L, [ns, Ts], allow_unused=True)
+                P = self.problems[i]
+                g_n0, g_top = backward_from_checkpoints(P, ck, controls[i][1], gns, gTs)
+                out[i] = (float(L.detach()), g_n0, g_top)
+                P._scratch = None
+            del finals, ckpts
+        return out
+
+
 def _fn_class():
     import torch
 
@@ -316,33 +404,8 @@ def _fn_class():
 
         @staticmethod
         def backward(ctx, g_ns, g_Ts):
-            import torch
-
-            P = ctx.problem
             n0, Ttop = ctx.saved_tensors
-            zeros = lambda t: torch.zeros_like(t)
-            ns_f = P.base[0:LSP]
-            cot = [g_ns if g_ns is not None else zeros(ns_f), zeros(ns_f),
-                   g_Ts if g_Ts is not None else zeros(ns_f), zeros(P.lo0), zeros(P.hi0)]
-            g_top = torch.zeros_like(Ttop) if Ttop is not None else None
-            starts = sorted(ctx.ckpt)
-            for seg_i in range(len(starts) - 1, -1, -1):
-                j0 = starts[seg_i]
-                j1 = starts[seg_i + 1] if seg_i + 1 < len(starts) else P.nsteps
-                # recompute the states of the segment from its checkpoint
-                P._load(*ctx.ckpt[j0], Ttop)
-                states = [ctx.ckpt[j0]]
-                for j in range(j0, j1 - 1):
-                    P.cuda_step(j)
-                    states.append(P._save())
-                for j in range(j1 - 1, j0 - 1, -1):
-                    cot, gt = P.step_vjp(states[j - j0], Ttop, j, cot, P.cuda_diffusion_adjoint)
-                    if gt is not None:
-                        g_top = g_top + gt
-            g = P.grid
-            I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
-            gns = cot[0][(slice(None),) + I]
-            g_n0 = gns[:LSP - 1] + gns[LSP - 1].unsqueeze(0)  # electrons = sum of ions
+            g_n0, g_top = backward_from_checkpoints(ctx.problem, ctx.ckpt, Ttop, g_ns, g_Ts)
             return g_n0, g_top, None
 
     return Fn

@@ -50,6 +50,16 @@ class Batch:
     def step(self, stream=None) -> None:
         _lib.check(_lib.lib().gem_batch_step(self.handle, _stream(stream)))
 
+    def step_fixed_dt(self, dts, stream=None) -> None:
+        """One step with prescribed per-instance time steps (dt_calc skipped)."""
+        import numpy as np
+
+        a = np.ascontiguousarray(np.asarray(dts, dtype=np.float64))
+        if a.shape != (len(self),):
+            raise ValueError(f"need {len(self)} time steps, got shape {a.shape}")
+        self._dt_host = a  # the copy is asynchronous: keep the host array alive
+        _lib.check(_lib.lib().gem_batch_step_fixed_dt(self.handle, a.ctypes.data_as(_lib._D), _stream(stream)))
+
     def dts(self):
         import numpy as np
 

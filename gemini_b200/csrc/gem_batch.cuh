@@ -36,6 +36,12 @@ __global__ void kb_zero_acc(const InstDev* inst, int ninst) {
   if (i < ninst && threadIdx.x < 3 * LSP) inst[i].acc[threadIdx.x] = 0ull;
 }
 
+// fixed time steps (differentiable path): instance i takes dt_in[i]
+__global__ void kb_set_dt(const InstDev* inst, const double* dt_in, int ninst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ninst) *inst[i].sw.dtp_w = dt_in[i];
+}
+
 // k_dt_finalize per instance
 __global__ void kb_dt_finalize(const InstDev* inst, int ninst) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -170,6 +176,9 @@ struct gem_batch {
   cudaStream_t cap_stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph_fixed = nullptr;  // the step with prescribed time steps
+  cudaGraphExec_t exec_fixed = nullptr;
+  double* d_dt_in = nullptr;  // per-instance prescribed dt (device)
   int use_graph = 1;
 };
 
@@ -321,17 +330,26 @@ int batch_build_lists(gem_batch* b) {
 void batch_drop_graph(gem_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->exec_fixed) cudaGraphExecDestroy(b->exec_fixed);
+  if (b->graph_fixed) cudaGraphDestroy(b->graph_fixed);
   b->exec = nullptr;
   b->graph = nullptr;
+  b->exec_fixed = nullptr;
+  b->graph_fixed = nullptr;
 }
 
-int batch_enqueue(gem_batch* b, cudaStream_t st) {
+// fixed_dt: the instances' dt slots are loaded from d_dt_in instead of dt_calc
+int batch_enqueue(gem_batch* b, cudaStream_t st, bool fixed_dt = false) {
   const InstDev* I = b->d_inst;
-  kb_zero_acc<<<b->n, 32, 0, st>>>(I, b->n);
-  bool finalized = false;
+  if (fixed_dt)
+    kb_set_dt<<<(b->n + 63) / 64, 64, 0, st>>>(I, b->d_dt_in, b->n);
+  else
+    kb_zero_acc<<<b->n, 32, 0, st>>>(I, b->n);
+  bool finalized = fixed_dt;
   for (const auto& L : b->launches) {
     const int n = (int)L.items.size();
     const bool u = L.unit != 0;
+    if (fixed_dt && L.kernel == BK_DT) continue;
     if (L.kernel != BK_DT && !finalized) {
       kb_dt_finalize<<<(b->n + 63) / 64, 64, 0, st>>>(I, b->n);
       finalized = true;
@@ -458,6 +476,7 @@ int gem_batch_destroy(gem_batch* b) {
   for (auto& L : b->launches)
     if (L.d_items) cudaFree(L.d_items);
   if (b->d_inst) cudaFree(b->d_inst);
+  if (b->d_dt_in) cudaFree(b->d_dt_in);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   delete b;
   return GEM_OK;
@@ -503,6 +522,32 @@ int gem_batch_step(gem_batch* b, void* stream) {
     GEM_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
   }
   GEM_CUDA(cudaGraphLaunch(b->exec, st));
+  return GEM_OK;
+}
+
+int gem_batch_step_fixed_dt(gem_batch* b, const double* host_dts, void* stream) {
+  if (!b || !host_dts) return set_err(GEM_EINVAL, "null argument");
+  cudaStream_t st = S(stream);
+  if (!b->d_dt_in && cudaMalloc(&b->d_dt_in, sizeof(double) * b->n) != cudaSuccess) {
+    b->d_dt_in = nullptr;
+    return set_err(GEM_ENOMEM, "cudaMalloc of the prescribed-dt buffer failed");
+  }
+  GEM_CUDA(cudaMemcpyAsync(b->d_dt_in, host_dts, sizeof(double) * b->n, cudaMemcpyHostToDevice, st));
+  if (!b->use_graph) return batch_enqueue(b, st, true);
+  if (!b->exec_fixed) {
+    GEM_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = batch_enqueue(b, b->cap_stream, true);
+    cudaGraph_t gph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->cap_stream, &gph);
+    if (rc) {
+      if (gph) cudaGraphDestroy(gph);
+      return rc;
+    }
+    if (e != cudaSuccess) return set_err(GEM_ECUDA, "stream capture of the batched step failed: %s", cudaGetErrorString(e));
+    b->graph_fixed = gph;
+    GEM_CUDA(cudaGraphInstantiate(&b->exec_fixed, b->graph_fixed, 0));
+  }
+  GEM_CUDA(cudaGraphLaunch(b->exec_fixed, st));
   return GEM_OK;
 }
 

@@ -182,6 +182,10 @@ int gem_batch_destroy(gem_batch* b);
 int gem_batch_size(const gem_batch* b);
 int gem_batch_set_param(gem_batch* b, int param, int value);
 int gem_batch_step(gem_batch* b, void* stream);
+/* The same step with prescribed time steps (host array of n values, copied to the device on
+ * `stream` before the step): dt_calc is skipped and instance i advances by host_dts[i].
+ * Used by the differentiable path, whose time steps follow a frozen schedule. */
+int gem_batch_step_fixed_dt(gem_batch* b, const double* host_dts, void* stream);
 /* per-instance dt of the last step (synchronous device->host copies) */
 int gem_batch_dts(const gem_batch* b, double* host_dt);
 /* launches per step and (instance, block) work items per step */
