@@ -44,6 +44,9 @@ class DiffProblem:
         self.cuda_diffusion_adjoint = bool(cuda_diffusion_adjoint)
         self.cuda_sweep_adjoint = bool(cuda_sweep_adjoint)
         self._dtt = {}
+        self._capturing = False
+        self._graphs = {}  # (Ttop given) -> captured step VJP
+        self.vjp_graph = True
         self.grid = grid
         self.nsteps = int(nsteps)
         self.k = max(1, int(checkpoint_every))
@@ -141,27 +144,26 @@ class DiffProblem:
         return out, ckpt
 
     # -- the energy diffusion with its hand-written CUDA adjoint ----------------------
-    def diffusion_forward(self, n, T, Ttop, j):
-        """gem_energy_diffusion_dev on (n, T): the diffusion output (max(T,100) applied)."""
+    def diffusion_forward(self, n, T, Ttop, dt):
+        """gem_energy_diffusion_dev on (n, T): the diffusion output (max(T,100) applied);
+        dt is a 1-element device tensor."""
         import torch
 
         fv = torch.zeros(self.shape, dtype=torch.float64, device=n.device)
         fv[0:LSP] = n
         fv[4 * LSP:] = T
         self._set_top(Ttop)
-        dt = torch.full((1,), self.dts[j], dtype=torch.float64, device=n.device)
         c = self.cfg.c()
         _lib.check(_lib.lib().gem_energy_diffusion_dev(ctypes.byref(c), self.dg.handle, F._ptr(fv),
                                                        F._ptr(self.ds.electrovars), self.ds.work, F._ptr(dt),
                                                        F._stream()))
         return fv[4 * LSP:].clone()
 
-    def diffusion_vjp(self, n, T, Ttop, j, Ybar):
+    def diffusion_vjp(self, n, T, Ttop, dt, Ybar):
         import torch
 
         g = self.grid
         self._set_top(Ttop)
-        dt = torch.full((1,), self.dts[j], dtype=torch.float64, device=n.device)
         n = n.contiguous()
         T = T.contiguous()
         Yb = Ybar.contiguous()
@@ -193,6 +195,8 @@ class DiffProblem:
         return nb, Tb, tb.sum(0)
 
     def _set_top(self, Ttop):
+        if self._capturing:  # set before the capture / replay (a synchronous copy)
+            return
         if Ttop is None:
             _lib.check(_lib.lib().gem_work_set_top_temperature(self.ds.work, None, 0))
         else:
@@ -206,29 +210,82 @@ class DiffProblem:
 
         inp = [t.detach().requires_grad_(True) for t in state]
         tt = None if Ttop is None else Ttop.detach().requires_grad_(True)
+        if (self.vjp_graph and use_cuda_diffusion_adjoint and self.cuda_sweep_adjoint
+                and all(c is not None for c in cot)):
+            try:
+                return self._step_vjp_graphed(state, Ttop, j, cot)
+            except RuntimeError as e:  # capture unavailable: stay eager
+                self.vjp_graph = False
+                self.vjp_graph_error = str(e)
+                self._capturing = False
+        return self._vjp_body(inp, tt, self.dt_tensor(j), cot, use_cuda_diffusion_adjoint)
+
+    def _vjp_body(self, inp, tt, dt, cot, use_cuda_diffusion_adjoint=True):
+        """The step VJP on given tensors (inp require grad); dt: 1-element device tensor."""
+        import torch
+
         diff = None
         sweep = None
+        P = self
         if use_cuda_diffusion_adjoint:
-            P = self
-
             def diff(n, T, Ttop_):
-                return _diffusion_fn().apply(n, T, Ttop_, P, j)
+                return _diffusion_fn().apply(n, T, Ttop_, P, dt)
 
         if self.cuda_sweep_adjoint:
-            P = self
-
             def sweep(f, v, dim, frank, nsp):
-                return _sweep_fn().apply(f, v, P, dim, frank, nsp, j)
+                return _sweep_fn().apply(f, v, P, dim, frank, nsp, dt)
         with torch.enable_grad():
             out = TS.step(self.tg, inp[0], inp[1], self.vs2, self.vs3, inp[2], inp[3], inp[4], self.nn,
-                          self.Tn, self.J1, self.dts[j], self.Teinf, tt, self.diffsolvetype, diffusion=diff,
+                          self.Tn, self.J1, dt, self.Teinf, tt, self.diffsolvetype, diffusion=diff,
                           sweep_impl=sweep)
             pairs = [(o, c) for o, c in zip(out, cot) if c is not None]
-            wrt = inp + ([tt] if tt is not None else [])
+            wrt = list(inp) + ([tt] if tt is not None else [])
             grads = torch.autograd.grad([o for o, _ in pairs], wrt, [c for _, c in pairs], allow_unused=True)
         g_state = [torch.zeros_like(t) if g is None else g for g, t in zip(grads[:5], inp)]
         g_top = None if tt is None else (torch.zeros_like(tt) if grads[5] is None else grads[5])
         return g_state, g_top
+
+    def _step_vjp_graphed(self, state, Ttop, j, cot):
+        """The step VJP replayed from a CUDA graph captured once per problem (static input
+        buffers: state, cotangent, dt, top temperature)."""
+        import torch
+
+        key = Ttop is not None
+        G = self._graphs.get(key)
+        if G is None:
+            G = {"state": [t.detach().clone() for t in state], "cot": [c.detach().clone() for c in cot],
+                 "dt": self.dt_tensor(j).clone(), "top": Ttop.detach().clone() if key else None}
+            self._set_top(Ttop)
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                for _ in range(2):  # warm-up outside the capture
+                    inp = [t.detach().requires_grad_(True) for t in G["state"]]
+                    tt = G["top"].detach().requires_grad_(True) if key else None
+                    self._vjp_body(inp, tt, G["dt"], G["cot"])
+            torch.cuda.current_stream().wait_stream(side)
+            graph = torch.cuda.CUDAGraph()
+            self._capturing = True
+            try:
+                with torch.cuda.graph(graph, capture_error_mode="relaxed"):
+                    inp = [t.detach().requires_grad_(True) for t in G["state"]]
+                    tt = G["top"].detach().requires_grad_(True) if key else None
+                    G["out"] = self._vjp_body(inp, tt, G["dt"], G["cot"])
+            finally:
+                self._capturing = False
+            G["graph"] = graph
+            self._graphs[key] = G
+        for buf, t in zip(G["state"], state):
+            buf.copy_(t)
+        for buf, c in zip(G["cot"], cot):
+            buf.copy_(c)
+        G["dt"].fill_(self.dts[j])
+        if key:
+            G["top"].copy_(Ttop)
+            self._set_top(Ttop)
+        G["graph"].replay()
+        g_state, g_top = G["out"]
+        return [t.clone() for t in g_state], (g_top.clone() if g_top is not None else None)
 
 
 _DIFF_FN = None
@@ -243,14 +300,13 @@ def _sweep_fn():
 
         class SweepFn(torch.autograd.Function):
             @staticmethod
-            def forward(ctx, f, v, problem, dim, frank, nsp, j):
+            def forward(ctx, f, v, problem, dim, frank, nsp, dt):
                 f = f.contiguous()
                 v = v.contiguous()
                 out = f.clone()
-                dt = problem.dt_tensor(j)
                 _lib.check(_lib.lib().gem_sweep_field_dev(problem.dg.handle, dim, frank, nsp, F._ptr(out), F._ptr(v),
                                                           F._ptr(dt), F._stream()))
-                ctx.problem, ctx.dim, ctx.frank, ctx.nsp, ctx.j = problem, dim, frank, nsp, j
+                ctx.problem, ctx.dim, ctx.frank, ctx.nsp, ctx.dt = problem, dim, frank, nsp, dt
                 ctx.save_for_backward(f, v)
                 return out
 
@@ -261,7 +317,7 @@ def _sweep_fn():
                 obar = obar.contiguous()
                 fbar = obar.clone()
                 vbar = torch.zeros_like(v) if ctx.needs_input_grad[1] else None
-                dt = P.dt_tensor(ctx.j)
+                dt = ctx.dt
                 _lib.check(_lib.lib().gem_sweep_field_vjp_dev(
                     P.dg.handle, ctx.dim, ctx.frank, ctx.nsp, F._ptr(f), F._ptr(v), F._ptr(dt), F._ptr(obar),
                     F._ptr(fbar), None if vbar is None else F._ptr(vbar), F._stream()))
@@ -279,15 +335,15 @@ def _diffusion_fn():
 
         class DiffusionFn(torch.autograd.Function):
             @staticmethod
-            def forward(ctx, n, T, Ttop, problem, j):
-                ctx.problem, ctx.j = problem, j
+            def forward(ctx, n, T, Ttop, problem, dt):
+                ctx.problem, ctx.dt = problem, dt
                 ctx.save_for_backward(n, T, Ttop)
-                return problem.diffusion_forward(n, T, Ttop, j)
+                return problem.diffusion_forward(n, T, Ttop, dt)
 
             @staticmethod
             def backward(ctx, Ybar):
                 n, T, Ttop = ctx.saved_tensors
-                nb, Tb, tb = ctx.problem.diffusion_vjp(n, T, Ttop, ctx.j, Ybar)
+                nb, Tb, tb = ctx.problem.diffusion_vjp(n, T, Ttop, ctx.dt, Ybar)
                 return nb, Tb, (tb if Ttop is not None else None), None, None
 
         _DIFF_FN = DiffusionFn
@@ -386,6 +442,7 @@ class BatchedAdjoint:
                 g_n0, g_top = backward_from_checkpoints(P, ck, controls[i][1], gns, gTs)
                 out[i] = (float(L.detach()), g_n0, g_top)
                 P._scratch = None
+                P._graphs = {}  # release the captured VJP's memory pool
             del finals, ckpts
         return out
 

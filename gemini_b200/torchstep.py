@@ -28,10 +28,20 @@ TCOEF = np.array([0.1019e-12, 0.0747e-12, 0.0754e-12, 0.0701e-12, 0.1068e-12, 0.
                  dtype=np.float32).astype(np.float64)
 
 
-def _t(a, like):
+_CONST = {}
+
+
+def _const(name, arr, device, shape):
+    """Species constants as device tensors, created once per device (so that a captured
+    CUDA graph of the step contains no host-to-device copy)."""
     import torch
 
-    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=like.device)
+    key = (name, str(device))
+    t = _CONST.get(key)
+    if t is None:
+        t = torch.as_tensor(np.asarray(arr, dtype=np.float64), device=device).reshape(shape)
+        _CONST[key] = t
+    return t
 
 
 @dataclass
@@ -207,9 +217,9 @@ def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf,
 
     lx1, lx2, lx3 = G.lx1, G.lx2, G.lx3
     dev = ns.device
-    ms = torch.as_tensor(MS, device=dev).reshape(7, 1, 1, 1)
-    qs = torch.as_tensor(QS, device=dev).reshape(7, 1, 1, 1)
-    gam = torch.as_tensor(GAMMAS, device=dev).reshape(7, 1, 1, 1)
+    ms = _const("ms", MS, dev, (7, 1, 1, 1))
+    qs = _const("qs", QS, dev, (7, 1, 1, 1))
+    gam = _const("gam", GAMMAS, dev, (7, 1, 1, 1))
     h1, h2, h3 = G.h
     # v12rhov1, T2rhoe (multifluid.f90:193-214)
     rv = ns * ms * vs1
@@ -345,7 +355,7 @@ def energy_diffusion(G: TGrid, n, T, J1, nn, Tn, dt, Teinf, Ttop=None, diffsolve
     h1, h2, h3 = (h[2:lx3 + 2, 2:lx2 + 2, 2:lx1 + 2] for h in G.h)
     Tc = T[:, 2:lx3 + 2, 2:lx2 + 2, 2:lx1 + 2]
     nc = n[:, 2:lx3 + 2, 2:lx2 + 2, 2:lx1 + 2]
-    tco = torch.as_tensor(TCOEF, device=T.device).reshape(6, 1, 1, 1)
+    tco = _const("tcoef", TCOEF, T.device, (6, 1, 1, 1))
     lam_i = tco * pow25(Tc[:6])
     te = Tc[6]
     X = nn[0] * 1.1e-16 * (1 + 5.7e-4 * te) + nn[1] * 2.82e-17 * torch.sqrt(te) * (1 - 1.21e-4 * te) + \
@@ -354,7 +364,7 @@ def energy_diffusion(G: TGrid, n, T, J1, nn, Tn, dt, Teinf, Ttop=None, diffsolve
     lam = torch.cat([lam_i, lam_e.unsqueeze(0)], 0)
     beta = torch.zeros_like(lam)
     beta = torch.cat([beta[:6], (5.0 / 2 * KB / ELCHRG * J1[2:lx3 + 2, 2:lx2 + 2, 2:lx1 + 2]).unsqueeze(0)], 0)
-    gam = torch.as_tensor(GAMMAS, device=T.device).reshape(7, 1, 1, 1)
+    gam = _const("gam", GAMMAS, T.device, (7, 1, 1, 1))
     C = (gam - 1.0) / KB / torch.clamp(nc, min=MINDENSDIV) / (h1 * h2 * h3)
     B = C * beta / h1
     D = lam * h2 * h3 / h1
