@@ -336,8 +336,8 @@ def run_b200(args, world, rank, local):
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         ems = float(te.item())
         ng = (w["lx1"] + 4) * (w["lx2"] + 4) * (w["lx3"] + 4)
-        h2d = ng * 8 * (5 * LSP + 2 * LSP + 9 + 7)
-        d2h = ng * 8 * (5 * LSP + 2 * LSP + 9) + 8
+        h2d = ng * 8 * (5 * LSP + 1)        # fluidvars + J1
+        d2h = ng * 8 * (5 * LSP + 2 * LSP) + 8  # fluidvars + rhovs1|rhoes + dt
         e2e = {"value": world * cells * LSP * args.e2e_steps / (ems / 1e3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "api": "gem_fluid_adv_host (host blocks, pinned)", "steps": args.e2e_steps,

@@ -939,9 +939,11 @@ int gem_fluid_adv_host(const gem_cfg* cfg, const gem_grid* g, double* fluidvars,
     w->nE = nE;
   }
   cudaStream_t st = S(stream);
+  // Only what the step reads goes in: fluidvars and J1 (electrovars field 4).  rhovs1 and
+  // rhoes are recomputed from ns, vs1, Ts over every cell (v12rhov1/T2rhoe), the 9 MHD
+  // scalars and the other electrovars fields are not touched.
   GEM_CUDA(cudaMemcpyAsync(w->F, fluidvars, nF * sizeof(double), cudaMemcpyHostToDevice, st));
-  GEM_CUDA(cudaMemcpyAsync(w->A, fluidauxvars, nA * sizeof(double), cudaMemcpyHostToDevice, st));
-  GEM_CUDA(cudaMemcpyAsync(w->E, electrovars, nE * sizeof(double), cudaMemcpyHostToDevice, st));
+  GEM_CUDA(cudaMemcpyAsync(w->E + 3 * ng, electrovars + 3 * ng, ng * sizeof(double), cudaMemcpyHostToDevice, st));
   int rc;
   if (*dt_inout < 0) {
     if ((rc = gem_dt_calc_dev(g, cfg->tcfl, w->F, w, w->dt, stream))) return rc;
@@ -949,8 +951,9 @@ int gem_fluid_adv_host(const gem_cfg* cfg, const gem_grid* g, double* fluidvars,
     GEM_CUDA(cudaMemcpyAsync(w->dt, dt_inout, sizeof(double), cudaMemcpyHostToDevice, st));
   }
   if ((rc = gem_fluid_adv_dev(cfg, g, w->F, w->A, w->E, w, w->dt, stream))) return rc;
+  // ... and only what it writes comes out: fluidvars and rhovs1|rhoes
   GEM_CUDA(cudaMemcpyAsync(fluidvars, w->F, nF * sizeof(double), cudaMemcpyDeviceToHost, st));
-  GEM_CUDA(cudaMemcpyAsync(fluidauxvars, w->A, nA * sizeof(double), cudaMemcpyDeviceToHost, st));
+  GEM_CUDA(cudaMemcpyAsync(fluidauxvars, w->A, ng * 2 * LSP * sizeof(double), cudaMemcpyDeviceToHost, st));
   GEM_CUDA(cudaMemcpyAsync(dt_inout, w->dt, sizeof(double), cudaMemcpyDeviceToHost, st));
   GEM_CUDA(cudaStreamSynchronize(st));
   return GEM_OK;

@@ -203,10 +203,13 @@ int gem_batch_info(const gem_batch* b, int* launches_per_step, long long* items_
 int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
                       const double* electrovars, gem_work* w, const double* dt, void* stream);
 
-/* The same step through host buffers: copies the three blocks to the device, runs
- * gem_dt_calc_dev (if dt_inout < 0, else uses *dt_inout) and gem_fluid_adv_dev, copies the
- * blocks back and synchronises.  Device staging buffers are allocated on first use and
- * kept in the work object. */
+/* The same step through host buffers: copies what the step reads to the device (fluidvars
+ * and the J1 field of electrovars), runs gem_dt_calc_dev (if dt_inout < 0, else uses
+ * *dt_inout) and gem_fluid_adv_dev, copies back what it writes (fluidvars and the rhovs1 |
+ * rhoes fields of fluidauxvars) and synchronises.  The host blocks end exactly as a full
+ * round trip would leave them: rhovs1 and rhoes are recomputed from fluidvars over every
+ * cell, and the 9 MHD scalars and the other electrovars fields are not touched.  Device
+ * staging buffers are allocated on first use and kept in the work object. */
 int gem_fluid_adv_host(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
                        const double* electrovars, gem_work* w, double* dt_inout, void* stream);
 

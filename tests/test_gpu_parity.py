@@ -192,8 +192,17 @@ def test_host_entry_point_matches_device():
     F.fluid_adv(cfg, a, dt)
     b = F.DeviceState.from_host(dg, st.copy())
     h = st.copy()
+    # the step recomputes rhovs1|rhoes, ignores all electrovars but J1 and leaves the MHD
+    # scalars alone: garbage there must not matter, and the MHD scalars must survive
+    rng = np.random.default_rng(0)
+    h.fluidauxvars[...] = rng.uniform(-1e3, 1e3, h.fluidauxvars.shape)
+    mhd = h.fluidauxvars[..., 2 * 7:].copy()
+    keep_J1 = h.electrovars[..., 3].copy()
+    h.electrovars[...] = rng.uniform(-1, 1, h.electrovars.shape)
+    h.electrovars[..., 3] = keep_J1
     dth = F.fluid_adv_host(cfg, dg, b, h.fluidvars, h.fluidauxvars, h.electrovars, -1.0)
     assert dth == float(dt.item())
     ga = a.to_host(st)
     assert np.array_equal(ga.fluidvars, h.fluidvars)
-    assert np.array_equal(ga.fluidauxvars, h.fluidauxvars)
+    assert np.array_equal(ga.fluidauxvars[..., :2 * 7], h.fluidauxvars[..., :2 * 7])
+    assert np.array_equal(h.fluidauxvars[..., 2 * 7:], mhd)
