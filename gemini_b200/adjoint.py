@@ -170,14 +170,11 @@ class DiffProblem:
         Tb = torch.zeros_like(T)
         nb = torch.zeros_like(n)
         tb = torch.zeros((LSP, g.lx3, g.lx2), dtype=torch.float64, device=n.device)
-        need = int(_lib.lib().gem_diffusion_vjp_scratch_doubles(self.dg.handle))
-        if getattr(self, "_scratch", None) is None or self._scratch.numel() < need:
-            self._scratch = torch.empty(need, dtype=torch.float64, device=n.device)
         c = self.cfg.c()
         _lib.check(_lib.lib().gem_diffusion_vjp_dev(ctypes.byref(c), self.dg.handle, F._ptr(T), F._ptr(n),
                                                     F._ptr(self.ds.electrovars), self.ds.work, F._ptr(dt),
                                                     F._ptr(Yb), F._ptr(Tb), F._ptr(nb), F._ptr(tb),
-                                                    F._ptr(self._scratch), F._stream()))
+                                                    F._stream()))
         # ghost cells: out = max(T, 100) except the x1 boundary layers, which hold the
         # Dirichlet values max(tmin, 100) / max(tmax, 100)
         ghost = torch.ones_like(T[0], dtype=torch.bool)
@@ -441,7 +438,6 @@ class BatchedAdjoint:
                 P = self.problems[i]
                 g_n0, g_top = backward_from_checkpoints(P, ck, controls[i][1], gns, gTs)
                 out[i] = (float(L.detach()), g_n0, g_top)
-                P._scratch = None
                 P._graphs = {}  # release the captured VJP's memory pool
             del finals, ckpts
         return out

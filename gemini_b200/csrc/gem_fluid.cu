@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -716,42 +717,47 @@ int gem_sweep_field_vjp_dev(const gem_grid* g, int dim, int frank, int nsp, cons
   a.frank = (dim == 1) ? 0 : frank;
   a.nsp = nsp;
   const Dims& d = g->dev.d;
+  // tiles of 32 lines x a segment of at most SVJ_TJ cells (ghosts along the line included)
+  const int lx = (dim == 1) ? d.lx1 : (dim == 2) ? d.lx2 : d.lx3;
   const long long nl = (dim == 1) ? (long long)d.lx2 * d.lx3 : (dim == 2) ? (long long)d.lx1 * d.lx3
-                                                                          : (long long)d.lx1 * d.lx2;
-  const unsigned nb = grid_for(nl * nsp, 128, 16);
+                                                                         : (long long)d.lx1 * d.lx2;
+  SweepVjpTiles T;
+  T.nseg = (lx + 4 + SVJ_TJ - 1) / SVJ_TJ;
+  T.TJ = (lx + 4 + T.nseg - 1) / T.nseg;
+  const long long npan = (nl + 31) / 32;
+  const long long nwork = npan * T.nseg * nsp;
+  if (nwork > INT_MAX) return set_err(GEM_EINVAL, "grid too large for the sweep adjoint");
+  T.npan = (int)npan;
+  T.nwork = (int)nwork;
+  const unsigned nb = (unsigned)std::min<long long>(nwork, (long long)num_sms() * 8);
   cudaStream_t st = S(stream);
   const bool u = g->dev.unit != 0;
   if (dim == 1) {
-    if (u) k_sweep_vjp<1, true><<<nb, 128, 0, st>>>(a); else k_sweep_vjp<1, false><<<nb, 128, 0, st>>>(a);
+    if (u) k_sweep_vjp<1, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<1, false><<<nb, 256, 0, st>>>(a, T);
   } else if (dim == 2) {
-    if (u) k_sweep_vjp<2, true><<<nb, 128, 0, st>>>(a); else k_sweep_vjp<2, false><<<nb, 128, 0, st>>>(a);
+    if (u) k_sweep_vjp<2, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<2, false><<<nb, 256, 0, st>>>(a, T);
   } else {
-    if (u) k_sweep_vjp<3, true><<<nb, 128, 0, st>>>(a); else k_sweep_vjp<3, false><<<nb, 128, 0, st>>>(a);
+    if (u) k_sweep_vjp<3, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<3, false><<<nb, 256, 0, st>>>(a, T);
   }
   GEM_LAUNCHED("k_sweep_vjp");
   return GEM_OK;
 }
 
 // Vector-Jacobian product of the energy diffusion (differentiable path).
-long long gem_diffusion_vjp_scratch_doubles(const gem_grid* g) {
-  if (!g) return -1;
-  const Dims& d = g->dev.d;
-  return (long long)DADJ_N * d.lx1 * d.lx2 * d.lx3 * LSP;
-}
-
 int gem_diffusion_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const double* Ts, const double* ns,
                           const double* electrovars, const gem_work* w, const double* dt, const double* Ybar,
-                          double* Tbar, double* nbar, double* Ttop_bar, double* scratch, void* stream) {
-  if (!cfg || check_grid(g) || !Ts || !ns || !electrovars || !w || !dt || !Ybar || !Tbar || !nbar || !scratch)
+                          double* Tbar, double* nbar, double* Ttop_bar, void* stream) {
+  if (!cfg || check_grid(g) || !Ts || !ns || !electrovars || !w || !dt || !Ybar || !Tbar || !nbar)
     return set_err(GEM_EINVAL, "null argument");
   if (cfg->diffsolvetype != 1 && cfg->diffsolvetype != 2)
     return set_err(GEM_EINVAL, "Unsupported diffusion solver type/mode: %d. Should be either 1 or 2.", cfg->diffsolvetype);
-  if (g->dev.d.lx1 < 4) return set_err(GEM_EINVAL, "lx1=%d: the diffusion needs lx1 >= 4", g->dev.d.lx1);
+  const Dims& d = g->dev.d;
+  if (d.lx1 < 4) return set_err(GEM_EINVAL, "lx1=%d: the diffusion needs lx1 >= 4", d.lx1);
   DiffAdjArgs a;
   a.G = g->dev;
   a.T = Ts;
   a.ns = ns;
-  a.J1 = electrovars + 3 * g->dev.d.ng;
+  a.J1 = electrovars + 3 * d.ng;
   a.nn = w->nn;
   a.Tn = w->Tn;
   a.Ttop = w->Ttop;
@@ -762,13 +768,31 @@ int gem_diffusion_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const double* T
   a.Tbar = Tbar;
   a.nbar = nbar;
   a.Ttop_bar = Ttop_bar;
-  a.scratch = scratch;
-  const long long ncs = (long long)g->dev.d.lx2 * g->dev.d.lx3 * LSP;
+  // one warp per (column, species); VNA per-row arrays of M rows per lane in shared memory
+  const int M = std::max(2, (d.lx1 + 31) / 32);
+  a.M = M;
+  const size_t per_warp = (size_t)VNA * M * 32 * sizeof(double);
+  const int wpb = (int)std::min<size_t>(4, (227 * 1024) / per_warp);
+  if (wpb < 1) return set_err(GEM_EINVAL, "lx1=%d too long for the on-chip column adjoint", d.lx1);
+  const size_t smem = per_warp * wpb;
+  const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
+  long long nblk = (ncs + wpb - 1) / wpb;
+  int per_sm = 0;
   cudaStream_t st = S(stream);
+  if (g->dev.unit) {
+    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_vjp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion_vjp<true>, 32 * wpb, smem));
+  } else {
+    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_vjp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion_vjp<false>, 32 * wpb, smem));
+  }
+  if (per_sm < 1) per_sm = 1;
+  const long long cap = (long long)num_sms() * per_sm;
+  if (nblk > cap) nblk = cap;
   if (g->dev.unit)
-    k_diffusion_vjp<true><<<grid_for(ncs, 128, 16), 128, 0, st>>>(a);
+    k_diffusion_vjp<true><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
   else
-    k_diffusion_vjp<false><<<grid_for(ncs, 128, 16), 128, 0, st>>>(a);
+    k_diffusion_vjp<false><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
   GEM_LAUNCHED("k_diffusion_vjp");
   return GEM_OK;
 }

@@ -1186,6 +1186,10 @@ struct WarpMem {
   double* b;   // warp base + lane
   __device__ __forceinline__ double& at(int arr, int k) const { return b[(k * DNA + arr) * 32]; }
   __device__ __forceinline__ double& at_lane(int arr, int k, int l) const { return wb[(k * DNA + arr) * 32 + l]; }
+  // the factorisation arrays of the band solver
+  __device__ __forceinline__ double& ss(int k) const { return at(DA_SS, k); }
+  __device__ __forceinline__ double& ib(int k) const { return at(DA_IB, k); }
+  __device__ __forceinline__ double& tt(int k) const { return at(DA_TT, k); }
 };
 
 // 1/b to about one ulp for the solver's pivots and elimination multipliers (not for the
@@ -1240,23 +1244,23 @@ struct IfaceLU {
   double iloB, ihiB;  // reciprocal pivots of the lo row and of the reduced hi row
 };
 
-template <class RowM>
-__device__ __forceinline__ void band_factor(const WarpMem& W, int M, int lane, RowM rowm, IfaceLU& F) {
+template <class WM, class RowM>
+__device__ __forceinline__ void band_factor(const WM& W, int M, int lane, RowM rowm, IfaceLU& F) {
   double a, b, c;
   rowm(1, a, b, c);
   double s_prev = a, c_prev = c, bp = b, ib_prev = rcp_nr(b);
-  W.at(DA_SS, 1) = s_prev;
-  W.at(DA_IB, 1) = ib_prev;
-  W.at(DA_TT, 1) = c;
+  W.ss(1) = s_prev;
+  W.ib(1) = ib_prev;
+  W.tt(1) = c;
   for (int k = 2; k < M; ++k) {
     rowm(k, a, b, c);
     const double f = a * ib_prev;
     const double sk = -f * s_prev;
     const double bk = b - f * c_prev;
     const double ibk = rcp_nr(bk);
-    W.at(DA_SS, k) = sk;
-    W.at(DA_IB, k) = ibk;
-    W.at(DA_TT, k) = c;
+    W.ss(k) = sk;
+    W.ib(k) = ibk;
+    W.tt(k) = c;
     s_prev = sk;
     c_prev = c;
     bp = bk;
@@ -1265,16 +1269,16 @@ __device__ __forceinline__ void band_factor(const WarpMem& W, int M, int lane, R
   const double hiA = s_prev, hiC = c_prev;
   double hiB = bp;
   for (int k = M - 3; k >= 1; --k) {
-    const double g = W.at(DA_TT, k) * W.at(DA_IB, k + 1);
-    W.at(DA_SS, k) = W.at(DA_SS, k) - g * W.at(DA_SS, k + 1);
-    W.at(DA_TT, k) = -g * W.at(DA_TT, k + 1);
+    const double g = W.tt(k) * W.ib(k + 1);
+    W.ss(k) = W.ss(k) - g * W.ss(k + 1);
+    W.tt(k) = -g * W.tt(k + 1);
   }
   rowm(0, a, b, c);
   if (M >= 3) {
-    F.g0 = c * W.at(DA_IB, 1);
+    F.g0 = c * W.ib(1);
     F.loA = a;
-    F.loB = b - F.g0 * W.at(DA_SS, 1);
-    F.loC = -F.g0 * W.at(DA_TT, 1);
+    F.loB = b - F.g0 * W.ss(1);
+    F.loC = -F.g0 * W.tt(1);
   } else {
     F.g0 = 0.0;
     F.loA = a;
@@ -1325,21 +1329,21 @@ __device__ __forceinline__ void band_factor(const WarpMem& W, int M, int lane, R
 }
 
 // Solve for the right-hand side in array ARR (in place: the solution replaces it).
-template <class RowM>
-__device__ __forceinline__ void band_solve(const WarpMem& W, int M, int lane, RowM rowm, const IfaceLU& F,
+template <class WM, class RowM>
+__device__ __forceinline__ void band_solve(const WM& W, int M, int lane, RowM rowm, const IfaceLU& F,
                                            int ARR) {
   double a, b, c;
   double rp = W.at(ARR, 1);
   for (int k = 2; k < M; ++k) {
     rowm(k, a, b, c);
-    rp = W.at(ARR, k) - a * W.at(DA_IB, k - 1) * rp;
+    rp = W.at(ARR, k) - a * W.ib(k - 1) * rp;
     W.at(ARR, k) = rp;
   }
   const double hiR = rp;
   double rn = (M >= 3) ? W.at(ARR, M - 2) : 0.0;
   for (int k = M - 3; k >= 1; --k) {
     rowm(k, a, b, c);
-    rn = W.at(ARR, k) - c * W.at(DA_IB, k + 1) * rn;
+    rn = W.at(ARR, k) - c * W.ib(k + 1) * rn;
     W.at(ARR, k) = rn;
   }
   const double loR = (M >= 3) ? W.at(ARR, 0) - F.g0 * W.at(ARR, 1) : W.at(ARR, 0);
@@ -1361,7 +1365,7 @@ __device__ __forceinline__ void band_solve(const WarpMem& W, int M, int lane, Ro
   const double x0 = (loR - F.loA * xlp - F.loC * xl) * F.iloB;
   for (int k = 1; k <= M - 2; ++k)
     W.at(ARR, k) =
-        (W.at(ARR, k) - W.at(DA_SS, k) * x0 - W.at(DA_TT, k) * xl) * W.at(DA_IB, k);
+        (W.at(ARR, k) - W.ss(k) * x0 - W.tt(k) * xl) * W.ib(k);
   W.at(ARR, 0) = x0;
   W.at(ARR, M - 1) = xl;
 }
@@ -1689,14 +1693,16 @@ __global__ void k_diffusion_ghost_floor(GridDev G, Blocks B) {
 
 // ======================================================================================
 // 7b. Adjoint (vector-Jacobian product) of the energy diffusion, for the differentiable
-//     path.  One thread per (x1 column, species) -- species slowest, so neighbouring threads
-//     hold neighbouring columns -- with per-row work arrays in global scratch laid out
-//     [array][row][thread] (coalesced).  The thread recomputes the forward coefficients and
-//     both stage solutions (Thomas), then runs the transposed solves and chains the
-//     cotangents of the band entries and right-hand sides through q+-, Dh, C, B and the
-//     conductivity lambda(T, n) back to T, n and the exospheric boundary temperature.
-//     Cotangent inputs/outputs are ghosted 7-species blocks; only interior rows are
-//     written (the caller zero-initialises Tbar and nbar).
+//     path.  One warp per (x1 column, species), lanes owning blocks of M consecutive rows,
+//     as in the forward solver: the kernel recomputes the per-row conduction factors
+//     q-, q+, bq (with the partial derivatives of lambda(T, n) and C(n)), both TRBDF2
+//     stage solutions X and Y, then solves the transposed stage systems with the same
+//     lane-blocked band solver and chains the cotangents of the band entries and
+//     right-hand sides back through q+-, Dh, C, B and lambda to T, n and the column's
+//     exospheric boundary value.  Every per-row array lives in shared memory; T, n, Ybar,
+//     Tbar and nbar move along x1 (coalesced).  Cotangent inputs/outputs are ghosted
+//     7-species blocks; only interior rows are written (the caller zero-initialises Tbar
+//     and nbar).
 // ======================================================================================
 struct DiffAdjArgs {
   GridDev G;
@@ -1709,92 +1715,149 @@ struct DiffAdjArgs {
   double Teinf;
   const double* dtp;
   int solver;
+  int M;               // rows per lane
   const double* Ybar;  // cotangent of the diffusion output (after max(T,100))
   double* Tbar;
   double* nbar;
   double* Ttop_bar;    // optional: (lx2*lx3) per species, species slowest
-  double* scratch;     // DADJ_N * lx1 * (lx2*lx3*7) doubles
 };
-constexpr int DJ_QM = 0, DJ_QP = 1, DJ_BQ = 2, DJ_X = 3, DJ_Y = 4, DJ_CP = 5, DJ_DP = 6, DJ_L2 = 7, DJ_G = 8,
-              DJ_QMB = 9, DJ_QPB = 10, DJ_BQB = 11, DJ_TB = 12;
-constexpr int DADJ_N = 13;
+
+// per-row shared-memory arrays of the adjoint (row-interleaved as WarpMem).  Slots are
+// reused once their first content is dead: D becomes the stage-1 solution X, Y becomes the
+// temperature cotangent TB, R carries Ybar -> lambda2 -> xbar -> lambda1, and after the
+// last pass QMB / QPB / BQB hold EM / EP / the density cotangent.
+constexpr int VA_T = 0, VA_C = 1, VA_DDT = 2, VA_DDN = 3, VA_DCN = 4, VA_BQ = 5, VA_QM = 6, VA_QP = 7,
+              VA_X = 8, VA_SS = 9, VA_IB = 10, VA_TT = 11, VA_Y = 12, VA_R = 13, VA_QMB = 14, VA_QPB = 15,
+              VA_BQB = 16;
+constexpr int VNA = 17;
+constexpr int VA_D = VA_X, VA_TB = VA_Y;
+
+struct WarpMemA {
+  double* wb;
+  double* b;
+  __device__ __forceinline__ double& at(int arr, int k) const { return b[(k * VNA + arr) * 32]; }
+  __device__ __forceinline__ double& at_lane(int arr, int k, int l) const { return wb[(k * VNA + arr) * 32 + l]; }
+  __device__ __forceinline__ double& ss(int k) const { return at(VA_SS, k); }
+  __device__ __forceinline__ double& ib(int k) const { return at(VA_IB, k); }
+  __device__ __forceinline__ double& tt(int k) const { return at(VA_TT, k); }
+};
 
 template <bool UNIT>
 __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
+  extern __shared__ double smem[];
   const GridDev& G = P.G;
   const Dims d = G.d;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  const int M = P.M;
+  const WarpMemA W{smem + warp * VNA * M * 32, smem + warp * VNA * M * 32 + lane};
   const int n = d.lx1;
+  const double dt = *P.dtp;
   const long long ncol = (long long)d.lx2 * d.lx3;
   const long long ncs = ncol * LSP;
-  const double dt = *P.dtp;
+  const long long nc = nci(d);
   const Line1D& L1 = G.L[0];
-  for (long long cs = blockIdx.x * (long long)blockDim.x + threadIdx.x; cs < ncs;
-       cs += (long long)gridDim.x * blockDim.x) {
-    const int s = (int)(cs / ncol);
-    const long long col = cs - (long long)s * ncol;
-    const int i2 = (int)(col % d.lx2) + 1, i3 = (int)(col / d.lx2) + 1;
+  const bool trbdf = P.solver == 2;
+  const double dA = trbdf ? 1 / (dt / 2) : 1 / dt;  // first-stage diagonal term
+  const double d2 = 1 / (dt / 3);                   // BDF2 diagonal term
+  // coalesced passes: row idx = 32c + lane lives in the slot (lane idx/M, row idx%M)
+  const int lp0 = lane / M, kp0 = lane - lp0 * M, q32 = 32 / M, r32 = 32 - q32 * M;
+  for (long long cs = (long long)blockIdx.x * wpb + warp; cs < ncs; cs += (long long)gridDim.x * wpb) {
+    const int s = (int)(cs % LSP);
+    const int col = (int)(cs / LSP);
+    const int i2 = col % d.lx2 + 1, i3 = col / d.lx2 + 1;
     const long long m0 = gi(d, 0, i2, i3);
     const long long mm0 = cmi(G, 0, i2, i3);
     const long long q0 = ci(d, 1, i2, i3) - 1;
-    const long long nc = nci(d);
     const double* Tc = P.T + (long long)s * d.ng + m0;
     const double* nsc = P.ns + (long long)s * d.ng + m0;
-    auto S = [&](int arr, int i) -> double& { return P.scratch[((long long)arr * n + (i - 1)) * ncs + cs]; };
     const double c0 = (c_gammas[s] - 1.0) / KB;
-    // conductivity and its partial derivatives at row i
-    auto lam_d = [&](int i, double& lam, double& dl_dT, double& dl_dn) {
-      const double T = Tc[i];
-      const double T25 = pow25(T);
-      if (s < LSP - 1) {
-        lam = c_tcoef[s] * T25;
-        dl_dT = 2.5 * lam / T;
-        dl_dn = 0.0;
-      } else {
-        const long long q = q0 + i;
-        const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
-        const double sq = sqrt(T);
-        const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
-                         n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
-        const double Xp = n1 * 1.1e-16 * 5.7e-4 + n2 * 2.82e-17 * (0.5 / sq * (1 - 1.21e-4 * T) - 1.21e-4 * sq) +
-                          n3 * 2.2e-16 * 3.6e-2 * 0.5 / sq;
-        const double ne = nsc[i];
-        const double den = 1 + 3.22e4 * (T * T) / ne * X;
-        lam = ELCHRG * 100 * 7.7e5 * T25 / den;
-        const double dden_dT = 3.22e4 * (2 * T * X + T * T * Xp) / ne;
-        dl_dT = lam * (2.5 / T - dden_dT / den);
-        dl_dn = lam * (3.22e4 * T * T * X / (ne * ne)) / den;
+    // ---- pass 1 (along x1): T, D = lambda h2 h3 / h1 with dD/dT, dD/dn, C with dC/dn, bq
+    {
+      int lp = lp0, kp = kp0;
+      for (int c = 0; c < M; ++c) {
+        const int i = 1 + 32 * c + lane;
+        double T = 0, D = 0, C = 0, ddt = 0, ddn = 0, dcn = 0, bq = 0;
+        if (i <= n) {
+          T = Tc[i];
+          const double nv = nsc[i];
+          const long long mk = mm0 + i;
+          const double h1v = UNIT ? 1.0 : __ldg(G.h1 + mk);
+          const double h23 = UNIT ? 1.0 : __ldg(G.h2 + mk) * __ldg(G.h3 + mk);
+          const double ha1 = UNIT ? 1.0 : __ldg(G.ha1_0 + mk);
+          const double T25 = pow25(T);
+          double lam, dl_dT, dl_dn = 0.0;
+          if (s < LSP - 1) {
+            lam = c_tcoef[s] * T25;
+            dl_dT = 2.5 * lam / T;
+          } else {
+            const long long q = q0 + i;
+            const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
+            const double sq = sqrt(T);
+            const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
+                             n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
+            const double Xp = n1 * 1.1e-16 * 5.7e-4 + n2 * 2.82e-17 * (0.5 / sq * (1 - 1.21e-4 * T) - 1.21e-4 * sq) +
+                              n3 * 2.2e-16 * 3.6e-2 * 0.5 / sq;
+            const double den = 1 + 3.22e4 * (T * T) / nv * X;
+            lam = ELCHRG * 100 * 7.7e5 * T25 / den;
+            const double dden_dT = 3.22e4 * (2 * T * X + T * T * Xp) / nv;
+            dl_dT = lam * (2.5 / T - dden_dT / den);
+            dl_dn = lam * (3.22e4 * T * T * X / (nv * nv)) / den;
+          }
+          const double g = h23 / h1v;
+          D = lam * g;
+          ddt = dl_dT * g;
+          ddn = dl_dn * g;
+          C = c0 / fmax_f(nv, MINDENSDIV) / ha1;
+          dcn = (nv > MINDENSDIV) ? -C / nv : 0.0;
+          if (s == LSP - 1 && i >= 2 && i <= n - 1) {
+            const double beta = 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i];  // collisions.f90:197
+            bq = C * beta / h1v / (__ldg(L1.dx + i + 1) + __ldg(L1.dx + i));
+          }
+        }
+        W.at_lane(VA_T, kp, lp) = T;
+        W.at_lane(VA_D, kp, lp) = D;
+        W.at_lane(VA_C, kp, lp) = C;
+        W.at_lane(VA_DDT, kp, lp) = ddt;
+        W.at_lane(VA_DDN, kp, lp) = ddn;
+        W.at_lane(VA_DCN, kp, lp) = dcn;
+        W.at_lane(VA_BQ, kp, lp) = bq;
+        kp += r32;
+        lp += q32;
+        if (kp >= M) {
+          kp -= M;
+          ++lp;
+        }
       }
-    };
-    auto coefC = [&](int i, double& C, double& dC_dn) {
-      const double nv = nsc[i];
-      const double ha1 = UNIT ? 1.0 : __ldg(G.ha1_0 + mm0 + i);
-      C = c0 / fmax_f(nv, MINDENSDIV) / ha1;
-      dC_dn = (nv > MINDENSDIV) ? -C / nv : 0.0;
-    };
-    auto h1_ = [&](int i) { return UNIT ? 1.0 : __ldg(G.h1 + mm0 + i); };
-    auto h23 = [&](int i) { return UNIT ? 1.0 : __ldg(G.h2 + mm0 + i) * __ldg(G.h3 + mm0 + i); };
-    auto beta_ = [&](int i) { return (s < LSP - 1) ? 0.0 : 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i]; };
-    auto Dv = [&](int i) {
-      double lam, a, b;
-      lam_d(i, lam, a, b);
-      return lam * h23(i) / h1_(i);
-    };
-    auto Cv = [&](int i) {
-      double C, dc;
-      coefC(i, C, dc);
-      return C;
-    };
-    // ---- forward: q-, q+, bq for rows 2..n-1
-    for (int i = 2; i <= n - 1; ++i) {
-      const double Dm = Dv(i - 1), Dc = Dv(i), Dp = Dv(i + 1);
-      const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);
-      const double C = Cv(i);
-      const double B = C * beta_(i) / h1_(i);
-      const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
-      S(DJ_QM, i) = C * Dhm / dxi / dxm;
-      S(DJ_QP, i) = C * Dhp / dxi / dxp;
-      S(DJ_BQ, i) = B / (dxp + dxm);
     }
+    __syncwarp();
+    // value of array arr at the row delta (-1, 0, +1) away from slot k, across lanes; 0 past
+    // the ends of the lane blocks
+    auto nb = [&](int arr, int k, int delta) -> double {
+      int kk = k + delta, ll = lane;
+      if (kk < 0) { kk = M - 1; --ll; }
+      if (kk >= M) { kk = 0; ++ll; }
+      return (ll < 0 || ll > 31) ? 0.0 : W.at_lane(arr, kk, ll);
+    };
+    // ---- q-, q+ per slot (rows 2..n-1): Dh(i) = (D(i-1) + D(i))/2
+    {
+      for (int k = 0; k < M; ++k) {
+        const int i = 1 + lane * M + k;
+        double qm = 0.0, qp = 0.0;
+        if (i >= 2 && i <= n - 1) {
+          const double Dm = nb(VA_D, k, -1), Dc = W.at(VA_D, k), Dp = nb(VA_D, k, 1);
+          const double C = W.at(VA_C, k);
+          const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
+          qm = C * (0.5 * (Dm + Dc)) / dxi / dxm;
+          qp = C * (0.5 * (Dc + Dp)) / dxi / dxp;
+        }
+        W.at(VA_QM, k) = qm;
+        W.at(VA_QP, k) = qp;
+      }
+    }
+    __syncwarp();
+    // Dirichlet values (diffusion.f90:54-79)
     double tmin, tmax;
     {
       const double tn1 = __ldg(P.Tn + ci(d, 1, i2, i3)), tnl = __ldg(P.Tn + ci(d, n, i2, i3));
@@ -1803,195 +1866,240 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
       else if (G.gridflag == 1) { tmin = tinf; tmax = tnl; }
       else { tmin = tn1; tmax = tinf; }
     }
-    const bool trbdf = P.solver == 2;
-    const double dA = trbdf ? 1 / (dt / 2) : 1 / dt;  // first-stage diagonal term
-    const double hA = trbdf ? 0.5 : 1.0;              // first-stage scale of the q's
-    // first-stage rows (TR half step, or the backward-Euler step)
-    auto rowA = [&](int i, double& a, double& b, double& c) {
-      if (i == 1 || i == n) { a = 0; b = 1; c = 0; return; }
-      const double qm = S(DJ_QM, i), qp = S(DJ_QP, i), bq = S(DJ_BQ, i);
-      if (trbdf) {
+    // stage matrix rows: stage 0 = the first stage (TR half step, or backward Euler), 1 = BDF2;
+    // the row in slot kk of lane ll; rows 1, n, the padding past n and rows outside the
+    // warp are identity rows
+    auto row_at = [&](int stage, int kk, int ll, double& a, double& b, double& c) {
+      const int i = 1 + ll * M + kk;
+      if (ll < 0 || ll > 31 || i == 1 || i >= n) { a = 0; b = 1; c = 0; return; }
+      const double qm = W.at_lane(VA_QM, kk, ll), qp = W.at_lane(VA_QP, kk, ll), bq = W.at_lane(VA_BQ, kk, ll);
+      if (stage == 0 && trbdf) {
         a = -(qm / 2) + bq / 2;
         b = dA + qp / 2 + qm / 2;
         c = -(qp / 2) - bq / 2;
       } else {
         a = -qm + bq;
-        b = dA + qp + qm;
+        b = ((stage == 0) ? dA : d2) + qp + qm;
         c = -qp - bq;
       }
     };
-    auto rowB = [&](int i, double& a, double& b, double& c) {  // BDF2 rows
-      if (i == 1 || i == n) { a = 0; b = 1; c = 0; return; }
-      const double qm = S(DJ_QM, i), qp = S(DJ_QP, i), bq = S(DJ_BQ, i);
-      a = -qm + bq;
-      b = 1 / (dt / 3) + qp + qm;
-      c = -qp - bq;
+    auto row0 = [&](int k, double& a, double& b, double& c) { row_at(0, k, lane, a, b, c); };
+    auto row1 = [&](int k, double& a, double& b, double& c) { row_at(1, k, lane, a, b, c); };
+    // the transposed matrix: sub-diagonal c(i-1), diagonal b(i), super-diagonal a(i+1)
+    auto rowT = [&](int stage, int k, double& a, double& b, double& c) {
+      double x, y, z;
+      row_at(stage, k, lane, x, b, z);
+      int kk = k - 1, ll = lane;
+      if (kk < 0) { kk = M - 1; --ll; }
+      row_at(stage, kk, ll, x, y, z);
+      a = z;
+      kk = k + 1;
+      ll = lane;
+      if (kk >= M) { kk = 0; ++ll; }
+      row_at(stage, kk, ll, x, y, z);
+      c = x;
     };
-    // Thomas solve of rows rowf with right-hand side in array R, solution into array OUT
-    auto thomas = [&](auto rowf, int R, int OUT) {
-      double cp = 0.0, dp = 0.0;
-      for (int i = 1; i <= n; ++i) {
-        double a, b, c;
-        rowf(i, a, b, c);
-        const double den = b - a * cp;
-        cp = c / den;
-        dp = (S(R, i) - a * dp) / den;
-        S(DJ_CP, i) = cp;
-        S(DJ_DP, i) = dp;
-      }
-      double x = 0.0;
-      for (int i = n; i >= 1; --i) {
-        x = S(DJ_DP, i) - S(DJ_CP, i) * x;
-        S(OUT, i) = x;
-      }
-    };
-    // transposed solve: A^T has sub-diagonal c(i-1), diagonal b(i), super-diagonal a(i+1)
-    auto thomasT = [&](auto rowf, int R, int OUT) {
-      double cp = 0.0, dp = 0.0;
-      double a_i, b_i, c_i, a_n, b_n, c_n, c_prev = 0.0;
-      rowf(1, a_i, b_i, c_i);
-      for (int i = 1; i <= n; ++i) {
-        double sup = 0.0;
-        if (i < n) {
-          rowf(i + 1, a_n, b_n, c_n);
-          sup = a_n;
-        }
-        const double sub = (i > 1) ? c_prev : 0.0;
-        const double den = b_i - sub * cp;
-        cp = sup / den;
-        dp = (S(R, i) - sub * dp) / den;
-        S(DJ_CP, i) = cp;
-        S(DJ_DP, i) = dp;
-        c_prev = c_i;
-        if (i < n) { a_i = a_n; b_i = b_n; c_i = c_n; }
-      }
-      double x = 0.0;
-      for (int i = n; i >= 1; --i) {
-        x = S(DJ_DP, i) - S(DJ_CP, i) * x;
-        S(OUT, i) = x;
-      }
-    };
-    // first-stage right-hand side into DJ_G
-    for (int i = 1; i <= n; ++i) {
-      double r;
-      if (i == 1) r = tmin;
-      else if (i == n) r = tmax;
-      else if (trbdf) {
-        double a, b, c;
-        rowA(i, a, b, c);
-        const double qm = S(DJ_QM, i), qp = S(DJ_QP, i);
-        const double Pd = qp / 2 + qm / 2;
-        r = Tc[i] / (dt / 2) - a * Tc[i - 1] - Pd * Tc[i] - c * Tc[i + 1];
-      } else {
-        r = Tc[i] / dt;
-      }
-      S(DJ_G, i) = r;
-    }
-    thomas(rowA, DJ_G, DJ_X);
-    if (trbdf) {
-      for (int i = 1; i <= n; ++i) {
+    auto row0T = [&](int k, double& a, double& b, double& c) { rowT(0, k, a, b, c); };
+    auto row1T = [&](int k, double& a, double& b, double& c) { rowT(1, k, a, b, c); };
+    IfaceLU F;
+    // ---- forward replay: first stage into X (the slot of D, now dead)
+    {
+      for (int k = 0; k < M; ++k) {
+        const int i = 1 + lane * M + k;
         double r;
         if (i == 1) r = tmin;
         else if (i == n) r = tmax;
-        else r = -(1 / 3.0 * Tc[i] / (dt / 3)) + 4 / 3.0 * S(DJ_X, i) / (dt / 3);
-        S(DJ_G, i) = r;
+        else if (i > n) r = 0.0;
+        else if (trbdf) {
+          double a, b, c;
+          row0(k, a, b, c);
+          const double qm = W.at(VA_QM, k), qp = W.at(VA_QP, k);
+          const double Tv = W.at(VA_T, k);
+          r = Tv / (dt / 2) - a * nb(VA_T, k, -1) - (qp / 2 + qm / 2) * Tv - c * nb(VA_T, k, 1);
+        } else {
+          r = W.at(VA_T, k) / dt;
+        }
+        W.at(VA_X, k) = r;
       }
-      thomas(rowB, DJ_G, DJ_Y);
     }
-    const int YOUT = trbdf ? DJ_Y : DJ_X;
-    // ---- adjoint
-    const double* Yb = P.Ybar + (long long)s * d.ng + m0;
-    for (int i = 1; i <= n; ++i) {
-      S(DJ_G, i) = (S(YOUT, i) >= 100.0) ? Yb[i] : 0.0;  // max(T,100)
-      S(DJ_QMB, i) = 0.0;
-      S(DJ_QPB, i) = 0.0;
-      S(DJ_BQB, i) = 0.0;
-      S(DJ_TB, i) = 0.0;
-    }
-    double tminb = 0.0, tmaxb = 0.0;
-    int LA = DJ_L2;  // adjoint of the first stage, in DJ_L2 after the loop below
+    band_factor(W, M, lane, row0, F);
+    band_solve(W, M, lane, row0, F, VA_X);
+    __syncwarp();
+    int YOUT = VA_X;
     if (trbdf) {
-      thomasT(rowB, DJ_G, DJ_L2);  // lambda2 = A2^-T ybar
-      tminb += S(DJ_L2, 1);
-      tmaxb += S(DJ_L2, n);
-      for (int i = 2; i <= n - 1; ++i) {
-        const double l2 = S(DJ_L2, i);
-        const double ab = -l2 * S(DJ_Y, i - 1), bb = -l2 * S(DJ_Y, i), cb = -l2 * S(DJ_Y, i + 1);
-        S(DJ_QMB, i) += -ab + bb;
-        S(DJ_QPB, i) += bb - cb;
-        S(DJ_BQB, i) += ab - cb;
-        S(DJ_TB, i) += l2 * (-(1 / 3.0) / (dt / 3));
-        S(DJ_G, i) = l2 * ((4 / 3.0) / (dt / 3));  // xbar
+      for (int k = 0; k < M; ++k) {
+        const int i = 1 + lane * M + k;
+        double r;
+        if (i == 1) r = tmin;
+        else if (i == n) r = tmax;
+        else if (i > n) r = 0.0;
+        else r = -(1 / 3.0 * W.at(VA_T, k) / (dt / 3)) + 4 / 3.0 * W.at(VA_X, k) / (dt / 3);
+        W.at(VA_Y, k) = r;
       }
-      S(DJ_G, 1) = 0.0;
-      S(DJ_G, n) = 0.0;
+      band_factor(W, M, lane, row1, F);
+      band_solve(W, M, lane, row1, F, VA_Y);
+      YOUT = VA_Y;
     }
-    thomasT(rowA, DJ_G, LA);  // lambda1 = A1^-T xbar (or A^-T ybar for backward Euler)
-    tminb += S(LA, 1);
-    tmaxb += S(LA, n);
-    for (int i = 2; i <= n - 1; ++i) {
-      const double l1 = S(LA, i);
-      double a, b, c;
-      rowA(i, a, b, c);
-      const double xm = S(DJ_X, i - 1), xc = S(DJ_X, i), xp = S(DJ_X, i + 1);
+    __syncwarp();
+    // ---- Ybar along x1 into R, masked by max(T,100) of the output
+    const double* Yb = P.Ybar + (long long)s * d.ng + m0;
+    {
+      int lp = lp0, kp = kp0;
+      for (int c = 0; c < M; ++c) {
+        const int i = 1 + 32 * c + lane;
+        W.at_lane(VA_R, kp, lp) = (i <= n) ? Yb[i] : 0.0;
+        kp += r32;
+        lp += q32;
+        if (kp >= M) {
+          kp -= M;
+          ++lp;
+        }
+      }
+    }
+    __syncwarp();
+    for (int k = 0; k < M; ++k)
+      if (!(W.at(YOUT, k) >= 100.0)) W.at(VA_R, k) = 0.0;
+    double tminb = 0.0, tmaxb = 0.0;  // on the lanes that own rows 1 and n
+    const int lane_n = (n - 1) / M, k_n = (n - 1) - lane_n * M;
+    if (trbdf) {
+      // lambda2 = A2^-T g; then the BDF2 cotangents of q-, q+, bq and T, and xbar
+      band_factor(W, M, lane, row1T, F);
+      band_solve(W, M, lane, row1T, F, VA_R);
+      __syncwarp();
+      if (lane == 0) tminb += W.at(VA_R, 0);
+      if (lane == lane_n) tmaxb += W.at(VA_R, k_n);
+      // Y(k-1) is read after slot k-1 of Y became TB: keep a sliding window
+      double ym = nb(VA_Y, 0, -1), yc = W.at(VA_Y, 0);
+      const double ynext = nb(VA_Y, M - 1, 1);
+      __syncwarp();
+      for (int k = 0; k < M; ++k) {
+        const int i = 1 + lane * M + k;
+        const double yp = (k < M - 1) ? W.at(VA_Y, k + 1) : ynext;
+        double qmb = 0.0, qpb = 0.0, bqb = 0.0, tb = 0.0, xb = 0.0;
+        if (i >= 2 && i <= n - 1) {
+          const double l2 = W.at(VA_R, k);
+          const double ab = -l2 * ym, bb = -l2 * yc, cb = -l2 * yp;
+          qmb = -ab + bb;
+          qpb = bb - cb;
+          bqb = ab - cb;
+          tb = l2 * (-(1 / 3.0) / (dt / 3));
+          xb = l2 * ((4 / 3.0) / (dt / 3));
+        }
+        W.at(VA_QMB, k) = qmb;
+        W.at(VA_QPB, k) = qpb;
+        W.at(VA_BQB, k) = bqb;
+        W.at(VA_TB, k) = tb;  // the slot of Y (read above)
+        W.at(VA_R, k) = xb;
+        ym = yc;
+        yc = yp;
+      }
+    } else {
+      for (int k = 0; k < M; ++k) {
+        W.at(VA_QMB, k) = 0.0;
+        W.at(VA_QPB, k) = 0.0;
+        W.at(VA_BQB, k) = 0.0;
+        W.at(VA_TB, k) = 0.0;
+      }
+    }
+    __syncwarp();
+    // lambda1 = A1^-T xbar (or A^-T g for backward Euler)
+    band_factor(W, M, lane, row0T, F);
+    band_solve(W, M, lane, row0T, F, VA_R);
+    __syncwarp();
+    if (lane == 0) tminb += W.at(VA_R, 0);
+    if (lane == lane_n) tmaxb += W.at(VA_R, k_n);
+    // first-stage cotangents, then EM / EP (the Dh cotangent parts) and the C part of nbar
+    for (int k = 0; k < M; ++k) {
+      const int i = 1 + lane * M + k;
+      if (i > n) continue;
+      double tb = W.at(VA_TB, k);
+      // T(i) in the right-hand sides of rows i-1 and i+1 (TR only)
       if (trbdf) {
-        const double qm = S(DJ_QM, i), qp = S(DJ_QP, i);
-        const double Pd = qp / 2 + qm / 2;
-        const double ab = -l1 * (xm + Tc[i - 1]), cb = -l1 * (xp + Tc[i + 1]), bb = -l1 * xc, pb = -l1 * Tc[i];
-        S(DJ_QMB, i) += -ab / 2 + bb / 2 + pb / 2;
-        S(DJ_QPB, i) += -cb / 2 + bb / 2 + pb / 2;
-        S(DJ_BQB, i) += ab / 2 - cb / 2;
-        S(DJ_TB, i) += l1 * (dA - Pd);
-        S(DJ_TB, i - 1) += -l1 * a;
-        S(DJ_TB, i + 1) += -l1 * c;
-      } else {
-        const double ab = -l1 * xm, cb = -l1 * xp, bb = -l1 * xc;
-        S(DJ_QMB, i) += -ab + bb;
-        S(DJ_QPB, i) += bb - cb;
-        S(DJ_BQB, i) += ab - cb;
-        S(DJ_TB, i) += l1 * dA;
+        if (i + 1 >= 2 && i + 1 <= n - 1) {
+          double a, b, c;
+          int kk = k + 1, ll = lane;
+          if (kk >= M) { kk = 0; ++ll; }
+          row_at(0, kk, ll, a, b, c);
+          tb += -nb(VA_R, k, 1) * a;
+        }
+        if (i - 1 >= 2 && i - 1 <= n - 1) {
+          double a, b, c;
+          int kk = k - 1, ll = lane;
+          if (kk < 0) { kk = M - 1; --ll; }
+          row_at(0, kk, ll, a, b, c);
+          tb += -nb(VA_R, k, -1) * c;
+        }
       }
-    }
-    (void)hA;
-    // ---- chain through q-, q+, bq -> C, Dh -> D -> lambda(T, n)
-    double* Tbo = P.Tbar + (long long)s * d.ng + m0;
-    double* nbo = P.nbar + (long long)s * d.ng + m0;
-    for (int i = 1; i <= n; ++i) {
-      double C, dC_dn;
-      coefC(i, C, dC_dn);
-      double Cb = 0.0, Dhb_i = 0.0, Dhb_ip1 = 0.0;
+      double em = 0.0, ep = 0.0, nbc = 0.0;
       if (i >= 2 && i <= n - 1) {
+        const double l1 = W.at(VA_R, k);
+        const double qm = W.at(VA_QM, k), qp = W.at(VA_QP, k), bq = W.at(VA_BQ, k);
+        const double xm = nb(VA_X, k, -1), xc = W.at(VA_X, k), xp = nb(VA_X, k, 1);
+        double qmb = W.at(VA_QMB, k), qpb = W.at(VA_QPB, k), bqb = W.at(VA_BQB, k);
+        if (trbdf) {
+          const double Tm = nb(VA_T, k, -1), Tv = W.at(VA_T, k), Tp = nb(VA_T, k, 1);
+          const double ab = -l1 * (xm + Tm), cb = -l1 * (xp + Tp), bb = -l1 * xc, pb = -l1 * Tv;
+          qmb += -ab / 2 + bb / 2 + pb / 2;
+          qpb += -cb / 2 + bb / 2 + pb / 2;
+          bqb += ab / 2 - cb / 2;
+          tb += l1 * (dA - (qp / 2 + qm / 2));
+        } else {
+          const double ab = -l1 * xm, cb = -l1 * xp, bb = -l1 * xc;
+          qmb += -ab + bb;
+          qpb += bb - cb;
+          bqb += ab - cb;
+          tb += l1 * dA;
+        }
+        // q- = C Dh(i) / (dxi dx(i)), q+ = C Dh(i+1) / (dxi dx(i+1)), bq = C beta/h1/(dx(i)+dx(i+1))
+        const double C = W.at(VA_C, k);
         const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
-        const double Dm = Dv(i - 1), Dc = Dv(i), Dp = Dv(i + 1);
-        const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);
-        const double qmb = S(DJ_QMB, i), qpb = S(DJ_QPB, i);
-        Cb += qmb * Dhm / (dxi * dxm) + qpb * Dhp / (dxi * dxp);
-        Dhb_i += qmb * C / (dxi * dxm);
-        Dhb_ip1 += qpb * C / (dxi * dxp);
-        const double Bb = S(DJ_BQB, i) / (dxp + dxm);
-        Cb += Bb * beta_(i) / h1_(i);
+        em = qmb * C / (dxi * dxm);  // -> Dh(i)
+        ep = qpb * C / (dxi * dxp);  // -> Dh(i+1)
+        const double Cb = (qmb * qm + qpb * qp + bqb * bq) / C;
+        nbc = Cb * W.at(VA_DCN, k);
       }
-      // Dh(i) also collects q+ of row i-1; Dh(i+1) the q- of row i+1
-      if (i - 1 >= 2 && i - 1 <= n - 1) {
-        const double dxi = __ldg(L1.dxi + i - 2), dxp = __ldg(L1.dx + i);
-        Dhb_i += S(DJ_QPB, i - 1) * Cv(i - 1) / (dxi * dxp);
+      W.at(VA_TB, k) = tb;
+      W.at(VA_QMB, k) = em;
+      W.at(VA_QPB, k) = ep;
+      W.at(VA_BQB, k) = nbc;
+    }
+    __syncwarp();
+    // D(i) feeds Dh(i) (i >= 2) and Dh(i+1) (i < n); Dh(j) collects EM(j) and EP(j-1)
+    for (int k = 0; k < M; ++k) {
+      const int i = 1 + lane * M + k;
+      if (i > n) continue;
+      const double dh_i = (i >= 2) ? W.at(VA_QMB, k) + nb(VA_QPB, k, -1) : 0.0;
+      const double dh_ip1 = (i < n) ? nb(VA_QMB, k, 1) + W.at(VA_QPB, k) : 0.0;
+      const double Db = 0.5 * (dh_i + dh_ip1);
+      W.at(VA_R, k) = W.at(VA_TB, k) + Db * W.at(VA_DDT, k);   // Tbar
+      W.at(VA_C, k) = W.at(VA_BQB, k) + Db * W.at(VA_DDN, k);  // nbar
+    }
+    __syncwarp();
+    // ---- Tbar, nbar along x1
+    {
+      double* Tbo = P.Tbar + (long long)s * d.ng + m0;
+      double* nbo = P.nbar + (long long)s * d.ng + m0;
+      int lp = lp0, kp = kp0;
+      for (int c = 0; c < M; ++c) {
+        const int i = 1 + 32 * c + lane;
+        if (i <= n) {
+          Tbo[i] = W.at_lane(VA_R, kp, lp);
+          nbo[i] = W.at_lane(VA_C, kp, lp);
+        }
+        kp += r32;
+        lp += q32;
+        if (kp >= M) {
+          kp -= M;
+          ++lp;
+        }
       }
-      if (i + 1 >= 2 && i + 1 <= n - 1) {
-        const double dxi = __ldg(L1.dxi + i), dxm = __ldg(L1.dx + i + 1);
-        Dhb_ip1 += S(DJ_QMB, i + 1) * Cv(i + 1) / (dxi * dxm);
-      }
-      // Dh(j) = 0.5*(D(j-1) + D(j)) for j = 2..n: D(i) feeds Dh(i) (i >= 2) and Dh(i+1) (i < n)
-      const double Db = 0.5 * ((i >= 2 ? Dhb_i : 0.0) + (i < n ? Dhb_ip1 : 0.0));
-      double lam, dl_dT, dl_dn;
-      lam_d(i, lam, dl_dT, dl_dn);
-      const double lamb = Db * h23(i) / h1_(i);
-      Tbo[i] = S(DJ_TB, i) + lamb * dl_dT;
-      nbo[i] = Cb * dC_dn + lamb * dl_dn;
     }
     if (P.Ttop_bar) {
-      const double tb = (G.gridflag == 1) ? tminb : (G.gridflag == 2) ? tmaxb : 0.0;
-      P.Ttop_bar[cs] = tb;
+      double tb = (G.gridflag == 1) ? tminb : (G.gridflag == 2) ? tmaxb : 0.0;
+      for (int o = 16; o > 0; o >>= 1) tb += __shfl_xor_sync(0xffffffffu, tb, o);
+      if (lane == 0) P.Ttop_bar[(long long)s * ncol + col] = tb;
     }
+    __syncwarp();
   }
 }
 
@@ -1999,11 +2107,15 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
 // 7c. Adjoint (vector-Jacobian product) of one field sweep (advec.f90:384-435 along x1, x2
 //     or x3, species 0..nsp-1), for the differentiable path.  With the limiter and upwind
 //     branches of the forward sweep replayed, the line update is linear in f, and its
-//     transpose is a local stencil: each face's flux cotangent goes to the one or two cells
-//     its phi reads and, through the selected slope (zero, centred, or twice the left or
-//     right difference), to two more cells.  One thread per (line, species), i1 fastest for
-//     the x2/x3 lines.  fbar enters holding the output cotangent (the identity part) and
-//     receives the flux parts; vbar (optional) gets the face-velocity cotangent.
+//     transpose is a local stencil: the cotangent of face i's flux reaches the upwind cell
+//     directly and, through the selected slope (zero, centred, or twice the left or right
+//     difference), the cells around it -- cells i-2 .. i+1 in all.  A block stages a tile
+//     of 32 lines by one segment of each line (with 3 halo cells per side) in shared memory
+//     and computes each slope branch once, each face's cotangent parts once, then lets
+//     every cell gather from its four faces j-1 .. j+2: no two threads write the same cell,
+//     and global memory moves along i1 in every direction.  fbar enters holding the output
+//     cotangent (the identity part) and receives the flux parts; vbar (optional) gets the
+//     face-velocity cotangent.
 // ======================================================================================
 struct SweepVjpArgs {
   GridDev G;
@@ -2022,105 +2134,187 @@ __device__ __forceinline__ int minmod_branch(double a, double b) {
   return (fabs(a) < fabs(b)) ? 1 : 2;
 }
 
+// Tiles: 32 lines (consecutive in the flattened line index, i1 fastest for the x2/x3 lines)
+// times a segment of up to SVJ_TJ cells along the line, staged with 3 halo cells per side.
+constexpr int SVJ_TJ = 28;
+constexpr int SVJ_R = SVJ_TJ + 6;  // staged rows: cells j0-3 .. j0+TJ+2
+constexpr int SVJ_LD = 33;         // padded row (32 lines)
+
+struct SweepVjpTiles {
+  int TJ, nseg, npan, nwork;
+};
+
 template <int DIM, bool UNIT>
-__global__ void __launch_bounds__(128) k_sweep_vjp(SweepVjpArgs P) {
+__global__ void __launch_bounds__(256) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles T) {
+  __shared__ double sf[SVJ_R][SVJ_LD];    // f at cell j0-3+row
+  __shared__ double skob[SVJ_R][SVJ_LD];  // kappa*obar at that cell (0 outside 1..lx)
+  __shared__ double ssl[SVJ_R][SVJ_LD];   // slope at that cell
+  __shared__ double sdir[SVJ_R][SVJ_LD];  // face i = j0-3+row: v*phib (to its upwind cell)
+  __shared__ double sw[SVJ_R][SVJ_LD];    // face: weight of its slope cotangent
+  __shared__ unsigned char scode[SVJ_R][SVJ_LD];  // slope branch at the cell
+  __shared__ unsigned char sflag[SVJ_R][SVJ_LD];  // face: branch of its slope | 4 (v<0) | 8 (face exists)
+  __shared__ long long sbase[32];                 // cell index of position 0 of each line
+  __shared__ int sa[32], sb_[32];
   const GridDev& G = P.G;
   const Dims d = G.d;
-  const double dt = *P.dtp;
   const int lx = (DIM == 1) ? d.lx1 : (DIM == 2) ? d.lx2 : d.lx3;
+  if (lx <= 1) return;  // single-cell lines pass through
+  const double dt = *P.dtp;
   const int na = (DIM == 1) ? d.lx2 : d.lx1;  // fastest line coordinate
-  const int nb = (DIM == 3) ? d.lx2 : d.lx3;
-  const long long nlines = (long long)na * nb;
-  const long long nthr = nlines * P.nsp;
+  const int nl = na * ((DIM == 3) ? d.lx2 : d.lx3);
   const Line1D& L = G.L[DIM - 1];
   const FaceTab& FT = G.F[DIM - 1];
-  if (lx <= 1) return;  // single-cell lines pass through
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nthr;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int s = (int)(t / nlines);
-    const long long ln = t - (long long)s * nlines;
-    const int a = (int)(ln % na) + 1, b = (int)(ln / na) + 1;
-    long long base, stride, nfaces;
-    if (DIM == 1) { base = gi(d, 0, a, b) - 1; stride = 1; nfaces = nf1(d); }
-    else if (DIM == 2) { base = gi(d, a, 0, b) - d.s2; stride = d.s2; nfaces = nf2(d); }
-    else { base = gi(d, a, b, 0) - d.s3; stride = d.s3; nfaces = nf3(d); }
+  const long long nfaces = (DIM == 1) ? nf1(d) : (DIM == 2) ? nf2(d) : nf3(d);
+  const long long stride = (DIM == 1) ? 1 : (DIM == 2) ? d.s2 : d.s3;
+  const int TJ = T.TJ;
+  const int tid = threadIdx.x;
+  // element e of a 32 x SVJ_R sweep: line-fastest for x2/x3 (i1 coalesced), position-fastest
+  // for x1 (x1 contiguous)
+  auto elem = [&](int e, int& row, int& ln) {
+    if (DIM == 1) { ln = e / SVJ_R; row = e - ln * SVJ_R; }
+    else { ln = e & 31; row = e >> 5; }
+  };
+  auto cmk = [&](int ln, int k) -> long long {
+    const int a = sa[ln], b = sb_[ln];
+    return (DIM == 1) ? cmi(G, k, a, b) : (DIM == 2) ? cmi(G, a, k, b) : cmi(G, a, b, k);
+  };
+  auto fmk = [&](int ln, int k) -> long long {
+    const int a = sa[ln], b = sb_[ln];
+    return (DIM == 1) ? fmi(FT, k, a, b) : (DIM == 2) ? fmi(FT, a, k, b) : fmi(FT, a, b, k);
+  };
+  auto face = [&](int s, int ln, int k) -> long long {
+    const int a = sa[ln], b = sb_[ln];
+    const long long q = (DIM == 1) ? f1i(d, k, a, b) : (DIM == 2) ? f2i(d, a, k, b) : f3i(d, a, b, k);
+    return (long long)s * nfaces + q;
+  };
+  for (int w = blockIdx.x; w < T.nwork; w += gridDim.x) {
+    const int pn = w % T.npan;
+    const int r = w / T.npan;
+    const int g = r % T.nseg, s = r / T.nseg;
+    const int q0 = pn * 32;
+    const int j0 = -1 + g * TJ;  // first cell of the segment
+    const int jend = min(j0 + TJ - 1, lx + 2);
     const long long so = (long long)s * d.ng;
-    auto cell = [&](int j) -> long long { return so + base + (long long)(j + 1) * stride; };
-    auto face = [&](int j) -> long long {
-      const long long k = (DIM == 1) ? f1i(d, j, a, b) : (DIM == 2) ? f2i(d, a, j, b) : f3i(d, a, b, j);
-      return (long long)s * nfaces + k;
-    };
-    auto fmk = [&](int j) -> long long {
-      return (DIM == 1) ? fmi(FT, j, a, b) : (DIM == 2) ? fmi(FT, a, j, b) : fmi(FT, a, b, j);
-    };
-    auto cmk = [&](int j) -> long long {
-      return (DIM == 1) ? cmi(G, j, a, b) : (DIM == 2) ? cmi(G, a, j, b) : cmi(G, a, b, j);
-    };
-    auto F = [&](int j) { return P.f[cell(j)]; };
-    auto kappa = [&](int c) {  // d out(c) / d P(c) = dt / dxi(c) / ha1(c)
-      double ha1 = 1.0;
-      if (!UNIT) ha1 = (P.frank == 1) ? __ldg(G.ha1_1 + cmk(c)) : __ldg(G.ha1_0 + cmk(c));
-      return dt / __ldg(L.dxi + c - 1) / ha1;
-    };
-    // slope(k) with its branch, and the accumulation of a slope cotangent into fbar
-    auto slope = [&](int k, int& code) -> double {
-      const double fm = F(k - 1), f0 = F(k), fp = F(k + 1);
+    if (tid < 32) {
+      const int q = q0 + tid;
+      int a = 1, b = 1;
+      if (q < nl) { a = q % na + 1; b = q / na + 1; }
+      sa[tid] = a;
+      sb_[tid] = b;
+      sbase[tid] = (DIM == 1) ? gi(d, 0, a, b) : (DIM == 2) ? gi(d, a, 0, b) : gi(d, a, b, 0);
+    }
+    __syncthreads();
+    // S1: f and kappa*obar of cells j0-3 .. j0+TJ+2
+    for (int e = tid; e < 32 * SVJ_R; e += blockDim.x) {
+      int row, ln;
+      elem(e, row, ln);
+      const int j = j0 - 3 + row;
+      double fv = 0.0, kob = 0.0;
+      if (q0 + ln < nl && j >= -1 && j <= lx + 2) {
+        const long long c = so + sbase[ln] + (long long)j * stride;
+        fv = __ldg(P.f + c);
+        if (j >= 1 && j <= lx) {
+          double yha1 = 1.0;
+          if (!UNIT) yha1 = (P.frank == 1) ? __ldg(G.yha1_1 + cmk(ln, j)) : __ldg(G.yha1_0 + cmk(ln, j));
+          kob = dt * __ldg(L.ydxi + j - 1) * yha1 * __ldg(P.obar + c);  // d out(j)/d P(j) * obar(j)
+        }
+      }
+      sf[row][ln] = fv;
+      skob[row][ln] = kob;
+    }
+    __syncthreads();
+    // S2: slope branch and value at cells j0-2 .. j0+TJ+1 (0 .. lx+1 exist); the forward's
+    // divisions, so that the branch replays exactly
+    for (int e = tid; e < 32 * SVJ_R; e += blockDim.x) {
+      int row, ln;
+      elem(e, row, ln);
+      const int k = j0 - 3 + row;
+      if (row < 1 || row > TJ + 4 || k < 0 || k > lx + 1) continue;
+      const double fm = sf[row - 1][ln], f0 = sf[row][ln], fp = sf[row + 1][ln];
       const double dxk = __ldg(L.dx + k), dxk1 = __ldg(L.dx + k + 1);
       const double Ls = (f0 - fm) / dxk, Rs = (fp - f0) / dxk1, Cs = (fp - fm) / (dxk + dxk1);
       const int inner = minmod_branch(2 * Ls, 2 * Rs);
       const double m1 = (inner == 0) ? 0.0 : (inner == 1) ? 2 * Ls : 2 * Rs;
       const int outer = minmod_branch(Cs, m1);
       // 0 zero, 1 centred, 2 twice left, 3 twice right
-      code = (outer == 0) ? 0 : (outer == 1) ? 1 : (inner == 0) ? 0 : (inner == 1) ? 2 : 3;
-      return (code == 0) ? 0.0 : (code == 1) ? Cs : (code == 2) ? 2 * Ls : 2 * Rs;
-    };
-    auto add_slope_bar = [&](int k, int code, double sb) {
-      if (code == 0 || sb == 0.0) return;
-      const double dxk = __ldg(L.dx + k), dxk1 = __ldg(L.dx + k + 1);
-      if (code == 1) {
-        const double w = sb / (dxk + dxk1);
-        P.fbar[cell(k + 1)] += w;
-        P.fbar[cell(k - 1)] -= w;
-      } else if (code == 2) {
-        const double w = 2 * sb / dxk;
-        P.fbar[cell(k)] += w;
-        P.fbar[cell(k - 1)] -= w;
-      } else {
-        const double w = 2 * sb / dxk1;
-        P.fbar[cell(k + 1)] += w;
-        P.fbar[cell(k)] -= w;
+      const int code = (outer == 0) ? 0 : (outer == 1) ? 1 : (inner == 0) ? 0 : (inner == 1) ? 2 : 3;
+      ssl[row][ln] = (code == 0) ? 0.0 : (code == 1) ? Cs : (code == 2) ? 2 * Ls : 2 * Rs;
+      scode[row][ln] = (unsigned char)code;
+    }
+    __syncthreads();
+    // S3: faces j0-1 .. j0+TJ+1 (1 .. lx+1 exist), the ones the segment's cells gather from:
+    // flux cotangent, its direct and slope parts; the face velocity cotangent for the faces
+    // j0 .. jend
+    for (int e = tid; e < 32 * SVJ_R; e += blockDim.x) {
+      int row, ln;
+      elem(e, row, ln);
+      const int i = j0 - 3 + row;
+      if (row < 2 || row > TJ + 4) continue;
+      if (q0 + ln >= nl || i < 1 || i > lx + 1) {
+        sflag[row][ln] = 0;
+        continue;
       }
-    };
-    for (int i = 1; i <= lx + 1; ++i) {
-      double Pb = 0.0;
-      if (i - 1 >= 1) Pb -= kappa(i - 1) * P.obar[cell(i - 1)];
-      if (i <= lx) Pb += kappa(i) * P.obar[cell(i)];
-      double ha2 = 1.0, hc = 1.0;
+      const long long fc = face(s, ln, i);
+      const double v = __ldg(P.v + fc);
+      const double Pb = skob[row][ln] - skob[row - 1][ln];
+      double ha2 = 1.0, yhc = 1.0;
       if (!UNIT) {
-        const long long fk = fmk(i);
+        const long long fk = fmk(ln, i);
         ha2 = (P.frank == 1) ? __ldg(FT.ha2i1 + fk) : __ldg(FT.ha2i0 + fk);
-        hc = __ldg(FT.hc + fk);
+        yhc = __ldg(FT.yhc + fk);
       }
       const double phib = ha2 * Pb;
-      const double v = P.v[face(i)];
-      const double dxi_ = __ldg(L.dx + i);
-      const double vq = v / hc * dt;
-      double vb;
-      if (v < 0) {
-        int code;
-        const double sl = slope(i, code);
-        P.fbar[cell(i)] += v * phib;
-        add_slope_bar(i, code, -0.5 * v * (dxi_ + vq) * phib);
-        vb = phib * (F(i) - 0.5 * (dxi_ + vq) * sl - 0.5 * v * (dt / hc) * sl);
-      } else {
-        int code;
-        const double sl = slope(i - 1, code);
-        P.fbar[cell(i - 1)] += v * phib;
-        add_slope_bar(i - 1, code, 0.5 * v * (dxi_ - vq) * phib);
-        vb = phib * (F(i - 1) + 0.5 * (dxi_ - vq) * sl - 0.5 * v * (dt / hc) * sl);
+      const double dxf = __ldg(L.dx + i);
+      const double vq = v * yhc * dt;
+      const bool neg = v < 0;
+      const int krow = neg ? row : row - 1;  // the upwind cell
+      const int k = i - row + krow;
+      const int code = scode[krow][ln];
+      const double sl = ssl[krow][ln];
+      const double sbar = neg ? -0.5 * v * (dxf + vq) * phib : 0.5 * v * (dxf - vq) * phib;
+      const double dxk = __ldg(L.dx + k), dxk1 = __ldg(L.dx + k + 1);
+      const double wgt = (code == 1) ? sbar / (dxk + dxk1) : (code == 2) ? 2 * sbar / dxk
+                         : (code == 3) ? 2 * sbar / dxk1 : 0.0;
+      sdir[row][ln] = v * phib;
+      sw[row][ln] = wgt;
+      sflag[row][ln] = (unsigned char)(code | (neg ? 4 : 0) | 8);
+      if (P.vbar && i >= j0 && i <= jend) {
+        const double f0 = sf[krow][ln];
+        const double vb = neg ? phib * (f0 - 0.5 * (dxf + vq) * sl - 0.5 * v * (dt * yhc) * sl)
+                              : phib * (f0 + 0.5 * (dxf - vq) * sl - 0.5 * v * (dt * yhc) * sl);
+        P.vbar[fc] = vb;
       }
-      if (P.vbar) P.vbar[face(i)] = vb;
     }
+    __syncthreads();
+    // S4: cells j0 .. jend gather from faces j-1 .. j+2
+    for (int e = tid; e < 32 * SVJ_R; e += blockDim.x) {
+      int row, ln;
+      elem(e, row, ln);
+      const int j = j0 - 3 + row;
+      if (row < 3 || j > jend || q0 + ln >= nl) continue;
+      double acc = 0.0;
+#pragma unroll
+      for (int fr = row - 1; fr <= row + 2; ++fr) {
+        const int fl = sflag[fr][ln];
+        if (!(fl & 8)) continue;
+        const int kr = (fl & 4) ? fr : fr - 1;
+        const int code = fl & 3;
+        if (kr == row) acc += sdir[fr][ln];
+        const double wgt = sw[fr][ln];
+        if (code == 1) {
+          if (row == kr + 1) acc += wgt;
+          if (row == kr - 1) acc -= wgt;
+        } else if (code == 2) {
+          if (row == kr) acc += wgt;
+          if (row == kr - 1) acc -= wgt;
+        } else if (code == 3) {
+          if (row == kr + 1) acc += wgt;
+          if (row == kr) acc -= wgt;
+        }
+      }
+      if (acc != 0.0) P.fbar[so + sbase[ln] + (long long)j * stride] += acc;
+    }
+    __syncthreads();
   }
 }
 

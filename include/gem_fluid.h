@@ -128,8 +128,9 @@ int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, cons
  * nbar (densities; both ghosted 7-species blocks, interior rows written, caller zeroes
  * them) and, if not NULL, Ttop_bar (lx2*lx3 per species, species slowest: the exospheric
  * boundary value of each column and species).  Ts / ns are the inputs of the forward call;
- * the kernel recomputes the forward coefficients and both TRBDF2 stages (Thomas), then
- * solves the transposed systems.  scratch: gem_diffusion_vjp_scratch_doubles(g) doubles. */
+ * the kernel recomputes the forward coefficients and both TRBDF2 stages, then solves the
+ * transposed systems, one warp per column and species with every per-row array on chip
+ * (lx1 up to about 1600). */
 /* One field sweep (advec.f90:384-435 along dim, species 0..nsp-1, frank 0/1; x1 sweeps use
  * frank 0) on a caller-provided ghosted field f (nsp species blocks, updated in place) with
  * face velocities v in the reference face layout; dt is a device pointer. */
@@ -140,10 +141,9 @@ int gem_sweep_field_dev(const gem_grid* g, int dim, int frank, int nsp, double* 
  * cotangent of v. */
 int gem_sweep_field_vjp_dev(const gem_grid* g, int dim, int frank, int nsp, const double* f, const double* v,
                             const double* dt, const double* obar, double* fbar, double* vbar, void* stream);
-long long gem_diffusion_vjp_scratch_doubles(const gem_grid* g);
 int gem_diffusion_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const double* Ts, const double* ns,
                           const double* electrovars, const gem_work* w, const double* dt, const double* Ybar,
-                          double* Tbar, double* nbar, double* Ttop_bar, double* scratch, void* stream);
+                          double* Tbar, double* nbar, double* Ttop_bar, void* stream);
 
 /* No counterpart in the reference.  dt_calc (the same result as gem_dt_calc_dev) for callers
  * that cannot allocate device memory or hold a gem_work (for example code that runs inside

@@ -93,6 +93,9 @@ DIFF_CASES = [
     ("cart_inverted", lambda: G.cartesian_grid(20, 3, 4, inverted=True), dict(seed=3, perturb=0.1)),
     ("dipole", lambda: G.dipole_grid(36, 4, 3), dict(seed=5, perturb=0.2)),
     ("cart_J1", lambda: G.cartesian_grid(22, 3, 3), dict(seed=7, J1_amp=1e-5)),
+    # several rows per lane in the warp solver (lx1 = 150: 5 per lane, the last lane partial)
+    ("cart_long", lambda: G.cartesian_grid(150, 5, 4), dict(seed=11, perturb=0.1, J1_amp=1e-5)),
+    ("dipole_long", lambda: G.dipole_grid(100, 4, 3), dict(seed=13, perturb=0.2)),
 ]
 
 
@@ -132,6 +135,9 @@ def test_cuda_diffusion_adjoint_matches_autograd(name, mk, kw, solver):
 SWEEP_CASES = [
     ("cart", lambda: G.cartesian_grid(20, 6, 5), dict(seed=1)),
     ("dipole", lambda: G.dipole_grid(24, 6, 5), dict(seed=5, perturb=0.2)),
+    # several line segments and 32-line panels per direction
+    ("cart_big", lambda: G.cartesian_grid(70, 40, 35), dict(seed=3)),
+    ("dipole_big", lambda: G.dipole_grid(64, 34, 33), dict(seed=6, perturb=0.2)),
 ]
 
 
