@@ -72,6 +72,9 @@ _SIGS = [
     ("gem_sweep_field_dev", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _VP]),
     ("gem_sweep_field_vjp_dev", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_VP] * 7),
     ("gem_diffusion_vjp_dev", ctypes.c_int, [ctypes.POINTER(GemCfg)] + [_VP] * 11),
+    ("gem_step_adjoint_create", ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+    ("gem_step_adjoint_destroy", ctypes.c_int, [_VP]),
+    ("gem_step_vjp_dev", ctypes.c_int, [ctypes.POINTER(GemCfg)] + [_VP] * 24),
     ("gem_fluid_adv_dev", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("gem_fluid_adv_host", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _D, _VP]),
     ("gem_check_finite", ctypes.c_int, [_VP, _VP, _VP, ctypes.POINTER(ctypes.c_longlong), _VP]),

@@ -38,11 +38,13 @@ class DiffProblem:
 
     def __init__(self, grid, st, nsteps: int, checkpoint_every: int = 5, tcfl: float = 0.5,
                  diffsolvetype: int = 2, device="cuda", cuda_diffusion_adjoint: bool = True,
-                 cuda_sweep_adjoint: bool = True):
+                 cuda_sweep_adjoint: bool = True, cuda_step_adjoint: bool = True):
         import torch
 
         self.cuda_diffusion_adjoint = bool(cuda_diffusion_adjoint)
         self.cuda_sweep_adjoint = bool(cuda_sweep_adjoint)
+        self.cuda_step_adjoint = bool(cuda_step_adjoint)
+        self._sa = None  # gem_step_adjoint workspace, made on first use
         self._dtt = {}
         self._capturing = False
         self._graphs = {}  # (Ttop given) -> captured step VJP
@@ -202,9 +204,13 @@ class DiffProblem:
 
     def step_vjp(self, state, Ttop, j, cot, use_cuda_diffusion_adjoint=False):
         """Pull the cotangent of the state after step j back to the state before it (and
-        to Ttop).  state / cot: (ns, vs1, Ts, lo, hi)."""
+        to Ttop).  state / cot: (ns, vs1, Ts, lo, hi).  With cuda_step_adjoint the whole
+        step's VJP runs in CUDA (gem_step_vjp_dev); otherwise autograd through the tensor
+        transcription, its sweeps and diffusion optionally replaced by their CUDA VJPs."""
         import torch
 
+        if self.cuda_step_adjoint:
+            return self.step_vjp_cuda(state, Ttop, j, cot)
         inp = [t.detach().requires_grad_(True) for t in state]
         tt = None if Ttop is None else Ttop.detach().requires_grad_(True)
         if (self.vjp_graph and use_cuda_diffusion_adjoint and self.cuda_sweep_adjoint
@@ -216,6 +222,44 @@ class DiffProblem:
                 self.vjp_graph_error = str(e)
                 self._capturing = False
         return self._vjp_body(inp, tt, self.dt_tensor(j), cot, use_cuda_diffusion_adjoint)
+
+    def step_vjp_cuda(self, state, Ttop, j, cot):
+        """The step VJP by gem_step_vjp_dev: forward replay and every adjoint piece on the
+        device.  Cotangents at ghost cells of the step's outputs are ignored (the next step
+        never reads them); the state's ghost cells get zero."""
+        import torch
+
+        if self._sa is None:
+            h = ctypes.c_void_p()
+            _lib.check(_lib.lib().gem_step_adjoint_create(self.dg.handle, ctypes.byref(h)))
+            self._sa = h
+        ns, vs1, Ts, lo, hi = (t.detach().contiguous() for t in state)
+        z = [torch.zeros_like(t) if c is None else c.detach().contiguous()
+             for c, t in zip(cot, (ns, vs1, Ts, lo, hi))]
+        out = [torch.empty_like(t) for t in (ns, vs1, Ts, lo, hi)]
+        tb = torch.empty((self.grid.lx3, self.grid.lx2), dtype=torch.float64, device=ns.device) \
+            if Ttop is not None else None
+        self._set_top(Ttop)
+        c = self.cfg.c()
+        p = F._ptr
+        _lib.check(_lib.lib().gem_step_vjp_dev(
+            ctypes.byref(c), self.dg.handle, self.ds.work, self._sa, p(ns), p(vs1), p(self.vs2), p(self.vs3),
+            p(Ts), p(lo), p(hi), p(self.ds.electrovars), p(self.dt_tensor(j)), p(z[0]), p(z[1]), p(z[2]),
+            p(z[3]), p(z[4]), p(out[0]), p(out[1]), p(out[2]), p(out[3]), p(out[4]),
+            None if tb is None else p(tb), F._stream()))
+        return out, tb
+
+    def close(self):
+        """Release the step adjoint workspace."""
+        if self._sa is not None:
+            _lib.lib().gem_step_adjoint_destroy(self._sa)
+            self._sa = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def _vjp_body(self, inp, tt, dt, cot, use_cuda_diffusion_adjoint=True):
         """The step VJP on given tensors (inp require grad); dt: 1-element device tensor."""
@@ -439,6 +483,7 @@ class BatchedAdjoint:
                 g_n0, g_top = backward_from_checkpoints(P, ck, controls[i][1], gns, gTs)
                 out[i] = (float(L.detach()), g_n0, g_top)
                 P._graphs = {}  # release the captured VJP's memory pool
+                P.close()
             del finals, ckpts
         return out
 

@@ -234,6 +234,77 @@ int launch_diffusion(const gem_grid* g, DiffArgs a, cudaStream_t st) {
   return GEM_OK;
 }
 
+// Vector-Jacobian product of one field sweep (differentiable path): tiles of 32 lines x a
+// segment of at most SVJ_TJ cells (ghosts along the line included).
+int launch_sweep_vjp(const gem_grid* g, int dim, int frank, int nsp, const double* f, const double* v,
+                     const double* dt, const double* obar, double* fbar, double* vbar, int vacc, cudaStream_t st) {
+  SweepVjpArgs a;
+  a.G = g->dev;
+  a.f = f;
+  a.v = v;
+  a.dtp = dt;
+  a.obar = obar;
+  a.fbar = fbar;
+  a.vbar = vbar;
+  a.frank = (dim == 1) ? 0 : frank;
+  a.nsp = nsp;
+  a.vacc = vacc;
+  const Dims& d = g->dev.d;
+  const int lx = (dim == 1) ? d.lx1 : (dim == 2) ? d.lx2 : d.lx3;
+  const long long nl = (dim == 1) ? (long long)d.lx2 * d.lx3 : (dim == 2) ? (long long)d.lx1 * d.lx3
+                                                                         : (long long)d.lx1 * d.lx2;
+  SweepVjpTiles T;
+  T.nseg = (lx + 4 + SVJ_TJ - 1) / SVJ_TJ;
+  T.TJ = (lx + 4 + T.nseg - 1) / T.nseg;
+  const long long npan = (nl + 31) / 32;
+  const long long nwork = npan * T.nseg * nsp;
+  if (nwork > INT_MAX) return set_err(GEM_EINVAL, "grid too large for the sweep adjoint");
+  T.npan = (int)npan;
+  T.nwork = (int)nwork;
+  const unsigned nb = (unsigned)std::min<long long>(nwork, (long long)num_sms() * 8);
+  const bool u = g->dev.unit != 0;
+  if (dim == 1) {
+    if (u) k_sweep_vjp<1, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<1, false><<<nb, 256, 0, st>>>(a, T);
+  } else if (dim == 2) {
+    if (u) k_sweep_vjp<2, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<2, false><<<nb, 256, 0, st>>>(a, T);
+  } else {
+    if (u) k_sweep_vjp<3, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<3, false><<<nb, 256, 0, st>>>(a, T);
+  }
+  GEM_LAUNCHED("k_sweep_vjp");
+  return GEM_OK;
+}
+
+// Vector-Jacobian product of the energy diffusion: one warp per (column, species), VNA
+// per-row arrays of M rows per lane in shared memory.
+int launch_diffusion_vjp(const gem_grid* g, DiffAdjArgs a, cudaStream_t st) {
+  const Dims& d = g->dev.d;
+  const int M = std::max(2, (d.lx1 + 31) / 32);
+  a.M = M;
+  const size_t per_warp = (size_t)VNA * M * 32 * sizeof(double);
+  const int wpb = (int)std::min<size_t>(4, (227 * 1024) / per_warp);
+  if (wpb < 1) return set_err(GEM_EINVAL, "lx1=%d too long for the on-chip column adjoint", d.lx1);
+  const size_t smem = per_warp * wpb;
+  const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
+  long long nblk = (ncs + wpb - 1) / wpb;
+  int per_sm = 0;
+  if (g->dev.unit) {
+    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_vjp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion_vjp<true>, 32 * wpb, smem));
+  } else {
+    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_vjp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion_vjp<false>, 32 * wpb, smem));
+  }
+  if (per_sm < 1) per_sm = 1;
+  const long long cap = (long long)num_sms() * per_sm;
+  if (nblk > cap) nblk = cap;
+  if (g->dev.unit)
+    k_diffusion_vjp<true><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
+  else
+    k_diffusion_vjp<false><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
+  GEM_LAUNCHED("k_diffusion_vjp");
+  return GEM_OK;
+}
+
 }  // namespace
 
 // Static scratch of gem_dt_calc_noalloc_dev: 3*LSP partial maxima per x3 plane.
@@ -706,41 +777,7 @@ int gem_sweep_field_vjp_dev(const gem_grid* g, int dim, int frank, int nsp, cons
   if (check_grid(g) || !f || !v || !dt || !obar || !fbar) return set_err(GEM_EINVAL, "null argument");
   if (dim < 1 || dim > 3 || frank < 0 || frank > 1 || nsp < 1 || nsp > LSP)
     return set_err(GEM_EINVAL, "dim %d / frank %d / nsp %d out of range", dim, frank, nsp);
-  SweepVjpArgs a;
-  a.G = g->dev;
-  a.f = f;
-  a.v = v;
-  a.dtp = dt;
-  a.obar = obar;
-  a.fbar = fbar;
-  a.vbar = vbar;
-  a.frank = (dim == 1) ? 0 : frank;
-  a.nsp = nsp;
-  const Dims& d = g->dev.d;
-  // tiles of 32 lines x a segment of at most SVJ_TJ cells (ghosts along the line included)
-  const int lx = (dim == 1) ? d.lx1 : (dim == 2) ? d.lx2 : d.lx3;
-  const long long nl = (dim == 1) ? (long long)d.lx2 * d.lx3 : (dim == 2) ? (long long)d.lx1 * d.lx3
-                                                                         : (long long)d.lx1 * d.lx2;
-  SweepVjpTiles T;
-  T.nseg = (lx + 4 + SVJ_TJ - 1) / SVJ_TJ;
-  T.TJ = (lx + 4 + T.nseg - 1) / T.nseg;
-  const long long npan = (nl + 31) / 32;
-  const long long nwork = npan * T.nseg * nsp;
-  if (nwork > INT_MAX) return set_err(GEM_EINVAL, "grid too large for the sweep adjoint");
-  T.npan = (int)npan;
-  T.nwork = (int)nwork;
-  const unsigned nb = (unsigned)std::min<long long>(nwork, (long long)num_sms() * 8);
-  cudaStream_t st = S(stream);
-  const bool u = g->dev.unit != 0;
-  if (dim == 1) {
-    if (u) k_sweep_vjp<1, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<1, false><<<nb, 256, 0, st>>>(a, T);
-  } else if (dim == 2) {
-    if (u) k_sweep_vjp<2, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<2, false><<<nb, 256, 0, st>>>(a, T);
-  } else {
-    if (u) k_sweep_vjp<3, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<3, false><<<nb, 256, 0, st>>>(a, T);
-  }
-  GEM_LAUNCHED("k_sweep_vjp");
-  return GEM_OK;
+  return launch_sweep_vjp(g, dim, frank, nsp, f, v, dt, obar, fbar, vbar, 0, S(stream));
 }
 
 // Vector-Jacobian product of the energy diffusion (differentiable path).
@@ -768,33 +805,7 @@ int gem_diffusion_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const double* T
   a.Tbar = Tbar;
   a.nbar = nbar;
   a.Ttop_bar = Ttop_bar;
-  // one warp per (column, species); VNA per-row arrays of M rows per lane in shared memory
-  const int M = std::max(2, (d.lx1 + 31) / 32);
-  a.M = M;
-  const size_t per_warp = (size_t)VNA * M * 32 * sizeof(double);
-  const int wpb = (int)std::min<size_t>(4, (227 * 1024) / per_warp);
-  if (wpb < 1) return set_err(GEM_EINVAL, "lx1=%d too long for the on-chip column adjoint", d.lx1);
-  const size_t smem = per_warp * wpb;
-  const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
-  long long nblk = (ncs + wpb - 1) / wpb;
-  int per_sm = 0;
-  cudaStream_t st = S(stream);
-  if (g->dev.unit) {
-    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_vjp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion_vjp<true>, 32 * wpb, smem));
-  } else {
-    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_vjp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion_vjp<false>, 32 * wpb, smem));
-  }
-  if (per_sm < 1) per_sm = 1;
-  const long long cap = (long long)num_sms() * per_sm;
-  if (nblk > cap) nblk = cap;
-  if (g->dev.unit)
-    k_diffusion_vjp<true><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
-  else
-    k_diffusion_vjp<false><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
-  GEM_LAUNCHED("k_diffusion_vjp");
-  return GEM_OK;
+  return launch_diffusion_vjp(g, a, S(stream));
 }
 
 // dt_calc variant that allocates nothing: its scratch (per-x3-plane partial maxima) is
@@ -1000,3 +1011,4 @@ int gem_check_finite(const gem_grid* g, const double* fluidvars, gem_work* w, lo
 }  // extern "C"
 
 #include "gem_batch.cuh"
+#include "gem_adjoint.cuh"

@@ -2126,6 +2126,7 @@ struct SweepVjpArgs {
   double* fbar;        // in: a copy of obar; out: the cotangent of f
   double* vbar;        // optional: cotangent of v (same layout as v)
   int frank, nsp;
+  int vacc;            // 1: vbar += the face cotangents (several sweeps share v), 0: vbar =
 };
 
 // minmod(a,b) branch: 0 zero, 1 a, 2 b (advec.f90:438-447)
@@ -2282,7 +2283,7 @@ __global__ void __launch_bounds__(256) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles
         const double f0 = sf[krow][ln];
         const double vb = neg ? phib * (f0 - 0.5 * (dxf + vq) * sl - 0.5 * v * (dt * yhc) * sl)
                               : phib * (f0 + 0.5 * (dxf - vq) * sl - 0.5 * v * (dt * yhc) * sl);
-        P.vbar[fc] = vb;
+        if (P.vacc) P.vbar[fc] += vb; else P.vbar[fc] = vb;
       }
     }
     __syncthreads();

@@ -145,6 +145,27 @@ int gem_diffusion_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const double* T
                           const double* electrovars, const gem_work* w, const double* dt, const double* Ybar,
                           double* Tbar, double* nbar, double* Ttop_bar, void* stream);
 
+/* Adjoint of one whole fused step (gem_fluid_adv_dev without compression and sources, on
+ * a prescribed dt): given the state before the step (ns, vs1, vs2, vs3, Ts: ghosted
+ * 7-species blocks; v1i_lo / v1i_hi: the stale x1 boundary faces of vs1i, (LSP, lx3, lx2)
+ * with i2 fastest) and the cotangents of the step's outputs (ns, vs1, Ts after the step,
+ * interior cells used; lo_bar_out / hi_bar_out: cotangents of the new boundary faces, may
+ * be NULL), write the cotangents of ns, vs1, Ts (ghost cells 0), of the stale faces and,
+ * if Ttop_bar is not NULL, of the per-column exospheric temperature set on w (lx2*lx3).
+ * vs2 / vs3 are held fixed.  The step's sweeps and conversions are replayed on the
+ * device; everything runs on the stream without host synchronisation or allocation.
+ * Output buffers must not alias input buffers.  Grids without null cells.  The workspace
+ * (about 27 ghosted 7-species fields) belongs to one grid. */
+typedef struct gem_step_adjoint gem_step_adjoint;
+int gem_step_adjoint_create(const gem_grid* g, gem_step_adjoint** out);
+int gem_step_adjoint_destroy(gem_step_adjoint* a);
+int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, gem_step_adjoint* a,
+                     const double* ns, const double* vs1, const double* vs2, const double* vs3, const double* Ts,
+                     const double* v1i_lo, const double* v1i_hi, const double* electrovars, const double* dt,
+                     const double* ns_bar_out, const double* vs1_bar_out, const double* Ts_bar_out,
+                     const double* lo_bar_out, const double* hi_bar_out, double* ns_bar, double* vs1_bar,
+                     double* Ts_bar, double* lo_bar, double* hi_bar, double* Ttop_bar, void* stream);
+
 /* No counterpart in the reference.  dt_calc (the same result as gem_dt_calc_dev) for callers
  * that cannot allocate device memory or hold a gem_work (for example code that runs inside
  * a pool-managed or already-captured context): it calls no allocator.  Its scratch is a

@@ -219,6 +219,7 @@ def test_graphed_step_vjp_equals_eager():
     import torch
 
     g, P, n0, Ttop, tT, tn = _problem(nsteps=4, k=2)
+    P.cuda_step_adjoint = False  # the autograd step VJP (CUDA sweep and diffusion VJPs inside)
     grads = []
     for graphed in (False, True):
         P.vjp_graph = graphed
@@ -231,3 +232,60 @@ def test_graphed_step_vjp_equals_eager():
     assert P.vjp_graph, f"graph capture fell back to eager: {getattr(P, 'vjp_graph_error', '')}"
     for x, y in zip(grads[0], grads[1]):
         assert float((x - y).abs().max() / x.abs().max()) < 1e-12
+
+
+# (name, grid, state kwargs, floor-free): the dipole state after one step has temperatures
+# floored at 100 K, where the diffusion solution sits on the kink of max(T, 100) to within
+# round-off -- there any subgradient is valid and two implementations may pick differently,
+# so the dipole is compared with autograd running the same CUDA sweep and diffusion VJP
+# kernels (the same branch decisions), not with the pure transcription.
+STEP_CASES = [
+    ("cart", lambda: G.cartesian_grid(24, 6, 5), dict(seed=1, perturb=0.1), True),
+    ("cart_inverted", lambda: G.cartesian_grid(20, 5, 4, inverted=True), dict(seed=2, perturb=0.1), True),
+    ("dipole", lambda: G.dipole_grid(28, 6, 5), dict(seed=5, perturb=0.2), False),
+    ("cart_periodic", lambda: G.cartesian_grid(22, 5, 6, flagper=1), dict(seed=3, perturb=0.1, J1_amp=1e-5), True),
+    ("cart_big", lambda: G.cartesian_grid(40, 36, 34), dict(seed=4, perturb=0.1), True),
+]
+
+
+@pytest.mark.parametrize("name,mk,kw,floor_free", STEP_CASES, ids=[c[0] for c in STEP_CASES])
+@pytest.mark.parametrize("solver,top", [(2, True), (1, True), (2, False)])
+def test_cuda_step_vjp_matches_autograd(name, mk, kw, floor_free, solver, top):
+    """The fused CUDA step VJP (gem_step_vjp_dev) against autograd through the tensor step,
+    on random interior output cotangents and random boundary-face cotangents: with the
+    CUDA sweep and diffusion VJPs inside autograd (every grid) and through the pure
+    transcription (grids whose step stays clear of the temperature floor)."""
+    import torch
+
+    g = mk()
+    st = S.init_state(g, **kw)
+    P = AD.DiffProblem(g, st, 2, checkpoint_every=1, diffsolvetype=solver)
+    rng = np.random.default_rng(7)
+    I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
+    n0 = P.base[(slice(0, 6),) + I].clone()
+    Ttop = torch.from_numpy(st.Teinf * (1 + 0.05 * rng.uniform(-1, 1, (g.lx3, g.lx2)))).cuda() if top else None
+    _, ck = P.run(n0, Ttop, keep=True)
+    state = ck[1]  # the state after one step
+    cot = []
+    for t in state[:3]:
+        c = torch.zeros_like(t)
+        c[(slice(None),) + I] = torch.from_numpy(rng.standard_normal(c[(slice(None),) + I].shape)).cuda()
+        cot.append(c)
+    cot += [torch.from_numpy(rng.standard_normal(t.shape)).cuda() for t in state[3:]]
+    got, gtop = P.step_vjp_cuda(state, Ttop, 1, cot)
+    refs = [True] + ([False] if floor_free else [])
+    for cuda_pieces in refs:
+        P.cuda_sweep_adjoint = cuda_pieces
+        inp = [t.detach().clone().requires_grad_(True) for t in state]
+        tt = None if Ttop is None else Ttop.clone().requires_grad_(True)
+        exp, etop = P._vjp_body(inp, tt, P.dt_tensor(1), cot, use_cuda_diffusion_adjoint=cuda_pieces)
+        for nm, x, y in zip(("ns", "vs1", "Ts", "lo", "hi"), got, exp):
+            scale = float(y.abs().max())
+            err = float((x - y).abs().max()) / scale if scale > 0 else float(x.abs().max())
+            assert err < 1e-9, (name, cuda_pieces, nm, err)
+        if Ttop is not None:
+            if g.gridflag == 0:  # closed dipole: no exospheric boundary
+                assert float(gtop.abs().max()) == 0.0
+            else:
+                err = float((gtop - etop).abs().max() / etop.abs().max())
+                assert err < 1e-9, (name, cuda_pieces, "Ttop", err)
