@@ -79,9 +79,10 @@ __global__ void ka_post_fwd(GridDev G, const double* __restrict__ F, double* nou
 // 553-688): from the cotangents of the step's n and v1 outputs (interior), of the diffusion
 // input T (TPb) and of the diffusion's n input (NDb), the cotangents of the swept n, rv, re
 // (C: n | rv | re blocks; ghost cells 0).
-__global__ void ka_post_vjp(GridDev G, const double* __restrict__ F, const double* __restrict__ nbo,
-                            const double* __restrict__ vbo, const double* __restrict__ TPb,
-                            const double* __restrict__ NDb, double* C) {
+__global__ void __launch_bounds__(256) ka_post_vjp(GridDev G, const double* __restrict__ F,
+                                                   const double* __restrict__ nbo, const double* __restrict__ vbo,
+                                                   const double* __restrict__ TPb, const double* __restrict__ NDb,
+                                                   double* C) {
   const Dims d = G.d;
   const long long ng = d.ng;
   const double* rv = F + LSP * ng;
@@ -100,53 +101,48 @@ __global__ void ka_post_vjp(GridDev G, const double* __restrict__ F, const doubl
       }
       continue;
     }
-    double n3[LSP], nout[LSP], nob[LSP];
-    double nsum = 0.0, ne = 0.0;
-#pragma unroll
-    for (int s = 0; s < LSP; ++s) n3[s] = F[s * ng + k];
-#pragma unroll
+    // sums over the ions: n, the floored n (the electron density), the charge flux
+    double nsum = 0.0, ne = 0.0, csum = 0.0;
+#pragma unroll 1
     for (int s = 0; s < LSP - 1; ++s) {
-      nout[s] = fmax_f(n3[s], MINDENS);
-      ne += nout[s];
-      nsum += n3[s];
+      const double n = F[s * ng + k];
+      nsum += n;
+      ne += fmax_f(n, MINDENS);
+      const double v1 = rv[s * ng + k] / (c_ms[s] * fmax_f(n, MINDENSDIV));
+      csum += n * c_qs[s] * v1;
     }
-    nout[LSP - 1] = ne;
-    // energy: T = max((gamma-1)/kB re / max(n_out, 1e-5), 100)
-#pragma unroll
-    for (int s = 0; s < LSP; ++s) {
-      nob[s] = nbo[s * ng + k] + NDb[s * ng + k];
-      const double D = fmax_f(nout[s], MINDENSDIV);
+    // energy: T = max((gamma-1)/kB re / max(n_out, 1e-5), 100), n_out the floored density
+    auto energy = [&](int s, double nout) -> double {  // returns the cotangent of n_out
+      const double D = fmax_f(nout, MINDENSDIV);
       const double Tr = (c_gammas[s] - 1) / KB * re[s * ng + k] / D;
       const double Tb = (Tr >= 100.0) ? TPb[s * ng + k] : 0.0;
       cre[s * ng + k] = Tb * ((c_gammas[s] - 1) / KB) / D;
-      if (nout[s] >= MINDENSDIV) nob[s] += -Tb * Tr / D;
-    }
-    // clean_param(1): ions max(n, 1e-100), electrons their sum
-    double cnv[LSP - 1];
-#pragma unroll
-    for (int s = 0; s < LSP - 1; ++s) cnv[s] = (n3[s] >= MINDENS) ? nob[s] + nob[LSP - 1] : 0.0;
+      double nb = nbo[s * ng + k] + NDb[s * ng + k];
+      if (nout >= MINDENSDIV) nb += -Tb * Tr / D;
+      return nb;
+    };
+    const double nbe = energy(LSP - 1, ne);  // electrons: n_out = the ion sum
+    cn[(LSP - 1) * ng + k] = 0.0;   // the swept electron density is replaced by the ion sum
+    crv[(LSP - 1) * ng + k] = 0.0;  // the electron momentum is not advected
     // rhov12v1: v1 = rv/(ms max(n,1e-5)); ve = -(sum n qs v1)/max(sum n, 1e-5)/qs_e
-    double v1[LSP - 1], Dv[LSP - 1], csum = 0.0;
-#pragma unroll
-    for (int s = 0; s < LSP - 1; ++s) {
-      Dv[s] = fmax_f(n3[s], MINDENSDIV);
-      v1[s] = rv[s * ng + k] / (c_ms[s] * Dv[s]);
-      csum += n3[s] * c_qs[s] * v1[s];
-    }
     const double Nn = fmax_f(nsum, MINDENSDIV);
     const double veb = vbo[(LSP - 1) * ng + k];
     const double csb = veb * (-1 / Nn / c_qs[LSP - 1]);
     const double nsb = (nsum >= MINDENSDIV) ? veb * csum / (Nn * Nn) / c_qs[LSP - 1] : 0.0;
-#pragma unroll
+#pragma unroll 1
     for (int s = 0; s < LSP - 1; ++s) {
-      const double v1b = vbo[s * ng + k] + csb * n3[s] * c_qs[s];
-      double c = cnv[s] + nsb + csb * c_qs[s] * v1[s];
-      if (n3[s] >= MINDENSDIV) c += -v1b * v1[s] / Dv[s];
+      const double n = F[s * ng + k];
+      const double nb = energy(s, fmax_f(n, MINDENS));
+      // clean_param(1): ions max(n, 1e-100), electrons their sum
+      double c = (n >= MINDENS) ? nb + nbe : 0.0;
+      const double Dv = fmax_f(n, MINDENSDIV);
+      const double v1 = rv[s * ng + k] / (c_ms[s] * Dv);
+      const double v1b = vbo[s * ng + k] + csb * n * c_qs[s];
+      c += nsb + csb * c_qs[s] * v1;
+      if (n >= MINDENSDIV) c += -v1b * v1 / Dv;
       cn[s * ng + k] = c;
-      crv[s * ng + k] = v1b / (c_ms[s] * Dv[s]);
+      crv[s * ng + k] = v1b / (c_ms[s] * Dv);
     }
-    cn[(LSP - 1) * ng + k] = 0.0;  // the swept electron density is replaced by the ion sum
-    crv[(LSP - 1) * ng + k] = 0.0;  // the electron momentum is not advected
   }
 }
 
@@ -212,10 +208,11 @@ __device__ __forceinline__ void min_split(double a, double b, double g, double& 
 
 // Adjoint of the x1 boundary of set_global_boundaries (advec.f90:42-79) on the interior
 // x1 rows: density ratio extrapolation, momentum reflected from the stale boundary faces,
-// constant-temperature energy.  One thread per row (i2, i3), all species: the ghost
+// constant-temperature energy.  The ghost
 // cotangents of n, rv, re go to the row's cells 1..3 / lx1-2..lx1, to the stale faces
 // (lob, hib: (LSP, lx3, lx2)) and to v1 at cells 1 and lx1 (vext: 2 x LSP per row, for the
-// conversion adjoint).  Also sums the exospheric-temperature cotangent over species.
+// conversion adjoint).  One thread per (row, species); the species-0 thread also sums the
+// exospheric-temperature cotangent over species.
 __global__ void ka_x1bc_vjp(GridDev G, const double* __restrict__ ns, const double* __restrict__ vs1,
                             const double* __restrict__ Ts, const double* __restrict__ lo,
                             const double* __restrict__ hi, double* C, double* vext, double* lob, double* hib,
@@ -224,12 +221,13 @@ __global__ void ka_x1bc_vjp(GridDev G, const double* __restrict__ ns, const doub
   const long long ng = d.ng;
   const long long ncol = (long long)d.lx2 * d.lx3;
   const int lx = d.lx1;
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncol;
-       c += (long long)gridDim.x * blockDim.x) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncol * LSP;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(t / ncol);
+    const long long c = t - s * ncol;
     const int i2 = (int)(c % d.lx2) + 1, i3 = (int)(c / d.lx2) + 1;
     auto at = [&](int i1) { return gi(d, i1, i2, i3); };
-    double tsum = 0.0;
-    for (int s = 0; s < LSP; ++s) {
+    {
       const long long o = (long long)s * ng;
       const double* n = ns + o;
       double* cn = C + o;
@@ -324,9 +322,12 @@ __global__ void ka_x1bc_vjp(GridDev G, const double* __restrict__ ns, const doub
       }
       vext[(2 * s) * ncol + c] = v1b1;
       vext[(2 * s + 1) * ncol + c] = v1bl;
-      if (ttb) tsum += ttb[s * ncol + c];
     }
-    if (Ttop_bar) Ttop_bar[c] = tsum;
+    if (Ttop_bar && s == 0) {
+      double tsum = 0.0;
+      for (int q = 0; q < LSP; ++q) tsum += ttb[q * ncol + c];
+      Ttop_bar[c] = tsum;
+    }
   }
 }
 
@@ -511,8 +512,8 @@ int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, g
     GEM_LAUNCHED("k_halo_wrap");
   }
   GEM_CUDA(cudaMemcpyAsync(S0, WF, FB, cudaMemcpyDeviceToDevice, st));
-  k_interface_vels<<<grid_for((nf1(d) + nf2(d) + nf3(d)) * LSP, 256), 256, 0, st>>>(G, B, A->V1, A->V2, A->V3,
-                                                                                   LSP);
+  k_interface_vels<<<dim3(grid_for(nf1(d) + nf2(d) + nf3(d), 256, 4), LSP), 256, 0, st>>>(G, B, A->V1, A->V2,
+                                                                                         A->V3);
   GEM_LAUNCHED("k_interface_vels");
   // the nine sweeps: (dim, velocities) per stage, fields n (frank 0, 6 species), rv (frank 1
   // for x2/x3, 6 species), re (frank 0, 7 species)
@@ -597,7 +598,7 @@ int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, g
   }
   ka_copy_vjp<2><<<grid_for((long long)(d.lx1 + 4) * (d.lx3 + 4) * 3 * LSP, 256), 256, 0, st>>>(G, C);
   GEM_LAUNCHED("ka_copy_vjp<2>");
-  ka_x1bc_vjp<<<grid_for(ncol, 128), 128, 0, st>>>(G, ns, vs1, Ts, v1i_lo, v1i_hi, C, A->vext, lo_bar, hi_bar,
+  ka_x1bc_vjp<<<grid_for(ncol * LSP, 128), 128, 0, st>>>(G, ns, vs1, Ts, v1i_lo, v1i_hi, C, A->vext, lo_bar, hi_bar,
                                                     Ttop_bar ? A->ttb : nullptr, Ttop_bar);
   GEM_LAUNCHED("ka_x1bc_vjp");
   ka_conv_vjp<<<ngb, 256, 0, st>>>(G, ns, vs1, Ts, C, A->VB, lo_bar_out, hi_bar_out, A->vext, ns_bar, vs1_bar,

@@ -263,13 +263,20 @@ int launch_sweep_vjp(const gem_grid* g, int dim, int frank, int nsp, const doubl
   T.nwork = (int)nwork;
   const unsigned nb = (unsigned)std::min<long long>(nwork, (long long)num_sms() * 8);
   const bool u = g->dev.unit != 0;
+  const size_t sm = svj_smem(u);
+#define SVJ_LAUNCH(D, U)                                                                         \
+  do {                                                                                           \
+    GEM_CUDA(cudaFuncSetAttribute(k_sweep_vjp<D, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+    k_sweep_vjp<D, U><<<nb, SVJ_THREADS, sm, st>>>(a, T);                                        \
+  } while (0)
   if (dim == 1) {
-    if (u) k_sweep_vjp<1, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<1, false><<<nb, 256, 0, st>>>(a, T);
+    if (u) SVJ_LAUNCH(1, true); else SVJ_LAUNCH(1, false);
   } else if (dim == 2) {
-    if (u) k_sweep_vjp<2, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<2, false><<<nb, 256, 0, st>>>(a, T);
+    if (u) SVJ_LAUNCH(2, true); else SVJ_LAUNCH(2, false);
   } else {
-    if (u) k_sweep_vjp<3, true><<<nb, 256, 0, st>>>(a, T); else k_sweep_vjp<3, false><<<nb, 256, 0, st>>>(a, T);
+    if (u) SVJ_LAUNCH(3, true); else SVJ_LAUNCH(3, false);
   }
+#undef SVJ_LAUNCH
   GEM_LAUNCHED("k_sweep_vjp");
   return GEM_OK;
 }
@@ -669,9 +676,8 @@ int gem_interface_vels_allspec_dev(const gem_grid* g, const double* fluidvars, g
   if (check_grid(g) || !fluidvars || !w) return set_err(GEM_EINVAL, "null argument");
   if (lsp < 1 || lsp > LSP) return set_err(GEM_EINVAL, "number of interface vels must be in 1..%d", LSP);
   const Dims& d = g->dev.d;
-  const long long n = (nf1(d) + nf2(d) + nf3(d)) * lsp;
-  k_interface_vels<<<grid_for(n, 256), 256, 0, S(stream)>>>(g->dev, blocks(g, const_cast<double*>(fluidvars), nullptr),
-                                                          w->vs1i, w->vs2i, w->vs3i, lsp);
+  k_interface_vels<<<dim3(grid_for(nf1(d) + nf2(d) + nf3(d), 256, 4), lsp), 256, 0, S(stream)>>>(
+      g->dev, blocks(g, const_cast<double*>(fluidvars), nullptr), w->vs1i, w->vs2i, w->vs3i);
   GEM_LAUNCHED("k_interface_vels");
   return GEM_OK;
 }

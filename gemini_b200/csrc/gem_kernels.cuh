@@ -554,20 +554,19 @@ __global__ void k_halo_wrap(GridDev G, Blocks B, int with_v23) {
 // ======================================================================================
 // 5. Interface velocities (advec.f90:155-229), standalone form
 // ======================================================================================
-__global__ void k_interface_vels(GridDev G, Blocks B, double* vs1i, double* vs2i, double* vs3i, int lsp) {
+// One thread per face of the three families (enumerated back to back, 32-bit indices: the
+// per-species face counts stay below 2^31), blockIdx.y the species.
+__global__ void k_interface_vels(GridDev G, Blocks B, double* vs1i, double* vs2i, double* vs3i) {
   const Dims d = G.d;
-  // faces of the three families, enumerated back to back
-  const long long n1 = nf1(d), n2 = nf2(d), n3 = nf3(d);
-  const long long tot = (n1 + n2 + n3) * lsp;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long per = n1 + n2 + n3;
-    const int s = (int)(t / per);
-    long long q = t - s * per;
+  const int n1 = (int)nf1(d), n2 = (int)nf2(d), n3 = (int)nf3(d);
+  const int s = blockIdx.y;
+  const int per = n1 + n2 + n3;
+  for (int q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < per; q0 += gridDim.x * blockDim.x) {
+    int q = q0;
     if (q < n1) {
-      const int i1 = (int)(q % (d.lx1 + 1)) + 1;
-      const long long r = q / (d.lx1 + 1);
-      const int i2 = (int)(r % d.lx2) + 1, i3 = (int)(r / d.lx2) + 1;
+      const int i1 = q % (d.lx1 + 1) + 1;
+      const int r = q / (d.lx1 + 1);
+      const int i2 = r % d.lx2 + 1, i3 = r / d.lx2 + 1;
       const double* v = B.vs1(s);
       double val;
       if (i1 >= 2 && i1 <= d.lx1) {
@@ -583,25 +582,25 @@ __global__ void k_interface_vels(GridDev G, Blocks B, double* vs1i, double* vs2i
         else
           val = fmax_f(0.5 * (v[gi(d, d.lx1 - 1, i2, i3)] + v[gi(d, d.lx1, i2, i3)]), 0.0);
       }
-      vs1i[s * n1 + q] = val;
+      vs1i[(long long)s * n1 + q] = val;
       continue;
     }
     q -= n1;
     if (q < n2) {
-      const int i1 = (int)(q % d.lx1) + 1;
-      const long long r = q / d.lx1;
-      const int i2 = (int)(r % (d.lx2 + 1)) + 1, i3 = (int)(r / (d.lx2 + 1)) + 1;
+      const int i1 = q % d.lx1 + 1;
+      const int r = q / d.lx1;
+      const int i2 = r % (d.lx2 + 1) + 1, i3 = r / (d.lx2 + 1) + 1;
       const double* v = B.vs2(s);
-      vs2i[s * n2 + q] = 0.5 * (v[gi(d, i1, i2 - 1, i3)] + v[gi(d, i1, i2, i3)]);
+      vs2i[(long long)s * n2 + q] = 0.5 * (v[gi(d, i1, i2 - 1, i3)] + v[gi(d, i1, i2, i3)]);
       continue;
     }
     q -= n2;
     {
-      const int i1 = (int)(q % d.lx1) + 1;
-      const long long r = q / d.lx1;
-      const int i2 = (int)(r % d.lx2) + 1, i3 = (int)(r / d.lx2) + 1;
+      const int i1 = q % d.lx1 + 1;
+      const int r = q / d.lx1;
+      const int i2 = r % d.lx2 + 1, i3 = r / d.lx2 + 1;
       const double* v = B.vs3(s);
-      vs3i[s * n3 + q] = 0.5 * (v[gi(d, i1, i2, i3 - 1)] + v[gi(d, i1, i2, i3)]);
+      vs3i[(long long)s * n3 + q] = 0.5 * (v[gi(d, i1, i2, i3 - 1)] + v[gi(d, i1, i2, i3)]);
     }
   }
 }
@@ -2140,21 +2139,34 @@ __device__ __forceinline__ int minmod_branch(double a, double b) {
 constexpr int SVJ_TJ = 28;
 constexpr int SVJ_R = SVJ_TJ + 6;  // staged rows: cells j0-3 .. j0+TJ+2
 constexpr int SVJ_LD = 33;         // padded row (32 lines)
+constexpr int SVJ_THREADS = 256;
+constexpr int SVJ_NIT = (32 * SVJ_R + SVJ_THREADS - 1) / SVJ_THREADS;  // staged elements per thread
+// dynamic shared memory: 6 double arrays (8 with the face metrics of curvilinear grids) and
+// 2 byte arrays of SVJ_R x SVJ_LD
+__host__ __device__ constexpr size_t svj_smem(bool unit) {
+  return (size_t)((unit ? 6 : 8) * 8 + 2) * SVJ_R * SVJ_LD;
+}
 
 struct SweepVjpTiles {
   int TJ, nseg, npan, nwork;
 };
 
 template <int DIM, bool UNIT>
-__global__ void __launch_bounds__(256) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles T) {
-  __shared__ double sf[SVJ_R][SVJ_LD];    // f at cell j0-3+row
-  __shared__ double skob[SVJ_R][SVJ_LD];  // kappa*obar at that cell (0 outside 1..lx)
-  __shared__ double ssl[SVJ_R][SVJ_LD];   // slope at that cell
-  __shared__ double sdir[SVJ_R][SVJ_LD];  // face i = j0-3+row: v*phib (to its upwind cell)
-  __shared__ double sw[SVJ_R][SVJ_LD];    // face: weight of its slope cotangent
-  __shared__ unsigned char scode[SVJ_R][SVJ_LD];  // slope branch at the cell
-  __shared__ unsigned char sflag[SVJ_R][SVJ_LD];  // face: branch of its slope | 4 (v<0) | 8 (face exists)
-  __shared__ long long sbase[32];                 // cell index of position 0 of each line
+__global__ void __launch_bounds__(SVJ_THREADS) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles T) {
+  extern __shared__ double svj[];
+  using Row = double[SVJ_LD];
+  Row* sf = reinterpret_cast<Row*>(svj);  // f at cell j0-3+row
+  Row* skob = sf + SVJ_R;                 // kappa*obar at that cell (0 outside 1..lx)
+  Row* ssl = skob + SVJ_R;                // slope at that cell
+  Row* sdir = ssl + SVJ_R;                // face i = j0-3+row: v*phib (to its upwind cell)
+  Row* sw = sdir + SVJ_R;                 // face: weight of its slope cotangent
+  Row* sv = sw + SVJ_R;                   // face velocity
+  Row* sha2 = sv + SVJ_R;                 // face metrics (curvilinear grids only)
+  Row* syhc = sha2 + SVJ_R;
+  using Row8 = unsigned char[SVJ_LD];
+  Row8* scode = reinterpret_cast<Row8*>(svj + (UNIT ? 6 : 8) * SVJ_R * SVJ_LD);  // slope branch at the cell
+  Row8* sflag = scode + SVJ_R;  // face: branch of its slope | 4 (v<0) | 8 (face exists)
+  __shared__ long long sbase[32];  // cell index of position 0 of each line
   __shared__ int sa[32], sb_[32];
   const GridDev& G = P.G;
   const Dims d = G.d;
@@ -2205,13 +2217,19 @@ __global__ void __launch_bounds__(256) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles
       sbase[tid] = (DIM == 1) ? gi(d, 0, a, b) : (DIM == 2) ? gi(d, a, 0, b) : gi(d, a, b, 0);
     }
     __syncthreads();
-    // S1: f and kappa*obar of cells j0-3 .. j0+TJ+2
-    for (int e = tid; e < 32 * SVJ_R; e += blockDim.x) {
+    // S1: f and kappa*obar of cells j0-3 .. j0+TJ+2; velocity (and metrics) of the faces
+    // j0-1 .. j0+TJ+1 the segment's cells gather from.  Unrolled: every load of the thread
+    // is in flight together.
+#pragma unroll
+    for (int it = 0; it < SVJ_NIT; ++it) {
+      const int e = tid + it * SVJ_THREADS;
+      if (e >= 32 * SVJ_R) break;
       int row, ln;
       elem(e, row, ln);
       const int j = j0 - 3 + row;
-      double fv = 0.0, kob = 0.0;
-      if (q0 + ln < nl && j >= -1 && j <= lx + 2) {
+      const bool line = q0 + ln < nl;
+      double fv = 0.0, kob = 0.0, vv = 0.0, ha2 = 1.0, yhc = 1.0;
+      if (line && j >= -1 && j <= lx + 2) {
         const long long c = so + sbase[ln] + (long long)j * stride;
         fv = __ldg(P.f + c);
         if (j >= 1 && j <= lx) {
@@ -2220,20 +2238,34 @@ __global__ void __launch_bounds__(256) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles
           kob = dt * __ldg(L.ydxi + j - 1) * yha1 * __ldg(P.obar + c);  // d out(j)/d P(j) * obar(j)
         }
       }
+      if (line && row >= 2 && row <= TJ + 4 && j >= 1 && j <= lx + 1) {  // face i = j
+        vv = __ldg(P.v + face(s, ln, j));
+        if (!UNIT) {
+          const long long fk = fmk(ln, j);
+          ha2 = (P.frank == 1) ? __ldg(FT.ha2i1 + fk) : __ldg(FT.ha2i0 + fk);
+          yhc = __ldg(FT.yhc + fk);
+        }
+      }
       sf[row][ln] = fv;
       skob[row][ln] = kob;
+      sv[row][ln] = vv;
+      if (!UNIT) {
+        sha2[row][ln] = ha2;
+        syhc[row][ln] = yhc;
+      }
     }
     __syncthreads();
-    // S2: slope branch and value at cells j0-2 .. j0+TJ+1 (0 .. lx+1 exist); the forward's
-    // divisions, so that the branch replays exactly
-    for (int e = tid; e < 32 * SVJ_R; e += blockDim.x) {
+    // S2: slope branch and value at cells j0-2 .. j0+TJ+1 (0 .. lx+1 exist), with the
+    // forward's correctly rounded quotients, so that the branch replays exactly
+    for (int e = tid; e < 32 * SVJ_R; e += SVJ_THREADS) {
       int row, ln;
       elem(e, row, ln);
       const int k = j0 - 3 + row;
       if (row < 1 || row > TJ + 4 || k < 0 || k > lx + 1) continue;
       const double fm = sf[row - 1][ln], f0 = sf[row][ln], fp = sf[row + 1][ln];
-      const double dxk = __ldg(L.dx + k), dxk1 = __ldg(L.dx + k + 1);
-      const double Ls = (f0 - fm) / dxk, Rs = (fp - f0) / dxk1, Cs = (fp - fm) / (dxk + dxk1);
+      const double Ls = mdiv(f0 - fm, __ldg(L.dx + k), __ldg(L.ydx + k));
+      const double Rs = mdiv(fp - f0, __ldg(L.dx + k + 1), __ldg(L.ydx + k + 1));
+      const double Cs = mdiv(fp - fm, __ldg(L.dxs + k), __ldg(L.ydxs + k));
       const int inner = minmod_branch(2 * Ls, 2 * Rs);
       const double m1 = (inner == 0) ? 0.0 : (inner == 1) ? 2 * Ls : 2 * Rs;
       const int outer = minmod_branch(Cs, m1);
@@ -2246,7 +2278,7 @@ __global__ void __launch_bounds__(256) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles
     // S3: faces j0-1 .. j0+TJ+1 (1 .. lx+1 exist), the ones the segment's cells gather from:
     // flux cotangent, its direct and slope parts; the face velocity cotangent for the faces
     // j0 .. jend
-    for (int e = tid; e < 32 * SVJ_R; e += blockDim.x) {
+    for (int e = tid; e < 32 * SVJ_R; e += SVJ_THREADS) {
       int row, ln;
       elem(e, row, ln);
       const int i = j0 - 3 + row;
@@ -2255,15 +2287,10 @@ __global__ void __launch_bounds__(256) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles
         sflag[row][ln] = 0;
         continue;
       }
-      const long long fc = face(s, ln, i);
-      const double v = __ldg(P.v + fc);
+      const double v = sv[row][ln];
       const double Pb = skob[row][ln] - skob[row - 1][ln];
-      double ha2 = 1.0, yhc = 1.0;
-      if (!UNIT) {
-        const long long fk = fmk(ln, i);
-        ha2 = (P.frank == 1) ? __ldg(FT.ha2i1 + fk) : __ldg(FT.ha2i0 + fk);
-        yhc = __ldg(FT.yhc + fk);
-      }
+      const double ha2 = UNIT ? 1.0 : sha2[row][ln];
+      const double yhc = UNIT ? 1.0 : syhc[row][ln];
       const double phib = ha2 * Pb;
       const double dxf = __ldg(L.dx + i);
       const double vq = v * yhc * dt;
@@ -2273,9 +2300,8 @@ __global__ void __launch_bounds__(256) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles
       const int code = scode[krow][ln];
       const double sl = ssl[krow][ln];
       const double sbar = neg ? -0.5 * v * (dxf + vq) * phib : 0.5 * v * (dxf - vq) * phib;
-      const double dxk = __ldg(L.dx + k), dxk1 = __ldg(L.dx + k + 1);
-      const double wgt = (code == 1) ? sbar / (dxk + dxk1) : (code == 2) ? 2 * sbar / dxk
-                         : (code == 3) ? 2 * sbar / dxk1 : 0.0;
+      const double wgt = (code == 1) ? sbar * __ldg(L.ydxs + k) : (code == 2) ? 2 * sbar * __ldg(L.ydx + k)
+                         : (code == 3) ? 2 * sbar * __ldg(L.ydx + k + 1) : 0.0;
       sdir[row][ln] = v * phib;
       sw[row][ln] = wgt;
       sflag[row][ln] = (unsigned char)(code | (neg ? 4 : 0) | 8);
@@ -2283,12 +2309,13 @@ __global__ void __launch_bounds__(256) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles
         const double f0 = sf[krow][ln];
         const double vb = neg ? phib * (f0 - 0.5 * (dxf + vq) * sl - 0.5 * v * (dt * yhc) * sl)
                               : phib * (f0 + 0.5 * (dxf - vq) * sl - 0.5 * v * (dt * yhc) * sl);
+        const long long fc = face(s, ln, i);
         if (P.vacc) P.vbar[fc] += vb; else P.vbar[fc] = vb;
       }
     }
     __syncthreads();
     // S4: cells j0 .. jend gather from faces j-1 .. j+2
-    for (int e = tid; e < 32 * SVJ_R; e += blockDim.x) {
+    for (int e = tid; e < 32 * SVJ_R; e += SVJ_THREADS) {
       int row, ln;
       elem(e, row, ln);
       const int j = j0 - 3 + row;
