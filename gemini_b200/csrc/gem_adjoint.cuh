@@ -37,9 +37,24 @@ __global__ void ka_set_faces(Dims d, const double* __restrict__ lo, const double
   }
 }
 
-__device__ __forceinline__ bool interior_cell(const Dims& d, long long k, int& i1, int& i2, int& i3) {
-  decode_cell(d, k, i1, i2, i3);
-  return i1 >= 1 && i1 <= d.lx1 && i2 >= 1 && i2 <= d.lx2 && i3 >= 1 && i3 <= d.lx3;
+// Traversal of the ghosted grid by 32-cell chunks of x1 rows (i2, i3 ghosts included): one
+// warp per chunk, a lane per cell along the contiguous x1, 32-bit index arithmetic; calls
+// body(k, i1, i2, i3, interior) for every cell.
+template <class Body>
+__device__ __forceinline__ void for_rows(const Dims& d, Body body) {
+  const int X1 = d.lx1 + 4, X2 = d.lx2 + 4, X3 = d.lx3 + 4;
+  const int nch = (X1 + 31) / 32;
+  const int nunit = X2 * X3 * nch;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int u = blockIdx.x * wpb + (threadIdx.x >> 5); u < nunit; u += gridDim.x * wpb) {
+    const int r = u / nch, ch = u - r * nch;
+    const int i2 = r % X2 - 1, i3 = r / X2 - 1;
+    const int i1 = ch * 32 + lane - 1;
+    if (i1 > d.lx1 + 2) continue;
+    const bool in = i1 >= 1 && i1 <= d.lx1 && i2 >= 1 && i2 <= d.lx2 && i3 >= 1 && i3 <= d.lx3;
+    body(gi(d, i1, i2, i3), i1, i2, i3, in);
+  }
 }
 
 // Post-sweep forward values the diffusion adjoint needs: n after clean_param(1) (ion floor,
@@ -49,15 +64,13 @@ __global__ void ka_post_fwd(GridDev G, const double* __restrict__ F, double* nou
   const Dims d = G.d;
   const long long ng = d.ng;
   const double* re = F + 2 * LSP * ng;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ng;
-       k += (long long)gridDim.x * blockDim.x) {
-    int i1, i2, i3;
-    if (!interior_cell(d, k, i1, i2, i3)) {
+  for_rows(d, [&](long long k, int, int, int, bool in) {
+    if (!in) {
       for (int s = 0; s < LSP; ++s) {
         nout[s * ng + k] = MINDENSDIV;
         Tpre[s * ng + k] = 100.0;
       }
-      continue;
+      return;
     }
     double ne = 0.0;
     for (int s = 0; s < LSP; ++s) {
@@ -72,7 +85,7 @@ __global__ void ka_post_fwd(GridDev G, const double* __restrict__ F, double* nou
       const double T = (c_gammas[s] - 1) / KB * re[s * ng + k] / fmax_f(nv, MINDENSDIV);
       Tpre[s * ng + k] = fmax_f(T, 100.0);
     }
-  }
+  });
 }
 
 // Adjoint of rhov12v1 + clean_param(1) + rhoe2T + clean_param(3) (multifluid.f90:218-233,
@@ -90,16 +103,14 @@ __global__ void __launch_bounds__(256) ka_post_vjp(GridDev G, const double* __re
   double* cn = C;
   double* crv = C + LSP * ng;
   double* cre = C + 2 * LSP * ng;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ng;
-       k += (long long)gridDim.x * blockDim.x) {
-    int i1, i2, i3;
-    if (!interior_cell(d, k, i1, i2, i3)) {
+  for_rows(d, [&](long long k, int, int, int, bool in) {
+    if (!in) {
       for (int s = 0; s < LSP; ++s) {
         cn[s * ng + k] = 0.0;
         crv[s * ng + k] = 0.0;
         cre[s * ng + k] = 0.0;
       }
-      continue;
+      return;
     }
     // sums over the ions: n, the floored n (the electron density), the charge flux
     double nsum = 0.0, ne = 0.0, csum = 0.0;
@@ -143,7 +154,7 @@ __global__ void __launch_bounds__(256) ka_post_vjp(GridDev G, const double* __re
       cn[s * ng + k] = c;
       crv[s * ng + k] = v1b / (c_ms[s] * Dv);
     }
-  }
+  });
 }
 
 // Adjoint of the periodic x3 self-wrap (mpihalo.f90:147-151) on n, rv, re: rows 1:lx2,
@@ -196,6 +207,36 @@ __global__ void ka_copy_vjp(GridDev G, double* C) {
     p[at(lx + 2)] = 0.0;
     p[at(1)] += g0;
     p[at(lx)] += g1;
+  }
+}
+
+// Before a sweep adjoint writes the cotangent stage Cn from C: the cells its lines do not
+// cover -- the ghost frame of the other two directions, and the species past a field's
+// nsp -- keep C's value.
+template <int DIM>
+__global__ void ka_frame_copy(GridDev G, const double* __restrict__ C, double* Cn) {
+  const Dims d = G.d;
+  const long long ng = d.ng;
+  const int X2 = d.lx2 + 4, X3 = d.lx3 + 4;
+  const int nrow = X2 * X3 * 3 * LSP;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int r = blockIdx.x * wpb + (threadIdx.x >> 5); r < nrow; r += gridDim.x * wpb) {
+    const int b = r / (X2 * X3);  // field-species block
+    const int rr = r - b * (X2 * X3);
+    const int i2 = rr % X2 - 1, i3 = rr / X2 - 1;
+    const int s = b % LSP, fld = b / LSP;
+    const bool in2 = i2 >= 1 && i2 <= d.lx2, in3 = i3 >= 1 && i3 <= d.lx3;
+    const bool swept = s < ((fld == 2) ? LSP : LSP - 1);
+    // rows whose every cell some line covers (x1 lines), or whose interior x1 cells lines cover
+    const bool row_line = (DIM == 1) ? (in2 && in3) : (DIM == 2) ? in3 : in2;
+    if (swept && row_line && DIM == 1) continue;
+    const long long k0 = (long long)b * ng + gi(d, 0, i2, i3);
+    for (int i1 = lane - 1; i1 <= d.lx1 + 2; i1 += 32) {
+      const bool in1 = i1 >= 1 && i1 <= d.lx1;
+      if (swept && row_line && in1) continue;
+      Cn[k0 + i1] = C[k0 + i1];
+    }
   }
 }
 
@@ -333,7 +374,8 @@ __global__ void ka_x1bc_vjp(GridDev G, const double* __restrict__ ns, const doub
 
 // Adjoint of interface_vels for x1 (advec.f90:155-229) and of v12rhov1 / T2rhoe
 // (multifluid.f90:193-214), writing the state cotangents (ghost cells 0).  v1ib: the x1
-// face cotangent accumulated by the x1 sweep adjoints; lob_out / hib_out: cotangents of the
+// face cotangents of the three x1 sweep adjoints (n, rv, re slices of LSP*nf1 each, summed
+// here); lob_out / hib_out: cotangents of the
 // step's boundary-face outputs (may be null).
 __global__ void ka_conv_vjp(GridDev G, const double* __restrict__ ns, const double* __restrict__ vs1,
                             const double* __restrict__ Ts, const double* __restrict__ C,
@@ -345,12 +387,10 @@ __global__ void ka_conv_vjp(GridDev G, const double* __restrict__ ns, const doub
   const long long ncol = (long long)d.lx2 * d.lx3;
   const long long nf = nf1(d);
   const int lx = d.lx1;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ng;
-       k += (long long)gridDim.x * blockDim.x) {
-    int i1, i2, i3;
-    if (!interior_cell(d, k, i1, i2, i3)) {
+  for_rows(d, [&](long long k, int i1, int i2, int i3, bool in) {
+    if (!in) {
       for (int s = 0; s < LSP; ++s) nsb[s * ng + k] = vs1b[s * ng + k] = Tsb[s * ng + k] = 0.0;
-      continue;
+      return;
     }
     const long long col = (i2 - 1) + (long long)d.lx2 * (i3 - 1);
     for (int s = 0; s < LSP; ++s) {
@@ -362,7 +402,8 @@ __global__ void ka_conv_vjp(GridDev G, const double* __restrict__ ns, const doub
       Tsb[o + k] = gre * n * ke;
       // faces of this row: cotangent g(f), boundary outputs included
       auto gface = [&](int f) {
-        double g = v1ib[s * nf + f1i(d, f, i2, i3)];
+        const long long q = s * nf + f1i(d, f, i2, i3);
+        double g = v1ib[q] + v1ib[LSP * nf + q] + v1ib[2 * LSP * nf + q];
         if (f == 1 && lob_out) g += lob_out[s * ncol + col];
         if (f == lx + 1 && hib_out) g += hib_out[s * ncol + col];
         return g;
@@ -393,7 +434,7 @@ __global__ void ka_conv_vjp(GridDev G, const double* __restrict__ ns, const doub
       if (i1 == lx) vb += vext[(2 * s + 1) * ncol + col];
       vs1b[o + k] = vb;
     }
-  }
+  });
 }
 
 }  // namespace gemk
@@ -411,6 +452,9 @@ struct gem_step_adjoint {
   double* CB = nullptr;  // its copy (3F)
   double *V1 = nullptr, *V2 = nullptr, *V3 = nullptr, *VP = nullptr, *VB = nullptr;  // faces
   double *vext = nullptr, *ttb = nullptr;
+  // the three fields of a direction are swept concurrently: two side streams, fork/join events
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
 };
 
 extern "C" {
@@ -426,7 +470,7 @@ int gem_step_adjoint_create(const gem_grid* g, gem_step_adjoint** out) {
   a->F = (long long)LSP * d.ng;
   const long long n1 = (long long)LSP * nf1(d), n2 = (long long)LSP * nf2(d), n3 = (long long)LSP * nf3(d);
   const long long ncol = (long long)d.lx2 * d.lx3;
-  const long long total = 5 * a->F + 12 * a->F + 6 * a->F + 3 * n1 + n2 + n3 + 2 * LSP * ncol + LSP * ncol;
+  const long long total = 5 * a->F + 12 * a->F + 6 * a->F + 5 * n1 + n2 + n3 + 2 * LSP * ncol + LSP * ncol;
   if (cudaMalloc(&a->base, sizeof(double) * total) != cudaSuccess) {
     delete a;
     cudaGetLastError();
@@ -445,8 +489,8 @@ int gem_step_adjoint_create(const gem_grid* g, gem_step_adjoint** out) {
   p += n1;
   a->VP = p;
   p += n1;
-  a->VB = p;
-  p += n1;
+  a->VB = p;  // three fields' vs1i cotangents
+  p += 3 * n1;
   a->V2 = p;
   p += n2;
   a->V3 = p;
@@ -456,12 +500,22 @@ int gem_step_adjoint_create(const gem_grid* g, gem_step_adjoint** out) {
   a->ttb = p;
   // VP holds the stale boundary faces only; its other faces are never read, keep them finite
   GEM_CUDA(cudaMemset(a->VP, 0, sizeof(double) * n1));
+  for (int i = 0; i < 2; ++i) {
+    GEM_CUDA(cudaStreamCreateWithFlags(&a->side[i], cudaStreamNonBlocking));
+    GEM_CUDA(cudaEventCreateWithFlags(&a->join[i], cudaEventDisableTiming));
+  }
+  GEM_CUDA(cudaEventCreateWithFlags(&a->fork, cudaEventDisableTiming));
   *out = a;
   return GEM_OK;
 }
 
 int gem_step_adjoint_destroy(gem_step_adjoint* a) {
   if (!a) return GEM_OK;
+  for (int i = 0; i < 2; ++i) {
+    if (a->side[i]) cudaStreamDestroy(a->side[i]);
+    if (a->join[i]) cudaEventDestroy(a->join[i]);
+  }
+  if (a->fork) cudaEventDestroy(a->fork);
   cudaFree(a->base);
   delete a;
   return GEM_OK;
@@ -522,8 +576,12 @@ int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, g
   for (int q = 0; q < 3; ++q) {
     double* Sin = Sx[q];
     double* So = Sx[q + 1];
-    GEM_CUDA(cudaMemcpyAsync(So, Sin, 3 * FB, cudaMemcpyDeviceToDevice, st));
+    // fork: field 0 on the caller's stream, fields 1 and 2 on the side streams
+    GEM_CUDA(cudaEventRecord(A->fork, st));
+    for (int i = 0; i < 2; ++i) GEM_CUDA(cudaStreamWaitEvent(A->side[i], A->fork, 0));
     for (int fld = 0; fld < 3; ++fld) {
+      cudaStream_t fs = (fld == 0) ? st : A->side[fld - 1];
+      GEM_CUDA(cudaMemcpyAsync(So + fld * F, Sin + fld * F, FB, cudaMemcpyDeviceToDevice, fs));
       const int frank = (fld == 1 && dims[q] != 1) ? 1 : 0;
       SweepArgs sa;
       Blocks fb;
@@ -536,7 +594,11 @@ int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, g
       sa.dtp = dt;
       sa.dtp_w = nullptr;
       sa.which = frank;
-      if ((rc = launch_sweep(g, dims[q], false, sa, fld == 2 ? LSP : LSP - 1, st))) return rc;
+      if ((rc = launch_sweep(g, dims[q], false, sa, fld == 2 ? LSP : LSP - 1, fs))) return rc;
+    }
+    for (int i = 0; i < 2; ++i) {  // join
+      GEM_CUDA(cudaEventRecord(A->join[i], A->side[i]));
+      GEM_CUDA(cudaStreamWaitEvent(st, A->join[i], 0));
     }
     if (q == 1 && G.flagper) {  // halo_allparams self-wrap between the x1 and x2 sweeps
       Blocks wb = blocks(g, So, So + F);
@@ -573,18 +635,37 @@ int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, g
   double* Cn = A->CB;
   ka_post_vjp<<<ngb, 256, 0, st>>>(G, Sx[3], ns_bar_out, vs1_bar_out, TPB, NDB, C);
   GEM_LAUNCHED("ka_post_vjp");
-  GEM_CUDA(cudaMemsetAsync(A->VB, 0, sizeof(double) * LSP * nf1(d), st));
+  const long long nvf = (long long)LSP * nf1(d);  // one field's vs1i cotangent slice
+  GEM_CUDA(cudaMemsetAsync(A->VB, 0, sizeof(double) * 3 * nvf, st));
   for (int q = 2; q >= 0; --q) {
     if (q == 1 && G.flagper) {
       ka_wrap3_vjp<<<grid_for((long long)(d.lx1 + 4) * d.lx2 * 3 * LSP, 256), 256, 0, st>>>(G, C);
       GEM_LAUNCHED("ka_wrap3_vjp");
     }
-    GEM_CUDA(cudaMemcpyAsync(Cn, C, 3 * FB, cudaMemcpyDeviceToDevice, st));
+    if (dims[q] == 1)
+      ka_frame_copy<1><<<ngb, 256, 0, st>>>(G, C, Cn);
+    else if (dims[q] == 2)
+      ka_frame_copy<2><<<ngb, 256, 0, st>>>(G, C, Cn);
+    else
+      ka_frame_copy<3><<<ngb, 256, 0, st>>>(G, C, Cn);
+    GEM_LAUNCHED("ka_frame_copy");
+    // the three fields in one launch; x1 also gives each field's vs1i cotangent (its own
+    // slice of VB, summed by ka_conv_vjp); the x2/x3 velocities are fixed
+    SweepVjpFields FS;
     for (int fld = 0; fld < 3; ++fld) {
-      const int frank = (fld == 1 && dims[q] != 1) ? 1 : 0;
-      if ((rc = launch_sweep_vjp(g, dims[q], frank, fld == 2 ? LSP : LSP - 1, Sx[q] + fld * F, vel[q], dt,
-                                 C + fld * F, Cn + fld * F, dims[q] == 1 ? A->VB : nullptr, 1, st)))
-        return rc;
+      FS.f[fld] = Sx[q] + fld * F;
+      FS.obar[fld] = C + fld * F;
+      FS.fbar[fld] = Cn + fld * F;
+      FS.vbar[fld] = (dims[q] == 1) ? A->VB + fld * nvf : nullptr;
+      FS.nsp[fld] = fld == 2 ? LSP : LSP - 1;
+      FS.frank[fld] = (fld == 1 && dims[q] != 1) ? 1 : 0;
+    }
+    FS.nfld = 3;
+    FS.nfs = 3 * LSP - 2;
+    if (dims[q] == 1) {
+      if ((rc = launch_sweep_vjp_x1(g, FS, vel[q], dt, 0, st))) return rc;
+    } else {
+      if ((rc = launch_sweep_vjp_march(g, dims[q], FS, vel[q], dt, nullptr, 0, st))) return rc;
     }
     std::swap(C, Cn);
   }

@@ -234,51 +234,78 @@ int launch_diffusion(const gem_grid* g, DiffArgs a, cudaStream_t st) {
   return GEM_OK;
 }
 
-// Vector-Jacobian product of one field sweep (differentiable path): tiles of 32 lines x a
-// segment of at most SVJ_TJ cells (ghosts along the line included).
-int launch_sweep_vjp(const gem_grid* g, int dim, int frank, int nsp, const double* f, const double* v,
-                     const double* dt, const double* obar, double* fbar, double* vbar, int vacc, cudaStream_t st) {
+// x2 / x3 sweep adjoints of up to three fields sharing the face velocities v: one marching
+// thread per (line, segment of SVM_TJ cells, species, field).
+int launch_sweep_vjp_march(const gem_grid* g, int dim, const SweepVjpFields& FS, const double* v, const double* dt,
+                           double* vbar, int vacc, cudaStream_t st) {
   SweepVjpArgs a;
   a.G = g->dev;
-  a.f = f;
+  a.f = nullptr;
   a.v = v;
   a.dtp = dt;
-  a.obar = obar;
-  a.fbar = fbar;
+  a.obar = nullptr;
+  a.fbar = nullptr;
   a.vbar = vbar;
-  a.frank = (dim == 1) ? 0 : frank;
-  a.nsp = nsp;
+  a.frank = 0;
+  a.nsp = 0;
   a.vacc = vacc;
   const Dims& d = g->dev.d;
-  const int lx = (dim == 1) ? d.lx1 : (dim == 2) ? d.lx2 : d.lx3;
-  const long long nl = (dim == 1) ? (long long)d.lx2 * d.lx3 : (dim == 2) ? (long long)d.lx1 * d.lx3
-                                                                         : (long long)d.lx1 * d.lx2;
-  SweepVjpTiles T;
-  T.nseg = (lx + 4 + SVJ_TJ - 1) / SVJ_TJ;
-  T.TJ = (lx + 4 + T.nseg - 1) / T.nseg;
-  const long long npan = (nl + 31) / 32;
-  const long long nwork = npan * T.nseg * nsp;
-  if (nwork > INT_MAX) return set_err(GEM_EINVAL, "grid too large for the sweep adjoint");
-  T.npan = (int)npan;
-  T.nwork = (int)nwork;
-  const unsigned nb = (unsigned)std::min<long long>(nwork, (long long)num_sms() * 8);
-  const bool u = g->dev.unit != 0;
-  const size_t sm = svj_smem(u);
-#define SVJ_LAUNCH(D, U)                                                                         \
-  do {                                                                                           \
-    GEM_CUDA(cudaFuncSetAttribute(k_sweep_vjp<D, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
-    k_sweep_vjp<D, U><<<nb, SVJ_THREADS, sm, st>>>(a, T);                                        \
-  } while (0)
-  if (dim == 1) {
-    if (u) SVJ_LAUNCH(1, true); else SVJ_LAUNCH(1, false);
-  } else if (dim == 2) {
-    if (u) SVJ_LAUNCH(2, true); else SVJ_LAUNCH(2, false);
+  const int lx = (dim == 2) ? d.lx2 : d.lx3;
+  const int nseg = (lx + 4 + SVM_TJ - 1) / SVM_TJ;
+  const long long nl = (long long)d.lx1 * ((dim == 2) ? d.lx3 : d.lx2);
+  const unsigned nb = grid_for(nl * nseg * FS.nfs, 256, 8);
+  if (g->dev.unit) {
+    if (dim == 2) k_sweep_vjp_march<2, true><<<nb, 256, 0, st>>>(a, FS, nseg);
+    else k_sweep_vjp_march<3, true><<<nb, 256, 0, st>>>(a, FS, nseg);
   } else {
-    if (u) SVJ_LAUNCH(3, true); else SVJ_LAUNCH(3, false);
+    if (dim == 2) k_sweep_vjp_march<2, false><<<nb, 256, 0, st>>>(a, FS, nseg);
+    else k_sweep_vjp_march<3, false><<<nb, 256, 0, st>>>(a, FS, nseg);
   }
-#undef SVJ_LAUNCH
-  GEM_LAUNCHED("k_sweep_vjp");
+  GEM_LAUNCHED("k_sweep_vjp_march");
   return GEM_OK;
+}
+
+// x1 sweep adjoints of up to three fields sharing the face velocities v: one warp per
+// (x1 line, species, field); FS.vbar[f] (optional) receives field f's velocity cotangent.
+int launch_sweep_vjp_x1(const gem_grid* g, const SweepVjpFields& FS, const double* v, const double* dt, int vacc,
+                        cudaStream_t st) {
+  SweepVjpArgs a;
+  a.G = g->dev;
+  a.f = nullptr;
+  a.v = v;
+  a.dtp = dt;
+  a.obar = nullptr;
+  a.fbar = nullptr;
+  a.vbar = nullptr;
+  a.frank = 0;
+  a.nsp = 0;
+  a.vacc = vacc;
+  const Dims& d = g->dev.d;
+  const long long nwarp = (long long)d.lx2 * d.lx3 * FS.nfs;
+  const unsigned nb = (unsigned)std::min<long long>((nwarp + 7) / 8, (long long)num_sms() * 8);
+  if (g->dev.unit)
+    k_sweep_vjp_x1<true><<<nb, 256, 0, st>>>(a, FS);
+  else
+    k_sweep_vjp_x1<false><<<nb, 256, 0, st>>>(a, FS);
+  GEM_LAUNCHED("k_sweep_vjp_x1");
+  return GEM_OK;
+}
+
+// Vector-Jacobian product of one field sweep (differentiable path): x1 by warps along the
+// lines, x2 / x3 by marching threads.
+int launch_sweep_vjp(const gem_grid* g, int dim, int frank, int nsp, const double* f, const double* v,
+                     const double* dt, const double* obar, double* fbar, double* vbar, int vacc, cudaStream_t st) {
+  SweepVjpFields FS;
+  FS.f[0] = f;
+  FS.obar[0] = obar;
+  FS.fbar[0] = fbar;
+  FS.vbar[0] = vbar;
+  FS.nsp[0] = nsp;
+  FS.frank[0] = (dim == 1) ? 0 : frank;
+  FS.nfld = 1;
+  FS.nfs = nsp;
+  if (dim == 1) return launch_sweep_vjp_x1(g, FS, v, dt, vacc, st);
+  return launch_sweep_vjp_march(g, dim, FS, v, dt, vbar, vacc, st);
 }
 
 // Vector-Jacobian product of the energy diffusion: one warp per (column, species), VNA

@@ -2108,13 +2108,11 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
 //     branches of the forward sweep replayed, the line update is linear in f, and its
 //     transpose is a local stencil: the cotangent of face i's flux reaches the upwind cell
 //     directly and, through the selected slope (zero, centred, or twice the left or right
-//     difference), the cells around it -- cells i-2 .. i+1 in all.  A block stages a tile
-//     of 32 lines by one segment of each line (with 3 halo cells per side) in shared memory
-//     and computes each slope branch once, each face's cotangent parts once, then lets
-//     every cell gather from its four faces j-1 .. j+2: no two threads write the same cell,
-//     and global memory moves along i1 in every direction.  fbar enters holding the output
-//     cotangent (the identity part) and receives the flux parts; vbar (optional) gets the
-//     face-velocity cotangent.
+//     difference), the cells around it -- cells i-2 .. i+1 in all.  Each slope branch and
+//     each face's cotangent parts are computed once: x2 / x3 lines by threads marching along
+//     the line (lanes along i1), x1 lines by warps with lanes along the contiguous x1 and
+//     neighbours exchanged by shuffles.  Every cell is written by one thread, as obar plus
+//     its flux parts; vbar (optional) gets the face-velocity cotangent.
 // ======================================================================================
 struct SweepVjpArgs {
   GridDev G;
@@ -2122,7 +2120,9 @@ struct SweepVjpArgs {
   const double* v;  // face velocities (reference face layout, species blocks)
   const double* dtp;
   const double* obar;  // cotangent of the output field
-  double* fbar;        // in: a copy of obar; out: the cotangent of f
+  double* fbar;        // out: the cotangent of f.  The kernels write obar + the flux parts
+                       // to every cell of the swept lines; the other cells (ghost frame of
+                       // the other directions, species past nsp) must hold obar already
   double* vbar;        // optional: cotangent of v (same layout as v)
   int frank, nsp;
   int vacc;            // 1: vbar += the face cotangents (several sweeps share v), 0: vbar =
@@ -2134,215 +2134,314 @@ __device__ __forceinline__ int minmod_branch(double a, double b) {
   return (fabs(a) < fabs(b)) ? 1 : 2;
 }
 
-// Tiles: 32 lines (consecutive in the flattened line index, i1 fastest for the x2/x3 lines)
-// times a segment of up to SVJ_TJ cells along the line, staged with 3 halo cells per side.
-constexpr int SVJ_TJ = 28;
-constexpr int SVJ_R = SVJ_TJ + 6;  // staged rows: cells j0-3 .. j0+TJ+2
-constexpr int SVJ_LD = 33;         // padded row (32 lines)
-constexpr int SVJ_THREADS = 256;
-constexpr int SVJ_NIT = (32 * SVJ_R + SVJ_THREADS - 1) / SVJ_THREADS;  // staged elements per thread
-// dynamic shared memory: 6 double arrays (8 with the face metrics of curvilinear grids) and
-// 2 byte arrays of SVJ_R x SVJ_LD
-__host__ __device__ constexpr size_t svj_smem(bool unit) {
-  return (size_t)((unit ? 6 : 8) * 8 + 2) * SVJ_R * SVJ_LD;
-}
+// x2 / x3 sweep adjoints by marching (several fields in one launch).  One thread per (line,
+// segment, species, field), lanes along i1 (coalesced): the thread walks the faces
+// j0-1 .. jend+2 of its segment once, keeping the slopes of the two candidate upwind cells,
+// the flux-cotangent inputs of the previous cell and the pending cotangents of cells i-2 ..
+// i+1 in registers; cell i-2 is final after face i and is added to fbar.
+constexpr int SVM_TJ = 32;  // cells per segment
+constexpr int SVM_MAXF = 3;
 
-struct SweepVjpTiles {
-  int TJ, nseg, npan, nwork;
+struct SweepVjpFields {
+  const double* f[SVM_MAXF];
+  const double* obar[SVM_MAXF];
+  double* fbar[SVM_MAXF];
+  double* vbar[SVM_MAXF];  // x1: per-field face-velocity cotangent (written), or null
+  int nsp[SVM_MAXF];
+  int frank[SVM_MAXF];
+  int nfld;
+  int nfs;  // sum of nsp
 };
 
+// (field, species) of the flattened index fs; selects instead of indexing keep the parameter
+// block out of local memory
+__device__ __forceinline__ void field_of(const SweepVjpFields& FS, int fs, int& fld, int& s) {
+  fld = 0;
+  if (FS.nfld > 1 && fs >= FS.nsp[0]) { fs -= FS.nsp[0]; fld = 1; }
+  if (FS.nfld > 2 && fld == 1 && fs >= FS.nsp[1]) { fs -= FS.nsp[1]; fld = 2; }
+  s = fs;
+}
+template <class T>
+__device__ __forceinline__ T pick3(int i, T a, T b, T c) { return (i == 0) ? a : (i == 1) ? b : c; }
+
+struct SlopeBr {
+  double val;
+  int code;  // 0 zero, 1 centred, 2 twice left, 3 twice right
+};
+
+// slope(k) of advec.f90:438-447 with its branch, from f(k-1), f(k), f(k+1) (correctly rounded
+// quotients, as the forward)
+__device__ __forceinline__ SlopeBr slope_br(const Line1D& L, int k, double fm, double f0, double fp) {
+  const double Ls = mdiv(f0 - fm, __ldg(L.dx + k), __ldg(L.ydx + k));
+  const double Rs = mdiv(fp - f0, __ldg(L.dx + k + 1), __ldg(L.ydx + k + 1));
+  const double Cs = mdiv(fp - fm, __ldg(L.dxs + k), __ldg(L.ydxs + k));
+  const int inner = minmod_branch(2 * Ls, 2 * Rs);
+  const double m1 = (inner == 0) ? 0.0 : (inner == 1) ? 2 * Ls : 2 * Rs;
+  const int outer = minmod_branch(Cs, m1);
+  SlopeBr r;
+  r.code = (outer == 0) ? 0 : (outer == 1) ? 1 : (inner == 0) ? 0 : (inner == 1) ? 2 : 3;
+  r.val = (r.code == 0) ? 0.0 : (r.code == 1) ? Cs : (r.code == 2) ? 2 * Ls : 2 * Rs;
+  return r;
+}
+
 template <int DIM, bool UNIT>
-__global__ void __launch_bounds__(SVJ_THREADS) k_sweep_vjp(SweepVjpArgs P, SweepVjpTiles T) {
-  extern __shared__ double svj[];
-  using Row = double[SVJ_LD];
-  Row* sf = reinterpret_cast<Row*>(svj);  // f at cell j0-3+row
-  Row* skob = sf + SVJ_R;                 // kappa*obar at that cell (0 outside 1..lx)
-  Row* ssl = skob + SVJ_R;                // slope at that cell
-  Row* sdir = ssl + SVJ_R;                // face i = j0-3+row: v*phib (to its upwind cell)
-  Row* sw = sdir + SVJ_R;                 // face: weight of its slope cotangent
-  Row* sv = sw + SVJ_R;                   // face velocity
-  Row* sha2 = sv + SVJ_R;                 // face metrics (curvilinear grids only)
-  Row* syhc = sha2 + SVJ_R;
-  using Row8 = unsigned char[SVJ_LD];
-  Row8* scode = reinterpret_cast<Row8*>(svj + (UNIT ? 6 : 8) * SVJ_R * SVJ_LD);  // slope branch at the cell
-  Row8* sflag = scode + SVJ_R;  // face: branch of its slope | 4 (v<0) | 8 (face exists)
-  __shared__ long long sbase[32];  // cell index of position 0 of each line
-  __shared__ int sa[32], sb_[32];
+__global__ void __launch_bounds__(256) k_sweep_vjp_march(SweepVjpArgs P, SweepVjpFields FS, int nseg) {
   const GridDev& G = P.G;
   const Dims d = G.d;
-  const int lx = (DIM == 1) ? d.lx1 : (DIM == 2) ? d.lx2 : d.lx3;
-  if (lx <= 1) return;  // single-cell lines pass through
+  const int lx = (DIM == 2) ? d.lx2 : d.lx3;
+  if (lx <= 1) return;
   const double dt = *P.dtp;
-  const int na = (DIM == 1) ? d.lx2 : d.lx1;  // fastest line coordinate
-  const int nl = na * ((DIM == 3) ? d.lx2 : d.lx3);
+  const int na = d.lx1;
+  const int nb = (DIM == 2) ? d.lx3 : d.lx2;
+  const long long nl = (long long)na * nb;
+  const long long total = nl * nseg * FS.nfs;
   const Line1D& L = G.L[DIM - 1];
   const FaceTab& FT = G.F[DIM - 1];
-  const long long nfaces = (DIM == 1) ? nf1(d) : (DIM == 2) ? nf2(d) : nf3(d);
-  const long long stride = (DIM == 1) ? 1 : (DIM == 2) ? d.s2 : d.s3;
-  const int TJ = T.TJ;
-  const int tid = threadIdx.x;
-  // element e of a 32 x SVJ_R sweep: line-fastest for x2/x3 (i1 coalesced), position-fastest
-  // for x1 (x1 contiguous)
-  auto elem = [&](int e, int& row, int& ln) {
-    if (DIM == 1) { ln = e / SVJ_R; row = e - ln * SVJ_R; }
-    else { ln = e & 31; row = e >> 5; }
-  };
-  auto cmk = [&](int ln, int k) -> long long {
-    const int a = sa[ln], b = sb_[ln];
-    return (DIM == 1) ? cmi(G, k, a, b) : (DIM == 2) ? cmi(G, a, k, b) : cmi(G, a, b, k);
-  };
-  auto fmk = [&](int ln, int k) -> long long {
-    const int a = sa[ln], b = sb_[ln];
-    return (DIM == 1) ? fmi(FT, k, a, b) : (DIM == 2) ? fmi(FT, a, k, b) : fmi(FT, a, b, k);
-  };
-  auto face = [&](int s, int ln, int k) -> long long {
-    const int a = sa[ln], b = sb_[ln];
-    const long long q = (DIM == 1) ? f1i(d, k, a, b) : (DIM == 2) ? f2i(d, a, k, b) : f3i(d, a, b, k);
-    return (long long)s * nfaces + q;
-  };
-  for (int w = blockIdx.x; w < T.nwork; w += gridDim.x) {
-    const int pn = w % T.npan;
-    const int r = w / T.npan;
-    const int g = r % T.nseg, s = r / T.nseg;
-    const int q0 = pn * 32;
-    const int j0 = -1 + g * TJ;  // first cell of the segment
-    const int jend = min(j0 + TJ - 1, lx + 2);
-    const long long so = (long long)s * d.ng;
-    if (tid < 32) {
-      const int q = q0 + tid;
-      int a = 1, b = 1;
-      if (q < nl) { a = q % na + 1; b = q / na + 1; }
-      sa[tid] = a;
-      sb_[tid] = b;
-      sbase[tid] = (DIM == 1) ? gi(d, 0, a, b) : (DIM == 2) ? gi(d, a, 0, b) : gi(d, a, b, 0);
-    }
-    __syncthreads();
-    // S1: f and kappa*obar of cells j0-3 .. j0+TJ+2; velocity (and metrics) of the faces
-    // j0-1 .. j0+TJ+1 the segment's cells gather from.  Unrolled: every load of the thread
-    // is in flight together.
-#pragma unroll
-    for (int it = 0; it < SVJ_NIT; ++it) {
-      const int e = tid + it * SVJ_THREADS;
-      if (e >= 32 * SVJ_R) break;
-      int row, ln;
-      elem(e, row, ln);
-      const int j = j0 - 3 + row;
-      const bool line = q0 + ln < nl;
-      double fv = 0.0, kob = 0.0, vv = 0.0, ha2 = 1.0, yhc = 1.0;
-      if (line && j >= -1 && j <= lx + 2) {
-        const long long c = so + sbase[ln] + (long long)j * stride;
-        fv = __ldg(P.f + c);
-        if (j >= 1 && j <= lx) {
-          double yha1 = 1.0;
-          if (!UNIT) yha1 = (P.frank == 1) ? __ldg(G.yha1_1 + cmk(ln, j)) : __ldg(G.yha1_0 + cmk(ln, j));
-          kob = dt * __ldg(L.ydxi + j - 1) * yha1 * __ldg(P.obar + c);  // d out(j)/d P(j) * obar(j)
-        }
-      }
-      if (line && row >= 2 && row <= TJ + 4 && j >= 1 && j <= lx + 1) {  // face i = j
-        vv = __ldg(P.v + face(s, ln, j));
-        if (!UNIT) {
-          const long long fk = fmk(ln, j);
-          ha2 = (P.frank == 1) ? __ldg(FT.ha2i1 + fk) : __ldg(FT.ha2i0 + fk);
-          yhc = __ldg(FT.yhc + fk);
-        }
-      }
-      sf[row][ln] = fv;
-      skob[row][ln] = kob;
-      sv[row][ln] = vv;
+  const long long nfaces = (DIM == 2) ? nf2(d) : nf3(d);
+  const long long stride = (DIM == 2) ? d.s2 : d.s3;                        // cells along the line
+  const long long fstride = (DIM == 2) ? (long long)d.lx1 : (long long)d.lx1 * d.lx2;  // faces
+  const long long mstride = (DIM == 2) ? d.s2 : G.c3;                       // cell metrics
+  const long long tstride = (DIM == 2) ? FT.t2 : FT.t3;                     // face metrics
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long ln = t % nl;
+    const long long r = t / nl;
+    const int g = (int)(r % nseg);
+    // (field, species); selects instead of indexing keep the parameter block out of local memory
+    int fs = (int)(r / nseg);
+    int fld = 0;
+    if (FS.nfld > 1 && fs >= FS.nsp[0]) { fs -= FS.nsp[0]; fld = 1; }
+    if (FS.nfld > 2 && fld == 1 && fs >= FS.nsp[1]) { fs -= FS.nsp[1]; fld = 2; }
+    const int s = fs;
+    const int frank = (fld == 0) ? FS.frank[0] : (fld == 1) ? FS.frank[1] : FS.frank[2];
+    const int a = (int)(ln % na) + 1, b = (int)(ln / na) + 1;
+    const long long c0 = (long long)s * d.ng + ((DIM == 2) ? gi(d, a, 0, b) : gi(d, a, b, 0));  // cell 0
+    const long long v0 = (long long)s * nfaces + ((DIM == 2) ? f2i(d, a, 1, b) : f3i(d, a, b, 1)) - fstride;
+    const long long m0 = (DIM == 2) ? cmi(G, a, 0, b) : cmi(G, a, b, 0);
+    const long long t0 = ((DIM == 2) ? fmi(FT, a, 1, b) : fmi(FT, a, b, 1)) - tstride;
+    const double* f = (fld == 0) ? FS.f[0] : (fld == 1) ? FS.f[1] : FS.f[2];
+    const double* ob = (fld == 0) ? FS.obar[0] : (fld == 1) ? FS.obar[1] : FS.obar[2];
+    double* fb = (fld == 0) ? FS.fbar[0] : (fld == 1) ? FS.fbar[1] : FS.fbar[2];
+    const double* yha1 = (frank == 1) ? G.yha1_1 : G.yha1_0;
+    const double* ha2t = (frank == 1) ? FT.ha2i1 : FT.ha2i0;
+    auto F = [&](int j) { return __ldg(f + c0 + j * stride); };
+    auto kob = [&](int j) -> double {  // d out(j)/d P(j) * obar(j), 0 outside 1..lx
+      if (j < 1 || j > lx) return 0.0;
+      const double y = UNIT ? 1.0 : __ldg(yha1 + m0 + j * mstride);
+      return dt * __ldg(L.ydxi + j - 1) * y * __ldg(ob + c0 + j * stride);
+    };
+    // the global inputs of face i: f(i+1), obar(i), v(i) and the metrics, loaded two faces
+    // ahead of their use so that the march is not bound by load latency
+    struct In {
+      double fn, ob, v, y, h, yc;
+    };
+    auto load = [&](int i) {
+      In q;
+      q.fn = F(i + 1);
+      q.ob = (i >= 1 && i <= lx) ? __ldg(ob + c0 + i * stride) : 0.0;
+      q.v = __ldg(P.v + v0 + i * fstride);
+      q.y = q.h = q.yc = 1.0;
       if (!UNIT) {
-        sha2[row][ln] = ha2;
-        syhc[row][ln] = yhc;
+        if (i >= 1 && i <= lx) q.y = __ldg(yha1 + m0 + i * mstride);
+        q.h = __ldg(ha2t + t0 + i * tstride);
+        q.yc = __ldg(FT.yhc + t0 + i * tstride);
       }
-    }
-    __syncthreads();
-    // S2: slope branch and value at cells j0-2 .. j0+TJ+1 (0 .. lx+1 exist), with the
-    // forward's correctly rounded quotients, so that the branch replays exactly
-    for (int e = tid; e < 32 * SVJ_R; e += SVJ_THREADS) {
-      int row, ln;
-      elem(e, row, ln);
-      const int k = j0 - 3 + row;
-      if (row < 1 || row > TJ + 4 || k < 0 || k > lx + 1) continue;
-      const double fm = sf[row - 1][ln], f0 = sf[row][ln], fp = sf[row + 1][ln];
-      const double Ls = mdiv(f0 - fm, __ldg(L.dx + k), __ldg(L.ydx + k));
-      const double Rs = mdiv(fp - f0, __ldg(L.dx + k + 1), __ldg(L.ydx + k + 1));
-      const double Cs = mdiv(fp - fm, __ldg(L.dxs + k), __ldg(L.ydxs + k));
-      const int inner = minmod_branch(2 * Ls, 2 * Rs);
-      const double m1 = (inner == 0) ? 0.0 : (inner == 1) ? 2 * Ls : 2 * Rs;
-      const int outer = minmod_branch(Cs, m1);
-      // 0 zero, 1 centred, 2 twice left, 3 twice right
-      const int code = (outer == 0) ? 0 : (outer == 1) ? 1 : (inner == 0) ? 0 : (inner == 1) ? 2 : 3;
-      ssl[row][ln] = (code == 0) ? 0.0 : (code == 1) ? Cs : (code == 2) ? 2 * Ls : 2 * Rs;
-      scode[row][ln] = (unsigned char)code;
-    }
-    __syncthreads();
-    // S3: faces j0-1 .. j0+TJ+1 (1 .. lx+1 exist), the ones the segment's cells gather from:
-    // flux cotangent, its direct and slope parts; the face velocity cotangent for the faces
-    // j0 .. jend
-    for (int e = tid; e < 32 * SVJ_R; e += SVJ_THREADS) {
-      int row, ln;
-      elem(e, row, ln);
-      const int i = j0 - 3 + row;
-      if (row < 2 || row > TJ + 4) continue;
-      if (q0 + ln >= nl || i < 1 || i > lx + 1) {
-        sflag[row][ln] = 0;
-        continue;
-      }
-      const double v = sv[row][ln];
-      const double Pb = skob[row][ln] - skob[row - 1][ln];
-      const double ha2 = UNIT ? 1.0 : sha2[row][ln];
-      const double yhc = UNIT ? 1.0 : syhc[row][ln];
-      const double phib = ha2 * Pb;
+      return q;
+    };
+    const int j0 = -1 + g * SVM_TJ;
+    const int jend = min(j0 + SVM_TJ - 1, lx + 2);
+    const int i0 = max(1, j0 - 1), i1e = min(lx + 1, jend + 2);
+    double fc = F(i0 - 1), fp = F(i0);                              // f(i-1), f(i)
+    SlopeBr sprev = slope_br(L, i0 - 1, F(i0 - 2), fc, fp);         // slope(i-1)
+    double kprev = kob(i0 - 1);
+    double A0 = 0, A1 = 0, A2 = 0, A3 = 0;                          // pending cells i-2 .. i+1
+    In qa = load(i0), qb;
+    if (i0 + 1 <= i1e) qb = load(i0 + 1);
+    for (int i = i0; i <= i1e; ++i) {
+      In qc;
+      if (i + 2 <= i1e) qc = load(i + 2);
+      const double fn = qa.fn;
+      const SlopeBr scur = slope_br(L, i, fc, fp, fn);  // slope(i)
+      const double kc = (i >= 1 && i <= lx) ? dt * __ldg(L.ydxi + i - 1) * qa.y * qa.ob : 0.0;
+      const double v = qa.v;
+      const double ha2 = qa.h, yhc = qa.yc;
+      const double phib = ha2 * (kc - kprev);
       const double dxf = __ldg(L.dx + i);
       const double vq = v * yhc * dt;
       const bool neg = v < 0;
-      const int krow = neg ? row : row - 1;  // the upwind cell
-      const int k = i - row + krow;
-      const int code = scode[krow][ln];
-      const double sl = ssl[krow][ln];
+      const SlopeBr sk = neg ? scur : sprev;  // slope of the upwind cell k
+      const int k = neg ? i : i - 1;
       const double sbar = neg ? -0.5 * v * (dxf + vq) * phib : 0.5 * v * (dxf - vq) * phib;
-      const double wgt = (code == 1) ? sbar * __ldg(L.ydxs + k) : (code == 2) ? 2 * sbar * __ldg(L.ydx + k)
-                         : (code == 3) ? 2 * sbar * __ldg(L.ydx + k + 1) : 0.0;
-      sdir[row][ln] = v * phib;
-      sw[row][ln] = wgt;
-      sflag[row][ln] = (unsigned char)(code | (neg ? 4 : 0) | 8);
+      const double w = (sk.code == 1) ? sbar * __ldg(L.ydxs + k) : (sk.code == 2) ? 2 * sbar * __ldg(L.ydx + k)
+                       : (sk.code == 3) ? 2 * sbar * __ldg(L.ydx + k + 1) : 0.0;
+      // contributions to cells k-1, k, k+1 (k = i-1: A0 A1 A2; k = i: A1 A2 A3)
+      const double cm = (sk.code == 1 || sk.code == 2) ? -w : 0.0;
+      const double cc = v * phib + ((sk.code == 2) ? w : (sk.code == 3) ? -w : 0.0);
+      const double cp = (sk.code == 1 || sk.code == 3) ? w : 0.0;
+      if (neg) { A1 += cm; A2 += cc; A3 += cp; }
+      else { A0 += cm; A1 += cc; A2 += cp; }
       if (P.vbar && i >= j0 && i <= jend) {
-        const double f0 = sf[krow][ln];
-        const double vb = neg ? phib * (f0 - 0.5 * (dxf + vq) * sl - 0.5 * v * (dt * yhc) * sl)
-                              : phib * (f0 + 0.5 * (dxf - vq) * sl - 0.5 * v * (dt * yhc) * sl);
-        const long long fc = face(s, ln, i);
-        if (P.vacc) P.vbar[fc] += vb; else P.vbar[fc] = vb;
+        const double f0 = neg ? fp : fc;  // f(k)
+        const double vb = neg ? phib * (f0 - 0.5 * (dxf + vq) * sk.val - 0.5 * v * (dt * yhc) * sk.val)
+                              : phib * (f0 + 0.5 * (dxf - vq) * sk.val - 0.5 * v * (dt * yhc) * sk.val);
+        const long long fc_ = v0 + i * fstride;
+        if (P.vacc) P.vbar[fc_] += vb; else P.vbar[fc_] = vb;
+      }
+      // cell i-2 is final: its cotangent is obar plus the flux parts
+      if (i - 2 >= j0 && i - 2 <= jend) {
+        const long long q = c0 + (i - 2) * stride;
+        fb[q] = __ldg(ob + q) + A0;
+      }
+      A0 = A1;
+      A1 = A2;
+      A2 = A3;
+      A3 = 0.0;
+      fc = fp;
+      fp = fn;
+      sprev = scur;
+      kprev = kc;
+      qa = qb;
+      qb = qc;
+    }
+    // cells i1e-1 .. i1e+1 are final after the last face
+    const double Af[3] = {A0, A1, A2};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const int j = i1e - 1 + m;
+      if (j >= j0 && j <= jend) {
+        const long long q = c0 + j * stride;
+        fb[q] = __ldg(ob + q) + Af[m];
       }
     }
-    __syncthreads();
-    // S4: cells j0 .. jend gather from faces j-1 .. j+2
-    for (int e = tid; e < 32 * SVJ_R; e += SVJ_THREADS) {
-      int row, ln;
-      elem(e, row, ln);
-      const int j = j0 - 3 + row;
-      if (row < 3 || j > jend || q0 + ln >= nl) continue;
-      double acc = 0.0;
-#pragma unroll
-      for (int fr = row - 1; fr <= row + 2; ++fr) {
-        const int fl = sflag[fr][ln];
-        if (!(fl & 8)) continue;
-        const int kr = (fl & 4) ? fr : fr - 1;
-        const int code = fl & 3;
-        if (kr == row) acc += sdir[fr][ln];
-        const double wgt = sw[fr][ln];
-        if (code == 1) {
-          if (row == kr + 1) acc += wgt;
-          if (row == kr - 1) acc -= wgt;
-        } else if (code == 2) {
-          if (row == kr) acc += wgt;
-          if (row == kr - 1) acc -= wgt;
-        } else if (code == 3) {
-          if (row == kr + 1) acc += wgt;
-          if (row == kr) acc -= wgt;
+  }
+}
+
+// x1 sweep adjoints (several fields in one launch).  One warp per (x1 line, species, field),
+// lanes along the contiguous x1, the line walked in chunks of 32 positions p = -1 + 32c +
+// lane.  Each lane computes the slope branch of cell p and the cotangent parts of face p
+// (the upwind slope of face p is its own or lane p-1's, by shuffle, carried across chunks);
+// cell p-2 then gathers from faces p-3 .. p (the four that reach it) by shuffles from this
+// chunk and the previous one.  Face-velocity cotangents go to the field's own vbar slice.
+template <bool UNIT>
+__global__ void __launch_bounds__(256) k_sweep_vjp_x1(SweepVjpArgs P, SweepVjpFields FS) {
+  const GridDev& G = P.G;
+  const Dims d = G.d;
+  const int lx = d.lx1;
+  if (lx <= 1) return;
+  const double dt = *P.dtp;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const long long ncol = (long long)d.lx2 * d.lx3;
+  const long long nwarp = ncol * FS.nfs;
+  const Line1D& L = G.L[0];
+  const FaceTab& FT = G.F[0];
+  const long long nfaces = nf1(d);
+  const int nch = (lx + 4 + 31) / 32 + 1;  // one chunk past the line flushes its last cells
+  for (long long w = (long long)blockIdx.x * wpb + (threadIdx.x >> 5); w < nwarp; w += (long long)gridDim.x * wpb) {
+    const long long col = w % ncol;
+    int fld, s;
+    field_of(FS, (int)(w / ncol), fld, s);
+    const int frank = pick3(fld, FS.frank[0], FS.frank[1], FS.frank[2]);
+    (void)frank;  // x1 sweeps use the frank-0 metrics
+    const double* f = pick3(fld, FS.f[0], FS.f[1], FS.f[2]);
+    const double* ob = pick3(fld, FS.obar[0], FS.obar[1], FS.obar[2]);
+    double* fb = pick3(fld, FS.fbar[0], FS.fbar[1], FS.fbar[2]);
+    double* vbar = pick3(fld, FS.vbar[0], FS.vbar[1], FS.vbar[2]);
+    const int i2 = (int)(col % d.lx2) + 1, i3 = (int)(col / d.lx2) + 1;
+    const long long c0 = (long long)s * d.ng + gi(d, 0, i2, i3);        // cell 0 of the line
+    const long long v0 = (long long)s * nfaces + f1i(d, 1, i2, i3) - 1;  // face p at v0 + p
+    const long long m0 = cmi(G, 0, i2, i3);
+    const long long t0 = fmi(FT, 1, i2, i3) - FT.t1;                     // face metrics at t0 + p*t1
+    // carried from the previous chunk: slope and kappa*obar of position p-1 for lane 0, and
+    // the face contributions of lanes 29..31
+    int ccode = 0;
+    double cval = 0.0, ckob = 0.0;
+    double h1p = 0.0, h2p = 0.0, h3p = 0.0;
+    // f(p), obar(p), v(p) of the next chunk are loaded one chunk ahead
+    auto ldf = [&](int p) { return (p >= -1 && p <= lx + 2) ? __ldg(f + c0 + p) : 0.0; };
+    auto ldo = [&](int p) { return (p >= 1 && p <= lx) ? __ldg(ob + c0 + p) : 0.0; };
+    auto ldv = [&](int p) { return (p >= 1 && p <= lx + 1) ? __ldg(P.v + v0 + p) : 0.0; };
+    double f0n = ldf(lane - 1), obn = ldo(lane - 1), vn = ldv(lane - 1);
+    for (int c = 0; c < nch; ++c) {
+      const int p = -1 + 32 * c + lane;
+      const double f0 = f0n, obp = obn, vp = vn;
+      f0n = ldf(p + 32);
+      obn = ldo(p + 32);
+      vn = ldv(p + 32);
+      // slope of cell p (0 .. lx+1), from f(p-1), f(p), f(p+1)
+      double fm = __shfl_up_sync(0xffffffffu, f0, 1);
+      double fp = __shfl_down_sync(0xffffffffu, f0, 1);
+      if (lane == 0 && p - 1 >= -1) fm = __ldg(f + c0 + p - 1);
+      if (lane == 31 && p + 1 <= lx + 2) fp = __ldg(f + c0 + p + 1);
+      SlopeBr sc;
+      sc.code = 0;
+      sc.val = 0.0;
+      if (p >= 0 && p <= lx + 1) sc = slope_br(L, p, fm, f0, fp);
+      // kappa*obar of cell p (0 outside 1..lx)
+      double kc = 0.0;
+      if (p >= 1 && p <= lx) {
+        const double y = UNIT ? 1.0 : __ldg(G.yha1_0 + m0 + p);
+        kc = dt * __ldg(L.ydxi + p - 1) * y * obp;
+      }
+      // the same of position p-1
+      int pcode = __shfl_up_sync(0xffffffffu, sc.code, 1);
+      double pval = __shfl_up_sync(0xffffffffu, sc.val, 1);
+      double pkob = __shfl_up_sync(0xffffffffu, kc, 1);
+      if (lane == 0) { pcode = ccode; pval = cval; pkob = ckob; }
+      // face p (1 .. lx+1): contributions to cells k-1, k, k+1 of its upwind cell k, as the
+      // parts cell p-2 collects from the faces 3, 2, 1, 0 lanes up the line (g3 .. g0)
+      double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
+      if (p >= 1 && p <= lx + 1) {
+        const double v = vp;
+        double ha2 = 1.0, yhc = 1.0;
+        if (!UNIT) {
+          ha2 = __ldg(FT.ha2i0 + t0 + p * FT.t1);
+          yhc = __ldg(FT.yhc + t0 + p * FT.t1);
+        }
+        const double phib = ha2 * (kc - pkob);
+        const double dxf = __ldg(L.dx + p);
+        const double vq = v * yhc * dt;
+        const bool neg = v < 0;
+        const int code = neg ? sc.code : pcode;
+        const double sl = neg ? sc.val : pval;
+        const int k = neg ? p : p - 1;
+        const double sbar = neg ? -0.5 * v * (dxf + vq) * phib : 0.5 * v * (dxf - vq) * phib;
+        const double wt = (code == 1) ? sbar * __ldg(L.ydxs + k) : (code == 2) ? 2 * sbar * __ldg(L.ydx + k)
+                          : (code == 3) ? 2 * sbar * __ldg(L.ydx + k + 1) : 0.0;
+        const double cm = (code == 1 || code == 2) ? -wt : 0.0;
+        const double cc = v * phib + ((code == 2) ? wt : (code == 3) ? -wt : 0.0);
+        const double cp = (code == 1 || code == 3) ? wt : 0.0;
+        // g_m: the part for cell p-2+m (gathered by the lane m up the line)
+        if (neg) { g3 = cp; g2 = cc; g1 = cm; g0 = 0.0; }
+        else { g3 = 0.0; g2 = cp; g1 = cc; g0 = cm; }
+        if (vbar) {
+          const double fk = neg ? f0 : fm;  // f(k)
+          const double vb = neg ? phib * (fk - 0.5 * (dxf + vq) * sl - 0.5 * v * (dt * yhc) * sl)
+                                : phib * (fk + 0.5 * (dxf - vq) * sl - 0.5 * v * (dt * yhc) * sl);
+          if (P.vacc) vbar[v0 + p] += vb; else vbar[v0 + p] = vb;
         }
       }
-      if (acc != 0.0) P.fbar[so + sbase[ln] + (long long)j * stride] += acc;
+      // cell p-2 gathers g3 of face p-3, g2 of face p-2, g1 of face p-1 and its own g0 of face p
+      double acc = g0;
+      {
+        const int src1 = (lane - 1) & 31, src2 = (lane - 2) & 31, src3 = (lane - 3) & 31;
+        const double a1 = __shfl_sync(0xffffffffu, g1, src1), b1 = __shfl_sync(0xffffffffu, h1p, src1);
+        const double a2 = __shfl_sync(0xffffffffu, g2, src2), b2 = __shfl_sync(0xffffffffu, h2p, src2);
+        const double a3 = __shfl_sync(0xffffffffu, g3, src3), b3 = __shfl_sync(0xffffffffu, h3p, src3);
+        acc += (lane >= 1) ? a1 : b1;
+        acc += (lane >= 2) ? a2 : b2;
+        acc += (lane >= 3) ? a3 : b3;
+      }
+      const int pc = p - 2;
+      if (pc >= -1 && pc <= lx + 2) fb[c0 + pc] = __ldg(ob + c0 + pc) + acc;
+      // carry to the next chunk
+      ccode = __shfl_sync(0xffffffffu, sc.code, 31);
+      cval = __shfl_sync(0xffffffffu, sc.val, 31);
+      ckob = __shfl_sync(0xffffffffu, kc, 31);
+      h1p = g1;
+      h2p = g2;
+      h3p = g3;
     }
-    __syncthreads();
   }
 }
 
