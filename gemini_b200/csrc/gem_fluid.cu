@@ -315,26 +315,29 @@ int launch_diffusion_vjp(const gem_grid* g, DiffAdjArgs a, cudaStream_t st) {
   const int M = std::max(2, (d.lx1 + 31) / 32);
   a.M = M;
   const size_t per_warp = (size_t)VNA * M * 32 * sizeof(double);
-  const int wpb = (int)std::min<size_t>(4, (227 * 1024) / per_warp);
-  if (wpb < 1) return set_err(GEM_EINVAL, "lx1=%d too long for the on-chip column adjoint", d.lx1);
+  if (per_warp > 227 * 1024) return set_err(GEM_EINVAL, "lx1=%d too long for the on-chip column adjoint", d.lx1);
+  auto kern = g->dev.unit ? k_diffusion_vjp<true> : k_diffusion_vjp<false>;
+  // warps per block: the choice (4, 2 or 1) that keeps the most warps resident per SM
+  int wpb = 1, best = 0, best_per_sm = 1;
+  for (int w : {4, 2, 1}) {
+    const size_t sm = per_warp * w;
+    if (sm > 227 * 1024) continue;
+    GEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int per_sm = 0;
+    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * w, sm));
+    if (per_sm * w > best) {
+      best = per_sm * w;
+      wpb = w;
+      best_per_sm = per_sm;
+    }
+  }
   const size_t smem = per_warp * wpb;
+  GEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
   long long nblk = (ncs + wpb - 1) / wpb;
-  int per_sm = 0;
-  if (g->dev.unit) {
-    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_vjp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion_vjp<true>, 32 * wpb, smem));
-  } else {
-    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_vjp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion_vjp<false>, 32 * wpb, smem));
-  }
-  if (per_sm < 1) per_sm = 1;
-  const long long cap = (long long)num_sms() * per_sm;
+  const long long cap = (long long)num_sms() * std::max(best_per_sm, 1);
   if (nblk > cap) nblk = cap;
-  if (g->dev.unit)
-    k_diffusion_vjp<true><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
-  else
-    k_diffusion_vjp<false><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
+  kern<<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
   GEM_LAUNCHED("k_diffusion_vjp");
   return GEM_OK;
 }

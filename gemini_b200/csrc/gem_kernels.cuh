@@ -1369,6 +1369,60 @@ __device__ __forceinline__ void band_solve(const WM& W, int M, int lane, RowM ro
   W.at(ARR, M - 1) = xl;
 }
 
+// Solve with the transposed matrix, A^T y = g (g in ARR, replaced by y), reusing A's
+// factorisation: band_solve is a fixed sequence of linear operations r -> A^-1 r (lane-block
+// eliminations, the interface reduction, the cyclic-reduction levels, back substitution), so
+// A^-T g is that sequence transposed and applied in reverse order -- every axpy y_j += m y_i
+// becomes y_i += m y_j and every shuffle up becomes a shuffle down.  rowm gives A's rows.
+template <class WM, class RowM>
+__device__ __forceinline__ void band_solve_T(const WM& W, int M, int lane, RowM rowm, const IfaceLU& F,
+                                             int ARR) {
+  double a, b, c;
+  // back substitution: x(k) = (r(k) - SS x0 - TT xl) IB (k = 1..M-2), x(0) = x0, x(M-1) = xl
+  double x0b = W.at(ARR, 0), xlb = W.at(ARR, M - 1);
+  for (int k = 1; k <= M - 2; ++k) {
+    const double gk = W.at(ARR, k) * W.ib(k);
+    x0b -= W.ss(k) * gk;
+    xlb -= W.tt(k) * gk;
+    W.at(ARR, k) = gk;
+  }
+  // x0 = (loR - loA xl(lane-1) - loC xl) iloB, xl = R ihiB
+  double loRb = x0b * F.iloB;
+  double t = __shfl_down_sync(0xffffffffu, -F.loA * F.iloB * x0b, 1);
+  if (lane == 31) t = 0.0;
+  xlb += -F.loC * F.iloB * x0b + t;
+  double Rb = xlb * F.ihiB;
+  // cyclic-reduction levels, last first: R = R - k1 R(lane-sh) - k2 R(lane+sh)
+#pragma unroll
+  for (int lv = 4; lv >= 0; --lv) {
+    const int sh = 1 << lv;
+    double t1 = __shfl_down_sync(0xffffffffu, F.k1[lv] * Rb, sh);
+    double t2 = __shfl_up_sync(0xffffffffu, F.k2[lv] * Rb, sh);
+    if (lane + sh > 31) t1 = 0.0;
+    if (lane < sh) t2 = 0.0;
+    Rb = Rb - t1 - t2;
+  }
+  // R = hiR - e1 loR - e2 loR(lane+1)
+  loRb += -F.e1 * Rb;
+  double u = __shfl_up_sync(0xffffffffu, -F.e2 * Rb, 1);
+  if (lane == 0) u = 0.0;
+  loRb += u;
+  // loR = r(0) - g0 r(1); hiR = r(M-1) after the downward elimination
+  if (M >= 3) W.at(ARR, 1) += -F.g0 * loRb;
+  W.at(ARR, 0) = loRb;
+  W.at(ARR, M - 1) = Rb;
+  // upward elimination r(k) -= c(k) IB(k+1) r(k+1) (k = M-3 .. 1), transposed and reversed
+  for (int k = 1; k <= M - 3; ++k) {
+    rowm(k, a, b, c);
+    W.at(ARR, k + 1) += -c * W.ib(k + 1) * W.at(ARR, k);
+  }
+  // downward elimination r(k) -= a(k) IB(k-1) r(k-1) (k = 2 .. M-1), transposed and reversed
+  for (int k = M - 1; k >= 2; --k) {
+    rowm(k, a, b, c);
+    W.at(ARR, k - 1) += -a * W.ib(k - 1) * W.at(ARR, k);
+  }
+}
+
 // exact-error accumulation for the refinement residual r - (a xm + b x + c xp)
 __device__ __forceinline__ double residual3(double r, double a, double xm, double b, double x, double c, double xp) {
   const double p1 = a * xm, e1 = __fma_rn(a, xm, -p1);
@@ -1694,9 +1748,9 @@ __global__ void k_diffusion_ghost_floor(GridDev G, Blocks B) {
 // 7b. Adjoint (vector-Jacobian product) of the energy diffusion, for the differentiable
 //     path.  One warp per (x1 column, species), lanes owning blocks of M consecutive rows,
 //     as in the forward solver: the kernel recomputes the per-row conduction factors
-//     q-, q+, bq (with the partial derivatives of lambda(T, n) and C(n)), both TRBDF2
-//     stage solutions X and Y, then solves the transposed stage systems with the same
-//     lane-blocked band solver and chains the cotangents of the band entries and
+//     q-, q+, bq, both TRBDF2 stage solutions X and Y, then solves the transposed stage
+//     systems by the transpose of the lane-blocked band solve (reusing each stage's
+//     factorisation) and chains the cotangents of the band entries and
 //     right-hand sides back through q+-, Dh, C, B and lambda to T, n and the column's
 //     exospheric boundary value.  Every per-row array lives in shared memory; T, n, Ybar,
 //     Tbar and nbar move along x1 (coalesced).  Cotangent inputs/outputs are ghosted
@@ -1724,11 +1778,10 @@ struct DiffAdjArgs {
 // per-row shared-memory arrays of the adjoint (row-interleaved as WarpMem).  Slots are
 // reused once their first content is dead: D becomes the stage-1 solution X, Y becomes the
 // temperature cotangent TB, R carries Ybar -> lambda2 -> xbar -> lambda1, and after the
-// last pass QMB / QPB / BQB hold EM / EP / the density cotangent.
-constexpr int VA_T = 0, VA_C = 1, VA_DDT = 2, VA_DDN = 3, VA_DCN = 4, VA_BQ = 5, VA_QM = 6, VA_QP = 7,
-              VA_X = 8, VA_SS = 9, VA_IB = 10, VA_TT = 11, VA_Y = 12, VA_R = 13, VA_QMB = 14, VA_QPB = 15,
-              VA_BQB = 16;
-constexpr int VNA = 17;
+// first-stage pass QMB / QPB / BQB hold EM / EP / the C cotangent.
+constexpr int VA_T = 0, VA_C = 1, VA_BQ = 2, VA_QM = 3, VA_QP = 4, VA_X = 5, VA_SS = 6, VA_IB = 7, VA_TT = 8,
+              VA_Y = 9, VA_R = 10, VA_QMB = 11, VA_QPB = 12, VA_BQB = 13;
+constexpr int VNA = 14;
 constexpr int VA_D = VA_X, VA_TB = VA_Y;
 
 struct WarpMemA {
@@ -1740,6 +1793,30 @@ struct WarpMemA {
   __device__ __forceinline__ double& ib(int k) const { return at(VA_IB, k); }
   __device__ __forceinline__ double& tt(int k) const { return at(VA_TT, k); }
 };
+
+// thermal conductivity lambda(T, n) (collisions.f90:162-199) and its partial derivatives;
+// q: the cell in the interior-only neutral arrays (electrons)
+__device__ __forceinline__ void lam_deriv(const DiffAdjArgs& P, int s, double T, double nv, long long q,
+                                          long long nc, double& lam, double& dl_dT, double& dl_dn) {
+  const double T25 = pow25(T);
+  if (s < LSP - 1) {
+    lam = c_tcoef[s] * T25;
+    dl_dT = 2.5 * lam / T;
+    dl_dn = 0.0;
+    return;
+  }
+  const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
+  const double sq = sqrt(T);
+  const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
+                   n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
+  const double Xp = n1 * 1.1e-16 * 5.7e-4 + n2 * 2.82e-17 * (0.5 / sq * (1 - 1.21e-4 * T) - 1.21e-4 * sq) +
+                    n3 * 2.2e-16 * 3.6e-2 * 0.5 / sq;
+  const double den = 1 + 3.22e4 * (T * T) / nv * X;
+  lam = ELCHRG * 100 * 7.7e5 * T25 / den;
+  const double dden_dT = 3.22e4 * (2 * T * X + T * T * Xp) / nv;
+  dl_dT = lam * (2.5 / T - dden_dT / den);
+  dl_dn = lam * (3.22e4 * T * T * X / (nv * nv)) / den;
+}
 
 template <bool UNIT>
 __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
@@ -1772,12 +1849,12 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
     const double* Tc = P.T + (long long)s * d.ng + m0;
     const double* nsc = P.ns + (long long)s * d.ng + m0;
     const double c0 = (c_gammas[s] - 1.0) / KB;
-    // ---- pass 1 (along x1): T, D = lambda h2 h3 / h1 with dD/dT, dD/dn, C with dC/dn, bq
+    // ---- pass 1 (along x1): T, D = lambda h2 h3 / h1, C, bq
     {
       int lp = lp0, kp = kp0;
       for (int c = 0; c < M; ++c) {
         const int i = 1 + 32 * c + lane;
-        double T = 0, D = 0, C = 0, ddt = 0, ddn = 0, dcn = 0, bq = 0;
+        double T = 0, D = 0, C = 0, bq = 0;
         if (i <= n) {
           T = Tc[i];
           const double nv = nsc[i];
@@ -1785,31 +1862,10 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
           const double h1v = UNIT ? 1.0 : __ldg(G.h1 + mk);
           const double h23 = UNIT ? 1.0 : __ldg(G.h2 + mk) * __ldg(G.h3 + mk);
           const double ha1 = UNIT ? 1.0 : __ldg(G.ha1_0 + mk);
-          const double T25 = pow25(T);
-          double lam, dl_dT, dl_dn = 0.0;
-          if (s < LSP - 1) {
-            lam = c_tcoef[s] * T25;
-            dl_dT = 2.5 * lam / T;
-          } else {
-            const long long q = q0 + i;
-            const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
-            const double sq = sqrt(T);
-            const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
-                             n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
-            const double Xp = n1 * 1.1e-16 * 5.7e-4 + n2 * 2.82e-17 * (0.5 / sq * (1 - 1.21e-4 * T) - 1.21e-4 * sq) +
-                              n3 * 2.2e-16 * 3.6e-2 * 0.5 / sq;
-            const double den = 1 + 3.22e4 * (T * T) / nv * X;
-            lam = ELCHRG * 100 * 7.7e5 * T25 / den;
-            const double dden_dT = 3.22e4 * (2 * T * X + T * T * Xp) / nv;
-            dl_dT = lam * (2.5 / T - dden_dT / den);
-            dl_dn = lam * (3.22e4 * T * T * X / (nv * nv)) / den;
-          }
-          const double g = h23 / h1v;
-          D = lam * g;
-          ddt = dl_dT * g;
-          ddn = dl_dn * g;
+          double lam, dl_dT, dl_dn;
+          lam_deriv(P, s, T, nv, q0 + i, nc, lam, dl_dT, dl_dn);
+          D = lam * h23 / h1v;
           C = c0 / fmax_f(nv, MINDENSDIV) / ha1;
-          dcn = (nv > MINDENSDIV) ? -C / nv : 0.0;
           if (s == LSP - 1 && i >= 2 && i <= n - 1) {
             const double beta = 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i];  // collisions.f90:197
             bq = C * beta / h1v / (__ldg(L1.dx + i + 1) + __ldg(L1.dx + i));
@@ -1818,9 +1874,6 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
         W.at_lane(VA_T, kp, lp) = T;
         W.at_lane(VA_D, kp, lp) = D;
         W.at_lane(VA_C, kp, lp) = C;
-        W.at_lane(VA_DDT, kp, lp) = ddt;
-        W.at_lane(VA_DDN, kp, lp) = ddn;
-        W.at_lane(VA_DCN, kp, lp) = dcn;
         W.at_lane(VA_BQ, kp, lp) = bq;
         kp += r32;
         lp += q32;
@@ -1840,20 +1893,18 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
       return (ll < 0 || ll > 31) ? 0.0 : W.at_lane(arr, kk, ll);
     };
     // ---- q-, q+ per slot (rows 2..n-1): Dh(i) = (D(i-1) + D(i))/2
-    {
-      for (int k = 0; k < M; ++k) {
-        const int i = 1 + lane * M + k;
-        double qm = 0.0, qp = 0.0;
-        if (i >= 2 && i <= n - 1) {
-          const double Dm = nb(VA_D, k, -1), Dc = W.at(VA_D, k), Dp = nb(VA_D, k, 1);
-          const double C = W.at(VA_C, k);
-          const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
-          qm = C * (0.5 * (Dm + Dc)) / dxi / dxm;
-          qp = C * (0.5 * (Dc + Dp)) / dxi / dxp;
-        }
-        W.at(VA_QM, k) = qm;
-        W.at(VA_QP, k) = qp;
+    for (int k = 0; k < M; ++k) {
+      const int i = 1 + lane * M + k;
+      double qm = 0.0, qp = 0.0;
+      if (i >= 2 && i <= n - 1) {
+        const double Dm = nb(VA_D, k, -1), Dc = W.at(VA_D, k), Dp = nb(VA_D, k, 1);
+        const double C = W.at(VA_C, k);
+        const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
+        qm = C * (0.5 * (Dm + Dc)) / dxi / dxm;
+        qp = C * (0.5 * (Dc + Dp)) / dxi / dxp;
       }
+      W.at(VA_QM, k) = qm;
+      W.at(VA_QP, k) = qp;
     }
     __syncwarp();
     // Dirichlet values (diffusion.f90:54-79)
@@ -1882,47 +1933,31 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
         c = -qp - bq;
       }
     };
-    auto row0 = [&](int k, double& a, double& b, double& c) { row_at(0, k, lane, a, b, c); };
-    auto row1 = [&](int k, double& a, double& b, double& c) { row_at(1, k, lane, a, b, c); };
-    // the transposed matrix: sub-diagonal c(i-1), diagonal b(i), super-diagonal a(i+1)
-    auto rowT = [&](int stage, int k, double& a, double& b, double& c) {
-      double x, y, z;
-      row_at(stage, k, lane, x, b, z);
-      int kk = k - 1, ll = lane;
-      if (kk < 0) { kk = M - 1; --ll; }
-      row_at(stage, kk, ll, x, y, z);
-      a = z;
-      kk = k + 1;
-      ll = lane;
-      if (kk >= M) { kk = 0; ++ll; }
-      row_at(stage, kk, ll, x, y, z);
-      c = x;
-    };
-    auto row0T = [&](int k, double& a, double& b, double& c) { rowT(0, k, a, b, c); };
-    auto row1T = [&](int k, double& a, double& b, double& c) { rowT(1, k, a, b, c); };
+    // one row function for both stages (the band solver is instantiated once)
+    int stage = 0;
+    auto rowf = [&](int k, double& a, double& b, double& c) { row_at(stage, k, lane, a, b, c); };
     IfaceLU F;
     // ---- forward replay: first stage into X (the slot of D, now dead)
-    {
-      for (int k = 0; k < M; ++k) {
-        const int i = 1 + lane * M + k;
-        double r;
-        if (i == 1) r = tmin;
-        else if (i == n) r = tmax;
-        else if (i > n) r = 0.0;
-        else if (trbdf) {
-          double a, b, c;
-          row0(k, a, b, c);
-          const double qm = W.at(VA_QM, k), qp = W.at(VA_QP, k);
-          const double Tv = W.at(VA_T, k);
-          r = Tv / (dt / 2) - a * nb(VA_T, k, -1) - (qp / 2 + qm / 2) * Tv - c * nb(VA_T, k, 1);
-        } else {
-          r = W.at(VA_T, k) / dt;
-        }
-        W.at(VA_X, k) = r;
+    for (int k = 0; k < M; ++k) {
+      const int i = 1 + lane * M + k;
+      double r;
+      if (i == 1) r = tmin;
+      else if (i == n) r = tmax;
+      else if (i > n) r = 0.0;
+      else if (trbdf) {
+        double a, b, c;
+        row_at(0, k, lane, a, b, c);
+        const double qm = W.at(VA_QM, k), qp = W.at(VA_QP, k);
+        const double Tv = W.at(VA_T, k);
+        r = Tv / (dt / 2) - a * nb(VA_T, k, -1) - (qp / 2 + qm / 2) * Tv - c * nb(VA_T, k, 1);
+      } else {
+        r = W.at(VA_T, k) / dt;
       }
+      W.at(VA_X, k) = r;
     }
-    band_factor(W, M, lane, row0, F);
-    band_solve(W, M, lane, row0, F, VA_X);
+    stage = 0;
+    band_factor(W, M, lane, rowf, F);
+    band_solve(W, M, lane, rowf, F, VA_X);
     __syncwarp();
     int YOUT = VA_X;
     if (trbdf) {
@@ -1935,8 +1970,9 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
         else r = -(1 / 3.0 * W.at(VA_T, k) / (dt / 3)) + 4 / 3.0 * W.at(VA_X, k) / (dt / 3);
         W.at(VA_Y, k) = r;
       }
-      band_factor(W, M, lane, row1, F);
-      band_solve(W, M, lane, row1, F, VA_Y);
+      stage = 1;
+      band_factor(W, M, lane, rowf, F);
+      band_solve(W, M, lane, rowf, F, VA_Y);
       YOUT = VA_Y;
     }
     __syncwarp();
@@ -1961,9 +1997,9 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
     double tminb = 0.0, tmaxb = 0.0;  // on the lanes that own rows 1 and n
     const int lane_n = (n - 1) / M, k_n = (n - 1) - lane_n * M;
     if (trbdf) {
-      // lambda2 = A2^-T g; then the BDF2 cotangents of q-, q+, bq and T, and xbar
-      band_factor(W, M, lane, row1T, F);
-      band_solve(W, M, lane, row1T, F, VA_R);
+      // lambda2 = A2^-T g (A2's factorisation is still in place); then the BDF2 cotangents
+      // of q-, q+, bq and T, and xbar
+      band_solve_T(W, M, lane, rowf, F, VA_R);
       __syncwarp();
       if (lane == 0) tminb += W.at(VA_R, 0);
       if (lane == lane_n) tmaxb += W.at(VA_R, k_n);
@@ -2001,13 +2037,14 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
       }
     }
     __syncwarp();
-    // lambda1 = A1^-T xbar (or A^-T g for backward Euler)
-    band_factor(W, M, lane, row0T, F);
-    band_solve(W, M, lane, row0T, F, VA_R);
+    // lambda1 = A1^-T xbar (or A^-T g for backward Euler, whose factorisation is in place)
+    stage = 0;
+    if (trbdf) band_factor(W, M, lane, rowf, F);
+    band_solve_T(W, M, lane, rowf, F, VA_R);
     __syncwarp();
     if (lane == 0) tminb += W.at(VA_R, 0);
     if (lane == lane_n) tmaxb += W.at(VA_R, k_n);
-    // first-stage cotangents, then EM / EP (the Dh cotangent parts) and the C part of nbar
+    // first-stage cotangents, then EM / EP (the Dh cotangent parts) and the C cotangent
     for (int k = 0; k < M; ++k) {
       const int i = 1 + lane * M + k;
       if (i > n) continue;
@@ -2029,7 +2066,7 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
           tb += -nb(VA_R, k, -1) * c;
         }
       }
-      double em = 0.0, ep = 0.0, nbc = 0.0;
+      double em = 0.0, ep = 0.0, cb = 0.0;
       if (i >= 2 && i <= n - 1) {
         const double l1 = W.at(VA_R, k);
         const double qm = W.at(VA_QM, k), qp = W.at(VA_QP, k), bq = W.at(VA_BQ, k);
@@ -2037,16 +2074,16 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
         double qmb = W.at(VA_QMB, k), qpb = W.at(VA_QPB, k), bqb = W.at(VA_BQB, k);
         if (trbdf) {
           const double Tm = nb(VA_T, k, -1), Tv = W.at(VA_T, k), Tp = nb(VA_T, k, 1);
-          const double ab = -l1 * (xm + Tm), cb = -l1 * (xp + Tp), bb = -l1 * xc, pb = -l1 * Tv;
+          const double ab = -l1 * (xm + Tm), cbv = -l1 * (xp + Tp), bb = -l1 * xc, pb = -l1 * Tv;
           qmb += -ab / 2 + bb / 2 + pb / 2;
-          qpb += -cb / 2 + bb / 2 + pb / 2;
-          bqb += ab / 2 - cb / 2;
+          qpb += -cbv / 2 + bb / 2 + pb / 2;
+          bqb += ab / 2 - cbv / 2;
           tb += l1 * (dA - (qp / 2 + qm / 2));
         } else {
-          const double ab = -l1 * xm, cb = -l1 * xp, bb = -l1 * xc;
+          const double ab = -l1 * xm, cbv = -l1 * xp, bb = -l1 * xc;
           qmb += -ab + bb;
-          qpb += bb - cb;
-          bqb += ab - cb;
+          qpb += bb - cbv;
+          bqb += ab - cbv;
           tb += l1 * dA;
         }
         // q- = C Dh(i) / (dxi dx(i)), q+ = C Dh(i+1) / (dxi dx(i+1)), bq = C beta/h1/(dx(i)+dx(i+1))
@@ -2054,27 +2091,16 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
         const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
         em = qmb * C / (dxi * dxm);  // -> Dh(i)
         ep = qpb * C / (dxi * dxp);  // -> Dh(i+1)
-        const double Cb = (qmb * qm + qpb * qp + bqb * bq) / C;
-        nbc = Cb * W.at(VA_DCN, k);
+        cb = (qmb * qm + qpb * qp + bqb * bq) / C;
       }
       W.at(VA_TB, k) = tb;
       W.at(VA_QMB, k) = em;
       W.at(VA_QPB, k) = ep;
-      W.at(VA_BQB, k) = nbc;
+      W.at(VA_BQB, k) = cb;
     }
     __syncwarp();
-    // D(i) feeds Dh(i) (i >= 2) and Dh(i+1) (i < n); Dh(j) collects EM(j) and EP(j-1)
-    for (int k = 0; k < M; ++k) {
-      const int i = 1 + lane * M + k;
-      if (i > n) continue;
-      const double dh_i = (i >= 2) ? W.at(VA_QMB, k) + nb(VA_QPB, k, -1) : 0.0;
-      const double dh_ip1 = (i < n) ? nb(VA_QMB, k, 1) + W.at(VA_QPB, k) : 0.0;
-      const double Db = 0.5 * (dh_i + dh_ip1);
-      W.at(VA_R, k) = W.at(VA_TB, k) + Db * W.at(VA_DDT, k);   // Tbar
-      W.at(VA_C, k) = W.at(VA_BQB, k) + Db * W.at(VA_DDN, k);  // nbar
-    }
-    __syncwarp();
-    // ---- Tbar, nbar along x1
+    // ---- along x1: D(i) feeds Dh(i) (i >= 2) and Dh(i+1) (i < n), Dh(j) collects EM(j) and
+    // EP(j-1); then through lambda(T, n) and C(n) to Tbar, nbar
     {
       double* Tbo = P.Tbar + (long long)s * d.ng + m0;
       double* nbo = P.nbar + (long long)s * d.ng + m0;
@@ -2082,8 +2108,20 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
       for (int c = 0; c < M; ++c) {
         const int i = 1 + 32 * c + lane;
         if (i <= n) {
-          Tbo[i] = W.at_lane(VA_R, kp, lp);
-          nbo[i] = W.at_lane(VA_C, kp, lp);
+          int km = kp - 1, lm = lp, kq = kp + 1, lq = lp;
+          if (km < 0) { km = M - 1; --lm; }
+          if (kq >= M) { kq = 0; ++lq; }
+          const double dh_i = (i >= 2) ? W.at_lane(VA_QMB, kp, lp) + W.at_lane(VA_QPB, km, lm) : 0.0;
+          const double dh_ip1 = (i < n) ? W.at_lane(VA_QMB, kq, lq) + W.at_lane(VA_QPB, kp, lp) : 0.0;
+          const double Db = 0.5 * (dh_i + dh_ip1);
+          const double T = W.at_lane(VA_T, kp, lp), nv = nsc[i];
+          const long long mk = mm0 + i;
+          const double g = UNIT ? 1.0 : __ldg(G.h2 + mk) * __ldg(G.h3 + mk) / __ldg(G.h1 + mk);
+          double lam, dl_dT, dl_dn;
+          lam_deriv(P, s, T, nv, q0 + i, nc, lam, dl_dT, dl_dn);
+          const double dcn = (nv > MINDENSDIV) ? -W.at_lane(VA_C, kp, lp) / nv : 0.0;
+          Tbo[i] = W.at_lane(VA_TB, kp, lp) + Db * dl_dT * g;
+          nbo[i] = W.at_lane(VA_BQB, kp, lp) * dcn + Db * dl_dn * g;
         }
         kp += r32;
         lp += q32;
