@@ -44,7 +44,8 @@ class DiffProblem:
         self.cuda_diffusion_adjoint = bool(cuda_diffusion_adjoint)
         self.cuda_sweep_adjoint = bool(cuda_sweep_adjoint)
         self.cuda_step_adjoint = bool(cuda_step_adjoint)
-        self._sa = None  # gem_step_adjoint workspace, made on first use
+        self._sa = None  # gem_step_adjoint workspaces (two, for the pipelined backward), made on first use
+        self._side = None  # the replay stream of the pipelined backward
         self._dtt = {}
         self._capturing = False
         self._graphs = {}  # (Ttop given) -> captured step VJP
@@ -224,35 +225,96 @@ class DiffProblem:
         return self._vjp_body(inp, tt, self.dt_tensor(j), cot, use_cuda_diffusion_adjoint)
 
     def step_vjp_cuda(self, state, Ttop, j, cot):
-        """The step VJP by gem_step_vjp_dev: forward replay and every adjoint piece on the
-        device.  Cotangents at ghost cells of the step's outputs are ignored (the next step
-        never reads them); the state's ghost cells get zero."""
-        import torch
+        """The step VJP in CUDA (the replay and backward halves of gem_step_vjp_dev): forward
+        replay and every adjoint piece on the device.  Cotangents at ghost cells of the step's
+        outputs are ignored (the next step never reads them); the state's ghost cells get
+        zero."""
+        state = tuple(t.detach().contiguous() for t in state)
+        self._set_top(Ttop)
+        self._replay(0, state, j)
+        return self._backward(0, state, Ttop, j, cot)
 
+    def _workspace(self, i):
         if self._sa is None:
+            self._sa = [None, None]
+        if self._sa[i] is None:
             h = ctypes.c_void_p()
             _lib.check(_lib.lib().gem_step_adjoint_create(self.dg.handle, ctypes.byref(h)))
-            self._sa = h
-        ns, vs1, Ts, lo, hi = (t.detach().contiguous() for t in state)
-        z = [torch.zeros_like(t) if c is None else c.detach().contiguous()
-             for c, t in zip(cot, (ns, vs1, Ts, lo, hi))]
-        out = [torch.empty_like(t) for t in (ns, vs1, Ts, lo, hi)]
+            self._sa[i] = h
+        return self._sa[i]
+
+    def _replay(self, i, state, j):
+        """gem_step_vjp_replay_dev of step j into workspace i, on the current stream."""
+        ns, vs1, Ts, lo, hi = state
+        p = F._ptr
+        c = self.cfg.c()
+        _lib.check(_lib.lib().gem_step_vjp_replay_dev(
+            ctypes.byref(c), self.dg.handle, self.ds.work, self._workspace(i), p(ns), p(vs1), p(self.vs2),
+            p(self.vs3), p(Ts), p(lo), p(hi), p(self.dt_tensor(j)), F._stream()))
+
+    def _backward(self, i, state, Ttop, j, cot):
+        """gem_step_vjp_backward_dev of step j from workspace i (replayed), on the current stream."""
+        import torch
+
+        ns, vs1, Ts, lo, hi = state
+        z = [torch.zeros_like(t) if c is None else c.detach().contiguous() for c, t in zip(cot, state)]
+        out = [torch.empty_like(t) for t in state]
         tb = torch.empty((self.grid.lx3, self.grid.lx2), dtype=torch.float64, device=ns.device) \
             if Ttop is not None else None
-        self._set_top(Ttop)
-        c = self.cfg.c()
         p = F._ptr
-        _lib.check(_lib.lib().gem_step_vjp_dev(
-            ctypes.byref(c), self.dg.handle, self.ds.work, self._sa, p(ns), p(vs1), p(self.vs2), p(self.vs3),
-            p(Ts), p(lo), p(hi), p(self.ds.electrovars), p(self.dt_tensor(j)), p(z[0]), p(z[1]), p(z[2]),
-            p(z[3]), p(z[4]), p(out[0]), p(out[1]), p(out[2]), p(out[3]), p(out[4]),
-            None if tb is None else p(tb), F._stream()))
+        c = self.cfg.c()
+        _lib.check(_lib.lib().gem_step_vjp_backward_dev(
+            ctypes.byref(c), self.dg.handle, self.ds.work, self._workspace(i), p(ns), p(vs1), p(Ts), p(lo), p(hi),
+            p(self.ds.electrovars), p(self.dt_tensor(j)), p(z[0]), p(z[1]), p(z[2]), p(z[3]), p(z[4]),
+            p(out[0]), p(out[1]), p(out[2]), p(out[3]), p(out[4]), None if tb is None else p(tb), F._stream()))
         return out, tb
 
+    def backward_segment_cuda(self, states, j0, Ttop, cot):
+        """Pull cot back through the steps j0 .. j0+len(states)-1 (states[m]: the state before
+        step j0+m), last step first: the replay of step j-1 runs on a side stream into the
+        other workspace while step j's backward runs.  Returns (cot, g_top)."""
+        import torch
+
+        main = torch.cuda.current_stream()
+        if self._side is None:
+            self._side = torch.cuda.Stream()
+        side = self._side
+        states = [tuple(t.detach().contiguous() for t in st) for st in states]
+        self._set_top(Ttop)
+        n = len(states)
+        for m in range(n):  # the cached dt tensors, made on the main stream before the fork
+            self.dt_tensor(j0 + m)
+        side.wait_stream(main)  # the states were recomputed on the main stream
+        ev_rep, ev_back = [None] * n, [None] * n
+        g_top = None
+
+        def replay(m):
+            with torch.cuda.stream(side):
+                if m + 2 < n:  # workspace m % 2 was last read by the backward of step m+2
+                    side.wait_event(ev_back[m + 2])
+                self._replay(m % 2, states[m], j0 + m)
+                ev_rep[m] = torch.cuda.Event()
+                ev_rep[m].record(side)
+
+        replay(n - 1)
+        for m in range(n - 1, -1, -1):
+            if m >= 1:
+                replay(m - 1)
+            main.wait_event(ev_rep[m])
+            cot, gt = self._backward(m % 2, states[m], Ttop, j0 + m, cot)
+            ev_back[m] = torch.cuda.Event()
+            ev_back[m].record(main)
+            if gt is not None:
+                g_top = gt if g_top is None else g_top + gt
+        main.wait_stream(side)
+        return cot, g_top
+
     def close(self):
-        """Release the step adjoint workspace."""
+        """Release the step adjoint workspaces."""
         if self._sa is not None:
-            _lib.lib().gem_step_adjoint_destroy(self._sa)
+            for h in self._sa:
+                if h is not None:
+                    _lib.lib().gem_step_adjoint_destroy(h)
             self._sa = None
 
     def __del__(self):
@@ -418,6 +480,11 @@ def backward_from_checkpoints(P: "DiffProblem", ckpt, Ttop, g_ns, g_Ts):
         for j in range(j0, j1 - 1):
             P.cuda_step(j)
             states.append(P._save())
+        if P.cuda_step_adjoint:
+            cot, gt = P.backward_segment_cuda(states, j0, Ttop, cot)
+            if gt is not None:
+                g_top = g_top + gt
+            continue
         for j in range(j1 - 1, j0 - 1, -1):
             cot, gt = P.step_vjp(states[j - j0], Ttop, j, cot, P.cuda_diffusion_adjoint)
             if gt is not None:

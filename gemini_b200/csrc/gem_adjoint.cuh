@@ -521,38 +521,41 @@ int gem_step_adjoint_destroy(gem_step_adjoint* a) {
   return GEM_OK;
 }
 
-int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, gem_step_adjoint* A,
-                     const double* ns, const double* vs1, const double* vs2, const double* vs3, const double* Ts,
-                     const double* v1i_lo, const double* v1i_hi, const double* electrovars, const double* dt,
-                     const double* ns_bar_out, const double* vs1_bar_out, const double* Ts_bar_out,
-                     const double* lo_bar_out, const double* hi_bar_out, double* ns_bar, double* vs1_bar,
-                     double* Ts_bar, double* lo_bar, double* hi_bar, double* Ttop_bar, void* stream) {
-  if (!cfg || check_grid(g) || !w || !A || !ns || !vs1 || !vs2 || !vs3 || !Ts || !v1i_lo || !v1i_hi ||
-      !electrovars || !dt || !ns_bar_out || !vs1_bar_out || !Ts_bar_out || !ns_bar || !vs1_bar || !Ts_bar ||
-      !lo_bar || !hi_bar)
-    return set_err(GEM_EINVAL, "null argument");
+static int step_adjoint_check(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, const gem_step_adjoint* A) {
+  if (!cfg || check_grid(g) || !w || !A) return set_err(GEM_EINVAL, "null argument");
   if (A->g != g) return set_err(GEM_EINVAL, "step adjoint workspace made for another grid");
   if (cfg->diffsolvetype != 1 && cfg->diffsolvetype != 2)
     return set_err(GEM_EINVAL, "Unsupported diffusion solver type/mode: %d. Should be either 1 or 2.", cfg->diffsolvetype);
   if (g->dev.has_null) return set_err(GEM_EINVAL, "the step adjoint supports grids without null cells");
-  int rc = check_step(g);
-  if (rc) return rc;
+  return check_step(g);
+}
+
+int gem_step_vjp_replay_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, gem_step_adjoint* A,
+                            const double* ns, const double* vs1, const double* vs2, const double* vs3,
+                            const double* Ts, const double* v1i_lo, const double* v1i_hi, const double* dt,
+                            void* stream) {
+  int rc0 = step_adjoint_check(cfg, g, w, A);
+  if (rc0) return rc0;
+  if (!ns || !vs1 || !vs2 || !vs3 || !Ts || !v1i_lo || !v1i_hi || !dt) return set_err(GEM_EINVAL, "null argument");
   cudaStream_t st = S(stream);
   const GridDev& G = g->dev;
   const Dims& d = G.d;
   const long long F = A->F;
-  const size_t FB = sizeof(double) * F;
   const unsigned ngb = grid_for(d.ng, 256);
+  const long long ncol = (long long)d.lx2 * d.lx3;
   double* WF = A->WF;
-  double* S0 = A->ST;
   double* Sx[4] = {A->ST, A->ST + 3 * F, A->ST + 6 * F, A->ST + 9 * F};
+  const int dims[3] = {3, 1, 2};
+  const double* vel[3] = {A->V3, A->V1, A->V2};
+  int rc = GEM_OK;
+  const size_t FB = sizeof(double) * F;
+  double* S0 = A->ST;
   // ---------------- forward replay
   GEM_CUDA(cudaMemcpyAsync(WF, ns, FB, cudaMemcpyDeviceToDevice, st));
   GEM_CUDA(cudaMemcpyAsync(WF + F, vs1, FB, cudaMemcpyDeviceToDevice, st));
   GEM_CUDA(cudaMemcpyAsync(WF + 2 * F, vs2, FB, cudaMemcpyDeviceToDevice, st));
   GEM_CUDA(cudaMemcpyAsync(WF + 3 * F, vs3, FB, cudaMemcpyDeviceToDevice, st));
   GEM_CUDA(cudaMemcpyAsync(WF + 4 * F, Ts, FB, cudaMemcpyDeviceToDevice, st));
-  const long long ncol = (long long)d.lx2 * d.lx3;
   ka_set_faces<<<grid_for(ncol * LSP, 256), 256, 0, st>>>(d, v1i_lo, v1i_hi, A->VP);
   GEM_LAUNCHED("ka_set_faces");
   Blocks B = blocks(g, WF, S0 + F);  // rv, re straight into stage 0
@@ -571,8 +574,6 @@ int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, g
   GEM_LAUNCHED("k_interface_vels");
   // the nine sweeps: (dim, velocities) per stage, fields n (frank 0, 6 species), rv (frank 1
   // for x2/x3, 6 species), re (frank 0, 7 species)
-  const int dims[3] = {3, 1, 2};
-  const double* vel[3] = {A->V3, A->V1, A->V2};
   for (int q = 0; q < 3; ++q) {
     double* Sin = Sx[q];
     double* So = Sx[q + 1];
@@ -606,13 +607,41 @@ int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, g
       GEM_LAUNCHED("k_halo_wrap");
     }
   }
-  // ---------------- backward
-  double* NO = WF;          // n after clean_param(1)
-  double* TP = WF + F;      // T into the diffusion
-  double* TPB = WF + 2 * F;  // its cotangent
-  double* NDB = WF + 3 * F;  // cotangent of the diffusion's n input
+  // the post-sweep values the diffusion adjoint needs (WF's state copy is dead now)
+  double* NO = WF;
+  double* TP = WF + F;
   ka_post_fwd<<<ngb, 256, 0, st>>>(G, Sx[3], NO, TP);
   GEM_LAUNCHED("ka_post_fwd");
+  return GEM_OK;
+}
+
+int gem_step_vjp_backward_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, gem_step_adjoint* A,
+                              const double* ns, const double* vs1, const double* Ts, const double* v1i_lo,
+                              const double* v1i_hi, const double* electrovars, const double* dt,
+                              const double* ns_bar_out, const double* vs1_bar_out, const double* Ts_bar_out,
+                              const double* lo_bar_out, const double* hi_bar_out, double* ns_bar, double* vs1_bar,
+                              double* Ts_bar, double* lo_bar, double* hi_bar, double* Ttop_bar, void* stream) {
+  int rc0 = step_adjoint_check(cfg, g, w, A);
+  if (rc0) return rc0;
+  if (!ns || !vs1 || !Ts || !v1i_lo || !v1i_hi || !electrovars || !dt || !ns_bar_out || !vs1_bar_out ||
+      !Ts_bar_out || !ns_bar || !vs1_bar || !Ts_bar || !lo_bar || !hi_bar)
+    return set_err(GEM_EINVAL, "null argument");
+  cudaStream_t st = S(stream);
+  const GridDev& G = g->dev;
+  const Dims& d = G.d;
+  const long long F = A->F;
+  const unsigned ngb = grid_for(d.ng, 256);
+  const long long ncol = (long long)d.lx2 * d.lx3;
+  double* WF = A->WF;
+  double* Sx[4] = {A->ST, A->ST + 3 * F, A->ST + 6 * F, A->ST + 9 * F};
+  const int dims[3] = {3, 1, 2};
+  const double* vel[3] = {A->V3, A->V1, A->V2};
+  int rc = GEM_OK;
+  // ---------------- backward
+  double* NO = WF;           // n after clean_param(1) (from the replay)
+  double* TP = WF + F;       // T into the diffusion (from the replay)
+  double* TPB = WF + 2 * F;  // its cotangent
+  double* NDB = WF + 3 * F;  // cotangent of the diffusion's n input
   {
     DiffAdjArgs da;
     da.G = G;
@@ -686,6 +715,19 @@ int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, g
                                    Ts_bar);
   GEM_LAUNCHED("ka_conv_vjp");
   return GEM_OK;
+}
+
+int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, gem_step_adjoint* A,
+                     const double* ns, const double* vs1, const double* vs2, const double* vs3, const double* Ts,
+                     const double* v1i_lo, const double* v1i_hi, const double* electrovars, const double* dt,
+                     const double* ns_bar_out, const double* vs1_bar_out, const double* Ts_bar_out,
+                     const double* lo_bar_out, const double* hi_bar_out, double* ns_bar, double* vs1_bar,
+                     double* Ts_bar, double* lo_bar, double* hi_bar, double* Ttop_bar, void* stream) {
+  int rc = gem_step_vjp_replay_dev(cfg, g, w, A, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, dt, stream);
+  if (rc) return rc;
+  return gem_step_vjp_backward_dev(cfg, g, w, A, ns, vs1, Ts, v1i_lo, v1i_hi, electrovars, dt, ns_bar_out,
+                                   vs1_bar_out, Ts_bar_out, lo_bar_out, hi_bar_out, ns_bar, vs1_bar, Ts_bar, lo_bar,
+                                   hi_bar, Ttop_bar, stream);
 }
 
 }  // extern "C"

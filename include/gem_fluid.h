@@ -166,6 +166,22 @@ int gem_step_vjp_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, g
                      const double* lo_bar_out, const double* hi_bar_out, double* ns_bar, double* vs1_bar,
                      double* Ts_bar, double* lo_bar, double* hi_bar, double* Ttop_bar, void* stream);
 
+/* The same in two halves.  The replay (conversions, ghost fill, interface velocities, the
+ * nine sweeps with their inputs kept, the post-sweep values) needs only the state before the
+ * step, so a backward loop may replay step j-1 into a second workspace, on another stream,
+ * while step j's backward runs; the backward then takes the same state pointers (ns, vs1,
+ * Ts, faces) and the cotangents.  Order the two halves of one workspace on the device. */
+int gem_step_vjp_replay_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, gem_step_adjoint* a,
+                            const double* ns, const double* vs1, const double* vs2, const double* vs3,
+                            const double* Ts, const double* v1i_lo, const double* v1i_hi, const double* dt,
+                            void* stream);
+int gem_step_vjp_backward_dev(const gem_cfg* cfg, const gem_grid* g, const gem_work* w, gem_step_adjoint* a,
+                              const double* ns, const double* vs1, const double* Ts, const double* v1i_lo,
+                              const double* v1i_hi, const double* electrovars, const double* dt,
+                              const double* ns_bar_out, const double* vs1_bar_out, const double* Ts_bar_out,
+                              const double* lo_bar_out, const double* hi_bar_out, double* ns_bar, double* vs1_bar,
+                              double* Ts_bar, double* lo_bar, double* hi_bar, double* Ttop_bar, void* stream);
+
 /* No counterpart in the reference.  dt_calc (the same result as gem_dt_calc_dev) for callers
  * that cannot allocate device memory or hold a gem_work (for example code that runs inside
  * a pool-managed or already-captured context): it calls no allocator.  Its scratch is a
