@@ -472,6 +472,9 @@ def backward_from_checkpoints(P: "DiffProblem", ckpt, Ttop, g_ns, g_Ts):
            g_Ts if g_Ts is not None else zeros(ns_f), zeros(P.lo0), zeros(P.hi0)]
     g_top = torch.zeros_like(Ttop) if Ttop is not None else None
     starts = sorted(ckpt)
+    if P.cuda_step_adjoint:
+        cot, g_top = _backward_cuda(P, ckpt, starts, Ttop, cot, g_top)
+        starts = []
     for seg_i in range(len(starts) - 1, -1, -1):
         j0 = starts[seg_i]
         j1 = starts[seg_i + 1] if seg_i + 1 < len(starts) else P.nsteps
@@ -480,11 +483,6 @@ def backward_from_checkpoints(P: "DiffProblem", ckpt, Ttop, g_ns, g_Ts):
         for j in range(j0, j1 - 1):
             P.cuda_step(j)
             states.append(P._save())
-        if P.cuda_step_adjoint:
-            cot, gt = P.backward_segment_cuda(states, j0, Ttop, cot)
-            if gt is not None:
-                g_top = g_top + gt
-            continue
         for j in range(j1 - 1, j0 - 1, -1):
             cot, gt = P.step_vjp(states[j - j0], Ttop, j, cot, P.cuda_diffusion_adjoint)
             if gt is not None:
@@ -494,6 +492,50 @@ def backward_from_checkpoints(P: "DiffProblem", ckpt, Ttop, g_ns, g_Ts):
     gns = cot[0][(slice(None),) + I]
     g_n0 = gns[:LSP - 1] + gns[LSP - 1].unsqueeze(0)  # electrons = sum of ions
     return g_n0, g_top
+
+
+def _backward_cuda(P: "DiffProblem", ckpt, starts, Ttop, cot, g_top):
+    """The CUDA backward over the checkpoint segments, last first.  With a checkpoint at every
+    step the whole run is one pipelined segment; otherwise the recompute of segment s-1 (the
+    CUDA forward from its checkpoint, on a third stream) runs while segment s is pulled back."""
+    import torch
+
+    main = torch.cuda.current_stream()
+    if P._side is None:
+        P._side = torch.cuda.Stream()
+    if getattr(P, "_rec", None) is None:
+        P._rec = torch.cuda.Stream()
+    rec = P._rec
+    bounds = [(starts[i], starts[i + 1] if i + 1 < len(starts) else P.nsteps) for i in range(len(starts))]
+    if all(j1 - j0 == 1 for j0, j1 in bounds):  # every state is a checkpoint: nothing to recompute
+        cot, gt = P.backward_segment_cuda([ckpt[j] for j, _ in bounds], bounds[0][0], Ttop, cot)
+        return cot, (g_top + gt if gt is not None else g_top)
+
+    def recompute(j0, j1):
+        rec.wait_stream(main)
+        with torch.cuda.stream(rec):
+            P._load(*ckpt[j0], Ttop)
+            states = [ckpt[j0]]
+            for j in range(j0, j1 - 1):
+                P.cuda_step(j)
+                st = P._save()
+                for t in st:  # read on the main and replay streams before they are freed
+                    t.record_stream(main)
+                    t.record_stream(P._side)
+                states.append(st)
+        return states
+
+    states = recompute(*bounds[-1])
+    main.wait_stream(rec)
+    for s_i in range(len(bounds) - 1, -1, -1):
+        nxt = recompute(*bounds[s_i - 1]) if s_i > 0 else None
+        cot, gt = P.backward_segment_cuda(states, bounds[s_i][0], Ttop, cot)
+        if gt is not None:
+            g_top = g_top + gt
+        if nxt is not None:
+            main.wait_stream(rec)
+            states = nxt
+    return cot, g_top
 
 
 class BatchedAdjoint:
