@@ -460,14 +460,16 @@ def run_batched(args, world, rank):
     return out
 
 
-ADJOINT = dict(lx1=128, lx2=64, lx3=64, steps=20, checkpoint_every=5, seed=11)
+# every step's state kept (20 states of this grid: 2 GB of HBM); the recompute variant keeps
+# one state in checkpoint_every_recompute and recomputes the others in the backward
+ADJOINT = dict(lx1=128, lx2=64, lx3=64, steps=20, checkpoint_every=1, checkpoint_every_recompute=5, seed=11)
 
 
-def run_adjoint(args):
+def run_adjoint(args, checkpoint_every=None):
     """Adjoint workload: Cartesian 128x64x64 x 7 species, 20 steps, L2 misfit of the final Te
     and n_O+ against a seeded target; gradient w.r.t. the initial ion densities and the
     per-column top temperature.  Reports forward time, forward+backward time and the ratio
-    (device time, CUDA events)."""
+    (device time, CUDA events), and the same with checkpoint recomputation."""
     import torch
 
     from gemini_b200 import adjoint as AD
@@ -475,9 +477,10 @@ def run_adjoint(args):
     from gemini_b200 import state as S
 
     a = ADJOINT
+    k = a["checkpoint_every"] if checkpoint_every is None else checkpoint_every
     g = G.cartesian_grid(a["lx1"], a["lx2"], a["lx3"])
     st = S.init_state(g, seed=a["seed"], perturb=0.1)
-    P = AD.DiffProblem(g, st, a["steps"], checkpoint_every=a["checkpoint_every"])
+    P = AD.DiffProblem(g, st, a["steps"], checkpoint_every=k)
     I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
     n0 = P.base[(slice(0, 6),) + I].clone()
     rng = np.random.default_rng(a["seed"])
@@ -510,14 +513,21 @@ def run_adjoint(args):
         return e0.elapsed_time(e1) / reps
 
     ms_f = timed(fwd, 3)
-    ms_fb = timed(fwd_bwd, 1)
-    return {"workload": f"Cartesian {a['lx1']}x{a['lx2']}x{a['lx3']} x 7 species, {a['steps']} steps, "
-                        f"checkpoint every {a['checkpoint_every']}; loss = L2 misfit of final Te and n_O+",
-            "forward_ms": ms_f, "forward_backward_ms": ms_fb, "adjoint_over_forward": (ms_fb - ms_f) / ms_f,
-            "gradient_wrt": "initial ion densities (6 x cells) and per-column top temperature",
-            "backward": "per step: hand-written CUDA adjoints of the 9 field sweeps and of the TRBDF2 "
-                        "diffusion; autograd through the tensor transcription for the boundaries, "
-                        "interface velocities and conversions; CUDA recompute per checkpoint segment"}
+    ms_fb = timed(fwd_bwd, 2)
+    out = {"workload": f"Cartesian {a['lx1']}x{a['lx2']}x{a['lx3']} x 7 species, {a['steps']} steps, "
+                       f"checkpoint every {k}; loss = L2 misfit of final Te and n_O+",
+           "forward_ms": ms_f, "forward_backward_ms": ms_fb, "adjoint_over_forward": (ms_fb - ms_f) / ms_f,
+           "gradient_wrt": "initial ion densities (6 x cells) and per-column top temperature",
+           "backward": "per step: gem_step_vjp_dev, the whole step's adjoint in CUDA (device replay of the "
+                       "conversions, ghost fill and nine sweeps; hand-written VJPs of the sweeps, the TRBDF2 "
+                       "diffusion, the floors/conversions, the ghost copies and the x1 boundary); the replay of "
+                       "step j-1 runs on a side stream during step j's backward"}
+    P.close()
+    if checkpoint_every is None and a.get("checkpoint_every_recompute"):
+        r = run_adjoint(args, a["checkpoint_every_recompute"])
+        out["recompute"] = {kk: r[kk] for kk in ("workload", "forward_ms", "forward_backward_ms",
+                                                  "adjoint_over_forward")}
+    return out
 
 
 BATCHED_ADJOINT = dict(instances=32, steps=200, checkpoint_every=10, group=8, seed=77)
