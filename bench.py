@@ -601,7 +601,15 @@ def main():
                     help="also measure the batched adjoint workload (32 instances x 200 steps; minutes)")
     ap.add_argument("--lx", type=int, nargs=3, default=None, metavar=("LX1", "LX2", "LX3"),
                     help="override the grid size (profiling runs on a smaller case)")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the adjoint measurement (profiling of the adjoint kernels)")
+    ap.add_argument("--adjoint-steps", type=int, default=None, help="time steps of the adjoint workload")
     args = ap.parse_args()
+    if args.adjoint_steps:
+        ADJOINT["steps"] = args.adjoint_steps
+    if args.adjoint_only:
+        print(json.dumps({"adjoint": run_adjoint(args)}))
+        return
     if args.lx:
         WORKLOAD.update(lx1=args.lx[0], lx2=args.lx[1], lx3=args.lx[2])
     if args.impl == "reference":
