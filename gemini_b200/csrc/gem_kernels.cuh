@@ -2361,7 +2361,7 @@ __global__ void __launch_bounds__(256) k_sweep_vjp_march(SweepVjpArgs P, SweepVj
 // cell p-2 then gathers from faces p-3 .. p (the four that reach it) by shuffles from this
 // chunk and the previous one.  Face-velocity cotangents go to the field's own vbar slice.
 template <bool UNIT>
-__global__ void __launch_bounds__(256) k_sweep_vjp_x1(SweepVjpArgs P, SweepVjpFields FS) {
+__global__ void __launch_bounds__(256, 3) k_sweep_vjp_x1(SweepVjpArgs P, SweepVjpFields FS) {
   const GridDev& G = P.G;
   const Dims d = G.d;
   const int lx = d.lx1;
