@@ -2223,7 +2223,7 @@ __device__ __forceinline__ SlopeBr slope_br(const Line1D& L, int k, double fm, d
 }
 
 template <int DIM, bool UNIT>
-__global__ void __launch_bounds__(256) k_sweep_vjp_march(SweepVjpArgs P, SweepVjpFields FS, int nseg) {
+__global__ void __launch_bounds__(256, 3) k_sweep_vjp_march(SweepVjpArgs P, SweepVjpFields FS, int nseg) {
   const GridDev& G = P.G;
   const Dims d = G.d;
   const int lx = (DIM == 2) ? d.lx2 : d.lx3;
@@ -2268,8 +2268,7 @@ __global__ void __launch_bounds__(256) k_sweep_vjp_march(SweepVjpArgs P, SweepVj
       const double y = UNIT ? 1.0 : __ldg(yha1 + m0 + j * mstride);
       return dt * __ldg(L.ydxi + j - 1) * y * __ldg(ob + c0 + j * stride);
     };
-    // the global inputs of face i: f(i+1), obar(i), v(i) and the metrics, loaded two faces
-    // ahead of their use so that the march is not bound by load latency
+    // the global inputs of face i: f(i+1), obar(i), v(i) and the metrics
     struct In {
       double fn, ob, v, y, h, yc;
     };
@@ -2293,11 +2292,8 @@ __global__ void __launch_bounds__(256) k_sweep_vjp_march(SweepVjpArgs P, SweepVj
     SlopeBr sprev = slope_br(L, i0 - 1, F(i0 - 2), fc, fp);         // slope(i-1)
     double kprev = kob(i0 - 1);
     double A0 = 0, A1 = 0, A2 = 0, A3 = 0;                          // pending cells i-2 .. i+1
-    In qa = load(i0), qb;
-    if (i0 + 1 <= i1e) qb = load(i0 + 1);
     for (int i = i0; i <= i1e; ++i) {
-      In qc;
-      if (i + 2 <= i1e) qc = load(i + 2);
+      const In qa = load(i);
       const double fn = qa.fn;
       const SlopeBr scur = slope_br(L, i, fc, fp, fn);  // slope(i)
       const double kc = (i >= 1 && i <= lx) ? dt * __ldg(L.ydxi + i - 1) * qa.y * qa.ob : 0.0;
@@ -2338,8 +2334,6 @@ __global__ void __launch_bounds__(256) k_sweep_vjp_march(SweepVjpArgs P, SweepVj
       fp = fn;
       sprev = scur;
       kprev = kc;
-      qa = qb;
-      qb = qc;
     }
     // cells i1e-1 .. i1e+1 are final after the last face
     const double Af[3] = {A0, A1, A2};
