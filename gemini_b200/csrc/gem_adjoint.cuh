@@ -57,6 +57,27 @@ __device__ __forceinline__ void for_rows(const Dims& d, Body body) {
   }
 }
 
+// The same traversal with the species as the slowest coordinate: body(k, i1, i2, i3,
+// interior, s) for every cell and species (for per-species work with no coupling).
+template <class Body>
+__device__ __forceinline__ void for_rows_s(const Dims& d, Body body) {
+  const int X1 = d.lx1 + 4, X2 = d.lx2 + 4, X3 = d.lx3 + 4;
+  const int nch = (X1 + 31) / 32;
+  const int nper = X2 * X3 * nch;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int u = blockIdx.x * wpb + (threadIdx.x >> 5); u < nper * LSP; u += gridDim.x * wpb) {
+    const int s = u / nper;
+    const int uu = u - s * nper;
+    const int r = uu / nch, ch = uu - r * nch;
+    const int i2 = r % X2 - 1, i3 = r / X2 - 1;
+    const int i1 = ch * 32 + lane - 1;
+    if (i1 > d.lx1 + 2) continue;
+    const bool in = i1 >= 1 && i1 <= d.lx1 && i2 >= 1 && i2 <= d.lx2 && i3 >= 1 && i3 <= d.lx3;
+    body(gi(d, i1, i2, i3), i1, i2, i3, in, s);
+  }
+}
+
 // Post-sweep forward values the diffusion adjoint needs: n after clean_param(1) (ion floor,
 // electrons the ion sum; ghosts 1e-5) and T after rhoe2T + clean_param(3) (ghosts 100).
 // F: the swept stage (n | rv | re blocks).
@@ -373,7 +394,8 @@ __global__ void ka_x1bc_vjp(GridDev G, const double* __restrict__ ns, const doub
 }
 
 // Adjoint of interface_vels for x1 (advec.f90:155-229) and of v12rhov1 / T2rhoe
-// (multifluid.f90:193-214), writing the state cotangents (ghost cells 0).  v1ib: the x1
+// (multifluid.f90:193-214), writing the state cotangents (ghost cells 0), one thread per
+// cell and species.  v1ib: the x1
 // face cotangents of the three x1 sweep adjoints (n, rv, re slices of LSP*nf1 each, summed
 // here); lob_out / hib_out: cotangents of the
 // step's boundary-face outputs (may be null).
@@ -387,14 +409,14 @@ __global__ void ka_conv_vjp(GridDev G, const double* __restrict__ ns, const doub
   const long long ncol = (long long)d.lx2 * d.lx3;
   const long long nf = nf1(d);
   const int lx = d.lx1;
-  for_rows(d, [&](long long k, int i1, int i2, int i3, bool in) {
+  for_rows_s(d, [&](long long k, int i1, int i2, int i3, bool in, int s) {
+    const long long o = (long long)s * ng;
     if (!in) {
-      for (int s = 0; s < LSP; ++s) nsb[s * ng + k] = vs1b[s * ng + k] = Tsb[s * ng + k] = 0.0;
+      nsb[o + k] = vs1b[o + k] = Tsb[o + k] = 0.0;
       return;
     }
     const long long col = (i2 - 1) + (long long)d.lx2 * (i3 - 1);
-    for (int s = 0; s < LSP; ++s) {
-      const long long o = (long long)s * ng;
+    {
       const double n = ns[o + k], v = vs1[o + k], T = Ts[o + k];
       const double gn = C[o + k], grv = C[LSP * ng + o + k], gre = C[2 * LSP * ng + o + k];
       const double ke = KB / (c_gammas[s] - 1);
