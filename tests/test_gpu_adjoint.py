@@ -62,6 +62,26 @@ def test_gradient_matches_autograd_of_transcription(solver):
     assert float(t.grad.abs().max()) > 0
 
 
+def test_gradient_independent_of_checkpoint_interval():
+    """Every state kept (one pipelined backward segment), and recomputation every 2 or 4
+    steps (the recompute of a segment overlapping the previous segment's backward), give the
+    same gradients."""
+    import torch
+
+    grads = []
+    for k in (1, 2, 4):
+        g, P, n0, Ttop, tT, tn = _problem(nsteps=7, k=k)
+        a = n0.clone().requires_grad_(True)
+        t = Ttop.clone().requires_grad_(True)
+        ns, Ts = AD.FluidAdvance.apply(a, t, P)
+        AD.misfit(ns, Ts, tT, tn, g).backward()
+        grads.append((a.grad, t.grad))
+        P.close()
+    for other in grads[1:]:
+        for x, y in zip(grads[0], other):
+            assert float((x - y).abs().max() / x.abs().max()) < 1e-12
+
+
 def test_gradient_vs_central_differences_32_directions():
     import torch
 
