@@ -1798,24 +1798,29 @@ struct WarpMemA {
 // q: the cell in the interior-only neutral arrays (electrons)
 __device__ __forceinline__ void lam_deriv(const DiffAdjArgs& P, int s, double T, double nv, long long q,
                                           long long nc, double& lam, double& dl_dT, double& dl_dn) {
+  // the adjoint needs no exact quotients: each reciprocal is formed once and multiplied
   const double T25 = pow25(T);
+  const double yT = 1.0 / T;
   if (s < LSP - 1) {
     lam = c_tcoef[s] * T25;
-    dl_dT = 2.5 * lam / T;
+    dl_dT = 2.5 * lam * yT;
     dl_dn = 0.0;
     return;
   }
   const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
   const double sq = sqrt(T);
+  const double hy = 0.5 / sq;
+  const double ynv = 1.0 / nv;
   const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
                    n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
-  const double Xp = n1 * 1.1e-16 * 5.7e-4 + n2 * 2.82e-17 * (0.5 / sq * (1 - 1.21e-4 * T) - 1.21e-4 * sq) +
-                    n3 * 2.2e-16 * 3.6e-2 * 0.5 / sq;
-  const double den = 1 + 3.22e4 * (T * T) / nv * X;
-  lam = ELCHRG * 100 * 7.7e5 * T25 / den;
-  const double dden_dT = 3.22e4 * (2 * T * X + T * T * Xp) / nv;
-  dl_dT = lam * (2.5 / T - dden_dT / den);
-  dl_dn = lam * (3.22e4 * T * T * X / (nv * nv)) / den;
+  const double Xp = n1 * 1.1e-16 * 5.7e-4 + n2 * 2.82e-17 * (hy * (1 - 1.21e-4 * T) - 1.21e-4 * sq) +
+                    n3 * 2.2e-16 * 3.6e-2 * hy;
+  const double den = 1 + 3.22e4 * (T * T) * ynv * X;
+  const double yden = 1.0 / den;
+  lam = ELCHRG * 100 * 7.7e5 * T25 * yden;
+  const double dden_dT = 3.22e4 * (2 * T * X + T * T * Xp) * ynv;
+  dl_dT = lam * (2.5 * yT - dden_dT * yden);
+  dl_dn = lam * (3.22e4 * T * T * X * ynv * ynv) * yden;
 }
 
 template <bool UNIT>
@@ -1859,16 +1864,16 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
           T = Tc[i];
           const double nv = nsc[i];
           const long long mk = mm0 + i;
-          const double h1v = UNIT ? 1.0 : __ldg(G.h1 + mk);
+          const double yh1 = UNIT ? 1.0 : __ldg(G.yh1 + mk);
           const double h23 = UNIT ? 1.0 : __ldg(G.h2 + mk) * __ldg(G.h3 + mk);
-          const double ha1 = UNIT ? 1.0 : __ldg(G.ha1_0 + mk);
+          const double yha1 = UNIT ? 1.0 : __ldg(G.yha1_0 + mk);
           double lam, dl_dT, dl_dn;
           lam_deriv(P, s, T, nv, q0 + i, nc, lam, dl_dT, dl_dn);
-          D = lam * h23 / h1v;
-          C = c0 / fmax_f(nv, MINDENSDIV) / ha1;
+          D = lam * h23 * yh1;
+          C = c0 / fmax_f(nv, MINDENSDIV) * yha1;
           if (s == LSP - 1 && i >= 2 && i <= n - 1) {
             const double beta = 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i];  // collisions.f90:197
-            bq = C * beta / h1v / (__ldg(L1.dx + i + 1) + __ldg(L1.dx + i));
+            bq = C * beta * yh1 * __ldg(L1.ydxs + i);  // 1/(dx1(i) + dx1(i+1))
           }
         }
         W.at_lane(VA_T, kp, lp) = T;
@@ -1898,10 +1903,9 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
       double qm = 0.0, qp = 0.0;
       if (i >= 2 && i <= n - 1) {
         const double Dm = nb(VA_D, k, -1), Dc = W.at(VA_D, k), Dp = nb(VA_D, k, 1);
-        const double C = W.at(VA_C, k);
-        const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
-        qm = C * (0.5 * (Dm + Dc)) / dxi / dxm;
-        qp = C * (0.5 * (Dc + Dp)) / dxi / dxp;
+        const double Cy = W.at(VA_C, k) * __ldg(L1.ydxi + i - 1);
+        qm = Cy * (0.5 * (Dm + Dc)) * __ldg(L1.ydx + i);
+        qp = Cy * (0.5 * (Dc + Dp)) * __ldg(L1.ydx + i + 1);
       }
       W.at(VA_QM, k) = qm;
       W.at(VA_QP, k) = qp;
@@ -1949,9 +1953,9 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
         row_at(0, k, lane, a, b, c);
         const double qm = W.at(VA_QM, k), qp = W.at(VA_QP, k);
         const double Tv = W.at(VA_T, k);
-        r = Tv / (dt / 2) - a * nb(VA_T, k, -1) - (qp / 2 + qm / 2) * Tv - c * nb(VA_T, k, 1);
+        r = Tv * dA - a * nb(VA_T, k, -1) - (qp / 2 + qm / 2) * Tv - c * nb(VA_T, k, 1);
       } else {
-        r = W.at(VA_T, k) / dt;
+        r = W.at(VA_T, k) * dA;
       }
       W.at(VA_X, k) = r;
     }
@@ -1967,7 +1971,7 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
         if (i == 1) r = tmin;
         else if (i == n) r = tmax;
         else if (i > n) r = 0.0;
-        else r = -(1 / 3.0 * W.at(VA_T, k) / (dt / 3)) + 4 / 3.0 * W.at(VA_X, k) / (dt / 3);
+        else r = -(1 / 3.0 * W.at(VA_T, k) * d2) + 4 / 3.0 * W.at(VA_X, k) * d2;
         W.at(VA_Y, k) = r;
       }
       stage = 1;
@@ -2017,8 +2021,8 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
           qmb = -ab + bb;
           qpb = bb - cb;
           bqb = ab - cb;
-          tb = l2 * (-(1 / 3.0) / (dt / 3));
-          xb = l2 * ((4 / 3.0) / (dt / 3));
+          tb = l2 * (-(1 / 3.0) * d2);
+          xb = l2 * ((4 / 3.0) * d2);
         }
         W.at(VA_QMB, k) = qmb;
         W.at(VA_QPB, k) = qpb;
@@ -2088,9 +2092,9 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
         }
         // q- = C Dh(i) / (dxi dx(i)), q+ = C Dh(i+1) / (dxi dx(i+1)), bq = C beta/h1/(dx(i)+dx(i+1))
         const double C = W.at(VA_C, k);
-        const double dxi = __ldg(L1.dxi + i - 1), dxm = __ldg(L1.dx + i), dxp = __ldg(L1.dx + i + 1);
-        em = qmb * C / (dxi * dxm);  // -> Dh(i)
-        ep = qpb * C / (dxi * dxp);  // -> Dh(i+1)
+        const double Cy = C * __ldg(L1.ydxi + i - 1);
+        em = qmb * Cy * __ldg(L1.ydx + i);      // -> Dh(i)
+        ep = qpb * Cy * __ldg(L1.ydx + i + 1);  // -> Dh(i+1)
         cb = (qmb * qm + qpb * qp + bqb * bq) / C;
       }
       W.at(VA_TB, k) = tb;
@@ -2116,7 +2120,7 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
           const double Db = 0.5 * (dh_i + dh_ip1);
           const double T = W.at_lane(VA_T, kp, lp), nv = nsc[i];
           const long long mk = mm0 + i;
-          const double g = UNIT ? 1.0 : __ldg(G.h2 + mk) * __ldg(G.h3 + mk) / __ldg(G.h1 + mk);
+          const double g = UNIT ? 1.0 : __ldg(G.h2 + mk) * __ldg(G.h3 + mk) * __ldg(G.yh1 + mk);
           double lam, dl_dT, dl_dn;
           lam_deriv(P, s, T, nv, q0 + i, nc, lam, dl_dT, dl_dn);
           const double dcn = (nv > MINDENSDIV) ? -W.at_lane(VA_C, kp, lp) / nv : 0.0;
