@@ -140,17 +140,18 @@ __global__ void __launch_bounds__(256) ka_post_vjp(GridDev G, const double* __re
       const double n = F[s * ng + k];
       nsum += n;
       ne += fmax_f(n, MINDENS);
-      const double v1 = rv[s * ng + k] / (c_ms[s] * fmax_f(n, MINDENSDIV));
+      const double v1 = rv[s * ng + k] * c_yms[s] / fmax_f(n, MINDENSDIV);
       csum += n * c_qs[s] * v1;
     }
     // energy: T = max((gamma-1)/kB re / max(n_out, 1e-5), 100), n_out the floored density
     auto energy = [&](int s, double nout) -> double {  // returns the cotangent of n_out
       const double D = fmax_f(nout, MINDENSDIV);
-      const double Tr = (c_gammas[s] - 1) / KB * re[s * ng + k] / D;
+      const double Tr = (c_gammas[s] - 1) / KB * re[s * ng + k] / D;  // as the forward: the floor test
       const double Tb = (Tr >= 100.0) ? TPb[s * ng + k] : 0.0;
-      cre[s * ng + k] = Tb * ((c_gammas[s] - 1) / KB) / D;
+      const double TbyD = Tb / D;
+      cre[s * ng + k] = TbyD * ((c_gammas[s] - 1) / KB);
       double nb = nbo[s * ng + k] + NDb[s * ng + k];
-      if (nout >= MINDENSDIV) nb += -Tb * Tr / D;
+      if (nout >= MINDENSDIV) nb += -TbyD * Tr;
       return nb;
     };
     const double nbe = energy(LSP - 1, ne);  // electrons: n_out = the ion sum
@@ -167,13 +168,13 @@ __global__ void __launch_bounds__(256) ka_post_vjp(GridDev G, const double* __re
       const double nb = energy(s, fmax_f(n, MINDENS));
       // clean_param(1): ions max(n, 1e-100), electrons their sum
       double c = (n >= MINDENS) ? nb + nbe : 0.0;
-      const double Dv = fmax_f(n, MINDENSDIV);
-      const double v1 = rv[s * ng + k] / (c_ms[s] * Dv);
+      const double yDv = 1.0 / fmax_f(n, MINDENSDIV);
+      const double v1 = rv[s * ng + k] * c_yms[s] * yDv;
       const double v1b = vbo[s * ng + k] + csb * n * c_qs[s];
       c += nsb + csb * c_qs[s] * v1;
-      if (n >= MINDENSDIV) c += -v1b * v1 / Dv;
+      if (n >= MINDENSDIV) c += -v1b * v1 * yDv;
       cn[s * ng + k] = c;
-      crv[s * ng + k] = v1b / (c_ms[s] * Dv);
+      crv[s * ng + k] = v1b * c_yms[s] * yDv;
     }
   });
 }
