@@ -1798,8 +1798,10 @@ struct WarpMemA {
 // q: the cell in the interior-only neutral arrays (electrons)
 __device__ __forceinline__ void lam_deriv(const DiffAdjArgs& P, int s, double T, double nv, long long q,
                                           long long nc, double& lam, double& dl_dT, double& dl_dn) {
-  // the adjoint needs no exact quotients: each reciprocal is formed once and multiplied
-  const double T25 = pow25(T);
+  // the adjoint needs no exact quotients or correctly rounded powers: each reciprocal is
+  // formed once and multiplied, and T^2.5 = T^2 sqrt(T) in plain arithmetic
+  const double sq = sqrt(T);
+  const double T25 = T * T * sq;
   const double yT = 1.0 / T;
   if (s < LSP - 1) {
     lam = c_tcoef[s] * T25;
@@ -1808,8 +1810,7 @@ __device__ __forceinline__ void lam_deriv(const DiffAdjArgs& P, int s, double T,
     return;
   }
   const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
-  const double sq = sqrt(T);
-  const double hy = 0.5 / sq;
+  const double hy = 0.5 * yT * sq;  // 1 / (2 sqrt(T))
   const double ynv = 1.0 / nv;
   const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
                    n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
