@@ -309,3 +309,39 @@ def test_cuda_step_vjp_matches_autograd(name, mk, kw, floor_free, solver, top):
             else:
                 err = float((gtop - etop).abs().max() / etop.abs().max())
                 assert err < 1e-9, (name, cuda_pieces, "Ttop", err)
+
+
+def test_combined_step_vjp_entry_equals_its_halves():
+    """gem_step_vjp_dev (one call) gives the bits of gem_step_vjp_replay_dev followed by
+    gem_step_vjp_backward_dev (what the Python backward calls)."""
+    import ctypes
+
+    import torch
+
+    from gemini_b200 import _lib
+    from gemini_b200 import fluid as F
+
+    g = G.cartesian_grid(30, 7, 6, flagper=1)
+    st = S.init_state(g, seed=8, perturb=0.1)
+    P = AD.DiffProblem(g, st, 2, checkpoint_every=1)
+    rng = np.random.default_rng(3)
+    I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
+    Ttop = torch.from_numpy(st.Teinf * (1 + 0.05 * rng.uniform(-1, 1, (g.lx3, g.lx2)))).cuda()
+    _, ck = P.run(P.base[(slice(0, 6),) + I].clone(), Ttop, keep=True)
+    state = ck[1]
+    cot = [torch.from_numpy(rng.standard_normal(t.shape)).cuda() for t in state]
+    halves, top_h = P.step_vjp_cuda(state, Ttop, 1, cot)
+    out = [torch.empty_like(t) for t in state]
+    tb = torch.empty_like(Ttop)
+    c = P.cfg.c()
+    p = F._ptr
+    ns, vs1, Ts, lo, hi = state
+    _lib.check(_lib.lib().gem_step_vjp_dev(
+        ctypes.byref(c), P.dg.handle, P.ds.work, P._workspace(1), p(ns), p(vs1), p(P.vs2), p(P.vs3), p(Ts), p(lo),
+        p(hi), p(P.ds.electrovars), p(P.dt_tensor(1)), *[p(t) for t in cot], *[p(t) for t in out], p(tb),
+        F._stream()))
+    torch.cuda.synchronize()
+    for x, y in zip(out, halves):
+        assert torch.equal(x, y)
+    assert torch.equal(tb, top_h)
+    P.close()
