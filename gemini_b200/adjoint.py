@@ -269,46 +269,6 @@ class DiffProblem:
             p(out[0]), p(out[1]), p(out[2]), p(out[3]), p(out[4]), None if tb is None else p(tb), F._stream()))
         return out, tb
 
-    def backward_segment_cuda(self, states, j0, Ttop, cot):
-        """Pull cot back through the steps j0 .. j0+len(states)-1 (states[m]: the state before
-        step j0+m), last step first: the replay of step j-1 runs on a side stream into the
-        other workspace while step j's backward runs.  Returns (cot, g_top)."""
-        import torch
-
-        main = torch.cuda.current_stream()
-        if self._side is None:
-            self._side = torch.cuda.Stream()
-        side = self._side
-        states = [tuple(t.detach().contiguous() for t in st) for st in states]
-        self._set_top(Ttop)
-        n = len(states)
-        for m in range(n):  # the cached dt tensors, made on the main stream before the fork
-            self.dt_tensor(j0 + m)
-        side.wait_stream(main)  # the states were recomputed on the main stream
-        ev_rep, ev_back = [None] * n, [None] * n
-        g_top = None
-
-        def replay(m):
-            with torch.cuda.stream(side):
-                if m + 2 < n:  # workspace m % 2 was last read by the backward of step m+2
-                    side.wait_event(ev_back[m + 2])
-                self._replay(m % 2, states[m], j0 + m)
-                ev_rep[m] = torch.cuda.Event()
-                ev_rep[m].record(side)
-
-        replay(n - 1)
-        for m in range(n - 1, -1, -1):
-            if m >= 1:
-                replay(m - 1)
-            main.wait_event(ev_rep[m])
-            cot, gt = self._backward(m % 2, states[m], Ttop, j0 + m, cot)
-            ev_back[m] = torch.cuda.Event()
-            ev_back[m].record(main)
-            if gt is not None:
-                g_top = gt if g_top is None else g_top + gt
-        main.wait_stream(side)
-        return cot, g_top
-
     def close(self):
         """Release the step adjoint workspaces."""
         if self._sa is not None:
@@ -495,9 +455,11 @@ def backward_from_checkpoints(P: "DiffProblem", ckpt, Ttop, g_ns, g_Ts):
 
 
 def _backward_cuda(P: "DiffProblem", ckpt, starts, Ttop, cot, g_top):
-    """The CUDA backward over the checkpoint segments, last first.  With a checkpoint at every
-    step the whole run is one pipelined segment; otherwise the recompute of segment s-1 (the
-    CUDA forward from its checkpoint, on a third stream) runs while segment s is pulled back."""
+    """The CUDA backward over all steps, last first, as one pipeline: the replay of step j-1
+    (gem_step_vjp_replay_dev, on a side stream, into workspace (j-1) % 2) runs while step j's
+    backward runs (workspace j % 2); with checkpoints every k > 1 steps, the recompute of a
+    segment's states (the CUDA forward from its checkpoint, on a third stream) runs while
+    the following segment is pulled back."""
     import torch
 
     main = torch.cuda.current_stream()
@@ -505,36 +467,61 @@ def _backward_cuda(P: "DiffProblem", ckpt, starts, Ttop, cot, g_top):
         P._side = torch.cuda.Stream()
     if getattr(P, "_rec", None) is None:
         P._rec = torch.cuda.Stream()
-    rec = P._rec
-    bounds = [(starts[i], starts[i + 1] if i + 1 < len(starts) else P.nsteps) for i in range(len(starts))]
-    if all(j1 - j0 == 1 for j0, j1 in bounds):  # every state is a checkpoint: nothing to recompute
-        cot, gt = P.backward_segment_cuda([ckpt[j] for j, _ in bounds], bounds[0][0], Ttop, cot)
-        return cot, (g_top + gt if gt is not None else g_top)
+    side, rec = P._side, P._rec
+    n = P.nsteps
+    bounds = [(starts[i], starts[i + 1] if i + 1 < len(starts) else n) for i in range(len(starts))]
+    seg_of = {j: si for si, (j0, j1) in enumerate(bounds) for j in range(j0, j1)}
+    P._set_top(Ttop)
+    for j in range(n):  # the cached dt tensors, made on the main stream before the fork
+        P.dt_tensor(j)
+    states, ready = {}, {}
 
-    def recompute(j0, j1):
+    def recompute(si):
+        j0, j1 = bounds[si]
+        states[j0] = tuple(t.detach().contiguous() for t in ckpt[j0])  # on the main stream
         rec.wait_stream(main)
         with torch.cuda.stream(rec):
-            P._load(*ckpt[j0], Ttop)
-            states = [ckpt[j0]]
-            for j in range(j0, j1 - 1):
-                P.cuda_step(j)
-                st = P._save()
-                for t in st:  # read on the main and replay streams before they are freed
-                    t.record_stream(main)
-                    t.record_stream(P._side)
-                states.append(st)
-        return states
+            if j1 - j0 > 1:
+                P._load(*ckpt[j0], Ttop)
+                for j in range(j0, j1 - 1):
+                    P.cuda_step(j)
+                    st = P._save()
+                    for t in st:  # read on the main and replay streams before they are freed
+                        t.record_stream(main)
+                        t.record_stream(side)
+                    states[j + 1] = st
+            ready[si] = torch.cuda.Event()
+            ready[si].record(rec)
 
-    states = recompute(*bounds[-1])
-    main.wait_stream(rec)
-    for s_i in range(len(bounds) - 1, -1, -1):
-        nxt = recompute(*bounds[s_i - 1]) if s_i > 0 else None
-        cot, gt = P.backward_segment_cuda(states, bounds[s_i][0], Ttop, cot)
+    ev_rep, ev_back = {}, {}
+
+    def replay(j):
+        with torch.cuda.stream(side):
+            side.wait_event(ready[seg_of[j]])
+            if j + 2 in ev_back:  # workspace j % 2 was last read by the backward of step j+2
+                side.wait_event(ev_back[j + 2])
+            P._replay(j % 2, states[j], j)
+            ev_rep[j] = torch.cuda.Event()
+            ev_rep[j].record(side)
+
+    recompute(len(bounds) - 1)
+    replay(n - 1)
+    for j in range(n - 1, -1, -1):
+        si = seg_of[j]
+        if j == bounds[si][1] - 1 and si > 0:
+            recompute(si - 1)  # overlaps this segment's backward
+        if j >= 1:
+            replay(j - 1)
+        main.wait_event(ev_rep[j])
+        cot, gt = P._backward(j % 2, states[j], Ttop, j, cot)
+        ev_back[j] = torch.cuda.Event()
+        ev_back[j].record(main)
         if gt is not None:
             g_top = g_top + gt
-        if nxt is not None:
-            main.wait_stream(rec)
-            states = nxt
+        if j + 2 in states:
+            del states[j + 2]  # its replay and backward are queued; record_stream keeps it safe
+    main.wait_stream(side)
+    main.wait_stream(rec)
     return cot, g_top
 
 
