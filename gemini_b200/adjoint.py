@@ -44,8 +44,9 @@ class DiffProblem:
         self.cuda_diffusion_adjoint = bool(cuda_diffusion_adjoint)
         self.cuda_sweep_adjoint = bool(cuda_sweep_adjoint)
         self.cuda_step_adjoint = bool(cuda_step_adjoint)
-        self._sa = None  # gem_step_adjoint workspaces (two, for the pipelined backward), made on first use
+        self._sa = None  # gem_step_adjoint workspaces (the backward's replay slots), made on first use
         self._side = None  # the replay stream of the pipelined backward
+        self.replay_slots = True  # recompute by replay + finish when k+1 workspaces fit
         self._dtt = {}
         self._capturing = False
         self._graphs = {}  # (Ttop given) -> captured step VJP
@@ -236,7 +237,9 @@ class DiffProblem:
 
     def _workspace(self, i):
         if self._sa is None:
-            self._sa = [None, None]
+            self._sa = []
+        while len(self._sa) <= i:
+            self._sa.append(None)
         if self._sa[i] is None:
             h = ctypes.c_void_p()
             _lib.check(_lib.lib().gem_step_adjoint_create(self.dg.handle, ctypes.byref(h)))
@@ -268,6 +271,31 @@ class DiffProblem:
             p(self.ds.electrovars), p(self.dt_tensor(j)), p(z[0]), p(z[1]), p(z[2]), p(z[3]), p(z[4]),
             p(out[0]), p(out[1]), p(out[2]), p(out[3]), p(out[4]), None if tb is None else p(tb), F._stream()))
         return out, tb
+
+    def _finish(self, i, j):
+        """gem_step_vjp_finish_dev of step j from workspace i (replayed), on the current
+        stream: the state after step j, as the forward writes it, in new tensors."""
+        import torch
+
+        g = self.grid
+        lo = torch.empty((LSP, g.lx3, g.lx2), dtype=torch.float64, device=self.base.device)
+        hi = torch.empty_like(lo)
+        p = F._ptr
+        c = self.cfg.c()
+        _lib.check(_lib.lib().gem_step_vjp_finish_dev(
+            ctypes.byref(c), self.dg.handle, self.ds.work, self._workspace(i), p(self.ds.fluidvars),
+            p(self.ds.fluidauxvars), p(self.ds.electrovars), p(self.dt_tensor(j)), p(lo), p(hi), F._stream()))
+        fv = self.ds.fluidvars.view(self.shape)
+        return (fv[0:LSP].clone(), fv[LSP:2 * LSP].clone(), fv[4 * LSP:].clone(), lo, hi)
+
+    def workspace_bytes(self):
+        """Device bytes of one step adjoint workspace (gem_step_adjoint_create)."""
+        g = self.grid
+        F1 = LSP * (g.lx1 + 4) * (g.lx2 + 4) * (g.lx3 + 4)
+        n1 = LSP * (g.lx1 + 1) * g.lx2 * g.lx3
+        n2 = LSP * g.lx1 * (g.lx2 + 1) * g.lx3
+        n3 = LSP * g.lx1 * g.lx2 * (g.lx3 + 1)
+        return 8 * (23 * F1 + 5 * n1 + n2 + n3 + 3 * LSP * g.lx2 * g.lx3)
 
     def close(self):
         """Release the step adjoint workspaces."""
@@ -455,6 +483,89 @@ def backward_from_checkpoints(P: "DiffProblem", ckpt, Ttop, g_ns, g_Ts):
 
 
 def _backward_cuda(P: "DiffProblem", ckpt, starts, Ttop, cot, g_top):
+    """The CUDA backward over all steps, last first.  With room on the device for k+1 step
+    adjoint workspaces (k: the longest checkpoint segment), each step is replayed once and
+    the replay serves both the recompute of the next state and the step's backward
+    (_backward_cuda_slots); otherwise two workspaces alternate and the recompute runs the
+    plain forward step (_backward_cuda_pingpong)."""
+    import torch
+
+    n = P.nsteps
+    kmax = max((starts[i + 1] if i + 1 < len(starts) else n) - starts[i] for i in range(len(starts)))
+    have = sum(1 for h in (P._sa or []) if h is not None)
+    F1 = 8 * LSP * (P.grid.lx1 + 4) * (P.grid.lx2 + 4) * (P.grid.lx3 + 4)
+    need = max(0, kmax + 1 - have) * P.workspace_bytes() + 2 * kmax * 3 * F1
+    free, _ = torch.cuda.mem_get_info()
+    spare = free + torch.cuda.memory_reserved() - torch.cuda.memory_allocated()
+    if P.replay_slots and need <= 0.8 * spare:
+        return _backward_cuda_slots(P, ckpt, starts, Ttop, cot, g_top, kmax + 1)
+    return _backward_cuda_pingpong(P, ckpt, starts, Ttop, cot, g_top)
+
+
+def _backward_cuda_slots(P: "DiffProblem", ckpt, starts, Ttop, cot, g_top, nslot):
+    """The backward with nslot (>= k+1) replay slots.  The steps are recomputed in the order
+    the backward needs them (segments last first, each from its checkpoint forward) on a
+    second stream: gem_step_vjp_replay_dev of step j into a free slot, then, inside the
+    segment, gem_step_vjp_finish_dev from that slot gives the state before step j+1.  Step
+    j's backward (gem_step_vjp_backward_dev on the main stream) reads its slot and frees it;
+    the next recompute step takes the freed slot.  With k+1 slots the recompute of a segment
+    runs one step behind the backward of the segment after it, so no replay is exposed."""
+    import collections
+
+    import torch
+
+    main = torch.cuda.current_stream()
+    if getattr(P, "_rec", None) is None:
+        P._rec = torch.cuda.Stream()
+    rec = P._rec
+    n = P.nsteps
+    bounds = [(starts[i], starts[i + 1] if i + 1 < len(starts) else n) for i in range(len(starts))]
+    seg_end = {j: j1 for j0, j1 in bounds for j in range(j0, j1)}
+    P._set_top(Ttop)
+    for j in range(n):  # the cached dt tensors, made on the main stream before the fork
+        P.dt_tensor(j)
+    states = {j0: tuple(t.detach().contiguous() for t in ckpt[j0]) for j0, _ in bounds}
+    for i in range(nslot):  # workspaces are made (cudaMalloc) before the pipeline starts
+        P._workspace(i)
+    rec.wait_stream(main)
+    pending = collections.deque(j for j0, j1 in reversed(bounds) for j in range(j0, j1))
+    free = collections.deque(range(nslot))
+    free_ev, slot_of, rep_ev = {}, {}, {}
+
+    def issue():
+        while pending and free:
+            j = pending.popleft()
+            sl = free.popleft()
+            with torch.cuda.stream(rec):
+                if sl in free_ev:  # the slot's last reader: a backward on the main stream
+                    rec.wait_event(free_ev.pop(sl))
+                P._replay(sl, states[j], j)
+                slot_of[j] = sl
+                rep_ev[j] = torch.cuda.Event()
+                rep_ev[j].record(rec)
+                if j + 1 < seg_end[j]:
+                    st = P._finish(sl, j)
+                    for t in st:  # read on the main stream before they are freed
+                        t.record_stream(main)
+                    states[j + 1] = st
+
+    issue()
+    for j in range(n - 1, -1, -1):
+        main.wait_event(rep_ev.pop(j))
+        sl = slot_of.pop(j)
+        cot, gt = P._backward(sl, states.pop(j), Ttop, j, cot)
+        if gt is not None:
+            g_top = g_top + gt
+        ev = torch.cuda.Event()
+        ev.record(main)
+        free_ev[sl] = ev
+        free.append(sl)
+        issue()
+    main.wait_stream(rec)
+    return cot, g_top
+
+
+def _backward_cuda_pingpong(P: "DiffProblem", ckpt, starts, Ttop, cot, g_top):
     """The CUDA backward over all steps, last first, as one pipeline: the replay of step j-1
     (gem_step_vjp_replay_dev, on a side stream, into workspace (j-1) % 2) runs while step j's
     backward runs (workspace j % 2); with checkpoints every k > 1 steps, the recompute of a

@@ -109,6 +109,68 @@ __global__ void ka_post_fwd(GridDev G, const double* __restrict__ F, double* nou
   });
 }
 
+// The forward step's x2 epilogue (rhov12v1 + clean_param(1) + clean_param(2) null fill +
+// rhoe2T + clean_param(3), multifluid.f90:179-233) recomputed from a replay's swept stage F
+// (n | rv | re): the same operations in the same order as the fused x2 sweep's epilogue
+// (products rounded where that kernel rounds them through shared memory), so the interior
+// ns, rv, vs1, Ts written into B are the forward step's bits. Ghost cells get the swept n and
+// rv, which k_ghost_epilogue then turns into the forward's ghost values.
+__global__ void ka_finish_fwd(GridDev G, const double* __restrict__ F, Blocks B) {
+  const Dims d = G.d;
+  const long long ng = d.ng;
+  const double* fn = F;
+  const double* frv = F + LSP * ng;
+  const double* fre = F + 2 * LSP * ng;
+  for_rows(d, [&](long long k, int i1, int i2, int i3, bool in) {
+    if (!in) {
+      for (int s = 0; s < LSP - 1; ++s) {
+        B.ns(s)[k] = fn[s * ng + k];
+        B.rv(s)[k] = frv[s * ng + k];
+      }
+      return;
+    }
+    const bool nul = is_null(G, i1, i2, i3);
+    double npre = 0.0, chrg = 0.0, npost = 0.0;
+    for (int s = 0; s < LSP - 1; ++s) {
+      const double n = fn[s * ng + k], r = frv[s * ng + k], e = fre[s * ng + k];
+      const double v = r / (c_ms[s] * fmax_f(n, MINDENSDIV));
+      npre = npre + n;
+      chrg = __dadd_rn(chrg, __dmul_rn(__dmul_rn(n, c_qs[s]), v));
+      npost = npost + fmax_f(n, MINDENS);
+      double nc = fmax_f(n, MINDENS);
+      if (nul) nc = (s == 0) ? MINDENSNULL * 1e-2 : MINDENSNULL;
+      double T = fmax_f((c_gammas[s] - 1) / KB * e / fmax_f(nc, MINDENSDIV), 100.0);
+      if (nul) T = 100;
+      B.ns(s)[k] = nc;
+      B.rv(s)[k] = r;
+      B.vs1(s)[k] = nul ? 0.0 : v;
+      B.Ts(s)[k] = T;
+    }
+    const int s = LSP - 1;
+    const double ve = -1 / fmax_f(npre, MINDENSDIV) / c_qs[LSP - 1] * chrg;
+    const double ne = nul ? MINDENSNULL : npost;
+    double T = fmax_f((c_gammas[s] - 1) / KB * fre[s * ng + k] / fmax_f(ne, MINDENSDIV), 100.0);
+    if (nul) T = 100;
+    B.ns(s)[k] = ne;
+    B.vs1(s)[k] = nul ? 0.0 : ve;
+    B.Ts(s)[k] = T;
+  });
+}
+
+// The two boundary faces of every x1 column (the state's lo / hi), read from a face array:
+// the inverse of ka_set_faces.
+__global__ void ka_get_faces(Dims d, const double* __restrict__ v1i, double* lo, double* hi) {
+  const long long ncol = (long long)d.lx2 * d.lx3;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncol * LSP;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(t / ncol);
+    const long long c = t - s * ncol;
+    const int i2 = (int)(c % d.lx2) + 1, i3 = (int)(c / d.lx2) + 1;
+    lo[t] = v1i[s * nf1(d) + f1i(d, 1, i2, i3)];
+    hi[t] = v1i[s * nf1(d) + f1i(d, d.lx1 + 1, i2, i3)];
+  }
+}
+
 // Adjoint of rhov12v1 + clean_param(1) + rhoe2T + clean_param(3) (multifluid.f90:218-233,
 // 553-688): from the cotangents of the step's n and v1 outputs (interior), of the diffusion
 // input T (TPb) and of the diffusion's n input (NDb), the cotangents of the swept n, rv, re
@@ -635,6 +697,47 @@ int gem_step_vjp_replay_dev(const gem_cfg* cfg, const gem_grid* g, const gem_wor
   double* TP = WF + F;
   ka_post_fwd<<<ngb, 256, 0, st>>>(G, Sx[3], NO, TP);
   GEM_LAUNCHED("ka_post_fwd");
+  return GEM_OK;
+}
+
+int gem_step_vjp_finish_dev(const gem_cfg* cfg, const gem_grid* g, gem_work* w, const gem_step_adjoint* A,
+                            double* fluidvars, double* fluidauxvars, const double* electrovars, const double* dt,
+                            double* v1i_lo, double* v1i_hi, void* stream) {
+  int rc = step_adjoint_check(cfg, g, w, A);
+  if (rc) return rc;
+  if (!fluidvars || !fluidauxvars || !electrovars || !dt || !v1i_lo || !v1i_hi)
+    return set_err(GEM_EINVAL, "null argument");
+  cudaStream_t st = S(stream);
+  const GridDev& G = g->dev;
+  const Dims& d = G.d;
+  const long long ncol = (long long)d.lx2 * d.lx3;
+  Blocks B = blocks(g, fluidvars, fluidauxvars);
+  // the x2 sweep's epilogue from the replay's last stage, then the rest of gem_fluid_adv_dev
+  ka_finish_fwd<<<grid_for(d.ng, 256), 256, 0, st>>>(G, A->ST + 9 * A->F, B);
+  GEM_LAUNCHED("ka_finish_fwd");
+  k_ghost_epilogue<<<grid_for(d.ng, 256), 256, 0, st>>>(G, B);
+  GEM_LAUNCHED("k_ghost_epilogue");
+  if (G.has_null && (G.gridflag == 0 || G.gridflag == 1)) {
+    k_clean_vel_edges<<<grid_for(ncol * LSP, 128), 128, 0, st>>>(G, fluidvars + LSP * d.ng);
+    GEM_LAUNCHED("k_clean_vel_edges");
+  }
+  DiffArgs da;
+  da.G = G;
+  da.B = B;
+  da.J1 = electrovars + 3 * d.ng;
+  da.nn = w->nn;
+  da.Tn = w->Tn;
+  da.dtp = dt;
+  da.Teinf = cfg->Teinf;
+  da.Ttop = w->Ttop;
+  da.coef = w->dcoef;
+  da.solver = cfg->diffsolvetype;
+  da.fused = 1;
+  if ((rc = launch_diffusion(g, da, st))) return rc;
+  // the boundary faces the forward's x1 sweep stores for the next step: the replay's x1
+  // interface velocities there (the same formulas, advec.f90:170-196)
+  ka_get_faces<<<grid_for(ncol * LSP, 256), 256, 0, st>>>(d, A->V1, v1i_lo, v1i_hi);
+  GEM_LAUNCHED("ka_get_faces");
   return GEM_OK;
 }
 

@@ -181,6 +181,18 @@ int gem_step_vjp_backward_dev(const gem_cfg* cfg, const gem_grid* g, const gem_w
                               const double* ns_bar_out, const double* vs1_bar_out, const double* Ts_bar_out,
                               const double* lo_bar_out, const double* hi_bar_out, double* ns_bar, double* vs1_bar,
                               double* Ts_bar, double* lo_bar, double* hi_bar, double* Ttop_bar, void* stream);
+/* The rest of the forward step from a replayed workspace: the x2 sweep's epilogue
+ * (rhov12v1, clean_param, rhoe2T) from the replay's last stage, the ghost epilogue and the
+ * energy diffusion, written into fluidvars / fluidauxvars (ns, vs1, Ts and the auxiliary
+ * blocks; vs2, vs3 untouched) as gem_fluid_adv_dev on the same state and dt writes them,
+ * and the new x1 boundary faces into v1i_lo / v1i_hi ((LSP, lx3, lx2), i2 fastest).  A
+ * checkpointed backward recomputes a segment's states with replay + finish, so each step's
+ * replay serves both the recompute and that step's backward.  Call it after
+ * gem_step_vjp_replay_dev on the same workspace (ordered on the device); it leaves the
+ * workspace's replay intact. */
+int gem_step_vjp_finish_dev(const gem_cfg* cfg, const gem_grid* g, gem_work* w, const gem_step_adjoint* a,
+                            double* fluidvars, double* fluidauxvars, const double* electrovars, const double* dt,
+                            double* v1i_lo, double* v1i_hi, void* stream);
 
 /* No counterpart in the reference.  dt_calc (the same result as gem_dt_calc_dev) for callers
  * that cannot allocate device memory or hold a gem_work (for example code that runs inside

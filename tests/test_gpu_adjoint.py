@@ -345,3 +345,50 @@ def test_combined_step_vjp_entry_equals_its_halves():
         assert torch.equal(x, y)
     assert torch.equal(tb, top_h)
     P.close()
+
+
+@pytest.mark.parametrize("name,mk,kw,floor_free", STEP_CASES, ids=[c[0] for c in STEP_CASES])
+@pytest.mark.parametrize("solver", [2, 1])
+def test_replay_finish_gives_the_forward_step(name, mk, kw, floor_free, solver):
+    """gem_step_vjp_replay_dev + gem_step_vjp_finish_dev from the state before a step give
+    the forward step's next state (ns, vs1, Ts with their ghost cells, the boundary faces)
+    bit for bit, so a backward that recomputes by replay + finish sees the forward's states."""
+    import torch
+
+    g = mk()
+    st = S.init_state(g, **kw)
+    P = AD.DiffProblem(g, st, 3, checkpoint_every=1, diffsolvetype=solver)
+    rng = np.random.default_rng(5)
+    I = (slice(2, g.lx3 + 2), slice(2, g.lx2 + 2), slice(2, g.lx1 + 2))
+    Ttop = torch.from_numpy(st.Teinf * (1 + 0.05 * rng.uniform(-1, 1, (g.lx3, g.lx2)))).cuda()
+    fin, ck = P.run(P.base[(slice(0, 6),) + I].clone(), Ttop, keep=True)
+    P._set_top(Ttop)
+    for j in range(3):
+        P._replay(0, ck[j], j)
+        got = P._finish(0, j)
+        want = ck[j + 1] if j + 1 < 3 else fin
+        for name_, x, y in zip(("ns", "vs1", "Ts", "lo", "hi"), got, want):
+            assert torch.equal(x, y), (j, name_, float((x - y).abs().max()))
+    P.close()
+
+
+def test_slot_backward_equals_two_workspace_backward():
+    """The backward that recomputes by replay + finish into k+1 slots and the one that
+    recomputes with the plain forward step into two alternating workspaces give the same
+    gradients bit for bit (checkpoints every 3 steps over 8 steps: uneven segments)."""
+    import torch
+
+    grads = []
+    for slots in (True, False):
+        g, P, n0, Ttop, tT, tn = _problem(nsteps=8, k=3)
+        P.replay_slots = slots
+        a = n0.clone().requires_grad_(True)
+        t = Ttop.clone().requires_grad_(True)
+        ns, Ts = AD.FluidAdvance.apply(a, t, P)
+        AD.misfit(ns, Ts, tT, tn, g).backward()
+        grads.append((a.grad, t.grad))
+        nws = len(P._sa)
+        P.close()
+        assert nws == (4 if slots else 2)
+    for x, y in zip(*grads):
+        assert torch.equal(x, y)
