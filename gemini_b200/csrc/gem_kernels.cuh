@@ -692,6 +692,17 @@ __device__ __forceinline__ void cell_metric(const GridDev& G, long long k, int f
 }
 
 // ---- x2 / x3 sweeps ---------------------------------------------------------------------
+// asynchronous global -> shared copies (cp.async, 8 bytes per thread) and their groups
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 template <int DIM, bool UNIT, bool FUSED>
 __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
   const GridDev& G = P.G;
@@ -820,8 +831,47 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
     vq = vcell(0);
     vq1 = vcell(1);
   }
+  // Fused x2 on non-unit grids: the metrics change from cell to cell along x2 and the 7
+  // species warps of the block read the same ones, so the block fetches them once, three
+  // steps ahead, into a 4-slot shared ring (cp.async; warp s copies table s, warp 0 also
+  // table 7): step j reads slot j&3 -- face j's hc, yhc, ha2i0, ha2i1 and cell j-1's ha1,
+  // yha1 for frank 0 and 1.  Every step ends in a block barrier (the epilogue's, or its
+  // own for j < 2), and a thread waits for its copies two steps old before it, so step j+3's
+  // slot is complete and visible when step j+3 starts, and the slot written during step j
+  // was last read during step j-1, before that step's barrier.
+  constexpr bool SMETA = FUSED && DIM == 2 && !UNIT;
+  __shared__ double sh_m[SMETA ? 4 : 1][SMETA ? 8 : 1][32];
+  auto meta_issue = [&](int jj) {
+    if constexpr (SMETA) {
+      if (jj >= 1 && jj <= lx + 1) {
+        double* slot = &sh_m[jj & 3][0][0];
+        auto one = [&](int t) {
+          const double* src;
+          if (t < 4) {
+            const long long fk = fmet(jj);
+            src = (t == 0 ? FT.hc : t == 1 ? FT.yhc : t == 2 ? FT.ha2i0 : FT.ha2i1) + fk;
+          } else {
+            if (jj < 2) return;
+            const long long ck = cmet(jj - 1);
+            src = (t == 4 ? G.ha1_0 : t == 5 ? G.yha1_0 : t == 6 ? G.ha1_1 : G.yha1_1) + ck;
+          }
+          cp_async8(slot + t * 32 + threadIdx.x, src);
+        };
+        one(s);
+        if (s == 0) one(7);
+      }
+      cp_async_commit();
+    }
+  };
+  if constexpr (SMETA) {
+    meta_issue(1);
+    meta_issue(2);
+    cp_async_wait<0>();
+    __syncthreads();
+  }
 
   for (int j = 0; j <= lx + 1; ++j) {
+    meta_issue(j + 3);
     // values of this step
     double fn[3];
     if (FUSED && DIM == 3 && j + 1 > lx) {
@@ -849,12 +899,17 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
         v = 0.5 * (vprev + vc);
         vprev = vc;
       }
-      const long long fk = fmet(j);
       const double dxc = __ldg(L.dx + j);
       if (UNIT) {
         F = make_face(v, 1.0, 1.0, dxc, dt);
         ha2j0 = ha2j1 = 1.0;
+      } else if constexpr (SMETA) {
+        const double* m = &sh_m[j & 3][0][threadIdx.x];
+        F = make_face(v, m[0], m[32], dxc, dt);
+        ha2j0 = m[64];
+        ha2j1 = m[96];
       } else {
+        const long long fk = fmet(j);
         F = make_face(v, __ldg(FT.hc + fk), __ldg(FT.yhc + fk), dxc, dt);
         ha2j0 = __ldg(FT.ha2i0 + fk);
         ha2j1 = __ldg(FT.ha2i1 + fk);
@@ -866,9 +921,19 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
     if (j >= 2) {
       dxi = __ldg(L.dxi + j - 2);
       ydxi = __ldg(L.ydxi + j - 2);
-      const long long ck = cmet(j - 1);
-      cell_metric<UNIT>(G, ck, 0, ha1_0, yha1_0);
-      if (frank[0] == 1 || frank[1] == 1) cell_metric<UNIT>(G, ck, 1, ha1_1, yha1_1);
+      if constexpr (SMETA) {
+        const double* m = &sh_m[j & 3][4][threadIdx.x];
+        ha1_0 = m[0];
+        yha1_0 = m[32];
+        if (frank[0] == 1 || frank[1] == 1) {
+          ha1_1 = m[64];
+          yha1_1 = m[96];
+        }
+      } else {
+        const long long ck = cmet(j - 1);
+        cell_metric<UNIT>(G, ck, 0, ha1_0, yha1_0);
+        if (frank[0] == 1 || frank[1] == 1) cell_metric<UNIT>(G, ck, 1, ha1_1, yha1_1);
+      }
     }
     double outv[3];
 #pragma unroll
@@ -893,6 +958,12 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
     }
     ha2prev0 = ha2j0;
     ha2prev1 = ha2j1;
+    if constexpr (SMETA) {
+      if (j < 2) {
+        cp_async_wait<2>();
+        __syncthreads();
+      }
+    }
     if (j < 2) continue;
     const int c = j - 1;  // finished cell
     const long long kc = cell(c);
@@ -928,6 +999,7 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
           B.Ts(s)[kc] = T;
         }
       }
+      if constexpr (SMETA) cp_async_wait<2>();
       __syncthreads();
       if (s == LSP - 1) {
         double npre = 0.0, chrg = 0.0, npost = 0.0;
@@ -950,6 +1022,7 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
       }
     }
   }
+  if constexpr (SMETA) cp_async_wait<0>();
 }
 
 template <int DIM, bool UNIT, bool FUSED>
