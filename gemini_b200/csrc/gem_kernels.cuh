@@ -1078,16 +1078,61 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
   }
   double carry_sl[3] = {0.0, 0.0, 0.0}, carry_P[3] = {0.0, 0.0, 0.0};
   const int nchunk = (n + 2 + 31) / 32;
+  // Fused: each warp stages its next chunk while it computes this one, by cp.async into a
+  // two-slot ring of its own in shared memory -- the fields' values at x1 indices
+  // 32c-1 .. 32c+32 (clamped to the ghost n+2), the cell velocities there (indices outside
+  // 1..n read cell 1, as the unstaged loads do) and, on non-unit grids, the chunk's face
+  // (hc, yhc, ha2i0) and cell (ha1, yha1) metrics.  Only the warp reads its slots: it waits
+  // for its own copies and __syncwarp orders them; the __syncwarp ending a chunk frees the
+  // slot that the next chunk's staging overwrites.
+  constexpr int XW = 34;
+  __shared__ double xs_f[FUSED ? LSP : 1][2][4][XW];
+  __shared__ double xs_m[(FUSED && !UNIT) ? LSP : 1][2][5][32];
+  auto x1_issue = [&](int cc) {
+    if constexpr (FUSED) {
+      if (cc < nchunk) {
+        const int slot = cc & 1;
+        for (int t = lane; t < XW; t += 32) {
+          const int e = 32 * cc - 1 + t;
+          const int ef = (e <= n + 2) ? e : n + 2;
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+            if (f < nf) cp_async8(&xs_f[s][slot][f][t], fld[f] + col + ef);
+          cp_async8(&xs_f[s][slot][3][t], V1 + ((e >= 1 && e <= n) ? e : 1));
+        }
+        if constexpr (!UNIT) {
+          const int pp = 32 * cc + lane;
+          const int ppc = (pp <= n + 1) ? pp : n + 1;
+          const long long fk = fmi(FT, (ppc >= 1) ? ppc : 1, i2, i3);
+          cp_async8(&xs_m[s][slot][0][lane], FT.hc + fk);
+          cp_async8(&xs_m[s][slot][1][lane], FT.yhc + fk);
+          cp_async8(&xs_m[s][slot][2][lane], FT.ha2i0 + fk);
+          const int qq = (ppc - 1 >= 1 && ppc - 1 <= n) ? ppc - 1 : 1;
+          const long long ck = cmi(G, qq, i2, i3);
+          cp_async8(&xs_m[s][slot][3][lane], G.ha1_0 + ck);
+          cp_async8(&xs_m[s][slot][4][lane], G.yha1_0 + ck);
+        }
+      }
+      cp_async_commit();
+    }
+  };
+  x1_issue(0);
   for (int c = 0; c < nchunk; ++c) {
     const int p = 32 * c + lane;  // 0 .. n+1 when active
     const bool act = p <= n + 1;
     const int pc = act ? p : n + 1;  // clamped for loads
+    x1_issue(c + 1);
+    if constexpr (FUSED) {
+      cp_async_wait<1>();
+      __syncwarp();
+    }
+    const double* sf = &xs_f[FUSED ? s : 0][c & 1][0][0];
+    const double* sm = &xs_m[(FUSED && !UNIT) ? s : 0][c & 1][0][0];
     // face p velocity (p >= 1)
     double v = 0.0;
     if (FUSED) {
-      const double vcur = V1[(pc >= 1 && pc <= n) ? pc : 1];
-      double vleft = __shfl_up_sync(0xffffffffu, vcur, 1);
-      if (lane == 0) vleft = V1[(pc - 1 >= 1) ? pc - 1 : 1];
+      const double vcur = sf[3 * XW + lane + 1];
+      const double vleft = sf[3 * XW + lane];
       if (pc == 1) v = vface1;
       else if (pc == n + 1) v = vfaceN;
       else v = 0.5 * (vleft + vcur);
@@ -1103,6 +1148,9 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
     {
       if (UNIT) {
         F = make_face(v, 1.0, 1.0, dxc, dt);
+      } else if constexpr (FUSED) {
+        F = make_face(v, sm[lane], sm[32 + lane], dxc, dt);
+        ha2 = sm[64 + lane];
       } else {
         const long long fk = fmi(FT, pf, i2, i3);
         F = make_face(v, __ldg(FT.hc + fk), __ldg(FT.yhc + fk), dxc, dt);
@@ -1115,17 +1163,29 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
     if (q >= 1 && q <= n) {
       dxi = __ldg(L.dxi + q - 1);
       ydxi = __ldg(L.ydxi + q - 1);
-      cell_metric<UNIT>(G, cmi(G, q, i2, i3), 0, ha1, yha1);
+      if constexpr (FUSED && !UNIT) {
+        ha1 = sm[96 + lane];
+        yha1 = sm[128 + lane];
+      } else {
+        cell_metric<UNIT>(G, cmi(G, q, i2, i3), 0, ha1, yha1);
+      }
     }
     double outv[3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
       if (f < nf) {
         const double* fc = fld[f] + col;
-        const double f0 = fc[pc];
-        const double fpl = fc[pc + 1];
-        double fm = __shfl_up_sync(0xffffffffu, f0, 1);
-        if (lane == 0) fm = fc[pc - 1];
+        double f0, fpl, fm;
+        if constexpr (FUSED) {
+          fm = sf[f * XW + lane];
+          f0 = sf[f * XW + lane + 1];
+          fpl = sf[f * XW + lane + 2];
+        } else {
+          f0 = fc[pc];
+          fpl = fc[pc + 1];
+          fm = __shfl_up_sync(0xffffffffu, f0, 1);
+          if (lane == 0) fm = fc[pc - 1];
+        }
         // slope(p) (advec.f90:407-414) with lslope = rslope(p-1) from the lane below
         const double rs = mdiv(fpl - f0, dxn, ydxn);
         double ls = __shfl_up_sync(0xffffffffu, rs, 1);
