@@ -784,11 +784,6 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
       out[0] = r.x[0]; out[1] = r.x[1]; out[2] = r.x[2];
     }
   };
-  auto vcell = [&](int j) -> double {  // cell velocity for on-the-fly faces (fused)
-    if (DIM == 3) return B.vs3(s)[cell(map3(j))];
-    const int jj = (j < 1) ? 1 : (j > lx ? lx : j);
-    return B.vs2(s)[cell(jj)];
-  };
 
   if (lx <= 1) {
     // advec1D_MC_curv passes a single-cell line through; the fused x3 sweep still
@@ -823,14 +818,38 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
     }
   }
   double ha2prev0 = 0.0, ha2prev1 = 0.0;
-  // prefetch pipeline: raw values of f(j+1) (next) and f(j+2) (next2); fused cell
-  // velocities v(j) (vq) and v(j+1) (vq1); vprev = v(j-1)
-  Raw next = load_raw(1), next2 = load_raw(2);
-  double vprev = 0.0, vq = 0.0, vq1 = 0.0;
-  if (FUSED) {
-    vq = vcell(0);
-    vq1 = vcell(1);
+  // prefetch pipeline.  Unfused: raw values of f(j+1) (next) and f(j+2) (next2) in
+  // registers.  Fused: each warp stages, three steps ahead, the raw values of f(jj) and the
+  // cell velocity v(jj-1) by cp.async into slot jj&3 of a 4-slot shared ring of its own;
+  // step j reads slot (j+1)&3.  The sweep writes cell j-1 in place at step j, behind every
+  // staged index (up to j+4).  vprev = v(j-1).
+  Raw next, next2;
+  if constexpr (!FUSED) {
+    next = load_raw(1);
+    next2 = load_raw(2);
   }
+  double vprev = 0.0;
+  __shared__ double xm_f[FUSED ? LSP : 1][4][4][32];
+  auto stage = [&](int jj) {
+    if constexpr (FUSED) {
+      if (jj >= 1 && jj <= lx + 2) {
+        double* sl = &xm_f[s][jj & 3][0][threadIdx.x];
+        if constexpr (DIM == 3) {
+          const long long k = cell(map3(jj));
+          cp_async8(sl, B.ns(s) + k);
+          if (s < LSP - 1) cp_async8(sl + 32, B.vs1(s) + k);
+          cp_async8(sl + 64, B.Ts(s) + k);
+          cp_async8(sl + 96, B.vs3(s) + cell(map3(jj - 1)));
+        } else {
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+            if (f < nf) cp_async8(sl + 32 * f, fld[f] + cell(jj));
+          const int jv = (jj - 1 < 1) ? 1 : (jj - 1 > lx ? lx : jj - 1);
+          cp_async8(sl + 96, B.vs2(s) + cell(jv));
+        }
+      }
+    }
+  };
   // Fused x2 on non-unit grids: the metrics change from cell to cell along x2 and the 7
   // species warps of the block read the same ones, so the block fetches them once, three
   // steps ahead, into a 4-slot shared ring (cp.async; warp s copies table s, warp 0 also
@@ -860,33 +879,54 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
         one(s);
         if (s == 0) one(7);
       }
-      cp_async_commit();
     }
   };
-  if constexpr (SMETA) {
+  // one cp.async group per step: the group committed at step j holds the metrics of step
+  // j+3 and the staged values of slot (j+4)&3 (read at step j+3); the prologue commits the
+  // groups that steps 0..2 read
+  if constexpr (FUSED) {
     meta_issue(1);
+    stage(1);
+    cp_async_commit();
     meta_issue(2);
+    stage(2);
+    cp_async_commit();
+    stage(3);
+    cp_async_commit();
+  }
+  if constexpr (SMETA) {
     cp_async_wait<0>();
     __syncthreads();
   }
 
   for (int j = 0; j <= lx + 1; ++j) {
-    meta_issue(j + 3);
     // values of this step
     double fn[3];
-    if (FUSED && DIM == 3 && j + 1 > lx) {
+    double vc = 0.0;  // v(j)
+    if constexpr (FUSED) {
+      __syncwarp();  // every lane is done with the slot staged below (read at step j-1)
+      meta_issue(j + 3);
+      stage(j + 4);
+      cp_async_commit();
+      cp_async_wait<3>();  // this thread's copies of step j-3's group (slot (j+1)&3)
+      __syncwarp();
+      const double* sl = &xm_f[s][(j + 1) & 3][0][threadIdx.x];
+      if (DIM == 3 && j + 1 > lx) {
 #pragma unroll
-      for (int f = 0; f < 3; ++f) fn[f] = per ? ((j + 1 == lx + 1) ? wrap1[f] : wrap2[f]) : run[f].fc;
+        for (int f = 0; f < 3; ++f) fn[f] = per ? ((j + 1 == lx + 1) ? wrap1[f] : wrap2[f]) : run[f].fc;
+      } else {
+        Raw nx;
+        nx.x[0] = sl[0];
+        nx.x[1] = (DIM == 3) ? ((s < LSP - 1) ? sl[32] : 0.0) : ((nf > 1) ? sl[32] : 0.0);
+        nx.x[2] = (DIM == 3 || nf > 2) ? sl[64] : 0.0;
+        fields_of(nx, fn);
+      }
+      vc = sl[96];
     } else {
       fields_of(next, fn);
-    }
-    const double vc = vq;  // v(j)
-    // issue the loads two steps ahead
-    next = next2;
-    if (j + 3 <= lx + 2) next2 = load_raw(j + 3);
-    if (FUSED) {
-      vq = vq1;
-      if (j + 2 <= lx + 1) vq1 = vcell(j + 2);
+      // issue the loads two steps ahead
+      next = next2;
+      if (j + 3 <= lx + 2) next2 = load_raw(j + 3);
     }
 
     Face F = {0.0, 0.0, 0.0, 0.0};
@@ -1022,7 +1062,10 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
       }
     }
   }
-  if constexpr (SMETA) cp_async_wait<0>();
+  if constexpr (FUSED) {  // nothing in flight when the next work item (batched path) restages
+    cp_async_wait<0>();
+    __syncwarp();
+  }
 }
 
 template <int DIM, bool UNIT, bool FUSED>
