@@ -697,6 +697,12 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+// the same with zero fill when !valid (no bytes read; src must still be a valid address)
+__device__ __forceinline__ void cp_async8z(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(valid ? 8 : 0)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -1751,22 +1757,17 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
     const double tn1 = __ldg(P.Tn + ci(d, 1, i2, i3)), tnl = __ldg(P.Tn + ci(d, n, i2, i3));
     const double tinf = P.Ttop ? __ldg(P.Ttop + (i2 - 1) + (long long)d.lx2 * (i3 - 1)) : P.Teinf;
     int lp = lp0, kp = kp0;
-    // independent chunks: unrolled so that their loads are in flight together
+    // global -> shared by cp.async, every chunk's copies in flight together (zero fill for
+    // the padding rows past n and for bq of the ions)
 #pragma unroll 4
     for (int c = 0; c < M; ++c) {
       const int i = 1 + 32 * c + lane;
-      double T = 0.0, qm = 0.0, qp = 0.0, bq = 0.0;
-      if (i <= n) {
-        const long long q = q0 + i;
-        T = Tcol[i];
-        qm = P.coef[(long long)s * nc + q];
-        qp = P.coef[(long long)(LSP + s) * nc + q];
-        if (s == LSP - 1) bq = P.coef[(long long)2 * LSP * nc + q];
-      }
-      W.at_lane(DA_T, kp, lp) = T;
-      W.at_lane(DA_QM, kp, lp) = qm;
-      W.at_lane(DA_QP, kp, lp) = qp;
-      W.at_lane(DA_BQ, kp, lp) = bq;
+      const bool in = i <= n;
+      const long long q = q0 + (in ? i : 1);
+      cp_async8z(&W.at_lane(DA_T, kp, lp), Tcol + (in ? i : 1), in);
+      cp_async8z(&W.at_lane(DA_QM, kp, lp), P.coef + (long long)s * nc + q, in);
+      cp_async8z(&W.at_lane(DA_QP, kp, lp), P.coef + (long long)(LSP + s) * nc + q, in);
+      cp_async8z(&W.at_lane(DA_BQ, kp, lp), P.coef + (long long)2 * LSP * nc + q, in && s == LSP - 1);
       kp += r32;
       lp += q32;
       if (kp >= M) {
@@ -1774,6 +1775,8 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
         ++lp;
       }
     }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncwarp();
     const double Tprev = __shfl_up_sync(0xffffffffu, W.at(DA_T, M - 1), 1);
     const double Tnext = __shfl_down_sync(0xffffffffu, W.at(DA_T, 0), 1);
