@@ -1796,6 +1796,25 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
     // identity rows: Dirichlet rows 1 and lx1 (PDEparabolic.f90:59-63, 131-136) and padding
     // Dirichlet rows i = 1 and i = n and the padding rows past n are identity rows
     auto ident_rhs = [&](int i) -> double { return (i == 1) ? tmin : (i == n) ? tmax : 0.0; };
+    // fused store phase: ns (for T2rhoe) staged by cp.async into the T rows once T is dead
+    // (after the last right-hand side), its copies in flight during the last stage's solve
+    auto stage_ns = [&]() {
+      if (!P.fused) return;
+      __syncwarp();  // every lane is done reading its T rows
+      int lq = lp0, kq = kp0;
+      for (int c = 0; c < M; ++c) {
+        const int i = 1 + 32 * c + lane;
+        const bool in = i <= n;
+        cp_async8z(&W.at_lane(DA_T, kq, lq), ncol + (in ? i : 1), in);
+        kq += r32;
+        lq += q32;
+        if (kq >= M) {
+          kq -= M;
+          ++lq;
+        }
+      }
+      cp_async_commit();
+    };
     if (P.solver == 2) {
       // TR half step (PDEparabolic.f90:66-127), A = E = 0
       const double dt2 = dt / 2, ydt2 = 1 / (dt / 2);  // 1/(dt/2) is also the diagonal term
@@ -1836,6 +1855,7 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
           r = -mdiv(1 / 3.0 * W.at(DA_T, k), dt3, ydt3) + mdiv(4 / 3.0 * W.at(DA_R, k), dt3, ydt3);
         W.at(DA_RHS, k) = r;
       }
+      stage_ns();
       auto rowBDF = [&](int k, double& a, double& b, double& c) {
         const int i = 1 + lane * M + k;
         if (i == 1 || i >= n) {
@@ -1855,6 +1875,7 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
         const int i = 1 + lane * M + k;
         W.at(DA_RHS, k) = (i == 1 || i >= n) ? ident_rhs(i) : mdiv(W.at(DA_T, k), dt, ydt);
       }
+      stage_ns();
       auto rowBE = [&](int k, double& a, double& b, double& c) {
         const int i = 1 + lane * M + k;
         if (i == 1 || i >= n) {
@@ -1871,6 +1892,7 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
     // ---- store: max(T,100) (multifluid.f90:340); fused: clean_param(3) and T2rhoe
     // written along x1 (coalesced): row idx = 32c + lane sits in slot (idx/M, idx%M)
     double* Tout = P.B.Ts(s) + m0;
+    if (P.fused) cp_async_wait<0>();
     __syncwarp();
     {
       int lq = lp0, kq = kp0;
@@ -1882,7 +1904,7 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
           if (P.fused) {
             if (is_null(G, i, i2, i3)) T = 100;
             Tout[i] = T;
-            P.B.re(s)[m0 + i] = conv_re(ncol[i], T, s);
+            P.B.re(s)[m0 + i] = conv_re(W.at_lane(DA_T, kq, lq), T, s);
           } else {
             Tout[i] = T;
           }
