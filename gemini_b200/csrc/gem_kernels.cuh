@@ -824,34 +824,31 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
     }
   }
   double ha2prev0 = 0.0, ha2prev1 = 0.0;
-  // prefetch pipeline.  Unfused: raw values of f(j+1) (next) and f(j+2) (next2) in
-  // registers.  Fused: each warp stages, three steps ahead, the raw values of f(jj) and the
-  // cell velocity v(jj-1) by cp.async into slot jj&3 of a 4-slot shared ring of its own;
-  // step j reads slot (j+1)&3.  The sweep writes cell j-1 in place at step j, behind every
-  // staged index (up to j+4).  vprev = v(j-1).
-  Raw next, next2;
-  if constexpr (!FUSED) {
-    next = load_raw(1);
-    next2 = load_raw(2);
-  }
+  // prefetch pipeline: each warp stages, three steps ahead, the raw values of f(jj) and the
+  // velocity of step jj-1 (fused: the cell velocity v(jj-1); unfused: the face velocity
+  // of face jj-1) by cp.async into slot jj&3 of a 4-slot shared ring of its own; step j
+  // reads slot (j+1)&3.  The sweep writes cell j-1 in place at step j, behind every staged
+  // index (up to j+4).  vprev = v(j-1).
   double vprev = 0.0;
-  __shared__ double xm_f[FUSED ? LSP : 1][4][4][32];
+  __shared__ double xm_f[LSP][4][4][32];
   auto stage = [&](int jj) {
-    if constexpr (FUSED) {
-      if (jj >= 1 && jj <= lx + 2) {
-        double* sl = &xm_f[s][jj & 3][0][threadIdx.x];
-        if constexpr (DIM == 3) {
-          const long long k = cell(map3(jj));
-          cp_async8(sl, B.ns(s) + k);
-          if (s < LSP - 1) cp_async8(sl + 32, B.vs1(s) + k);
-          cp_async8(sl + 64, B.Ts(s) + k);
-          cp_async8(sl + 96, B.vs3(s) + cell(map3(jj - 1)));
-        } else {
+    if (jj >= 1 && jj <= lx + 2) {
+      double* sl = &xm_f[s][jj & 3][0][threadIdx.x];
+      if constexpr (FUSED && DIM == 3) {
+        const long long k = cell(map3(jj));
+        cp_async8(sl, B.ns(s) + k);
+        if (s < LSP - 1) cp_async8(sl + 32, B.vs1(s) + k);
+        cp_async8(sl + 64, B.Ts(s) + k);
+        cp_async8(sl + 96, B.vs3(s) + cell(map3(jj - 1)));
+      } else {
 #pragma unroll
-          for (int f = 0; f < 3; ++f)
-            if (f < nf) cp_async8(sl + 32 * f, fld[f] + cell(jj));
+        for (int f = 0; f < 3; ++f)
+          if (f < nf) cp_async8(sl + 32 * f, fld[f] + cell(jj));
+        if constexpr (FUSED) {
           const int jv = (jj - 1 < 1) ? 1 : (jj - 1 > lx ? lx : jj - 1);
           cp_async8(sl + 96, B.vs2(s) + cell(jv));
+        } else if (jj >= 2) {
+          cp_async8(sl + 96, P.vsi + (long long)s * ((DIM == 3) ? nf3(d) : nf2(d)) + fvel(jj - 1));
         }
       }
     }
@@ -890,16 +887,14 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
   // one cp.async group per step: the group committed at step j holds the metrics of step
   // j+3 and the staged values of slot (j+4)&3 (read at step j+3); the prologue commits the
   // groups that steps 0..2 read
-  if constexpr (FUSED) {
-    meta_issue(1);
-    stage(1);
-    cp_async_commit();
-    meta_issue(2);
-    stage(2);
-    cp_async_commit();
-    stage(3);
-    cp_async_commit();
-  }
+  meta_issue(1);
+  stage(1);
+  cp_async_commit();
+  meta_issue(2);
+  stage(2);
+  cp_async_commit();
+  stage(3);
+  cp_async_commit();
   if constexpr (SMETA) {
     cp_async_wait<0>();
     __syncthreads();
@@ -908,8 +903,8 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
   for (int j = 0; j <= lx + 1; ++j) {
     // values of this step
     double fn[3];
-    double vc = 0.0;  // v(j)
-    if constexpr (FUSED) {
+    double vc = 0.0;  // fused: v(j); unfused: the velocity of face j
+    {
       __syncwarp();  // every lane is done with the slot staged below (read at step j-1)
       meta_issue(j + 3);
       stage(j + 4);
@@ -917,22 +912,17 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
       cp_async_wait<3>();  // this thread's copies of step j-3's group (slot (j+1)&3)
       __syncwarp();
       const double* sl = &xm_f[s][(j + 1) & 3][0][threadIdx.x];
-      if (DIM == 3 && j + 1 > lx) {
+      if (FUSED && DIM == 3 && j + 1 > lx) {
 #pragma unroll
         for (int f = 0; f < 3; ++f) fn[f] = per ? ((j + 1 == lx + 1) ? wrap1[f] : wrap2[f]) : run[f].fc;
       } else {
         Raw nx;
         nx.x[0] = sl[0];
-        nx.x[1] = (DIM == 3) ? ((s < LSP - 1) ? sl[32] : 0.0) : ((nf > 1) ? sl[32] : 0.0);
-        nx.x[2] = (DIM == 3 || nf > 2) ? sl[64] : 0.0;
+        nx.x[1] = (FUSED && DIM == 3) ? ((s < LSP - 1) ? sl[32] : 0.0) : ((nf > 1) ? sl[32] : 0.0);
+        nx.x[2] = ((FUSED && DIM == 3) || nf > 2) ? sl[64] : 0.0;
         fields_of(nx, fn);
       }
       vc = sl[96];
-    } else {
-      fields_of(next, fn);
-      // issue the loads two steps ahead
-      next = next2;
-      if (j + 3 <= lx + 2) next2 = load_raw(j + 3);
     }
 
     Face F = {0.0, 0.0, 0.0, 0.0};
@@ -940,7 +930,7 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
     if (j >= 1) {
       double v;
       if (!FUSED) {
-        v = P.vsi[(long long)s * ((DIM == 3) ? nf3(d) : nf2(d)) + fvel(j)];
+        v = vc;
       } else {
         v = 0.5 * (vprev + vc);
         vprev = vc;
@@ -1068,10 +1058,9 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
       }
     }
   }
-  if constexpr (FUSED) {  // nothing in flight when the next work item (batched path) restages
-    cp_async_wait<0>();
-    __syncwarp();
-  }
+  // nothing in flight when the next work item (batched path) restages
+  cp_async_wait<0>();
+  __syncwarp();
 }
 
 template <int DIM, bool UNIT, bool FUSED>
@@ -1127,18 +1116,18 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
   }
   double carry_sl[3] = {0.0, 0.0, 0.0}, carry_P[3] = {0.0, 0.0, 0.0};
   const int nchunk = (n + 2 + 31) / 32;
-  // Fused: each warp stages its next chunk while it computes this one, by cp.async into a
-  // two-slot ring of its own in shared memory -- the fields' values at x1 indices
-  // 32c-1 .. 32c+32 (clamped to the ghost n+2), the cell velocities there (indices outside
-  // 1..n read cell 1, as the unstaged loads do) and, on non-unit grids, the chunk's face
-  // (hc, yhc, ha2i0) and cell (ha1, yha1) metrics.  Only the warp reads its slots: it waits
-  // for its own copies and __syncwarp orders them; the __syncwarp ending a chunk frees the
-  // slot that the next chunk's staging overwrites.
+  // Each warp stages its next chunk while it computes this one, by cp.async into a two-slot
+  // ring of its own in shared memory -- the fields' values at x1 indices 32c-1 .. 32c+32
+  // (clamped to the ghost n+2), the velocities (fused: the cells' there, indices outside
+  // 1..n reading cell 1 as the unstaged loads do; unfused: face p of each lane) and, on
+  // non-unit grids, the chunk's face (hc, yhc, ha2i0) and cell (ha1, yha1) metrics.  Only
+  // the warp reads its slots: it waits for its own copies and __syncwarp orders them; the
+  // __syncwarp ending a chunk frees the slot that the next chunk's staging overwrites.
   constexpr int XW = 34;
-  __shared__ double xs_f[FUSED ? LSP : 1][2][4][XW];
-  __shared__ double xs_m[(FUSED && !UNIT) ? LSP : 1][2][5][32];
+  __shared__ double xs_f[LSP][2][4][XW];
+  __shared__ double xs_m[UNIT ? 1 : LSP][2][5][32];
   auto x1_issue = [&](int cc) {
-    if constexpr (FUSED) {
+    {
       if (cc < nchunk) {
         const int slot = cc & 1;
         for (int t = lane; t < XW; t += 32) {
@@ -1147,7 +1136,12 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
 #pragma unroll
           for (int f = 0; f < 3; ++f)
             if (f < nf) cp_async8(&xs_f[s][slot][f][t], fld[f] + col + ef);
-          cp_async8(&xs_f[s][slot][3][t], V1 + ((e >= 1 && e <= n) ? e : 1));
+          if constexpr (FUSED) cp_async8(&xs_f[s][slot][3][t], V1 + ((e >= 1 && e <= n) ? e : 1));
+        }
+        if constexpr (!FUSED) {
+          const int pp = 32 * cc + lane;
+          const int ppc = (pp <= n + 1) ? pp : n + 1;
+          cp_async8(&xs_f[s][slot][3][lane], P.vsi + (long long)s * nf1(d) + f1i(d, (ppc >= 1) ? ppc : 1, i2, i3));
         }
         if constexpr (!UNIT) {
           const int pp = 32 * cc + lane;
@@ -1171,12 +1165,10 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
     const bool act = p <= n + 1;
     const int pc = act ? p : n + 1;  // clamped for loads
     x1_issue(c + 1);
-    if constexpr (FUSED) {
-      cp_async_wait<1>();
-      __syncwarp();
-    }
-    const double* sf = &xs_f[FUSED ? s : 0][c & 1][0][0];
-    const double* sm = &xs_m[(FUSED && !UNIT) ? s : 0][c & 1][0][0];
+    cp_async_wait<1>();
+    __syncwarp();
+    const double* sf = &xs_f[s][c & 1][0][0];
+    const double* sm = &xs_m[UNIT ? 0 : s][c & 1][0][0];
     // face p velocity (p >= 1)
     double v = 0.0;
     if (FUSED) {
@@ -1186,24 +1178,19 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
       else if (pc == n + 1) v = vfaceN;
       else v = 0.5 * (vleft + vcur);
     } else {
-      v = P.vsi[(long long)s * nf1(d) + f1i(d, (pc >= 1) ? pc : 1, i2, i3)];
+      v = sf[3 * XW + lane];
     }
     Face F = {0.0, 0.0, 0.0, 0.0};
     double ha2 = 1.0;
-    const int pf = (pc >= 1) ? pc : 1;
     const double dxc = __ldg(L.dx + pc), ydxc = __ldg(L.ydx + pc);
     const double dxn = __ldg(L.dx + pc + 1), ydxn = __ldg(L.ydx + pc + 1);
     const double dxs = __ldg(L.dxs + pc), ydxs = __ldg(L.ydxs + pc);
     {
       if (UNIT) {
         F = make_face(v, 1.0, 1.0, dxc, dt);
-      } else if constexpr (FUSED) {
+      } else {
         F = make_face(v, sm[lane], sm[32 + lane], dxc, dt);
         ha2 = sm[64 + lane];
-      } else {
-        const long long fk = fmi(FT, pf, i2, i3);
-        F = make_face(v, __ldg(FT.hc + fk), __ldg(FT.yhc + fk), dxc, dt);
-        ha2 = __ldg(FT.ha2i0 + fk);
       }
     }
     // cell p-1 metrics for the update
@@ -1212,29 +1199,18 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
     if (q >= 1 && q <= n) {
       dxi = __ldg(L.dxi + q - 1);
       ydxi = __ldg(L.ydxi + q - 1);
-      if constexpr (FUSED && !UNIT) {
+      if constexpr (!UNIT) {
         ha1 = sm[96 + lane];
         yha1 = sm[128 + lane];
-      } else {
-        cell_metric<UNIT>(G, cmi(G, q, i2, i3), 0, ha1, yha1);
       }
     }
     double outv[3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
       if (f < nf) {
-        const double* fc = fld[f] + col;
-        double f0, fpl, fm;
-        if constexpr (FUSED) {
-          fm = sf[f * XW + lane];
-          f0 = sf[f * XW + lane + 1];
-          fpl = sf[f * XW + lane + 2];
-        } else {
-          f0 = fc[pc];
-          fpl = fc[pc + 1];
-          fm = __shfl_up_sync(0xffffffffu, f0, 1);
-          if (lane == 0) fm = fc[pc - 1];
-        }
+        const double fm = sf[f * XW + lane];
+        const double f0 = sf[f * XW + lane + 1];
+        const double fpl = sf[f * XW + lane + 2];
         // slope(p) (advec.f90:407-414) with lslope = rslope(p-1) from the lane below
         const double rs = mdiv(fpl - f0, dxn, ydxn);
         double ls = __shfl_up_sync(0xffffffffu, rs, 1);
@@ -1275,6 +1251,7 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
     }
     __syncwarp();
   }
+  cp_async_wait<0>();  // nothing in flight when the next work item (batched path) restages
 }
 
 template <bool UNIT, bool FUSED>
@@ -1996,9 +1973,9 @@ struct WarpMemA {
 };
 
 // thermal conductivity lambda(T, n) (collisions.f90:162-199) and its partial derivatives;
-// q: the cell in the interior-only neutral arrays (electrons)
-__device__ __forceinline__ void lam_deriv(const DiffAdjArgs& P, int s, double T, double nv, long long q,
-                                          long long nc, double& lam, double& dl_dT, double& dl_dn) {
+// n1, n2, n3: the neutral densities of the cell (electrons)
+__device__ __forceinline__ void lam_deriv(int s, double T, double nv, double n1, double n2, double n3, double& lam,
+                                          double& dl_dT, double& dl_dn) {
   // the adjoint needs no exact quotients or correctly rounded powers: each reciprocal is
   // formed once and multiplied, and T^2.5 = T^2 sqrt(T) in plain arithmetic
   const double sq = sqrt(T);
@@ -2010,7 +1987,6 @@ __device__ __forceinline__ void lam_deriv(const DiffAdjArgs& P, int s, double T,
     dl_dn = 0.0;
     return;
   }
-  const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
   const double hy = 0.5 * yT * sq;  // 1 / (2 sqrt(T))
   const double ynv = 1.0 / nv;
   const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
@@ -2056,6 +2032,45 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
     const double* Tc = P.T + (long long)s * d.ng + m0;
     const double* nsc = P.ns + (long long)s * d.ng + m0;
     const double c0 = (c_gammas[s] - 1.0) / KB;
+    const bool el = s == LSP - 1;
+    // ---- the column's inputs, global -> shared by cp.async with every chunk in flight (zero
+    //      fill past n): T into T; ns, J1 and the neutral densities into the q-, q+ and
+    //      factorisation rows, the metrics into the cotangent rows (all written later), and
+    //      Ybar into R, where the backward starts
+    {
+      const double* Yb = P.Ybar + (long long)s * d.ng + m0;
+      int lp = lp0, kp = kp0;
+      for (int c = 0; c < M; ++c) {
+        const int i = 1 + 32 * c + lane;
+        const bool in = i <= n;
+        const int ii = in ? i : 1;
+        const long long q = q0 + ii, mk = mm0 + ii;
+        cp_async8z(&W.at_lane(VA_T, kp, lp), Tc + ii, in);
+        cp_async8z(&W.at_lane(VA_QM, kp, lp), nsc + ii, in);
+        cp_async8z(&W.at_lane(VA_R, kp, lp), Yb + ii, in);
+        if (el) {
+          cp_async8z(&W.at_lane(VA_QP, kp, lp), P.J1 + m0 + ii, in);
+          cp_async8z(&W.at_lane(VA_SS, kp, lp), P.nn + q, in);
+          cp_async8z(&W.at_lane(VA_IB, kp, lp), P.nn + nc + q, in);
+          cp_async8z(&W.at_lane(VA_TT, kp, lp), P.nn + 2 * nc + q, in);
+        }
+        if (!UNIT) {
+          cp_async8z(&W.at_lane(VA_Y, kp, lp), G.yh1 + mk, in);
+          cp_async8z(&W.at_lane(VA_QMB, kp, lp), G.h2 + mk, in);
+          cp_async8z(&W.at_lane(VA_QPB, kp, lp), G.h3 + mk, in);
+          cp_async8z(&W.at_lane(VA_BQB, kp, lp), G.yha1_0 + mk, in);
+        }
+        kp += r32;
+        lp += q32;
+        if (kp >= M) {
+          kp -= M;
+          ++lp;
+        }
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncwarp();
+    }
     // ---- pass 1 (along x1): T, D = lambda h2 h3 / h1, C, bq
     {
       int lp = lp0, kp = kp0;
@@ -2063,18 +2078,21 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
         const int i = 1 + 32 * c + lane;
         double T = 0, D = 0, C = 0, bq = 0;
         if (i <= n) {
-          T = Tc[i];
-          const double nv = nsc[i];
-          const long long mk = mm0 + i;
-          const double yh1 = UNIT ? 1.0 : __ldg(G.yh1 + mk);
-          const double h23 = UNIT ? 1.0 : __ldg(G.h2 + mk) * __ldg(G.h3 + mk);
-          const double yha1 = UNIT ? 1.0 : __ldg(G.yha1_0 + mk);
+          T = W.at_lane(VA_T, kp, lp);
+          const double nv = W.at_lane(VA_QM, kp, lp);
+          const double yh1 = UNIT ? 1.0 : W.at_lane(VA_Y, kp, lp);
+          const double h23 = UNIT ? 1.0 : W.at_lane(VA_QMB, kp, lp) * W.at_lane(VA_QPB, kp, lp);
+          const double yha1 = UNIT ? 1.0 : W.at_lane(VA_BQB, kp, lp);
           double lam, dl_dT, dl_dn;
-          lam_deriv(P, s, T, nv, q0 + i, nc, lam, dl_dT, dl_dn);
+          if (el)
+            lam_deriv(s, T, nv, W.at_lane(VA_SS, kp, lp), W.at_lane(VA_IB, kp, lp), W.at_lane(VA_TT, kp, lp), lam,
+                      dl_dT, dl_dn);
+          else
+            lam_deriv(s, T, nv, 0.0, 0.0, 0.0, lam, dl_dT, dl_dn);
           D = lam * h23 * yh1;
           C = c0 / fmax_f(nv, MINDENSDIV) * yha1;
-          if (s == LSP - 1 && i >= 2 && i <= n - 1) {
-            const double beta = 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i];  // collisions.f90:197
+          if (el && i >= 2 && i <= n - 1) {
+            const double beta = 5.0 / 2 * KB / ELCHRG * W.at_lane(VA_QP, kp, lp);  // collisions.f90:197
             bq = C * beta * yh1 * __ldg(L1.ydxs + i);  // 1/(dx1(i) + dx1(i+1))
           }
         }
@@ -2182,22 +2200,7 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
       YOUT = VA_Y;
     }
     __syncwarp();
-    // ---- Ybar along x1 into R, masked by max(T,100) of the output
-    const double* Yb = P.Ybar + (long long)s * d.ng + m0;
-    {
-      int lp = lp0, kp = kp0;
-      for (int c = 0; c < M; ++c) {
-        const int i = 1 + 32 * c + lane;
-        W.at_lane(VA_R, kp, lp) = (i <= n) ? Yb[i] : 0.0;
-        kp += r32;
-        lp += q32;
-        if (kp >= M) {
-          kp -= M;
-          ++lp;
-        }
-      }
-    }
-    __syncwarp();
+    // ---- Ybar (staged into R with the inputs), masked by max(T,100) of the output
     for (int k = 0; k < M; ++k)
       if (!(W.at(YOUT, k) >= 100.0)) W.at(VA_R, k) = 0.0;
     double tminb = 0.0, tmaxb = 0.0;  // on the lanes that own rows 1 and n
@@ -2305,6 +2308,37 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
       W.at(VA_BQB, k) = cb;
     }
     __syncwarp();
+    // ---- ns, the neutral densities and the metrics again, staged by cp.async into rows
+    //      that are dead now (factorisation, R, X, q-, q+)
+    {
+      int lp = lp0, kp = kp0;
+      for (int c = 0; c < M; ++c) {
+        const int i = 1 + 32 * c + lane;
+        const bool in = i <= n;
+        const int ii = in ? i : 1;
+        const long long q = q0 + ii, mk = mm0 + ii;
+        cp_async8z(&W.at_lane(VA_SS, kp, lp), nsc + ii, in);
+        if (el) {
+          cp_async8z(&W.at_lane(VA_IB, kp, lp), P.nn + q, in);
+          cp_async8z(&W.at_lane(VA_TT, kp, lp), P.nn + nc + q, in);
+          cp_async8z(&W.at_lane(VA_R, kp, lp), P.nn + 2 * nc + q, in);
+        }
+        if (!UNIT) {
+          cp_async8z(&W.at_lane(VA_X, kp, lp), G.h2 + mk, in);
+          cp_async8z(&W.at_lane(VA_QM, kp, lp), G.h3 + mk, in);
+          cp_async8z(&W.at_lane(VA_QP, kp, lp), G.yh1 + mk, in);
+        }
+        kp += r32;
+        lp += q32;
+        if (kp >= M) {
+          kp -= M;
+          ++lp;
+        }
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncwarp();
+    }
     // ---- along x1: D(i) feeds Dh(i) (i >= 2) and Dh(i+1) (i < n), Dh(j) collects EM(j) and
     // EP(j-1); then through lambda(T, n) and C(n) to Tbar, nbar
     {
@@ -2320,11 +2354,15 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
           const double dh_i = (i >= 2) ? W.at_lane(VA_QMB, kp, lp) + W.at_lane(VA_QPB, km, lm) : 0.0;
           const double dh_ip1 = (i < n) ? W.at_lane(VA_QMB, kq, lq) + W.at_lane(VA_QPB, kp, lp) : 0.0;
           const double Db = 0.5 * (dh_i + dh_ip1);
-          const double T = W.at_lane(VA_T, kp, lp), nv = nsc[i];
-          const long long mk = mm0 + i;
-          const double g = UNIT ? 1.0 : __ldg(G.h2 + mk) * __ldg(G.h3 + mk) * __ldg(G.yh1 + mk);
+          const double T = W.at_lane(VA_T, kp, lp), nv = W.at_lane(VA_SS, kp, lp);
+          const double g =
+              UNIT ? 1.0 : W.at_lane(VA_X, kp, lp) * W.at_lane(VA_QM, kp, lp) * W.at_lane(VA_QP, kp, lp);
           double lam, dl_dT, dl_dn;
-          lam_deriv(P, s, T, nv, q0 + i, nc, lam, dl_dT, dl_dn);
+          if (el)
+            lam_deriv(s, T, nv, W.at_lane(VA_IB, kp, lp), W.at_lane(VA_TT, kp, lp), W.at_lane(VA_R, kp, lp), lam,
+                      dl_dT, dl_dn);
+          else
+            lam_deriv(s, T, nv, 0.0, 0.0, 0.0, lam, dl_dT, dl_dn);
           const double dcn = (nv > MINDENSDIV) ? -W.at_lane(VA_C, kp, lp) / nv : 0.0;
           Tbo[i] = W.at_lane(VA_TB, kp, lp) + Db * dl_dT * g;
           nbo[i] = W.at_lane(VA_BQB, kp, lp) * dcn + Db * dl_dn * g;
