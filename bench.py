@@ -52,15 +52,16 @@ def algorithmic_doubles_per_cell(unit_metrics: bool) -> dict:
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per interior cell and launch,
-# from one ncu --set full capture of each phase's kernel on the 384x48x32 dipole case
-# (profiles/kernels_ncu_full_dipole384x48x32.md); traffic scales with the cells processed,
-# so the full-size figure is this times the cell count.  Re-measure when a kernel changes.
+# from one ncu --set full capture of each phase's kernels on the 384x48x32 dipole case
+# (profiles/kernels_ncu_full_dipole384x48x32.md; the diffusion phase is k_diffusion_coef +
+# k_diffusion); traffic scales with the cells processed, so the full-size figure is this
+# times the cell count.  Re-measure when a kernel changes.
 NCU_TRAFFIC_BYTES_PER_CELL = {
-    "dt_calc": 142.37e6 / 589824,
-    "sweep_x3": 196.78e6 / 589824,
-    "sweep_x1": 163.58e6 / 589824,
-    "sweep_x2_epilogue": 215.91e6 / 589824,
-    "diffusion": 103.81e6 / 589824,
+    "dt_calc": (134.450176e6 + 5.546752e6) / 589824,
+    "sweep_x3": (135.896064e6 + 57.693696e6) / 589824,
+    "sweep_x1": (125.113856e6 + 48.169728e6) / 589824,
+    "sweep_x2_epilogue": (134.884864e6 + 77.871616e6) / 589824,
+    "diffusion": (86.669056e6 + 32.594944e6 + 138.413568e6 + 32.928000e6) / 589824,
 }
 
 
