@@ -612,11 +612,13 @@ __global__ void k_interface_vels(GridDev G, Blocks B, double* vs1i, double* vs2i
 //    and per-cell/per-face metric tables), so every update is bit-identical to the
 //    reference's a/b chain.  Two kernels:
 //      k_sweep_march<DIM=2|3>: one thread per (x2 or x3 line, species), a warp covering 32
-//        adjacent x1 -- every load is a coalesced 256-byte row; the thread marches along its
-//        line with the running state of its fields in registers, prefetching the values of
-//        step j+2 while computing step j, and writes cell j-1 in place.
+//        adjacent x1 -- every copy is a coalesced 256-byte row; the thread marches along its
+//        line with the running state of its fields in registers, its warp staging the
+//        values of step j+4 by cp.async into a shared ring while computing step j, and
+//        writes cell j-1 in place.
 //      k_sweep_x1: one warp per (x1 column, species), lanes along the contiguous x1, the
-//        column processed in chunks of 32 cells with neighbours exchanged by shuffles.
+//        column processed in chunks of 32 cells with neighbours exchanged by shuffles, the
+//        next chunk staged by cp.async into a shared ring while the current one computes.
 //    Standalone (FUSED=false): one field set (which: 0 ns, 1 rhovs1 (frank 1), 2 rhoes),
 //    interface velocities from the work arrays, ghosts from memory.
 //    Fused x3: v12rhov1/T2rhoe folded in, x3 ghosts and vs3i formed on the fly.
