@@ -4,7 +4,9 @@
 // the MC-limited advection sweeps, the global-boundary ghost fill, the interface
 // velocities, the state conversions, clean_param, thermal conductivity, the
 // TRBDF2 / backward-Euler field-aligned diffusion (with LAPACK's partial-pivoting
-// band LU restated from its published algorithm) and the CFL time step.
+// band LU restated from its published algorithm) and the CFL time step; and, ahead of
+// its device version, the compression sub-step (artificial viscosity, the RK2
+// zero-order-hold ghosts, div3D_curv_23 and the two-stage energy update).
 //
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 // library, as the checker.  The product (gemini_b200/) never links or calls it.
@@ -1068,6 +1070,176 @@ int ora_fluid_adv(const ora_grid* G, double* fluidvars, double* fluidauxvars, co
   ora_rhov12v1(G, ns, rhovs1, vs1);
   ora_clean_param(G, 1, ns);
   ora_clean_param(G, 2, vs1);
+  ora_rhoe2T(G, ns, rhoes, Ts);
+  ora_clean_param(G, 3, Ts);
+  const int rc = ora_energy_diffusion(G, ns, Ts, J1, nn, Tn, dt, diffsolvetype, Teinf);
+  if (rc != 0) return rc;
+  ora_clean_param(G, 3, Ts);
+  ora_T2rhoe(G, ns, Ts, rhoes);
+  return 0;
+}
+
+// ---- the compression sub-step (app/main.f90:320-338) ------------------------------
+
+// multifluid.f90:237-268 VNRicht_artvisc with xicon = 3 (multifluid.f90:43).  Q: interior
+// (1:lx1,1:lx2,1:lx3,lsp), column-major.  Reads vs1 at x1 indices 0..lx1+1, ghosts as they
+// stand after the advection (the reference notes this at multifluid.f90:255-256).
+void ora_vnricht_artvisc(const ora_grid* G, const double* ns, const double* vs1, double* Q) {
+  Ix X(G);
+  const double xicon = 3.0;
+  const double xicon2 = xicon * xicon;  // xicon**2
+  const long long nc = X.nc();
+  std::vector<double> v1i(G->lx1 + 1);
+  for (int s = 0; s < LSP - 1; ++s) {
+    const double* n = ns + s * X.ng;
+    const double* v = vs1 + s * X.ng;
+    for (int i3 = 1; i3 <= G->lx3; ++i3)
+      for (int i2 = 1; i2 <= G->lx2; ++i2) {
+        // v1iupdate(1:lx1+1) = 0.5*(vs1(0:lx1) + vs1(1:lx1+1))
+        for (int i = 1; i <= G->lx1 + 1; ++i) v1i[i - 1] = 0.5 * (v[X.g(i - 1, i2, i3)] + v[X.g(i, i2, i3)]);
+        for (int i1 = 1; i1 <= G->lx1; ++i1) {
+          const double dv = v1i[i1] - v1i[i1 - 1];  // dv1iupdate
+          const double m = fmin_f(dv, 0.0);
+          Q[s * nc + X.c(i1, i2, i3)] = n[X.g(i1, i2, i3)] * K.ms[s] * 0.25 * xicon2 * (m * m);
+        }
+      }
+  }
+  for (long long q = 0; q < nc; ++q) Q[(LSP - 1) * nc + q] = 0.0;
+}
+
+// sources_mpi.f90:68-111 RK2_global_boundary(_allspec) on a single rank (every global
+// boundary is local): zero-order hold of vs1 along x1, then of vs1, vs2, vs3 along x2 and,
+// unless x3 is periodic, along x3 -- each over the full extent of the other indices.
+void ora_rk2_global_boundary_allspec(const ora_grid* G, double* vs1, double* vs2, double* vs3) {
+  Ix X(G);
+  const int lx1 = G->lx1, lx2 = G->lx2, lx3 = G->lx3;
+  for (int s = 0; s < LSP; ++s) {
+    double* v[3] = {vs1 + s * X.ng, vs2 + s * X.ng, vs3 + s * X.ng};
+    for (int i3 = -1; i3 <= lx3 + 2; ++i3)
+      for (int i2 = -1; i2 <= lx2 + 2; ++i2) {
+        v[0][X.g(0, i2, i3)] = v[0][X.g(1, i2, i3)];
+        v[0][X.g(lx1 + 1, i2, i3)] = v[0][X.g(lx1, i2, i3)];
+      }
+    for (int c = 0; c < 3; ++c)
+      for (int i3 = -1; i3 <= lx3 + 2; ++i3)
+        for (int i1 = -1; i1 <= lx1 + 2; ++i1) v[c][X.g(i1, 0, i3)] = v[c][X.g(i1, 1, i3)];
+    for (int c = 0; c < 3; ++c)
+      for (int i3 = -1; i3 <= lx3 + 2; ++i3)
+        for (int i1 = -1; i1 <= lx1 + 2; ++i1) v[c][X.g(i1, lx2 + 1, i3)] = v[c][X.g(i1, lx2, i3)];
+    if (!G->flagper) {
+      for (int c = 0; c < 3; ++c)
+        for (int i2 = -1; i2 <= lx2 + 2; ++i2)
+          for (int i1 = -1; i1 <= lx1 + 2; ++i1) v[c][X.g(i1, i2, 0)] = v[c][X.g(i1, i2, 1)];
+      for (int c = 0; c < 3; ++c)
+        for (int i2 = -1; i2 <= lx2 + 2; ++i2)
+          for (int i1 = -1; i1 <= lx1 + 2; ++i1) v[c][X.g(i1, i2, lx3 + 1)] = v[c][X.g(i1, i2, lx3)];
+    }
+  }
+}
+
+// calculus/div.f90:110-200 div3D_curv_23 as compression calls it (multifluid.f90:289-291):
+// the slab of grid indices 0..lx+1 in each direction.  f1, f2, f3: one species, ghosted;
+// div: (lx1+2, lx2+2, lx3+2), column-major, slab index j <-> grid index j-1.  One-sided
+// differences on the slab's faces, centred ones inside; dx arrays are backward differences.
+void ora_div3D(const ora_grid* G, const double* f1, const double* f2, const double* f3, double* div) {
+  Ix X(G);
+  const int L1 = G->lx1 + 2, L2 = G->lx2 + 2, L3 = G->lx3 + 2;
+  auto D = [&](int j1, int j2, int j3) -> double& {
+    return div[(j1 - 1) + (long long)L1 * ((j2 - 1) + (long long)L2 * (j3 - 1))];
+  };
+  auto at = [&](const double* a, int j1, int j2, int j3) { return a[X.g(j1 - 1, j2 - 1, j3 - 1)]; };
+  auto dx1 = [&](int j) { return G->dx1[j - 1]; };  // x%dx1(0:lx1+1) re-based at 1
+  auto dx2 = [&](int j) { return G->dx2[j - 1]; };
+  auto dx3 = [&](int j) { return G->dx3[j - 1]; };
+  const double *h1 = G->h1, *h2 = G->h2, *h3 = G->h3;
+  for (int j3 = 1; j3 <= L3; ++j3)
+    for (int j2 = 1; j2 <= L2; ++j2) {
+      auto t = [&](int j) { return at(h2, j, j2, j3) * at(h3, j, j2, j3) * at(f1, j, j2, j3); };
+      D(1, j2, j3) = (t(2) - t(1)) / dx1(2);
+      for (int j = 2; j <= L1 - 1; ++j) D(j, j2, j3) = (t(j + 1) - t(j - 1)) / (dx1(j + 1) + dx1(j));
+      D(L1, j2, j3) = (t(L1) - t(L1 - 1)) / dx1(L1);
+    }
+  if (G->lx2 > 1)
+    for (int j3 = 1; j3 <= L3; ++j3)
+      for (int j1 = 1; j1 <= L1; ++j1) {
+        auto t = [&](int j) { return at(h1, j1, j, j3) * at(h3, j1, j, j3) * at(f2, j1, j, j3); };
+        D(j1, 1, j3) = D(j1, 1, j3) + (t(2) - t(1)) / dx2(2);
+        for (int j = 2; j <= L2 - 1; ++j) D(j1, j, j3) = D(j1, j, j3) + (t(j + 1) - t(j - 1)) / (dx2(j + 1) + dx2(j));
+        D(j1, L2, j3) = D(j1, L2, j3) + (t(L2) - t(L2 - 1)) / dx2(L2);
+      }
+  if (G->lx3 > 1)
+    for (int j2 = 1; j2 <= L2; ++j2)
+      for (int j1 = 1; j1 <= L1; ++j1) {
+        auto t = [&](int j) { return at(h1, j1, j2, j) * at(h2, j1, j2, j) * at(f3, j1, j2, j); };
+        D(j1, j2, 1) = D(j1, j2, 1) + (t(2) - t(1)) / dx3(2);
+        for (int j = 2; j <= L3 - 1; ++j) D(j1, j2, j) = D(j1, j2, j) + (t(j + 1) - t(j - 1)) / (dx3(j + 1) + dx3(j));
+        D(j1, j2, L3) = D(j1, j2, L3) + (t(L3) - t(L3 - 1)) / dx3(L3);
+      }
+  for (int j3 = 1; j3 <= L3; ++j3)
+    for (int j2 = 1; j2 <= L2; ++j2)
+      for (int j1 = 1; j1 <= L1; ++j1)
+        D(j1, j2, j3) = D(j1, j2, j3) / (at(h1, j1, j2, j3) * at(h2, j1, j2, j3) * at(h3, j1, j2, j3));
+}
+
+// multifluid.f90:274-302 compression: the half-step and full-step energy updates with
+// the slab divergence of each species' velocity.  Q: interior (lsp species); rhoes ghosted.
+void ora_compression(const ora_grid* G, double dt, const double* vs1, const double* vs2, const double* vs3,
+                     const double* Q, double* rhoes) {
+  Ix X(G);
+  const long long nc = X.nc();
+  const int L1 = G->lx1 + 2, L2 = G->lx2 + 2;
+  std::vector<double> div((size_t)(G->lx1 + 2) * (G->lx2 + 2) * (G->lx3 + 2));
+  for (int s = 0; s < LSP; ++s) {
+    ora_div3D(G, vs1 + s * X.ng, vs2 + s * X.ng, vs3 + s * X.ng, div.data());
+    double* re = rhoes + s * X.ng;
+    for (int i3 = 1; i3 <= G->lx3; ++i3)
+      for (int i2 = 1; i2 <= G->lx2; ++i2)
+        for (int i1 = 1; i1 <= G->lx1; ++i1) {
+          const double dv = div[i1 + (long long)L1 * (i2 + (long long)L2 * i3)];  // slab (i+1)
+          const double q = Q[s * nc + X.c(i1, i2, i3)];
+          const double p = re[X.g(i1, i2, i3)];
+          const double half = p - dt / 2 * (p * (K.gammas[s] - 1) + q) * dv;
+          re[X.g(i1, i2, i3)] = p - dt * (half * (K.gammas[s] - 1) + q) * dv;
+        }
+  }
+}
+
+// app/main.f90:280-355 with the compression sub-step (main.f90:320-338) between the
+// post-advection clean_param(2) and rhoe2T; otherwise ora_fluid_adv.
+int ora_fluid_adv_compression(const ora_grid* G, double* fluidvars, double* fluidauxvars, const double* J1,
+                              double* vs1i, double* vs2i, double* vs3i, const double* nn, const double* Tn,
+                              double dt, double Teinf, int diffsolvetype) {
+  Ix X(G);
+  double* ns = fluidvars;
+  double* vs1 = fluidvars + LSP * X.ng;
+  double* vs2 = fluidvars + 2 * LSP * X.ng;
+  double* vs3 = fluidvars + 3 * LSP * X.ng;
+  double* Ts = fluidvars + 4 * LSP * X.ng;
+  double* rhovs1 = fluidauxvars;
+  double* rhoes = fluidauxvars + LSP * X.ng;
+  ora_v12rhov1(G, ns, vs1, rhovs1);
+  ora_T2rhoe(G, ns, Ts, rhoes);
+  ora_set_global_boundaries_allspec(G, ns, rhovs1, vs1, vs2, vs3, rhoes, vs1i, LSP);
+  ora_halo_fluidvars(G, ns, rhovs1, rhoes, vs2, vs3);
+  ora_interface_vels_allspec(G, vs1, vs2, vs3, vs1i, vs2i, vs3i, LSP);
+  ora_sweep_allspec(G, 3, ns, vs3i, dt, 0, 6);
+  ora_sweep_allspec(G, 3, rhovs1, vs3i, dt, 1, 6);
+  ora_sweep_allspec(G, 3, rhoes, vs3i, dt, 0, 7);
+  ora_sweep_allspec(G, 1, ns, vs1i, dt, 0, 6);
+  ora_sweep_allspec(G, 1, rhovs1, vs1i, dt, 0, 6);
+  ora_sweep_allspec(G, 1, rhoes, vs1i, dt, 0, 7);
+  ora_halo_allparams(G, ns, rhovs1, rhoes);
+  ora_sweep_allspec(G, 2, ns, vs2i, dt, 0, 6);
+  ora_sweep_allspec(G, 2, rhovs1, vs2i, dt, 1, 6);
+  ora_sweep_allspec(G, 2, rhoes, vs2i, dt, 0, 7);
+  ora_rhov12v1(G, ns, rhovs1, vs1);
+  ora_clean_param(G, 1, ns);
+  ora_clean_param(G, 2, vs1);
+  std::vector<double> Q((size_t)LSP * X.nc());
+  ora_vnricht_artvisc(G, ns, vs1, Q.data());
+  ora_halo_fluidvars(G, ns, rhovs1, rhoes, vs2, vs3);
+  ora_rk2_global_boundary_allspec(G, vs1, vs2, vs3);
+  ora_compression(G, dt, vs1, vs2, vs3, Q.data(), rhoes);
   ora_rhoe2T(G, ns, rhoes, Ts);
   ora_clean_param(G, 3, Ts);
   const int rc = ora_energy_diffusion(G, ns, Ts, J1, nn, Tn, dt, diffsolvetype, Teinf);

@@ -76,6 +76,12 @@ def lib():
         L.ora_fluid_adv.argtypes = [G, _D, _D, _D, _D, _D, _D, _D, _D, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_int]
         L.ora_fluid_adv.restype = ctypes.c_int
+        L.ora_fluid_adv_compression.argtypes = L.ora_fluid_adv.argtypes
+        L.ora_fluid_adv_compression.restype = ctypes.c_int
+        L.ora_vnricht_artvisc.argtypes = [G, _D, _D, _D]
+        L.ora_rk2_global_boundary_allspec.argtypes = [G, _D, _D, _D]
+        L.ora_div3D.argtypes = [G, _D, _D, _D, _D]
+        L.ora_compression.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
         L.ora_constants.argtypes = [_D, _D, _D, _D]
         L.ora_num_threads.restype = ctypes.c_int
         L.ora_set_diffusion_solver.argtypes = [ctypes.c_int]
@@ -292,6 +298,49 @@ def fluid_adv(grid, st, dt: float, diffsolvetype: int = 2):
                              float(st.Teinf), int(diffsolvetype))
     if rc != 0:
         raise ValueError(f"ora_fluid_adv failed: {rc}")
+
+
+def fluid_adv_compression(grid, st, dt: float, diffsolvetype: int = 2):
+    """fluid_adv with the compression sub-step (app/main.f90:320-338) between the
+    post-advection clean_param(2) and rhoe2T, in place."""
+    g = _GridHandle(grid)
+    J1 = np.asfortranarray(st.electrovars[..., 3])
+    rc = lib().ora_fluid_adv_compression(g.ref, _p(st.fluidvars), _p(st.fluidauxvars), _p(J1), _p(st.vs1i),
+                                         _p(st.vs2i), _p(st.vs3i), _p(st.nn), _p(st.Tn), float(dt),
+                                         float(st.Teinf), int(diffsolvetype))
+    if rc != 0:
+        raise ValueError(f"ora_fluid_adv_compression failed: {rc}")
+
+
+def vnricht_artvisc(grid, st):
+    """Artificial viscosity Q (multifluid.f90:237-268): interior (lx1, lx2, lx3, lsp)."""
+    g = _GridHandle(grid); b = _blocks(st)
+    Q = np.zeros((grid.lx1, grid.lx2, grid.lx3, LSP), order="F")
+    lib().ora_vnricht_artvisc(g.ref, b["ns"], b["vs1"], _p(Q))
+    return Q
+
+
+def rk2_global_boundary(grid, st):
+    """Zero-order-hold velocity ghosts for the compression sub-step (sources_mpi.f90:68-111)."""
+    g = _GridHandle(grid); b = _blocks(st)
+    lib().ora_rk2_global_boundary_allspec(g.ref, b["vs1"], b["vs2"], b["vs3"])
+
+
+def div3D(grid, f1, f2, f3):
+    """div3D_curv_23 over the slab of grid indices 0..lx+1 (calculus/div.f90:110-200).
+    f1, f2, f3: one species, ghosted (lx1+4, lx2+4, lx3+4); returns (lx1+2, lx2+2, lx3+2)."""
+    g = _GridHandle(grid)
+    fs = [np.asfortranarray(f, dtype=np.float64) for f in (f1, f2, f3)]
+    out = np.zeros((grid.lx1 + 2, grid.lx2 + 2, grid.lx3 + 2), order="F")
+    lib().ora_div3D(g.ref, _p(fs[0]), _p(fs[1]), _p(fs[2]), _p(out))
+    return out
+
+
+def compression(grid, st, dt: float, Q):
+    """The compression energy update (multifluid.f90:274-302) of st's rhoes, in place."""
+    g = _GridHandle(grid); b = _blocks(st)
+    Qf = np.asfortranarray(Q, dtype=np.float64)
+    lib().ora_compression(g.ref, float(dt), b["vs1"], b["vs2"], b["vs3"], _p(Qf), b["rhoes"])
 
 
 def run_steps(grid, st, nsteps: int, tcfl: float = 0.5, diffsolvetype: int = 2):
