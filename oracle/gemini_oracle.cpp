@@ -6,7 +6,8 @@
 // TRBDF2 / backward-Euler field-aligned diffusion (with LAPACK's partial-pivoting
 // band LU restated from its published algorithm) and the CFL time step; and, ahead of
 // its device version, the compression sub-step (artificial viscosity, the RK2
-// zero-order-hold ghosts, div3D_curv_23 and the two-stage energy update).
+// zero-order-hold ghosts, div3D_curv_23 and the two-stage energy update) and the
+// source/loss ETD solves for given production/loss rates.
 //
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 // library, as the checker.  The product (gemini_b200/) never links or calls it.
@@ -1247,6 +1248,96 @@ int ora_fluid_adv_compression(const ora_grid* G, double* fluidvars, double* flui
   ora_clean_param(G, 3, Ts);
   ora_T2rhoe(G, ns, Ts, rhoes);
   return 0;
+}
+
+// ---- the source/loss sub-step's solves, with given production/loss rates ----------
+// (the rates themselves come from sources.f90, not restated here)
+
+// calculus.in.f90:174-196 ETD_uncoupled on interior arrays of n values.
+void ora_etd_uncoupled(long long n, const double* f, const double* P, const double* L, double dt, double* out) {
+  for (long long q = 0; q < n; ++q) {
+    const double Ldt = L[q] * dt;
+    const double expL = std::exp(-1.0 * Ldt);
+    out[q] = (Ldt > 1e-10) ? f[q] * expL + P[q] / L[q] * (1 - expL) : f[q] + P[q] * dt;
+  }
+}
+
+// multifluid.f90:532-549 mass_source_loss_solve.  Pr, Lo, Prprecip: interior
+// (lx1,lx2,lx3,lsp) / (.,lsp-1); Pr is updated in place as the reference does; ns ghosted.
+void ora_mass_source_loss_solve(const ora_grid* G, double dt, double* Pr, const double* Lo, const double* Prprecip,
+                                double* ns) {
+  Ix X(G);
+  const long long nc = X.nc();
+  for (int s = 0; s < LSP - 1; ++s)
+    for (long long q = 0; q < nc; ++q) Pr[s * nc + q] = Pr[s * nc + q] + Prprecip[s * nc + q];
+  std::vector<double> f(nc), o(nc);
+  for (int s = 0; s < LSP - 1; ++s) {
+    double* n = ns + s * X.ng;
+    for (int i3 = 1; i3 <= G->lx3; ++i3)
+      for (int i2 = 1; i2 <= G->lx2; ++i2)
+        for (int i1 = 1; i1 <= G->lx1; ++i1) f[X.c(i1, i2, i3)] = n[X.g(i1, i2, i3)];
+    ora_etd_uncoupled(nc, f.data(), Pr + s * nc, Lo + s * nc, dt, o.data());
+    for (int i3 = 1; i3 <= G->lx3; ++i3)
+      for (int i2 = 1; i2 <= G->lx2; ++i2)
+        for (int i1 = 1; i1 <= G->lx1; ++i1) n[X.g(i1, i2, i3)] = o[X.c(i1, i2, i3)];
+  }
+  // ns(:,:,:,lsp) = sum(ns(:,:,:,1:lsp-1),4), ghosts included
+  for (long long k = 0; k < X.ng; ++k) {
+    double sum = 0.0;
+    for (int s = 0; s < LSP - 1; ++s) sum = sum + ns[s * X.ng + k];
+    ns[(LSP - 1) * X.ng + k] = sum;
+  }
+}
+
+// multifluid.f90:500-528 momentum_source_loss_solve (J1 not used, as in the reference).
+void ora_momentum_source_loss_solve(const ora_grid* G, double dt, const double* Pr, const double* Lo,
+                                    const double* ns, double* rhovs1, double* vs1) {
+  Ix X(G);
+  const long long nc = X.nc();
+  std::vector<double> f(nc), o(nc);
+  for (int s = 0; s < LSP - 1; ++s) {
+    double* r = rhovs1 + s * X.ng;
+    for (int i3 = 1; i3 <= G->lx3; ++i3)
+      for (int i2 = 1; i2 <= G->lx2; ++i2)
+        for (int i1 = 1; i1 <= G->lx1; ++i1) f[X.c(i1, i2, i3)] = r[X.g(i1, i2, i3)];
+    ora_etd_uncoupled(nc, f.data(), Pr + s * nc, Lo + s * nc, dt, o.data());
+    for (int i3 = 1; i3 <= G->lx3; ++i3)
+      for (int i2 = 1; i2 <= G->lx2; ++i2)
+        for (int i1 = 1; i1 <= G->lx1; ++i1) r[X.g(i1, i2, i3)] = o[X.c(i1, i2, i3)];
+    for (long long k = 0; k < X.ng; ++k)
+      vs1[s * X.ng + k] = r[k] / (K.ms[s] * fmax_f(ns[s * X.ng + k], mindensdiv));
+  }
+  for (long long k = 0; k < X.ng; ++k) {
+    double chrgflux = 0.0;
+    for (int s = 0; s < LSP - 1; ++s) chrgflux = chrgflux + ns[s * X.ng + k] * K.qs[s] * vs1[s * X.ng + k];
+    const long long ke = (LSP - 1) * X.ng + k;
+    vs1[ke] = -1 / fmax_f(ns[ke], mindensdiv) / K.qs[LSP - 1] * chrgflux;
+    rhovs1[ke] = ns[ke] * K.ms[LSP - 1] * vs1[ke];
+  }
+}
+
+// multifluid.f90:474-495 energy_source_loss_solve.  Qeprecip: interior (lx1,lx2,lx3).
+void ora_energy_source_loss_solve(const ora_grid* G, double dt, double* Pr, const double* Lo,
+                                  const double* Qeprecip, double* rhoes, double* Ts, const double* ns) {
+  Ix X(G);
+  const long long nc = X.nc();
+  std::vector<double> f(nc), o(nc);
+  for (int s = 0; s < LSP; ++s) {
+    if (s == LSP - 1)
+      for (long long q = 0; q < nc; ++q) Pr[s * nc + q] = Pr[s * nc + q] + Qeprecip[q];
+    double* re = rhoes + s * X.ng;
+    for (int i3 = 1; i3 <= G->lx3; ++i3)
+      for (int i2 = 1; i2 <= G->lx2; ++i2)
+        for (int i1 = 1; i1 <= G->lx1; ++i1) f[X.c(i1, i2, i3)] = re[X.g(i1, i2, i3)];
+    ora_etd_uncoupled(nc, f.data(), Pr + s * nc, Lo + s * nc, dt, o.data());
+    for (int i3 = 1; i3 <= G->lx3; ++i3)
+      for (int i2 = 1; i2 <= G->lx2; ++i2)
+        for (int i1 = 1; i1 <= G->lx1; ++i1) re[X.g(i1, i2, i3)] = o[X.c(i1, i2, i3)];
+    for (long long k = 0; k < X.ng; ++k) {
+      const double T = (K.gammas[s] - 1) / kB * re[k] / fmax_f(ns[s * X.ng + k], mindensdiv);
+      Ts[s * X.ng + k] = fmax_f(T, 100.0);
+    }
+  }
 }
 
 void ora_set_diffusion_solver(int mode) { g_diff_solver = mode; }

@@ -82,6 +82,10 @@ def lib():
         L.ora_rk2_global_boundary_allspec.argtypes = [G, _D, _D, _D]
         L.ora_div3D.argtypes = [G, _D, _D, _D, _D]
         L.ora_compression.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
+        L.ora_etd_uncoupled.argtypes = [ctypes.c_longlong, _D, _D, _D, ctypes.c_double, _D]
+        L.ora_mass_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D]
+        L.ora_momentum_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
+        L.ora_energy_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D, _D]
         L.ora_constants.argtypes = [_D, _D, _D, _D]
         L.ora_num_threads.restype = ctypes.c_int
         L.ora_set_diffusion_solver.argtypes = [ctypes.c_int]
@@ -341,6 +345,40 @@ def compression(grid, st, dt: float, Q):
     g = _GridHandle(grid); b = _blocks(st)
     Qf = np.asfortranarray(Q, dtype=np.float64)
     lib().ora_compression(g.ref, float(dt), b["vs1"], b["vs2"], b["vs3"], _p(Qf), b["rhoes"])
+
+
+def etd_uncoupled(f, P, L, dt: float):
+    """ETD_uncoupled (calculus.in.f90:174-196) on same-shaped arrays."""
+    f, P, L = (np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (f, P, L))
+    out = np.empty_like(f)
+    lib().ora_etd_uncoupled(f.size, _p(f), _p(P), _p(L), float(dt), _p(out))
+    return out
+
+
+def mass_source_loss_solve(grid, st, dt: float, Pr, Lo, Prprecip):
+    """multifluid.f90:532-549 with given rates (interior, (lx1, lx2, lx3, species)); returns Pr
+    as updated by the routine."""
+    g = _GridHandle(grid); b = _blocks(st)
+    Pr = np.asfortranarray(Pr, dtype=np.float64).copy(order="F")
+    Lo, Pp = (np.asfortranarray(a, dtype=np.float64) for a in (Lo, Prprecip))
+    lib().ora_mass_source_loss_solve(g.ref, float(dt), _p(Pr), _p(Lo), _p(Pp), b["ns"])
+    return Pr
+
+
+def momentum_source_loss_solve(grid, st, dt: float, Pr, Lo):
+    """multifluid.f90:500-528 with given rates (interior, (lx1, lx2, lx3, species))."""
+    g = _GridHandle(grid); b = _blocks(st)
+    Pr, Lo = (np.asfortranarray(a, dtype=np.float64) for a in (Pr, Lo))
+    lib().ora_momentum_source_loss_solve(g.ref, float(dt), _p(Pr), _p(Lo), b["ns"], b["rhovs1"], b["vs1"])
+
+
+def energy_source_loss_solve(grid, st, dt: float, Pr, Lo, Qeprecip):
+    """multifluid.f90:474-495 with given rates; returns Pr as updated by the routine."""
+    g = _GridHandle(grid); b = _blocks(st)
+    Pr = np.asfortranarray(Pr, dtype=np.float64).copy(order="F")
+    Lo, Qe = (np.asfortranarray(a, dtype=np.float64) for a in (Lo, Qeprecip))
+    lib().ora_energy_source_loss_solve(g.ref, float(dt), _p(Pr), _p(Lo), _p(Qe), b["rhoes"], b["Ts"], b["ns"])
+    return Pr
 
 
 def run_steps(grid, st, nsteps: int, tcfl: float = 0.5, diffsolvetype: int = 2):
