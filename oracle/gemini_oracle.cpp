@@ -7,7 +7,7 @@
 // band LU restated from its published algorithm) and the CFL time step; and, ahead of
 // its device version, the compression sub-step (artificial viscosity, the RK2
 // zero-order-hold ghosts, div3D_curv_23 and the two-stage energy update) and the
-// source/loss ETD solves for given production/loss rates.
+// source/loss ETD solves, with the continuity equations' production/loss rates.
 //
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 // library, as the checker.  The product (gemini_b200/) never links or calls it.
@@ -1252,6 +1252,151 @@ int ora_fluid_adv_compression(const ora_grid* G, double* fluidvars, double* flui
 
 // ---- the source/loss sub-step's solves, with given production/loss rates ----------
 // (the rates themselves come from sources.f90, not restated here)
+
+// sources.f90:18-276 srcsContinuity: production and loss rates of the continuity
+// equations.  nn: interior (lx1,lx2,lx3,>=6) neutral densities (O, N2, O2, H, N, NO); vn1..3,
+// Tn: interior; ns, vs1, vs2, vs3, Ts: ghosted; Pr, Lo: interior (lx1,lx2,lx3,lsp), zeroed
+// first.  Integer powers as gfortran expands them (x**2 = x*x, x**3 = (x*x)*x, x**4 =
+// (x*x)*(x*x)), real powers through pow; each rate expression in the reference's order.
+void ora_srcs_continuity(const ora_grid* G, const double* nn, const double* vn1, const double* vn2,
+                         const double* vn3, const double* Tn, const double* ns, const double* vs1,
+                         const double* vs2, const double* vs3, const double* Ts, double* Pr, double* Lo) {
+  Ix X(G);
+  const long long nc = X.nc();
+  auto p2 = [](double x) { return x * x; };
+  auto p3 = [](double x) { return x * x * x; };
+  auto p4 = [](double x) { const double t = x * x; return t * t; };
+  for (long long q = 0; q < LSP * nc; ++q) Pr[q] = Lo[q] = 0.0;
+  double kreac = 0.0;  // where-masked: keeps its last value where no branch applies
+  for (int i3 = 1; i3 <= G->lx3; ++i3)
+    for (int i2 = 1; i2 <= G->lx2; ++i2)
+      for (int i1 = 1; i1 <= G->lx1; ++i1) {
+        const long long c = X.c(i1, i2, i3), k = X.g(i1, i2, i3);
+        auto N = [&](int j) { return nn[(j - 1) * nc + c]; };           // nn(:,:,:,j)
+        auto NS = [&](int sp) { return ns[(sp - 1) * X.ng + k]; };      // ns(1:lx1,..,sp)
+        auto TS = [&](int sp) { return Ts[(sp - 1) * X.ng + k]; };
+        auto PR = [&](int sp) -> double& { return Pr[(sp - 1) * nc + c]; };
+        auto LO = [&](int sp) -> double& { return Lo[(sp - 1) * nc + c]; };
+        const double tn = Tn[c];
+        const double Te = TS(LSP);
+        const double dv2 = p2(vs1[k] - vn1[c]) + p2(vs2[k] - vn2[c]) + p2(vs3[k] - vn3[c]);  // species 1
+        double Teff, betanow;
+        // O+ + N2 --> NO+ + N
+        Teff = 28 / (16 + 28.0) * (16 * amu / 3 / kB * (dv2) + TS(1) - tn) + tn;
+        if (Teff <= 3725)
+          kreac = 1.71676e-12 - 7.19934e-13 * (Teff / 300) + 1.33276e-13 * p2(Teff / 300) -
+                  9.28213e-15 * p3(Teff / 300) + 6.39557e-16 * p4(Teff / 300);
+        if (Teff > 3725 && Teff <= 30000)
+          kreac = -1.52489e-11 + 7.67112e-13 * (Teff / 300) + 1.19064e-13 * p2(Teff / 300) -
+                  1.30858e-15 * p3(Teff / 300) + 4.67756e-18 * p4(Teff / 300);
+        if (Teff > 30000)
+          kreac = -1.52489e-11 + 7.67112e-13 * (100) + 1.19064e-13 * (10000) - 1.30858e-15 * (1000000) +
+                  4.67756e-18 * (100000000);
+        betanow = kreac * N(2) * 1e-6;
+        PR(2) = PR(2) + betanow * NS(1);
+        LO(1) = LO(1) + betanow;
+        // O+ + O2 --> O2+ + O
+        Teff = 32 / (16 + 32.0) * (16 * amu / 3 / kB * (dv2) + TS(1) - tn) + tn;
+        if (Teff <= 4800)
+          kreac = 2.78932e-11 - 6.92612e-12 * (Teff / 300) + 8.67684e-13 * p2(Teff / 300) -
+                  3.47251e-14 * p3(Teff / 300) + 5.07097e-16 * p4(Teff / 300);
+        if (Teff > 4800 && Teff <= 30000)
+          kreac = -1.74046e-11 + 3.02328e-12 * Teff / 300 - 2.39214e-15 * p2(Teff / 300) -
+                  4.02394e-17 * p3(Teff / 300);
+        if (Teff > 30000) kreac = -1.74046e-11 + 3.02328e-12 * 100 - 2.39214e-15 * 10000 - 4.02394e-17 * 1000000;
+        betanow = kreac * N(3) * 1e-6;
+        PR(4) = PR(4) + betanow * NS(1);
+        LO(1) = LO(1) + betanow;
+        // O+ + NO --> NO+ + O
+        Teff = 30 / (16 + 30.0) * (16 * amu / 3 / kB * (dv2) + TS(1) - tn) + tn;
+        if (Teff <= 3800)
+          kreac = 6.40408e-13 - 1.33888e-13 * (Teff / 300) + 7.65103e-14 * p2(Teff / 300) -
+                  3.11509e-15 * p3(Teff / 300) + 6.62374e-17 * p4(Teff / 300);
+        if (Teff > 3800 && Teff <= 30000)
+          kreac = -7.48312e-13 + 2.31502e-13 * (Teff / 300) + 3.07160e-14 * p2(Teff / 300) -
+                  2.65436e-16 * p3(Teff / 300) + 7.76665e-19 * p4(Teff / 300);
+        if (Teff > 30000)
+          kreac = -7.48312e-13 + 2.31502e-13 * (100) + 3.07160e-14 * (10000) - 2.65436e-16 * (1000000) +
+                  7.76665e-19 * (100000000);
+        betanow = kreac * N(6) * 1e-6;
+        PR(2) = PR(2) + betanow * NS(1);
+        LO(1) = LO(1) + betanow;
+        // O+ + e --> O + hv
+        betanow = 3.7e-12 * std::pow(250 / TS(LSP), 0.7) * NS(LSP) * 1e-6;
+        LO(1) = LO(1) + betanow;
+        // N2+ + O --> O+ + N2
+        Teff = 16 / (28 + 16.0) * (28 * amu / 3 / kB * (dv2) + TS(3) - tn) + tn;
+        kreac = (Teff <= 1500) ? 1e-11 * std::pow(300 / Teff, 0.23) : 3.6e-12 * std::pow(300 / Teff, -0.41);
+        betanow = kreac * N(1) * 1e-6;
+        PR(1) = PR(1) + betanow * NS(3);
+        LO(3) = LO(3) + betanow;
+        // N+ + O --> O+ + N
+        betanow = 5e-13 * N(1) * 1e-6;
+        PR(1) = PR(1) + betanow * NS(5);
+        LO(5) = LO(5) + betanow;
+        // H+ + O --> O+ + H
+        Teff = TS(6);
+        betanow = (6.e-10) * (8 / 9.0) * (std::pow((Teff + tn / 4) / (tn + Teff / 16), 0.5)) * N(1) * 1e-6;
+        PR(1) = PR(1) + betanow * NS(6);
+        LO(6) = LO(6) + betanow;
+        // O+ + H --> H+ + O
+        betanow = 6.0e-10 * N(4) * 1e-6;
+        PR(6) = PR(6) + betanow * NS(1);
+        LO(1) = LO(1) + betanow;
+        // O2+ + N2 --> NO+ + NO
+        betanow = 5e-16 * N(3) * 1e-6;
+        PR(2) = PR(2) + betanow * NS(4);
+        LO(4) = LO(4) + betanow;
+        // O2+ + N --> NO+ + O
+        betanow = 1.2e-10 * N(5) * 1e-6;
+        PR(2) = PR(2) + betanow * NS(4);
+        LO(4) = LO(4) + betanow;
+        // O2+ + NO --> NO+ + O2
+        betanow = 4.6e-10 * N(6) * 1e-6;
+        PR(2) = PR(2) + betanow * NS(4);
+        LO(4) = LO(4) + betanow;
+        // N2+ + O --> NO+ + N
+        Teff = 16 / (28 + 16.0) * (28 * amu / 3 / kB * (dv2) + TS(3) - tn) + tn;
+        kreac = (Teff <= 1500) ? 1.4e-10 * std::pow(300 / Teff, 0.44) : 5.2e-11 * std::pow(300 / Teff, -0.2);
+        betanow = kreac * N(1) * 1e-6;
+        PR(2) = PR(2) + betanow * NS(3);
+        LO(3) = LO(3) + betanow;
+        // N2+ + NO --> NO+ + N2
+        betanow = 4.1e-10 * N(6) * 1e-6;
+        PR(2) = PR(2) + betanow * NS(3);
+        LO(3) = LO(3) + betanow;
+        // N+ + O2 --> NO+ + O
+        betanow = 2.6e-10 * N(3) * 1e-6;
+        PR(2) = PR(2) + betanow * NS(5);
+        LO(5) = LO(5) + betanow;
+        // NO+ + e --> N + O
+        betanow = 4.2e-7 * std::pow(300 / TS(LSP), 0.85) * NS(LSP) * 1e-6;
+        LO(2) = LO(2) + betanow;
+        // N2+ + O2 --> O2+ + N2
+        Teff = 32 / (28 + 32.0) * (28 * amu / 3 / kB * (dv2) + TS(3) - tn) + tn;
+        betanow = 5e-11 * (300 / Teff) * N(3) * 1e-6;
+        PR(4) = PR(4) + betanow * NS(3);
+        LO(3) = LO(3) + betanow;
+        // N2+ + e --> N + N
+        betanow = 1.8e-7 * std::pow(300 / TS(LSP), 0.39) * NS(LSP) * 1e-6;
+        LO(3) = LO(3) + betanow;
+        // N+ + O2 --> O2+ + N
+        betanow = 3.1e-10 * N(3) * 1e-6;
+        PR(4) = PR(4) + betanow * NS(5);
+        LO(5) = LO(5) + betanow;
+        // O2+ + e- --> O + O
+        kreac = (Te <= 1200) ? 1.95e-7 * std::pow(300 / Te, 0.70) : 7.38e-8 * std::pow(1200 / Te, 0.56);
+        betanow = kreac * NS(LSP) * 1e-6;
+        LO(4) = LO(4) + betanow;
+        // N+ + H --> H+ + N
+        betanow = 3.6e-12 * N(4) * 1e-6;
+        PR(6) = PR(6) + betanow * NS(5);
+        LO(5) = LO(5) + betanow;
+        // H+ + e --> H + hv
+        betanow = 3.7e-12 * std::pow(250 / TS(LSP), 0.7) * NS(LSP) * 1e-6;
+        LO(6) = LO(6) + betanow;
+      }
+}
 
 // calculus.in.f90:174-196 ETD_uncoupled on interior arrays of n values.
 void ora_etd_uncoupled(long long n, const double* f, const double* P, const double* L, double dt, double* out) {

@@ -83,6 +83,7 @@ def lib():
         L.ora_div3D.argtypes = [G, _D, _D, _D, _D]
         L.ora_compression.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
         L.ora_etd_uncoupled.argtypes = [ctypes.c_longlong, _D, _D, _D, ctypes.c_double, _D]
+        L.ora_srcs_continuity.argtypes = [G, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
         L.ora_mass_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D]
         L.ora_momentum_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
         L.ora_energy_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D, _D]
@@ -353,6 +354,19 @@ def etd_uncoupled(f, P, L, dt: float):
     out = np.empty_like(f)
     lib().ora_etd_uncoupled(f.size, _p(f), _p(P), _p(L), float(dt), _p(out))
     return out
+
+
+def srcs_continuity(grid, st, nn, vn1, vn2, vn3, Tn):
+    """Production and loss rates of the continuity equations (sources.f90:18-276).  nn:
+    interior (lx1, lx2, lx3, >=6) neutral densities O, N2, O2, H, N, NO; vn1..3, Tn:
+    interior.  Returns (Pr, Lo), interior (lx1, lx2, lx3, lsp)."""
+    g = _GridHandle(grid); b = _blocks(st)
+    nn, vn1, vn2, vn3, Tn = (np.asfortranarray(a, dtype=np.float64) for a in (nn, vn1, vn2, vn3, Tn))
+    Pr = np.zeros((grid.lx1, grid.lx2, grid.lx3, LSP), order="F")
+    Lo = np.zeros_like(Pr)
+    lib().ora_srcs_continuity(g.ref, _p(nn), _p(vn1), _p(vn2), _p(vn3), _p(Tn), b["ns"], b["vs1"], b["vs2"],
+                              b["vs3"], b["Ts"], _p(Pr), _p(Lo))
+    return Pr, Lo
 
 
 def mass_source_loss_solve(grid, st, dt: float, Pr, Lo, Prprecip):

@@ -106,3 +106,76 @@ def test_energy_source_loss_solve():
         assert np.array_equal(Ts[..., s], np.maximum((gam[s] - 1) / kB * re[..., s] / np.maximum(ns[..., s], 1e-5), 100.0))
     assert not np.array_equal(re, re0)
     assert (Ts >= 100.0).all()
+
+
+def _neutrals(g, seed, scale=1.0):
+    rng = np.random.default_rng(seed)
+    shp = (g.lx1, g.lx2, g.lx3)
+    nn = np.asfortranarray(np.stack([10 ** rng.uniform(10, 16, shp) for _ in range(7)], axis=-1) * scale)
+    vn = [np.asfortranarray(rng.uniform(-100, 100, shp)) for _ in range(3)]
+    Tn = np.asfortranarray(rng.uniform(200, 1500, shp))
+    return nn, vn, Tn
+
+
+def _recombination(ns, Ts):
+    """The five electron recombination rates of srcsContinuity (per ion density), with the C
+    library's pow."""
+    pw = np.vectorize(math.pow)
+    ne, Te = ns[..., LSP - 1], Ts[..., LSP - 1]
+    o2 = np.where(Te <= 1200, 1.95e-7 * pw(300 / Te, 0.70), 7.38e-8 * pw(1200 / Te, 0.56))
+    return {0: 3.7e-12 * pw(250 / Te, 0.7) * ne * 1e-6, 1: 4.2e-7 * pw(300 / Te, 0.85) * ne * 1e-6,
+            2: 1.8e-7 * pw(300 / Te, 0.39) * ne * 1e-6, 3: o2 * ne * 1e-6,
+            5: 3.7e-12 * pw(250 / Te, 0.7) * ne * 1e-6}
+
+
+def test_srcs_continuity_with_no_neutrals_is_recombination_alone():
+    g = G.dipole_grid(10, 4, 3)
+    st = S.init_state(g, seed=2, perturb=0.3)
+    nn, vn, Tn = _neutrals(g, 1, scale=0.0)
+    Pr, Lo = O.srcs_continuity(g, st, nn, *vn, Tn)
+    I = (slice(2, g.lx1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+    rec = _recombination(st.fluidvars[I + (slice(0, LSP),)], st.fluidvars[I + (slice(4 * LSP, 5 * LSP),)])
+    assert not Pr.any()
+    for s in range(LSP):
+        assert np.array_equal(Lo[..., s], rec.get(s, np.zeros_like(Lo[..., s])))
+
+
+def test_srcs_continuity_n_atoms_alone():
+    """With only atomic nitrogen, O2+ + N --> NO+ + O is the one ion-neutral reaction."""
+    g = G.cartesian_grid(9, 4, 3)
+    st = S.init_state(g, seed=5, perturb=0.2)
+    nn, vn, Tn = _neutrals(g, 2)
+    nn[..., [0, 1, 2, 3, 5, 6]] = 0.0
+    Pr, Lo = O.srcs_continuity(g, st, nn, *vn, Tn)
+    I = (slice(2, g.lx1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+    ns = st.fluidvars[I + (slice(0, LSP),)]
+    beta = 1.2e-10 * nn[..., 4] * 1e-6
+    assert np.array_equal(Pr[..., 1], 0.0 + beta * ns[..., 3])
+    rec = _recombination(ns, st.fluidvars[I + (slice(4 * LSP, 5 * LSP),)])
+    assert np.array_equal(Lo[..., 3], (0.0 + beta) + rec[3])
+    assert not Pr[..., [0, 2, 3, 4, 5, 6]].any()
+
+
+def test_srcs_continuity_conserves_ions_up_to_recombination():
+    """Every ion-neutral reaction moves density from one ion species to another, so the
+    ions' total production minus loss is minus the electron recombination alone."""
+    for mk, seed in ((lambda: G.dipole_grid(16, 5, 4), 3), (lambda: G.cartesian_grid(12, 5, 4), 4)):
+        g = mk()
+        st = S.init_state(g, seed=seed, perturb=0.3)
+        I = (slice(2, g.lx1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+        fv = st.fluidvars
+        rng = np.random.default_rng(seed)
+        fv[I + (slice(LSP, 2 * LSP),)] = rng.uniform(-2000, 2000, fv[I + (slice(LSP, 2 * LSP),)].shape)
+        nn, vn, Tn = _neutrals(g, seed)
+        Pr, Lo = O.srcs_continuity(g, st, nn, *vn, Tn)
+        ns = fv[I + (slice(0, LSP),)]
+        rec = _recombination(ns, fv[I + (slice(4 * LSP, 5 * LSP),)])
+        net = np.zeros(ns.shape[:3])
+        scale = np.zeros(ns.shape[:3])
+        for s in range(LSP - 1):
+            net = net + Pr[..., s] - Lo[..., s] * ns[..., s]
+            scale = scale + Pr[..., s] + Lo[..., s] * ns[..., s]
+        for s, r in rec.items():
+            net = net + r * ns[..., s]
+        assert (np.abs(net) <= 1e-13 * scale).all()
+        assert (Pr >= 0).all() and (Lo >= 0).all()
