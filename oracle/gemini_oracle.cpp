@@ -7,7 +7,8 @@
 // band LU restated from its published algorithm) and the CFL time step; and, ahead of
 // its device version, the compression sub-step (artificial viscosity, the RK2
 // zero-order-hold ghosts, div3D_curv_23 and the two-stage energy update) and the
-// source/loss ETD solves, with the continuity equations' production/loss rates.
+// source/loss ETD solves, with the continuity and energy equations' production/loss
+// rates and the collision frequencies they use.
 //
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 // library, as the checker.  The product (gemini_b200/) never links or calls it.
@@ -1395,6 +1396,152 @@ void ora_srcs_continuity(const ora_grid* G, const double* nn, const double* vn1,
         // H+ + e --> H + hv
         betanow = 3.7e-12 * std::pow(250 / TS(LSP), 0.7) * NS(LSP) * 1e-6;
         LO(6) = LO(6) + betanow;
+      }
+}
+
+// ---- collisions.f90:12-55 collision coefficient tables (lsp x ln and lsp x lsp, filled
+// row by row by reshape(..., order=[2,1])); default-REAL literals widened to real(wp) --------
+constexpr int LN = 4;  // phys_consts.in.f90:39 (O, N2, O2, H)
+struct CollTables {
+  double Csn[LSP][LN], C2sn1[LSP][LN], C2sn2[LSP][LN], Csj[LSP][LSP], mn[LN];
+  CollTables() {
+    const float csn[LSP][LN] = {{-1, 6.82e-10f, 6.64e-10f, -1},       {2.44e-10f, 4.34e-10f, 4.27e-10f, 0.69e-10f},
+                                {2.58e-10f, -1, 4.49e-10f, 0.74e-10f}, {2.31e-10f, 4.13e-10f, -1, 0.65e-10f},
+                                {4.42e-10f, 7.47e-10f, 7.25e-10f, 1.45e-10f}, {-1, 33.6e-10f, 32.0e-10f, -1},
+                                {-1, -1, -1, -1}};
+    const float c1[LSP][LN] = {{3.67e-11f, 0, 0, 4.63e-12f}, {0, 0, 0, 0}, {0, 5.14e-11f, 0, 0},
+                               {0, 0, 2.59e-11f, 0},         {0, 0, 0, 0}, {6.61e-11f, 0, 0, 2.65e-10f},
+                               {-1, -1, -1, -1}};
+    const float c2[LSP][LN] = {{0.064f, 0, 0, -1}, {0, 0, 0, 0},         {0, 0.069f, 0, 0},   {0, 0, 0.073f, 0},
+                               {0, 0, 0, 0},       {0.047f, 0, 0, 0.083f}, {-1, -1, -1, -1}};
+    const float csj[LSP][LSP] = {{0.22f, 0.26f, 0.25f, 0.26f, 0.22f, 0.077f, 1.87e-3f},
+                                 {0.14f, 0.16f, 0.16f, 0.17f, 0.13f, 0.042f, 9.97e-4f},
+                                 {0.15f, 0.17f, 0.17f, 0.18f, 0.14f, 0.045f, 1.07e-3f},
+                                 {0.13f, 0.16f, 0.15f, 0.16f, 0.12f, 0.039f, 9.347e-4f},
+                                 {0.25f, 0.28f, 0.28f, 0.28f, 0.24f, 0.088f, 2.136e-3f},
+                                 {1.23f, 1.25f, 1.25f, 1.25f, 1.23f, 0.90f, 29.7e-3f},
+                                 {54.5f, 54.5f, 54.5f, 54.5f, 54.5f, 54.5f, 38.537f}};
+    for (int i = 0; i < LSP; ++i) {
+      for (int j = 0; j < LN; ++j) {
+        Csn[i][j] = (double)csn[i][j];
+        C2sn1[i][j] = (double)c1[i][j];
+        C2sn2[i][j] = (double)c2[i][j];
+      }
+      for (int j = 0; j < LSP; ++j) Csj[i][j] = (double)csj[i][j];
+    }
+    const double m[LN] = {16, 28, 32, 1};  // phys_consts.in.f90:41
+    for (int j = 0; j < LN; ++j) mn[j] = m[j] * amu;
+  }
+};
+const CollTables KC;
+const double pi_c = 4 * std::atan(1.0);  // phys_consts.in.f90:20
+
+// collisions.f90:58-114 maxwell_colln for one cell: isp (0-based species), isp2 (0-based
+// neutral); nn2 = nn(.,isp2), Tn and Ts(isp) of the cell.
+inline double maxwell_colln(int isp, int isp2, double nn2, double tn, double ts) {
+  if (isp < LSP - 1) {
+    if (KC.Csn[isp][isp2] < 0) {  // resonant
+      if (isp == 0 && isp2 == 3) {
+        const double Teff = tn + ts / 16;
+        return KC.C2sn1[isp][isp2] * std::pow(Teff, 0.5) * nn2 * 1e-6;
+      }
+      const double Teff = 0.5 * (tn + ts);
+      const double a = 1 - KC.C2sn2[isp][isp2] * std::log10(Teff);
+      return KC.C2sn1[isp][isp2] * (a * a) * (std::pow(Teff, 0.5)) * nn2 * 1e-6;
+    }
+    return KC.Csn[isp][isp2] * nn2 * 1e-6;  // nonresonant
+  }
+  const double Teff = ts;  // electron-neutral
+  switch (isp2) {
+    case 0: return 8.9e-11 * (1.0 + 5.7e-4 * Teff) * (std::pow(Teff, 0.5)) * nn2 * 1e-6;
+    case 1: return 2.33e-11 * (1.0 - 1.21e-4 * Teff) * (Teff)*nn2 * 1e-6;
+    case 2: return 1.82e-10 * (1.0 + 3.6e-2 * (std::pow(Teff, 0.5))) * (std::pow(Teff, 0.5)) * nn2 * 1e-6;
+    default: return 4.5e-9 * (1.0 - 1.35e-4 * Teff) * (std::pow(Teff, 0.5)) * nn2 * 1e-6;
+  }
+}
+
+// collisions.f90:117-159 coulomb_colln for one cell: nusj, Phisj, Psisj (zero for isp == isp2).
+inline void coulomb_colln(int isp, int isp2, double ns2, double ts1, double ts2, double v1, double v2, double& nu,
+                          double& Phi, double& Psi) {
+  if (isp == isp2) {
+    nu = Phi = Psi = 0.0;
+    return;
+  }
+  const double ms1 = K.ms[isp], ms2 = K.ms[isp2];
+  const double Teff = (ms2 * ts1 + ms1 * ts2) / (ms2 + ms1);
+  nu = KC.Csj[isp][isp2] * ns2 * 1e-6 / std::pow(Teff, 1.5);
+  const double mred = ms1 * ms2 / (ms1 + ms2);
+  const double W = std::fabs(v1 - v2) / std::sqrt(2 * kB * Teff / mred);
+  Psi = std::exp(-(W * W));
+  if (W < 0.1)
+    Phi = 1;
+  else
+    Phi = 3.0 / 4 * std::sqrt(pi_c) * std::erf(W) / (W * W * W) - 3.0 / 2 / (W * W) * Psi;
+}
+
+// sources.f90:396-485 srcsEnergy: production and loss rates of the energy equations.
+// nn: interior (lx1,lx2,lx3,>=4) neutral densities O, N2, O2, H; the rest as
+// ora_srcs_continuity.  Pr, Lo zeroed first.
+void ora_srcs_energy(const ora_grid* G, const double* nn, const double* vn1, const double* vn2, const double* vn3,
+                     const double* Tn, const double* ns, const double* vs1, const double* vs2, const double* vs3,
+                     const double* Ts, double* Pr, double* Lo) {
+  Ix X(G);
+  const long long nc = X.nc();
+  for (long long q = 0; q < LSP * nc; ++q) Pr[q] = Lo[q] = 0.0;
+  const double sfact = elchrg / kB * (K.gammas[LSP - 1] - 1);
+  for (int i3 = 1; i3 <= G->lx3; ++i3)
+    for (int i2 = 1; i2 <= G->lx2; ++i2)
+      for (int i1 = 1; i1 <= G->lx1; ++i1) {
+        const long long c = X.c(i1, i2, i3), k = X.g(i1, i2, i3);
+        const double tn = Tn[c];
+        auto NS = [&](int s) { return ns[s * X.ng + k]; };
+        auto TS = [&](int s) { return Ts[s * X.ng + k]; };
+        auto V1 = [&](int s) { return vs1[s * X.ng + k]; };
+        auto V2 = [&](int s) { return vs2[s * X.ng + k]; };
+        auto V3 = [&](int s) { return vs3[s * X.ng + k]; };
+        for (int isp = 0; isp < LSP; ++isp) {
+          double& pr = Pr[isp * nc + c];
+          double& lo = Lo[isp * nc + c];
+          const double ms = K.ms[isp], gm1 = K.gammas[isp] - 1;
+          for (int isp2 = 0; isp2 < LN; ++isp2) {  // ion-neutral
+            const double nu = maxwell_colln(isp, isp2, nn[isp2 * nc + c], tn, TS(isp));
+            double fact = 2 * nu / (ms + KC.mn[isp2]);
+            pr = pr + NS(isp) * ms * kB / gm1 * fact * tn;
+            lo = lo + ms * fact;
+            fact = fact * KC.mn[isp2] / 3;
+            const double d1 = V1(isp) - vn1[c], d2 = V2(isp) - vn2[c], d3 = V3(isp) - vn3[c];
+            pr = pr + NS(isp) * ms / gm1 * ((d1 * d1) + (d2 * d2) + (d3 * d3)) * fact;
+          }
+          for (int isp2 = 0; isp2 < LSP; ++isp2) {  // ion-ion
+            double nu, Phi, Psi;
+            coulomb_colln(isp, isp2, NS(isp2), TS(isp), TS(isp2), V1(isp), V1(isp2), nu, Phi, Psi);
+            double fact = 2 * nu * Psi / (ms + K.ms[isp2]);
+            pr = pr + NS(isp) * ms * kB / gm1 * fact * TS(isp2);
+            lo = lo + ms * fact;
+            fact = 2 * nu * Phi / (ms + K.ms[isp2]) * K.ms[isp2] / 3;
+            const double d1 = V1(isp) - V1(isp2), d2 = V2(isp) - V2(isp2), d3 = V3(isp) - V3(isp2);
+            pr = pr + NS(isp) * ms / gm1 * ((d1 * d1) + (d2 * d2) + (d3 * d3)) * fact;
+          }
+        }
+        // inelastic electron collisions: rotational, then vibrational excitation
+        const double Te = TS(LSP - 1);
+        double nu = sfact * 6.9e-14 * nn[2 * nc + c] * 1e-6 / std::sqrt(Te);  // O2 rotational
+        double iePT = nu * tn;
+        double ieLT = nu;
+        nu = sfact * 2.9e-14 * nn[1 * nc + c] * 1e-6 / std::sqrt(Te);  // N2 rotational
+        iePT = iePT + nu * tn;
+        ieLT = ieLT + nu;
+        double f = 1.06e4 + 7.51e3 * std::tanh(1.10e-3 * (Te - 1800));
+        const double g = 3300 + 1.233 * (Te - 1000) - 2.056e-4 * (Te - 1000) * (Te - 4000);
+        double fact = sfact * 2.99e-12 * nn[1 * nc + c] * 1e-6 * std::exp(f * (Te - 2000) / Te / 2000) *
+                      (std::exp(-g * (Te - tn) / Te / tn) - 1);  // N2 vibrational
+        iePT = iePT - fmax_f(fact, 0.0);
+        f = 3300 - 839 * std::sin(1.91e-4 * (Te - 2700));
+        fact = sfact * 5.196e-13 * nn[2 * nc + c] * 1e-6 * std::exp(f * (Te - 700) / Te / 700) *
+               (std::exp(-2770 * (Te - tn) / Te / tn) - 1);  // O2 vibrational
+        iePT = iePT - fmax_f(fact, 0.0);
+        Pr[(LSP - 1) * nc + c] = Pr[(LSP - 1) * nc + c] + iePT * NS(LSP - 1) * kB / (K.gammas[LSP - 1] - 1);
+        Lo[(LSP - 1) * nc + c] = Lo[(LSP - 1) * nc + c] + ieLT;
       }
 }
 

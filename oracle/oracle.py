@@ -84,6 +84,7 @@ def lib():
         L.ora_compression.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
         L.ora_etd_uncoupled.argtypes = [ctypes.c_longlong, _D, _D, _D, ctypes.c_double, _D]
         L.ora_srcs_continuity.argtypes = [G, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
+        L.ora_srcs_energy.argtypes = [G, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
         L.ora_mass_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D]
         L.ora_momentum_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
         L.ora_energy_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D, _D]
@@ -366,6 +367,19 @@ def srcs_continuity(grid, st, nn, vn1, vn2, vn3, Tn):
     Lo = np.zeros_like(Pr)
     lib().ora_srcs_continuity(g.ref, _p(nn), _p(vn1), _p(vn2), _p(vn3), _p(Tn), b["ns"], b["vs1"], b["vs2"],
                               b["vs3"], b["Ts"], _p(Pr), _p(Lo))
+    return Pr, Lo
+
+
+def srcs_energy(grid, st, nn, vn1, vn2, vn3, Tn):
+    """Production and loss rates of the energy equations (sources.f90:396-485, with
+    collisions.f90:58-159).  nn: interior (lx1, lx2, lx3, >=4) neutral densities O, N2, O2,
+    H; vn1..3, Tn: interior.  Returns (Pr, Lo), interior (lx1, lx2, lx3, lsp)."""
+    g = _GridHandle(grid); b = _blocks(st)
+    nn, vn1, vn2, vn3, Tn = (np.asfortranarray(a, dtype=np.float64) for a in (nn, vn1, vn2, vn3, Tn))
+    Pr = np.zeros((grid.lx1, grid.lx2, grid.lx3, LSP), order="F")
+    Lo = np.zeros_like(Pr)
+    lib().ora_srcs_energy(g.ref, _p(nn), _p(vn1), _p(vn2), _p(vn3), _p(Tn), b["ns"], b["vs1"], b["vs2"],
+                          b["vs3"], b["Ts"], _p(Pr), _p(Lo))
     return Pr, Lo
 
 

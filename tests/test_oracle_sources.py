@@ -179,3 +179,130 @@ def test_srcs_continuity_conserves_ions_up_to_recombination():
             net = net + r * ns[..., s]
         assert (np.abs(net) <= 1e-13 * scale).all()
         assert (Pr >= 0).all() and (Lo >= 0).all()
+
+
+# ---- srcsEnergy: an independent, vectorised numpy statement (C library functions) ----------
+
+_F32 = lambda rows: np.array(rows, dtype=np.float32).astype(np.float64)
+_CSN = _F32([[-1, 6.82e-10, 6.64e-10, -1], [2.44e-10, 4.34e-10, 4.27e-10, 0.69e-10],
+             [2.58e-10, -1, 4.49e-10, 0.74e-10], [2.31e-10, 4.13e-10, -1, 0.65e-10],
+             [4.42e-10, 7.47e-10, 7.25e-10, 1.45e-10], [-1, 33.6e-10, 32.0e-10, -1], [-1, -1, -1, -1]])
+_C2SN1 = _F32([[3.67e-11, 0, 0, 4.63e-12], [0, 0, 0, 0], [0, 5.14e-11, 0, 0], [0, 0, 2.59e-11, 0],
+               [0, 0, 0, 0], [6.61e-11, 0, 0, 2.65e-10], [-1, -1, -1, -1]])
+_C2SN2 = _F32([[0.064, 0, 0, -1], [0, 0, 0, 0], [0, 0.069, 0, 0], [0, 0, 0.073, 0], [0, 0, 0, 0],
+               [0.047, 0, 0, 0.083], [-1, -1, -1, -1]])
+_CSJ = _F32([[0.22, 0.26, 0.25, 0.26, 0.22, 0.077, 1.87e-3], [0.14, 0.16, 0.16, 0.17, 0.13, 0.042, 9.97e-4],
+             [0.15, 0.17, 0.17, 0.18, 0.14, 0.045, 1.07e-3], [0.13, 0.16, 0.15, 0.16, 0.12, 0.039, 9.347e-4],
+             [0.25, 0.28, 0.28, 0.28, 0.24, 0.088, 2.136e-3], [1.23, 1.25, 1.25, 1.25, 1.23, 0.90, 29.7e-3],
+             [54.5, 54.5, 54.5, 54.5, 54.5, 54.5, 38.537]])
+_AMU, _KB, _EL = 1.660539040e-27, 1.38064852e-23, 1.60217662e-19
+_MN = np.array([16.0, 28.0, 32.0, 1.0]) * _AMU
+_V = {n: np.vectorize(getattr(math, n)) for n in ("pow", "erf", "log10", "exp", "tanh", "sin", "sqrt")}
+
+
+def _np_maxwell(isp, j, nnj, tn, ts):
+    pw = _V["pow"]
+    if isp < LSP - 1:
+        if _CSN[isp, j] < 0:
+            if isp == 0 and j == 3:
+                return _C2SN1[isp, j] * pw(tn + ts / 16, 0.5) * nnj * 1e-6
+            te = 0.5 * (tn + ts)
+            a = 1 - _C2SN2[isp, j] * _V["log10"](te)
+            return _C2SN1[isp, j] * (a * a) * pw(te, 0.5) * nnj * 1e-6
+        return _CSN[isp, j] * nnj * 1e-6
+    te = ts
+    r = [lambda: 8.9e-11 * (1.0 + 5.7e-4 * te) * pw(te, 0.5), lambda: 2.33e-11 * (1.0 - 1.21e-4 * te) * te,
+         lambda: 1.82e-10 * (1.0 + 3.6e-2 * pw(te, 0.5)) * pw(te, 0.5),
+         lambda: 4.5e-9 * (1.0 - 1.35e-4 * te) * pw(te, 0.5)][j]()
+    return r * nnj * 1e-6
+
+
+def _np_coulomb(isp, t, ms, ns2, ts1, ts2, v1, v2):
+    if isp == t:
+        z = np.zeros_like(ts1)
+        return z, z, z
+    te = (ms[t] * ts1 + ms[isp] * ts2) / (ms[t] + ms[isp])
+    nu = _CSJ[isp, t] * ns2 * 1e-6 / _V["pow"](te, 1.5)
+    mred = ms[isp] * ms[t] / (ms[isp] + ms[t])
+    W = np.abs(v1 - v2) / _V["sqrt"](2 * _KB * te / mred)
+    psi = _V["exp"](-(W * W))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        phi = np.where(W < 0.1, 1.0, 3.0 / 4 * math.sqrt(math.pi) * _V["erf"](W) / (W * W * W) - 3.0 / 2 / (W * W) * psi)
+    return nu, phi, psi
+
+
+def _np_srcs_energy(g, st, nn, vn1, vn2, vn3, Tn):
+    ms, _, gam, _ = O.constants()
+    I = (slice(2, g.lx1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+    fv = st.fluidvars
+    ns, v1, v2, v3, Ts = (fv[I + (slice(k * LSP, (k + 1) * LSP),)] for k in range(5))
+    Pr = np.zeros(ns.shape)
+    Lo = np.zeros(ns.shape)
+    for s in range(LSP):
+        for j in range(4):
+            nu = _np_maxwell(s, j, nn[..., j], Tn, Ts[..., s])
+            fact = 2 * nu / (ms[s] + _MN[j])
+            Pr[..., s] = Pr[..., s] + ns[..., s] * ms[s] * _KB / (gam[s] - 1) * fact * Tn
+            Lo[..., s] = Lo[..., s] + ms[s] * fact
+            fact = fact * _MN[j] / 3
+            d = ((v1[..., s] - vn1) * (v1[..., s] - vn1) + (v2[..., s] - vn2) * (v2[..., s] - vn2)
+                 + (v3[..., s] - vn3) * (v3[..., s] - vn3))
+            Pr[..., s] = Pr[..., s] + ns[..., s] * ms[s] / (gam[s] - 1) * d * fact
+        for t in range(LSP):
+            nu, phi, psi = _np_coulomb(s, t, ms, ns[..., t], Ts[..., s], Ts[..., t], v1[..., s], v1[..., t])
+            fact = 2 * nu * psi / (ms[s] + ms[t])
+            Pr[..., s] = Pr[..., s] + ns[..., s] * ms[s] * _KB / (gam[s] - 1) * fact * Ts[..., t]
+            Lo[..., s] = Lo[..., s] + ms[s] * fact
+            fact = 2 * nu * phi / (ms[s] + ms[t]) * ms[t] / 3
+            d = ((v1[..., s] - v1[..., t]) * (v1[..., s] - v1[..., t]) + (v2[..., s] - v2[..., t]) * (v2[..., s] - v2[..., t])
+                 + (v3[..., s] - v3[..., t]) * (v3[..., s] - v3[..., t]))
+            Pr[..., s] = Pr[..., s] + ns[..., s] * ms[s] / (gam[s] - 1) * d * fact
+    sf = _EL / _KB * (gam[LSP - 1] - 1)
+    Te = Ts[..., LSP - 1]
+    nu = sf * 6.9e-14 * nn[..., 2] * 1e-6 / _V["sqrt"](Te)
+    pT, lT = nu * Tn, nu
+    nu = sf * 2.9e-14 * nn[..., 1] * 1e-6 / _V["sqrt"](Te)
+    pT, lT = pT + nu * Tn, lT + nu
+    f = 1.06e4 + 7.51e3 * _V["tanh"](1.10e-3 * (Te - 1800))
+    gg = 3300 + 1.233 * (Te - 1000) - 2.056e-4 * (Te - 1000) * (Te - 4000)
+    fact = (sf * 2.99e-12 * nn[..., 1] * 1e-6 * _V["exp"](f * (Te - 2000) / Te / 2000)
+            * (_V["exp"](-gg * (Te - Tn) / Te / Tn) - 1))
+    pT = pT - np.maximum(fact, 0.0)
+    f = 3300 - 839 * _V["sin"](1.91e-4 * (Te - 2700))
+    fact = (sf * 5.196e-13 * nn[..., 2] * 1e-6 * _V["exp"](f * (Te - 700) / Te / 700)
+            * (_V["exp"](-2770 * (Te - Tn) / Te / Tn) - 1))
+    pT = pT - np.maximum(fact, 0.0)
+    Pr[..., LSP - 1] = Pr[..., LSP - 1] + pT * ns[..., LSP - 1] * _KB / (gam[LSP - 1] - 1)
+    Lo[..., LSP - 1] = Lo[..., LSP - 1] + lT
+    return Pr, Lo
+
+
+def test_srcs_energy_matches_numpy_statement():
+    g = G.dipole_grid(10, 4, 3)
+    st = S.init_state(g, seed=12, perturb=0.3)
+    rng = np.random.default_rng(12)
+    fv = st.fluidvars
+    I = (slice(2, g.lx1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+    for k in (1, 2, 3):  # velocities of every species, some pairs far apart (Phi branch)
+        fv[I + (slice(k * LSP, (k + 1) * LSP),)] = rng.uniform(-3000, 3000, fv[I + (slice(0, LSP),)].shape)
+    nn, vn, Tn = _neutrals(g, 12)
+    Pr, Lo = O.srcs_energy(g, st, nn, *vn, Tn)
+    Pw, Lw = _np_srcs_energy(g, st, nn, *vn, Tn)
+    assert np.array_equal(Lo, Lw)
+    assert np.array_equal(Pr, Pw)
+    # finite everywhere; Lo is not sign-definite: the electron-N2 and electron-H collision
+    # fits (1 - 1.21e-4 Te, 1 - 1.35e-4 Te) turn negative above ~8300 K and ~7400 K
+    assert np.isfinite(Lo).all() and np.isfinite(Pr).all()
+
+
+def test_srcs_energy_electron_rotational_cooling_alone():
+    """With only O2 as neutral and no ions in motion, the electrons' loss rate holds the O2
+    rotational term and the ion-neutral / Coulomb terms."""
+    g = G.cartesian_grid(8, 3, 3)
+    st = S.init_state(g, seed=3, perturb=0.1)
+    nn, vn, Tn = _neutrals(g, 3)
+    nn[..., [0, 1, 3]] = 0.0
+    Pr, Lo = O.srcs_energy(g, st, nn, *vn, Tn)
+    Pw, Lw = _np_srcs_energy(g, st, nn, *vn, Tn)
+    assert np.array_equal(Lo, Lw) and np.array_equal(Pr, Pw)
+    assert (Lo[..., LSP - 1] > 0).all()
