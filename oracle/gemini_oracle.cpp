@@ -7,8 +7,8 @@
 // band LU restated from its published algorithm) and the CFL time step; and, ahead of
 // its device version, the compression sub-step (artificial viscosity, the RK2
 // zero-order-hold ghosts, div3D_curv_23 and the two-stage energy update) and the
-// source/loss ETD solves, with the continuity and energy equations' production/loss
-// rates and the collision frequencies they use.
+// source/loss ETD solves, with the continuity, momentum and energy equations'
+// production/loss rates and the collision frequencies they use.
 //
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 // library, as the checker.  The product (gemini_b200/) never links or calls it.
@@ -1543,6 +1543,89 @@ void ora_srcs_energy(const ora_grid* G, const double* nn, const double* vn1, con
         Pr[(LSP - 1) * nc + c] = Pr[(LSP - 1) * nc + c] + iePT * NS(LSP - 1) * kB / (K.gammas[LSP - 1] - 1);
         Lo[(LSP - 1) * nc + c] = Lo[(LSP - 1) * nc + c] + ieLT;
       }
+}
+
+// calculus/gradient.f90:79-150 grad3D1_curv_23 along one x1 line of n points with grid x1
+// indices i0 .. i0+n-1: f[j], h1 at those cells, dx1 = x%dx1(i0:i0+n-1) (dx1[j] is grid
+// index i0+j).  The first point divides by dx1(i0), as the reference does.
+inline void grad1_line(int n, const double* f, const double* h1, const double* dx1, double* out) {
+  out[0] = (f[1] - f[0]) / dx1[0] / h1[0];
+  for (int j = 1; j < n - 1; ++j) out[j] = (f[j + 1] - f[j - 1]) / (dx1[j + 1] + dx1[j]) / h1[j];
+  out[n - 1] = (f[n - 1] - f[n - 2]) / dx1[n - 1] / h1[n - 1];
+}
+
+// sources.f90:279-393 srcsMomentum_curv on a single rank (both x1 ends global: the x1
+// gradients over 1..lx1).  nn: interior (lx1,lx2,lx3,>=4); vn1, Tn, Q (lx1,lx2,lx3,lsp), alt,
+// g1: interior; ns, vs1, vs2, vs3, Ts, E1: ghosted.  Pr, Lo zeroed first.
+void ora_srcs_momentum(const ora_grid* G, const double* nn, const double* vn1, const double* Tn, const double* ns,
+                       const double* vs1, const double* vs2, const double* vs3, const double* Ts, const double* E1,
+                       const double* Q, const double* alt, const double* g1, double* Pr, double* Lo) {
+  Ix X(G);
+  const long long nc = X.nc();
+  const int n = G->lx1;
+  for (long long q = 0; q < LSP * nc; ++q) Pr[q] = Lo[q] = 0.0;
+  std::vector<double> hl(n + 2), dl(n + 2), fl(n + 2), gl(n + 2), h1l(n), dxl(n), dh2(n), dh3(n), epol(n), pg(n),
+      gq(n), pr_(n);
+  for (int i3 = 1; i3 <= G->lx3; ++i3)
+    for (int i2 = 1; i2 <= G->lx2; ++i2) {
+      // dh2/dx1, dh3/dx1: grad3D1 over x1 indices 0..lx1+1, kept at 1..lx1
+      for (int j = 0; j < n + 2; ++j) dl[j] = G->dx1[j];  // x%dx1(0:lx1+1)
+      for (int j = 0; j < n + 2; ++j) hl[j] = G->h1[X.g(j, i2, i3)];
+      for (int j = 0; j < n + 2; ++j) fl[j] = G->h2[X.g(j, i2, i3)];
+      grad1_line(n + 2, fl.data(), hl.data(), dl.data(), gl.data());
+      for (int j = 0; j < n; ++j) dh2[j] = gl[j + 1];
+      for (int j = 0; j < n + 2; ++j) fl[j] = G->h3[X.g(j, i2, i3)];
+      grad1_line(n + 2, fl.data(), hl.data(), dl.data(), gl.data());
+      for (int j = 0; j < n; ++j) dh3[j] = gl[j + 1];
+      // x1 gradients over 1..lx1
+      for (int j = 0; j < n; ++j) {
+        h1l[j] = G->h1[X.g(j + 1, i2, i3)];
+        dxl[j] = G->dx1[j + 1];  // x%dx1(1:lx1)
+      }
+      // ambipolar field: Epol1 = kB Te / qe * d log(ne kB Te)/dx1
+      for (int j = 0; j < n; ++j) {
+        const long long k = X.g(j + 1, i2, i3) + (LSP - 1) * X.ng;
+        fl[j] = std::log(ns[k] * kB * Ts[k]);
+      }
+      grad1_line(n, fl.data(), h1l.data(), dxl.data(), gl.data());
+      for (int j = 0; j < n; ++j) epol[j] = kB * Ts[X.g(j + 1, i2, i3) + (LSP - 1) * X.ng] / K.qs[LSP - 1] * gl[j];
+      for (int isp = 0; isp < LSP; ++isp) {
+        // ion pressure term pressure * d log(pressure)/dx1, and dQ/dx1
+        for (int j = 0; j < n; ++j) {
+          const long long k = X.g(j + 1, i2, i3) + isp * X.ng;
+          pr_[j] = ns[k] * kB * Ts[k];
+          fl[j] = std::log(pr_[j]);
+        }
+        grad1_line(n, fl.data(), h1l.data(), dxl.data(), pg.data());
+        for (int j = 0; j < n; ++j) fl[j] = Q[isp * nc + X.c(j + 1, i2, i3)];
+        grad1_line(n, fl.data(), h1l.data(), dxl.data(), gq.data());
+        for (int j = 0; j < n; ++j) {
+          const int i1 = j + 1;
+          const long long c = X.c(i1, i2, i3), kg = X.g(i1, i2, i3), k = kg + isp * X.ng;
+          double& pr = Pr[isp * nc + c];
+          double& lo = Lo[isp * nc + c];
+          const double ms = K.ms[isp];
+          for (int isp2 = 0; isp2 < LN; ++isp2) {  // ion-neutral
+            const double nu = maxwell_colln(isp, isp2, nn[isp2 * nc + c], Tn[c], Ts[k]);
+            lo = lo + nu;
+            pr = pr + ns[k] * ms * nu * vn1[c];
+          }
+          for (int isp2 = 0; isp2 < LSP; ++isp2) {  // ion-ion
+            double nu, Phi, Psi;
+            const long long k2 = kg + isp2 * X.ng;
+            coulomb_colln(isp, isp2, ns[k2], Ts[k], Ts[k2], vs1[k], vs1[k2], nu, Phi, Psi);
+            lo = lo + nu * Phi;
+            pr = pr + ns[k] * ms * nu * Phi * vs1[k2];
+          }
+          const double ionpress = pr_[j] * pg[j];
+          const double h1h2h3 = G->h1[kg] * G->h2[kg] * G->h3[kg];
+          const double geom = (vs2[k] * vs2[k] * G->h3[kg] * dh2[j] + vs3[k] * vs3[k] * G->h2[kg] * dh3[j]) * ns[k] *
+                              ms / h1h2h3;
+          const double e1f = (alt[c] < 100e3) ? 0.0 : E1[kg];
+          pr = pr + ns[k] * K.qs[isp] * (e1f + epol[j]) - ionpress - gq[j] + geom + ns[k] * ms * g1[c];
+        }
+      }
+    }
 }
 
 // calculus.in.f90:174-196 ETD_uncoupled on interior arrays of n values.

@@ -85,6 +85,7 @@ def lib():
         L.ora_etd_uncoupled.argtypes = [ctypes.c_longlong, _D, _D, _D, ctypes.c_double, _D]
         L.ora_srcs_continuity.argtypes = [G, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
         L.ora_srcs_energy.argtypes = [G, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
+        L.ora_srcs_momentum.argtypes = [G] + [_D] * 14
         L.ora_mass_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D]
         L.ora_momentum_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
         L.ora_energy_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D, _D]
@@ -380,6 +381,22 @@ def srcs_energy(grid, st, nn, vn1, vn2, vn3, Tn):
     Lo = np.zeros_like(Pr)
     lib().ora_srcs_energy(g.ref, _p(nn), _p(vn1), _p(vn2), _p(vn3), _p(Tn), b["ns"], b["vs1"], b["vs2"],
                           b["vs3"], b["Ts"], _p(Pr), _p(Lo))
+    return Pr, Lo
+
+
+def srcs_momentum(grid, st, nn, vn1, Tn, E1, Q, g1):
+    """Production and loss rates of the momentum equations (sources.f90:279-393), single
+    rank.  nn: interior (lx1, lx2, lx3, >=4); vn1, Tn, g1: interior; E1: ghosted; Q: interior
+    (lx1, lx2, lx3, lsp); the altitude filter reads grid.alt.  Returns (Pr, Lo)."""
+    g = _GridHandle(grid); b = _blocks(st)
+    alt = grid.alt
+    if alt.shape[0] == grid.lx1 + 4:
+        alt = alt[2:-2, 2:-2, 2:-2]
+    nn, vn1, Tn, E1, Q, g1, alt = (np.asfortranarray(a, dtype=np.float64) for a in (nn, vn1, Tn, E1, Q, g1, alt))
+    Pr = np.zeros((grid.lx1, grid.lx2, grid.lx3, LSP), order="F")
+    Lo = np.zeros_like(Pr)
+    lib().ora_srcs_momentum(g.ref, _p(nn), _p(vn1), _p(Tn), b["ns"], b["vs1"], b["vs2"], b["vs3"], b["Ts"], _p(E1),
+                            _p(Q), _p(alt), _p(g1), _p(Pr), _p(Lo))
     return Pr, Lo
 
 

@@ -306,3 +306,92 @@ def test_srcs_energy_electron_rotational_cooling_alone():
     Pw, Lw = _np_srcs_energy(g, st, nn, *vn, Tn)
     assert np.array_equal(Lo, Lw) and np.array_equal(Pr, Pw)
     assert (Lo[..., LSP - 1] > 0).all()
+
+
+# ---- srcsMomentum_curv (single rank): numpy statement and a plasma at rest -----------------
+
+def _np_grad1(f, h1, dx1):
+    """grad3D1_curv_23 along axis 0 (the first point divides by dx1[0], as the reference)."""
+    out = np.empty_like(f)
+    out[0] = (f[1] - f[0]) / dx1[0] / h1[0]
+    out[1:-1] = (f[2:] - f[:-2]) / (dx1[2:] + dx1[1:-1])[:, None, None] / h1[1:-1]
+    out[-1] = (f[-1] - f[-2]) / dx1[-1] / h1[-1]
+    return out
+
+
+def _np_srcs_momentum(g, st, nn, vn1, Tn, E1, Q, g1):
+    ms, qs, _, _ = O.constants()
+    n1 = g.lx1
+    I = (slice(2, n1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+    J = (slice(1, n1 + 3), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))  # x1 indices 0..lx1+1
+    fv = st.fluidvars
+    ns, v1, v2, v3, Ts = (fv[I + (slice(k * LSP, (k + 1) * LSP),)] for k in range(5))
+    h1, h2, h3 = g.h1[I], g.h2[I], g.h3[I]
+    dh2 = _np_grad1(g.h2[J], g.h1[J], g.dx1[0:n1 + 2])[1:-1]
+    dh3 = _np_grad1(g.h3[J], g.h1[J], g.dx1[0:n1 + 2])[1:-1]
+    dxi = g.dx1[1:n1 + 1]
+    lg = np.vectorize(math.log)
+    Te = Ts[..., LSP - 1]
+    epol = _KB * Te / qs[LSP - 1] * _np_grad1(lg(ns[..., LSP - 1] * _KB * Te), h1, dxi)
+    alt = g.alt[I]
+    e1f = np.where(alt < 100e3, 0.0, E1[I])
+    Pr = np.zeros(ns.shape)
+    Lo = np.zeros(ns.shape)
+    for s in range(LSP):
+        for j in range(4):
+            nu = _np_maxwell(s, j, nn[..., j], Tn, Ts[..., s])
+            Lo[..., s] = Lo[..., s] + nu
+            Pr[..., s] = Pr[..., s] + ns[..., s] * ms[s] * nu * vn1
+        for t in range(LSP):
+            nu, phi, _ = _np_coulomb(s, t, ms, ns[..., t], Ts[..., s], Ts[..., t], v1[..., s], v1[..., t])
+            Lo[..., s] = Lo[..., s] + nu * phi
+            Pr[..., s] = Pr[..., s] + ns[..., s] * ms[s] * nu * phi * v1[..., t]
+        p = ns[..., s] * _KB * Ts[..., s]
+        ionpress = p * _np_grad1(lg(p), h1, dxi)
+        gq = _np_grad1(Q[..., s], h1, dxi)
+        geom = (v2[..., s] * v2[..., s] * h3 * dh2 + v3[..., s] * v3[..., s] * h2 * dh3) * ns[..., s] * ms[s] / (h1 * h2 * h3)
+        Pr[..., s] = Pr[..., s] + ns[..., s] * qs[s] * (e1f + epol) - ionpress - gq + geom + ns[..., s] * ms[s] * g1
+    return Pr, Lo
+
+
+def _momentum_inputs(g, seed):
+    rng = np.random.default_rng(seed)
+    shp = (g.lx1, g.lx2, g.lx3)
+    nn, vn, Tn = _neutrals(g, seed)
+    E1 = np.asfortranarray(rng.uniform(-1e-3, 1e-3, (g.lx1 + 4, g.lx2 + 4, g.lx3 + 4)))
+    Q = np.asfortranarray(rng.uniform(0, 1e-12, shp + (LSP,)))
+    g1 = np.asfortranarray(rng.uniform(-9.8, -8.0, shp))
+    return nn, vn[0], Tn, E1, Q, g1
+
+
+def test_srcs_momentum_matches_numpy_statement():
+    g = G.dipole_grid(12, 4, 3)
+    st = S.init_state(g, seed=21, perturb=0.3)
+    rng = np.random.default_rng(21)
+    fv = st.fluidvars
+    I = (slice(2, g.lx1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+    for k in (1, 2, 3):
+        fv[I + (slice(k * LSP, (k + 1) * LSP),)] = rng.uniform(-3000, 3000, fv[I + (slice(0, LSP),)].shape)
+    args = _momentum_inputs(g, 21)
+    Pr, Lo = O.srcs_momentum(g, st, *args)
+    Pw, Lw = _np_srcs_momentum(g, st, *args)
+    assert np.array_equal(Lo, Lw)
+    assert np.array_equal(Pr, Pw)
+    assert np.isfinite(Pr).all() and (g.alt[I] < 100e3).any() and (g.alt[I] >= 100e3).any()
+
+
+def test_srcs_momentum_of_a_uniform_plasma_at_rest_is_zero():
+    """No flow, no neutral wind, no field, no gravity, uniform density and temperature:
+    every force term vanishes, while the collision loss rates do not."""
+    g = G.cartesian_grid(10, 4, 3)
+    st = S.init_state(g, seed=1, perturb=0.0)
+    fv = st.fluidvars
+    for s in range(LSP):
+        fv[..., s] = 1e11 if s < LSP - 1 else 6e11
+        fv[..., 4 * LSP + s] = 1500.0
+    fv[..., LSP:4 * LSP] = 0.0
+    nn, vn1, Tn, E1, Q, g1 = _momentum_inputs(g, 2)
+    Pr, Lo = O.srcs_momentum(g, st, nn, np.zeros_like(vn1), Tn, np.zeros_like(E1), np.zeros_like(Q),
+                             np.zeros_like(g1))
+    assert (Pr == 0).all()
+    assert (Lo > 0).all()
