@@ -1208,9 +1208,9 @@ void ora_compression(const ora_grid* G, double dt, const double* vs1, const doub
 
 // app/main.f90:280-355 with the compression sub-step (main.f90:320-338) between the
 // post-advection clean_param(2) and rhoe2T; otherwise ora_fluid_adv.
-int ora_fluid_adv_compression(const ora_grid* G, double* fluidvars, double* fluidauxvars, const double* J1,
-                              double* vs1i, double* vs2i, double* vs3i, const double* nn, const double* Tn,
-                              double dt, double Teinf, int diffsolvetype) {
+static int fluid_adv_compression_q(const ora_grid* G, double* fluidvars, double* fluidauxvars, const double* J1,
+                                   double* vs1i, double* vs2i, double* vs3i, const double* nn, const double* Tn,
+                                   double dt, double Teinf, int diffsolvetype, std::vector<double>& Q) {
   Ix X(G);
   double* ns = fluidvars;
   double* vs1 = fluidvars + LSP * X.ng;
@@ -1237,7 +1237,7 @@ int ora_fluid_adv_compression(const ora_grid* G, double* fluidvars, double* flui
   ora_rhov12v1(G, ns, rhovs1, vs1);
   ora_clean_param(G, 1, ns);
   ora_clean_param(G, 2, vs1);
-  std::vector<double> Q((size_t)LSP * X.nc());
+  Q.assign((size_t)LSP * X.nc(), 0.0);
   ora_vnricht_artvisc(G, ns, vs1, Q.data());
   ora_halo_fluidvars(G, ns, rhovs1, rhoes, vs2, vs3);
   ora_rk2_global_boundary_allspec(G, vs1, vs2, vs3);
@@ -1713,6 +1713,52 @@ void ora_energy_source_loss_solve(const ora_grid* G, double dt, double* Pr, cons
       Ts[s * X.ng + k] = fmax_f(T, 100.0);
     }
   }
+}
+
+int ora_fluid_adv_compression(const ora_grid* G, double* fluidvars, double* fluidauxvars, const double* J1,
+                              double* vs1i, double* vs2i, double* vs3i, const double* nn, const double* Tn,
+                              double dt, double Teinf, int diffsolvetype) {
+  std::vector<double> Q;
+  return fluid_adv_compression_q(G, fluidvars, fluidauxvars, J1, vs1i, vs2i, vs3i, nn, Tn, dt, Teinf, diffsolvetype,
+                                 Q);
+}
+
+// app/main.f90:280-381 fluid_adv in full on a single rank: the step with compression, then
+// (after the ionization, whose rates Prionize (lx1,lx2,lx3,lsp-1) and Qeionize (lx1,lx2,lx3)
+// are inputs here) set_global_boundaries, the energy, momentum and mass source/loss solves
+// (libgemini.f90:1154-1200) with the compression step's Q, and clean_param(3), (2), (1).
+// nn: interior (lx1,lx2,lx3,>=6) neutral densities O, N2, O2, H, N, NO (the diffusion reads
+// the first three); vn1..3, Tn, alt, g1: interior; E1, J1: ghosted.
+int ora_fluid_adv_full(const ora_grid* G, double* fluidvars, double* fluidauxvars, const double* E1,
+                       const double* J1, double* vs1i, double* vs2i, double* vs3i, const double* nn,
+                       const double* vn1, const double* vn2, const double* vn3, const double* Tn, const double* alt,
+                       const double* g1, const double* Prionize, const double* Qeionize, double dt, double Teinf,
+                       int diffsolvetype) {
+  Ix X(G);
+  std::vector<double> Q;
+  const int rc = fluid_adv_compression_q(G, fluidvars, fluidauxvars, J1, vs1i, vs2i, vs3i, nn, Tn, dt, Teinf,
+                                         diffsolvetype, Q);
+  if (rc != 0) return rc;
+  double* ns = fluidvars;
+  double* vs1 = fluidvars + LSP * X.ng;
+  double* vs2 = fluidvars + 2 * LSP * X.ng;
+  double* vs3 = fluidvars + 3 * LSP * X.ng;
+  double* Ts = fluidvars + 4 * LSP * X.ng;
+  double* rhovs1 = fluidauxvars;
+  double* rhoes = fluidauxvars + LSP * X.ng;
+  const long long nc = X.nc();
+  std::vector<double> Pr((size_t)LSP * nc), Lo((size_t)LSP * nc), Prion(Prionize, Prionize + (LSP - 1) * nc);
+  ora_set_global_boundaries_allspec(G, ns, rhovs1, vs1, vs2, vs3, rhoes, vs1i, LSP);
+  ora_srcs_energy(G, nn, vn1, vn2, vn3, Tn, ns, vs1, vs2, vs3, Ts, Pr.data(), Lo.data());
+  ora_energy_source_loss_solve(G, dt, Pr.data(), Lo.data(), Qeionize, rhoes, Ts, ns);
+  ora_srcs_momentum(G, nn, vn1, Tn, ns, vs1, vs2, vs3, Ts, E1, Q.data(), alt, g1, Pr.data(), Lo.data());
+  ora_momentum_source_loss_solve(G, dt, Pr.data(), Lo.data(), ns, rhovs1, vs1);
+  ora_srcs_continuity(G, nn, vn1, vn2, vn3, Tn, ns, vs1, vs2, vs3, Ts, Pr.data(), Lo.data());
+  ora_mass_source_loss_solve(G, dt, Pr.data(), Lo.data(), Prion.data(), ns);
+  ora_clean_param(G, 3, Ts);
+  ora_clean_param(G, 2, vs1);
+  ora_clean_param(G, 1, ns);
+  return 0;
 }
 
 void ora_set_diffusion_solver(int mode) { g_diff_solver = mode; }

@@ -86,6 +86,8 @@ def lib():
         L.ora_srcs_continuity.argtypes = [G, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
         L.ora_srcs_energy.argtypes = [G, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
         L.ora_srcs_momentum.argtypes = [G] + [_D] * 14
+        L.ora_fluid_adv_full.argtypes = [G] + [_D] * 16 + [ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.ora_fluid_adv_full.restype = ctypes.c_int
         L.ora_mass_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D]
         L.ora_momentum_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
         L.ora_energy_source_loss_solve.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D, _D]
@@ -317,6 +319,24 @@ def fluid_adv_compression(grid, st, dt: float, diffsolvetype: int = 2):
                                          float(st.Teinf), int(diffsolvetype))
     if rc != 0:
         raise ValueError(f"ora_fluid_adv_compression failed: {rc}")
+
+
+def fluid_adv_full(grid, st, dt: float, nn, vn1, vn2, vn3, g1, Prionize, Qeionize, diffsolvetype: int = 2):
+    """fluid_adv in full (app/main.f90:280-381, single rank), in place: the step with
+    compression, then the source/loss sub-step with the given neutral state (nn: interior
+    (lx1, lx2, lx3, >=6) O, N2, O2, H, N, NO; the diffusion reads the first three), gravity g1
+    and ionization rates (Prionize (lx1, lx2, lx3, lsp-1), Qeionize (lx1, lx2, lx3)); Tn is st.Tn,
+    E1 and J1 the state's electrovars."""
+    g = _GridHandle(grid)
+    E1 = np.asfortranarray(st.electrovars[..., 0])
+    J1 = np.asfortranarray(st.electrovars[..., 3])
+    alt = grid.alt[2:-2, 2:-2, 2:-2] if grid.alt.shape[0] == grid.lx1 + 4 else grid.alt
+    arrs = [np.asfortranarray(a, dtype=np.float64) for a in (nn, vn1, vn2, vn3, st.Tn, alt, g1, Prionize, Qeionize)]
+    rc = lib().ora_fluid_adv_full(g.ref, _p(st.fluidvars), _p(st.fluidauxvars), _p(E1), _p(J1), _p(st.vs1i),
+                                  _p(st.vs2i), _p(st.vs3i), *[_p(a) for a in arrs], float(dt), float(st.Teinf),
+                                  int(diffsolvetype))
+    if rc != 0:
+        raise ValueError(f"ora_fluid_adv_full failed: {rc}")
 
 
 def vnricht_artvisc(grid, st):

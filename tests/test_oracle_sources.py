@@ -395,3 +395,48 @@ def test_srcs_momentum_of_a_uniform_plasma_at_rest_is_zero():
                              np.zeros_like(g1))
     assert (Pr == 0).all()
     assert (Lo > 0).all()
+
+
+def test_srcs_energy_balances_at_thermal_equilibrium():
+    """Every species at the neutral temperature and moving with the neutral wind: heat
+    transfer, friction and the electrons' inelastic terms all vanish, so each species'
+    production equals its loss times its energy density."""
+    g = G.dipole_grid(12, 4, 3)
+    st = S.init_state(g, seed=4, perturb=0.2)
+    nn, vn, Tn = _neutrals(g, 4)
+    fv = st.fluidvars
+    I = (slice(2, g.lx1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+    for s in range(LSP):
+        fv[I + (4 * LSP + s,)] = Tn
+        for k in range(3):
+            fv[I + ((1 + k) * LSP + s,)] = vn[k]
+    O.T2rhoe(g, st)
+    Pr, Lo = O.srcs_energy(g, st, nn, *vn, Tn)
+    re = st.fluidauxvars[I + (slice(LSP, 2 * LSP),)]
+    np.testing.assert_allclose(Pr, Lo * re, rtol=1e-12, atol=0)
+    assert (Lo > 0).all()
+
+
+def test_full_step_runs_and_stays_physical():
+    """fluid_adv with compression and the source/loss sub-step (synthetic neutral state and
+    ionization): finite, densities above the floor, temperatures at or above 100 K, and a
+    different state from the step without sources."""
+    g = G.dipole_grid(20, 5, 4)
+    a = S.init_state(g, seed=6, perturb=0.2)
+    b = a.copy()
+    rng = np.random.default_rng(6)
+    shp = (g.lx1, g.lx2, g.lx3)
+    nn = np.asfortranarray(np.concatenate([a.nn, np.stack([10 ** rng.uniform(9, 12, shp) for _ in range(4)], -1)], -1))
+    vn = [np.asfortranarray(rng.uniform(-50, 50, shp)) for _ in range(3)]
+    g1 = np.asfortranarray(np.full(shp, -9.0))
+    Pi = np.asfortranarray(rng.uniform(0, 1e8, shp + (LSP - 1,)))
+    Qe = np.asfortranarray(rng.uniform(0, 1e-12, shp))
+    dt = 0.05
+    O.fluid_adv_full(g, a, dt, nn, *vn, g1, Pi, Qe)
+    O.fluid_adv_compression(g, b, dt)
+    fv = a.fluidvars
+    assert np.isfinite(fv).all() and np.isfinite(a.fluidauxvars[..., :2 * LSP]).all()
+    I = (slice(2, g.lx1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+    assert (fv[I + (slice(0, LSP),)] > 0).all()
+    assert (fv[I + (slice(4 * LSP, 5 * LSP),)] >= 100.0).all()
+    assert not np.array_equal(fv, b.fluidvars)
