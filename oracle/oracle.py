@@ -230,6 +230,19 @@ def sweep(grid, st, dim: int, which: str, dt: float):
     lib().ora_sweep_allspec(g.ref, dim, b[key], _p(vsi), float(dt), frank, lsp)
 
 
+def advec1D_MC_curv(f, v1i, dt: float, dx, dxi, ha1, ha2i, h1i):
+    """advec.f90:384-435 on one line of lx cells: f, ha1 (lx+4, index -1..lx+2); v1i, ha2i,
+    h1i (lx+1 faces); dx (lx+3, 0..lx+2); dxi (lx).  Returns the updated line (lx+4)."""
+    f, v1i, dx, dxi, ha1, ha2i, h1i = (np.ascontiguousarray(a, dtype=np.float64)
+                                       for a in (f, v1i, dx, dxi, ha1, ha2i, h1i))
+    lx = f.size - 4
+    assert v1i.size == lx + 1 and dx.size == lx + 3 and dxi.size == lx and ha1.size == lx + 4
+    out = np.empty_like(f)
+    lib().ora_advec1D_MC_curv(_p(f), _p(v1i), float(dt), _p(dx), _p(dxi), _p(ha1), _p(ha2i), _p(h1i), lx,
+                              _p(out))
+    return out
+
+
 def set_global_boundaries(grid, st, lsp: int = LSP):
     g = _GridHandle(grid)
     b = _blocks(st)
