@@ -74,3 +74,36 @@ def test_library_builds_and_exports_header_symbols():
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
     assert _lib.lib().gem_version() >= 1
+
+
+def test_device_abi_rejects_bad_arguments_without_a_gpu():
+    """The device C ABI checks its arguments before any CUDA call: null handles, null
+    buffers and impossible sizes come back as GEM_EINVAL with a message (no exit, no fault),
+    on a machine without a GPU as on one with."""
+    try:
+        build.build()
+    except RuntimeError as e:  # no nvcc in this environment
+        if not os.path.exists(build.LIB):
+            pytest.skip(str(e))
+    L = _lib.lib()
+    EINVAL = 1
+    out = ctypes.c_void_p()
+    desc = _lib.GemGridDesc()
+    desc.lx1, desc.lx2, desc.lx3, desc.gridflag = 0, 4, 4, 0
+    cfg = _lib.GemCfg()
+    cfg.Teinf, cfg.diffsolvetype = 1500.0, 2
+    calls = {
+        "gem_grid_create (null desc)": lambda: L.gem_grid_create(None, ctypes.byref(out)),
+        "gem_grid_create (lx1 = 0)": lambda: L.gem_grid_create(ctypes.byref(desc), ctypes.byref(out)),
+        "gem_work_create": lambda: L.gem_work_create(None, ctypes.byref(out)),
+        "gem_step_adjoint_create": lambda: L.gem_step_adjoint_create(None, ctypes.byref(out)),
+        "gem_fluid_adv_dev": lambda: L.gem_fluid_adv_dev(ctypes.byref(cfg), None, None, None, None, None, None, None),
+        "gem_dt_calc_noalloc_dev": lambda: L.gem_dt_calc_noalloc_dev(None, 0.5, None, None, None),
+        "gem_step_vjp_replay_dev": lambda: L.gem_step_vjp_replay_dev(ctypes.byref(cfg), *([None] * 12)),
+        "gem_step_vjp_finish_dev": lambda: L.gem_step_vjp_finish_dev(ctypes.byref(cfg), *([None] * 10)),
+        "gem_batch_create": lambda: L.gem_batch_create(0, None, None, None, None, None, None, ctypes.byref(out)),
+    }
+    for name, call in calls.items():
+        assert call() == EINVAL, name
+        assert L.gem_last_error().decode(), name
+    assert out.value is None
