@@ -107,3 +107,37 @@ def test_device_abi_rejects_bad_arguments_without_a_gpu():
         assert call() == EINVAL, name
         assert L.gem_last_error().decode(), name
     assert out.value is None
+
+
+_CAPI_PROBE = r"""
+import ctypes, sys
+L = ctypes.CDLL(sys.argv[1])
+PP = ctypes.POINTER(ctypes.c_void_p)
+L.v12rhov1_C.argtypes = [PP, PP]
+L.gem_capi_set_error_mode.argtypes = [ctypes.c_int]
+L.gem_capi_set_error_mode(int(sys.argv[2]))
+fv, fav = ctypes.c_void_p(None), ctypes.c_void_p(None)
+L.v12rhov1_C(ctypes.byref(fv), ctypes.byref(fav))   # no grid bound
+print("returned", L.gem_capi_last_status())
+"""
+
+
+def test_capi_error_behaviour_without_a_gpu():
+    """The reference-named *_C entry points stop the program on error, printing the
+    message and exiting 1 as the reference's error stop does; in record-only mode they return
+    and leave the status to gem_capi_last_status.  Called with no grid bound, they fail before
+    any CUDA call."""
+    import subprocess
+    import sys
+
+    try:
+        build.build()
+    except RuntimeError as e:  # no nvcc in this environment
+        if not os.path.exists(build.LIB):
+            pytest.skip(str(e))
+    r = subprocess.run([sys.executable, "-c", _CAPI_PROBE, build.LIB, "0"], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 1 and "v12rhov1_C" in r.stderr and "returned" not in r.stdout
+    r = subprocess.run([sys.executable, "-c", _CAPI_PROBE, build.LIB, "1"], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0 and "returned 1" in r.stdout
