@@ -141,3 +141,28 @@ def test_capi_error_behaviour_without_a_gpu():
     r = subprocess.run([sys.executable, "-c", _CAPI_PROBE, build.LIB, "1"], capture_output=True, text=True,
                        timeout=120)
     assert r.returncode == 0 and "returned 1" in r.stdout
+
+
+def test_bench_reference_arm_line_without_a_gpu():
+    """bench.py --impl reference times the oracle port on the host cores and prints one JSON
+    line with the contract's keys: impl, the same metric/unit/config as the product arm, a
+    cpu_baseline describing the run with its value equal to the line's, and an e2e block with
+    no host<->device bytes."""
+    import json
+    import subprocess
+    import sys
+
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(here, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0", "--cpu-seconds", "0.5"], capture_output=True, text=True, timeout=600,
+                       cwd=here)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == "fluid Gcell-species-steps/s"
+    assert line["unit"] == "Gcell-species-steps/s" and line["value"] > 0 and line["steps"] == 1
+    assert line["higher_is_better"] is True and line["n_gpus"] == 1
+    assert line["config"]["lx1"] == 384 and line["config"]["lx2"] == 192 and line["config"]["lx3"] == 192
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"] and cb["value"] == line["value"]
+    e2e = line["e2e"]
+    assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
