@@ -19,6 +19,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -84,11 +85,10 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, path: str | None = None):
         self.idx = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv") \
-            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/gemini_b200_clocks_{os.getpid()}.csv"
+        self.path = path or os.path.join(tempfile.gettempdir(), f"gemini_b200_clocks_{os.getpid()}_{gpu_index}.csv")
 
     def start(self):
         try:
@@ -266,7 +266,7 @@ def run_b200(args, world, rank, local):
     if world > 1:
         dist.barrier()
     _lib.check(L.gem_work_phase_timing(ds.work, args.steps))
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(local, args.clocks_csv.format(rank=rank) if args.clocks_csv else None)
     sampler.start()
     time.sleep(0.3)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -303,7 +303,10 @@ def run_b200(args, world, rank, local):
     peak, peak_src = measured_hbm_peak()
     step_bytes = sum(alg[p] for p in PHASES) * 8 * cells
     step_achieved = step_bytes / (ms_max / args.steps / 1e3) / 1e9
-    survey_bytes = 8 * (162 + (0 if unit else 21)) * cells
+    # the same step with each sweep as its own pass: 3 sweeps x (19 fields read + 19 written
+    # + 7 face velocities) + 2 epilogue writes + the diffusion's 25 = 162 doubles per cell,
+    # plus 21 metric doubles on curvilinear grids
+    unfused_bytes = 8 * (162 + (0 if unit else 21)) * cells
 
     # end to end through the host-buffer entry point (state copied in and out each step)
     e2e = None
@@ -364,8 +367,8 @@ def run_b200(args, world, rank, local):
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "step_achieved_GBs": step_achieved, "step_frac": step_achieved / peak,
                      "step_algorithmic_bytes": step_bytes,
-                     "survey_algorithmic_bytes_per_step": survey_bytes,
-                     "survey_frac": survey_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak},
+                     "unfused_algorithmic_bytes_per_step": unfused_bytes,
+                     "unfused_frac": unfused_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak},
         "phases_ms": phase_ms,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -594,6 +597,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--clocks-csv", default=None,
+                    help="keep the nvidia-smi samples of the timed region in this file ({rank} is replaced)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched instances")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instance measurement")
