@@ -1761,6 +1761,23 @@ int ora_fluid_adv_full(const ora_grid* G, double* fluidvars, double* fluidauxvar
   return 0;
 }
 
+// libgemini_mpi.f90:449-482 dt_select with temporal_mpi.f90:26-66 dt_comm on a single rank:
+// the CFL step, clipped so that t + dt does not pass the next GLOW output (when flagglow)
+// and then the next output, floored at 1e-6, and -- from the second iteration -- grown by
+// at most dtscale = 2 (libgemini_mpi.f90:38) over the previous step.  (ora_dt_calc floors
+// first; flooring before and after the clips gives the reference's clip-then-floor.)
+double ora_dt_select(const ora_grid* G, double tcfl, const double* Ts, const double* vs1, const double* vs2,
+                     const double* vs3, double t, double tout, double tglowout, int flagglow, int it,
+                     double dtprev) {
+  double dt = ora_dt_calc(G, tcfl, Ts, vs1, vs2, vs3, nullptr);
+  if (flagglow != 0 && t + dt > tglowout) dt = tglowout - t;
+  if (t + dt > tout) dt = tout - t;
+  dt = fmax_f(dt, 1e-6);
+  const double dtscale = 2;
+  if (it > 1 && dt / dtprev > dtscale) dt = dtscale * dtprev;
+  return dt;
+}
+
 void ora_set_diffusion_solver(int mode) { g_diff_solver = mode; }
 void ora_set_pow_mode(int mode) { g_pow_mode = mode; }
 double ora_pow25(double x) { return pow25(x); }

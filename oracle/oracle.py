@@ -73,6 +73,9 @@ def lib():
         L.ora_energy_diffusion.restype = ctypes.c_int
         L.ora_dt_calc.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, _D]
         L.ora_dt_calc.restype = ctypes.c_double
+        L.ora_dt_select.argtypes = [G, ctypes.c_double, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        L.ora_dt_select.restype = ctypes.c_double
         L.ora_fluid_adv.argtypes = [G, _D, _D, _D, _D, _D, _D, _D, _D, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_int]
         L.ora_fluid_adv.restype = ctypes.c_int
@@ -309,6 +312,16 @@ def dt_calc(grid, st, tcfl: float = 0.5):
     gr = np.zeros(3 * LSP)
     dt = lib().ora_dt_calc(g.ref, float(tcfl), b["Ts"], b["vs1"], b["vs2"], b["vs3"], _p(gr))
     return float(dt), gr.reshape(3, LSP)
+
+
+def dt_select(grid, st, t: float, tout: float, it: int, dtprev: float, tcfl: float = 0.5,
+              tglowout: float = float("inf"), flagglow: int = 0) -> float:
+    """The step's dt as dt_select chooses it (libgemini_mpi.f90:449-482, single rank): the CFL
+    step clipped to the next GLOW / regular output, floored at 1e-6, throttled to at most
+    twice the previous step from iteration 2 on."""
+    g = _GridHandle(grid); b = _blocks(st)
+    return float(lib().ora_dt_select(g.ref, float(tcfl), b["Ts"], b["vs1"], b["vs2"], b["vs3"], float(t),
+                                     float(tout), float(tglowout), int(flagglow), int(it), float(dtprev)))
 
 
 def fluid_adv(grid, st, dt: float, diffsolvetype: int = 2):
