@@ -78,6 +78,9 @@ _SIGS = [
     ("gem_step_vjp_replay_dev", ctypes.c_int, [ctypes.POINTER(GemCfg)] + [_VP] * 12),
     ("gem_step_vjp_backward_dev", ctypes.c_int, [ctypes.POINTER(GemCfg)] + [_VP] * 22),
     ("gem_step_vjp_finish_dev", ctypes.c_int, [ctypes.POINTER(GemCfg)] + [_VP] * 10),
+    ("gem_vnricht_artvisc_dev", ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    ("gem_rk2_global_boundary_allspec_dev", ctypes.c_int, [_VP, _VP, _VP]),
+    ("gem_compression_dev", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     ("gem_fluid_adv_dev", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("gem_fluid_adv_host", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _D, _VP]),
     ("gem_check_finite", ctypes.c_int, [_VP, _VP, _VP, ctypes.POINTER(ctypes.c_longlong), _VP]),

@@ -214,6 +214,31 @@ def interface_vels_allspec(ds: DeviceState, lsp: int = LSP, stream=None):
     _lib.check(_lib.lib().gem_interface_vels_allspec_dev(ds.g, _ptr(ds.fluidvars), ds.work, lsp, _stream(stream)))
 
 
+# ---- the compression sub-step (app/main.f90:320-338) -----------------------------------------
+
+def vnricht_artvisc(ds: DeviceState, Q=None, stream=None):
+    """VNRicht_artvisc (multifluid.f90:237-268): Q (lx1, lx2, lx3, lsp), Fortran order, as a
+    flat float64 device tensor; Q is allocated when not given."""
+    torch = _torch()
+    lx1, lx2, lx3 = ds.dgrid.dims
+    if Q is None:
+        Q = torch.empty(lx1 * lx2 * lx3 * LSP, dtype=torch.float64, device=ds.fluidvars.device)
+    _lib.check(_lib.lib().gem_vnricht_artvisc_dev(ds.g, _ptr(ds.fluidvars), _ptr(Q), _stream(stream)))
+    return Q
+
+
+def rk2_global_boundary_allspec(ds: DeviceState, stream=None):
+    """RK2_global_boundary (sources_mpi.f90:68-111) of vs1, vs2, vs3 on a single rank."""
+    _lib.check(_lib.lib().gem_rk2_global_boundary_allspec_dev(ds.g, _ptr(ds.fluidvars), _stream(stream)))
+
+
+def compression(ds: DeviceState, Q, dt, stream=None):
+    """compression (multifluid.f90:274-302): rhoes updated in place with Q from vnricht_artvisc."""
+    d = ds._dt(dt)
+    _lib.check(_lib.lib().gem_compression_dev(ds.g, _ptr(ds.fluidvars), _ptr(ds.fluidauxvars), _ptr(Q), _ptr(d),
+                                              _stream(stream)))
+
+
 def _sweep(ds: DeviceState, dim: int, which: int, dt, stream=None):
     d = ds._dt(dt)
     _lib.check(_lib.lib().gem_sweep_allspec_dev(ds.g, dim, which, _ptr(ds.fluidvars), _ptr(ds.fluidauxvars),

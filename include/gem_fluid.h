@@ -120,6 +120,24 @@ int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem
 /* temporal.f90:12-49 cflcalc; writes *maxcfl_out (device) */
 int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, const double* dt,
                    double* maxcfl_out, void* stream);
+/* The compression sub-step (app/main.f90:320-338) as the reference's separate calls, after
+ * the post-advection clean_param(1), (2):
+ *   gem_vnricht_artvisc_dev: multifluid.f90:237-268 VNRicht_artvisc (libgemini.f90
+ *     VNRicht_artvisc_C), xicon = 3; writes Q (device, interior (lx1, lx2, lx3, LSP),
+ *     column-major; 0 for the electrons) from ns and vs1 as they stand, x1 ghosts included;
+ *   gem_rk2_global_boundary_allspec_dev: sources_mpi.f90:68-111 RK2_global_boundary on a
+ *     single rank (RK2_global_boundary_allspec_C): zero-order-hold velocity ghosts, x1 (vs1)
+ *     then x2 and, unless x3 is periodic, x3 (vs1, vs2, vs3); on periodic grids call
+ *     gem_halo_fluidvars_dev first, as the reference does;
+ *   gem_compression_dev: multifluid.f90:274-302 compression (compression_C) with
+ *     calculus/div.f90:110-200 div3D: the half- and full-step update of rhoes (fluidauxvars
+ *     block 2) from each species' velocity divergence and Q; dt is a device pointer.
+ * Results equal the reference restatement bit for bit (IEEE divisions, the reference's
+ * operation order). */
+int gem_vnricht_artvisc_dev(const gem_grid* g, const double* fluidvars, double* Q, void* stream);
+int gem_rk2_global_boundary_allspec_dev(const gem_grid* g, double* fluidvars, void* stream);
+int gem_compression_dev(const gem_grid* g, const double* fluidvars, double* fluidauxvars, const double* Q,
+                        const double* dt, void* stream);
 
 /* ---- differentiable path (no counterpart in the reference) ------------------------
  * Vector-Jacobian product of gem_energy_diffusion_dev: given Ybar, the cotangent of the
