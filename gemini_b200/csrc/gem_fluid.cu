@@ -1049,3 +1049,4 @@ int gem_check_finite(const gem_grid* g, const double* fluidvars, gem_work* w, lo
 #include "gem_batch.cuh"
 #include "gem_adjoint.cuh"
 #include "gem_compression_dev.cuh"
+#include "gem_sources_dev.cuh"

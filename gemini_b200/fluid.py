@@ -239,6 +239,30 @@ def compression(ds: DeviceState, Q, dt, stream=None):
                                               _stream(stream)))
 
 
+# ---- the source/loss solves (multifluid.f90:474-549) -----------------------------------------
+# Pr, Lo, Prprecip, Qeprecip: flat float64 device tensors holding the interior arrays
+# (lx1, lx2, lx3, species) in column-major order; Pr is updated in place where the reference
+# updates it.
+
+def energy_source_loss_solve(ds: DeviceState, dt, Pr, Lo, Qeprecip, stream=None):
+    d = ds._dt(dt)
+    _lib.check(_lib.lib().gem_energy_source_loss_solve_dev(ds.g, _ptr(d), _ptr(Pr), _ptr(Lo), _ptr(Qeprecip),
+                                                           _ptr(ds.fluidvars), _ptr(ds.fluidauxvars),
+                                                           _stream(stream)))
+
+
+def momentum_source_loss_solve(ds: DeviceState, dt, Pr, Lo, stream=None):
+    d = ds._dt(dt)
+    _lib.check(_lib.lib().gem_momentum_source_loss_solve_dev(ds.g, _ptr(d), _ptr(Pr), _ptr(Lo), _ptr(ds.fluidvars),
+                                                             _ptr(ds.fluidauxvars), _stream(stream)))
+
+
+def mass_source_loss_solve(ds: DeviceState, dt, Pr, Lo, Prprecip, stream=None):
+    d = ds._dt(dt)
+    _lib.check(_lib.lib().gem_mass_source_loss_solve_dev(ds.g, _ptr(d), _ptr(Pr), _ptr(Lo), _ptr(Prprecip),
+                                                         _ptr(ds.fluidvars), _stream(stream)))
+
+
 def _sweep(ds: DeviceState, dim: int, which: int, dt, stream=None):
     d = ds._dt(dt)
     _lib.check(_lib.lib().gem_sweep_allspec_dev(ds.g, dim, which, _ptr(ds.fluidvars), _ptr(ds.fluidauxvars),

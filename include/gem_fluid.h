@@ -139,6 +139,28 @@ int gem_rk2_global_boundary_allspec_dev(const gem_grid* g, double* fluidvars, vo
 int gem_compression_dev(const gem_grid* g, const double* fluidvars, double* fluidauxvars, const double* Q,
                         const double* dt, void* stream);
 
+/* The source/loss solves of the source sub-step (libgemini.f90:1154-1200, after the rates):
+ * Pr, Lo: device, interior (lx1, lx2, lx3, LSP), column-major, as the rate routines leave
+ * them; dt: device pointer.  The exponential time differencing step
+ * (calculus.in.f90:174-196 ETD_uncoupled) of each species at interior cells, then the
+ * derived fields over every cell, ghosts included:
+ *   gem_energy_source_loss_solve_dev: multifluid.f90:474-495 energy_source_loss_solve
+ *     (inside source_loss_energy_C): Pr(:,:,:,LSP) += Qeprecip (interior (lx1, lx2, lx3)),
+ *     in place as the reference does; rhoes (fluidauxvars block 2) stepped; Ts formed;
+ *   gem_momentum_source_loss_solve_dev: multifluid.f90:500-528 momentum_source_loss_solve
+ *     (inside source_loss_momentum_C): ion rhovs1 stepped, vs1 formed, electron vs1 and
+ *     rhovs1 from the ion current;
+ *   gem_mass_source_loss_solve_dev: multifluid.f90:532-549 mass_source_loss_solve (inside
+ *     source_loss_mass_C): Pr(:,:,:,1:LSP-1) += Prprecip (interior, LSP-1 species), in
+ *     place; ion ns stepped; electron ns = sum of the ion densities.
+ * Results equal the reference restatement up to the device's double exp (within 1 ulp). */
+int gem_energy_source_loss_solve_dev(const gem_grid* g, const double* dt, double* Pr, const double* Lo,
+                                     const double* Qeprecip, double* fluidvars, double* fluidauxvars, void* stream);
+int gem_momentum_source_loss_solve_dev(const gem_grid* g, const double* dt, const double* Pr, const double* Lo,
+                                       double* fluidvars, double* fluidauxvars, void* stream);
+int gem_mass_source_loss_solve_dev(const gem_grid* g, const double* dt, double* Pr, const double* Lo,
+                                   const double* Prprecip, double* fluidvars, void* stream);
+
 /* ---- differentiable path (no counterpart in the reference) ------------------------
  * Vector-Jacobian product of gem_energy_diffusion_dev: given Ybar, the cotangent of the
  * diffusion's output temperature (ghosted 7-species block; interior rows used, including
