@@ -263,6 +263,40 @@ def mass_source_loss_solve(ds: DeviceState, dt, Pr, Lo, Prprecip, stream=None):
                                                          _ptr(ds.fluidvars), _stream(stream)))
 
 
+# ---- the production/loss rates (sources.f90) --------------------------------------------------
+# nn, vn1..3, Tn, alt, g1, Q: flat float64 device tensors of the interior arrays in column-major
+# order; each returns (Pr, Lo), flat (lx1, lx2, lx3, lsp) device tensors.
+
+def _rate_out(ds: DeviceState):
+    torch = _torch()
+    lx1, lx2, lx3 = ds.dgrid.dims
+    mk = lambda: torch.empty(lx1 * lx2 * lx3 * LSP, dtype=torch.float64, device=ds.fluidvars.device)
+    return mk(), mk()
+
+
+def srcs_continuity(ds: DeviceState, nn, vn1, vn2, vn3, Tn, stream=None):
+    Pr, Lo = _rate_out(ds)
+    _lib.check(_lib.lib().gem_srcs_continuity_dev(ds.g, _ptr(nn), _ptr(vn1), _ptr(vn2), _ptr(vn3), _ptr(Tn),
+                                                  _ptr(ds.fluidvars), _ptr(Pr), _ptr(Lo), _stream(stream)))
+    return Pr, Lo
+
+
+def srcs_energy(ds: DeviceState, nn, vn1, vn2, vn3, Tn, stream=None):
+    Pr, Lo = _rate_out(ds)
+    _lib.check(_lib.lib().gem_srcs_energy_dev(ds.g, _ptr(nn), _ptr(vn1), _ptr(vn2), _ptr(vn3), _ptr(Tn),
+                                              _ptr(ds.fluidvars), _ptr(Pr), _ptr(Lo), _stream(stream)))
+    return Pr, Lo
+
+
+def srcs_momentum(ds: DeviceState, nn, vn1, Tn, Q, alt, g1, stream=None):
+    """E1 is read from the state's electrovars (block 1)."""
+    Pr, Lo = _rate_out(ds)
+    _lib.check(_lib.lib().gem_srcs_momentum_dev(ds.g, _ptr(nn), _ptr(vn1), _ptr(Tn), _ptr(ds.fluidvars),
+                                                _ptr(ds.electrovars), _ptr(Q), _ptr(alt), _ptr(g1), _ptr(Pr),
+                                                _ptr(Lo), _stream(stream)))
+    return Pr, Lo
+
+
 def _sweep(ds: DeviceState, dim: int, which: int, dt, stream=None):
     d = ds._dt(dt)
     _lib.check(_lib.lib().gem_sweep_allspec_dev(ds.g, dim, which, _ptr(ds.fluidvars), _ptr(ds.fluidauxvars),

@@ -161,6 +161,27 @@ int gem_momentum_source_loss_solve_dev(const gem_grid* g, const double* dt, cons
 int gem_mass_source_loss_solve_dev(const gem_grid* g, const double* dt, double* Pr, const double* Lo,
                                    const double* Prprecip, double* fluidvars, void* stream);
 
+/* The production and loss rates (sources.f90) the solves above take, into Pr and Lo (device,
+ * interior (lx1, lx2, lx3, LSP), column-major; every element written).  nn: device, interior
+ * (lx1, lx2, lx3, species), neutral densities O, N2, O2, H, N, NO (the energy and momentum
+ * rates read the first four); vn1, vn2, vn3, Tn, alt, g1: device, interior (lx1, lx2, lx3);
+ * fluidvars and electrovars: the device state blocks (ns, vs1, vs2, vs3, Ts and E1 read).
+ *   gem_srcs_continuity_dev: sources.f90:18-276 srcsContinuity (inside source_loss_mass_C);
+ *   gem_srcs_energy_dev: sources.f90:396-485 srcsEnergy with collisions.f90:58-159 (inside
+ *     source_loss_energy_C);
+ *   gem_srcs_momentum_dev: sources.f90:279-393 srcsMomentum_curv on a single rank (inside
+ *     source_loss_momentum_C), with Q from gem_vnricht_artvisc_dev; needs lx1 >= 2.
+ * Every expression follows the reference's operation order; the device's pow, exp, log,
+ * log10, erf, tanh and sin stand in for the C library's. */
+int gem_srcs_continuity_dev(const gem_grid* g, const double* nn, const double* vn1, const double* vn2,
+                            const double* vn3, const double* Tn, const double* fluidvars, double* Pr, double* Lo,
+                            void* stream);
+int gem_srcs_energy_dev(const gem_grid* g, const double* nn, const double* vn1, const double* vn2, const double* vn3,
+                        const double* Tn, const double* fluidvars, double* Pr, double* Lo, void* stream);
+int gem_srcs_momentum_dev(const gem_grid* g, const double* nn, const double* vn1, const double* Tn,
+                          const double* fluidvars, const double* electrovars, const double* Q, const double* alt,
+                          const double* g1, double* Pr, double* Lo, void* stream);
+
 /* ---- differentiable path (no counterpart in the reference) ------------------------
  * Vector-Jacobian product of gem_energy_diffusion_dev: given Ybar, the cotangent of the
  * diffusion's output temperature (ghosted 7-species block; interior rows used, including

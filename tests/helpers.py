@@ -65,3 +65,28 @@ def assert_identical(gpu, ref, what=""):
             i = tuple(bad[0])
             raise AssertionError(f"{what}: {name} differs at {len(bad)} cells, first {i}: "
                                  f"gpu {a[i]!r} oracle {b[i]!r}")
+
+
+def rate_inputs(g, seed):
+    """A state and neutral inputs for the production/loss rates: drifts of up to 3 km/s (both
+    branches of the Coulomb Phi), interior ion temperatures 150..40000 K (every piece of the
+    reaction-rate fits), electrons 150..10000 K, neutral densities 1e10..1e16, E1 ghosted, Q and g1 interior."""
+    rng = np.random.default_rng(seed)
+    shp = (g.lx1, g.lx2, g.lx3)
+    st = S.init_state(g, seed=seed, perturb=0.3)
+    fv = st.fluidvars
+    I = (slice(2, g.lx1 + 2), slice(2, g.lx2 + 2), slice(2, g.lx3 + 2))
+    for k in (1, 2, 3):  # drifts large enough for the W >= 0.1 branch and high Teff fits
+        fv[..., k * LSP:(k + 1) * LSP] = rng.uniform(-3000, 3000, fv[..., 0:LSP].shape)
+    fv[I + (slice(4 * LSP, 5 * LSP),)] = rng.uniform(150, 40000, fv[I + (slice(0, LSP),)].shape)
+    # electrons up to 10000 K: far above that the reference's N2 vibrational-loss fit overflows
+    # exp (argument ~700 at 33000 K over a 200 K neutral gas)
+    fv[I + (5 * LSP - 1,)] = rng.uniform(150, 10000, fv[I + (0,)].shape)
+    nn = np.asfortranarray(np.stack([10 ** rng.uniform(10, 16, shp) for _ in range(7)], axis=-1))
+    vn = [np.asfortranarray(rng.uniform(-100, 100, shp)) for _ in range(3)]
+    Tn = np.asfortranarray(rng.uniform(200, 1500, shp))
+    E1 = np.asfortranarray(rng.uniform(-1e-3, 1e-3, (g.lx1 + 4, g.lx2 + 4, g.lx3 + 4)))
+    Q = np.asfortranarray(rng.uniform(0, 1e-12, shp + (LSP,)))
+    g1 = np.asfortranarray(rng.uniform(-9.8, -8.0, shp))
+    alt = g.alt[2:-2, 2:-2, 2:-2] if g.alt.shape[0] == g.lx1 + 4 else g.alt
+    return st, nn, vn, Tn, E1, Q, g1, np.asfortranarray(alt, dtype=np.float64)
