@@ -87,6 +87,10 @@ _SIGS = [
     ("gem_srcs_continuity_dev", ctypes.c_int, [_VP] * 10),
     ("gem_srcs_energy_dev", ctypes.c_int, [_VP] * 10),
     ("gem_srcs_momentum_dev", ctypes.c_int, [_VP] * 12),
+    ("gem_fluid_adv_compression_dev", ctypes.c_int, [ctypes.POINTER(GemCfg)] + [_VP] * 7),
+    ("gem_source_loss_allparams_dev", ctypes.c_int, [_VP] * 11),
+    ("gem_fluid_adv_full_scratch_doubles", ctypes.c_longlong, [_VP]),
+    ("gem_fluid_adv_full_dev", ctypes.c_int, [ctypes.POINTER(GemCfg)] + [_VP] * 9),
     ("gem_fluid_adv_dev", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("gem_fluid_adv_host", ctypes.c_int, [ctypes.POINTER(GemCfg), _VP, _VP, _VP, _VP, _VP, _D, _VP]),
     ("gem_check_finite", ctypes.c_int, [_VP, _VP, _VP, ctypes.POINTER(ctypes.c_longlong), _VP]),

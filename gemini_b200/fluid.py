@@ -297,6 +297,58 @@ def srcs_momentum(ds: DeviceState, nn, vn1, Tn, Q, alt, g1, stream=None):
     return Pr, Lo
 
 
+# ---- fluid_adv in full (app/main.f90:280-381) ---------------------------------------------------
+
+class SourceInputs(ctypes.Structure):
+    """gem_source_inputs: device pointers of the interior neutral state (nn: O, N2, O2, H, N,
+    NO), altitude, gravity and ionization rates the source sub-step reads."""
+    _fields_ = [(n, ctypes.c_void_p) for n in ("nn", "vn1", "vn2", "vn3", "Tn", "alt", "g1", "Prionize", "Qeionize")]
+
+    @classmethod
+    def of(cls, **tensors):
+        s = cls(**{k: t.data_ptr() for k, t in tensors.items()})
+        s._keep = tensors  # the tensors must outlive the launches
+        return s
+
+
+def fluid_adv_compression(cfg: FluidCfg, ds: DeviceState, dt, Q=None, stream=None):
+    """The step with the compression sub-step, as the reference's sequence of routines;
+    returns Q (flat interior (lx1, lx2, lx3, lsp) device tensor) for the source sub-step."""
+    torch = _torch()
+    lx1, lx2, lx3 = ds.dgrid.dims
+    if Q is None:
+        Q = torch.empty(lx1 * lx2 * lx3 * LSP, dtype=torch.float64, device=ds.fluidvars.device)
+    d = ds._dt(dt)
+    c = cfg.c()
+    _lib.check(_lib.lib().gem_fluid_adv_compression_dev(ctypes.byref(c), ds.g, _ptr(ds.fluidvars),
+                                                         _ptr(ds.fluidauxvars), _ptr(ds.electrovars), ds.work,
+                                                         _ptr(Q), _ptr(d), _stream(stream)))
+    return Q
+
+
+def source_loss_allparams(ds: DeviceState, dt, inputs: SourceInputs, Q, stream=None):
+    """The source/loss sub-step (libgemini.f90:1154-1200) after the step with compression."""
+    Pr, Lo = _rate_out(ds)
+    d = ds._dt(dt)
+    _lib.check(_lib.lib().gem_source_loss_allparams_dev(ds.g, _ptr(ds.fluidvars), _ptr(ds.fluidauxvars),
+                                                         _ptr(ds.electrovars), ds.work, ctypes.byref(inputs), _ptr(Q),
+                                                         _ptr(Pr), _ptr(Lo), _ptr(d), _stream(stream)))
+
+
+def fluid_adv_full(cfg: FluidCfg, ds: DeviceState, dt, inputs: SourceInputs, scratch=None, stream=None):
+    """fluid_adv in full on a single rank: the step with compression, then the sources."""
+    torch = _torch()
+    if scratch is None:
+        n = _lib.lib().gem_fluid_adv_full_scratch_doubles(ds.g)
+        scratch = torch.empty(n, dtype=torch.float64, device=ds.fluidvars.device)
+    d = ds._dt(dt)
+    c = cfg.c()
+    _lib.check(_lib.lib().gem_fluid_adv_full_dev(ctypes.byref(c), ds.g, _ptr(ds.fluidvars), _ptr(ds.fluidauxvars),
+                                                  _ptr(ds.electrovars), ds.work, ctypes.byref(inputs), _ptr(scratch),
+                                                  _ptr(d), _stream(stream)))
+    return scratch
+
+
 def _sweep(ds: DeviceState, dim: int, which: int, dt, stream=None):
     d = ds._dt(dt)
     _lib.check(_lib.lib().gem_sweep_allspec_dev(ds.g, dim, which, _ptr(ds.fluidvars), _ptr(ds.fluidauxvars),

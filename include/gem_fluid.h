@@ -182,6 +182,39 @@ int gem_srcs_momentum_dev(const gem_grid* g, const double* nn, const double* vn1
                           const double* fluidvars, const double* electrovars, const double* Q, const double* alt,
                           const double* g1, double* Pr, double* Lo, void* stream);
 
+/* ---- fluid_adv in full on a single rank (app/main.f90:280-381) --------------------
+ * The reference's sequence of the routines above, each a separate launch:
+ *   gem_fluid_adv_compression_dev: the advection (v12rhov1, T2rhoe, boundaries, halo,
+ *     interface velocities, x3/x1/x2 sweeps, rhov12v1, clean_param(1), (2)), the compression
+ *     sub-step (VNRicht_artvisc into Q (device, interior (lx1, lx2, lx3, LSP)), halo,
+ *     RK2_global_boundary, compression, rhoe2T, clean_param(3)) and the diffusion
+ *     (energy_diffusion, clean_param(3), T2rhoe); the diffusion reads nn and Tn from w;
+ *   gem_source_loss_allparams_dev: source_loss_allparams_C's sequence (libgemini.f90
+ *     1154-1200): set_global_boundaries, the energy rates and solve (Qeionize added),
+ *     the momentum rates (with the compression step's Q) and solve, the continuity rates
+ *     and solve (Prionize added), clean_param(3), (2), (1); Pr, Lo: device scratch of
+ *     LSP*lx1*lx2*lx3 doubles each;
+ *   gem_fluid_adv_full_dev: both, with scratch of gem_fluid_adv_full_scratch_doubles(g)
+ *     device doubles (Q, Pr, Lo).
+ * The ionization rates (ionization.f90) are inputs, as the reference's impact_ionization
+ * and photoionization fill Prionize and Qeionize before this sub-step. */
+typedef struct gem_source_inputs {
+  const double* nn;        /* interior (lx1, lx2, lx3, 6): O, N2, O2, H, N, NO */
+  const double *vn1, *vn2, *vn3, *Tn; /* interior neutral winds and temperature */
+  const double *alt, *g1;  /* interior altitude and x1 gravity (meshobj.f90 x%alt, x%g1) */
+  const double* Prionize;  /* interior (lx1, lx2, lx3, LSP-1) ion production */
+  const double* Qeionize;  /* interior (lx1, lx2, lx3) electron heating */
+} gem_source_inputs;
+int gem_fluid_adv_compression_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                                  const double* electrovars, gem_work* w, double* Q, const double* dt, void* stream);
+int gem_source_loss_allparams_dev(const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                                  const double* electrovars, const gem_work* w, const gem_source_inputs* in,
+                                  const double* Q, double* Pr, double* Lo, const double* dt, void* stream);
+long long gem_fluid_adv_full_scratch_doubles(const gem_grid* g);
+int gem_fluid_adv_full_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                           const double* electrovars, gem_work* w, const gem_source_inputs* in, double* scratch,
+                           const double* dt, void* stream);
+
 /* ---- differentiable path (no counterpart in the reference) ------------------------
  * Vector-Jacobian product of gem_energy_diffusion_dev: given Ybar, the cotangent of the
  * diffusion's output temperature (ghosted 7-species block; interior rows used, including

@@ -13,7 +13,18 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libgemini_b200.so")
 
 
+# The sub-steps outside the fused hot path (compression, source/loss rates and solves, the
+# full step composed of them) run after the hot-path tests, so that under -x a failure there
+# stops the run only once the hot path's own results are in.
+LATE_MODULES = ("test_gpu_compression", "test_gpu_sources", "test_gpu_rates", "test_gpu_fullstep")
+
+
 def pytest_collection_modifyitems(config, items):
+    def rank(it):
+        name = it.module.__name__.rsplit(".", 1)[-1] if it.module else ""
+        return LATE_MODULES.index(name) + 1 if name in LATE_MODULES else 0
+
+    items.sort(key=rank)
     try:
         import torch
         have_gpu = torch.cuda.is_available()

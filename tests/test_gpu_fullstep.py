@@ -1,0 +1,100 @@
+"""GPU parity of fluid_adv in full on a single rank (app/main.f90:280-381) through the
+device C ABI against the oracle: the step with the compression sub-step, then the
+source/loss sub-step.
+
+Tolerances, written here:
+  step with compression: 1e-12 relative, as the fused hot-path step (cell-wise for n, T and
+      rho*e, norm-wise per species for the signed fields); its only difference from the
+      oracle is the diffusion's band solve, which the oracle runs in extended precision;
+  full step: 1e-9.  The source sub-step's rates call the device's pow, exp, log, erf, tanh
+      and sin (a few ulp from the C library's), and its ETD update
+      f exp(-L dt) + P/L (1 - exp(-L dt)) amplifies an exp that is one ulp apart by up to
+      1/(L dt) in the production term.  Neutral densities of 1e15..1e17 keep every ion loss
+      rate L dt above ~1e-6 here (checked with the oracle's rates), which bounds that term's
+      difference near 2e-10; the rest of the chain is continuous and adds a few ulp per
+      operation.
+The full step leaves out the parallel-current case: its thermoelectric heating takes the
+electrons past 1e5 K in one CFL step, where the reference's N2 vibrational-loss fit
+overflows exp (the electron energy production is -inf on both sides)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from gemini_b200 import fluid as F
+from gemini_b200 import state as S
+
+from helpers import LSP, cases, state_err
+
+pytestmark = pytest.mark.gpu
+
+CASES = cases()
+IDS = [c[0] for c in CASES]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _exact_dependencies():
+    """The oracle's diffusion with the extended-precision band solve and the correctly
+    rounded T**2.5, as the hot-path parity tests run it."""
+    O.set_exact_dependencies(True)
+    yield
+    O.set_exact_dependencies(False)
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.asfortranarray(a, dtype=np.float64).ravel(order="F").copy()).cuda()
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_step_with_compression_vs_oracle(case):
+    name, g, kw = case
+    st = S.init_state(g, **kw)
+    ds = F.DeviceState.from_host(F.DeviceGrid(g), st.copy())
+    try:
+        ref = st.copy()
+        dt, _ = O.dt_calc(g, ref, 0.5)
+        O.fluid_adv_compression(g, ref, dt)
+        F.fluid_adv_compression(F.FluidCfg(st.Teinf), ds, dt)
+        err = state_err(ds.to_host(st), ref)
+        assert max(err.values()) <= 1e-12, err
+    finally:
+        ds.close()
+
+
+def _source_inputs(g, st, seed):
+    rng = np.random.default_rng(seed)
+    shp = (g.lx1, g.lx2, g.lx3)
+    nn = np.asfortranarray(np.stack([10 ** rng.uniform(15, 17, shp) for _ in range(6)], axis=-1))
+    vn = [np.asfortranarray(rng.uniform(-100, 100, shp)) for _ in range(3)]
+    g1 = np.asfortranarray(rng.uniform(-9.8, -8.0, shp))
+    Pri = np.asfortranarray(rng.uniform(0, 1e6, shp + (LSP - 1,)))
+    Qei = np.asfortranarray(rng.uniform(0, 1e-13, shp))
+    alt = g.alt[2:-2, 2:-2, 2:-2] if g.alt.shape[0] == g.lx1 + 4 else g.alt
+    st.nn = np.asfortranarray(nn[..., :3])  # the diffusion's neutrals: O, N2, O2
+    st.electrovars[..., 0] = rng.uniform(-1e-3, 1e-3, st.electrovars.shape[:3])
+    return nn, vn, g1, Pri, Qei, np.asfortranarray(alt, dtype=np.float64)
+
+
+FULL_CASES = [c for c in CASES if "J1_amp" not in c[2]]
+
+
+@pytest.mark.parametrize("case", FULL_CASES, ids=[c[0] for c in FULL_CASES])
+def test_full_step_vs_oracle(case):
+    name, g, kw = case
+    st = S.init_state(g, **kw)
+    nn, vn, g1, Pri, Qei, alt = _source_inputs(g, st, 51)
+    ds = F.DeviceState.from_host(F.DeviceGrid(g), st.copy())
+    try:
+        ref = st.copy()
+        dt, _ = O.dt_calc(g, ref, 0.5)
+        O.fluid_adv_full(g, ref, dt, nn, *vn, g1, Pri, Qei)
+        inputs = F.SourceInputs.of(nn=_dev(nn), vn1=_dev(vn[0]), vn2=_dev(vn[1]), vn3=_dev(vn[2]), Tn=_dev(st.Tn),
+                                   alt=_dev(alt), g1=_dev(g1), Prionize=_dev(Pri), Qeionize=_dev(Qei))
+        F.fluid_adv_full(F.FluidCfg(st.Teinf), ds, dt, inputs)
+        got = ds.to_host(st)
+        assert np.isfinite(got.fluidvars).all() and np.isfinite(ref.fluidvars).all()
+        err = state_err(got, ref)
+        assert max(err.values()) <= 1e-9, err
+        assert not np.array_equal(got.fluidvars, st.fluidvars)
+    finally:
+        ds.close()
