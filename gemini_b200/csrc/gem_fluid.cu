@@ -1052,3 +1052,4 @@ int gem_check_finite(const gem_grid* g, const double* fluidvars, gem_work* w, lo
 #include "gem_sources_dev.cuh"
 #include "gem_rates_dev.cuh"
 #include "gem_fullstep_dev.cuh"
+#include "gem_clock_dev.cuh"

@@ -211,6 +211,25 @@ int gem_source_loss_allparams_dev(const gem_grid* g, double* fluidvars, double* 
                                   const double* electrovars, const gem_work* w, const gem_source_inputs* in,
                                   const double* Q, double* Pr, double* Lo, const double* dt, void* stream);
 long long gem_fluid_adv_full_scratch_doubles(const gem_grid* g);
+
+/* ---- device-resident time stepping --------------------------------------------------
+ * The simulation clock in device memory, so that a loop of steps keeps dt on the device.
+ * gem_dt_select_dev: libgemini_mpi.f90:450-483 dt_select with temporal_mpi.f90:27-84
+ *   dt_comm on a single rank: the CFL step (gem_dt_calc_dev, into clock->dtcfl), clipped
+ *   so that t + dt passes neither the next GLOW output (cfg->flagglow) nor the next output,
+ *   floored at 1e-6, and for it > 1 grown by at most 2x over the previous step, which *dt
+ *   holds on entry (the reference's intent(inout) dt); writes *dt (device).
+ * gem_clock_advance_dev: after a step, t = t + dt (app/main.f90:233) and it = it + 1.
+ * The output times are the caller's: it sets tout / tglowout when an output is written.
+ * Results equal the reference's arithmetic bit for bit. */
+typedef struct gem_clock {
+  double t, tout, tglowout; /* simulation time, next output, next GLOW output */
+  double dtcfl;             /* the CFL step of the latest selection (written) */
+  long long it;             /* iteration counter (get_it()), 1 on the first step */
+} gem_clock;
+int gem_dt_select_dev(const gem_cfg* cfg, const gem_grid* g, const double* fluidvars, gem_work* w, gem_clock* clock,
+                      double* dt, void* stream);
+int gem_clock_advance_dev(gem_clock* clock, const double* dt, void* stream);
 int gem_fluid_adv_full_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
                            const double* electrovars, gem_work* w, const gem_source_inputs* in, double* scratch,
                            const double* dt, void* stream);

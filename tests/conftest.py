@@ -16,7 +16,8 @@ def pytest_configure(config):
 # The sub-steps outside the fused hot path (compression, source/loss rates and solves, the
 # full step composed of them) run after the hot-path tests, so that under -x a failure there
 # stops the run only once the hot path's own results are in.  test_zz_no_alloc stays last.
-LATE_MODULES = ("test_gpu_compression", "test_gpu_sources", "test_gpu_rates", "test_gpu_fullstep", "test_zz_no_alloc")
+LATE_MODULES = ("test_gpu_clock", "test_gpu_compression", "test_gpu_sources", "test_gpu_rates", "test_gpu_fullstep",
+                "test_zz_no_alloc")
 
 
 def pytest_collection_modifyitems(config, items):
