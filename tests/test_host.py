@@ -102,11 +102,26 @@ def test_device_abi_rejects_bad_arguments_without_a_gpu():
         "gem_step_vjp_replay_dev": lambda: L.gem_step_vjp_replay_dev(ctypes.byref(cfg), *([None] * 12)),
         "gem_step_vjp_finish_dev": lambda: L.gem_step_vjp_finish_dev(ctypes.byref(cfg), *([None] * 10)),
         "gem_batch_create": lambda: L.gem_batch_create(0, None, None, None, None, None, None, ctypes.byref(out)),
+        "gem_vnricht_artvisc_dev": lambda: L.gem_vnricht_artvisc_dev(None, None, None, None),
+        "gem_rk2_global_boundary_allspec_dev": lambda: L.gem_rk2_global_boundary_allspec_dev(None, None, None),
+        "gem_compression_dev": lambda: L.gem_compression_dev(*([None] * 6)),
+        "gem_energy_source_loss_solve_dev": lambda: L.gem_energy_source_loss_solve_dev(*([None] * 8)),
+        "gem_momentum_source_loss_solve_dev": lambda: L.gem_momentum_source_loss_solve_dev(*([None] * 7)),
+        "gem_mass_source_loss_solve_dev": lambda: L.gem_mass_source_loss_solve_dev(*([None] * 7)),
+        "gem_srcs_continuity_dev": lambda: L.gem_srcs_continuity_dev(*([None] * 10)),
+        "gem_srcs_energy_dev": lambda: L.gem_srcs_energy_dev(*([None] * 10)),
+        "gem_srcs_momentum_dev": lambda: L.gem_srcs_momentum_dev(*([None] * 12)),
+        "gem_fluid_adv_compression_dev": lambda: L.gem_fluid_adv_compression_dev(ctypes.byref(cfg), *([None] * 7)),
+        "gem_source_loss_allparams_dev": lambda: L.gem_source_loss_allparams_dev(*([None] * 11)),
+        "gem_fluid_adv_full_dev": lambda: L.gem_fluid_adv_full_dev(ctypes.byref(cfg), *([None] * 9)),
+        "gem_dt_select_dev": lambda: L.gem_dt_select_dev(ctypes.byref(cfg), *([None] * 6)),
+        "gem_clock_advance_dev": lambda: L.gem_clock_advance_dev(None, None, None),
     }
     for name, call in calls.items():
         assert call() == EINVAL, name
         assert L.gem_last_error().decode(), name
     assert out.value is None
+    assert L.gem_fluid_adv_full_scratch_doubles(None) == -1
 
 
 _CAPI_PROBE = r"""
