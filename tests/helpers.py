@@ -90,3 +90,11 @@ def rate_inputs(g, seed):
     g1 = np.asfortranarray(rng.uniform(-9.8, -8.0, shp))
     alt = g.alt[2:-2, 2:-2, 2:-2] if g.alt.shape[0] == g.lx1 + 4 else g.alt
     return st, nn, vn, Tn, E1, Q, g1, np.asfortranarray(alt, dtype=np.float64)
+
+
+def harness_flags():
+    """Extra g++ flags for the host builds of the device kernel bodies (the *_harness.cpp
+    tests), e.g. "-fsanitize=address" to check their index arithmetic for out-of-bounds
+    accesses; taken from GEMINI_HARNESS_CFLAGS."""
+    import os
+    return os.environ.get("GEMINI_HARNESS_CFLAGS", "").split()

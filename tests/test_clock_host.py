@@ -14,6 +14,8 @@ import oracle as O
 from gemini_b200 import grid as G
 from gemini_b200 import state as S
 
+from helpers import harness_flags
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -23,7 +25,7 @@ def harness(tmp_path_factory):
     if not cxx:
         pytest.skip("no g++")
     out = str(tmp_path_factory.mktemp("clock") / "libclock.so")
-    subprocess.check_call([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-o", out,
+    subprocess.check_call([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", *harness_flags(), "-o", out,
                            os.path.join(HERE, "clock_harness.cpp")])
     L = ctypes.CDLL(out)
     d = ctypes.c_double

@@ -14,6 +14,8 @@ import oracle as O
 from gemini_b200 import grid as G
 from gemini_b200 import state as S
 
+from helpers import harness_flags
+
 LSP = 7
 HERE = os.path.dirname(os.path.abspath(__file__))
 _D = ctypes.POINTER(ctypes.c_double)
@@ -30,7 +32,7 @@ def harness(tmp_path_factory):
     if not cxx:
         pytest.skip("no g++")
     out = str(tmp_path_factory.mktemp("src") / "libsrc.so")
-    subprocess.check_call([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-o", out,
+    subprocess.check_call([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", *harness_flags(), "-o", out,
                            os.path.join(HERE, "sources_harness.cpp")])
     L = ctypes.CDLL(out)
     P = ctypes.POINTER(HSView)
