@@ -731,6 +731,7 @@ int gem_step_vjp_finish_dev(const gem_cfg* cfg, const gem_grid* g, gem_work* w, 
   da.Teinf = cfg->Teinf;
   da.Ttop = w->Ttop;
   da.coef = w->dcoef;
+  da.lu = w->lu;
   da.solver = cfg->diffsolvetype;
   da.fused = 1;
   if ((rc = launch_diffusion(g, da, st))) return rc;

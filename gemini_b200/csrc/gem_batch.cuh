@@ -140,6 +140,25 @@ __global__ void __launch_bounds__(128) kb_diffusion(const InstDev* __restrict__ 
   }
 }
 
+// The band-solve diffusion (k_diffusion_lu) over the batch: an item is one block's worth
+// (LU_WPB warp tasks) of an instance; the grid never exceeds the scratch slots, and each
+// resident warp keeps the slot of its (block, warp) for every item it runs.
+template <bool UNIT>
+__global__ void __launch_bounds__(32 * LU_WPB) kb_diffusion_lu(const InstDev* __restrict__ inst,
+                                                              const Item* __restrict__ it, int n, double* lu,
+                                                              long long lu_slot) {
+  const int warp = threadIdx.x >> 5;
+  double* slot = lu + (long long)(blockIdx.x * LU_WPB + warp) * lu_slot;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const Item q = it[w];
+    const DiffArgs& P = inst[q.x].df;
+    const int ncol = P.G.d.lx2 * P.G.d.lx3;
+    const int ntask = ((ncol + 31) / 32) * LSP;
+    const int t = q.y * LU_WPB + warp;
+    if (t < ntask) b_diffusion_lu<UNIT>(P, t, slot);
+  }
+}
+
 }  // namespace gemk
 
 // ---------------------------------------------------------------------------------------
@@ -179,6 +198,8 @@ struct gem_batch {
   cudaGraph_t graph_fixed = nullptr;  // the step with prescribed time steps
   cudaGraphExec_t exec_fixed = nullptr;
   double* d_dt_in = nullptr;  // per-instance prescribed dt (device)
+  double* d_lu = nullptr;     // band-solve scratch shared by the instances' diffusion items
+  long long lu_slot = 0;      // doubles per scratch slot (the longest column's)
   int use_graph = 1;
 };
 
@@ -234,6 +255,10 @@ int launch_grid(gem_batch* b, BatchLaunch& L) {
       GEM_CUDA(cudaFuncSetAttribute(kb_diffusion_coef<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
       return occupancy_grid(kb_diffusion_coef<false>, 128, L.smem, n, sc, &L.grid);
     case BK_DIFF:
+      if (!use_pcr_diffusion()) {  // persistent, at most one block per LU_WPB scratch slots
+        L.grid = (int)std::max<long long>(1, std::min<long long>((long long)n, lu_slots() / LU_WPB));
+        return GEM_OK;
+      }
       // the dynamic shared-memory limit was raised to the largest bucket's size beforehand
       return u ? occupancy_grid(kb_diffusion<true>, 32 * L.wpb, L.smem, n, sc, &L.grid)
                : occupancy_grid(kb_diffusion<false>, 32 * L.wpb, L.smem, n, sc, &L.grid);
@@ -288,12 +313,18 @@ int batch_build_lists(gem_batch* b) {
               add_items(launch_for(k, 0), i, grid_for((long long)d.lx2 * d.lx3 * LSP, 128));
             break;
           case BK_DCOEF: {
+            if (!use_pcr_diffusion()) break;  // the band-solve diffusion forms its coefficients itself
             BatchLaunch& L = launch_for(k, u);
             L.smem = std::max<size_t>(L.smem, (size_t)3 * d.lx1 * sizeof(double));
             add_items(L, i, std::min<long long>((long long)d.lx2 * d.lx3 * LSP, (long long)num_sms() * 16));
             break;
           }
           case BK_DIFF: {
+            if (!use_pcr_diffusion()) {
+              const long long ntask = (((long long)d.lx2 * d.lx3 + 31) / 32) * LSP;
+              add_items(launch_for(k, u), i, (ntask + LU_WPB - 1) / LU_WPB);
+              break;
+            }
             const int Ms = diff_bucket_M(diff_M(g));
             BatchLaunch& L = launch_for(k, u, Ms);
             const size_t per_warp = (size_t)DNA * Ms * 32 * sizeof(double);
@@ -316,7 +347,7 @@ int batch_build_lists(gem_batch* b) {
   if (smem_max[0])
     GEM_CUDA(cudaFuncSetAttribute(kb_diffusion<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max[0]));
   for (auto& L : b->launches) {
-    if (L.kernel == BK_DIFF && (size_t)DNA * L.Mslot * 32 * sizeof(double) > 227 * 1024)
+    if (use_pcr_diffusion() && L.kernel == BK_DIFF && (size_t)DNA * L.Mslot * 32 * sizeof(double) > 227 * 1024)
       return set_err(GEM_EINVAL, "lx1 too long for the on-chip column solver (rows per lane %d)", L.Mslot);
     if (cudaMalloc(&L.d_items, L.items.size() * sizeof(Item)) != cudaSuccess)
       return set_err(GEM_ENOMEM, "cudaMalloc of a batch work list failed");
@@ -381,6 +412,11 @@ int batch_enqueue(gem_batch* b, cudaStream_t st, bool fixed_dt = false) {
         else kb_diffusion_coef<false><<<L.grid, 128, L.smem, st>>>(I, L.d_items, n);
         break;
       case BK_DIFF:
+        if (!use_pcr_diffusion()) {
+          if (u) kb_diffusion_lu<true><<<L.grid, 32 * LU_WPB, 0, st>>>(I, L.d_items, n, b->d_lu, b->lu_slot);
+          else kb_diffusion_lu<false><<<L.grid, 32 * LU_WPB, 0, st>>>(I, L.d_items, n, b->d_lu, b->lu_slot);
+          break;
+        }
         if (u) kb_diffusion<true><<<L.grid, 32 * L.wpb, L.smem, st>>>(I, L.d_items, n, L.Mslot);
         else kb_diffusion<false><<<L.grid, 32 * L.wpb, L.smem, st>>>(I, L.d_items, n, L.Mslot);
         break;
@@ -403,25 +439,33 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
   std::vector<InstDev> h(n);
   gem_batch* b = new gem_batch();
   b->n = n;
+  int lx1_max = 0;
+  for (int i = 0; i < n; ++i)
+    if (grids[i]) lx1_max = std::max(lx1_max, grids[i]->dev.d.lx1);
+  b->lu_slot = lu_slot_doubles(lx1_max);
+  if (cudaMalloc(&b->d_lu, sizeof(double) * lu_slots() * b->lu_slot) != cudaSuccess) {
+    delete b;
+    return set_err(GEM_ENOMEM, "cudaMalloc of the batch's band-solve scratch failed");
+  }
   for (int i = 0; i < n; ++i) {
     const gem_grid* g = grids[i];
     gem_work* w = works[i];
     if (!g || !w || !fluidvars[i] || !fluidauxvars[i] || !electrovars[i]) {
-      delete b;
+      gem_batch_destroy(b);
       return set_err(GEM_EINVAL, "gem_batch_create: instance %d has a null argument", i);
     }
     int rc = check_step(g);
     if (rc) {
-      delete b;
+      gem_batch_destroy(b);
       return set_err(rc, "gem_batch_create: instance %d: %s", i, g_err.c_str());
     }
     if (cfgs[i].diffsolvetype != 1 && cfgs[i].diffsolvetype != 2) {
-      delete b;
+      gem_batch_destroy(b);
       return set_err(GEM_EINVAL, "gem_batch_create: instance %d: diffsolvetype %d (1 or 2)", i,
                      cfgs[i].diffsolvetype);
     }
     if (w->lx1 != g->dev.d.lx1 || w->lx2 != g->dev.d.lx2 || w->lx3 != g->dev.d.lx3) {
-      delete b;
+      gem_batch_destroy(b);
       return set_err(GEM_EINVAL, "gem_batch_create: instance %d: work and grid sizes differ", i);
     }
     const int M = diff_M(g);
@@ -443,6 +487,9 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
     I.df.Teinf = cfgs[i].Teinf;
     I.df.Ttop = w->Ttop;
     I.df.coef = w->dcoef;
+    I.df.lu = b->d_lu;
+    I.df.lu_slot = b->lu_slot;
+    I.df.x3fast = (!g->dev.unit && g->dev.c3 == 0) ? 1 : 0;
     I.df.solver = cfgs[i].diffsolvetype;
     I.df.M = M;
     I.df.Mslot = diff_bucket_M(M);  // the slot size of the instance's diffusion launch
@@ -454,7 +501,7 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
   }
   int rc = GEM_OK;
   if (cudaMalloc(&b->d_inst, sizeof(InstDev) * n) != cudaSuccess) {
-    delete b;
+    gem_batch_destroy(b);
     return set_err(GEM_ENOMEM, "cudaMalloc of the batch instance table failed");
   }
   if (cudaMemcpy(b->d_inst, h.data(), sizeof(InstDev) * n, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -477,6 +524,7 @@ int gem_batch_destroy(gem_batch* b) {
     if (L.d_items) cudaFree(L.d_items);
   if (b->d_inst) cudaFree(b->d_inst);
   if (b->d_dt_in) cudaFree(b->d_dt_in);
+  if (b->d_lu) cudaFree(b->d_lu);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   delete b;
   return GEM_OK;

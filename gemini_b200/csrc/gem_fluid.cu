@@ -95,6 +95,7 @@ struct gem_work {
   double *vs1i, *vs2i, *vs3i, *nn, *Tn, *dt;
   double* Ttop;             // per-column exospheric temperature (lx2*lx3), or null for Teinf
   double* dcoef;            // diffusion coefficients C, D, B per interior cell (DCOEF_N * nc)
+  double* lu;               // band-solve scratch of k_diffusion_lu (lu_slots() slots of lx1 rows)
   unsigned long long* acc;  // 32 slots: CFL maxima / counters
   long long nf1, nf2, nf3;
   // device staging of the host blocks for gem_fluid_adv_host
@@ -193,7 +194,53 @@ int launch_ghost_fill(const gem_grid* g, Blocks B, const double* vs1i, int lsp, 
   return GEM_OK;
 }
 
+// Resident warps per SM of k_diffusion_lu, which is also the number of its scratch slots
+// per SM: the occupancy limit of the launch, at most LU_MAX_WARPS_PER_SM.
+constexpr int LU_MAX_WARPS_PER_SM = 16;
+int lu_warps_per_sm() {
+  static int wps = 0;
+  if (!wps) {
+    int a = 0, b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_diffusion_lu<true>, 32 * LU_WPB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_diffusion_lu<false>, 32 * LU_WPB, 0);
+    int w = std::min(a, b) * LU_WPB;
+    if (const char* e = getenv("GEM_LU_WARPS_PER_SM")) w = std::min(w, std::max(LU_WPB, atoi(e)));
+    wps = std::max(LU_WPB, std::min(w, LU_MAX_WARPS_PER_SM));
+  }
+  return wps;
+}
+long long lu_slots() { return (long long)num_sms() * lu_warps_per_sm(); }
+long long lu_slot_doubles(int lx1) { return (long long)lx1 * 4 * 32; }
+
+bool use_pcr_diffusion() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("GEM_DIFFUSION");
+    v = (e && strcmp(e, "pcr") == 0) ? 1 : 0;
+  }
+  return v == 1;
+}
+
+int launch_diffusion_lu(const gem_grid* g, DiffArgs a, cudaStream_t st) {
+  const Dims& d = g->dev.d;
+  if (!a.lu) return set_err(GEM_EINVAL, "diffusion without a band-solve scratch");
+  a.lu_slot = lu_slot_doubles(d.lx1);
+  a.x3fast = (!g->dev.unit && g->dev.c3 == 0) ? 1 : 0;
+  const long long ncol = (long long)d.lx2 * d.lx3;
+  const long long ntask = ((ncol + 31) / 32) * LSP;
+  long long nblk = (ntask + LU_WPB - 1) / LU_WPB;
+  const long long cap = lu_slots() / LU_WPB;
+  if (nblk > cap) nblk = cap;
+  if (g->dev.unit)
+    k_diffusion_lu<true><<<(unsigned)nblk, 32 * LU_WPB, 0, st>>>(a);
+  else
+    k_diffusion_lu<false><<<(unsigned)nblk, 32 * LU_WPB, 0, st>>>(a);
+  GEM_LAUNCHED("k_diffusion_lu");
+  return GEM_OK;
+}
+
 int launch_diffusion(const gem_grid* g, DiffArgs a, cudaStream_t st) {
+  if (!use_pcr_diffusion()) return launch_diffusion_lu(g, a, st);
   const Dims& d = g->dev.d;
   const int M = std::max(2, (d.lx1 + 31) / 32);
   const size_t per_warp = (size_t)DNA * M * 32 * sizeof(double);
@@ -564,6 +611,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
   w->acc = nullptr;
   w->Ttop = nullptr;
   w->dcoef = nullptr;
+  w->lu = nullptr;
   w->F = w->A = w->E = nullptr;
   w->nF = w->nA = w->nE = 0;
   w->lx1 = d.lx1;
@@ -583,7 +631,8 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
             {(void**)&w->Tn, sizeof(double) * nc},
             {(void**)&w->dt, sizeof(double) * 4},
             {(void**)&w->acc, sizeof(unsigned long long) * 32},
-            {(void**)&w->dcoef, sizeof(double) * nc * DCOEF_N}};
+            {(void**)&w->dcoef, sizeof(double) * nc * DCOEF_N},
+            {(void**)&w->lu, sizeof(double) * lu_slots() * lu_slot_doubles(d.lx1)}};
   for (auto& a : al) {
     if (cudaMalloc(a.p, a.bytes) != cudaSuccess) {
       gem_work_destroy(w);
@@ -602,7 +651,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
 int gem_work_destroy(gem_work* w) {
   if (!w) return GEM_OK;
   for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);
-  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop, w->dcoef};
+  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop, w->dcoef, w->lu};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete w;
@@ -758,6 +807,7 @@ int gem_energy_diffusion_dev(const gem_cfg* cfg, const gem_grid* g, double* flui
   a.Teinf = cfg->Teinf;
   a.Ttop = w->Ttop;
   a.coef = w->dcoef;
+  a.lu = w->lu;
   a.solver = cfg->diffsolvetype;
   a.fused = 0;
   int rc = launch_diffusion(g, a, S(stream));
@@ -950,6 +1000,7 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
   d.Teinf = cfg->Teinf;
   d.Ttop = w->Ttop;
   d.coef = w->dcoef;
+  d.lu = w->lu;
   d.solver = cfg->diffsolvetype;
   d.fused = 1;
   w->timer.record(6, st);

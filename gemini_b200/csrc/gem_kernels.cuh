@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "gem_diffusion_lu.cuh"
+
 namespace gemk {
 
 constexpr int LSP = 7;
@@ -1326,6 +1328,9 @@ struct DiffArgs {
   int Mslot;   // rows per lane that each warp's shared-memory slot is sized for (>= M)
   int fused;   // 1: clean_param(3) + T2rhoe folded into the store
   double* coef;  // per-cell C (7 species), D (7), B (electrons): written by k_diffusion_coef
+  double* lu;          // band-solve scratch of k_diffusion_lu (one slot per resident warp)
+  long long lu_slot;   // doubles per slot (>= lx1 * 4 * 32)
+  int x3fast;          // column order of k_diffusion_lu: x3 fastest (x3-invariant metrics)
 };
 
 // Coefficient scratch layout (interior cells q = ci(i1,i2,i3), nc of them): the per-row
@@ -1907,6 +1912,143 @@ __device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
 template <bool UNIT>
 __global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
   b_diffusion<UNIT>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+}
+
+// ======================================================================================
+// 7a. The diffusion with the reference's band solve (gem_diffusion_lu.cuh): one thread per
+//     (x1 column, species), a warp = 32 columns of one species.  Columns are enumerated x3
+//     fastest when the metric tables do not vary along x3 (the warp's metric loads are then
+//     one broadcast address), else x2 fastest.  Warp tasks run electrons first (their rows
+//     cost more).  Each resident warp owns a scratch slot of lx1 rows x 4 doubles x 32 lanes.
+// ======================================================================================
+constexpr int LU_WPB = 4;  // warps per block
+
+// column accessor of one thread (gemd::lu_column)
+template <bool UNIT>
+struct LuAccDev {
+  const double* Tc;  // Ts(s) + m0: [i] = cell i of the column (ghosted block)
+  const double* nc;  // ns(s) + m0
+  const double *h1, *h2, *h3, *yh1, *ha1, *yha1;  // cell metric tables + column offset
+  const double *n1, *n2, *n3;                     // neutral densities + (interior offset - 1)
+  const double* J1c;                              // J1 + m0
+  Line1D L;
+  double* sc;  // this lane's scratch: row i, slot k at sc[((i-1)*4 + k)*32]
+  __device__ __forceinline__ double T(int i) const { return Tc[i]; }
+  __device__ __forceinline__ double n(int i) const { return __ldg(nc + i); }
+  __device__ __forceinline__ void metrics(int i, double& a1, double& a2, double& a3, double& y1, double& ha,
+                                          double& yha) const {
+    a1 = __ldg(h1 + i);
+    a2 = __ldg(h2 + i);
+    a3 = __ldg(h3 + i);
+    y1 = __ldg(yh1 + i);
+    ha = __ldg(ha1 + i);
+    yha = __ldg(yha1 + i);
+  }
+  __device__ __forceinline__ void neutrals(int i, double& a, double& b, double& c, double& j) const {
+    a = __ldg(n1 + i);
+    b = __ldg(n2 + i);
+    c = __ldg(n3 + i);
+    j = __ldg(J1c + i);
+  }
+  __device__ __forceinline__ double dx(int i) const { return __ldg(L.dx + i); }
+  __device__ __forceinline__ double ydx(int i) const { return __ldg(L.ydx + i); }
+  __device__ __forceinline__ double dxi(int i) const { return __ldg(L.dxi + i - 1); }
+  __device__ __forceinline__ double ydxi(int i) const { return __ldg(L.ydxi + i - 1); }
+  __device__ __forceinline__ double dxs(int i) const { return __ldg(L.dxs + i); }
+  __device__ __forceinline__ double ydxs(int i) const { return __ldg(L.ydxs + i); }
+  __device__ __forceinline__ double& S(int i, int k) const { return sc[((i - 1) * 4 + k) * 32]; }
+};
+
+// One warp task: 32 columns of one species.  slot = this warp's scratch slot (lane 0).
+template <bool UNIT>
+__device__ __forceinline__ void b_diffusion_lu(const DiffArgs& P, int task, double* slot) {
+  const GridDev& G = P.G;
+  const Dims d = G.d;
+  const int n = d.lx1;
+  const int lane = threadIdx.x & 31;
+  const int ncol = d.lx2 * d.lx3;
+  const int tps = (ncol + 31) / 32;
+  const int s = LSP - 1 - task / tps;
+  const int col = (task % tps) * 32 + lane;
+  if (col >= ncol) return;
+  int i2, i3;
+  if (P.x3fast) {
+    i3 = col % d.lx3 + 1;
+    i2 = col / d.lx3 + 1;
+  } else {
+    i2 = col % d.lx2 + 1;
+    i3 = col / d.lx2 + 1;
+  }
+  const long long m0 = gi(d, 0, i2, i3);
+  const long long mm0 = cmi(G, 0, i2, i3);
+  const long long q0 = ci(d, 1, i2, i3) - 1;
+  const long long nc = nci(d);
+  LuAccDev<UNIT> a;
+  a.Tc = P.B.Ts(s) + m0;
+  a.nc = P.B.ns(s) + m0;
+  a.h1 = G.h1 + mm0;
+  a.h2 = G.h2 + mm0;
+  a.h3 = G.h3 + mm0;
+  a.yh1 = G.yh1 + mm0;
+  a.ha1 = G.ha1_0 + mm0;
+  a.yha1 = G.yha1_0 + mm0;
+  a.n1 = P.nn + q0;
+  a.n2 = P.nn + nc + q0;
+  a.n3 = P.nn + 2 * nc + q0;
+  a.J1c = P.J1 + m0;
+  a.L = G.L[0];
+  a.sc = slot + lane;
+  // Dirichlet values (diffusion.f90:54-79): the exospheric side takes Teinf or the column's value
+  const double tn1 = __ldg(P.Tn + ci(d, 1, i2, i3)), tnl = __ldg(P.Tn + ci(d, n, i2, i3));
+  const double tinf = P.Ttop ? __ldg(P.Ttop + (i2 - 1) + (long long)d.lx2 * (i3 - 1)) : P.Teinf;
+  gemd::LuK k;
+  k.n = n;
+  k.s = s;
+  k.dt = *P.dtp;
+  if (G.gridflag == 0) {
+    k.tmin = tn1;
+    k.tmax = tnl;
+  } else if (G.gridflag == 1) {
+    k.tmin = tinf;
+    k.tmax = tnl;
+  } else {
+    k.tmin = tn1;
+    k.tmax = tinf;
+  }
+  k.c0 = (c_gammas[s] - 1.0) / KB;
+  k.tcoef = (s < LSP - 1) ? c_tcoef[s] : 0.0;
+  double* Tout = P.B.Ts(s) + m0;
+  // max(T,100) (multifluid.f90:340); fused: clean_param(3) null cells and T2rhoe
+  auto store = [&](int i, double x) {
+    double T = fmax_f(x, 100.0);
+    if (P.fused) {
+      if (is_null(G, i, i2, i3)) T = 100;
+      Tout[i] = T;
+      P.B.re(s)[m0 + i] = conv_re(__ldg(a.nc + i), T, s);
+    } else {
+      Tout[i] = T;
+    }
+  };
+  if (s == LSP - 1)
+    gemd::lu_column<UNIT, true>(a, k, P.solver, store);
+  else
+    gemd::lu_column<UNIT, false>(a, k, P.solver, store);
+  if (!P.fused) {
+    Tout[0] = fmax_f(k.tmin, 100.0);
+    Tout[n + 1] = fmax_f(k.tmax, 100.0);
+  }
+}
+
+// plain launch: persistent warps over the warp tasks; scratch slot = the global warp index
+template <bool UNIT>
+__global__ void __launch_bounds__(32 * LU_WPB) k_diffusion_lu(DiffArgs P) {
+  const int warp = threadIdx.x >> 5;
+  const int gw = blockIdx.x * LU_WPB + warp;
+  const int nw = gridDim.x * LU_WPB;
+  const int ncol = P.G.d.lx2 * P.G.d.lx3;
+  const int ntask = ((ncol + 31) / 32) * LSP;
+  double* slot = P.lu + (long long)gw * P.lu_slot;
+  for (int t = gw; t < ntask; t += nw) b_diffusion_lu<UNIT>(P, t, slot);
 }
 
 

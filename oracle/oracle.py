@@ -147,6 +147,14 @@ def set_exact_dependencies(on: bool) -> None:
     set_pow_mode(1 if on else 0)
 
 
+def set_device_semantics(on: bool) -> None:
+    """The reference's arithmetic as the device reproduces it: the restated LAPACK band solve
+    (solver 0) with the correctly rounded T**2.5 (pow mode 1).  Off: the defaults (LAPACK,
+    C-library pow)."""
+    set_diffusion_solver(0)
+    set_pow_mode(1 if on else 0)
+
+
 def pow25(x: float) -> float:
     return float(lib().ora_pow25(float(x)))
 

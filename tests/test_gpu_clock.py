@@ -20,9 +20,9 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module", autouse=True)
 def _exact_dependencies():
-    O.set_exact_dependencies(True)
+    O.set_device_semantics(True)
     yield
-    O.set_exact_dependencies(False)
+    O.set_device_semantics(False)
 
 
 def _clock(t, tout, tglowout, it):

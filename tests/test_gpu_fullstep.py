@@ -33,11 +33,11 @@ IDS = [c[0] for c in CASES]
 
 @pytest.fixture(scope="module", autouse=True)
 def _exact_dependencies():
-    """The oracle's diffusion with the extended-precision band solve and the correctly
-    rounded T**2.5, as the hot-path parity tests run it."""
-    O.set_exact_dependencies(True)
+    """The oracle's diffusion with the restated LAPACK band solve and the correctly rounded
+    T**2.5, as the hot-path parity tests run it."""
+    O.set_device_semantics(True)
     yield
-    O.set_exact_dependencies(False)
+    O.set_device_semantics(False)
 
 
 def _dev(a):

@@ -1,10 +1,12 @@
 """GPU parity: every reference routine on the device against the CPU oracle.
 
-Advection, ghost fill, interface velocities, conversions and clean_param are restated
-with the reference's operation order and no FMA, so they must match bit for bit.  The
-diffusion is checked against the oracle's extended-precision solve of the reference's
-discrete system (tolerance 1e-12 relative), and the fused step over several steps at
-1e-12 relative (cell-wise for n, T, rho*e; norm-wise per species for the signed fields).
+Advection, ghost fill, interface velocities, conversions, clean_param and dt_calc are
+restated with the reference's operation order and no FMA.  The diffusion forms its band
+systems in the reference's order and factors/solves them in LAPACK dgbsv's order
+(dgbtf2 partial pivoting, dgbtrs/dtbsv), so every routine and the fused step must match the
+oracle bit for bit.  The oracle runs its restated LAPACK solve with the correctly rounded
+T**2.5 (the device's one departure from the reference's C-library pow; the spread that a
+one-ulp change of pow causes is measured in test_gpu_parity_sizes.py).
 """
 import numpy as np
 import pytest
@@ -13,23 +15,19 @@ import oracle as O
 from gemini_b200 import fluid as F
 from gemini_b200 import state as S
 
-from helpers import LSP, assert_identical, cases, randomize_interface_vels, rel_err_block, state_err
+from helpers import assert_identical, cases, randomize_interface_vels
 
 pytestmark = pytest.mark.gpu
 
 CASES = cases()
 IDS = [c[0] for c in CASES]
-TOL = 1e-12
 
 
 @pytest.fixture(scope="module", autouse=True)
-def _exact_dependencies():
-    """Run the oracle with the extended-precision band solve and the correctly rounded
-    T**2.5: the two third-party pieces (LAPACK dgbsv, libm pow) whose own results vary
-    between builds by more than 1e-12 in stiff columns (test_oracle.py measures that)."""
-    O.set_exact_dependencies(True)
+def _device_semantics():
+    O.set_device_semantics(True)
     yield
-    O.set_exact_dependencies(False)
+    O.set_device_semantics(False)
 
 
 def _setup(case, seed_iv=11):
@@ -112,17 +110,16 @@ def test_dt_calc_and_maxcfl_exact(case):
 
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 @pytest.mark.parametrize("solver", [2, 1])
-def test_energy_diffusion(case, solver):
+@pytest.mark.parametrize("dtscale", [1.0, 30.0])
+def test_energy_diffusion_exact(case, solver, dtscale):
+    """energy_diffusion bit for bit, at the CFL step and at a 30x stiffer one (pivots on
+    the Dirichlet rows and inside the columns)."""
     g, st, dg, ds = _setup(case)
     dt, _ = O.dt_calc(g, st, 0.5)
+    dt *= dtscale
     O.energy_diffusion(g, st, dt, solver)
     F.energy_diffusion(F.FluidCfg(st.Teinf, solver), ds, dt)
-    got = ds.to_host(st)
-    e = rel_err_block(got.Ts, st.Ts, set())
-    assert e <= TOL, f"Ts relative error {e:.3e}"
-    # everything but Ts untouched
-    mask = np.ones(got.fluidvars.shape[-1], bool); mask[4 * LSP:] = False
-    assert np.array_equal(got.fluidvars[..., mask], st.fluidvars[..., mask])
+    assert_identical(ds.to_host(st), st, f"energy_diffusion solver {solver}")
 
 
 @pytest.mark.parametrize("case", CASES, ids=IDS)
@@ -148,6 +145,7 @@ def test_fused_step_equals_reference_order(case):
 
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_fused_steps_vs_oracle(case):
+    """dt_calc + the fused step, five times: every dt and the whole state bit for bit."""
     name, g, kw = case
     st = S.init_state(g, **kw)
     dg = F.DeviceGrid(g)
@@ -158,28 +156,24 @@ def test_fused_steps_vs_oracle(case):
     dts_ref = O.run_steps(g, ref, nsteps)
     for k in range(nsteps):
         dt = F.dt_calc(ds, 0.5)
-        assert float(dt.item()) == pytest.approx(dts_ref[k], rel=1e-12)
+        assert float(dt.item()) == dts_ref[k]
         F.fluid_adv(cfg, ds, dt)
-    got = ds.to_host(st)
-    err = state_err(got, ref)
-    assert max(err.values()) <= TOL, err
+    assert_identical(ds.to_host(st), ref, f"{name}: {nsteps} fused steps")
     assert F.check_finite(ds) == 0
 
 
-def test_single_step_advection_bits_match():
-    """One fused step from identical inputs: every cell outside the temperature / energy
-    arrays (which carry the diffusion's reordered arithmetic) is bit-identical."""
-    name, g, kw = CASES[0]
+@pytest.mark.parametrize("solver", [2, 1])
+def test_single_step_bits_match(solver):
+    """One fused step from identical inputs, both diffusion solvers: the whole state."""
+    name, g, kw = CASES[4]
     st = S.init_state(g, **kw)
     dg = F.DeviceGrid(g)
     ds = F.DeviceState.from_host(dg, st.copy())
     ref = st.copy()
     dt, _ = O.dt_calc(g, ref, 0.5)
-    O.fluid_adv(g, ref, dt)
-    F.fluid_adv(F.FluidCfg(st.Teinf), ds, dt)
-    got = ds.to_host(st)
-    assert np.array_equal(got.fluidvars[..., :4 * LSP], ref.fluidvars[..., :4 * LSP])
-    assert np.array_equal(got.fluidauxvars[..., :LSP], ref.fluidauxvars[..., :LSP])
+    O.fluid_adv(g, ref, dt, solver)
+    F.fluid_adv(F.FluidCfg(st.Teinf, solver), ds, dt)
+    assert_identical(ds.to_host(st), ref, "one fused step")
 
 
 def test_host_entry_point_matches_device():
