@@ -450,7 +450,7 @@ def run_batched(args, world, rank):
         "sequential_plain_ms_per_step": ms_s / seq_steps,
         "launches_per_step": launches, "work_items_per_step": items,
         "graph": "one CUDA graph per step (replayed)", "instances_on_rank0": len(mine),
-        "autotune": {"params": {("grid_pct" if k == 2 else "diff_warps" if k == 1 else str(k)): v
+        "autotune": {"params": {("grid_pct" if k == 2 else "diff_blocks" if k == 1 else str(k)): v
                                 for k, v in tuned["params"].items()},
                      "cached": tuned["cached"],
                      "trials_ms": [round(t["ms_per_step"], 3) for t in tuned["trials"]]},

@@ -5,8 +5,8 @@ schedule); they change how the (instance, block) work items are laid onto the GP
 
 * ``GRID_PCT``: persistent grid as a percentage of the occupancy limit, or 0 for one block
   per work item (the hardware block scheduler balances the items);
-* ``DIFF_WARPS``: columns (warps) per diffusion block, which trades shared memory per block
-  against blocks per SM.
+* ``DIFF_BLOCKS``: resident diffusion blocks per SM (each four warps, each warp solving 32
+  columns): fewer blocks leave the SMs to the other phases' tails, more hide more latency.
 
 ``tune(batch)`` times each candidate with CUDA events over a few steps (after one warm-up
 step, which also captures the graph) and keeps the fastest; results are cached in a JSON
@@ -23,11 +23,11 @@ import os
 from . import batch as BT
 
 CANDIDATES = [
-    {BT.GRID_PCT: 0, BT.DIFF_WARPS: 4},
-    {BT.GRID_PCT: 100, BT.DIFF_WARPS: 4},
-    {BT.GRID_PCT: 200, BT.DIFF_WARPS: 4},
-    {BT.GRID_PCT: 0, BT.DIFF_WARPS: 2},
-    {BT.GRID_PCT: 0, BT.DIFF_WARPS: 3},
+    {BT.GRID_PCT: 0, BT.DIFF_BLOCKS: 4},
+    {BT.GRID_PCT: 100, BT.DIFF_BLOCKS: 4},
+    {BT.GRID_PCT: 200, BT.DIFF_BLOCKS: 4},
+    {BT.GRID_PCT: 0, BT.DIFF_BLOCKS: 2},
+    {BT.GRID_PCT: 0, BT.DIFF_BLOCKS: 3},
 ]
 
 
@@ -44,7 +44,8 @@ def signature(batch: BT.Batch) -> str:
     shapes = sorted((dg.grid.lx1, dg.grid.lx2, dg.grid.lx3, int(bool(dg.grid.unit_metrics)))
                     for dg, _, _ in batch.instances)
     dev = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
-    return hashlib.sha1(json.dumps([dev, shapes]).encode()).hexdigest()
+    # "diff_blocks": the tunables' meaning (a cache written for other tunables does not apply)
+    return hashlib.sha1(json.dumps(["diff_blocks", dev, shapes]).encode()).hexdigest()
 
 
 def _load() -> dict:

@@ -18,7 +18,7 @@ import ctypes
 from . import _lib
 from .fluid import DeviceGrid, DeviceState, FluidCfg, _stream
 
-USE_GRAPH, DIFF_WARPS, GRID_PCT = 0, 1, 2
+USE_GRAPH, DIFF_BLOCKS, GRID_PCT = 0, 1, 2
 
 
 class Batch:

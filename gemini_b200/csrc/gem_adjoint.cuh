@@ -730,7 +730,6 @@ int gem_step_vjp_finish_dev(const gem_cfg* cfg, const gem_grid* g, gem_work* w, 
   da.dtp = dt;
   da.Teinf = cfg->Teinf;
   da.Ttop = w->Ttop;
-  da.coef = w->dcoef;
   da.lu = w->lu;
   da.solver = cfg->diffsolvetype;
   da.fused = 1;

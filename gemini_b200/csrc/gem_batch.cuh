@@ -14,7 +14,7 @@ namespace gemk {
 // Everything a batched block needs about its instance (device copy, one per instance).
 struct InstDev {
   SweepArgs sw;  // fused-sweep arguments (grid, blocks, vs1i, dt)
-  DiffArgs df;   // fused-diffusion arguments (Mslot = the batch's slot size)
+  DiffArgs df;   // fused-diffusion arguments
   unsigned long long* acc;
   double tcfl;
 };
@@ -118,33 +118,11 @@ __global__ void __launch_bounds__(128) kb_clean_vel_edges(const InstDev* __restr
   }
 }
 
-template <bool UNIT>
-__global__ void __launch_bounds__(128) kb_diffusion_coef(const InstDev* __restrict__ inst, const Item* __restrict__ it,
-                                                        int n) {
-  for (int w = blockIdx.x; w < n; w += gridDim.x) {
-    const Item q = it[w];
-    b_diffusion_coef<UNIT>(inst[q.x].df, VB{q.y, q.z, q.w});
-  }
-}
-
-// one launch per (metric variant, rows-per-lane bucket); every instance of the launch
-// uses the bucket's slot size Mslot (>= its own M)
-template <bool UNIT>
-__global__ void __launch_bounds__(128) kb_diffusion(const InstDev* __restrict__ inst, const Item* __restrict__ it, int n,
-                                                   int Mslot) {
-  for (int w = blockIdx.x; w < n; w += gridDim.x) {
-    const Item q = it[w];
-    const InstDev& I = inst[q.x];
-    (void)Mslot;  // I.df.Mslot holds the instance's bucket slot size (set on the host)
-    b_diffusion<UNIT>(I.df, VB{q.y, q.z, q.w});
-  }
-}
-
 // The band-solve diffusion (k_diffusion_lu) over the batch: an item is one block's worth
 // (LU_WPB warp tasks) of an instance; the grid never exceeds the scratch slots, and each
 // resident warp keeps the slot of its (block, warp) for every item it runs.
 template <bool UNIT>
-__global__ void __launch_bounds__(32 * LU_WPB) kb_diffusion_lu(const InstDev* __restrict__ inst,
+__global__ void __launch_bounds__(32 * LU_WPB, GEM_LU_MINB) kb_diffusion_lu(const InstDev* __restrict__ inst,
                                                               const Item* __restrict__ it, int n, double* lu,
                                                               long long lu_slot) {
   const int warp = threadIdx.x >> 5;
@@ -166,17 +144,13 @@ __global__ void __launch_bounds__(32 * LU_WPB) kb_diffusion_lu(const InstDev* __
 // ---------------------------------------------------------------------------------------
 namespace {
 
-// One launch of the batched step: a phase, its variant (metric variant; for the diffusion
-// also the rows-per-lane bucket) and the work items of the instances it covers.
-enum BatchKernel {
-  BK_DT = 0, BK_GX1, BK_GX2, BK_GX3, BK_SW3, BK_SW1, BK_SW2, BK_EPI, BK_CVE, BK_DCOEF, BK_DIFF, BK_N
-};
+// One launch of the batched step: a phase, its metric variant and the work items of the
+// instances it covers.
+enum BatchKernel { BK_DT = 0, BK_GX1, BK_GX2, BK_GX3, BK_SW3, BK_SW1, BK_SW2, BK_EPI, BK_CVE, BK_DIFF, BK_N };
 
 struct BatchLaunch {
   int kernel = 0;
   int unit = 0;
-  int Mslot = 0, wpb = 0;  // diffusion only
-  size_t smem = 0;
   int grid = 0;
   std::vector<Item> items;
   Item* d_items = nullptr;
@@ -190,7 +164,7 @@ struct gem_batch {
   std::vector<gem_work*> works;
   InstDev* d_inst = nullptr;
   std::vector<BatchLaunch> launches;  // in step order
-  int wpb_max = 4;
+  int diff_blocks = LU_MINB_DEFAULT;  // diffusion blocks per SM (each LU_WPB warps)
   int per_sm_scale = 100;  // percent of the occupancy-limited persistent grid
   cudaStream_t cap_stream = nullptr;
   cudaGraph_t graph = nullptr;
@@ -204,10 +178,6 @@ struct gem_batch {
 };
 
 namespace {
-
-int diff_M(const gem_grid* g) { return std::max(2, (g->dev.d.lx1 + 31) / 32); }
-// rows-per-lane buckets: instances share a launch (and a slot size) within a bucket
-int diff_bucket_M(int M) { return M <= 4 ? 4 : M <= 8 ? 8 : M <= 12 ? 12 : M <= 16 ? 16 : ((M + 7) / 8) * 8; }
 
 void add_items(BatchLaunch& L, int idx, long long nbx, int nby = 1) {
   for (int by = 0; by < nby; ++by)
@@ -247,21 +217,11 @@ int launch_grid(gem_batch* b, BatchLaunch& L) {
                           : occupancy_grid(kb_sweep_march<2, false>, 32 * LSP, 0, n, sc, &L.grid);
     case BK_EPI: return occupancy_grid(kb_ghost_epilogue, 256, 0, n, sc, &L.grid);
     case BK_CVE: return occupancy_grid(kb_clean_vel_edges, 128, 0, n, sc, &L.grid);
-    case BK_DCOEF:
-      if (u) {
-        GEM_CUDA(cudaFuncSetAttribute(kb_diffusion_coef<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
-        return occupancy_grid(kb_diffusion_coef<true>, 128, L.smem, n, sc, &L.grid);
-      }
-      GEM_CUDA(cudaFuncSetAttribute(kb_diffusion_coef<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
-      return occupancy_grid(kb_diffusion_coef<false>, 128, L.smem, n, sc, &L.grid);
-    case BK_DIFF:
-      if (!use_pcr_diffusion()) {  // persistent, at most one block per LU_WPB scratch slots
-        L.grid = (int)std::max<long long>(1, std::min<long long>((long long)n, lu_slots() / LU_WPB));
-        return GEM_OK;
-      }
-      // the dynamic shared-memory limit was raised to the largest bucket's size beforehand
-      return u ? occupancy_grid(kb_diffusion<true>, 32 * L.wpb, L.smem, n, sc, &L.grid)
-               : occupancy_grid(kb_diffusion<false>, 32 * L.wpb, L.smem, n, sc, &L.grid);
+    case BK_DIFF: {  // persistent, never more blocks than the scratch has slots for
+      const long long cap = std::min<long long>((long long)num_sms() * b->diff_blocks, lu_slots() / LU_WPB);
+      L.grid = (int)std::max<long long>(1, std::min<long long>((long long)n, cap));
+      return GEM_OK;
+    }
   }
   return set_err(GEM_EINVAL, "unknown batched kernel %d", L.kernel);
 }
@@ -275,13 +235,12 @@ int batch_build_lists(gem_batch* b) {
   for (int i = 0; i < b->n; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(),
                    [&](int x, int y) { return b->grids[x]->dev.d.ng > b->grids[y]->dev.d.ng; });
-  auto launch_for = [&](int kernel, int unit, int Mslot = 0) -> BatchLaunch& {
+  auto launch_for = [&](int kernel, int unit) -> BatchLaunch& {
     for (auto& L : b->launches)
-      if (L.kernel == kernel && L.unit == unit && L.Mslot == Mslot) return L;
+      if (L.kernel == kernel && L.unit == unit) return L;
     BatchLaunch L;
     L.kernel = kernel;
     L.unit = unit;
-    L.Mslot = Mslot;
     b->launches.push_back(L);
     return b->launches.back();
   };
@@ -292,8 +251,7 @@ int batch_build_lists(gem_batch* b) {
         const gem_grid* g = b->grids[i];
         const Dims& d = g->dev.d;
         const bool unit = g->dev.unit != 0;
-        const bool variant = (k == BK_DT || k == BK_SW3 || k == BK_SW1 || k == BK_SW2 || k == BK_DCOEF ||
-                              k == BK_DIFF);
+        const bool variant = (k == BK_DT || k == BK_SW3 || k == BK_SW1 || k == BK_SW2 || k == BK_DIFF);
         if (variant && unit != (u == 1)) continue;
         if (!variant && u == 0) continue;  // unsplit phases: once
         const int gx13 = (d.lx1 + 31) / 32;
@@ -312,43 +270,16 @@ int batch_build_lists(gem_batch* b) {
             if (g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1))
               add_items(launch_for(k, 0), i, grid_for((long long)d.lx2 * d.lx3 * LSP, 128));
             break;
-          case BK_DCOEF: {
-            if (!use_pcr_diffusion()) break;  // the band-solve diffusion forms its coefficients itself
-            BatchLaunch& L = launch_for(k, u);
-            L.smem = std::max<size_t>(L.smem, (size_t)3 * d.lx1 * sizeof(double));
-            add_items(L, i, std::min<long long>((long long)d.lx2 * d.lx3 * LSP, (long long)num_sms() * 16));
-            break;
-          }
           case BK_DIFF: {
-            if (!use_pcr_diffusion()) {
-              const long long ntask = (((long long)d.lx2 * d.lx3 + 31) / 32) * LSP;
-              add_items(launch_for(k, u), i, (ntask + LU_WPB - 1) / LU_WPB);
-              break;
-            }
-            const int Ms = diff_bucket_M(diff_M(g));
-            BatchLaunch& L = launch_for(k, u, Ms);
-            const size_t per_warp = (size_t)DNA * Ms * 32 * sizeof(double);
-            L.wpb = (int)std::max<size_t>(1, std::min<size_t>((size_t)b->wpb_max, (227 * 1024) / per_warp));
-            L.smem = per_warp * L.wpb;
-            const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
-            add_items(L, i, std::min<long long>((ncs + L.wpb - 1) / L.wpb, (long long)num_sms() * 2));
+            const long long ntask = (((long long)d.lx2 * d.lx3 + 31) / 32) * LSP;
+            add_items(launch_for(k, u), i, (ntask + LU_WPB - 1) / LU_WPB);
             break;
           }
         }
       }
     }
   }
-  // one function attribute per kernel variant: the largest shared memory of its launches
-  size_t smem_max[2] = {0, 0};
-  for (const auto& L : b->launches)
-    if (L.kernel == BK_DIFF) smem_max[L.unit ? 1 : 0] = std::max(smem_max[L.unit ? 1 : 0], L.smem);
-  if (smem_max[1])
-    GEM_CUDA(cudaFuncSetAttribute(kb_diffusion<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max[1]));
-  if (smem_max[0])
-    GEM_CUDA(cudaFuncSetAttribute(kb_diffusion<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max[0]));
   for (auto& L : b->launches) {
-    if (use_pcr_diffusion() && L.kernel == BK_DIFF && (size_t)DNA * L.Mslot * 32 * sizeof(double) > 227 * 1024)
-      return set_err(GEM_EINVAL, "lx1 too long for the on-chip column solver (rows per lane %d)", L.Mslot);
     if (cudaMalloc(&L.d_items, L.items.size() * sizeof(Item)) != cudaSuccess)
       return set_err(GEM_ENOMEM, "cudaMalloc of a batch work list failed");
     GEM_CUDA(cudaMemcpy(L.d_items, L.items.data(), L.items.size() * sizeof(Item), cudaMemcpyHostToDevice));
@@ -407,18 +338,9 @@ int batch_enqueue(gem_batch* b, cudaStream_t st, bool fixed_dt = false) {
         break;
       case BK_EPI: kb_ghost_epilogue<<<L.grid, 256, 0, st>>>(I, L.d_items, n); break;
       case BK_CVE: kb_clean_vel_edges<<<L.grid, 128, 0, st>>>(I, L.d_items, n); break;
-      case BK_DCOEF:
-        if (u) kb_diffusion_coef<true><<<L.grid, 128, L.smem, st>>>(I, L.d_items, n);
-        else kb_diffusion_coef<false><<<L.grid, 128, L.smem, st>>>(I, L.d_items, n);
-        break;
       case BK_DIFF:
-        if (!use_pcr_diffusion()) {
-          if (u) kb_diffusion_lu<true><<<L.grid, 32 * LU_WPB, 0, st>>>(I, L.d_items, n, b->d_lu, b->lu_slot);
-          else kb_diffusion_lu<false><<<L.grid, 32 * LU_WPB, 0, st>>>(I, L.d_items, n, b->d_lu, b->lu_slot);
-          break;
-        }
-        if (u) kb_diffusion<true><<<L.grid, 32 * L.wpb, L.smem, st>>>(I, L.d_items, n, L.Mslot);
-        else kb_diffusion<false><<<L.grid, 32 * L.wpb, L.smem, st>>>(I, L.d_items, n, L.Mslot);
+        if (u) kb_diffusion_lu<true><<<L.grid, 32 * LU_WPB, 0, st>>>(I, L.d_items, n, b->d_lu, b->lu_slot);
+        else kb_diffusion_lu<false><<<L.grid, 32 * LU_WPB, 0, st>>>(I, L.d_items, n, b->d_lu, b->lu_slot);
         break;
     }
   }
@@ -468,7 +390,6 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
       gem_batch_destroy(b);
       return set_err(GEM_EINVAL, "gem_batch_create: instance %d: work and grid sizes differ", i);
     }
-    const int M = diff_M(g);
     InstDev& I = h[i];
     std::memset(&I, 0, sizeof(I));
     I.sw.G = g->dev;
@@ -486,13 +407,10 @@ int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works
     I.df.dtp = w->dt;
     I.df.Teinf = cfgs[i].Teinf;
     I.df.Ttop = w->Ttop;
-    I.df.coef = w->dcoef;
     I.df.lu = b->d_lu;
     I.df.lu_slot = b->lu_slot;
     I.df.x3fast = (!g->dev.unit && g->dev.c3 == 0) ? 1 : 0;
     I.df.solver = cfgs[i].diffsolvetype;
-    I.df.M = M;
-    I.df.Mslot = diff_bucket_M(M);  // the slot size of the instance's diffusion launch
     I.df.fused = 1;
     I.acc = w->acc;
     I.tcfl = cfgs[i].tcfl;
@@ -538,9 +456,10 @@ int gem_batch_set_param(gem_batch* b, int param, int value) {
     b->use_graph = value ? 1 : 0;
     return GEM_OK;
   }
-  if (param == GEM_BATCH_DIFF_WARPS) {
-    if (value < 1 || value > 4) return set_err(GEM_EINVAL, "diffusion warps per block %d: 1..4", value);
-    b->wpb_max = value;
+  if (param == GEM_BATCH_DIFF_BLOCKS) {
+    if (value < 1 || value > LU_MINB_DEFAULT)
+      return set_err(GEM_EINVAL, "diffusion blocks per SM %d: 1..%d", value, LU_MINB_DEFAULT);
+    b->diff_blocks = value;
   } else if (param == GEM_BATCH_GRID_PCT) {
     if (value != 0 && (value < 10 || value > 400))
       return set_err(GEM_EINVAL, "persistent grid percentage %d: 0 (one block per item) or 10..400", value);

@@ -28,10 +28,10 @@
 //
 // The forward elimination runs while the rows are formed; the factor rows U(i,i),
 // U(i,i+1), U(i,i+2) and the eliminated right-hand side y(i) go to a per-thread scratch
-// (4 doubles per row; the warp's 32 threads interleaved, so every scratch access is one
+// (LU_ROW slots per row; the warp's 32 threads interleaved, so every scratch access is one
 // coalesced 256-byte line), and the back substitution reads them back from the last row.
-// The TRBDF2 half-step solution replaces y(i) in place and the BDF2 stage re-forms the
-// coefficients from T and n.
+// The TRBDF2 half-step solution replaces y(i) in place; the per-row conduction factors are
+// formed once, in the TR stage, and kept in the scratch for the BDF2 stage.
 //
 // The body is written once for a column accessor, so the same code runs on the device
 // (thread per column) and, compiled for the host, over every column on a CPU.
@@ -98,6 +98,17 @@ GEMD_HD double qdiv(double a, double b, double y) {
   return div_rn_slow(a, b);
 }
 
+// qdiv for a divisor whose reciprocal comes from a grid table: gem_grid_create rejects grids
+// with a tabulated reciprocal outside [2^-400, 2^400], so only the numerator is range-checked.
+GEMD_HD double qdiv_t(double a, double b, double y) {
+  const double q0 = a * y;
+  const double r = fma_rn(-q0, b, a);
+  const double q1 = fma_rn(r, y, q0);
+  if (hi_abs(a) - (523u << 20) < (1000u << 20)) return q1;
+  if (a == 0.0) return q0;
+  return div_rn_slow(a, b);
+}
+
 GEMD_HD double fmax_f(double a, double b) { return (a > b) ? a : b; }
 GEMD_HD double fabs_f(double a) { return (a < 0.0) ? -a : a; }
 
@@ -131,12 +142,41 @@ struct LuK {
   double tcoef;       // ions: thermal_coeff(s) (collisions.f90:51-53)
 };
 
+// Correctly rounded 1/x (the reference's ONE / AB(KV+1,J) in DSCAL).
+GEMD_HD double rcp_rn(double x) {
+#ifdef __CUDA_ARCH__
+  return __drcp_rn(x);
+#else
+  return 1.0 / x;
+#endif
+}
+
+// The streaming inputs of one interior cell: state values and, for the electrons, the
+// neutral densities and J1.  Loaded ahead of use (the metric factors, small tables that the
+// warp's lanes share, are read when the coefficients are formed).
+struct CellIn {
+  double T, n, n1, n2, n3, j1;
+};
+
+template <bool ELEC, class Acc>
+GEMD_HD CellIn load_cell(const Acc& a, int i) {
+  CellIn c;
+  c.T = a.T(i);
+  c.n = a.n(i);
+  if (ELEC) {
+    a.neutrals(i, c.n1, c.n2, c.n3, c.j1);
+  } else {
+    c.n1 = c.n2 = c.n3 = c.j1 = 0.0;
+  }
+  return c;
+}
+
 // thermal_conduct + diffusion_prep of interior cell i (collisions.f90:162-199,
 // diffusion.f90:24-52; A = E = 0): C = (gamma-1)/kB / max(n,1e-5) / (h1 h2 h3),
 // D = lambda h2 h3 / h1, B = C beta / h1 (electrons; 0 for the ions).
 template <bool UNIT, bool ELEC, class Acc>
-GEMD_HD void cell_coef(const Acc& a, const LuK& k, int i, double& C, double& D, double& B) {
-  const double T = a.T(i), nv = a.n(i);
+GEMD_HD void cell_coef(const Acc& a, const LuK& k, int i, const CellIn& c, double& C, double& D, double& B) {
+  const double T = c.T, nv = c.n;
   double h1 = 1.0, h2 = 1.0, h3 = 1.0, yh1 = 1.0, ha1 = 1.0, yha1 = 1.0;
   if (!UNIT) a.metrics(i, h1, h2, h3, yh1, ha1, yha1);
   const double T25 = pow25(T);
@@ -144,17 +184,15 @@ GEMD_HD void cell_coef(const Acc& a, const LuK& k, int i, double& C, double& D, 
   if (!ELEC) {
     lam = k.tcoef * T25;
   } else {
-    double n1, n2, n3, j1;
-    a.neutrals(i, n1, n2, n3, j1);
     const double sq = sqrt_rn(T);
-    const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
-                     n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
+    const double X = c.n1 * 1.1e-16 * (1 + 5.7e-4 * T) + c.n2 * 2.82e-17 * sq * (1 - 1.21e-4 * T) +
+                     c.n3 * 2.2e-16 * (1 + 3.6e-2 * sq);
     lam = ELCHRG * 100 * 7.7e5 * T25 / (1 + 3.22e4 * (T * T) / nv * X);
-    Bc = 5.0 / 2 * KB / ELCHRG * j1;  // beta (collisions.f90:197)
+    Bc = 5.0 / 2 * KB / ELCHRG * c.j1;  // beta (collisions.f90:197)
   }
-  C = qdiv(k.c0 / fmax_f(nv, MINDENSDIV), ha1, yha1);
-  D = qdiv(lam * h2 * h3, h1, yh1);
-  B = ELEC ? qdiv(C * Bc, h1, yh1) : 0.0;
+  C = qdiv_t(k.c0 / fmax_f(nv, MINDENSDIV), ha1, yha1);
+  D = qdiv_t(lam * h2 * h3, h1, yh1);
+  B = ELEC ? qdiv_t(C * Bc, h1, yh1) : 0.0;
 }
 
 // The band rows (PDEparabolic.f90:66-136 TR, 150-210 BDF2, 250-319 backward Euler) from the
@@ -175,7 +213,7 @@ GEMD_HD void lu_step(const Acc& a, int j, LuState& st, double s, double d, doubl
     u1 = d;
     u2 = e;
     y = r;
-    m = (1.0 / s) * st.p;  // DSCAL(1/pivot)
+    m = rcp_rn(s) * st.p;  // DSCAL(1/pivot)
     const double p1 = st.q - m * d;
     st.q = 0.0 - m * e;
     st.p = p1;
@@ -185,113 +223,232 @@ GEMD_HD void lu_step(const Acc& a, int j, LuState& st, double s, double d, doubl
     u1 = st.q;
     u2 = 0.0;
     y = st.b;
-    m = (1.0 / st.p) * s;
+    m = rcp_rn(st.p) * s;
     st.p = d - m * st.q;
     st.q = e;
     st.b = r - m * st.b;
   }
-  a.S(j, 0) = u0;
-  a.S(j, 1) = u1;
-  a.S(j, 2) = u2;
-  a.S(j, 3) = y;
+  a.sst(j, 0, u0);
+  a.sst(j, 1, u1);
+  a.sst(j, 2, u2);
+  a.sst(j, 3, y);
 }
 
-// Forward pass of one stage over rows 1..n: forms every band row, eliminates, stores the
-// factor rows.  STG = ST_BDF2 reads the TR solution from the y slots (row i's slot is read
-// before row i's factor row is written).
+// Scratch slots of a row: the factor row U(i,i), U(i,i+1), U(i,i+2) and y(i) (slots 0-3;
+// the TR solution replaces y(i)), and for TRBDF2 the conduction/advection factors q-, q+,
+// bq of the row (slots 4-6), formed once for both stages.
+constexpr int LU_ROW = 8;  // scratch slots per row
+
+// Forward pass of the first stage (TR half step, or the backward-Euler step) over rows
+// 1..n: forms every band row from T and n, eliminates, stores the factor rows (and, for
+// TR, the row factors for the BDF2 stage).  Software-pipelined: each iteration forms row
+// i+1 (conductivities, factors, band row -- independent of the elimination) next to the
+// elimination step of row i, and the cell inputs are loaded two rows ahead of their use.
+struct BandRow {
+  double s, d, e, r;  // sub-diagonal, diagonal, super-diagonal, right-hand side
+};
+
 template <bool UNIT, bool ELEC, int STG, class Acc>
-GEMD_HD void lu_forward(const Acc& a, const LuK& k) {
+GEMD_HD void lu_forward_first(const Acc& a, const LuK& k) {
   const int n = k.n;
   const double dt = k.dt;
   const double dt2 = dt / 2, ydt2 = 1 / (dt / 2);
-  const double dt3 = dt / 3, ydt3 = 1 / (dt / 3);
   const double ydt = 1 / dt;
-  LuState st{1.0, 0.0, k.tmin};  // row 1: identity, right-hand side Tsminx1
+  auto cell = [&](int i) { return load_cell<ELEC>(a, i < n ? i : n); };
+  const CellIn c1 = cell(1), c2 = cell(2);
+  CellIn cA = cell(3), cB = cell(4);  // cells i+1, i+2 of the next row formed (i = 2)
   // sliding window over cells: D(i-1), D(i), C(i), B(i) and T(i-1), T(i)
-  double Cc, Dc, Bcur;
-  cell_coef<UNIT, ELEC>(a, k, 1, Cc, Dc, Bcur);
-  double Dm = Dc;  // D(1), becomes D(i-1) for i = 2
-  cell_coef<UNIT, ELEC>(a, k, 2, Cc, Dc, Bcur);
-  double Tm = a.T(1), Tc = a.T(2);
-  for (int j = 1; j < n; ++j) {
-    const int i = j + 1;  // the row brought in
-    double s, d, e, r;
+  double Cc, Dc, Bcur, Dm;
+  cell_coef<UNIT, ELEC>(a, k, 1, c1, Cc, Dm, Bcur);  // D(1)
+  cell_coef<UNIT, ELEC>(a, k, 2, c2, Cc, Dc, Bcur);
+  double Tm = c1.T, Tc = c2.T;
+  // forms row i (2 <= i <= n) and advances the window
+  auto form = [&](int i) -> BandRow {
+    BandRow w;
     if (i == n) {
-      s = 0.0;
-      d = 1.0;
-      e = 0.0;
-      r = k.tmax;
-    } else {
-      double Cn, Dn, Bn;
-      cell_coef<UNIT, ELEC>(a, k, i + 1, Cn, Dn, Bn);
-      const double Tp = a.T(i + 1);
-      const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dn);  // PDEparabolic.f90:49
-      const double qm = qdiv(qdiv(Cc * Dhm, a.dxi(i), a.ydxi(i)), a.dx(i), a.ydx(i));
-      const double qp = qdiv(qdiv(Cc * Dhp, a.dxi(i), a.ydxi(i)), a.dx(i + 1), a.ydx(i + 1));
-      const double bq = ELEC ? qdiv(Bcur, a.dxs(i), a.ydxs(i)) : 0.0;
-      if (STG == ST_TR) {
-        s = -(qm / 2) + bq / 2;
-        d = ydt2 + qp / 2 + qm / 2;
-        e = -(qp / 2) - bq / 2;
-        const double Pd = qp / 2 + qm / 2;
-        r = qdiv(Tc, dt2, ydt2) - s * Tm - Pd * Tc - e * Tp;
-      } else if (STG == ST_BDF2) {
-        s = -qm + bq;
-        d = ydt3 + qp + qm;
-        e = -qp - bq;
-        const double tr = a.S(i, 3);
-        r = -qdiv(1 / 3.0 * Tc, dt3, ydt3) + qdiv(4 / 3.0 * tr, dt3, ydt3);
-      } else {
-        s = -qm + bq;
-        d = ydt + qp + qm;
-        e = -qp - bq;
-        r = qdiv(Tc, dt, ydt);
-      }
-      Dm = Dc;
-      Dc = Dn;
-      Cc = Cn;
-      Bcur = Bn;
-      Tm = Tc;
-      Tc = Tp;
+      w.s = 0.0;
+      w.d = 1.0;
+      w.e = 0.0;
+      w.r = k.tmax;
+      return w;
     }
-    lu_step(a, j, st, s, d, e, r);
+    const CellIn cn = cA;  // cell i+1
+    cA = cB;
+    cB = cell(i + 3);
+    double Cn, Dn, Bn;
+    cell_coef<UNIT, ELEC>(a, k, i + 1, cn, Cn, Dn, Bn);
+    const double Tp = cn.T;
+    const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dn);  // PDEparabolic.f90:49
+    const double qm = qdiv_t(qdiv_t(Cc * Dhm, a.dxi(i), a.ydxi(i)), a.dx(i), a.ydx(i));
+    const double qp = qdiv_t(qdiv_t(Cc * Dhp, a.dxi(i), a.ydxi(i)), a.dx(i + 1), a.ydx(i + 1));
+    const double bq = ELEC ? qdiv_t(Bcur, a.dxs(i), a.ydxs(i)) : 0.0;
+    if (STG == ST_TR) {
+      a.sst(i, 4, qm);
+      a.sst(i, 5, qp);
+      if (ELEC) a.sst(i, 6, bq);
+      w.s = -(qm / 2) + bq / 2;
+      w.d = ydt2 + qp / 2 + qm / 2;
+      w.e = -(qp / 2) - bq / 2;
+      const double Pd = qp / 2 + qm / 2;
+      w.r = qdiv(Tc, dt2, ydt2) - w.s * Tm - Pd * Tc - w.e * Tp;
+    } else {
+      w.s = -qm + bq;
+      w.d = ydt + qp + qm;
+      w.e = -qp - bq;
+      w.r = qdiv(Tc, dt, ydt);
+    }
+    Dm = Dc;
+    Dc = Dn;
+    Cc = Cn;
+    Bcur = Bn;
+    Tm = Tc;
+    Tc = Tp;
+    return w;
+  };
+  LuState st{1.0, 0.0, k.tmin};  // row 1: identity, right-hand side Tsminx1
+  BandRow w = form(2);
+  for (int j = 1; j < n; ++j) {
+    const BandRow cur = w;  // row j+1
+    if (j + 2 <= n) w = form(j + 2);
+    lu_step(a, j, st, cur.s, cur.d, cur.e, cur.r);
   }
-  a.S(n, 0) = st.p;
-  a.S(n, 1) = 0.0;
-  a.S(n, 2) = 0.0;
-  a.S(n, 3) = st.b;
+  a.sst(n, 0, st.p);
+  a.sst(n, 1, 0.0);
+  a.sst(n, 2, 0.0);
+  a.sst(n, 3, st.b);
 }
 
-// dtbsv back substitution; OUT(i, x) receives the solution from row n down to row 1.
+// Forward pass of the BDF2 stage: the rows from the stored q-, q+, bq, the TR solution in
+// y(i) and T (all loaded two rows ahead; row r's slots 0-3 are rewritten only when row r+1
+// is brought in, after row r's TR value was read).
+template <bool ELEC, class Acc>
+GEMD_HD void lu_forward_bdf2(const Acc& a, const LuK& k) {
+  const int n = k.n;
+  const double dt3 = k.dt / 3, ydt3 = 1 / (k.dt / 3);
+  struct RowIn {
+    double qm, qp, bq, tr, T;
+  };
+  auto rin = [&](int i) {
+    const int c = i < n - 1 ? i : n - 1;
+    RowIn v;
+    v.qm = a.sld(c, 4);
+    v.qp = a.sld(c, 5);
+    v.bq = ELEC ? a.sld(c, 6) : 0.0;
+    v.tr = a.sld(c, 3);
+    v.T = a.T(c);
+    return v;
+  };
+  RowIn rA = rin(2), rB = rin(3);  // rows i, i+1 of the next row formed (i = 2)
+  auto form = [&](int i) -> BandRow {
+    BandRow w;
+    if (i == n) {
+      w.s = 0.0;
+      w.d = 1.0;
+      w.e = 0.0;
+      w.r = k.tmax;
+      return w;
+    }
+    const RowIn v = rA;
+    rA = rB;
+    rB = rin(i + 2);
+    w.s = -v.qm + v.bq;
+    w.d = ydt3 + v.qp + v.qm;
+    w.e = -v.qp - v.bq;
+    w.r = -qdiv(1 / 3.0 * v.T, dt3, ydt3) + qdiv(4 / 3.0 * v.tr, dt3, ydt3);
+    return w;
+  };
+  LuState st{1.0, 0.0, k.tmin};
+  BandRow w = form(2);
+  for (int j = 1; j < n; ++j) {
+    const BandRow cur = w;  // row j+1
+    if (j + 2 <= n) w = form(j + 2);
+    lu_step(a, j, st, cur.s, cur.d, cur.e, cur.r);
+  }
+  a.sst(n, 0, st.p);
+  a.sst(n, 1, 0.0);
+  a.sst(n, 2, 0.0);
+  a.sst(n, 3, st.b);
+}
+
+// dtbsv back substitution from row n down to row 1.  OUT.pre(i) loads what OUT needs for row
+// i; OUT(i, x, pre) receives the solution.  Factor rows and OUT's inputs are loaded
+// GEMD_BWD_DEPTH rows ahead of their use.
+struct RowF {
+  double u0, u1, u2, y;
+};
+#ifndef GEMD_BWD_DEPTH
+#define GEMD_BWD_DEPTH 4
+#endif
+
 template <class Acc, class Out>
-GEMD_HD void lu_backward(const Acc& a, int n, Out out) {
-  double x2 = 0.0;                   // x(i+2)
-  double x1 = a.S(n, 3) / a.S(n, 0);  // x(n)
-  out(n, x1);
-  for (int i = n - 1; i >= 1; --i) {
-    double x = a.S(i, 3);
-    if (i <= n - 2) x = x - x2 * a.S(i, 2);
-    x = x - x1 * a.S(i, 1);
-    x = x / a.S(i, 0);
-    out(i, x);
-    x2 = x1;
-    x1 = x;
+GEMD_HD void lu_backward(const Acc& a, int n, const Out& out) {
+  using Pre = decltype(out.pre(1));
+  auto row = [&](int i) {
+    RowF r;
+    r.u0 = a.sld(i, 0);
+    r.u1 = a.sld(i, 1);
+    r.u2 = a.sld(i, 2);
+    r.y = a.sld(i, 3);
+    return r;
+  };
+  constexpr int DP = GEMD_BWD_DEPTH;
+  RowF W[DP];
+  Pre P[DP];
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+  for (int q = 0; q < DP; ++q) {
+    const int i = n - q >= 1 ? n - q : 1;
+    W[q] = row(i);
+    P[q] = out.pre(i);
+  }
+  double x1 = 0.0, x2 = 0.0;  // x(i+1), x(i+2)
+  for (int i0 = n; i0 >= 1; i0 -= DP) {
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+    for (int q = 0; q < DP; ++q) {
+      const int i = i0 - q;
+      if (i >= 1) {
+        const RowF r = W[q];
+        const Pre pr = P[q];
+        if (i - DP >= 1) {
+          W[q] = row(i - DP);
+          P[q] = out.pre(i - DP);
+        }
+        double x = r.y;
+        if (i <= n - 2) x = x - x2 * r.u2;
+        if (i <= n - 1) x = x - x1 * r.u1;
+        x = x / r.u0;
+        out(i, x, pr);
+        x2 = x1;
+        x1 = x;
+      }
+    }
   }
 }
+
+// OUT for the TR stage: the half-step solution replaces y(i).
+template <class Acc>
+struct StoreTR {
+  const Acc& a;
+  GEMD_HD double pre(int) const { return 0.0; }
+  GEMD_HD void operator()(int i, double x, double) const { a.sst(i, 3, x); }
+};
 
 // The whole solve of one (column, species): TRBDF2 (solver 2) or backward Euler (solver 1).
-// STORE(i, T) receives the new temperature of row i (before the max(T,100) floor).
-template <bool UNIT, bool ELEC, class Acc, class Store>
-GEMD_HD void lu_column(const Acc& a, const LuK& k, int solver, Store store) {
+// OUT receives the new temperature of each row (before the max(T,100) floor).
+template <bool UNIT, bool ELEC, class Acc, class Out>
+GEMD_HD void lu_column(const Acc& a, const LuK& k, int solver, const Out& out) {
   const int n = k.n;
   if (solver == 2) {
-    lu_forward<UNIT, ELEC, ST_TR>(a, k);
-    lu_backward(a, n, [&](int i, double x) { a.S(i, 3) = x; });  // TR solution into y(i)
-    lu_forward<UNIT, ELEC, ST_BDF2>(a, k);
+    lu_forward_first<UNIT, ELEC, ST_TR>(a, k);
+    lu_backward(a, n, StoreTR<Acc>{a});
+    lu_forward_bdf2<ELEC>(a, k);
   } else {
-    lu_forward<UNIT, ELEC, ST_BE>(a, k);
+    lu_forward_first<UNIT, ELEC, ST_BE>(a, k);
   }
-  lu_backward(a, n, store);
+  lu_backward(a, n, out);
 }
 
 }  // namespace gemd

@@ -58,6 +58,14 @@ int num_sms() {
   return sms;
 }
 
+// |y| in [2^-400, 2^400] (as the device's exact-quotient range test reads the exponent)
+bool y_in_range(double y) {
+  unsigned long long u;
+  std::memcpy(&u, &y, 8);
+  const unsigned h = (unsigned)(u >> 32) & 0x7fffffffu;
+  return h - (623u << 20) < (800u << 20);
+}
+
 unsigned grid_for(long long n, int threads, int per_sm = 8) {
   long long b = (n + threads - 1) / threads;
   const long long cap = (long long)num_sms() * per_sm;
@@ -94,7 +102,6 @@ struct gem_work {
   int lx1, lx2, lx3;
   double *vs1i, *vs2i, *vs3i, *nn, *Tn, *dt;
   double* Ttop;             // per-column exospheric temperature (lx2*lx3), or null for Teinf
-  double* dcoef;            // diffusion coefficients C, D, B per interior cell (DCOEF_N * nc)
   double* lu;               // band-solve scratch of k_diffusion_lu (lu_slots() slots of lx1 rows)
   unsigned long long* acc;  // 32 slots: CFL maxima / counters
   long long nf1, nf2, nf3;
@@ -203,34 +210,27 @@ int lu_warps_per_sm() {
     int a = 0, b = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_diffusion_lu<true>, 32 * LU_WPB, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_diffusion_lu<false>, 32 * LU_WPB, 0);
-    int w = std::min(a, b) * LU_WPB;
-    if (const char* e = getenv("GEM_LU_WARPS_PER_SM")) w = std::min(w, std::max(LU_WPB, atoi(e)));
+    const int w = std::min(a, b) * LU_WPB;
     wps = std::max(LU_WPB, std::min(w, LU_MAX_WARPS_PER_SM));
   }
   return wps;
 }
 long long lu_slots() { return (long long)num_sms() * lu_warps_per_sm(); }
-long long lu_slot_doubles(int lx1) { return (long long)lx1 * 4 * 32; }
-
-bool use_pcr_diffusion() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("GEM_DIFFUSION");
-    v = (e && strcmp(e, "pcr") == 0) ? 1 : 0;
-  }
-  return v == 1;
+long long lu_slot_doubles(int lx1) { return (long long)lx1 * gemd::LU_ROW * 32; }
+// warp tasks of one grid's diffusion, rounded up to whole blocks
+long long lu_tasks(const Dims& d) {
+  const long long ntask = (((long long)d.lx2 * d.lx3 + 31) / 32) * LSP;
+  return ((ntask + LU_WPB - 1) / LU_WPB) * LU_WPB;
 }
+// scratch slots a grid's launches use: one per resident warp, no more than it has tasks
+long long lu_slots_for(const Dims& d) { return std::min(lu_slots(), lu_tasks(d)); }
 
 int launch_diffusion_lu(const gem_grid* g, DiffArgs a, cudaStream_t st) {
   const Dims& d = g->dev.d;
   if (!a.lu) return set_err(GEM_EINVAL, "diffusion without a band-solve scratch");
   a.lu_slot = lu_slot_doubles(d.lx1);
   a.x3fast = (!g->dev.unit && g->dev.c3 == 0) ? 1 : 0;
-  const long long ncol = (long long)d.lx2 * d.lx3;
-  const long long ntask = ((ncol + 31) / 32) * LSP;
-  long long nblk = (ntask + LU_WPB - 1) / LU_WPB;
-  const long long cap = lu_slots() / LU_WPB;
-  if (nblk > cap) nblk = cap;
+  const long long nblk = lu_slots_for(d) / LU_WPB;  // the work object holds this many slots
   if (g->dev.unit)
     k_diffusion_lu<true><<<(unsigned)nblk, 32 * LU_WPB, 0, st>>>(a);
   else
@@ -239,47 +239,7 @@ int launch_diffusion_lu(const gem_grid* g, DiffArgs a, cudaStream_t st) {
   return GEM_OK;
 }
 
-int launch_diffusion(const gem_grid* g, DiffArgs a, cudaStream_t st) {
-  if (!use_pcr_diffusion()) return launch_diffusion_lu(g, a, st);
-  const Dims& d = g->dev.d;
-  const int M = std::max(2, (d.lx1 + 31) / 32);
-  const size_t per_warp = (size_t)DNA * M * 32 * sizeof(double);
-  int wpb = (int)std::min<size_t>(4, (227 * 1024) / per_warp);
-  if (wpb < 1) return set_err(GEM_EINVAL, "lx1=%d too long for the on-chip column solver", d.lx1);
-  a.M = M;
-  a.Mslot = M;
-  const size_t smem = per_warp * wpb;
-  const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
-  long long nblk = (ncs + wpb - 1) / wpb;
-  int per_sm = 0;
-  if (g->dev.unit) {
-    GEM_CUDA(cudaFuncSetAttribute(k_diffusion<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion<true>, 32 * wpb, smem));
-  } else {
-    GEM_CUDA(cudaFuncSetAttribute(k_diffusion<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffusion<false>, 32 * wpb, smem));
-  }
-  if (per_sm < 1) per_sm = 1;
-  const long long cap = (long long)num_sms() * per_sm;
-  if (nblk > cap) nblk = cap;
-  if (!a.coef) return set_err(GEM_EINVAL, "diffusion without a coefficient buffer");
-  const unsigned nrow = (unsigned)std::min<long long>((long long)d.lx2 * d.lx3 * LSP, (long long)num_sms() * 16);
-  const size_t csm = (size_t)3 * d.lx1 * sizeof(double);
-  if (g->dev.unit) {
-    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_coef<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-    k_diffusion_coef<true><<<nrow, 128, csm, st>>>(a);
-  } else {
-    GEM_CUDA(cudaFuncSetAttribute(k_diffusion_coef<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-    k_diffusion_coef<false><<<nrow, 128, csm, st>>>(a);
-  }
-  GEM_LAUNCHED("k_diffusion_coef");
-  if (g->dev.unit)
-    k_diffusion<true><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
-  else
-    k_diffusion<false><<<(unsigned)nblk, 32 * wpb, smem, st>>>(a);
-  GEM_LAUNCHED("k_diffusion");
-  return GEM_OK;
-}
+int launch_diffusion(const gem_grid* g, DiffArgs a, cudaStream_t st) { return launch_diffusion_lu(g, a, st); }
 
 // x2 / x3 sweep adjoints of up to three fields sharing the face velocities v: one marching
 // thread per (line, segment of SVM_TJ cells, species, field).
@@ -448,6 +408,13 @@ int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
       ydxs[j] = 1.0 / dxs[j];
     }
     for (int j = 0; j < l; ++j) ydxi[j] = 1.0 / dxi[j];
+    if (dd == 0) {  // the diffusion's exact quotients assume these reciprocals are in range
+      bool ok = true;
+      for (int j = 2; j <= l; ++j) ok = ok && y_in_range(ydx[j]);
+      for (int j = 1; j <= l - 2; ++j) ok = ok && y_in_range(ydxi[j]);
+      for (int j = 2; j <= l - 1; ++j) ok = ok && y_in_range(ydxs[j]);
+      if (!ok) rc = set_err(GEM_EINVAL, "x1 grid spacings outside [2^-400, 2^400]");
+    }
     Line1D& L = G.L[dd];
     cp(dx.data(), dx.size(), &L.dx);
     cp(ydx.data(), ydx.size(), &L.ydx);
@@ -487,6 +454,17 @@ int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
       y0[k] = 1.0 / a0[k];
       y1[k] = 1.0 / a1[k];
       yh1[k] = 1.0 / h1[k];
+    }
+    {  // interior cells: the diffusion's exact quotients assume these reciprocals are in range
+      bool ok = true;
+      const int n3 = inv ? 1 : lx3;
+      for (int i3 = 1; i3 <= n3 && ok; ++i3)
+        for (int i2 = 1; i2 <= lx2 && ok; ++i2)
+          for (int i1 = 1; i1 <= lx1; ++i1) {
+            const size_t k = (size_t)((i1 + 1) + s2 * (i2 + 1) + (inv ? 0 : s3 * (i3 + 1)));
+            ok = ok && y_in_range(y0[k]) && y_in_range(yh1[k]);
+          }
+      if (!ok) rc = set_err(GEM_EINVAL, "metric factors outside [2^-400, 2^400]");
     }
     cp(h1.data(), ncell, &G.h1);
     cp(h2.data(), ncell, &G.h2);
@@ -610,7 +588,6 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
   w->vs1i = w->vs2i = w->vs3i = w->nn = w->Tn = w->dt = nullptr;
   w->acc = nullptr;
   w->Ttop = nullptr;
-  w->dcoef = nullptr;
   w->lu = nullptr;
   w->F = w->A = w->E = nullptr;
   w->nF = w->nA = w->nE = 0;
@@ -631,8 +608,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
             {(void**)&w->Tn, sizeof(double) * nc},
             {(void**)&w->dt, sizeof(double) * 4},
             {(void**)&w->acc, sizeof(unsigned long long) * 32},
-            {(void**)&w->dcoef, sizeof(double) * nc * DCOEF_N},
-            {(void**)&w->lu, sizeof(double) * lu_slots() * lu_slot_doubles(d.lx1)}};
+            {(void**)&w->lu, sizeof(double) * lu_slots_for(d) * lu_slot_doubles(d.lx1)}};
   for (auto& a : al) {
     if (cudaMalloc(a.p, a.bytes) != cudaSuccess) {
       gem_work_destroy(w);
@@ -651,7 +627,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
 int gem_work_destroy(gem_work* w) {
   if (!w) return GEM_OK;
   for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);
-  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop, w->dcoef, w->lu};
+  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop, w->lu};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete w;
@@ -806,7 +782,6 @@ int gem_energy_diffusion_dev(const gem_cfg* cfg, const gem_grid* g, double* flui
   a.dtp = dt;
   a.Teinf = cfg->Teinf;
   a.Ttop = w->Ttop;
-  a.coef = w->dcoef;
   a.lu = w->lu;
   a.solver = cfg->diffsolvetype;
   a.fused = 0;
@@ -999,7 +974,6 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
   d.dtp = dt;
   d.Teinf = cfg->Teinf;
   d.Ttop = w->Ttop;
-  d.coef = w->dcoef;
   d.lu = w->lu;
   d.solver = cfg->diffsolvetype;
   d.fused = 1;

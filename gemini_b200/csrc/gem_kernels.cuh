@@ -1298,21 +1298,11 @@ __global__ void k_ghost_epilogue(GridDev G, Blocks B) {
 
 // ======================================================================================
 // 7. Field-aligned heat diffusion (multifluid.f90:309-342; collisions.f90:162-199;
-//    diffusion.f90:24-152; PDEparabolic.f90:19-346).  One warp per (x1 column, species).
-//    Lane l owns the M contiguous cells 1+l*M .. l*M+M of the column.
-//
-//    Coefficients: lambda, beta, C, D, B, Dh and every band entry / right-hand side are
-//    formed with the reference's operation order (PDEparabolic.f90:59-136, 150-210), so the
-//    banded system is bit-identical to the one the reference hands to dgbsv (T**(5/2) is the
-//    correctly rounded value; see pow25).
-//    Solve: each tridiagonal system is eliminated by the partition method -- every lane
-//    eliminates its block down and up in shared memory, the 64-row interface system (2 rows
-//    per lane) is solved by parallel cyclic reduction with warp shuffles, and the block
-//    interiors are back-substituted -- followed by one step of iterative refinement with a
-//    compensated (TwoSum/TwoProd) residual.  The Dirichlet rows are identity rows, so the
-//    boundary values are exact.  The result is the solution of the reference's discrete
-//    system to ~1e-15 relative; the TR half step of a stiff column (Crank-Nicolson part)
-//    amplifies plain double-precision solve error to ~1e-12, which the refinement removes.
+//    diffusion.f90:24-152; PDEparabolic.f90:19-346).  The forward solve is k_diffusion_lu
+//    (7a, gem_diffusion_lu.cuh): the reference's band systems factored in LAPACK dgbsv's
+//    order.  This section also holds the warp-parallel tridiagonal solver (lane blocks,
+//    interface reduction, cyclic reduction) that the adjoint (7b) uses to solve the
+//    transposed stage systems; the adjoint needs no LAPACK-order rounding.
 // ======================================================================================
 struct DiffArgs {
   GridDev G;
@@ -1324,37 +1314,10 @@ struct DiffArgs {
   double Teinf;
   const double* Ttop;  // optional per-column (i2 fastest) exospheric temperature, else Teinf
   int solver;  // 1 backward Euler, 2 TRBDF2
-  int M;       // rows per lane
-  int Mslot;   // rows per lane that each warp's shared-memory slot is sized for (>= M)
   int fused;   // 1: clean_param(3) + T2rhoe folded into the store
-  double* coef;  // per-cell C (7 species), D (7), B (electrons): written by k_diffusion_coef
   double* lu;          // band-solve scratch of k_diffusion_lu (one slot per resident warp)
-  long long lu_slot;   // doubles per slot (>= lx1 * 4 * 32)
+  long long lu_slot;   // doubles per slot (>= lx1 * LU_ROW * 32)
   int x3fast;          // column order of k_diffusion_lu: x3 fastest (x3-invariant metrics)
-};
-
-// Coefficient scratch layout (interior cells q = ci(i1,i2,i3), nc of them): the per-row
-// conduction factors q-, q+ of species s at coef[s*nc + q], coef[(LSP+s)*nc + q], and the
-// electron advection factor bq at coef[2*LSP*nc + q] (rows 2..lx1-1; rows 1, lx1 hold 0).
-constexpr int DCOEF_N = 2 * LSP + 1;
-
-// shared-memory arrays per warp: inputs (T and the per-row conduction/advection factors),
-// the stage right-hand side / residual, the solution, and the factorisation (IB, SS, TT)
-constexpr int DA_T = 0, DA_QP = 1, DA_QM = 2, DA_BQ = 3, DA_RHS = 4, DA_SS = 5, DA_IB = 6, DA_TT = 7, DA_R = 8;
-constexpr int DNA = 9;
-
-// Row-interleaved layout: the DNA arrays of row k of every lane sit together, so one
-// pointer per row serves every array with an immediate offset:
-//   warp base + (k*DNA + arr)*32 + lane
-struct WarpMem {
-  double* wb;  // warp base
-  double* b;   // warp base + lane
-  __device__ __forceinline__ double& at(int arr, int k) const { return b[(k * DNA + arr) * 32]; }
-  __device__ __forceinline__ double& at_lane(int arr, int k, int l) const { return wb[(k * DNA + arr) * 32 + l]; }
-  // the factorisation arrays of the band solver
-  __device__ __forceinline__ double& ss(int k) const { return at(DA_SS, k); }
-  __device__ __forceinline__ double& ib(int k) const { return at(DA_IB, k); }
-  __device__ __forceinline__ double& tt(int k) const { return at(DA_TT, k); }
 };
 
 // 1/b to about one ulp for the solver's pivots and elimination multipliers (not for the
@@ -1371,21 +1334,6 @@ __device__ __forceinline__ double rcp_nr(double b) {
   const unsigned hb = (unsigned)__double2hiint(b) & 0x7fffffffu;
   if (hb - (123u << 20) < (1800u << 20)) return y;  // 2^-900 < |b| < 2^900
   return 1.0 / b;
-}
-
-// x**2.5 as x*x*sqrt(x) in double-double (fma for the exact product errors), rounded once:
-// correctly rounded except in vanishingly rare near-halfway cases.  The CPU checker
-// evaluates the same expression.
-__device__ __forceinline__ double pow25(double x) {
-  if (!(x > 0.0)) return pow(x, 2.5);
-  const double s = sqrt(x);
-  const double es = __fma_rn(-s, s, x);
-  const double sl = es / (2.0 * s);
-  const double x2 = x * x;
-  const double x2l = __fma_rn(x, x, -x2);
-  const double p = x2 * s;
-  const double pl = __fma_rn(x2, s, -p);
-  return p + (pl + (x2 * sl + x2l * s));
 }
 
 // Lane-blocked tridiagonal solver.  Row k of this lane's block (global row 32-lane block
@@ -1589,374 +1537,88 @@ __device__ __forceinline__ void band_solve_T(const WM& W, int M, int lane, RowM 
   }
 }
 
-// exact-error accumulation for the refinement residual r - (a xm + b x + c xp)
-__device__ __forceinline__ double residual3(double r, double a, double xm, double b, double x, double c, double xp) {
-  const double p1 = a * xm, e1 = __fma_rn(a, xm, -p1);
-  const double p2 = b * x, e2 = __fma_rn(b, x, -p2);
-  const double p3 = c * xp, e3 = __fma_rn(c, xp, -p3);
-  double s = r, comp = 0.0;
-  const double v[3] = {-p1, -p2, -p3};
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {  // TwoSum
-    const double t = s + v[q];
-    const double bp = t - s;
-    comp += (s - (t - bp)) + (v[q] - bp);
-    s = t;
-  }
-  return s + (comp - (e1 + e2 + e3));
-}
-
-// Solve the stage system (matrix rowm, right-hand side in DA_RHS) with one step of
-// iterative refinement; the solution ends in DA_R, DA_RHS is consumed.
-template <class RowM>
-__device__ void refined_solve(const WarpMem& W, int M, int lane, RowM rowm) {
-  IfaceLU F;
-  band_factor(W, M, lane, rowm, F);
-  for (int k = 0; k < M; ++k) W.at(DA_R, k) = W.at(DA_RHS, k);
-  band_solve(W, M, lane, rowm, F, DA_R);
-  __syncwarp();
-  const double xprev = __shfl_up_sync(0xffffffffu, W.at(DA_R, M - 1), 1);
-  const double xnext = __shfl_down_sync(0xffffffffu, W.at(DA_R, 0), 1);
-  double xm = xprev, xc = W.at(DA_R, 0);
-  for (int k = 0; k < M; ++k) {
-    double a, b, c;
-    rowm(k, a, b, c);
-    const double xp = (k < M - 1) ? W.at(DA_R, k + 1) : xnext;
-    W.at(DA_RHS, k) = residual3(W.at(DA_RHS, k), a, xm, b, xc, c, xp);
-    xm = xc;
-    xc = xp;
-  }
-  band_solve(W, M, lane, rowm, F, DA_RHS);
-  for (int k = 0; k < M; ++k) W.at(DA_R, k) = W.at(DA_R, k) + W.at(DA_RHS, k);
-  __syncwarp();
-}
-
-// thermal_conduct + diffusion_prep per cell (collisions.f90:162-199, diffusion.f90:24-52):
-// C = (gamma-1)/kB / max(n,1e-5) / (h1 h2 h3), D = lambda h2 h3 / h1, B = C beta / h1, then the
-// per-row factors of the band matrices (PDEparabolic.f90:70-80) q- = C Dh(i)/dx1i/dx1(i),
-// q+ = C Dh(i+1)/dx1i/dx1(i+1), bq = B/(dx1(i+1)+dx1(i)) with Dh(i) = (D(i-1)+D(i))/2.
-// One block per (i2, i3, species) row at a time, threads along x1 (coalesced, full
-// occupancy); C, D, B of the row in dynamic shared memory (3*lx1 doubles).
-template <bool UNIT>
-__device__ __forceinline__ void b_diffusion_coef(const DiffArgs& P, const VB vb) {
-  extern __shared__ double dsm[];
-  const GridDev& G = P.G;
-  const Dims d = G.d;
-  const int n = d.lx1;
-  double* sC = dsm;
-  double* sD = dsm + n;
-  double* sB = dsm + 2 * n;
-  const long long nc = nci(d);
-  const int ncol = d.lx2 * d.lx3;
-  const int nrow = ncol * LSP;
-  const Line1D& L1 = G.L[0];
-  for (int r = vb.bx; r < nrow; r += vb.gx) {
-    const int s = r / ncol;
-    const int col = r - s * ncol;
-    const int i2 = col % d.lx2 + 1, i3 = col / d.lx2 + 1;
-    const long long m0 = gi(d, 0, i2, i3);
-    const long long mm0 = cmi(G, 0, i2, i3);
-    const long long q0 = ci(d, 1, i2, i3) - 1;
-    const double* Tcol = P.B.Ts(s) + m0;
-    const double* ncol_ = P.B.ns(s) + m0;
-    const double c0 = (c_gammas[s] - 1.0) / KB;
-    for (int i = threadIdx.x + 1; i <= n; i += blockDim.x) {
-      const double T = Tcol[i];
-      const double nv = ncol_[i];
-      const long long mk = mm0 + i;
-      const double h1v = ldm<UNIT>(G.h1, mk), h2v = ldm<UNIT>(G.h2, mk), h3v = ldm<UNIT>(G.h3, mk);
-      const double yh1 = ldm<UNIT>(G.yh1, mk);
-      double ha1v = 1.0, yha1v = 1.0;
-      cell_metric<UNIT>(G, mk, 0, ha1v, yha1v);  // h1*h2*h3
-      const double T25 = pow25(T);
-      double lam, Bc = 0.0;
-      if (s < LSP - 1) {
-        lam = c_tcoef[s] * T25;
-      } else {
-        const long long q = q0 + i;
-        const double n1 = __ldg(P.nn + q), n2 = __ldg(P.nn + nc + q), n3 = __ldg(P.nn + 2 * nc + q);
-        const double X = n1 * 1.1e-16 * (1 + 5.7e-4 * T) + n2 * 2.82e-17 * sqrt(T) * (1 - 1.21e-4 * T) +
-                         n3 * 2.2e-16 * (1 + 3.6e-2 * sqrt(T));
-        lam = ELCHRG * 100 * 7.7e5 * T25 / (1 + 3.22e4 * (T * T) / nv * X);
-        Bc = 5.0 / 2 * KB / ELCHRG * P.J1[m0 + i];  // beta (collisions.f90:197)
-      }
-      const double Cc = mdiv(c0 / fmax_f(nv, MINDENSDIV), ha1v, yha1v);
-      sC[i - 1] = Cc;
-      sD[i - 1] = mdiv(lam * h2v * h3v, h1v, yh1);
-      sB[i - 1] = (s < LSP - 1) ? 0.0 : mdiv(Cc * Bc, h1v, yh1);
-    }
-    __syncthreads();
-    for (int i = threadIdx.x + 1; i <= n; i += blockDim.x) {
-      double qp = 0.0, qm = 0.0, bq = 0.0;
-      if (i >= 2 && i <= n - 1) {
-        const double Dm = sD[i - 2], Dc = sD[i - 1], Dp = sD[i];
-        const double Dhm = 0.5 * (Dm + Dc), Dhp = 0.5 * (Dc + Dp);  // PDEparabolic.f90:49
-        const double Cc = sC[i - 1];
-        const double dxi = __ldg(L1.dxi + i - 1), ydxi = __ldg(L1.ydxi + i - 1);
-        qm = mdiv(mdiv(Cc * Dhm, dxi, ydxi), __ldg(L1.dx + i), __ldg(L1.ydx + i));
-        qp = mdiv(mdiv(Cc * Dhp, dxi, ydxi), __ldg(L1.dx + i + 1), __ldg(L1.ydx + i + 1));
-        bq = mdiv(sB[i - 1], __ldg(L1.dxs + i), __ldg(L1.ydxs + i));  // dx1(i+1)+dx1(i)
-      }
-      const long long q = q0 + i;
-      P.coef[(long long)s * nc + q] = qm;
-      P.coef[(long long)(LSP + s) * nc + q] = qp;
-      if (s == LSP - 1) P.coef[(long long)2 * LSP * nc + q] = bq;
-    }
-    __syncthreads();
-  }
-}
-
-template <bool UNIT>
-__global__ void __launch_bounds__(128) k_diffusion_coef(DiffArgs P) {
-  b_diffusion_coef<UNIT>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
-}
-
-template <bool UNIT>
-__device__ __forceinline__ void b_diffusion(const DiffArgs& P, const VB vb) {
-  extern __shared__ double smem[];
-  const GridDev& G = P.G;
-  const Dims d = G.d;
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int M = P.M;
-  WarpMem W{smem + warp * DNA * P.Mslot * 32, smem + warp * DNA * P.Mslot * 32 + lane};
-  const int n = d.lx1;
-  const double dt = *P.dtp;
-  const long long ncs = (long long)d.lx2 * d.lx3 * LSP;
-  const long long nc = nci(d);
-  const int wpb = blockDim.x >> 5;
-  // coalesced pass: row index idx = 32c + lane lives in the slot (lane idx/M, row idx%M)
-  const int lp0 = lane / M, kp0 = lane - lp0 * M, q32 = 32 / M, r32 = 32 - q32 * M;
-  for (long long cs = (long long)vb.bx * wpb + warp; cs < ncs; cs += (long long)vb.gx * wpb) {
-    const int s = (int)(cs % LSP);
-    const int col = (int)(cs / LSP);
-    const int i2 = col % d.lx2 + 1, i3 = col / d.lx2 + 1;
-    const long long m0 = gi(d, 0, i2, i3);  // m0 + i = cell (i, i2, i3)
-    const long long mm0 = cmi(G, 0, i2, i3);
-    const long long q0 = ci(d, 1, i2, i3) - 1;  // q0 + i: (i, i2, i3) in the interior-only arrays
-    const double* Tcol = P.B.Ts(s) + m0;
-    const double* ncol = P.B.ns(s) + m0;
-    // ---- T and the band factors q-, q+, bq (k_diffusion_coef), read along x1
-    // Dirichlet values (diffusion.f90:54-79), loaded early
-    const double tn1 = __ldg(P.Tn + ci(d, 1, i2, i3)), tnl = __ldg(P.Tn + ci(d, n, i2, i3));
-    const double tinf = P.Ttop ? __ldg(P.Ttop + (i2 - 1) + (long long)d.lx2 * (i3 - 1)) : P.Teinf;
-    int lp = lp0, kp = kp0;
-    // global -> shared by cp.async, every chunk's copies in flight together (zero fill for
-    // the padding rows past n and for bq of the ions)
-#pragma unroll 4
-    for (int c = 0; c < M; ++c) {
-      const int i = 1 + 32 * c + lane;
-      const bool in = i <= n;
-      const long long q = q0 + (in ? i : 1);
-      cp_async8z(&W.at_lane(DA_T, kp, lp), Tcol + (in ? i : 1), in);
-      cp_async8z(&W.at_lane(DA_QM, kp, lp), P.coef + (long long)s * nc + q, in);
-      cp_async8z(&W.at_lane(DA_QP, kp, lp), P.coef + (long long)(LSP + s) * nc + q, in);
-      cp_async8z(&W.at_lane(DA_BQ, kp, lp), P.coef + (long long)2 * LSP * nc + q, in && s == LSP - 1);
-      kp += r32;
-      lp += q32;
-      if (kp >= M) {
-        kp -= M;
-        ++lp;
-      }
-    }
-    cp_async_commit();
-    cp_async_wait<0>();
-    __syncwarp();
-    const double Tprev = __shfl_up_sync(0xffffffffu, W.at(DA_T, M - 1), 1);
-    const double Tnext = __shfl_down_sync(0xffffffffu, W.at(DA_T, 0), 1);
-    // Dirichlet values (diffusion.f90:54-79)
-    double tmin, tmax;
-    {
-      // the exospheric side: Teinf, or the per-column value when one is set
-      if (G.gridflag == 0) { tmin = tn1; tmax = tnl; }
-      else if (G.gridflag == 1) { tmin = tinf; tmax = tnl; }
-      else { tmin = tn1; tmax = tinf; }
-    }
-    auto Tat = [&](int k) -> double {
-      if (k < 0) return Tprev;
-      if (k >= M) return Tnext;
-      return W.at(DA_T, k);
-    };
-    // identity rows: Dirichlet rows 1 and lx1 (PDEparabolic.f90:59-63, 131-136) and padding
-    // Dirichlet rows i = 1 and i = n and the padding rows past n are identity rows
-    auto ident_rhs = [&](int i) -> double { return (i == 1) ? tmin : (i == n) ? tmax : 0.0; };
-    // fused store phase: ns (for T2rhoe) staged by cp.async into the T rows once T is dead
-    // (after the last right-hand side), its copies in flight during the last stage's solve
-    auto stage_ns = [&]() {
-      if (!P.fused) return;
-      __syncwarp();  // every lane is done reading its T rows
-      int lq = lp0, kq = kp0;
-      for (int c = 0; c < M; ++c) {
-        const int i = 1 + 32 * c + lane;
-        const bool in = i <= n;
-        cp_async8z(&W.at_lane(DA_T, kq, lq), ncol + (in ? i : 1), in);
-        kq += r32;
-        lq += q32;
-        if (kq >= M) {
-          kq -= M;
-          ++lq;
-        }
-      }
-      cp_async_commit();
-    };
-    if (P.solver == 2) {
-      // TR half step (PDEparabolic.f90:66-127), A = E = 0
-      const double dt2 = dt / 2, ydt2 = 1 / (dt / 2);  // 1/(dt/2) is also the diagonal term
-      auto rowTR = [&](int k, double& a, double& b, double& c) {
-        const int i = 1 + lane * M + k;
-        if (i == 1 || i >= n) {
-          a = 0; b = 1; c = 0;
-          return;
-        }
-        const double qp = W.at(DA_QP, k), qm = W.at(DA_QM, k), bq = W.at(DA_BQ, k);
-        a = -(qm / 2) + bq / 2;
-        b = ydt2 + qp / 2 + qm / 2;
-        c = -(qp / 2) - bq / 2;
-      };
-      for (int k = 0; k < M; ++k) {
-        const int i = 1 + lane * M + k;
-        double r;
-        if (i == 1 || i >= n) {
-          r = ident_rhs(i);
-        } else {
-          const double qp = W.at(DA_QP, k), qm = W.at(DA_QM, k), bq = W.at(DA_BQ, k);
-          const double a = -(qm / 2) + bq / 2, c = -(qp / 2) - bq / 2;
-          const double Tc = W.at(DA_T, k);
-          const double Pd = qp / 2 + qm / 2;
-          r = mdiv(Tc, dt2, ydt2) - a * Tat(k - 1) - Pd * Tc - c * Tat(k + 1);
-        }
-        W.at(DA_RHS, k) = r;
-      }
-      refined_solve(W, M, lane, rowTR);
-      // BDF2 step (PDEparabolic.f90:167-202) from T and the TR solution
-      const double dt3 = dt / 3, ydt3 = 1 / (dt / 3);
-      for (int k = 0; k < M; ++k) {
-        const int i = 1 + lane * M + k;
-        double r;
-        if (i == 1 || i >= n)
-          r = ident_rhs(i);
-        else
-          r = -mdiv(1 / 3.0 * W.at(DA_T, k), dt3, ydt3) + mdiv(4 / 3.0 * W.at(DA_R, k), dt3, ydt3);
-        W.at(DA_RHS, k) = r;
-      }
-      stage_ns();
-      auto rowBDF = [&](int k, double& a, double& b, double& c) {
-        const int i = 1 + lane * M + k;
-        if (i == 1 || i >= n) {
-          a = 0; b = 1; c = 0;
-          return;
-        }
-        const double qp = W.at(DA_QP, k), qm = W.at(DA_QM, k), bq = W.at(DA_BQ, k);
-        a = -qm + bq;
-        b = ydt3 + qp + qm;
-        c = -qp - bq;
-      };
-      refined_solve(W, M, lane, rowBDF);
-    } else {
-      // backward Euler (PDEparabolic.f90:250-319)
-      const double ydt = 1 / dt;
-      for (int k = 0; k < M; ++k) {
-        const int i = 1 + lane * M + k;
-        W.at(DA_RHS, k) = (i == 1 || i >= n) ? ident_rhs(i) : mdiv(W.at(DA_T, k), dt, ydt);
-      }
-      stage_ns();
-      auto rowBE = [&](int k, double& a, double& b, double& c) {
-        const int i = 1 + lane * M + k;
-        if (i == 1 || i >= n) {
-          a = 0; b = 1; c = 0;
-          return;
-        }
-        const double qp = W.at(DA_QP, k), qm = W.at(DA_QM, k), bq = W.at(DA_BQ, k);
-        a = -qm + bq;
-        b = ydt + qp + qm;
-        c = -qp - bq;
-      };
-      refined_solve(W, M, lane, rowBE);
-    }
-    // ---- store: max(T,100) (multifluid.f90:340); fused: clean_param(3) and T2rhoe
-    // written along x1 (coalesced): row idx = 32c + lane sits in slot (idx/M, idx%M)
-    double* Tout = P.B.Ts(s) + m0;
-    if (P.fused) cp_async_wait<0>();
-    __syncwarp();
-    {
-      int lq = lp0, kq = kp0;
-#pragma unroll 4
-      for (int c = 0; c < M; ++c) {
-        const int i = 1 + 32 * c + lane;
-        if (i <= n) {
-          double T = fmax_f(W.at_lane(DA_R, kq, lq), 100.0);
-          if (P.fused) {
-            if (is_null(G, i, i2, i3)) T = 100;
-            Tout[i] = T;
-            P.B.re(s)[m0 + i] = conv_re(W.at_lane(DA_T, kq, lq), T, s);
-          } else {
-            Tout[i] = T;
-          }
-        }
-        kq += r32;
-        lq += q32;
-        if (kq >= M) {
-          kq -= M;
-          ++lq;
-        }
-      }
-    }
-    if (!P.fused && lane == 0) {
-      Tout[0] = fmax_f(tmin, 100.0);
-      Tout[n + 1] = fmax_f(tmax, 100.0);
-    }
-    __syncwarp();
-  }
-}
-
-template <bool UNIT>
-__global__ void __launch_bounds__(128) k_diffusion(DiffArgs P) {
-  b_diffusion<UNIT>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
-}
-
 // ======================================================================================
 // 7a. The diffusion with the reference's band solve (gem_diffusion_lu.cuh): one thread per
 //     (x1 column, species), a warp = 32 columns of one species.  Columns are enumerated x3
 //     fastest when the metric tables do not vary along x3 (the warp's metric loads are then
 //     one broadcast address), else x2 fastest.  Warp tasks run electrons first (their rows
-//     cost more).  Each resident warp owns a scratch slot of lx1 rows x 4 doubles x 32 lanes.
+//     cost more).  Each resident warp owns a scratch slot of lx1 rows x LU_ROW doubles x 32
+//     lanes.
 // ======================================================================================
 constexpr int LU_WPB = 4;  // warps per block
+#ifndef GEM_LU_MINB
+#define GEM_LU_MINB 4  // resident blocks per SM the register budget is sized for
+#endif
+constexpr int LU_MINB_DEFAULT = GEM_LU_MINB;
 
-// column accessor of one thread (gemd::lu_column)
+// column accessor of one thread (gemd::lu_column): four column offsets; the table base
+// addresses stay in the launch parameters (DiffArgs), so they cost no registers
 template <bool UNIT>
 struct LuAccDev {
-  const double* Tc;  // Ts(s) + m0: [i] = cell i of the column (ghosted block)
-  const double* nc;  // ns(s) + m0
-  const double *h1, *h2, *h3, *yh1, *ha1, *yha1;  // cell metric tables + column offset
-  const double *n1, *n2, *n3;                     // neutral densities + (interior offset - 1)
-  const double* J1c;                              // J1 + m0
-  Line1D L;
-  double* sc;  // this lane's scratch: row i, slot k at sc[((i-1)*4 + k)*32]
-  __device__ __forceinline__ double T(int i) const { return Tc[i]; }
-  __device__ __forceinline__ double n(int i) const { return __ldg(nc + i); }
+  const DiffArgs& P;
+  long long tofs;  // Ts(s) + tofs: cell 0 of the column (ghosted block); ns(s) at nofs
+  long long nofs;
+  long long mofs;  // cell 0 in the metric tables
+  long long qofs;  // interior offset of cell 1, minus 1 (neutral densities)
+  long long jofs;  // cell 0 in J1 (ghosted)
+  double* sc;      // this lane's scratch: row i, slot k at sc[((i-1)*LU_ROW + k)*32]
+  __device__ __forceinline__ double T(int i) const { return P.B.F[tofs + i]; }
+  __device__ __forceinline__ double n(int i) const { return __ldg(P.B.F + nofs + i); }
   __device__ __forceinline__ void metrics(int i, double& a1, double& a2, double& a3, double& y1, double& ha,
                                           double& yha) const {
-    a1 = __ldg(h1 + i);
-    a2 = __ldg(h2 + i);
-    a3 = __ldg(h3 + i);
-    y1 = __ldg(yh1 + i);
-    ha = __ldg(ha1 + i);
-    yha = __ldg(yha1 + i);
+    const long long k = mofs + i;
+    a1 = __ldg(P.G.h1 + k);
+    a2 = __ldg(P.G.h2 + k);
+    a3 = __ldg(P.G.h3 + k);
+    y1 = __ldg(P.G.yh1 + k);
+    ha = __ldg(P.G.ha1_0 + k);
+    yha = __ldg(P.G.yha1_0 + k);
   }
   __device__ __forceinline__ void neutrals(int i, double& a, double& b, double& c, double& j) const {
-    a = __ldg(n1 + i);
-    b = __ldg(n2 + i);
-    c = __ldg(n3 + i);
-    j = __ldg(J1c + i);
+    const long long nc = nci(P.G.d);
+    a = __ldg(P.nn + qofs + i);
+    b = __ldg(P.nn + nc + qofs + i);
+    c = __ldg(P.nn + 2 * nc + qofs + i);
+    j = __ldg(P.J1 + jofs + i);
   }
-  __device__ __forceinline__ double dx(int i) const { return __ldg(L.dx + i); }
-  __device__ __forceinline__ double ydx(int i) const { return __ldg(L.ydx + i); }
-  __device__ __forceinline__ double dxi(int i) const { return __ldg(L.dxi + i - 1); }
-  __device__ __forceinline__ double ydxi(int i) const { return __ldg(L.ydxi + i - 1); }
-  __device__ __forceinline__ double dxs(int i) const { return __ldg(L.dxs + i); }
-  __device__ __forceinline__ double ydxs(int i) const { return __ldg(L.ydxs + i); }
-  __device__ __forceinline__ double& S(int i, int k) const { return sc[((i - 1) * 4 + k) * 32]; }
+  __device__ __forceinline__ double dx(int i) const { return __ldg(P.G.L[0].dx + i); }
+  __device__ __forceinline__ double ydx(int i) const { return __ldg(P.G.L[0].ydx + i); }
+  __device__ __forceinline__ double dxi(int i) const { return __ldg(P.G.L[0].dxi + i - 1); }
+  __device__ __forceinline__ double ydxi(int i) const { return __ldg(P.G.L[0].ydxi + i - 1); }
+  __device__ __forceinline__ double dxs(int i) const { return __ldg(P.G.L[0].dxs + i); }
+  __device__ __forceinline__ double ydxs(int i) const { return __ldg(P.G.L[0].ydxs + i); }
+  // the scratch streams through L2 only (ld/st.global.cg), keeping L1 for the column inputs
+  // and the grid tables the warp re-reads
+  __device__ __forceinline__ double sld(int i, int k) const { return __ldcg(sc + ((i - 1) * gemd::LU_ROW + k) * 32); }
+  __device__ __forceinline__ void sst(int i, int k, double v) const {
+    __stcg(sc + ((i - 1) * gemd::LU_ROW + k) * 32, v);
+  }
+};
+
+// The solution's destination: max(T,100) (multifluid.f90:340) into Ts; fused with
+// clean_param(3) (null cells 100) and T2rhoe (rhoes from ns), whose inputs are loaded ahead.
+struct LuPre {
+  double nv;
+  bool nul;
+};
+struct LuStoreDev {
+  double* Tout;
+  double* re;                 // rhoes of the column (fused), else null
+  const double* nc;           // ns of the column
+  const unsigned char* nul;   // null-point flags of the column (interior offset - 1), or null
+  int s;
+  __device__ __forceinline__ LuPre pre(int i) const {
+    LuPre p;
+    p.nv = re ? __ldg(nc + i) : 0.0;
+    p.nul = nul ? nul[i] != 0 : false;
+    return p;
+  }
+  __device__ __forceinline__ void operator()(int i, double x, const LuPre& p) const {
+    double T = fmax_f(x, 100.0);
+    if (p.nul) T = 100;
+    Tout[i] = T;
+    if (re) re[i] = conv_re(p.nv, T, s);
+  }
 };
 
 // One warp task: 32 columns of one species.  slot = this warp's scratch slot (lane 0).
@@ -1982,22 +1644,8 @@ __device__ __forceinline__ void b_diffusion_lu(const DiffArgs& P, int task, doub
   const long long m0 = gi(d, 0, i2, i3);
   const long long mm0 = cmi(G, 0, i2, i3);
   const long long q0 = ci(d, 1, i2, i3) - 1;
-  const long long nc = nci(d);
-  LuAccDev<UNIT> a;
-  a.Tc = P.B.Ts(s) + m0;
-  a.nc = P.B.ns(s) + m0;
-  a.h1 = G.h1 + mm0;
-  a.h2 = G.h2 + mm0;
-  a.h3 = G.h3 + mm0;
-  a.yh1 = G.yh1 + mm0;
-  a.ha1 = G.ha1_0 + mm0;
-  a.yha1 = G.yha1_0 + mm0;
-  a.n1 = P.nn + q0;
-  a.n2 = P.nn + nc + q0;
-  a.n3 = P.nn + 2 * nc + q0;
-  a.J1c = P.J1 + m0;
-  a.L = G.L[0];
-  a.sc = slot + lane;
+
+  LuAccDev<UNIT> a{P, (long long)(4 * LSP + s) * d.ng + m0, (long long)s * d.ng + m0, mm0, q0, m0, slot + lane};
   // Dirichlet values (diffusion.f90:54-79): the exospheric side takes Teinf or the column's value
   const double tn1 = __ldg(P.Tn + ci(d, 1, i2, i3)), tnl = __ldg(P.Tn + ci(d, n, i2, i3));
   const double tinf = P.Ttop ? __ldg(P.Ttop + (i2 - 1) + (long long)d.lx2 * (i3 - 1)) : P.Teinf;
@@ -2017,22 +1665,17 @@ __device__ __forceinline__ void b_diffusion_lu(const DiffArgs& P, int task, doub
   }
   k.c0 = (c_gammas[s] - 1.0) / KB;
   k.tcoef = (s < LSP - 1) ? c_tcoef[s] : 0.0;
-  double* Tout = P.B.Ts(s) + m0;
-  // max(T,100) (multifluid.f90:340); fused: clean_param(3) null cells and T2rhoe
-  auto store = [&](int i, double x) {
-    double T = fmax_f(x, 100.0);
-    if (P.fused) {
-      if (is_null(G, i, i2, i3)) T = 100;
-      Tout[i] = T;
-      P.B.re(s)[m0 + i] = conv_re(__ldg(a.nc + i), T, s);
-    } else {
-      Tout[i] = T;
-    }
-  };
+  LuStoreDev st;
+  st.Tout = P.B.Ts(s) + m0;
+  st.re = P.fused ? P.B.re(s) + m0 : nullptr;
+  st.nc = P.B.ns(s) + m0;
+  st.nul = (P.fused && G.has_null) ? G.nullpts + (ci(d, 1, i2, i3) - 1) : nullptr;
+  st.s = s;
   if (s == LSP - 1)
-    gemd::lu_column<UNIT, true>(a, k, P.solver, store);
+    gemd::lu_column<UNIT, true>(a, k, P.solver, st);
   else
-    gemd::lu_column<UNIT, false>(a, k, P.solver, store);
+    gemd::lu_column<UNIT, false>(a, k, P.solver, st);
+  double* Tout = st.Tout;
   if (!P.fused) {
     Tout[0] = fmax_f(k.tmin, 100.0);
     Tout[n + 1] = fmax_f(k.tmax, 100.0);
@@ -2041,7 +1684,7 @@ __device__ __forceinline__ void b_diffusion_lu(const DiffArgs& P, int task, doub
 
 // plain launch: persistent warps over the warp tasks; scratch slot = the global warp index
 template <bool UNIT>
-__global__ void __launch_bounds__(32 * LU_WPB) k_diffusion_lu(DiffArgs P) {
+__global__ void __launch_bounds__(32 * LU_WPB, GEM_LU_MINB) k_diffusion_lu(DiffArgs P) {
   const int warp = threadIdx.x >> 5;
   const int gw = blockIdx.x * LU_WPB + warp;
   const int nw = gridDim.x * LU_WPB;
@@ -2097,7 +1740,8 @@ struct DiffAdjArgs {
   double* Ttop_bar;    // optional: (lx2*lx3) per species, species slowest
 };
 
-// per-row shared-memory arrays of the adjoint (row-interleaved as WarpMem).  Slots are
+// per-row shared-memory arrays of the adjoint, row-interleaved: the VNA arrays of row k of
+// every lane sit together (warp base + (k*VNA + arr)*32 + lane).  Slots are
 // reused once their first content is dead: D becomes the stage-1 solution X, Y becomes the
 // temperature cotangent TB, R carries Ybar -> lambda2 -> xbar -> lambda1, and after the
 // first-stage pass QMB / QPB / BQB hold EM / EP / the C cotangent.

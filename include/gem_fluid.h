@@ -114,7 +114,10 @@ int gem_clean_param_dev(const gem_grid* g, int iparm, double* fluidvars, void* s
 int gem_energy_diffusion_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars,
                              const double* electrovars, const gem_work* w, const double* dt,
                              void* stream);
-/* temporal_mpi.f90:86-167 dt_calc and the 1e-6 floor of dt_comm; writes *dt_out (device) */
+/* temporal_mpi.f90:86-167 dt_calc and the 1e-6 floor of dt_comm; writes *dt_out (device).
+ * The result is max(tcfl * min over cells of 1/rate, 1e-6): the reference's dt_calc has no
+ * floor (dt_comm applies it after its output clips, temporal_mpi.f90:55-66), so for a CFL step
+ * below 1e-6 s this returns the floored value. */
 int gem_dt_calc_dev(const gem_grid* g, double tcfl, const double* fluidvars, gem_work* w,
                     double* dt_out, void* stream);
 /* temporal.f90:12-49 cflcalc; writes *maxcfl_out (device) */
@@ -317,7 +320,11 @@ int gem_step_vjp_finish_dev(const gem_cfg* cfg, const gem_grid* g, gem_work* w, 
  * any stream capture.  Nothing in the scratch has to start at zero (every partial slot read
  * is written in the same call).  All calls on one device share the one scratch array, so
  * calls whose executions overlap (on different streams or host threads) race: serialise
- * them. */
+ * them.  The cached address belongs to the device's current context: after cudaDeviceReset
+ * the entry point must not be called again in that process.  The reduction runs one block per
+ * x3 plane, each scanning its plane's x2 rows in turn, so grids with few x3 planes (2-D runs
+ * have one) run far slower than gem_dt_calc_dev.  Like gem_dt_calc_dev it returns the CFL step
+ * floored at 1e-6. */
 #define GEM_DT_NOALLOC_MAX_PLANES 2048
 int gem_dt_calc_noalloc_dev(const gem_grid* g, double tcfl, const double* fluidvars, double* dt_out,
                             void* stream);
@@ -334,7 +341,7 @@ int gem_dt_calc_noalloc_dev(const gem_grid* g, double tcfl, const double* fluidv
  * move.  Tuning parameters (gem_batch_set_param) rebuild the work lists and the graph. */
 typedef struct gem_batch gem_batch;
 #define GEM_BATCH_USE_GRAPH 0  /* 1 (default): capture the step into a CUDA graph */
-#define GEM_BATCH_DIFF_WARPS 1 /* warps (columns) per diffusion block, 1..4 */
+#define GEM_BATCH_DIFF_BLOCKS 1 /* resident diffusion blocks (4 warps each) per SM, 1..4 (default 4) */
 #define GEM_BATCH_GRID_PCT 2   /* persistent grid size, % of the occupancy limit (10..400);
                                   0: one block per work item (no persistence) */
 int gem_batch_create(int n, const gem_grid* const* grids, gem_work* const* works, double* const* fluidvars,

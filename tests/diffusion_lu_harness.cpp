@@ -38,7 +38,14 @@ struct HostAcc {
   double ydxi(int i) const { return ydxi_[i - 1]; }
   double dxs(int i) const { return dxs_[i]; }
   double ydxs(int i) const { return ydxs_[i]; }
-  double& S(int i, int k) const { return sc[(i - 1) * 4 + k]; }
+  double sld(int i, int k) const { return sc[(i - 1) * gemd::LU_ROW + k]; }
+  void sst(int i, int k, double v) const { sc[(i - 1) * gemd::LU_ROW + k] = v; }
+};
+
+struct HostStore {
+  double* Tout;
+  double pre(int) const { return 0.0; }
+  void operator()(int i, double x, double) const { Tout[i] = gemd::fmax_f(x, 100.0); }
 };
 
 const double c_gammas[7] = {5.0 / 3, 7.0 / 5, 7.0 / 5, 7.0 / 5, 5.0 / 3, 5.0 / 3, 5.0 / 3};
@@ -81,7 +88,7 @@ int hd_energy_diffusion(const HDiff* h, const double* ns, double* Ts, const doub
     ydxs[j] = 1.0 / dxs[j];
   }
   for (int j = 0; j < lx1; ++j) ydxi[j] = 1.0 / h->dx1i[j];
-  std::vector<double> scr((size_t)lx1 * 4);
+  std::vector<double> scr((size_t)lx1 * gemd::LU_ROW);
   for (int s = 0; s < 7; ++s)
     for (int i3 = 1; i3 <= lx3; ++i3)
       for (int i2 = 1; i2 <= lx2; ++i2) {
@@ -118,7 +125,7 @@ int hd_energy_diffusion(const HDiff* h, const double* ns, double* Ts, const doub
         k.c0 = (c_gammas[s] - 1.0) / gemd::KB;
         k.tcoef = s < 6 ? c_tcoef[s] : 0.0;
         double* Tout = Ts + s * ng + m0;
-        auto store = [&](int i, double x) { Tout[i] = gemd::fmax_f(x, 100.0); };
+        const HostStore store{Tout};
         if (h->unit) {
           if (s == 6) gemd::lu_column<true, true>(a, k, h->solver, store);
           else gemd::lu_column<true, false>(a, k, h->solver, store);

@@ -48,21 +48,21 @@ def test_tune_keeps_the_fastest_and_caches_it(cache, monkeypatch):
     def fake_time(batch, steps=3):
         p = batch.current()
         calls.append(p)
-        return times[(p[BT.GRID_PCT], p[BT.DIFF_WARPS])]
+        return times[(p[BT.GRID_PCT], p[BT.DIFF_BLOCKS])]
 
     monkeypatch.setattr(AT, "time_steps", fake_time)
     b = FakeBatch([(96, 32, 32, True)])
     r = AT.tune(b)
     assert not r["cached"] and len(calls) == len(AT.CANDIDATES)
-    assert r["params"] == {BT.GRID_PCT: 0, BT.DIFF_WARPS: 2} and r["ms_per_step"] == 3.0
-    assert b.current() == {BT.GRID_PCT: 0, BT.DIFF_WARPS: 2}  # the winner is what stays applied
+    assert r["params"] == {BT.GRID_PCT: 0, BT.DIFF_BLOCKS: 2} and r["ms_per_step"] == 3.0
+    assert b.current() == {BT.GRID_PCT: 0, BT.DIFF_BLOCKS: 2}  # the winner is what stays applied
     stored = json.loads(cache.read_text())
-    assert stored[AT.signature(b)]["params"] == {str(BT.GRID_PCT): 0, str(BT.DIFF_WARPS): 2}
+    assert stored[AT.signature(b)]["params"] == {str(BT.GRID_PCT): 0, str(BT.DIFF_BLOCKS): 2}
     # a second batch of the same shapes: served from the cache, nothing timed
     calls.clear()
     b2 = FakeBatch([(96, 32, 32, True)])
     r2 = AT.tune(b2)
-    assert r2["cached"] and not calls and b2.current() == {BT.GRID_PCT: 0, BT.DIFF_WARPS: 2}
+    assert r2["cached"] and not calls and b2.current() == {BT.GRID_PCT: 0, BT.DIFF_BLOCKS: 2}
     # use_cache=False times again and leaves the cache alone
     r3 = AT.tune(FakeBatch([(96, 32, 32, True)]), use_cache=False)
     assert not r3["cached"] and len(calls) == len(AT.CANDIDATES)

@@ -74,7 +74,7 @@ def test_batch_params_do_not_change_results():
         b0.step()
     other = _device(insts)
     b1 = BT.Batch(other)
-    b1.set_param(BT.DIFF_WARPS, 2)
+    b1.set_param(BT.DIFF_BLOCKS, 2)
     b1.set_param(BT.GRID_PCT, 30)
     for _ in range(2):
         b1.step()
@@ -90,7 +90,7 @@ def test_batch_rejects_bad_params():
     insts = _instances()[:2]
     b = BT.Batch(_device(insts))
     with pytest.raises(_lib.GemError):
-        b.set_param(BT.DIFF_WARPS, 9)
+        b.set_param(BT.DIFF_BLOCKS, 9)
     with pytest.raises(_lib.GemError):
         b.set_param(99, 1)
 
