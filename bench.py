@@ -36,34 +36,40 @@ PHASES = ["dt_calc", "ghost_fill", "sweep_x3", "sweep_x1", "sweep_x2_epilogue", 
 
 
 def algorithmic_doubles_per_cell(unit_metrics: bool) -> dict:
-    """Minimum HBM traffic of each phase per interior cell, in 8-byte words: every input the
-    phase needs read once and every output written once.  A sweep reads 3 cell + 3 face
-    metric factors, dt_calc and the diffusion 3 cell factors; none on a unit-metric grid."""
+    """Algorithmic HBM traffic of each phase per interior cell, in 8-byte words: every input
+    read once and every output written once.  A sweep moves the 19 advected fields in and out
+    and reads 7 face velocities (45 words) plus 3 cell and 3 face metric factors; the x2 sweep
+    also writes the derived v1 and n_e; the diffusion reads T and n of 7 species, three
+    neutral densities and J1, writes T of 7 species (25 words) and reads h1, h2, h3.  The step
+    sums to 162 words per cell, 183 with metric factors (1296 / 1464 bytes).  dt_calc is timed
+    in the step but not part of that sum; its own count (T, v1, v2, v3 of 7 species and three
+    metric factors) is kept for its phase fraction."""
     ms = 0 if unit_metrics else 6
-    m3 = 0 if unit_metrics else 3
+    md = 0 if unit_metrics else 3
     return {
-        "dt_calc": 28 + m3,                  # in: Ts, vs1, vs2, vs3 (7 species each)
-        "ghost_fill": 0,                     # boundary layers only
-        "sweep_x3": 28 + ms + 20,            # in: ns, vs1, Ts, vs3 (7); out: ns (6), rhovs1, rhoes (7)
-        "sweep_x1": 26 + ms + 19,            # in: ns, rhovs1 (6), rhoes, vs1 (7); out: the 19 swept
-        "sweep_x2_epilogue": 26 + ms + 27,   # in: ns, rhovs1 (6), rhoes, vs2 (7); out: ns, vs1, Ts (7), rhovs1 (6)
-        "ghost_epilogue": 0,                 # ghost cells only
-        "diffusion": 18 + m3 + 14,           # in: Ts, ns (7), nn (3), J1; out: Ts, rhoes (7)
+        "dt_calc": 28 + md,
+        "ghost_fill": 0,
+        "sweep_x3": 45 + ms,
+        "sweep_x1": 45 + ms,
+        "sweep_x2_epilogue": 45 + ms + 2,
+        "ghost_epilogue": 0,
+        "diffusion": 25 + md,
     }
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per interior cell and launch,
-# from one ncu --set full capture of each phase's kernels on the 384x48x32 dipole case
-# (profiles/kernels_ncu_full_dipole384x48x32.md; the diffusion phase is k_diffusion_coef +
-# k_diffusion); traffic scales with the cells processed, so the full-size figure is this
-# times the cell count.  Re-measure when a kernel changes.
-NCU_TRAFFIC_BYTES_PER_CELL = {
-    "dt_calc": (134.450176e6 + 5.546752e6) / 589824,
-    "sweep_x3": (135.896064e6 + 57.693696e6) / 589824,
-    "sweep_x1": (125.113856e6 + 48.169728e6) / 589824,
-    "sweep_x2_epilogue": (134.884864e6 + 77.871616e6) / 589824,
-    "diffusion": (86.669056e6 + 32.594944e6 + 138.413568e6 + 32.928000e6) / 589824,
-}
+STEP_PHASES = ("sweep_x3", "sweep_x1", "sweep_x2_epilogue", "diffusion")  # the 162 (183) words
+
+
+def measured_traffic():
+    """DRAM bytes per interior cell and launch of each phase's kernels, from an ncu capture
+    (dram__bytes_read.sum + dram__bytes_write.sum), kept beside the profile summaries in
+    profiles/dram_bytes_per_cell.json; None when absent."""
+    p = os.path.join(ROOT, "profiles", "dram_bytes_per_cell.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:  # noqa: BLE001
+        return None
 
 
 def build_problem(lx1, lx2, lx3, seed, perturb, kind="dipole"):
@@ -297,16 +303,18 @@ def run_b200(args, world, rank, local):
     unit = g.unit_metrics
     alg = algorithmic_doubles_per_cell(unit)
     phase_ms = {PHASES[i]: float(phase[i]) for i in range(len(PHASES))}
-    dom = max((p for p in PHASES if alg.get(p, 0) > 0), key=lambda p: phase_ms[p])
+    dom = max(STEP_PHASES, key=lambda p: phase_ms[p])
     alg_bytes = alg[dom] * 8 * cells
     achieved = alg_bytes / (phase_ms[dom] / 1e3) / 1e9
     peak, peak_src = measured_hbm_peak()
-    step_bytes = sum(alg[p] for p in PHASES) * 8 * cells
+    step_bytes = sum(alg[p] for p in STEP_PHASES) * 8 * cells
     step_achieved = step_bytes / (ms_max / args.steps / 1e3) / 1e9
-    # the same step with each sweep as its own pass: 3 sweeps x (19 fields read + 19 written
-    # + 7 face velocities) + 2 epilogue writes + the diffusion's 25 = 162 doubles per cell,
-    # plus 21 metric doubles on curvilinear grids
-    unfused_bytes = 8 * (162 + (0 if unit else 21)) * cells
+    tr = measured_traffic()
+    traffic = None
+    if tr and not unit and dom in tr.get("phases", {}):
+        traffic = tr["phases"][dom] * cells
+    phase_frac = {p: alg[p] * 8 * cells / (phase_ms[p] / 1e3) / 1e9 / peak for p in PHASES
+                  if alg[p] > 0 and phase_ms[p] > 0}
 
     # end to end through the host-buffer entry point (state copied in and out each step)
     e2e = None
@@ -359,16 +367,13 @@ def run_b200(args, world, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_dict(world),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak,
-                     "traffic": (NCU_TRAFFIC_BYTES_PER_CELL[dom] * cells
-                                 if (not unit and dom in NCU_TRAFFIC_BYTES_PER_CELL) else None),
-                     "traffic_source": "ncu dram bytes of the 384x48x32 dipole launch, scaled by cells",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": (tr or {}).get("source"),
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": alg_bytes,
-                     "step_achieved_GBs": step_achieved, "step_frac": step_achieved / peak,
                      "step_algorithmic_bytes": step_bytes,
-                     "unfused_algorithmic_bytes_per_step": unfused_bytes,
-                     "unfused_frac": unfused_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak},
+                     "step_achieved_GBs": step_achieved, "step_frac": step_achieved / peak,
+                     "phase_frac": phase_frac},
         "phases_ms": phase_ms,
         "cpu_baseline": cpu,
         "e2e": e2e,
