@@ -24,7 +24,27 @@ struct Staging {
   gem_grid* grid = nullptr;
   double *F = nullptr, *A = nullptr, *E = nullptr, *dt = nullptr;
   size_t ng = 0;
+  gem_work* work = nullptr;  // the CFL reductions' work object of maxcfl_C / dt_select_C
 } g_st;
+
+void drop_staging() {
+  cudaFree(g_st.F);
+  cudaFree(g_st.A);
+  cudaFree(g_st.E);
+  cudaFree(g_st.dt);
+  if (g_st.work) gem_work_destroy(g_st.work);
+  g_st = Staging();
+}
+
+// the staging's own work object (created on first use, kept with the staging buffers)
+int staging_work(gem_grid* g, gem_work** w) {
+  if (!g_st.work) {
+    const int rc = gem_work_create(g, &g_st.work);
+    if (rc) return rc;
+  }
+  *w = g_st.work;
+  return GEM_OK;
+}
 
 void fail(int rc, const char* where) {
   g_status = rc;
@@ -43,11 +63,7 @@ size_t ghosted(gem_grid* g) {
 bool stage(gem_grid* g) {
   const size_t ng = ghosted(g);
   if (g_st.grid == g && g_st.ng == ng && g_st.F) return true;
-  cudaFree(g_st.F);
-  cudaFree(g_st.A);
-  cudaFree(g_st.E);
-  cudaFree(g_st.dt);
-  g_st = Staging();
+  drop_staging();
   if (cudaMalloc(&g_st.F, ng * 5 * LSP * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&g_st.A, ng * (2 * LSP + 9) * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&g_st.E, ng * 7 * sizeof(double)) != cudaSuccess ||
@@ -118,13 +134,7 @@ void gem_capi_bind_grid(gem_grid* g) {
 void gem_capi_forget_grid(gem_grid* g) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (g_grid == g) g_grid = nullptr;
-  if (g_st.grid == g) {
-    cudaFree(g_st.F);
-    cudaFree(g_st.A);
-    cudaFree(g_st.E);
-    cudaFree(g_st.dt);
-    g_st = Staging();
-  }
+  if (g_st.grid == g) drop_staging();
 }
 void gem_capi_set_error_mode(int record_only) { g_record = record_only ? 1 : 0; }
 int gem_capi_last_status(void) { return g_status; }
@@ -234,13 +244,102 @@ void maxcfl_C(double** fv, int* xtype, void** xC, double* dt, double* maxcfl) {
   roundtrip("maxcfl_C", g, *fv, nullptr, nullptr, BF, 0, [&]() {
     if (cudaMemcpy(g_st.dt, dt, sizeof(double), cudaMemcpyHostToDevice)) return GEM_ECUDA;
     gem_work* w = nullptr;
-    int rc = gem_work_create(g, &w);
+    int rc = staging_work(g, &w);
     if (rc) return rc;
     rc = gem_maxcfl_dev(g, g_st.F, w, g_st.dt, g_st.dt + 1, nullptr);
     if (!rc && cudaMemcpy(maxcfl, g_st.dt + 1, sizeof(double), cudaMemcpyDeviceToHost)) rc = GEM_ECUDA;
-    gem_work_destroy(w);
     return rc;
   });
+}
+
+// ---- the compression and source sub-steps (libgemini_c.f90:762-793, 852-970;
+// libgemini_mpi_c.f90:476-486): Q, Pr, Lo and the source inputs live in the work object
+
+void VNRicht_artvisc_C(double** fv, void** iv) {
+  gem_grid* g = g_grid;
+  gem_work* w = iv ? static_cast<gem_work*>(*iv) : nullptr;
+  roundtrip("VNRicht_artvisc_C", g, *fv, nullptr, nullptr, BF, 0, [&]() {
+    double* Q = nullptr;
+    if (!w) return GEM_EINVAL;
+    int rc = gem_work_substep_buffers(w, nullptr, &Q, nullptr, nullptr);
+    return rc ? rc : gem_vnricht_artvisc_dev(g, g_st.F, Q, nullptr);
+  });
+}
+
+void compression_C(double** fv, double** fav, void** iv, int* xtype, void** xC, double* dt) {
+  (void)xtype;
+  gem_grid* g = grid_of(xC);
+  gem_work* w = iv ? static_cast<gem_work*>(*iv) : nullptr;
+  roundtrip("compression_C", g, *fv, *fav, nullptr, BF | BA, BA, [&]() {
+    double* Q = nullptr;
+    if (!w) return GEM_EINVAL;
+    int rc = gem_work_substep_buffers(w, nullptr, &Q, nullptr, nullptr);
+    if (rc) return rc;
+    if (cudaMemcpy(g_st.dt, dt, sizeof(double), cudaMemcpyHostToDevice)) return GEM_ECUDA;
+    return gem_compression_dev(g, g_st.F, g_st.A, Q, g_st.dt, nullptr);
+  });
+}
+
+void RK2_global_boundary_allspec_C(int* xtype, void** xC, double** fv) {
+  (void)xtype;
+  gem_grid* g = grid_of(xC);
+  roundtrip("RK2_global_boundary_allspec_C", g, *fv, nullptr, nullptr, BF, BF,
+            [&]() { return gem_rk2_global_boundary_allspec_dev(g, g_st.F, nullptr); });
+}
+
+namespace {
+enum SrcPart { SRC_ENERGY = 1, SRC_MOMENTUM = 2, SRC_MASS = 4 };
+
+// source_loss_{energy,momentum,mass}_in (libgemini.f90:1132-1195): the rates of the part
+// (sources.f90), then its exponential time-differencing solve (multifluid.f90:474-549)
+void source_loss_c(const char* name, int parts, double** fv, double** fav, double** ev, void** iv, void** xC,
+                   double* dt) {
+  gem_grid* g = grid_of(xC);
+  gem_work* w = iv ? static_cast<gem_work*>(*iv) : nullptr;
+  roundtrip(name, g, *fv, *fav, *ev, BF | BA | BE, BF | BA, [&]() {
+    const gem_source_inputs* in = nullptr;
+    double *Q = nullptr, *Pr = nullptr, *Lo = nullptr;
+    if (!w) return GEM_EINVAL;
+    int rc = gem_work_substep_buffers(w, &in, &Q, &Pr, &Lo);
+    if (rc) return rc;
+    if (!in) return GEM_EINVAL;  // gem_work_set_sources has not run
+    if (cudaMemcpy(g_st.dt, dt, sizeof(double), cudaMemcpyHostToDevice)) return GEM_ECUDA;
+    if (parts & SRC_ENERGY) {
+      if ((rc = gem_srcs_energy_dev(g, in->nn, in->vn1, in->vn2, in->vn3, in->Tn, g_st.F, Pr, Lo, nullptr))) return rc;
+      if ((rc = gem_energy_source_loss_solve_dev(g, g_st.dt, Pr, Lo, in->Qeionize, g_st.F, g_st.A, nullptr)))
+        return rc;
+    }
+    if (parts & SRC_MOMENTUM) {
+      if ((rc = gem_srcs_momentum_dev(g, in->nn, in->vn1, in->Tn, g_st.F, g_st.E, Q, in->alt, in->g1, Pr, Lo,
+                                      nullptr)))
+        return rc;
+      if ((rc = gem_momentum_source_loss_solve_dev(g, g_st.dt, Pr, Lo, g_st.F, g_st.A, nullptr))) return rc;
+    }
+    if (parts & SRC_MASS) {
+      if ((rc = gem_srcs_continuity_dev(g, in->nn, in->vn1, in->vn2, in->vn3, in->Tn, g_st.F, Pr, Lo, nullptr)))
+        return rc;
+      if ((rc = gem_mass_source_loss_solve_dev(g, g_st.dt, Pr, Lo, in->Prionize, g_st.F, nullptr))) return rc;
+    }
+    return GEM_OK;
+  });
+}
+}  // namespace
+
+void source_loss_energy_C(double** fv, double** fav, double** ev, void** iv, int* xtype, void** xC, double* dt) {
+  (void)xtype;
+  source_loss_c("source_loss_energy_C", SRC_ENERGY, fv, fav, ev, iv, xC, dt);
+}
+void source_loss_momentum_C(double** fv, double** fav, double** ev, void** iv, int* xtype, void** xC, double* dt) {
+  (void)xtype;
+  source_loss_c("source_loss_momentum_C", SRC_MOMENTUM, fv, fav, ev, iv, xC, dt);
+}
+void source_loss_mass_C(double** fv, double** fav, double** ev, void** iv, int* xtype, void** xC, double* dt) {
+  (void)xtype;
+  source_loss_c("source_loss_mass_C", SRC_MASS, fv, fav, ev, iv, xC, dt);
+}
+void source_loss_allparams_C(double** fv, double** fav, double** ev, void** iv, int* xtype, void** xC, double* dt) {
+  (void)xtype;
+  source_loss_c("source_loss_allparams_C", SRC_ENERGY | SRC_MOMENTUM | SRC_MASS, fv, fav, ev, iv, xC, dt);
 }
 
 void dt_select_C(void** cfgC, int* xtype, void** xC, double** fv, double** fav, double* t, double* tout,
@@ -253,11 +352,10 @@ void dt_select_C(void** cfgC, int* xtype, void** xC, double** fv, double** fav, 
   roundtrip("dt_select_C", g, *fv, nullptr, nullptr, BF, 0, [&]() {
     if (!cfg) return GEM_EINVAL;
     gem_work* w = nullptr;
-    int rc = gem_work_create(g, &w);
+    int rc = staging_work(g, &w);
     if (rc) return rc;
     rc = gem_dt_calc_dev(g, cfg->tcfl, g_st.F, w, g_st.dt, nullptr);
     if (!rc && cudaMemcpy(&dtnew, g_st.dt, sizeof(double), cudaMemcpyDeviceToHost)) rc = GEM_ECUDA;
-    gem_work_destroy(w);
     return rc;
   });
   if (g_status != GEM_OK) return;

@@ -103,6 +103,13 @@ struct gem_work {
   double *vs1i, *vs2i, *vs3i, *nn, *Tn, *dt;
   double* Ttop;             // per-column exospheric temperature (lx2*lx3), or null for Teinf
   double* lu;               // band-solve scratch of k_diffusion_lu (lu_slots() slots of lx1 rows)
+  // the reference work object's sub-step contents for the host-memory *_C routines, allocated
+  // on first use: the neutral state and ionization rates (gem_work_set_sources) and the
+  // artificial viscosity Q, production and loss rates Pr, Lo
+  double* sub;
+  gem_source_inputs src;
+  int has_src;
+  double *Q, *Pr, *Lo;
   unsigned long long* acc;  // 32 slots: CFL maxima / counters
   long long nf1, nf2, nf3;
   // device staging of the host blocks for gem_fluid_adv_host
@@ -589,6 +596,10 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
   w->acc = nullptr;
   w->Ttop = nullptr;
   w->lu = nullptr;
+  w->sub = nullptr;
+  std::memset(&w->src, 0, sizeof(w->src));
+  w->has_src = 0;
+  w->Q = w->Pr = w->Lo = nullptr;
   w->F = w->A = w->E = nullptr;
   w->nF = w->nA = w->nE = 0;
   w->lx1 = d.lx1;
@@ -627,10 +638,93 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
 int gem_work_destroy(gem_work* w) {
   if (!w) return GEM_OK;
   for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);
-  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop, w->lu};
+  void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop, w->lu, w->sub};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete w;
+  return GEM_OK;
+}
+
+namespace {
+// the sub-step buffers of a work object (one allocation): Q, Pr, Lo (LSP*nc each), then the
+// source inputs nn (6*nc), vn1, vn2, vn3, Tn, alt, g1 (nc each), Prionize ((LSP-1)*nc), Qeionize (nc)
+int work_sub_alloc(gem_work* w) {
+  if (w->sub) return GEM_OK;
+  const size_t nc = (size_t)w->lx1 * w->lx2 * w->lx3;
+  const size_t n = nc * (3 * LSP + 6 + 6 + (LSP - 1) + 1);
+  if (cudaMalloc(&w->sub, n * sizeof(double)) != cudaSuccess) {
+    w->sub = nullptr;
+    return set_err(GEM_ENOMEM, "cudaMalloc of %zu doubles for the sub-step buffers failed", n);
+  }
+  double* p = w->sub;
+  w->Q = p;
+  p += LSP * nc;
+  w->Pr = p;
+  p += LSP * nc;
+  w->Lo = p;
+  p += LSP * nc;
+  double* nn = p;
+  p += 6 * nc;
+  double* v1 = p;
+  p += nc;
+  double* v2 = p;
+  p += nc;
+  double* v3 = p;
+  p += nc;
+  double* tn = p;
+  p += nc;
+  double* al = p;
+  p += nc;
+  double* g1 = p;
+  p += nc;
+  double* pri = p;
+  p += (LSP - 1) * nc;
+  double* qei = p;
+  w->src.nn = nn;
+  w->src.vn1 = v1;
+  w->src.vn2 = v2;
+  w->src.vn3 = v3;
+  w->src.Tn = tn;
+  w->src.alt = al;
+  w->src.g1 = g1;
+  w->src.Prionize = pri;
+  w->src.Qeionize = qei;
+  return GEM_OK;
+}
+}  // namespace
+
+int gem_work_set_sources(gem_work* w, const gem_source_inputs* host) {
+  if (!w || !host || !host->nn || !host->vn1 || !host->vn2 || !host->vn3 || !host->Tn || !host->alt || !host->g1 ||
+      !host->Prionize || !host->Qeionize)
+    return set_err(GEM_EINVAL, "null argument");
+  int rc = work_sub_alloc(w);
+  if (rc) return rc;
+  const size_t nc = (size_t)w->lx1 * w->lx2 * w->lx3, b = nc * sizeof(double);
+  const gem_source_inputs& d = w->src;
+  GEM_CUDA(cudaMemcpy((void*)d.nn, host->nn, 6 * b, cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy((void*)d.vn1, host->vn1, b, cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy((void*)d.vn2, host->vn2, b, cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy((void*)d.vn3, host->vn3, b, cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy((void*)d.Tn, host->Tn, b, cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy((void*)d.alt, host->alt, b, cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy((void*)d.g1, host->g1, b, cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy((void*)d.Prionize, host->Prionize, (LSP - 1) * b, cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy((void*)d.Qeionize, host->Qeionize, b, cudaMemcpyHostToDevice));
+  // the diffusion reads the same atmosphere: O, N2, O2 and Tn
+  GEM_CUDA(cudaMemcpy(w->nn, host->nn, 3 * b, cudaMemcpyHostToDevice));
+  GEM_CUDA(cudaMemcpy(w->Tn, host->Tn, b, cudaMemcpyHostToDevice));
+  w->has_src = 1;
+  return GEM_OK;
+}
+
+int gem_work_substep_buffers(gem_work* w, const gem_source_inputs** src, double** Q, double** Pr, double** Lo) {
+  if (!w) return set_err(GEM_EINVAL, "null work object");
+  int rc = work_sub_alloc(w);
+  if (rc) return rc;
+  if (src) *src = w->has_src ? &w->src : nullptr;
+  if (Q) *Q = w->Q;
+  if (Pr) *Pr = w->Pr;
+  if (Lo) *Lo = w->Lo;
   return GEM_OK;
 }
 

@@ -214,6 +214,17 @@ int gem_source_loss_allparams_dev(const gem_grid* g, double* fluidvars, double* 
                                   const double* electrovars, const gem_work* w, const gem_source_inputs* in,
                                   const double* Q, double* Pr, double* Lo, const double* dt, void* stream);
 long long gem_fluid_adv_full_scratch_doubles(const gem_grid* g);
+/* The reference's work object (gemini_work, libgemini.f90:92-129) carries the neutral
+ * atmosphere (intvars%atmos: nn, vn1..3, Tn), the ionization rates (Prionize, Qeionize), the
+ * artificial viscosity Q and the rate arrays Pr, Lo that the host-memory sub-step routines
+ * of gemini3d_fluid.h (VNRicht_artvisc_C, compression_C, source_loss_*_C) read and write.
+ * gem_work_set_sources copies those inputs (HOST memory, the layouts of gem_source_inputs)
+ * into device buffers owned by w, and also loads w's diffusion neutrals (O, N2, O2) and Tn
+ * from them; the reference fills them with neutral_atmos_winds_C and the ionization routines,
+ * which lie outside this library.  gem_work_substep_buffers returns those device buffers
+ * (src is NULL until gem_work_set_sources has run); both allocate them on first use. */
+int gem_work_set_sources(gem_work* w, const gem_source_inputs* host);
+int gem_work_substep_buffers(gem_work* w, const gem_source_inputs** src, double** Q, double** Pr, double** Lo);
 
 /* ---- device-resident time stepping --------------------------------------------------
  * The simulation clock in device memory, so that a loop of steps keeps dt on the device.

@@ -68,6 +68,26 @@ void set_global_boundaries_allspec_C(int* xtype, void** xC, double** fluidvars, 
  * resident grid only the x3 periodic self-wrap remains (mpihalo.f90:147-151) */
 void halo_allparams_C(int* xtype, void** xC, double** fluidvars, double** fluidauxvars);
 void halo_fluidvars_C(int* xtype, void** xC, double** fluidvars, double** fluidauxvars);
+/* gemini3d.h:81 -- multifluid.f90:237-268 VNRicht_artvisc via libgemini_c.f90:762-771; Q stays
+ * in the work object (intvars), as the reference keeps it in intvars%Q */
+void VNRicht_artvisc_C(double** fluidvars, void** intvars);
+/* gemini3d.h:82 -- multifluid.f90:274-302 compression via libgemini_c.f90:775-793 (reads Q) */
+void compression_C(double** fluidvars, double** fluidauxvars, void** intvars, int* xtype, void** xC, double* dt);
+/* gemini3d.h:139 -- sources_mpi.f90:68-111 RK2_global_boundary via libgemini_mpi_c.f90:476-486 */
+void RK2_global_boundary_allspec_C(int* xtype, void** xC, double** fluidvars);
+/* gemini3d.h:85-89 -- libgemini.f90:1117-1195 via libgemini_c.f90:852-970: the production and
+ * loss rates (sources.f90) and the exponential time-differencing solve (multifluid.f90:474-549)
+ * of energy, momentum, mass, or all three in that order.  They read the neutral atmosphere and
+ * the ionization rates that gem_work_set_sources loaded into the work object (intvars), and
+ * the Q that VNRicht_artvisc_C left there. */
+void source_loss_allparams_C(double** fluidvars, double** fluidauxvars, double** electrovars, void** intvars,
+                             int* xtype, void** xC, double* dt);
+void source_loss_mass_C(double** fluidvars, double** fluidauxvars, double** electrovars, void** intvars, int* xtype,
+                        void** xC, double* dt);
+void source_loss_momentum_C(double** fluidvars, double** fluidauxvars, double** electrovars, void** intvars,
+                            int* xtype, void** xC, double* dt);
+void source_loss_energy_C(double** fluidvars, double** fluidauxvars, double** electrovars, void** intvars,
+                          int* xtype, void** xC, double* dt);
 /* gemini3d.h:140 -- libgemini_mpi.f90:450-485 dt_select with temporal_mpi.f90:27-84 dt_comm
  * on one grid: dt = tcfl-limited CFL step, clipped so that t+dt does not pass tglowout (when
  * cfg->flagglow) or tout, floored at 1e-6; from the second call on, dt may at most double

@@ -116,6 +116,8 @@ def test_device_abi_rejects_bad_arguments_without_a_gpu():
         "gem_fluid_adv_full_dev": lambda: L.gem_fluid_adv_full_dev(ctypes.byref(cfg), *([None] * 9)),
         "gem_dt_select_dev": lambda: L.gem_dt_select_dev(ctypes.byref(cfg), *([None] * 6)),
         "gem_clock_advance_dev": lambda: L.gem_clock_advance_dev(None, None, None),
+        "gem_work_set_sources": lambda: L.gem_work_set_sources(None, None),
+        "gem_work_substep_buffers": lambda: L.gem_work_substep_buffers(None, None, None, None, None),
     }
     for name, call in calls.items():
         assert call() == EINVAL, name
