@@ -92,6 +92,7 @@ _SIGS = [
     ("gem_fluid_adv_full_scratch_doubles", ctypes.c_longlong, [_VP]),
     ("gem_fluid_adv_full_dev", ctypes.c_int, [ctypes.POINTER(GemCfg)] + [_VP] * 9),
     ("gem_work_set_sources", ctypes.c_int, [_VP, _VP]),
+    ("gem_work_prepare", ctypes.c_int, [_VP, _VP]),
     ("gem_work_substep_buffers", ctypes.c_int, [_VP] * 5),
     ("gem_dt_select_dev", ctypes.c_int, [ctypes.POINTER(GemCfg)] + [_VP] * 6),
     ("gem_clock_advance_dev", ctypes.c_int, [_VP] * 3),

@@ -235,6 +235,13 @@ class DiffProblem:
         self._replay(0, state, j)
         return self._backward(0, state, Ttop, j, cot)
 
+    def _drop_workspaces(self, keep: int = 0):
+        """Destroy the step adjoint workspaces beyond the first `keep`."""
+        for i in range(keep, len(self._sa or [])):
+            if self._sa[i] is not None:
+                _lib.lib().gem_step_adjoint_destroy(self._sa[i])
+                self._sa[i] = None
+
     def _workspace(self, i):
         if self._sa is None:
             self._sa = []
@@ -495,10 +502,19 @@ def _backward_cuda(P: "DiffProblem", ckpt, starts, Ttop, cot, g_top):
     have = sum(1 for h in (P._sa or []) if h is not None)
     F1 = 8 * LSP * (P.grid.lx1 + 4) * (P.grid.lx2 + 4) * (P.grid.lx3 + 4)
     need = max(0, kmax + 1 - have) * P.workspace_bytes() + 2 * kmax * 3 * F1
+    # the recompute's diffusion scratch first; the workspaces are raw cudaMalloc, which cannot
+    # use memory held in torch's cache, so release that before measuring
+    _lib.check(_lib.lib().gem_work_prepare(P.ds.work, P.dg.handle))
+    torch.cuda.empty_cache()
     free, _ = torch.cuda.mem_get_info()
-    spare = free + torch.cuda.memory_reserved() - torch.cuda.memory_allocated()
-    if P.replay_slots and need <= 0.8 * spare:
-        return _backward_cuda_slots(P, ckpt, starts, Ttop, cot, g_top, kmax + 1)
+    if P.replay_slots and need <= 0.8 * free:
+        try:
+            for i in range(kmax + 1):  # made before the pipeline starts
+                P._workspace(i)
+        except _lib.GemError:
+            P._drop_workspaces(keep=2)
+        else:
+            return _backward_cuda_slots(P, ckpt, starts, Ttop, cot, g_top, kmax + 1)
     return _backward_cuda_pingpong(P, ckpt, starts, Ttop, cot, g_top)
 
 

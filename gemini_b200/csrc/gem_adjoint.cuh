@@ -730,7 +730,7 @@ int gem_step_vjp_finish_dev(const gem_cfg* cfg, const gem_grid* g, gem_work* w, 
   da.dtp = dt;
   da.Teinf = cfg->Teinf;
   da.Ttop = w->Ttop;
-  da.lu = w->lu;
+  if ((rc = work_lu(w, g, &da.lu))) return rc;
   da.solver = cfg->diffsolvetype;
   da.fused = 1;
   if ((rc = launch_diffusion(g, da, st))) return rc;

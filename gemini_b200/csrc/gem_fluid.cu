@@ -232,6 +232,20 @@ long long lu_tasks(const Dims& d) {
 // scratch slots a grid's launches use: one per resident warp, no more than it has tasks
 long long lu_slots_for(const Dims& d) { return std::min(lu_slots(), lu_tasks(d)); }
 
+// The work object's band-solve scratch, allocated by the first diffusion launch that uses
+// the work object (the batched step uses its own; a work object only ever batched needs none).
+int work_lu(gem_work* w, const gem_grid* g, double** out) {
+  if (!w->lu) {
+    const size_t bytes = sizeof(double) * lu_slots_for(g->dev.d) * lu_slot_doubles(g->dev.d.lx1);
+    if (cudaMalloc(&w->lu, bytes) != cudaSuccess) {
+      w->lu = nullptr;
+      return set_err(GEM_ENOMEM, "cudaMalloc of %zu bytes for the diffusion's band-solve scratch failed", bytes);
+    }
+  }
+  *out = w->lu;
+  return GEM_OK;
+}
+
 int launch_diffusion_lu(const gem_grid* g, DiffArgs a, cudaStream_t st) {
   const Dims& d = g->dev.d;
   if (!a.lu) return set_err(GEM_EINVAL, "diffusion without a band-solve scratch");
@@ -618,8 +632,7 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
             {(void**)&w->nn, sizeof(double) * nc * 3},
             {(void**)&w->Tn, sizeof(double) * nc},
             {(void**)&w->dt, sizeof(double) * 4},
-            {(void**)&w->acc, sizeof(unsigned long long) * 32},
-            {(void**)&w->lu, sizeof(double) * lu_slots_for(d) * lu_slot_doubles(d.lx1)}};
+            {(void**)&w->acc, sizeof(unsigned long long) * 32}};
   for (auto& a : al) {
     if (cudaMalloc(a.p, a.bytes) != cudaSuccess) {
       gem_work_destroy(w);
@@ -715,6 +728,14 @@ int gem_work_set_sources(gem_work* w, const gem_source_inputs* host) {
   GEM_CUDA(cudaMemcpy(w->Tn, host->Tn, b, cudaMemcpyHostToDevice));
   w->has_src = 1;
   return GEM_OK;
+}
+
+int gem_work_prepare(gem_work* w, const gem_grid* g) {
+  if (!w || check_grid(g)) return set_err(GEM_EINVAL, "null argument");
+  if (w->lx1 != g->dev.d.lx1 || w->lx2 != g->dev.d.lx2 || w->lx3 != g->dev.d.lx3)
+    return set_err(GEM_EINVAL, "work object and grid sizes differ");
+  double* p = nullptr;
+  return work_lu(w, g, &p);
 }
 
 int gem_work_substep_buffers(gem_work* w, const gem_source_inputs** src, double** Q, double** Pr, double** Lo) {
@@ -876,7 +897,7 @@ int gem_energy_diffusion_dev(const gem_cfg* cfg, const gem_grid* g, double* flui
   a.dtp = dt;
   a.Teinf = cfg->Teinf;
   a.Ttop = w->Ttop;
-  a.lu = w->lu;
+  if (int rc0 = work_lu(const_cast<gem_work*>(w), g, &a.lu)) return rc0;
   a.solver = cfg->diffsolvetype;
   a.fused = 0;
   int rc = launch_diffusion(g, a, S(stream));
@@ -1068,7 +1089,7 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
   d.dtp = dt;
   d.Teinf = cfg->Teinf;
   d.Ttop = w->Ttop;
-  d.lu = w->lu;
+  if ((rc = work_lu(w, g, &d.lu))) return rc;
   d.solver = cfg->diffsolvetype;
   d.fused = 1;
   w->timer.record(6, st);

@@ -81,12 +81,50 @@ def tgrid(grid, device="cpu") -> TGrid:
                  [T(grid.h1), T(grid.h2), T(grid.h3)], hx)
 
 
+# ---- branch record ----------------------------------------------------------------------
+# The step is piecewise smooth: it branches at the limiter (minmod), the upwind choice and the
+# floors.  When BRANCHES is a list, every data-dependent branch decision of the step appends a
+# digest of its mask (the count of taken branches and a sum of fixed pseudo-random 31-bit
+# weights over them), so that two evaluations can be compared branch for branch: equal digest
+# lists mean (barring a collision of ~2^-31 per site) that both took the same branches.
+BRANCHES = None
+_WEIGHTS = {}
+
+
+def _digest(mask):
+    import torch
+
+    key = (mask.numel(), str(mask.device))
+    w = _WEIGHTS.get(key)
+    if w is None:
+        g = torch.Generator(device="cpu").manual_seed(mask.numel())
+        w = torch.randint(0, 2 ** 31, (mask.numel(),), generator=g, dtype=torch.int64).to(mask.device)
+        _WEIGHTS[key] = w
+    m = mask.reshape(-1).to(torch.int64)
+    return int(m.sum()), int((m * w).sum())
+
+
+def branch(mask):
+    """Record a branch mask (when recording) and return it."""
+    if BRANCHES is not None:
+        BRANCHES.append(_digest(mask))
+    return mask
+
+
+def floor(x, lo):
+    """torch.clamp(x, min=lo) with its branch recorded."""
+    import torch
+
+    branch(x < lo)
+    return torch.clamp(x, min=lo)
+
+
 # ---- helpers ---------------------------------------------------------------------------
 def minmod(a, b):
     import torch
 
     z = torch.zeros_like(a)
-    return torch.where(a * b <= 0.0, z, torch.where(a.abs() < b.abs(), a, b))
+    return torch.where(branch(a * b <= 0.0), z, torch.where(branch(a.abs() < b.abs()), a, b))
 
 
 def _axis(dim):  # tensor axis of direction dim in (S, X3, X2, X1)
@@ -125,7 +163,7 @@ def advec_line(f, v, dt, dx, dxi, ha1, ha2i, h1i, lx, axis):
     f_im1 = F(0, lx + 1)
     neg = f_i * v - 0.5 * v * (dxf + v / h1i * dt) * s_i
     pos = f_im1 * v + 0.5 * v * (dxf - v / h1i * dt) * s_im1
-    phi = torch.where(v < 0, neg, pos)
+    phi = torch.where(branch(v < 0), neg, pos)
     P = ha2i * phi
     upd = F(1, lx + 1) - dt * (sl(P, 1, lx + 1) - sl(P, 0, lx)) / bc(dxi) / sl(ha1, 2, lx + 2)
     return torch.cat([sl(f, 0, 2), upd, sl(f, lx + 2, lx + 4)], dim=axis)
@@ -232,10 +270,14 @@ def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf,
     # from the x2/x3 copies below)
     coeff_lo = ns[..., 3] / ns[..., 4]
     n0 = torch.minimum(coeff_lo * ns[..., 2], ns[..., 2])
+    branch(coeff_lo * ns[..., 2] < ns[..., 2])
     nm1 = torch.minimum(coeff_lo * n0, n0)
+    branch(coeff_lo * n0 < n0)
     coeff_hi = ns[..., lx1] / ns[..., lx1 - 1]
     nl1 = torch.minimum(coeff_hi * ns[..., lx1 + 1], ns[..., lx1 + 1])
+    branch(coeff_hi * ns[..., lx1 + 1] < ns[..., lx1 + 1])
     nl2 = torch.minimum(coeff_hi * nl1, nl1)
+    branch(coeff_hi * nl1 < nl1)
     n = torch.cat([nm1.unsqueeze(3), n0.unsqueeze(3), n_c, nl1.unsqueeze(3), nl2.unsqueeze(3)], dim=3)
     # rho v1 ghosts: reflection of the stale boundary faces, times n ms
     pad = lambda t: torch.nn.functional.pad(t, (2, 2, 2, 2))  # (7, lx3, lx2) -> (7, X3, X2)
@@ -274,10 +316,12 @@ def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf,
     mid = 0.5 * (v1c[..., :-1] + v1c[..., 1:])            # faces 2..lx1
     if G.gridflag == 1:
         f1 = torch.minimum(mid[..., :1], torch.zeros_like(mid[..., :1]))
+        branch(mid[..., :1] < 0)
     else:
         f1 = v1c[..., :1]
     if G.gridflag == 2:
         fN = torch.maximum(mid[..., -1:], torch.zeros_like(mid[..., -1:]))
+        branch(mid[..., -1:] > 0)
     else:
         fN = v1c[..., -1:]
     v1i = torch.cat([f1, mid, fN], dim=3)                   # (7, lx3, lx2, lx1+1)
@@ -308,7 +352,7 @@ def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf,
     re = sweep(re, 2, 0, 7)
 
     # ---- rhov12v1 (multifluid.f90:218-233)
-    v1 = rv[:6] / (ms[:6] * torch.clamp(n[:6], min=MINDENSDIV))
+    v1 = rv[:6] / (ms[:6] * floor(n[:6], MINDENSDIV))
     chrg = (n[:6] * qs[:6] * v1)
     csum = chrg[0]
     for s in range(1, 6):
@@ -316,10 +360,10 @@ def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf,
     nsum = n[0]
     for s in range(1, 6):
         nsum = nsum + n[s]
-    ve = -1 / torch.clamp(nsum, min=MINDENSDIV) / qs[6] * csum
+    ve = -1 / floor(nsum, MINDENSDIV) / qs[6] * csum
     v1 = torch.cat([v1, ve.unsqueeze(0)], 0)
     # clean_param(1): floors, electron sum, ghosts := 1e-5
-    ni = torch.clamp(n[:6], min=MINDENS)
+    ni = floor(n[:6], MINDENS)
     ne = ni[0]
     for s in range(1, 6):
         ne = ne + ni[s]
@@ -328,7 +372,7 @@ def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf,
     ghost[2:lx3 + 2, 2:lx2 + 2, 2:lx1 + 2] = False
     n = torch.where(ghost, torch.full_like(n, MINDENSDIV), n)
     # rhoe2T + clean_param(3)
-    T = torch.clamp((gam - 1) / KB * re / torch.clamp(n, min=MINDENSDIV), min=100.0)
+    T = floor((gam - 1) / KB * re / floor(n, MINDENSDIV), 100.0)
     T = torch.where(ghost, torch.full_like(T, 100.0), T)
 
     # ---- energy diffusion (multifluid.f90:309-342)
@@ -336,7 +380,7 @@ def step(G: TGrid, ns, vs1, vs2, vs3, Ts, v1i_lo, v1i_hi, nn, Tn, J1, dt, Teinf,
         T = energy_diffusion(G, n, T, J1, nn, Tn, dt, Teinf, Ttop, diffsolvetype)
     else:
         T = diffusion(n, T, Ttop)
-    T = torch.where(ghost, torch.full_like(T, 100.0), torch.clamp(T, min=100.0))
+    T = torch.where(ghost, torch.full_like(T, 100.0), floor(T, 100.0))
     return n, v1, T, v1i[..., 0], v1i[..., -1]
 
 
@@ -365,7 +409,7 @@ def energy_diffusion(G: TGrid, n, T, J1, nn, Tn, dt, Teinf, Ttop=None, diffsolve
     beta = torch.zeros_like(lam)
     beta = torch.cat([beta[:6], (5.0 / 2 * KB / ELCHRG * J1[2:lx3 + 2, 2:lx2 + 2, 2:lx1 + 2]).unsqueeze(0)], 0)
     gam = _const("gam", GAMMAS, T.device, (7, 1, 1, 1))
-    C = (gam - 1.0) / KB / torch.clamp(nc, min=MINDENSDIV) / (h1 * h2 * h3)
+    C = (gam - 1.0) / KB / floor(nc, MINDENSDIV) / (h1 * h2 * h3)
     B = C * beta / h1
     D = lam * h2 * h3 / h1
     # Dirichlet values (diffusion.f90:54-79)
@@ -430,7 +474,7 @@ def energy_diffusion(G: TGrid, n, T, J1, nn, Tn, dt, Teinf, Ttop=None, diffsolve
     rows = torch.cat([T[:, 2:lx3 + 2, 2:lx2 + 2, 0:1], lo, out, hi, T[:, 2:lx3 + 2, 2:lx2 + 2, lx1 + 3:]], -1)
     mid = torch.cat([T[:, 2:lx3 + 2, :2], rows, T[:, 2:lx3 + 2, lx2 + 2:]], 2)
     Tfull = torch.cat([T[:, :2], mid, T[:, lx3 + 2:]], 1)
-    return torch.clamp(Tfull, min=100.0)
+    return floor(Tfull, 100.0)
 
 
 def thomas(a, b, c, r):

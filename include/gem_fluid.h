@@ -68,7 +68,15 @@ int gem_version(void);
 int gem_grid_create(const gem_grid_desc* desc, gem_grid** out);
 int gem_grid_destroy(gem_grid* g);
 int gem_grid_dims(const gem_grid* g, int* lx1, int* lx2, int* lx3);
+/* The work object holds the per-grid state of the step (interface velocities, neutral inputs,
+ * dt, reductions).  The diffusion's band-solve scratch (one slot of lx1 x 8 x 32 doubles per
+ * resident warp, at most ~1 GB for 384-row columns) is allocated by the first
+ * gem_energy_diffusion_dev / gem_fluid_adv_dev call that uses the work object: make that
+ * first call before capturing these calls in a CUDA graph.  Work objects that only take part
+ * in a gem_batch never allocate it (the batch has its own). */
 int gem_work_create(const gem_grid* g, gem_work** out);
+/* allocate the work object's diffusion scratch now (before measuring free memory or capturing) */
+int gem_work_prepare(gem_work* w, const gem_grid* g);
 int gem_work_destroy(gem_work* w);
 /* copy neutral inputs (host pointers; nn (lx1,lx2,lx3,3), Tn (lx1,lx2,lx3)) */
 int gem_work_set_neutrals(gem_work* w, const double* nn, const double* Tn);
@@ -106,11 +114,13 @@ int gem_sweep_allspec_dev(const gem_grid* g, int dim, int which, double* fluidva
                           double* fluidauxvars, const gem_work* w, const double* dt, void* stream);
 /* multifluid.f90:553-688; iparm 1 density, 2 velocity, 3 temperature */
 int gem_clean_param_dev(const gem_grid* g, int iparm, double* fluidvars, void* stream);
-/* multifluid.f90:309-342 with collisions.f90:162-199 and diffusion.f90:24-152.  The
- * tridiagonal systems are eliminated without pivoting and the Dirichlet rows are exact
- * (LAPACK's partial pivoting on those identity rows adds rounding of up to ~1e-9 relative
- * in stiff columns).  Ghost cells: the x1 layers 0 and lx1+1 receive the Dirichlet
- * values, then max(T,100) over every cell. */
+/* multifluid.f90:309-342 with collisions.f90:162-199 and diffusion.f90:24-152.  Each band
+ * system (TRBDF2 stages or backward Euler, PDEparabolic.f90:19-346) is factored and solved in
+ * the operation order of the reference's LAPACK dgbsv call (dgbtf2 partial pivoting, dgbtrs
+ * and dtbsv with reference-BLAS semantics), so the result equals the reference arithmetic bit
+ * for bit, T**2.5 being the correctly rounded value.  Ghost cells: the x1 layers 0 and lx1+1
+ * receive the Dirichlet values, then max(T,100) over every cell.  The first call with a work
+ * object allocates its band-solve scratch (gem_work_create). */
 int gem_energy_diffusion_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars,
                              const double* electrovars, const gem_work* w, const double* dt,
                              void* stream);

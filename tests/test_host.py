@@ -117,6 +117,7 @@ def test_device_abi_rejects_bad_arguments_without_a_gpu():
         "gem_dt_select_dev": lambda: L.gem_dt_select_dev(ctypes.byref(cfg), *([None] * 6)),
         "gem_clock_advance_dev": lambda: L.gem_clock_advance_dev(None, None, None),
         "gem_work_set_sources": lambda: L.gem_work_set_sources(None, None),
+        "gem_work_prepare": lambda: L.gem_work_prepare(None, None),
         "gem_work_substep_buffers": lambda: L.gem_work_substep_buffers(None, None, None, None, None),
     }
     for name, call in calls.items():

@@ -67,3 +67,31 @@ def test_torch_step_matches_oracle(name, mk, kw, solver):
         else:
             err = np.max(np.abs(a - b) / np.abs(b))
         assert err < 1e-10, (name, err)
+
+
+def test_branch_record_compares_branch_decisions():
+    """The branch record of the transcription: the same inputs give the same digest list, a
+    change that flips one minmod decision gives a different one, and recording changes no
+    value."""
+    import torch
+
+    from gemini_b200 import torchstep as TS
+
+    a = torch.tensor([1.0, -2.0, 3.0, 0.5], dtype=torch.float64)
+    b = torch.tensor([2.0, 1.0, -1.0, 0.25], dtype=torch.float64)
+    TS.BRANCHES = []
+    try:
+        r1 = TS.minmod(a, b)
+        d1 = list(TS.BRANCHES)
+        TS.BRANCHES.clear()
+        r2 = TS.minmod(a.clone(), b.clone())
+        d2 = list(TS.BRANCHES)
+        TS.BRANCHES.clear()
+        a2 = a.clone()
+        a2[3] = 0.2  # |a| < |b| now at element 3
+        TS.minmod(a2, b)
+        d3 = list(TS.BRANCHES)
+    finally:
+        TS.BRANCHES = None
+    assert d1 == d2 and d1 != d3 and len(d1) == 2
+    assert torch.equal(r1, r2) and torch.equal(r1, TS.minmod(a, b))
