@@ -503,10 +503,12 @@ def _backward_cuda(P: "DiffProblem", ckpt, starts, Ttop, cot, g_top):
     F1 = 8 * LSP * (P.grid.lx1 + 4) * (P.grid.lx2 + 4) * (P.grid.lx3 + 4)
     need = max(0, kmax + 1 - have) * P.workspace_bytes() + 2 * kmax * 3 * F1
     # the recompute's diffusion scratch first; the workspaces are raw cudaMalloc, which cannot
-    # use memory held in torch's cache, so release that before measuring
+    # use memory held in torch's cache: release that only when the slots do not fit otherwise
     _lib.check(_lib.lib().gem_work_prepare(P.ds.work, P.dg.handle))
-    torch.cuda.empty_cache()
     free, _ = torch.cuda.mem_get_info()
+    if P.replay_slots and need > 0.8 * free:
+        torch.cuda.empty_cache()
+        free, _ = torch.cuda.mem_get_info()
     if P.replay_slots and need <= 0.8 * free:
         try:
             for i in range(kmax + 1):  # made before the pipeline starts
