@@ -608,8 +608,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched instances")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instance measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
-    ap.add_argument("--batched-adjoint", action="store_true",
-                    help="also measure the batched adjoint workload (32 instances x 200 steps; minutes)")
+    ap.add_argument("--no-batched-adjoint", action="store_true",
+                    help="skip the batched adjoint workload (32 instances x 200 steps, about a minute)")
     ap.add_argument("--lx", type=int, nargs=3, default=None, metavar=("LX1", "LX2", "LX3"),
                     help="override the grid size (profiling runs on a smaller case)")
     ap.add_argument("--adjoint-only", action="store_true",
@@ -640,7 +640,7 @@ def main():
         import torch
         torch.cuda.empty_cache()
         line["adjoint"] = run_adjoint(args)
-    if args.batched_adjoint and rank == 0:
+    if not args.no_batched_adjoint and not args.lx and rank == 0:
         import torch
         torch.cuda.empty_cache()
         line["batched_adjoint"] = run_batched_adjoint(args)
