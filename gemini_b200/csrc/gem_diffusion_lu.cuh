@@ -205,10 +205,14 @@ struct LuState {
 };
 
 // One dgbtf2/dgbtrs step with the original row j+1 = (s, d, e | r); writes U(j) and y(j).
+// U(j,j+2) is nonzero only on interchanged rows, so it is stored only from the first
+// interchange of the column on (fs: that row, n+1 while there is none); the back
+// substitution uses +0.0, the value an uninterchanged row holds, for the rows before it.
 template <class Acc>
-GEMD_HD void lu_step(const Acc& a, int j, LuState& st, double s, double d, double e, double r) {
+GEMD_HD void lu_step(const Acc& a, int j, LuState& st, int& fs, double s, double d, double e, double r) {
   double u0, u1, u2, y, m;
   if (fabs_f(s) > fabs_f(st.p)) {  // IDAMAX takes row j+1: interchange (DSWAP)
+    if (fs > j) fs = j;
     u0 = s;
     u1 = d;
     u2 = e;
@@ -230,7 +234,7 @@ GEMD_HD void lu_step(const Acc& a, int j, LuState& st, double s, double d, doubl
   }
   a.sst(j, 0, u0);
   a.sst(j, 1, u1);
-  a.sst(j, 2, u2);
+  if (j >= fs) a.sst(j, 2, u2);
   a.sst(j, 3, y);
 }
 
@@ -241,7 +245,7 @@ constexpr int LU_ROW = 8;  // scratch slots per row
 
 // Forward pass of the first stage (TR half step, or the backward-Euler step) over rows
 // 1..n: forms every band row from T and n, eliminates, stores the factor rows (and, for
-// TR, the row factors for the BDF2 stage).  Software-pipelined: each iteration forms row
+// TR, the row factors for the BDF2 stage); returns the first interchanged row (n+1: none).  Software-pipelined: each iteration forms row
 // i+1 (conductivities, factors, band row -- independent of the elimination) next to the
 // elimination step of row i, and the cell inputs are loaded two rows ahead of their use.
 struct BandRow {
@@ -249,7 +253,7 @@ struct BandRow {
 };
 
 template <bool UNIT, bool ELEC, int STG, class Acc>
-GEMD_HD void lu_forward_first(const Acc& a, const LuK& k) {
+GEMD_HD int lu_forward_first(const Acc& a, const LuK& k) {
   const int n = k.n;
   const double dt = k.dt;
   const double dt2 = dt / 2, ydt2 = 1 / (dt / 2);
@@ -306,23 +310,23 @@ GEMD_HD void lu_forward_first(const Acc& a, const LuK& k) {
     return w;
   };
   LuState st{1.0, 0.0, k.tmin};  // row 1: identity, right-hand side Tsminx1
+  int fs = n + 1;
   BandRow w = form(2);
   for (int j = 1; j < n; ++j) {
     const BandRow cur = w;  // row j+1
     if (j + 2 <= n) w = form(j + 2);
-    lu_step(a, j, st, cur.s, cur.d, cur.e, cur.r);
+    lu_step(a, j, st, fs, cur.s, cur.d, cur.e, cur.r);
   }
-  a.sst(n, 0, st.p);
-  a.sst(n, 1, 0.0);
-  a.sst(n, 2, 0.0);
+  a.sst(n, 0, st.p);  // U(n,n+1), U(n,n+2) lie outside the matrix: never read
   a.sst(n, 3, st.b);
+  return fs;
 }
 
 // Forward pass of the BDF2 stage: the rows from the stored q-, q+, bq, the TR solution in
 // y(i) and T (all loaded two rows ahead; row r's slots 0-3 are rewritten only when row r+1
-// is brought in, after row r's TR value was read).
+// is brought in, after row r's TR value was read).  Returns the first interchanged row.
 template <bool ELEC, class Acc>
-GEMD_HD void lu_forward_bdf2(const Acc& a, const LuK& k) {
+GEMD_HD int lu_forward_bdf2(const Acc& a, const LuK& k) {
   const int n = k.n;
   const double dt3 = k.dt / 3, ydt3 = 1 / (k.dt / 3);
   struct RowIn {
@@ -358,20 +362,21 @@ GEMD_HD void lu_forward_bdf2(const Acc& a, const LuK& k) {
     return w;
   };
   LuState st{1.0, 0.0, k.tmin};
+  int fs = n + 1;
   BandRow w = form(2);
   for (int j = 1; j < n; ++j) {
     const BandRow cur = w;  // row j+1
     if (j + 2 <= n) w = form(j + 2);
-    lu_step(a, j, st, cur.s, cur.d, cur.e, cur.r);
+    lu_step(a, j, st, fs, cur.s, cur.d, cur.e, cur.r);
   }
   a.sst(n, 0, st.p);
-  a.sst(n, 1, 0.0);
-  a.sst(n, 2, 0.0);
   a.sst(n, 3, st.b);
+  return fs;
 }
 
-// dtbsv back substitution from row n down to row 1.  OUT.pre(i) loads what OUT needs for row
-// i; OUT(i, x, pre) receives the solution.  Factor rows and OUT's inputs are loaded
+// dtbsv back substitution from row n down to row 1 (fs: the forward pass's first
+// interchanged row; U(i,i+2) = +0.0 above it).  OUT.pre(i) loads what OUT needs for row i;
+// OUT(i, x, pre) receives the solution.  Factor rows and OUT's inputs are loaded
 // GEMD_BWD_DEPTH rows ahead of their use.
 struct RowF {
   double u0, u1, u2, y;
@@ -381,13 +386,13 @@ struct RowF {
 #endif
 
 template <class Acc, class Out>
-GEMD_HD void lu_backward(const Acc& a, int n, const Out& out) {
+GEMD_HD void lu_backward(const Acc& a, int n, int fs, const Out& out) {
   using Pre = decltype(out.pre(1));
   auto row = [&](int i) {
     RowF r;
     r.u0 = a.sld(i, 0);
-    r.u1 = a.sld(i, 1);
-    r.u2 = a.sld(i, 2);
+    r.u1 = i < n ? a.sld(i, 1) : 0.0;
+    r.u2 = (i >= fs && i < n - 1) ? a.sld(i, 2) : 0.0;
     r.y = a.sld(i, 3);
     return r;
   };
@@ -441,14 +446,15 @@ struct StoreTR {
 template <bool UNIT, bool ELEC, class Acc, class Out>
 GEMD_HD void lu_column(const Acc& a, const LuK& k, int solver, const Out& out) {
   const int n = k.n;
+  int fs;
   if (solver == 2) {
-    lu_forward_first<UNIT, ELEC, ST_TR>(a, k);
-    lu_backward(a, n, StoreTR<Acc>{a});
-    lu_forward_bdf2<ELEC>(a, k);
+    fs = lu_forward_first<UNIT, ELEC, ST_TR>(a, k);
+    lu_backward(a, n, fs, StoreTR<Acc>{a});
+    fs = lu_forward_bdf2<ELEC>(a, k);
   } else {
-    lu_forward_first<UNIT, ELEC, ST_BE>(a, k);
+    fs = lu_forward_first<UNIT, ELEC, ST_BE>(a, k);
   }
-  lu_backward(a, n, out);
+  lu_backward(a, n, fs, out);
 }
 
 }  // namespace gemd
