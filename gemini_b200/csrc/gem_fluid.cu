@@ -429,12 +429,12 @@ int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
       ydxs[j] = 1.0 / dxs[j];
     }
     for (int j = 0; j < l; ++j) ydxi[j] = 1.0 / dxi[j];
-    if (dd == 0) {  // the diffusion's exact quotients assume these reciprocals are in range
+    if (l > 1) {  // the exact quotients of the sweeps and the diffusion assume these are in range
       bool ok = true;
-      for (int j = 2; j <= l; ++j) ok = ok && y_in_range(ydx[j]);
-      for (int j = 1; j <= l - 2; ++j) ok = ok && y_in_range(ydxi[j]);
-      for (int j = 2; j <= l - 1; ++j) ok = ok && y_in_range(ydxs[j]);
-      if (!ok) rc = set_err(GEM_EINVAL, "x1 grid spacings outside [2^-400, 2^400]");
+      for (int j = 0; j <= l + 2; ++j) ok = ok && y_in_range(ydx[j]);
+      for (int j = 0; j <= l - 1; ++j) ok = ok && y_in_range(ydxi[j]);
+      for (int j = 0; j <= l + 1; ++j) ok = ok && y_in_range(ydxs[j]);
+      if (!ok) rc = set_err(GEM_EINVAL, "x%d grid spacings (ghosts included) outside [2^-400, 2^400]", dd + 1);
     }
     Line1D& L = G.L[dd];
     cp(dx.data(), dx.size(), &L.dx);
@@ -476,14 +476,15 @@ int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
       y1[k] = 1.0 / a1[k];
       yh1[k] = 1.0 / h1[k];
     }
-    {  // interior cells: the diffusion's exact quotients assume these reciprocals are in range
+    {  // interior cells: the exact quotients of the sweeps and the diffusion assume these
+       // reciprocals are in range
       bool ok = true;
       const int n3 = inv ? 1 : lx3;
       for (int i3 = 1; i3 <= n3 && ok; ++i3)
         for (int i2 = 1; i2 <= lx2 && ok; ++i2)
           for (int i1 = 1; i1 <= lx1; ++i1) {
             const size_t k = (size_t)((i1 + 1) + s2 * (i2 + 1) + (inv ? 0 : s3 * (i3 + 1)));
-            ok = ok && y_in_range(y0[k]) && y_in_range(yh1[k]);
+            ok = ok && y_in_range(y0[k]) && y_in_range(y1[k]) && y_in_range(yh1[k]);
           }
       if (!ok) rc = set_err(GEM_EINVAL, "metric factors outside [2^-400, 2^400]");
     }
@@ -537,11 +538,14 @@ int gem_grid_create(const gem_grid_desc* desc, gem_grid** out) {
       const Fam& f = fam[dd];
       const size_t nfc = inv ? (size_t)(f.e1 * f.e2) : (size_t)(f.e1 * f.e2 * f.e3);
       std::vector<double> p0(nfc), p1(nfc), hc(f.hc, f.hc + nfc), yhc(nfc);
+      bool ok = true;
       for (size_t k = 0; k < nfc; ++k) {
         p0[k] = f.ha[k] * f.hb[k];
         p1[k] = f.ha[k] * f.ha[k] * f.hb[k];
         yhc[k] = 1.0 / hc[k];
+        ok = ok && y_in_range(yhc[k]);
       }
+      if (!ok) rc = set_err(GEM_EINVAL, "x%d face metric factors outside [2^-400, 2^400]", dd + 1);
       FaceTab& T = G.F[dd];
       T.t1 = 1;
       T.t2 = f.e1;

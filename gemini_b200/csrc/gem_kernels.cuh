@@ -134,18 +134,18 @@ __device__ __forceinline__ double ldm(const double* p, long long k) {
 // a/b from y = RN(1/b) with one exact correction (Markstein's theorem): q0 = RN(a*y),
 // r = a - b*q0 (exact with fma), q = RN(q0 + r*y) equals the IEEE quotient RN(a/b) as long
 // as nothing over- or underflows, which |a| in (2^-500, 2^500) and |y| in [2^-400, 2^400]
-// guarantee (q0 and the remainder stay normal).  Both ranges are tested on the exponent
-// bits (integer pipe).  A zero numerator returns q0 = a*y, the correctly signed zero of
-// a/b; anything else out of range takes the IEEE division.
+// guarantee (q0 and the remainder stay normal).  Every y mdiv receives comes from a grid
+// table that gem_grid_create has checked to lie in [2^-400, 2^400] (or is 1), so only the
+// numerator's exponent is tested (integer pipe).  A zero numerator returns q0 = a*y, the
+// correctly signed zero of a/b; anything else out of range takes the IEEE division.
 __device__ __noinline__ double slow_div(double a, double b) { return a / b; }
 __device__ __forceinline__ double mdiv(double a, double b, double y) {
   const double q0 = a * y;
   const double r = __fma_rn(-q0, b, a);
   const double q1 = __fma_rn(r, y, q0);
   const unsigned ha = (unsigned)__double2hiint(a) & 0x7fffffffu;
-  const unsigned hy = (unsigned)__double2hiint(y) & 0x7fffffffu;
-  if ((ha - (523u << 20) < (1000u << 20)) & (hy - (623u << 20) < (800u << 20))) return q1;
-  if (a == 0.0 && (hy - (623u << 20) < (800u << 20))) return q0;
+  if (ha - (523u << 20) < (1000u << 20)) return q1;
+  if (a == 0.0) return q0;
   return slow_div(a, b);
 }
 
@@ -1068,7 +1068,13 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
 }
 
 template <int DIM, bool UNIT, bool FUSED>
-__global__ void __launch_bounds__(224, 2) k_sweep_march(SweepArgs P) {
+#ifndef GEM_MARCH_MINB
+#define GEM_MARCH_MINB 2
+#endif
+#ifndef GEM_X1_MINB
+#define GEM_X1_MINB 3
+#endif
+__global__ void __launch_bounds__(224, GEM_MARCH_MINB) k_sweep_march(SweepArgs P) {
   b_sweep_march<DIM, UNIT, FUSED>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
 }
 
@@ -1259,7 +1265,7 @@ __device__ __forceinline__ void b_sweep_x1(const SweepArgs& P, const VB vb) {
 }
 
 template <bool UNIT, bool FUSED>
-__global__ void __launch_bounds__(224, 3) k_sweep_x1(SweepArgs P) {
+__global__ void __launch_bounds__(224, GEM_X1_MINB) k_sweep_x1(SweepArgs P) {
   b_sweep_x1<UNIT, FUSED>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
 }
 
@@ -2512,6 +2518,13 @@ __global__ void __launch_bounds__(256, 3) k_sweep_vjp_x1(SweepVjpArgs P, SweepVj
 // ======================================================================================
 // 8. CFL time step (temporal_mpi.f90:86-167), max CFL (temporal.f90:12-49), finiteness
 // ======================================================================================
+#ifndef GEM_DT_UNROLL
+#define GEM_DT_UNROLL 2
+#endif
+#ifndef GEM_DT_MINB
+#define GEM_DT_MINB 4
+#endif
+constexpr int kDtUnroll = GEM_DT_UNROLL;  // x1 cells per thread in flight
 // Rates are >= 0, so their IEEE bit patterns order like unsigned integers and the block
 // maxima combine with 64-bit atomicMax; max is exact, so the result is independent of the
 // reduction order and equals the reference's sequential loop.
@@ -2538,7 +2551,7 @@ __device__ __forceinline__ void b_dt_reduce(const GridDev& G, const Blocks& B, u
     const long long m0 = cmi(G, 0, i2, i3);
     const double dx2i = __ldg(G.L[1].dxi + i2 - 1), ydx2i = __ldg(G.L[1].ydxi + i2 - 1);
     const double dx3i = __ldg(G.L[2].dxi + i3 - 1), ydx3i = __ldg(G.L[2].ydxi + i3 - 1);
-#pragma unroll 2
+#pragma unroll kDtUnroll
     for (int i1 = lane + 1; i1 <= d.lx1; i1 += 32) {
       const long long k = k0 + i1;
       // dl = dxi*h (multifluid.f90:764-770), tabulated per cell with its reciprocal
@@ -2618,7 +2631,7 @@ __device__ __forceinline__ void b_dt_reduce(const GridDev& G, const Blocks& B, u
 }
 
 template <bool UNIT, int MODE /*0 gridrates, 1 maxcfl*/>
-__global__ void __launch_bounds__(32 * LSP, 4) k_dt_reduce(GridDev G, Blocks B, unsigned long long* acc /*3*LSP*/,
+__global__ void __launch_bounds__(32 * LSP, GEM_DT_MINB) k_dt_reduce(GridDev G, Blocks B, unsigned long long* acc /*3*LSP*/,
                                                         const double* dtp) {
   b_dt_reduce<UNIT, MODE>(G, B, acc, dtp, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
 }

@@ -200,3 +200,25 @@ def test_host_entry_point_matches_device():
     assert np.array_equal(ga.fluidvars, h.fluidvars)
     assert np.array_equal(ga.fluidauxvars[..., :2 * 7], h.fluidauxvars[..., :2 * 7])
     assert np.array_equal(h.fluidauxvars[..., 2 * 7:], mhd)
+
+
+@pytest.mark.parametrize("field,where", [("dx2", (0,)), ("dx3", (-1,)), ("dx1", (3,)), ("h1x1i", (5, 2, 1)),
+                                         ("h3", (4, 3, 3))])
+def test_grid_with_reciprocal_out_of_exact_range_is_rejected(field, where):
+    """The sweeps' and the diffusion's exact quotients take every grid reciprocal from tables
+    checked at grid creation to lie in [2^-400, 2^400] (ghost spacings included); a grid
+    with one entry outside is refused with GEM_EINVAL instead of dividing inexactly."""
+    import copy
+
+    from gemini_b200 import _lib
+    from gemini_b200 import grid as G
+
+    g = G.dipole_grid(12, 6, 5)
+    bad = copy.deepcopy(g)
+    a = np.array(getattr(bad, field), dtype=np.float64, copy=True)
+    a[where] = 1e-200  # its reciprocal (or that of a product with it) exceeds 2^400 ~ 2.6e120
+    setattr(bad, field, a)
+    F.DeviceGrid(g).close()
+    with pytest.raises(_lib.GemError) as e:
+        F.DeviceGrid(bad)
+    assert e.value.code == 1  # GEM_EINVAL
