@@ -103,7 +103,7 @@ __global__ void ka_post_fwd(GridDev G, const double* __restrict__ F, double* nou
         nv = ne;
       }
       nout[s * ng + k] = nv;
-      const double T = (c_gammas[s] - 1) / KB * re[s * ng + k] / fmax_f(nv, MINDENSDIV);
+      const double T = c_gm1kb[s] * re[s * ng + k] / fmax_f(nv, MINDENSDIV);
       Tpre[s * ng + k] = fmax_f(T, 100.0);
     }
   });
@@ -139,7 +139,7 @@ __global__ void ka_finish_fwd(GridDev G, const double* __restrict__ F, Blocks B)
       npost = npost + fmax_f(n, MINDENS);
       double nc = fmax_f(n, MINDENS);
       if (nul) nc = (s == 0) ? MINDENSNULL * 1e-2 : MINDENSNULL;
-      double T = fmax_f((c_gammas[s] - 1) / KB * e / fmax_f(nc, MINDENSDIV), 100.0);
+      double T = fmax_f(c_gm1kb[s] * e / fmax_f(nc, MINDENSDIV), 100.0);
       if (nul) T = 100;
       B.ns(s)[k] = nc;
       B.rv(s)[k] = r;
@@ -147,9 +147,9 @@ __global__ void ka_finish_fwd(GridDev G, const double* __restrict__ F, Blocks B)
       B.Ts(s)[k] = T;
     }
     const int s = LSP - 1;
-    const double ve = -1 / fmax_f(npre, MINDENSDIV) / c_qs[LSP - 1] * chrg;
+    const double ve = mdiv(-1 / fmax_f(npre, MINDENSDIV), QE, YQE) * chrg;
     const double ne = nul ? MINDENSNULL : npost;
-    double T = fmax_f((c_gammas[s] - 1) / KB * fre[s * ng + k] / fmax_f(ne, MINDENSDIV), 100.0);
+    double T = fmax_f(c_gm1kb[s] * fre[s * ng + k] / fmax_f(ne, MINDENSDIV), 100.0);
     if (nul) T = 100;
     B.ns(s)[k] = ne;
     B.vs1(s)[k] = nul ? 0.0 : ve;
@@ -208,10 +208,10 @@ __global__ void __launch_bounds__(256) ka_post_vjp(GridDev G, const double* __re
     // energy: T = max((gamma-1)/kB re / max(n_out, 1e-5), 100), n_out the floored density
     auto energy = [&](int s, double nout) -> double {  // returns the cotangent of n_out
       const double D = fmax_f(nout, MINDENSDIV);
-      const double Tr = (c_gammas[s] - 1) / KB * re[s * ng + k] / D;  // as the forward: the floor test
+      const double Tr = c_gm1kb[s] * re[s * ng + k] / D;  // as the forward: the floor test
       const double Tb = (Tr >= 100.0) ? TPb[s * ng + k] : 0.0;
       const double TbyD = Tb / D;
-      cre[s * ng + k] = TbyD * ((c_gammas[s] - 1) / KB);
+      cre[s * ng + k] = TbyD * (c_gm1kb[s]);
       double nb = nbo[s * ng + k] + NDb[s * ng + k];
       if (nout >= MINDENSDIV) nb += -TbyD * Tr;
       return nb;

@@ -166,6 +166,18 @@ int launch_sweep_t(const gem_grid* g, SweepArgs a, int nsp, cudaStream_t st) {
   }
   // one thread per (x2 or x3 line, species), 32 adjacent x1 per warp
   dim3 grid((d.lx1 + 31) / 32, (DIM == 3) ? d.lx2 : d.lx3);
+  if (DIM == 3 && FUSED) {  // periodicity as a template parameter
+    const bool per = g->dev.flagper != 0;
+    if (g->dev.unit) {
+      if (per) k_sweep_march<3, true, true, 1><<<grid, block, 0, st>>>(a);
+      else k_sweep_march<3, true, true, 0><<<grid, block, 0, st>>>(a);
+    } else {
+      if (per) k_sweep_march<3, false, true, 1><<<grid, block, 0, st>>>(a);
+      else k_sweep_march<3, false, true, 0><<<grid, block, 0, st>>>(a);
+    }
+    GEM_LAUNCHED("k_sweep_march");
+    return GEM_OK;
+  }
   if (g->dev.unit)
     k_sweep_march<DIM == 3 ? 3 : 2, true, FUSED><<<grid, block, 0, st>>>(a);
   else

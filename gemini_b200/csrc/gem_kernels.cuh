@@ -38,6 +38,16 @@ __constant__ double c_yms[LSP] = {1.0 / (16.0 * AMU), 1.0 / (30.0 * AMU), 1.0 / 
 __constant__ double c_qs[LSP] = {1.0 * ELCHRG, 1.0 * ELCHRG, 1.0 * ELCHRG, 1.0 * ELCHRG,
                                  1.0 * ELCHRG, 1.0 * ELCHRG, -1.0 * ELCHRG};
 __constant__ double c_gammas[LSP] = {5.0 / 3, 7.0 / 5, 7.0 / 5, 7.0 / 5, 5.0 / 3, 5.0 / 3, 5.0 / 3};
+// gammas-1, (gammas-1)/kB and the electron charge with its correctly rounded reciprocal,
+// each the IEEE value of the expression (constant-folded in double), so a kernel reading one
+// gets the bits its runtime evaluation would give
+#define GEM_G53 (5.0 / 3 - 1)
+#define GEM_G75 (7.0 / 5 - 1)
+__constant__ double c_gm1[LSP] = {GEM_G53, GEM_G75, GEM_G75, GEM_G75, GEM_G53, GEM_G53, GEM_G53};
+__constant__ double c_gm1kb[LSP] = {GEM_G53 / KB, GEM_G75 / KB, GEM_G75 / KB, GEM_G75 / KB,
+                                    GEM_G53 / KB, GEM_G53 / KB, GEM_G53 / KB};
+constexpr double QE = -1.0 * ELCHRG;
+constexpr double YQE = 1.0 / (-1.0 * ELCHRG);
 __constant__ double c_tcoef[LSP - 1] = {(double)0.1019e-12f, (double)0.0747e-12f,
                                         (double)0.0754e-12f, (double)0.0701e-12f,
                                         (double)0.1068e-12f, (double)0.3986e-12f};
@@ -190,9 +200,7 @@ struct Blocks {
 
 // v12rhov1 and T2rhoe on one value (multifluid.f90:193-214)
 __device__ __forceinline__ double conv_rv(double n, double v1, int s) { return n * c_ms[s] * v1; }
-__device__ __forceinline__ double conv_re(double n, double T, int s) {
-  return n * KB * T / (c_gammas[s] - 1);
-}
+__device__ __forceinline__ double conv_re(double n, double T, int s) { return n * KB * T / c_gm1[s]; }
 
 // ======================================================================================
 // 2. Elementwise conversions over the full ghosted arrays (multifluid.f90:179-233)
@@ -213,7 +221,7 @@ __global__ void k_rhoe2T(Blocks B) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < B.ng;
        k += (long long)gridDim.x * blockDim.x)
     for (int s = 0; s < LSP; ++s) {
-      const double T = (c_gammas[s] - 1) / KB * B.re(s)[k] / fmax_f(B.ns(s)[k], MINDENSDIV);
+      const double T = c_gm1kb[s] * B.re(s)[k] / fmax_f(B.ns(s)[k], MINDENSDIV);
       B.Ts(s)[k] = fmax_f(T, 100.0);
     }
 }
@@ -230,7 +238,7 @@ __global__ void k_rhov12v1(Blocks B) {
       nsum = nsum + n;
     }
     B.ns(LSP - 1)[k] = nsum;
-    B.vs1(LSP - 1)[k] = -1 / fmax_f(nsum, MINDENSDIV) / c_qs[LSP - 1] * chrg;
+    B.vs1(LSP - 1)[k] = mdiv(-1 / fmax_f(nsum, MINDENSDIV), QE, YQE) * chrg;
   }
 }
 
@@ -713,7 +721,9 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <int DIM, bool UNIT, bool FUSED>
+// PERM: the x3 periodicity of the fused x3 sweep, 0 / 1 known at compile time (the plain
+// launch: the wrap values stay out of the registers of non-periodic lines), 2 read from G
+template <int DIM, bool UNIT, bool FUSED, int PERM = 2>
 __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
   const GridDev& G = P.G;
   const Dims d = G.d;
@@ -756,7 +766,7 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
     fld[1] = fld[0]; fld[2] = fld[0];
     frank[0] = (P.which == 1) ? 1 : 0; frank[1] = frank[0]; frank[2] = frank[0];
   }
-  const bool per = G.flagper != 0;
+  const bool per = (PERM == 2) ? (G.flagper != 0) : (PERM == 1);
   auto map3 = [&](int j) -> int {  // x3 ghosts after set_global_boundaries / the self-wrap
     if (j >= 1 && j <= lx) return j;
     if (per) return (j < 1) ? j + lx : j - lx;
@@ -1030,7 +1040,7 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
         sh_t[buf][s][lane] = n * c_qs[s] * v;
         double nc = fmax_f(n, MINDENS);
         if (nul) nc = (s == 0) ? MINDENSNULL * 1e-2 : MINDENSNULL;
-        double T = fmax_f((c_gammas[s] - 1) / KB * e / fmax_f(nc, MINDENSDIV), 100.0);
+        double T = fmax_f(c_gm1kb[s] * e / fmax_f(nc, MINDENSDIV), 100.0);
         if (nul) T = 100;
         if (valid) {
           B.ns(s)[kc] = nc;
@@ -1050,9 +1060,9 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
           chrg = chrg + sh_t[buf][q][lane];
           npost = npost + fmax_f(nq, MINDENS);
         }
-        const double ve = -1 / fmax_f(npre, MINDENSDIV) / c_qs[LSP - 1] * chrg;
+        const double ve = mdiv(-1 / fmax_f(npre, MINDENSDIV), QE, YQE) * chrg;
         const double ne = nul ? MINDENSNULL : npost;
-        double T = fmax_f((c_gammas[s] - 1) / KB * outv[0] / fmax_f(ne, MINDENSDIV), 100.0);
+        double T = fmax_f(c_gm1kb[s] * outv[0] / fmax_f(ne, MINDENSDIV), 100.0);
         if (nul) T = 100;
         if (valid) {
           B.ns(s)[kc] = ne;
@@ -1067,15 +1077,15 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
   __syncwarp();
 }
 
-template <int DIM, bool UNIT, bool FUSED>
 #ifndef GEM_MARCH_MINB
 #define GEM_MARCH_MINB 2
 #endif
 #ifndef GEM_X1_MINB
 #define GEM_X1_MINB 3
 #endif
+template <int DIM, bool UNIT, bool FUSED, int PERM = 2>
 __global__ void __launch_bounds__(224, GEM_MARCH_MINB) k_sweep_march(SweepArgs P) {
-  b_sweep_march<DIM, UNIT, FUSED>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+  b_sweep_march<DIM, UNIT, FUSED, PERM>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
 }
 
 
@@ -1288,7 +1298,7 @@ __device__ __forceinline__ void b_ghost_epilogue(const GridDev& G, const Blocks&
       chrg = chrg + n * c_qs[s] * v;
       nsum = nsum + n;
     }
-    B.vs1(LSP - 1)[k] = -1 / fmax_f(nsum, MINDENSDIV) / c_qs[LSP - 1] * chrg;
+    B.vs1(LSP - 1)[k] = mdiv(-1 / fmax_f(nsum, MINDENSDIV), QE, YQE) * chrg;
     for (int s = 0; s < LSP; ++s) {
       B.ns(s)[k] = MINDENSDIV;
       B.Ts(s)[k] = 100.0;
@@ -1669,7 +1679,7 @@ __device__ __forceinline__ void b_diffusion_lu(const DiffArgs& P, int task, doub
     k.tmin = tn1;
     k.tmax = tinf;
   }
-  k.c0 = (c_gammas[s] - 1.0) / KB;
+  k.c0 = c_gm1kb[s];
   k.tcoef = (s < LSP - 1) ? c_tcoef[s] : 0.0;
   LuStoreDev st;
   st.Tout = P.B.Ts(s) + m0;
@@ -1825,7 +1835,7 @@ __global__ void __launch_bounds__(128) k_diffusion_vjp(DiffAdjArgs P) {
     const long long q0 = ci(d, 1, i2, i3) - 1;
     const double* Tc = P.T + (long long)s * d.ng + m0;
     const double* nsc = P.ns + (long long)s * d.ng + m0;
-    const double c0 = (c_gammas[s] - 1.0) / KB;
+    const double c0 = c_gm1kb[s];
     const bool el = s == LSP - 1;
     // ---- the column's inputs, global -> shared by cp.async with every chunk in flight (zero
     //      fill past n): T into T; ns, J1 and the neutral densities into the q-, q+ and
