@@ -715,7 +715,7 @@ int gem_step_vjp_finish_dev(const gem_cfg* cfg, const gem_grid* g, gem_work* w, 
   // the x2 sweep's epilogue from the replay's last stage, then the rest of gem_fluid_adv_dev
   ka_finish_fwd<<<grid_for(d.ng, 256), 256, 0, st>>>(G, A->ST + 9 * A->F, B);
   GEM_LAUNCHED("ka_finish_fwd");
-  k_ghost_epilogue<<<grid_for(d.ng, 256), 256, 0, st>>>(G, B);
+  k_ghost_epilogue<<<grid_for(ghost_cells(d), 256), 256, 0, st>>>(G, B);
   GEM_LAUNCHED("k_ghost_epilogue");
   if (G.has_null && (G.gridflag == 0 || G.gridflag == 1)) {
     k_clean_vel_edges<<<grid_for(ncol * LSP, 128), 128, 0, st>>>(G, fluidvars + LSP * d.ng);

@@ -265,7 +265,7 @@ int batch_build_lists(gem_batch* b) {
           case BK_SW3: add_items(launch_for(k, u), i, gx13, d.lx2); break;
           case BK_SW1: add_items(launch_for(k, u), i, d.lx2, d.lx3); break;
           case BK_SW2: add_items(launch_for(k, u), i, gx13, d.lx3); break;
-          case BK_EPI: add_items(launch_for(k, 0), i, grid_for(d.ng, 256)); break;
+          case BK_EPI: add_items(launch_for(k, 0), i, grid_for(ghost_cells(d), 256)); break;
           case BK_CVE:
             if (g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1))
               add_items(launch_for(k, 0), i, grid_for((long long)d.lx2 * d.lx3 * LSP, 128));

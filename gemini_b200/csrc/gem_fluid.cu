@@ -66,6 +66,12 @@ bool y_in_range(double y) {
   return h - (623u << 20) < (800u << 20);
 }
 
+// cells of the ghost shell (the ghost epilogue's work items)
+long long ghost_cells(const Dims& d) {
+  const long long a1 = d.lx1 + 4, a2 = d.lx2 + 4;
+  return 4 * (a1 * a2 + a1 * d.lx3 + (long long)d.lx2 * d.lx3);
+}
+
 unsigned grid_for(long long n, int threads, int per_sm = 8) {
   long long b = (n + threads - 1) / threads;
   const long long cap = (long long)num_sms() * per_sm;
@@ -1089,7 +1095,7 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
   w->timer.record(4, st);
   if ((rc = launch_sweep(g, 2, true, a, LSP, st))) return rc;
   w->timer.record(5, st);
-  k_ghost_epilogue<<<grid_for(g->dev.d.ng, 256), 256, 0, st>>>(g->dev, B);
+  k_ghost_epilogue<<<grid_for(ghost_cells(g->dev.d), 256), 256, 0, st>>>(g->dev, B);
   GEM_LAUNCHED("k_ghost_epilogue");
   if (g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1)) {
     const long long n = (long long)g->dev.d.lx2 * g->dev.d.lx3 * LSP;

@@ -257,6 +257,40 @@ __device__ __forceinline__ bool is_ghost(const Dims& d, int i1, int i2, int i3) 
   return i1 < 1 || i1 > d.lx1 || i2 < 1 || i2 > d.lx2 || i3 < 1 || i3 > d.lx3;
 }
 
+// The ghost shell, enumerated: the four x3 ghost planes (i1 fastest), then the four x2 ghost
+// rows of every interior x3 index, then the four x1 ghosts of every interior column --
+// nghost(d) = ng - lx1*lx2*lx3 cells, each once.
+__device__ __forceinline__ long long nghost(const Dims& d) {
+  const long long a1 = d.lx1 + 4, a2 = d.lx2 + 4;
+  return 4 * (a1 * a2 + a1 * d.lx3 + (long long)d.lx2 * d.lx3);
+}
+__device__ __forceinline__ void ghost_cell(const Dims& d, long long q, int& i1, int& i2, int& i3) {
+  const long long a1 = d.lx1 + 4, a2 = d.lx2 + 4;
+  const long long np = 4 * a1 * a2, nr = 4 * a1 * d.lx3;
+  if (q < np) {
+    const long long p = q / (a1 * a2), rem = q - p * (a1 * a2);
+    i3 = (p < 2) ? (int)p - 1 : d.lx3 + (int)p - 1;
+    i2 = (int)(rem / a1) - 1;
+    i1 = (int)(rem - (rem / a1) * a1) - 1;
+    return;
+  }
+  q -= np;
+  if (q < nr) {
+    const long long row = q / a1;
+    i1 = (int)(q - row * a1) - 1;
+    const int g = (int)(row & 3);
+    i2 = (g < 2) ? g - 1 : d.lx2 + g - 1;
+    i3 = (int)(row >> 2) + 1;
+    return;
+  }
+  q -= nr;
+  const int g = (int)(q & 3);
+  const long long col = q >> 2;
+  i1 = (g < 2) ? g - 1 : d.lx1 + g - 1;
+  i2 = (int)(col % d.lx2) + 1;
+  i3 = (int)(col / d.lx2) + 1;
+}
+
 // param: the 4-D block of ns (1), vs1 (2) or Ts (3), all lsp species
 __global__ void k_clean_elementwise(GridDev G, double* param, int iparm) {
   const Dims d = G.d;
@@ -1285,11 +1319,11 @@ __global__ void __launch_bounds__(224, GEM_X1_MINB) k_sweep_x1(SweepArgs P) {
 // 100; T2rhoe of those constants gives the final energy-density ghosts).
 __device__ __forceinline__ void b_ghost_epilogue(const GridDev& G, const Blocks& B, const VB vb) {
   const Dims d = G.d;
-  for (long long k = vb.bx * (long long)blockDim.x + threadIdx.x; k < d.ng;
-       k += (long long)vb.gx * blockDim.x) {
+  const long long ngh = nghost(d);
+  for (long long q = vb.bx * (long long)blockDim.x + threadIdx.x; q < ngh; q += (long long)vb.gx * blockDim.x) {
     int i1, i2, i3;
-    decode_cell(d, k, i1, i2, i3);
-    if (!is_ghost(d, i1, i2, i3)) continue;
+    ghost_cell(d, q, i1, i2, i3);
+    const long long k = gi(d, i1, i2, i3);
     double chrg = 0.0, nsum = 0.0;
     for (int s = 0; s < LSP - 1; ++s) {
       const double n = B.ns(s)[k];
@@ -1633,7 +1667,7 @@ struct LuStoreDev {
     double T = fmax_f(x, 100.0);
     if (p.nul) T = 100;
     Tout[i] = T;
-    if (re) re[i] = conv_re(p.nv, T, s);
+    if (re) re[i] = p.nv * KB * T / (c_gammas[s] - 1);  // T2rhoe (multifluid.f90:193-202)
   }
 };
 
@@ -1679,7 +1713,7 @@ __device__ __forceinline__ void b_diffusion_lu(const DiffArgs& P, int task, doub
     k.tmin = tn1;
     k.tmax = tinf;
   }
-  k.c0 = c_gm1kb[s];
+  k.c0 = (c_gammas[s] - 1.0) / KB;
   k.tcoef = (s < LSP - 1) ? c_tcoef[s] : 0.0;
   LuStoreDev st;
   st.Tout = P.B.Ts(s) + m0;
