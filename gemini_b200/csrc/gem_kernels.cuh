@@ -2574,6 +2574,70 @@ constexpr int kDtUnroll = GEM_DT_UNROLL;  // x1 cells per thread in flight
 // reduction order and equals the reference's sequential loop.
 // Block (32, LSP): threadIdx.y is the species, lanes run along x1, blocks stride over the
 // x1 rows (i2, i3).  Each thread keeps the three running maxima of its species.
+// The CFL rates of one interior cell and species (temporal_mpi.f90:127-150): dl = dxi*h
+// (multifluid.f90:764-770), tabulated per cell with its reciprocal; vsnd from T and Te for
+// the ions; every quotient exact (mdiv_try, else the IEEE division).  MODE 0 keeps the
+// per-direction maxima g1, g2, g3; MODE 1 (maxcfl) the largest dtv*rate in g1.
+template <bool UNIT, int MODE>
+__device__ __forceinline__ void dt_cell(const GridDev& G, long long mk, int i1, double dx2i, double ydx2i, double dx3i,
+                                        double ydx3i, int s, double T, double Te, double v1, double v2, double v3,
+                                        double dtv, double& g1, double& g2, double& g3) {
+  const double ms = c_ms[s], yms = c_yms[s];
+  double dl1, y1, dl2, y2, dl3, y3;
+  if (UNIT) {
+    dl1 = __ldg(G.L[0].dxi + i1 - 1);
+    y1 = __ldg(G.L[0].ydxi + i1 - 1);
+    dl2 = dx2i;
+    y2 = ydx2i;
+    dl3 = dx3i;
+    y3 = ydx3i;
+  } else {
+    dl1 = __ldg(G.dl[0] + mk);
+    y1 = __ldg(G.ydl[0] + mk);
+    dl2 = __ldg(G.dl[1] + mk);
+    y2 = __ldg(G.ydl[1] + mk);
+    if (G.dl3_tab) {
+      dl3 = __ldg(G.dl[2] + mk);
+      y3 = __ldg(G.ydl[2] + mk);
+    } else {
+      dl3 = dx3i * __ldg(G.h3 + mk);
+      y3 = 1.0 / dl3;
+    }
+  }
+  bool ok = true;
+  double vsnd = 0.0;
+  if (s < LSP - 1) vsnd = sqrt(mdiv_try(KB * T, ms, yms, ok) + mdiv_try(5.0 / 3.0 * KB * Te, ms, yms, ok));
+  double r1, r2, r3;
+  if (MODE == 0) {
+    r1 = mdiv_try(vsnd + fabs(v1), dl1, y1, ok);
+    r2 = mdiv_try(fabs(v2), dl2, y2, ok);
+    r3 = mdiv_try(fabs(v3), dl3, y3, ok);
+  } else {
+    r1 = mdiv_try(dtv * (vsnd + fabs(v1)), dl1, y1, ok);
+    r2 = mdiv_try(dtv * fabs(v2), dl2, y2, ok);
+    r3 = mdiv_try(dtv * fabs(v3), dl3, y3, ok);
+  }
+  if (!ok) {  // rare: a quotient outside the exact fast range
+    vsnd = 0.0;
+    if (s < LSP - 1) vsnd = sqrt(slow_div(KB * T, ms) + slow_div(5.0 / 3.0 * KB * Te, ms));
+    const double a1 = (MODE == 0) ? vsnd + fabs(v1) : dtv * (vsnd + fabs(v1));
+    const double a2 = (MODE == 0) ? fabs(v2) : dtv * fabs(v2);
+    const double a3 = (MODE == 0) ? fabs(v3) : dtv * fabs(v3);
+    r1 = slow_div(a1, dl1);
+    r2 = slow_div(a2, dl2);
+    r3 = slow_div(a3, dl3);
+  }
+  if (MODE == 0) {
+    g1 = fmax_f(r1, g1);
+    g2 = fmax_f(r2, g2);
+    g3 = fmax_f(r3, g3);
+  } else {
+    g1 = fmax_f(r1, g1);
+    g1 = fmax_f(r2, g1);
+    g1 = fmax_f(r3, g1);
+  }
+}
+
 template <bool UNIT, int MODE /*0 gridrates, 1 maxcfl*/>
 __device__ __forceinline__ void b_dt_reduce(const GridDev& G, const Blocks& B, unsigned long long* acc /*3*LSP*/,
                                                         const double* dtp, const VB vb) {
@@ -2588,7 +2652,6 @@ __device__ __forceinline__ void b_dt_reduce(const GridDev& G, const Blocks& B, u
   const double* v1p = B.vs1(s);
   const double* v2p = B.vs2(s);
   const double* v3p = B.vs3(s);
-  const double ms = c_ms[s], yms = c_yms[s];
   for (int row = vb.bx; row < nrow; row += vb.gx) {
     const int i2 = row % d.lx2 + 1, i3 = row / d.lx2 + 1;
     const long long k0 = gi(d, 0, i2, i3);
@@ -2598,62 +2661,8 @@ __device__ __forceinline__ void b_dt_reduce(const GridDev& G, const Blocks& B, u
 #pragma unroll kDtUnroll
     for (int i1 = lane + 1; i1 <= d.lx1; i1 += 32) {
       const long long k = k0 + i1;
-      // dl = dxi*h (multifluid.f90:764-770), tabulated per cell with its reciprocal
-      double dl1, y1, dl2, y2, dl3, y3;
-      if (UNIT) {
-        dl1 = __ldg(G.L[0].dxi + i1 - 1);
-        y1 = __ldg(G.L[0].ydxi + i1 - 1);
-        dl2 = dx2i;
-        y2 = ydx2i;
-        dl3 = dx3i;
-        y3 = ydx3i;
-      } else {
-        const long long mk = m0 + i1;
-        dl1 = __ldg(G.dl[0] + mk);
-        y1 = __ldg(G.ydl[0] + mk);
-        dl2 = __ldg(G.dl[1] + mk);
-        y2 = __ldg(G.ydl[1] + mk);
-        if (G.dl3_tab) {
-          dl3 = __ldg(G.dl[2] + mk);
-          y3 = __ldg(G.ydl[2] + mk);
-        } else {
-          dl3 = dx3i * __ldg(G.h3 + mk);
-          y3 = 1.0 / dl3;
-        }
-      }
-      const double T = Tsp[k], Te = Tep[k], v1 = v1p[k], v2 = v2p[k], v3 = v3p[k];
-      bool ok = true;
-      double vsnd = 0.0;
-      if (s < LSP - 1) vsnd = sqrt(mdiv_try(KB * T, ms, yms, ok) + mdiv_try(5.0 / 3.0 * KB * Te, ms, yms, ok));
-      double r1, r2, r3;
-      if (MODE == 0) {
-        r1 = mdiv_try(vsnd + fabs(v1), dl1, y1, ok);
-        r2 = mdiv_try(fabs(v2), dl2, y2, ok);
-        r3 = mdiv_try(fabs(v3), dl3, y3, ok);
-      } else {
-        r1 = mdiv_try(dtv * (vsnd + fabs(v1)), dl1, y1, ok);
-        r2 = mdiv_try(dtv * fabs(v2), dl2, y2, ok);
-        r3 = mdiv_try(dtv * fabs(v3), dl3, y3, ok);
-      }
-      if (!ok) {  // rare: a quotient outside the exact fast range
-        vsnd = 0.0;
-        if (s < LSP - 1) vsnd = sqrt(slow_div(KB * T, ms) + slow_div(5.0 / 3.0 * KB * Te, ms));
-        const double a1 = (MODE == 0) ? vsnd + fabs(v1) : dtv * (vsnd + fabs(v1));
-        const double a2 = (MODE == 0) ? fabs(v2) : dtv * fabs(v2);
-        const double a3 = (MODE == 0) ? fabs(v3) : dtv * fabs(v3);
-        r1 = slow_div(a1, dl1);
-        r2 = slow_div(a2, dl2);
-        r3 = slow_div(a3, dl3);
-      }
-      if (MODE == 0) {
-        g1 = fmax_f(r1, g1);
-        g2 = fmax_f(r2, g2);
-        g3 = fmax_f(r3, g3);
-      } else {
-        g1 = fmax_f(r1, g1);
-        g1 = fmax_f(r2, g1);
-        g1 = fmax_f(r3, g1);
-      }
+      dt_cell<UNIT, MODE>(G, m0 + i1, i1, dx2i, ydx2i, dx3i, ydx3i, s, Tsp[k], Tep[k], v1p[k], v2p[k], v3p[k], dtv, g1,
+                          g2, g3);
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
