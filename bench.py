@@ -386,6 +386,63 @@ def run_b200(args, world, rank, local):
     return line
 
 
+def run_full_step(args):
+    """fluid_adv in full (app/main.f90:280-381) on the config-1 grid: dt_calc, the step with
+    compression (VNRicht_artvisc, RK2 boundary, compression), the diffusion, and the
+    source/loss sub-step (rates and ETD solves of energy, momentum, mass), through
+    gem_fluid_adv_full_dev.  The neutral atmosphere and ionization rates are seeded
+    synthetic inputs (the reference computes them outside this path), made on the device."""
+    import torch
+
+    from gemini_b200 import fluid as F
+
+    w = WORKLOAD
+    g, st = build_problem(w["lx1"], w["lx2"], w["lx3"], w["seed"], w["perturb"])
+    dg = F.DeviceGrid(g)
+    ds = F.DeviceState.from_host(dg, st.copy())
+    cfg = F.FluidCfg(st.Teinf, 2, 0.5)
+    nc = g.lx1 * g.lx2 * g.lx3
+    gen = torch.Generator(device="cuda").manual_seed(w["seed"])
+    U = lambda lo, hi, *shape: torch.rand(*shape, dtype=torch.float64, device="cuda", generator=gen) * (hi - lo) + lo
+    # an exponential neutral atmosphere above 80 km and an ionization layer near 150 km, +-10%
+    alt = torch.from_numpy(np.ascontiguousarray(g.alt[2:-2, 2:-2, 2:-2].ravel(order="F"))).cuda()
+    z = torch.clamp(alt, min=80e3)
+    n100 = (4e17, 1e19, 2.6e18, 1e13, 1e14, 1e14)  # O, N2, O2, H, N, NO at 100 km [m^-3]
+    scale = (60e3, 40e3, 40e3, 600e3, 60e3, 40e3)
+    nn = torch.cat([n100[i] * torch.exp(-(z - 100e3) / scale[i]) * (1 + 0.1 * U(-1, 1, nc)) for i in range(6)])
+    layer = torch.exp(-((z - 150e3) / 60e3) ** 2)
+    inp = dict(nn=nn, vn1=U(-100, 100, nc), vn2=U(-100, 100, nc), vn3=U(-100, 100, nc),
+               Tn=torch.from_numpy(np.ascontiguousarray(st.Tn.ravel(order="F"))).cuda(), alt=alt,
+               g1=U(-9.8, -8.0, nc), Prionize=torch.cat([1e9 * layer * U(0.5, 1, nc) for _ in range(6)]),
+               Qeionize=1e-13 * layer * U(0.5, 1, nc))
+    inputs = F.SourceInputs.of(**inp)
+    scratch = torch.empty(F._lib.lib().gem_fluid_adv_full_scratch_doubles(ds.g), dtype=torch.float64, device="cuda")
+
+    def step():
+        dt = F.dt_calc(ds, 0.5, out=ds.dt)
+        F.fluid_adv_full(cfg, ds, dt, inputs, scratch)
+
+    for _ in range(2):
+        step()
+    K = 5
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(K):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    nonfinite = F.check_finite(ds)
+    ds.close()
+    dg.close()
+    return {"workload": "fluid_adv in full on the config-1 grid: dt_calc, advection, compression, diffusion, "
+                        "source/loss (seeded synthetic exponential neutral atmosphere and ionization layer)",
+            "ms_per_step": ms, "value": nc * LSP / (ms / 1e3) / 1e9, "unit": UNIT, "steps": K,
+            "nonfinite": nonfinite,
+            "api": "gem_dt_calc_dev + gem_fluid_adv_full_dev"}
+
+
 BATCHED = dict(instances=64, seed=2024, perturb=0.2)
 
 
@@ -608,6 +665,7 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched instances")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instance measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
+    ap.add_argument("--no-full-step", action="store_true", help="skip the full fluid_adv measurement")
     ap.add_argument("--no-batched-adjoint", action="store_true",
                     help="skip the batched adjoint workload (32 instances x 200 steps, about a minute)")
     ap.add_argument("--lx", type=int, nargs=3, default=None, metavar=("LX1", "LX2", "LX3"),
@@ -640,6 +698,10 @@ def main():
         import torch
         torch.cuda.empty_cache()
         line["adjoint"] = run_adjoint(args)
+    if not args.no_full_step and not args.lx and rank == 0:
+        import torch
+        torch.cuda.empty_cache()
+        line["full_step"] = run_full_step(args)
     if not args.no_batched_adjoint and not args.lx and rank == 0:
         import torch
         torch.cuda.empty_cache()
