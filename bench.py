@@ -694,15 +694,15 @@ def main():
         import torch
         torch.cuda.empty_cache()
         line["batched"] = run_batched(args, world, rank)
-    if not args.no_adjoint and not args.lx and rank == 0:
+    if not args.no_adjoint and not args.lx and world == 1:  # single-GPU figures, taken at N = 1
         import torch
         torch.cuda.empty_cache()
         line["adjoint"] = run_adjoint(args)
-    if not args.no_full_step and not args.lx and rank == 0:
+    if not args.no_full_step and not args.lx and world == 1:  # single-GPU figures, taken at N = 1
         import torch
         torch.cuda.empty_cache()
         line["full_step"] = run_full_step(args)
-    if not args.no_batched_adjoint and not args.lx and rank == 0:
+    if not args.no_batched_adjoint and not args.lx and world == 1:  # single-GPU figures, taken at N = 1
         import torch
         torch.cuda.empty_cache()
         line["batched_adjoint"] = run_batched_adjoint(args)
