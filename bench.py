@@ -349,7 +349,10 @@ def run_b200(args, world, rank, local):
         ems = float(te.item())
         ng = (w["lx1"] + 4) * (w["lx2"] + 4) * (w["lx3"] + 4)
         h2d = ng * 8 * (5 * LSP + 1)        # fluidvars + J1
-        d2h = ng * 8 * (5 * LSP + 2 * LSP) + 8  # fluidvars + rhovs1|rhoes + dt
+        # ns, vs1, Ts + the ghost shell of vs2, vs3 (their interior is not written) + rhovs1|rhoes + dt
+        s2, s3, nb = w["lx1"] + 4, (w["lx1"] + 4) * (w["lx2"] + 4), 2 * LSP
+        shell = 8 * nb * (4 * s3 + 4 * s2 * (w["lx3"] + 4) + 4 * (w["lx2"] + 4) * (w["lx3"] + 4))
+        d2h = ng * 8 * (3 * LSP) + shell + ng * 8 * (2 * LSP) + 8
         e2e = {"value": world * cells * LSP * args.e2e_steps / (ems / 1e3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "api": "gem_fluid_adv_host (host blocks, pinned)", "steps": args.e2e_steps,

@@ -118,9 +118,12 @@ struct gem_work {
   double *Q, *Pr, *Lo;
   unsigned long long* acc;  // 32 slots: CFL maxima / counters
   long long nf1, nf2, nf3;
-  // device staging of the host blocks for gem_fluid_adv_host
+  // device staging of the host blocks for gem_fluid_adv_host, and its copy-out stream with
+  // the events after the ghost fill, the ghost epilogue and the diffusion
   double *F, *A, *E;
   size_t nF, nA, nE;
+  cudaStream_t cs;
+  cudaEvent_t ev[4];
 };
 
 namespace {
@@ -638,6 +641,8 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
   w->Q = w->Pr = w->Lo = nullptr;
   w->F = w->A = w->E = nullptr;
   w->nF = w->nA = w->nE = 0;
+  w->cs = nullptr;
+  for (auto& e : w->ev) e = nullptr;
   w->lx1 = d.lx1;
   w->lx2 = d.lx2;
   w->lx3 = d.lx3;
@@ -673,6 +678,9 @@ int gem_work_create(const gem_grid* g, gem_work** out) {
 int gem_work_destroy(gem_work* w) {
   if (!w) return GEM_OK;
   for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : w->ev)
+    if (e) cudaEventDestroy(e);
+  if (w->cs) cudaStreamDestroy(w->cs);
   void* ps[] = {w->vs1i, w->vs2i, w->vs3i, w->nn, w->Tn, w->dt, w->acc, w->F, w->A, w->E, w->Ttop, w->lu, w->sub};
   for (void* p : ps)
     if (p) cudaFree(p);
@@ -1066,21 +1074,33 @@ int gem_maxcfl_dev(const gem_grid* g, const double* fluidvars, gem_work* w, cons
   return GEM_OK;
 }
 
+// The fused step; after_fill / after_epi (optional) are recorded once the ghost fill (vs2,
+// vs3 final from there on) and the ghost epilogue (ns, vs1, rhovs1 final) are done.
+static int fluid_adv_impl(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                          const double* electrovars, gem_work* w, const double* dt, cudaStream_t st,
+                          cudaEvent_t after_fill, cudaEvent_t after_epi);
+
 int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
                       const double* electrovars, gem_work* w, const double* dt, void* stream) {
   if (!cfg || check_grid(g) || !fluidvars || !fluidauxvars || !electrovars || !w || !dt)
     return set_err(GEM_EINVAL, "null argument");
   if (cfg->diffsolvetype != 1 && cfg->diffsolvetype != 2)
     return set_err(GEM_EINVAL, "Unsupported diffusion solver type/mode: %d. Should be either 1 or 2.", cfg->diffsolvetype);
+  return fluid_adv_impl(cfg, g, fluidvars, fluidauxvars, electrovars, w, dt, S(stream), nullptr, nullptr);
+}
+
+static int fluid_adv_impl(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                          const double* electrovars, gem_work* w, const double* dt, cudaStream_t st,
+                          cudaEvent_t after_fill, cudaEvent_t after_epi) {
   int rc = check_step(g);
   if (rc) return rc;
-  cudaStream_t st = S(stream);
   Blocks B = blocks(g, fluidvars, fluidauxvars);
   w->timer.record(1, st);
   // v12rhov1 + T2rhoe + set_global_boundaries + halo_fluidvars (the interior conversions
   // are folded into the x3 sweep)
   rc = launch_ghost_fill(g, B, w->vs1i, LSP, true, st);
   if (rc) return rc;
+  if (after_fill) GEM_CUDA(cudaEventRecord(after_fill, st));
   w->timer.record(2, st);
   SweepArgs a;
   a.G = g->dev;
@@ -1102,6 +1122,7 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
     k_clean_vel_edges<<<grid_for(n, 128), 128, 0, st>>>(g->dev, fluidvars + LSP * g->dev.d.ng);
     GEM_LAUNCHED("k_clean_vel_edges");
   }
+  if (after_epi) GEM_CUDA(cudaEventRecord(after_epi, st));
   DiffArgs d;
   d.G = g->dev;
   d.B = B;
@@ -1183,11 +1204,47 @@ int gem_fluid_adv_host(const gem_cfg* cfg, const gem_grid* g, double* fluidvars,
   } else {
     GEM_CUDA(cudaMemcpyAsync(w->dt, dt_inout, sizeof(double), cudaMemcpyHostToDevice, st));
   }
-  if ((rc = gem_fluid_adv_dev(cfg, g, w->F, w->A, w->E, w, w->dt, stream))) return rc;
-  // ... and only what it writes comes out: fluidvars and rhovs1|rhoes
-  GEM_CUDA(cudaMemcpyAsync(fluidvars, w->F, nF * sizeof(double), cudaMemcpyDeviceToHost, st));
-  GEM_CUDA(cudaMemcpyAsync(fluidauxvars, w->A, ng * 2 * LSP * sizeof(double), cudaMemcpyDeviceToHost, st));
-  GEM_CUDA(cudaMemcpyAsync(dt_inout, w->dt, sizeof(double), cudaMemcpyDeviceToHost, st));
+  // ... and only what it writes comes out: fluidvars and rhovs1|rhoes, each block as soon as
+  // the step is done with it, on a copy stream beside the step's kernels: vs2, vs3 after the
+  // ghost fill, ns, vs1 and rhovs1 after the ghost epilogue (the diffusion reads ns only),
+  // Ts and rhoes at the end
+  if (!w->cs) {
+    GEM_CUDA(cudaStreamCreateWithFlags(&w->cs, cudaStreamNonBlocking));
+    for (auto& e : w->ev) GEM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  if (cfg->diffsolvetype != 1 && cfg->diffsolvetype != 2)
+    return set_err(GEM_EINVAL, "Unsupported diffusion solver type/mode: %d. Should be either 1 or 2.", cfg->diffsolvetype);
+  if ((rc = fluid_adv_impl(cfg, g, w->F, w->A, w->E, w, w->dt, st, w->ev[0], w->ev[1]))) return rc;
+  GEM_CUDA(cudaEventRecord(w->ev[2], st));
+  const size_t blk = ng * LSP;  // one field of all species
+  GEM_CUDA(cudaStreamWaitEvent(w->cs, w->ev[0], 0));
+  {
+    // vs2 and vs3 change only in their ghost cells (the ghost fill), so only their ghost shell
+    // comes out, as strided copies over the 14 blocks -- the x3 ghost planes, the x2 ghost
+    // rows of every plane and the x1 ghost cells of every column -- and the host keeps its
+    // unchanged interior
+    const Dims& d = g->dev.d;
+    const size_t s2 = (size_t)d.lx1 + 4, s3 = s2 * (d.lx2 + 4), nb = 2 * LSP, D = sizeof(double);
+    double* hb = fluidvars + 2 * blk;
+    const double* db = w->F + 2 * blk;
+    const size_t o3 = (size_t)(d.lx3 + 2) * s3, o2 = (size_t)(d.lx2 + 2) * s2, o1 = (size_t)d.lx1 + 2;
+    const auto D2H = cudaMemcpyDeviceToHost;
+    GEM_CUDA(cudaMemcpy2DAsync(hb, ng * D, db, ng * D, 2 * s3 * D, nb, D2H, w->cs));
+    GEM_CUDA(cudaMemcpy2DAsync(hb + o3, ng * D, db + o3, ng * D, 2 * s3 * D, nb, D2H, w->cs));
+    GEM_CUDA(cudaMemcpy2DAsync(hb, s3 * D, db, s3 * D, 2 * s2 * D, nb * (d.lx3 + 4), D2H, w->cs));
+    GEM_CUDA(cudaMemcpy2DAsync(hb + o2, s3 * D, db + o2, s3 * D, 2 * s2 * D, nb * (d.lx3 + 4), D2H, w->cs));
+    GEM_CUDA(cudaMemcpy2DAsync(hb, s2 * D, db, s2 * D, 2 * D, nb * (d.lx2 + 4) * (d.lx3 + 4), D2H, w->cs));
+    GEM_CUDA(cudaMemcpy2DAsync(hb + o1, s2 * D, db + o1, s2 * D, 2 * D, nb * (d.lx2 + 4) * (d.lx3 + 4), D2H, w->cs));
+  }
+  GEM_CUDA(cudaStreamWaitEvent(w->cs, w->ev[1], 0));
+  GEM_CUDA(cudaMemcpyAsync(fluidvars, w->F, 2 * blk * sizeof(double), cudaMemcpyDeviceToHost, w->cs));
+  GEM_CUDA(cudaMemcpyAsync(fluidauxvars, w->A, blk * sizeof(double), cudaMemcpyDeviceToHost, w->cs));
+  GEM_CUDA(cudaStreamWaitEvent(w->cs, w->ev[2], 0));
+  GEM_CUDA(cudaMemcpyAsync(fluidvars + 4 * blk, w->F + 4 * blk, blk * sizeof(double), cudaMemcpyDeviceToHost, w->cs));
+  GEM_CUDA(cudaMemcpyAsync(fluidauxvars + blk, w->A + blk, blk * sizeof(double), cudaMemcpyDeviceToHost, w->cs));
+  GEM_CUDA(cudaMemcpyAsync(dt_inout, w->dt, sizeof(double), cudaMemcpyDeviceToHost, w->cs));
+  GEM_CUDA(cudaEventRecord(w->ev[3], w->cs));
+  GEM_CUDA(cudaStreamWaitEvent(st, w->ev[3], 0));
   GEM_CUDA(cudaStreamSynchronize(st));
   return GEM_OK;
 }

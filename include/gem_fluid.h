@@ -395,11 +395,14 @@ int gem_fluid_adv_dev(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, 
 
 /* The same step through host buffers: copies what the step reads to the device (fluidvars
  * and the J1 field of electrovars), runs gem_dt_calc_dev (if dt_inout < 0, else uses
- * *dt_inout) and gem_fluid_adv_dev, copies back what it writes (fluidvars and the rhovs1 |
- * rhoes fields of fluidauxvars) and synchronises.  The host blocks end exactly as a full
- * round trip would leave them: rhovs1 and rhoes are recomputed from fluidvars over every
- * cell, and the 9 MHD scalars and the other electrovars fields are not touched.  Device
- * staging buffers are allocated on first use and kept in the work object. */
+ * *dt_inout) and gem_fluid_adv_dev, copies back what it writes and synchronises.  The host
+ * blocks end exactly as a full round trip would leave them: rhovs1 and rhoes are recomputed
+ * from fluidvars over every cell, vs2 and vs3 change only in their ghost cells (so only
+ * their ghost shell is copied back), and the 9 MHD scalars and the other electrovars fields
+ * are not touched.  The copies back run on a stream of the work object beside the step,
+ * each block once the step is done with it (vs2, vs3 after the ghost fill; ns, vs1, rhovs1
+ * before the diffusion; Ts, rhoes at the end); pinned host blocks let them overlap the
+ * step.  Device staging buffers are allocated on first use and kept in the work object. */
 int gem_fluid_adv_host(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
                        const double* electrovars, gem_work* w, double* dt_inout, void* stream);
 

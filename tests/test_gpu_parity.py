@@ -176,8 +176,12 @@ def test_single_step_bits_match(solver):
     assert_identical(ds.to_host(st), ref, "one fused step")
 
 
-def test_host_entry_point_matches_device():
-    name, g, kw = CASES[4]
+@pytest.mark.parametrize("ci", [4, 2, 3], ids=["dipole", "cart_periodic", "cart_2d"])
+def test_host_entry_point_matches_device(ci):
+    """gem_fluid_adv_host leaves the host blocks exactly as the device step leaves its own:
+    every block, the ghost shell of vs2 and vs3 included (the only part of them copied back),
+    on a dipole, an x3-periodic and a single-x3-plane grid."""
+    name, g, kw = CASES[ci]
     st = S.init_state(g, **kw)
     dg = F.DeviceGrid(g)
     a = F.DeviceState.from_host(dg, st.copy())
