@@ -128,23 +128,48 @@ GEMR_HD double maxwell_colln(int isp, int isp2, double nn2, double tn, double ts
   }
 }
 
-// collisions.f90:117-159 for one cell: nu, Phi, Psi of species isp with isp2 (zero if equal)
+// collisions.f90:117-159, the part symmetric in the two species: Teff**1.5, Phi and Psi of
+// the pair (isp, isp2).  Every operation is a commutative sum or product of the two sides or
+// a function of such (no contraction into fused multiply-adds in these builds), so swapping
+// the species gives the same bits and one evaluation serves both.
+struct CoulPair {
+  double P, Phi, Psi;  // Teff**1.5, Phi, Psi
+};
+GEMR_HD CoulPair coulomb_pair(const View& v, int isp, int isp2, double ts1, double ts2, double v1, double v2) {
+  const double ms1 = v.ms[isp], ms2 = v.ms[isp2];
+  const double Teff = (ms2 * ts1 + ms1 * ts2) / (ms2 + ms1);
+  CoulPair q;
+  q.P = pow(Teff, 1.5);
+  const double mred = ms1 * ms2 / (ms1 + ms2);
+  const double W = fabs(v1 - v2) / sqrt(2 * KB_ * Teff / mred);
+  q.Psi = exp(-(W * W));
+  if (W < 0.1)
+    q.Phi = 1;
+  else
+    q.Phi = 3.0 / 4 * sqrt(v.pi) * erf(W) / (W * W * W) - 3.0 / 2 / (W * W) * q.Psi;
+  return q;
+}
+
+// Pair source that evaluates each pair where it is needed
+struct DirectPairs {
+  GEMR_HD CoulPair operator()(const View& v, int isp, int isp2, double ts1, double ts2, double v1, double v2) const {
+    return coulomb_pair(v, isp, isp2, ts1, ts2, v1, v2);
+  }
+};
+
+// collisions.f90:117-159 for one cell: nu, Phi, Psi of species isp with isp2 (zero if equal);
+// the pair's symmetric part comes from `pairs`
+template <class Pairs>
 GEMR_HD void coulomb_colln(const View& v, int isp, int isp2, double ns2, double ts1, double ts2, double v1, double v2,
-                           double& nu, double& Phi, double& Psi) {
+                           double& nu, double& Phi, double& Psi, const Pairs& pairs) {
   if (isp == isp2) {
     nu = Phi = Psi = 0.0;
     return;
   }
-  const double ms1 = v.ms[isp], ms2 = v.ms[isp2];
-  const double Teff = (ms2 * ts1 + ms1 * ts2) / (ms2 + ms1);
-  nu = Coll::csj(isp, isp2) * ns2 * 1e-6 / pow(Teff, 1.5);
-  const double mred = ms1 * ms2 / (ms1 + ms2);
-  const double W = fabs(v1 - v2) / sqrt(2 * KB_ * Teff / mred);
-  Psi = exp(-(W * W));
-  if (W < 0.1)
-    Phi = 1;
-  else
-    Phi = 3.0 / 4 * sqrt(v.pi) * erf(W) / (W * W * W) - 3.0 / 2 / (W * W) * Psi;
+  const CoulPair q = pairs(v, isp, isp2, ts1, ts2, v1, v2);
+  nu = Coll::csj(isp, isp2) * ns2 * 1e-6 / q.P;
+  Phi = q.Phi;
+  Psi = q.Psi;
 }
 
 // ---- continuity: one interior cell c ------------------------------------------------------
@@ -290,9 +315,10 @@ GEMR_HD void continuity_cell(const View& v, long long c, const double* nn, const
 
 // ---- energy: index t = isp * ncell + c ----------------------------------------------------
 // nn: interior (lx1,lx2,lx3, O N2 O2 H ...); the rest as continuity_cell
+template <class Pairs = DirectPairs>
 GEMR_HD void energy_rate(const View& v, long long t, const double* nn, const double* vn1, const double* vn2,
                          const double* vn3, const double* Tn, const double* ns, const double* vs1, const double* vs2,
-                         const double* vs3, const double* Ts, double* Pr, double* Lo) {
+                         const double* vs3, const double* Ts, double* Pr, double* Lo, const Pairs& pairs = Pairs()) {
   const long long nc = ncell(v);
   const int isp = (int)(t / nc);
   const long long c = t - isp * nc;
@@ -316,7 +342,7 @@ GEMR_HD void energy_rate(const View& v, long long t, const double* nn, const dou
   for (int j = 0; j < NSP; ++j) {  // with the charged species
     const long long kj = j * v.ng + k;
     double nu, Phi, Psi;
-    coulomb_colln(v, isp, j, ns[kj], tsk, Ts[kj], u1, vs1[kj], nu, Phi, Psi);
+    coulomb_colln(v, isp, j, ns[kj], tsk, Ts[kj], u1, vs1[kj], nu, Phi, Psi, pairs);
     double fact = 2 * nu * Psi / (ms + v.ms[j]);
     pr = pr + nsk * ms * KB_ / gm1 * fact * Ts[kj];
     lo = lo + ms * fact;
@@ -360,10 +386,11 @@ GEMR_HD double dx1_line(const View& v, int i, double fm, double f0, double fp, d
 
 // nn: interior (lx1,lx2,lx3, O N2 O2 H ...); vn1, Tn, alt, g1: interior; Q: interior
 // (lx1,lx2,lx3,lsp); ns, vs1..3, Ts, E1: ghosted
+template <class Pairs = DirectPairs>
 GEMR_HD void momentum_rate(const View& v, long long t, const double* nn, const double* vn1, const double* Tn,
                            const double* ns, const double* vs1, const double* vs2, const double* vs3, const double* Ts,
                            const double* E1, const double* Q, const double* alt, const double* g1, double* Pr,
-                           double* Lo) {
+                           double* Lo, const Pairs& pairs = Pairs()) {
   const long long nc = ncell(v);
   const int isp = (int)(t / nc);
   const long long c = t - isp * nc;
@@ -403,7 +430,7 @@ GEMR_HD void momentum_rate(const View& v, long long t, const double* nn, const d
   for (int j = 0; j < NSP; ++j) {  // with the charged species
     double nu, Phi, Psi;
     const long long k2 = kg + (long long)j * v.ng;
-    coulomb_colln(v, isp, j, ns[k2], Ts[k], Ts[k2], vs1[k], vs1[k2], nu, Phi, Psi);
+    coulomb_colln(v, isp, j, ns[k2], Ts[k], Ts[k2], vs1[k], vs1[k2], nu, Phi, Psi, pairs);
     lo = lo + nu * Phi;
     pr = pr + ns[k] * ms * nu * Phi * vs1[k2];
   }

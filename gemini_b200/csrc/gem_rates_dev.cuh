@@ -1,5 +1,6 @@
 // Device form of the production/loss rates (sources.f90): one thread per interior cell for
-// the continuity chemistry, one per (cell, species) for the energy and momentum exchange,
+// the continuity chemistry, one per (cell, species) for the energy and momentum exchange
+// (a warp per species over 32 cells, the charged pairs shared within the block),
 // running the bodies of gem_rates.cuh, behind the C ABI (include/gem_fluid.h).  Included by
 // gem_fluid.cu (one translation unit with the plain path).
 
@@ -20,23 +21,92 @@ __global__ void kr_continuity(gemr::View v, RateIn in, const double* __restrict_
     gemr::continuity_cell(v, c, in.nn, in.vn1, in.vn2, in.vn3, in.Tn, ns, vs1, vs2, vs3, Ts, Pr, Lo);
 }
 
-__global__ void kr_energy(gemr::View v, RateIn in, const double* __restrict__ fv, double* __restrict__ Pr,
-                          double* __restrict__ Lo) {
-  const long long n = gemr::ncell(v) * LSP;
-  const double *ns = fv, *vs1 = fv + LSP * v.ng, *vs2 = fv + 2 * LSP * v.ng, *vs3 = fv + 3 * LSP * v.ng,
-               *Ts = fv + 4 * LSP * v.ng;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-    gemr::energy_rate(v, t, in.nn, in.vn1, in.vn2, in.vn3, in.Tn, ns, vs1, vs2, vs3, Ts, Pr, Lo);
+// The energy and momentum exchange run one block per 32 interior cells, one warp per
+// species (thread = (cell, species) as before, 32 consecutive cells of one species per
+// warp).  Each of the 21 unordered charged pairs of a cell has its symmetric part (Teff**1.5,
+// Phi, Psi) evaluated once, by warp i for the pairs (i, i+1), (i, i+2), (i, i+3) mod 7, and
+// shared through shared memory: the bits are those of evaluating it in both threads.
+constexpr int kRateCells = 32;
+constexpr int kRateThreads = LSP * kRateCells;
+constexpr int kPairs = LSP * (LSP - 1) / 2;
+
+struct PairTab {
+  double P[kPairs][kRateCells], Phi[kPairs][kRateCells], Psi[kPairs][kRateCells];
+};
+
+// slot of the unordered pair {i, j}, i != j: owner i with offset d = j - i mod 7 in 1..3
+__device__ __forceinline__ int pair_slot(int i, int j) {
+  int d = j - i;
+  if (d < 0) d += LSP;
+  return (d <= 3) ? i * 3 + d - 1 : j * 3 + (LSP - d) - 1;
 }
 
-__global__ void kr_momentum(gemr::View v, RateIn in, const double* __restrict__ fv, const double* __restrict__ E1,
-                            const double* __restrict__ Q, const double* __restrict__ alt,
-                            const double* __restrict__ g1, double* __restrict__ Pr, double* __restrict__ Lo) {
-  const long long n = gemr::ncell(v) * LSP;
+struct SmemPairs {
+  const PairTab* tab;
+  int lane;
+  __device__ __forceinline__ gemr::CoulPair operator()(const gemr::View&, int isp, int isp2, double, double, double,
+                                                       double) const {
+    const int p = pair_slot(isp, isp2);
+    return gemr::CoulPair{tab->P[p][lane], tab->Phi[p][lane], tab->Psi[p][lane]};
+  }
+};
+
+// this thread's three pairs of cell c (ghosted index k), into the table
+__device__ __forceinline__ void fill_pairs(const gemr::View& v, int isp, int lane, long long k,
+                                           const double* __restrict__ vs1, const double* __restrict__ Ts,
+                                           PairTab& tab) {
+  const double t1 = Ts[isp * v.ng + k], u1 = vs1[isp * v.ng + k];
+#pragma unroll
+  for (int d = 1; d <= 3; ++d) {
+    const int j = (isp + d < LSP) ? isp + d : isp + d - LSP;
+    const gemr::CoulPair q = gemr::coulomb_pair(v, isp, j, t1, Ts[j * v.ng + k], u1, vs1[j * v.ng + k]);
+    const int p = isp * 3 + d - 1;
+    tab.P[p][lane] = q.P;
+    tab.Phi[p][lane] = q.Phi;
+    tab.Psi[p][lane] = q.Psi;
+  }
+}
+
+__global__ void __launch_bounds__(kRateThreads) kr_energy(gemr::View v, RateIn in, const double* __restrict__ fv,
+                                                          double* __restrict__ Pr, double* __restrict__ Lo) {
+  __shared__ PairTab tab;
+  const int isp = threadIdx.x / kRateCells, lane = threadIdx.x % kRateCells;
+  const long long nc = gemr::ncell(v);
+  const long long c = (long long)blockIdx.x * kRateCells + lane;
   const double *ns = fv, *vs1 = fv + LSP * v.ng, *vs2 = fv + 2 * LSP * v.ng, *vs3 = fv + 3 * LSP * v.ng,
                *Ts = fv + 4 * LSP * v.ng;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-    gemr::momentum_rate(v, t, in.nn, in.vn1, in.Tn, ns, vs1, vs2, vs3, Ts, E1, Q, alt, g1, Pr, Lo);
+  if (c < nc) {
+    int i1, i2, i3;
+    gemr::cell_of(v, c, i1, i2, i3);
+    fill_pairs(v, isp, lane, gemr::gix(v, i1, i2, i3), vs1, Ts, tab);
+  }
+  __syncthreads();
+  if (c < nc)
+    gemr::energy_rate(v, isp * nc + c, in.nn, in.vn1, in.vn2, in.vn3, in.Tn, ns, vs1, vs2, vs3, Ts, Pr, Lo,
+                      SmemPairs{&tab, lane});
+}
+
+__global__ void __launch_bounds__(kRateThreads) kr_momentum(gemr::View v, RateIn in, const double* __restrict__ fv,
+                                                            const double* __restrict__ E1,
+                                                            const double* __restrict__ Q,
+                                                            const double* __restrict__ alt,
+                                                            const double* __restrict__ g1, double* __restrict__ Pr,
+                                                            double* __restrict__ Lo) {
+  __shared__ PairTab tab;
+  const int isp = threadIdx.x / kRateCells, lane = threadIdx.x % kRateCells;
+  const long long nc = gemr::ncell(v);
+  const long long c = (long long)blockIdx.x * kRateCells + lane;
+  const double *ns = fv, *vs1 = fv + LSP * v.ng, *vs2 = fv + 2 * LSP * v.ng, *vs3 = fv + 3 * LSP * v.ng,
+               *Ts = fv + 4 * LSP * v.ng;
+  if (c < nc) {
+    int i1, i2, i3;
+    gemr::cell_of(v, c, i1, i2, i3);
+    fill_pairs(v, isp, lane, gemr::gix(v, i1, i2, i3), vs1, Ts, tab);
+  }
+  __syncthreads();
+  if (c < nc)
+    gemr::momentum_rate(v, isp * nc + c, in.nn, in.vn1, in.Tn, ns, vs1, vs2, vs3, Ts, E1, Q, alt, g1, Pr, Lo,
+                        SmemPairs{&tab, lane});
 }
 
 gemr::View rate_view(const gem_grid* g) {
@@ -87,8 +157,8 @@ int gem_srcs_energy_dev(const gem_grid* g, const double* nn, const double* vn1, 
   if (check_grid(g) || !nn || !vn1 || !vn2 || !vn3 || !Tn || !fluidvars || !Pr || !Lo)
     return set_err(GEM_EINVAL, "null argument");
   const gemr::View v = gemk::rate_view(g);
-  const long long n = gemr::ncell(v) * LSP;
-  gemk::kr_energy<<<grid_for(n, 128), 128, 0, S(stream)>>>(v, gemk::RateIn{nn, vn1, vn2, vn3, Tn}, fluidvars, Pr,
+  const long long nb = (gemr::ncell(v) + gemk::kRateCells - 1) / gemk::kRateCells;
+  gemk::kr_energy<<<(unsigned)nb, gemk::kRateThreads, 0, S(stream)>>>(v, gemk::RateIn{nn, vn1, vn2, vn3, Tn}, fluidvars, Pr,
                                                               Lo);
   GEM_LAUNCHED("kr_energy");
   return GEM_OK;
@@ -101,8 +171,8 @@ int gem_srcs_momentum_dev(const gem_grid* g, const double* nn, const double* vn1
     return set_err(GEM_EINVAL, "null argument");
   if (g->dev.d.lx1 < 2) return set_err(GEM_EINVAL, "the x1 gradients need lx1 >= 2");
   const gemr::View v = gemk::rate_view(g);
-  const long long n = gemr::ncell(v) * LSP;
-  gemk::kr_momentum<<<grid_for(n, 128), 128, 0, S(stream)>>>(v, gemk::RateIn{nn, vn1, nullptr, nullptr, Tn},
+  const long long nb = (gemr::ncell(v) + gemk::kRateCells - 1) / gemk::kRateCells;
+  gemk::kr_momentum<<<(unsigned)nb, gemk::kRateThreads, 0, S(stream)>>>(v, gemk::RateIn{nn, vn1, nullptr, nullptr, Tn},
                                                                 fluidvars, electrovars, Q, alt, g1, Pr, Lo);
   GEM_LAUNCHED("kr_momentum");
   return GEM_OK;
