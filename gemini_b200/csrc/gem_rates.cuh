@@ -384,13 +384,34 @@ GEMR_HD double dx1_line(const View& v, int i, double fm, double f0, double fp, d
   return (fp - fm) / (v.dx1[i + 1] + v.dx1[i]) / h1;
 }
 
+// The two x1 log-gradient terms of momentum_rate, evaluated where they are needed: the
+// ambipolar field kB Te / qe * d log(ne kB Te)/dx1 and the species' d log(ns kB Ts)/dx1 at
+// interior cell (i1, .) with ghosted index kg and x1 neighbours km, kp inside 1..lx1
+struct DirectX1 {
+  GEMR_HD double epol(const View& v, const double* ns, const double* Ts, int i1, long long kg, long long km,
+                      long long kp, double h1) const {
+    const long long e = (long long)(NSP - 1) * v.ng;
+    const double le0 = log(ns[e + kg] * KB_ * Ts[e + kg]);
+    const double lem = log(ns[e + km] * KB_ * Ts[e + km]);
+    const double lep = log(ns[e + kp] * KB_ * Ts[e + kp]);
+    return KB_ * Ts[e + kg] / v.qs[NSP - 1] * dx1_line(v, i1, lem, le0, lep, h1);
+  }
+  GEMR_HD double pg(const View& v, const double* ns, const double* Ts, long long s0, int i1, long long kg,
+                    long long km, long long kp, double h1) const {
+    const double lp0 = log(ns[s0 + kg] * KB_ * Ts[s0 + kg]);
+    const double lpm = log(ns[s0 + km] * KB_ * Ts[s0 + km]);
+    const double lpp = log(ns[s0 + kp] * KB_ * Ts[s0 + kp]);
+    return dx1_line(v, i1, lpm, lp0, lpp, h1);
+  }
+};
+
 // nn: interior (lx1,lx2,lx3, O N2 O2 H ...); vn1, Tn, alt, g1: interior; Q: interior
 // (lx1,lx2,lx3,lsp); ns, vs1..3, Ts, E1: ghosted
-template <class Pairs = DirectPairs>
+template <class Pairs = DirectPairs, class X1 = DirectX1>
 GEMR_HD void momentum_rate(const View& v, long long t, const double* nn, const double* vn1, const double* Tn,
                            const double* ns, const double* vs1, const double* vs2, const double* vs3, const double* Ts,
                            const double* E1, const double* Q, const double* alt, const double* g1, double* Pr,
-                           double* Lo, const Pairs& pairs = Pairs()) {
+                           double* Lo, const Pairs& pairs = Pairs(), const X1& x1 = X1()) {
   const long long nc = ncell(v);
   const int isp = (int)(t / nc);
   const long long c = t - isp * nc;
@@ -406,18 +427,11 @@ GEMR_HD void momentum_rate(const View& v, long long t, const double* nn, const d
   const int im = (i1 > 1) ? i1 - 1 : i1, ip = (i1 < v.lx1) ? i1 + 1 : i1;  // neighbours inside 1..lx1
   const long long km = gix(v, im, i2, i3), kp = gix(v, ip, i2, i3);
   // ambipolar field kB Te / qe * d log(ne kB Te)/dx1
-  const long long e = (long long)(NSP - 1) * v.ng;
-  const double le0 = log(ns[e + kg] * KB_ * Ts[e + kg]);
-  const double lem = log(ns[e + km] * KB_ * Ts[e + km]);
-  const double lep = log(ns[e + kp] * KB_ * Ts[e + kp]);
-  const double epol = KB_ * Ts[e + kg] / v.qs[NSP - 1] * dx1_line(v, i1, lem, le0, lep, h1);
+  const double epol = x1.epol(v, ns, Ts, i1, kg, km, kp, h1);
   // pressure * d log(pressure)/dx1 and dQ/dx1
   const long long s0 = (long long)isp * v.ng;
   const double pres = ns[s0 + kg] * KB_ * Ts[s0 + kg];
-  const double lp0 = log(pres);
-  const double lpm = log(ns[s0 + km] * KB_ * Ts[s0 + km]);
-  const double lpp = log(ns[s0 + kp] * KB_ * Ts[s0 + kp]);
-  const double pg = dx1_line(v, i1, lpm, lp0, lpp, h1);
+  const double pg = x1.pg(v, ns, Ts, s0, i1, kg, km, kp, h1);
   const long long qb = (long long)isp * nc;
   const long long cm = c - (i1 - im), cp = c + (ip - i1);
   const double gq = dx1_line(v, i1, Q[qb + cm], Q[qb + c], Q[qb + cp], h1);

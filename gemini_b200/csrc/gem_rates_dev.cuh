@@ -86,6 +86,25 @@ __global__ void __launch_bounds__(kRateThreads) kr_energy(gemr::View v, RateIn i
                       SmemPairs{&tab, lane});
 }
 
+// x1 log-gradient terms from values the block formed once: the electrons' ambipolar term
+// of the cell (shared memory, written by the electron warp) and this species' log(n kB T) at
+// the cell and its x1 neighbours (taken by the neighbouring lanes)
+struct SharedX1 {
+  double epol_v, lm, l0, lp;
+  __device__ __forceinline__ double epol(const gemr::View&, const double*, const double*, int, long long, long long,
+                                         long long, double) const {
+    return epol_v;
+  }
+  __device__ __forceinline__ double pg(const gemr::View& v, const double*, const double*, long long, int i1, long long,
+                                       long long, long long, double h1) const {
+    return gemr::dx1_line(v, i1, lm, l0, lp, h1);
+  }
+};
+
+// Each lane forms log(n kB T) of its own cell once; a cell's x1 neighbours on the same line
+// are the adjacent lanes (c +- 1), except across the block's edges (lanes 0 and 31), which
+// form that one neighbour's log themselves.  At the line ends the missing side is the cell
+// itself, as the direct form's clamped neighbour index gives.
 __global__ void __launch_bounds__(kRateThreads) kr_momentum(gemr::View v, RateIn in, const double* __restrict__ fv,
                                                             const double* __restrict__ E1,
                                                             const double* __restrict__ Q,
@@ -93,20 +112,44 @@ __global__ void __launch_bounds__(kRateThreads) kr_momentum(gemr::View v, RateIn
                                                             const double* __restrict__ g1, double* __restrict__ Pr,
                                                             double* __restrict__ Lo) {
   __shared__ PairTab tab;
+  __shared__ double s_epol[kRateCells];
   const int isp = threadIdx.x / kRateCells, lane = threadIdx.x % kRateCells;
   const long long nc = gemr::ncell(v);
   const long long c = (long long)blockIdx.x * kRateCells + lane;
+  const bool ok = c < nc;
   const double *ns = fv, *vs1 = fv + LSP * v.ng, *vs2 = fv + 2 * LSP * v.ng, *vs3 = fv + 3 * LSP * v.ng,
                *Ts = fv + 4 * LSP * v.ng;
-  if (c < nc) {
-    int i1, i2, i3;
+  const long long s0 = (long long)isp * v.ng;
+  int i1 = 1, i2 = 1, i3 = 1;
+  long long kg = 0;
+  double l0 = 0.0;
+  if (ok) {
     gemr::cell_of(v, c, i1, i2, i3);
-    fill_pairs(v, isp, lane, gemr::gix(v, i1, i2, i3), vs1, Ts, tab);
+    kg = gemr::gix(v, i1, i2, i3);
+    fill_pairs(v, isp, lane, kg, vs1, Ts, tab);
+    l0 = log(ns[s0 + kg] * gemr::KB_ * Ts[s0 + kg]);
+  }
+  double lm = __shfl_up_sync(0xffffffffu, l0, 1), lp = __shfl_down_sync(0xffffffffu, l0, 1);
+  if (ok) {
+    if (i1 == 1) lm = l0;
+    if (i1 == v.lx1) lp = l0;
+    const bool edge_m = lane == 0 && i1 > 1, edge_p = lane == kRateCells - 1 && i1 < v.lx1;
+    if (edge_m || edge_p) {
+      const long long kk = gemr::gix(v, edge_m ? i1 - 1 : i1 + 1, i2, i3);
+      const double x = log(ns[s0 + kk] * gemr::KB_ * Ts[s0 + kk]);
+      if (edge_m)
+        lm = x;
+      else
+        lp = x;
+    }
+    if (isp == LSP - 1)
+      s_epol[lane] = gemr::KB_ * Ts[s0 + kg] / v.qs[LSP - 1] *
+                     gemr::dx1_line(v, i1, lm, l0, lp, gemr::hm(v.h1, v, i1, i2, i3));
   }
   __syncthreads();
-  if (c < nc)
+  if (ok)
     gemr::momentum_rate(v, isp * nc + c, in.nn, in.vn1, in.Tn, ns, vs1, vs2, vs3, Ts, E1, Q, alt, g1, Pr, Lo,
-                        SmemPairs{&tab, lane});
+                        SmemPairs{&tab, lane}, SharedX1{s_epol[lane], lm, l0, lp});
 }
 
 gemr::View rate_view(const gem_grid* g) {
