@@ -3,7 +3,7 @@ srcsMomentum_curv with collisions.f90) through the device C ABI against the orac
 
 The device evaluates every expression in the reference's order with the same IEEE
 operations; only pow, exp, log, log10, erf, tanh and sin are the device's own (a few ulp
-from the C library's).  Tolerance, written here, for Pr and Lo alike:
+from the C library's), and x**0.5, x**1.5 are sqrt(x), x*sqrt(x) there (within 1.5 ulp).  Tolerance, written here, for Pr and Lo alike:
   |gpu - oracle| <= 1e-12 (|oracle| + max over the species' cells of |oracle|),
 i.e. relative where a rate is a sum of like-signed terms and norm-wise per species where
 terms of both signs cancel: the Coulomb Phi near W = 0.1 (two terms of ~150 cancel to ~1,
