@@ -50,6 +50,8 @@ struct View {
   const double* dx1;           // backward differences dx1(j), j = 0..lx1+2
   double ms[NSP], qs[NSP], gam[NSP];
   double pi;  // 4 atan(1), formed on the host
+  // device only: RN(1/(ms_i + mn_j)) and RN(1/(ms_i + ms_j)), formed on the host (qdk)
+  double ymn[NSP][NNEU], yms[NSP][NSP];
 };
 
 GEMR_HD long long ncell(const View& v) { return (long long)v.lx1 * v.lx2 * v.lx3; }
@@ -105,6 +107,26 @@ struct Coll {
   static GEMR_HD double csj(int i, int j) { return (double)kCsj[i][j]; }
   static GEMR_HD double mn(int j) { return kMn[j] * AMU_; }
 };
+
+// a/b for a constant divisor b whose correctly rounded reciprocal y = RN(1/b) was formed on
+// the host.  On the device: q0 = RN(a*y), the exact remainder a - b*q0 and RN(q0 + r*y),
+// which is the IEEE quotient whenever |a| lies in [2^-500, 2^500) (Markstein; every y here
+// is near 2^±90); a zero numerator gives the correctly signed zero, anything else the IEEE
+// division.  The host build divides.
+GEMR_HD double qdk(double a, double b, double y) {
+#ifdef __CUDA_ARCH__
+  const double q0 = a * y;
+  const double r = __fma_rn(-q0, b, a);
+  const double q1 = __fma_rn(r, y, q0);
+  if (((unsigned)__double2hiint(a) & 0x7fffffffu) - (523u << 20) < (1000u << 20)) return q1;
+  if (a == 0.0) return q0;
+  return a / b;
+#else
+  (void)y;
+  return a / b;
+#endif
+}
+constexpr double Y3 = 1.0 / 3;  // RN(1/3)
 
 // x**0.5 and x**1.5 of the collision and reaction fits.  The host build calls pow, as the
 // reference does; the device forms them from its correctly rounded square root (x**0.5
@@ -352,10 +374,10 @@ GEMR_HD void energy_rate(const View& v, long long t, const double* nn, const dou
   double pr = 0.0, lo = 0.0;
   for (int j = 0; j < NNEU; ++j) {  // with the neutrals
     const double nu = maxwell_colln(isp, j, nn[j * nc + c], tn, tsk);
-    double fact = 2 * nu / (ms + Coll::mn(j));
+    double fact = qdk(2 * nu, ms + Coll::mn(j), v.ymn[isp][j]);
     pr = pr + nsk * ms * KB_ / gm1 * fact * tn;
     lo = lo + ms * fact;
-    fact = fact * Coll::mn(j) / 3;
+    fact = qdk(fact * Coll::mn(j), 3, Y3);
     const double d1 = u1 - vn1[c], d2 = u2 - vn2[c], d3 = u3 - vn3[c];
     pr = pr + nsk * ms / gm1 * ((d1 * d1) + (d2 * d2) + (d3 * d3)) * fact;
   }
@@ -363,10 +385,10 @@ GEMR_HD void energy_rate(const View& v, long long t, const double* nn, const dou
     const long long kj = j * v.ng + k;
     double nu, Phi, Psi;
     coulomb_colln(v, isp, j, ns[kj], tsk, Ts[kj], u1, vs1[kj], nu, Phi, Psi, pairs);
-    double fact = 2 * nu * Psi / (ms + v.ms[j]);
+    double fact = qdk(2 * nu * Psi, ms + v.ms[j], v.yms[isp][j]);
     pr = pr + nsk * ms * KB_ / gm1 * fact * Ts[kj];
     lo = lo + ms * fact;
-    fact = 2 * nu * Phi / (ms + v.ms[j]) * v.ms[j] / 3;
+    fact = qdk(qdk(2 * nu * Phi, ms + v.ms[j], v.yms[isp][j]) * v.ms[j], 3, Y3);
     const double d1 = u1 - vs1[kj], d2 = u2 - vs2[kj], d3 = u3 - vs3[kj];
     pr = pr + nsk * ms / gm1 * ((d1 * d1) + (d2 * d2) + (d3 * d3)) * fact;
   }

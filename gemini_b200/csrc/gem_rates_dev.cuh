@@ -175,6 +175,12 @@ gemr::View rate_view(const gem_grid* g) {
     v.gam[s] = gam[s];
   }
   v.pi = 4 * std::atan(1.0);  // phys_consts.in.f90:20, on the host
+  // the divisors ms_i + mn_j and ms_i + ms_j exactly as the device forms them
+  const double mn[gemr::NNEU] = {16 * gemr::AMU_, 28 * gemr::AMU_, 32 * gemr::AMU_, 1 * gemr::AMU_};  // Coll::mn
+  for (int i = 0; i < LSP; ++i) {
+    for (int j = 0; j < gemr::NNEU; ++j) v.ymn[i][j] = 1.0 / (v.ms[i] + mn[j]);
+    for (int j = 0; j < LSP; ++j) v.yms[i][j] = 1.0 / (v.ms[i] + v.ms[j]);
+  }
   return v;
 }
 
