@@ -1143,6 +1143,46 @@ static int fluid_adv_impl(const gem_cfg* cfg, const gem_grid* g, double* fluidva
   return GEM_OK;
 }
 
+// The advection of the step with compression through the fused kernels: the ghost fill, the
+// fused x3 and x1 sweeps, the fused x2 sweep whose epilogue stops after rhov12v1 and
+// clean_param(1), (2) (the swept energy densities stay for the compression sub-step), and
+// that part of the ghost shell.  Bit for bit what v12rhov1, T2rhoe,
+// set_global_boundaries_allspec, halo_fluidvars, interface_vels_allspec, the nine sweeps,
+// halo_allparams, rhov12v1 and clean_param(1), (2) leave for the compression sub-step (which
+// converts rhoes and resets the ghost temperatures before anything reads them).  Needs what
+// the fused step needs (check_step).
+static int advection_keepre(const gem_grid* g, double* fluidvars, double* fluidauxvars, gem_work* w,
+                            const double* dt, cudaStream_t st) {
+  const Dims& d = g->dev.d;
+  Blocks B = blocks(g, fluidvars, fluidauxvars);
+  int rc = launch_ghost_fill(g, B, w->vs1i, LSP, true, st);
+  if (rc) return rc;
+  SweepArgs a;
+  a.G = g->dev;
+  a.B = B;
+  a.vsi = nullptr;
+  a.vs1i = w->vs1i;
+  a.dtp = dt;
+  a.dtp_w = nullptr;
+  a.which = 0;
+  if ((rc = launch_sweep(g, 3, true, a, LSP, st))) return rc;
+  if ((rc = launch_sweep(g, 1, true, a, LSP, st))) return rc;
+  const dim3 block(32, LSP), grid((d.lx1 + 31) / 32, d.lx3);
+  if (g->dev.unit)
+    k_sweep_march<2, true, true, 2, true><<<grid, block, 0, st>>>(a);
+  else
+    k_sweep_march<2, false, true, 2, true><<<grid, block, 0, st>>>(a);
+  GEM_LAUNCHED("k_sweep_march");
+  k_ghost_epilogue<true><<<grid_for(ghost_cells(d), 256), 256, 0, st>>>(g->dev, B);
+  GEM_LAUNCHED("k_ghost_epilogue");
+  if (g->dev.has_null && (g->dev.gridflag == 0 || g->dev.gridflag == 1)) {
+    const long long n = (long long)d.lx2 * d.lx3 * LSP;
+    k_clean_vel_edges<<<grid_for(n, 128), 128, 0, st>>>(g->dev, fluidvars + LSP * d.ng);
+    GEM_LAUNCHED("k_clean_vel_edges");
+  }
+  return GEM_OK;
+}
+
 int gem_work_phase_timing(gem_work* w, int max_steps) {
   if (!w || max_steps < 0) return set_err(GEM_EINVAL, "bad argument");
   for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);

@@ -18,21 +18,27 @@ int gem_fluid_adv_compression_dev(const gem_cfg* cfg, const gem_grid* g, double*
   if (cfg->diffsolvetype != 1 && cfg->diffsolvetype != 2)
     return set_err(GEM_EINVAL, "Unsupported diffusion solver type/mode: %d. Should be either 1 or 2.",
                    cfg->diffsolvetype);
-  // advection (app/main.f90:280-319)
-  GEM_TRY(gem_v12rhov1_dev(g, fluidvars, fluidauxvars, stream));
-  GEM_TRY(gem_T2rhoe_dev(g, fluidvars, fluidauxvars, stream));
-  GEM_TRY(gem_set_global_boundaries_allspec_dev(g, fluidvars, fluidauxvars, w, LSP, stream));
-  GEM_TRY(gem_halo_fluidvars_dev(g, fluidvars, fluidauxvars, stream));
-  GEM_TRY(gem_interface_vels_allspec_dev(g, fluidvars, w, LSP, stream));
-  for (int dim : {3, 1})
+  // advection (app/main.f90:280-319): the fused kernels where the grid allows them (the
+  // same results), else the reference's sequence of routines
+  const Dims& d = g->dev.d;
+  if (d.lx1 >= 4 && !(g->dev.flagper && d.lx3 < 2)) {
+    GEM_TRY(advection_keepre(g, fluidvars, fluidauxvars, w, dt, S(stream)));
+  } else {
+    GEM_TRY(gem_v12rhov1_dev(g, fluidvars, fluidauxvars, stream));
+    GEM_TRY(gem_T2rhoe_dev(g, fluidvars, fluidauxvars, stream));
+    GEM_TRY(gem_set_global_boundaries_allspec_dev(g, fluidvars, fluidauxvars, w, LSP, stream));
+    GEM_TRY(gem_halo_fluidvars_dev(g, fluidvars, fluidauxvars, stream));
+    GEM_TRY(gem_interface_vels_allspec_dev(g, fluidvars, w, LSP, stream));
+    for (int dim : {3, 1})
+      for (int which = 0; which < 3; ++which)
+        GEM_TRY(gem_sweep_allspec_dev(g, dim, which, fluidvars, fluidauxvars, w, dt, stream));
+    GEM_TRY(gem_halo_allparams_dev(g, fluidvars, fluidauxvars, stream));
     for (int which = 0; which < 3; ++which)
-      GEM_TRY(gem_sweep_allspec_dev(g, dim, which, fluidvars, fluidauxvars, w, dt, stream));
-  GEM_TRY(gem_halo_allparams_dev(g, fluidvars, fluidauxvars, stream));
-  for (int which = 0; which < 3; ++which)
-    GEM_TRY(gem_sweep_allspec_dev(g, 2, which, fluidvars, fluidauxvars, w, dt, stream));
-  GEM_TRY(gem_rhov12v1_dev(g, fluidvars, fluidauxvars, stream));
-  GEM_TRY(gem_clean_param_dev(g, 1, fluidvars, stream));
-  GEM_TRY(gem_clean_param_dev(g, 2, fluidvars, stream));
+      GEM_TRY(gem_sweep_allspec_dev(g, 2, which, fluidvars, fluidauxvars, w, dt, stream));
+    GEM_TRY(gem_rhov12v1_dev(g, fluidvars, fluidauxvars, stream));
+    GEM_TRY(gem_clean_param_dev(g, 1, fluidvars, stream));
+    GEM_TRY(gem_clean_param_dev(g, 2, fluidvars, stream));
+  }
   // compression (app/main.f90:320-338)
   GEM_TRY(gem_vnricht_artvisc_dev(g, fluidvars, Q, stream));
   GEM_TRY(gem_halo_fluidvars_dev(g, fluidvars, fluidauxvars, stream));

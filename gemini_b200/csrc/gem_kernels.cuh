@@ -756,8 +756,11 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // PERM: the x3 periodicity of the fused x3 sweep, 0 / 1 known at compile time (the plain
-// launch: the wrap values stay out of the registers of non-periodic lines), 2 read from G
-template <int DIM, bool UNIT, bool FUSED, int PERM = 2>
+// launch: the wrap values stay out of the registers of non-periodic lines), 2 read from G.
+// KEEPRE (fused x2 only): the epilogue stops after rhov12v1 and clean_param(1), (2) and
+// stores the swept energy densities instead of converting them (rhoe2T and clean_param(3)
+// come after the compression sub-step).
+template <int DIM, bool UNIT, bool FUSED, int PERM = 2, bool KEEPRE = false>
 __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
   const GridDev& G = P.G;
   const Dims d = G.d;
@@ -1074,13 +1077,22 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
         sh_t[buf][s][lane] = n * c_qs[s] * v;
         double nc = fmax_f(n, MINDENS);
         if (nul) nc = (s == 0) ? MINDENSNULL * 1e-2 : MINDENSNULL;
-        double T = fmax_f(c_gm1kb[s] * e / fmax_f(nc, MINDENSDIV), 100.0);
-        if (nul) T = 100;
-        if (valid) {
-          B.ns(s)[kc] = nc;
-          B.rv(s)[kc] = r;
-          B.vs1(s)[kc] = nul ? 0.0 : v;
-          B.Ts(s)[kc] = T;
+        if constexpr (KEEPRE) {
+          if (valid) {
+            B.ns(s)[kc] = nc;
+            B.rv(s)[kc] = r;
+            B.vs1(s)[kc] = nul ? 0.0 : v;
+            B.re(s)[kc] = e;
+          }
+        } else {
+          double T = fmax_f(c_gm1kb[s] * e / fmax_f(nc, MINDENSDIV), 100.0);
+          if (nul) T = 100;
+          if (valid) {
+            B.ns(s)[kc] = nc;
+            B.rv(s)[kc] = r;
+            B.vs1(s)[kc] = nul ? 0.0 : v;
+            B.Ts(s)[kc] = T;
+          }
         }
       }
       if constexpr (SMETA) cp_async_wait<2>();
@@ -1096,12 +1108,20 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
         }
         const double ve = mdiv(-1 / fmax_f(npre, MINDENSDIV), QE, YQE) * chrg;
         const double ne = nul ? MINDENSNULL : npost;
-        double T = fmax_f(c_gm1kb[s] * outv[0] / fmax_f(ne, MINDENSDIV), 100.0);
-        if (nul) T = 100;
-        if (valid) {
-          B.ns(s)[kc] = ne;
-          B.vs1(s)[kc] = nul ? 0.0 : ve;
-          B.Ts(s)[kc] = T;
+        if constexpr (KEEPRE) {
+          if (valid) {
+            B.ns(s)[kc] = ne;
+            B.vs1(s)[kc] = nul ? 0.0 : ve;
+            B.re(s)[kc] = outv[0];
+          }
+        } else {
+          double T = fmax_f(c_gm1kb[s] * outv[0] / fmax_f(ne, MINDENSDIV), 100.0);
+          if (nul) T = 100;
+          if (valid) {
+            B.ns(s)[kc] = ne;
+            B.vs1(s)[kc] = nul ? 0.0 : ve;
+            B.Ts(s)[kc] = T;
+          }
         }
       }
     }
@@ -1117,9 +1137,9 @@ __device__ __forceinline__ void b_sweep_march(const SweepArgs& P, const VB vb) {
 #ifndef GEM_X1_MINB
 #define GEM_X1_MINB 3
 #endif
-template <int DIM, bool UNIT, bool FUSED, int PERM = 2>
+template <int DIM, bool UNIT, bool FUSED, int PERM = 2, bool KEEPRE = false>
 __global__ void __launch_bounds__(224, GEM_MARCH_MINB) k_sweep_march(SweepArgs P) {
-  b_sweep_march<DIM, UNIT, FUSED, PERM>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+  b_sweep_march<DIM, UNIT, FUSED, PERM, KEEPRE>(P, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
 }
 
 
@@ -1317,6 +1337,9 @@ __global__ void __launch_bounds__(224, GEM_X1_MINB) k_sweep_x1(SweepArgs P) {
 // Fused step: the same epilogue for every ghost cell (rhov12v1 on the ghost values, then
 // clean_param(1) sets density ghosts to mindensdiv and clean_param(3) temperature ghosts to
 // 100; T2rhoe of those constants gives the final energy-density ghosts).
+// KEEPRE: the ghost shell's part of rhov12v1 and clean_param(1), (2) only (the fused x2
+// sweep's KEEPRE epilogue); Ts and rhoes stay for the compression sub-step.
+template <bool KEEPRE = false>
 __device__ __forceinline__ void b_ghost_epilogue(const GridDev& G, const Blocks& B, const VB vb) {
   const Dims d = G.d;
   const long long ngh = nghost(d);
@@ -1335,14 +1358,17 @@ __device__ __forceinline__ void b_ghost_epilogue(const GridDev& G, const Blocks&
     B.vs1(LSP - 1)[k] = mdiv(-1 / fmax_f(nsum, MINDENSDIV), QE, YQE) * chrg;
     for (int s = 0; s < LSP; ++s) {
       B.ns(s)[k] = MINDENSDIV;
-      B.Ts(s)[k] = 100.0;
-      B.re(s)[k] = conv_re(MINDENSDIV, 100.0, s);
+      if (!KEEPRE) {
+        B.Ts(s)[k] = 100.0;
+        B.re(s)[k] = conv_re(MINDENSDIV, 100.0, s);
+      }
     }
   }
 }
 
+template <bool KEEPRE = false>
 __global__ void k_ghost_epilogue(GridDev G, Blocks B) {
-  b_ghost_epilogue(G, B, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
+  b_ghost_epilogue<KEEPRE>(G, B, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
 }
 
 

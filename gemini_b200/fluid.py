@@ -312,8 +312,9 @@ class SourceInputs(ctypes.Structure):
 
 
 def fluid_adv_compression(cfg: FluidCfg, ds: DeviceState, dt, Q=None, stream=None):
-    """The step with the compression sub-step, as the reference's sequence of routines;
-    returns Q (flat interior (lx1, lx2, lx3, lsp) device tensor) for the source sub-step."""
+    """The step with the compression sub-step (the advection through the fused kernels where
+    the grid allows them, the rest as the reference's sequence of routines); returns Q (flat
+    interior (lx1, lx2, lx3, lsp) device tensor) for the source sub-step."""
     torch = _torch()
     lx1, lx2, lx3 = ds.dgrid.dims
     if Q is None:
@@ -323,6 +324,37 @@ def fluid_adv_compression(cfg: FluidCfg, ds: DeviceState, dt, Q=None, stream=Non
     _lib.check(_lib.lib().gem_fluid_adv_compression_dev(ctypes.byref(c), ds.g, _ptr(ds.fluidvars),
                                                          _ptr(ds.fluidauxvars), _ptr(ds.electrovars), ds.work,
                                                          _ptr(Q), _ptr(d), _stream(stream)))
+    return Q
+
+
+def fluid_adv_compression_reference_order(cfg: FluidCfg, ds: DeviceState, dt, Q=None, stream=None):
+    """The step with the compression sub-step as the reference's sequence of individual
+    routines (app/main.f90:280-355); fluid_adv_compression runs the advection part through
+    the fused kernels.  Returns Q as fluid_adv_compression does."""
+    d = ds._dt(dt)
+    v12rhov1(ds, stream)
+    T2rhoe(ds, stream)
+    set_global_boundaries_allspec(ds, LSP, stream)
+    halo_fluidvars(ds, stream)
+    interface_vels_allspec(ds, LSP, stream)
+    for dim in (3, 1):
+        for which in (0, 1, 2):
+            _sweep(ds, dim, which, d, stream)
+    halo_allparams(ds, stream)
+    for which in (0, 1, 2):
+        _sweep(ds, 2, which, d, stream)
+    rhov12v1(ds, stream)
+    clean_param(ds, 1, stream)
+    clean_param(ds, 2, stream)
+    Q = vnricht_artvisc(ds, Q, stream)
+    halo_fluidvars(ds, stream)
+    rk2_global_boundary_allspec(ds, stream)
+    compression(ds, Q, d, stream)
+    rhoe2T(ds, stream)
+    clean_param(ds, 3, stream)
+    energy_diffusion(cfg, ds, d, stream)
+    clean_param(ds, 3, stream)
+    T2rhoe(ds, stream)
     return Q
 
 
