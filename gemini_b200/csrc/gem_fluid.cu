@@ -1183,6 +1183,30 @@ static int advection_keepre(const gem_grid* g, double* fluidvars, double* fluida
   return GEM_OK;
 }
 
+// energy_diffusion, clean_param(3) and T2rhoe of the step with compression: the diffusion's
+// fused store applies clean_param(3) and T2rhoe to the interior cells and one pass over the
+// ghost shell does the rest; bit for bit the three routines in sequence.  Needs lx1 >= 4.
+static int diffusion_clean_T2rhoe(const gem_cfg* cfg, const gem_grid* g, double* fluidvars, double* fluidauxvars,
+                                  const double* electrovars, gem_work* w, const double* dt, cudaStream_t st) {
+  DiffArgs a;
+  a.G = g->dev;
+  a.B = blocks(g, fluidvars, fluidauxvars);
+  a.J1 = electrovars + 3 * g->dev.d.ng;
+  a.nn = w->nn;
+  a.Tn = w->Tn;
+  a.dtp = dt;
+  a.Teinf = cfg->Teinf;
+  a.Ttop = w->Ttop;
+  int rc = work_lu(w, g, &a.lu);
+  if (rc) return rc;
+  a.solver = cfg->diffsolvetype;
+  a.fused = 1;
+  if ((rc = launch_diffusion(g, a, st))) return rc;
+  k_ghost_T100<<<grid_for(ghost_cells(g->dev.d), 256), 256, 0, st>>>(g->dev, a.B);
+  GEM_LAUNCHED("k_ghost_T100");
+  return GEM_OK;
+}
+
 int gem_work_phase_timing(gem_work* w, int max_steps) {
   if (!w || max_steps < 0) return set_err(GEM_EINVAL, "bad argument");
   for (cudaEvent_t e : w->timer.ev) cudaEventDestroy(e);

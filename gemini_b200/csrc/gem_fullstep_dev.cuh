@@ -47,9 +47,13 @@ int gem_fluid_adv_compression_dev(const gem_cfg* cfg, const gem_grid* g, double*
   GEM_TRY(gem_rhoe2T_dev(g, fluidvars, fluidauxvars, stream));
   GEM_TRY(gem_clean_param_dev(g, 3, fluidvars, stream));
   // diffusion (app/main.f90:339-355)
-  GEM_TRY(gem_energy_diffusion_dev(cfg, g, fluidvars, electrovars, w, dt, stream));
-  GEM_TRY(gem_clean_param_dev(g, 3, fluidvars, stream));
-  GEM_TRY(gem_T2rhoe_dev(g, fluidvars, fluidauxvars, stream));
+  if (d.lx1 >= 4) {  // the diffusion store with clean_param(3) and T2rhoe folded in (the same results)
+    GEM_TRY(diffusion_clean_T2rhoe(cfg, g, fluidvars, fluidauxvars, electrovars, w, dt, S(stream)));
+  } else {
+    GEM_TRY(gem_energy_diffusion_dev(cfg, g, fluidvars, electrovars, w, dt, stream));
+    GEM_TRY(gem_clean_param_dev(g, 3, fluidvars, stream));
+    GEM_TRY(gem_T2rhoe_dev(g, fluidvars, fluidauxvars, stream));
+  }
   return GEM_OK;
 }
 

@@ -1371,6 +1371,22 @@ __global__ void k_ghost_epilogue(GridDev G, Blocks B) {
   b_ghost_epilogue<KEEPRE>(G, B, VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x});
 }
 
+// clean_param(3) and T2rhoe on the ghost shell after a fused diffusion store (which covers
+// the interior cells): every ghost temperature 100, rhoes from the cell's density.
+__global__ void k_ghost_T100(GridDev G, Blocks B) {
+  const Dims d = G.d;
+  const long long ngh = nghost(d);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ngh; q += (long long)gridDim.x * blockDim.x) {
+    int i1, i2, i3;
+    ghost_cell(d, q, i1, i2, i3);
+    const long long k = gi(d, i1, i2, i3);
+    for (int s = 0; s < LSP; ++s) {
+      B.Ts(s)[k] = 100.0;
+      B.re(s)[k] = conv_re(B.ns(s)[k], 100.0, s);
+    }
+  }
+}
+
 
 // ======================================================================================
 // 7. Field-aligned heat diffusion (multifluid.f90:309-342; collisions.f90:162-199;

@@ -47,6 +47,7 @@ struct View {
   int lx1, lx2, lx3;
   long long s2, s3, ng, c3;
   const double *h1, *h2, *h3;  // ghosted metric factors (x3 stride c3), or null (unit metric)
+  const double* yh1;           // device only: RN(1/h1) in the same layout, or null (unit metric)
   const double* dx1;           // backward differences dx1(j), j = 0..lx1+2
   double ms[NSP], qs[NSP], gam[NSP];
   double pi;  // 4 atan(1), formed on the host
@@ -128,6 +129,33 @@ GEMR_HD double qdk(double a, double b, double y) {
 }
 constexpr double Y3 = 1.0 / 3;  // RN(1/3)
 
+// qdk for a divisor formed at run time: y = RN(1/b) from the device's correctly rounded
+// reciprocal, and the fast form also requires |y| in [2^-400, 2^400].  The host build divides.
+GEMR_HD double qdk_v(double a, double b, double y) {
+#ifdef __CUDA_ARCH__
+  const double q0 = a * y;
+  const double r = __fma_rn(-q0, b, a);
+  const double q1 = __fma_rn(r, y, q0);
+  const unsigned ha = (unsigned)__double2hiint(a) & 0x7fffffffu, hy = (unsigned)__double2hiint(y) & 0x7fffffffu;
+  const bool yok = hy - (623u << 20) < (800u << 20);
+  if ((ha - (523u << 20) < (1000u << 20)) & yok) return q1;
+  if (a == 0.0 && yok) return q0;
+  return a / b;
+#else
+  (void)y;
+  return a / b;
+#endif
+}
+// RN(1/b) on the device (the reciprocal qdk_v needs); the host build, which divides, gets 0
+GEMR_HD double rcp_dev(double b) {
+#ifdef __CUDA_ARCH__
+  return __drcp_rn(b);
+#else
+  (void)b;
+  return 0.0;
+#endif
+}
+
 // x**0.5 and x**1.5 of the collision and reaction fits.  The host build calls pow, as the
 // reference does; the device forms them from its correctly rounded square root (x**0.5
 // correctly rounded, x**1.5 = x*sqrt(x) within 1.5 ulp), a fraction of the cost of its pow
@@ -176,12 +204,14 @@ GEMR_HD double maxwell_colln(int isp, int isp2, double nn2, double tn, double ts
 // the species gives the same bits and one evaluation serves both.
 struct CoulPair {
   double P, Phi, Psi;  // Teff**1.5, Phi, Psi
+  double yP;           // RN(1/P) on the device (rcp_dev)
 };
 GEMR_HD CoulPair coulomb_pair(const View& v, int isp, int isp2, double ts1, double ts2, double v1, double v2) {
   const double ms1 = v.ms[isp], ms2 = v.ms[isp2];
   const double Teff = (ms2 * ts1 + ms1 * ts2) / (ms2 + ms1);
   CoulPair q;
   q.P = pow_3half(Teff);
+  q.yP = rcp_dev(q.P);
   const double mred = ms1 * ms2 / (ms1 + ms2);
   const double W = fabs(v1 - v2) / sqrt(2 * KB_ * Teff / mred);
   q.Psi = exp(-(W * W));
@@ -209,7 +239,7 @@ GEMR_HD void coulomb_colln(const View& v, int isp, int isp2, double ns2, double 
     return;
   }
   const CoulPair q = pairs(v, isp, isp2, ts1, ts2, v1, v2);
-  nu = Coll::csj(isp, isp2) * ns2 * 1e-6 / q.P;
+  nu = qdk_v(Coll::csj(isp, isp2) * ns2 * 1e-6, q.P, q.yP);
   Phi = q.Phi;
   Psi = q.Psi;
 }
@@ -418,12 +448,31 @@ GEMR_HD void energy_rate(const View& v, long long t, const double* nn, const dou
 }
 
 // ---- momentum: index t = isp * ncell + c --------------------------------------------------
+// The divisors of the x1 gradients at interior cell (i1, i2, i3): e, the line difference's
+// divisor (dx1(i1+1) + dx1(i1) inside the line, dx1(1) and dx1(lx1) at its ends), and h1,
+// with their reciprocals for qdk_v on the device
+struct X1Div {
+  double e, ye, h1, yh1;
+};
+GEMR_HD X1Div x1_div(const View& v, int i1, int i2, int i3) {
+  X1Div q;
+  q.e = (i1 == 1) ? v.dx1[1] : (i1 == v.lx1) ? v.dx1[v.lx1] : v.dx1[i1 + 1] + v.dx1[i1];
+  q.ye = rcp_dev(q.e);
+  q.h1 = hm(v.h1, v, i1, i2, i3);
+#ifdef __CUDA_ARCH__
+  q.yh1 = hm(v.yh1, v, i1, i2, i3);
+#else
+  q.yh1 = 0.0;  // the host build divides
+#endif
+  return q;
+}
+
 // x1 derivative of f at interior x1 index i (1..lx1) over the line 1..lx1, as
 // grad3D1_curv_23 forms it: fm, f0, fp at i-1, i, i+1 (ends use only the side present)
-GEMR_HD double dx1_line(const View& v, int i, double fm, double f0, double fp, double h1) {
-  if (i == 1) return (fp - f0) / v.dx1[1] / h1;
-  if (i == v.lx1) return (f0 - fm) / v.dx1[v.lx1] / h1;
-  return (fp - fm) / (v.dx1[i + 1] + v.dx1[i]) / h1;
+GEMR_HD double dx1_line(const View& v, int i, double fm, double f0, double fp, const X1Div& q) {
+  if (i == 1) return qdk_v(qdk_v(fp - f0, q.e, q.ye), q.h1, q.yh1);
+  if (i == v.lx1) return qdk_v(qdk_v(f0 - fm, q.e, q.ye), q.h1, q.yh1);
+  return qdk_v(qdk_v(fp - fm, q.e, q.ye), q.h1, q.yh1);
 }
 
 // The two x1 log-gradient terms of momentum_rate, evaluated where they are needed: the
@@ -431,19 +480,19 @@ GEMR_HD double dx1_line(const View& v, int i, double fm, double f0, double fp, d
 // interior cell (i1, .) with ghosted index kg and x1 neighbours km, kp inside 1..lx1
 struct DirectX1 {
   GEMR_HD double epol(const View& v, const double* ns, const double* Ts, int i1, long long kg, long long km,
-                      long long kp, double h1) const {
+                      long long kp, const X1Div& q) const {
     const long long e = (long long)(NSP - 1) * v.ng;
     const double le0 = log(ns[e + kg] * KB_ * Ts[e + kg]);
     const double lem = log(ns[e + km] * KB_ * Ts[e + km]);
     const double lep = log(ns[e + kp] * KB_ * Ts[e + kp]);
-    return KB_ * Ts[e + kg] / v.qs[NSP - 1] * dx1_line(v, i1, lem, le0, lep, h1);
+    return KB_ * Ts[e + kg] / v.qs[NSP - 1] * dx1_line(v, i1, lem, le0, lep, q);
   }
   GEMR_HD double pg(const View& v, const double* ns, const double* Ts, long long s0, int i1, long long kg,
-                    long long km, long long kp, double h1) const {
+                    long long km, long long kp, const X1Div& q) const {
     const double lp0 = log(ns[s0 + kg] * KB_ * Ts[s0 + kg]);
     const double lpm = log(ns[s0 + km] * KB_ * Ts[s0 + km]);
     const double lpp = log(ns[s0 + kp] * KB_ * Ts[s0 + kp]);
-    return dx1_line(v, i1, lpm, lp0, lpp, h1);
+    return dx1_line(v, i1, lpm, lp0, lpp, q);
   }
 };
 
@@ -461,22 +510,25 @@ GEMR_HD void momentum_rate(const View& v, long long t, const double* nn, const d
   cell_of(v, c, i1, i2, i3);
   const long long kg = gix(v, i1, i2, i3), k = kg + isp * v.ng;
   const double ms = v.ms[isp];
-  const double h1 = hm(v.h1, v, i1, i2, i3), h2 = hm(v.h2, v, i1, i2, i3), h3 = hm(v.h3, v, i1, i2, i3);
-  // dh2/dx1, dh3/dx1 over the line 0..lx1+1 (centred at every interior cell)
+  const X1Div q = x1_div(v, i1, i2, i3);
+  const double h1 = q.h1, h2 = hm(v.h2, v, i1, i2, i3), h3 = hm(v.h3, v, i1, i2, i3);
+  // dh2/dx1, dh3/dx1 over the line 0..lx1+1 (centred at every interior cell; inside the
+  // line dd is the gradients' divisor e)
   const double dd = v.dx1[i1 + 1] + v.dx1[i1];
-  const double dh2 = (hm(v.h2, v, i1 + 1, i2, i3) - hm(v.h2, v, i1 - 1, i2, i3)) / dd / h1;
-  const double dh3 = (hm(v.h3, v, i1 + 1, i2, i3) - hm(v.h3, v, i1 - 1, i2, i3)) / dd / h1;
+  const double ydd = (i1 == 1 || i1 == v.lx1) ? rcp_dev(dd) : q.ye;
+  const double dh2 = qdk_v(qdk_v(hm(v.h2, v, i1 + 1, i2, i3) - hm(v.h2, v, i1 - 1, i2, i3), dd, ydd), h1, q.yh1);
+  const double dh3 = qdk_v(qdk_v(hm(v.h3, v, i1 + 1, i2, i3) - hm(v.h3, v, i1 - 1, i2, i3), dd, ydd), h1, q.yh1);
   const int im = (i1 > 1) ? i1 - 1 : i1, ip = (i1 < v.lx1) ? i1 + 1 : i1;  // neighbours inside 1..lx1
   const long long km = gix(v, im, i2, i3), kp = gix(v, ip, i2, i3);
   // ambipolar field kB Te / qe * d log(ne kB Te)/dx1
-  const double epol = x1.epol(v, ns, Ts, i1, kg, km, kp, h1);
+  const double epol = x1.epol(v, ns, Ts, i1, kg, km, kp, q);
   // pressure * d log(pressure)/dx1 and dQ/dx1
   const long long s0 = (long long)isp * v.ng;
   const double pres = ns[s0 + kg] * KB_ * Ts[s0 + kg];
-  const double pg = x1.pg(v, ns, Ts, s0, i1, kg, km, kp, h1);
+  const double pg = x1.pg(v, ns, Ts, s0, i1, kg, km, kp, q);
   const long long qb = (long long)isp * nc;
   const long long cm = c - (i1 - im), cp = c + (ip - i1);
-  const double gq = dx1_line(v, i1, Q[qb + cm], Q[qb + c], Q[qb + cp], h1);
+  const double gq = dx1_line(v, i1, Q[qb + cm], Q[qb + c], Q[qb + cp], q);
   double pr = 0.0, lo = 0.0;
   for (int j = 0; j < NNEU; ++j) {  // with the neutrals
     const double nu = maxwell_colln(isp, j, nn[j * nc + c], Tn[c], Ts[k]);

@@ -31,7 +31,7 @@ constexpr int kRateThreads = LSP * kRateCells;
 constexpr int kPairs = LSP * (LSP - 1) / 2;
 
 struct PairTab {
-  double P[kPairs][kRateCells], Phi[kPairs][kRateCells], Psi[kPairs][kRateCells];
+  double P[kPairs][kRateCells], Phi[kPairs][kRateCells], Psi[kPairs][kRateCells], yP[kPairs][kRateCells];
 };
 
 // slot of the unordered pair {i, j}, i != j: owner i with offset d = j - i mod 7 in 1..3
@@ -47,7 +47,7 @@ struct SmemPairs {
   __device__ __forceinline__ gemr::CoulPair operator()(const gemr::View&, int isp, int isp2, double, double, double,
                                                        double) const {
     const int p = pair_slot(isp, isp2);
-    return gemr::CoulPair{tab->P[p][lane], tab->Phi[p][lane], tab->Psi[p][lane]};
+    return gemr::CoulPair{tab->P[p][lane], tab->Phi[p][lane], tab->Psi[p][lane], tab->yP[p][lane]};
   }
 };
 
@@ -64,6 +64,7 @@ __device__ __forceinline__ void fill_pairs(const gemr::View& v, int isp, int lan
     tab.P[p][lane] = q.P;
     tab.Phi[p][lane] = q.Phi;
     tab.Psi[p][lane] = q.Psi;
+    tab.yP[p][lane] = q.yP;
   }
 }
 
@@ -92,12 +93,12 @@ __global__ void __launch_bounds__(kRateThreads) kr_energy(gemr::View v, RateIn i
 struct SharedX1 {
   double epol_v, lm, l0, lp;
   __device__ __forceinline__ double epol(const gemr::View&, const double*, const double*, int, long long, long long,
-                                         long long, double) const {
+                                         long long, const gemr::X1Div&) const {
     return epol_v;
   }
   __device__ __forceinline__ double pg(const gemr::View& v, const double*, const double*, long long, int i1, long long,
-                                       long long, long long, double h1) const {
-    return gemr::dx1_line(v, i1, lm, l0, lp, h1);
+                                       long long, long long, const gemr::X1Div& q) const {
+    return gemr::dx1_line(v, i1, lm, l0, lp, q);
   }
 };
 
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(kRateThreads) kr_momentum(gemr::View v, RateIn
     }
     if (isp == LSP - 1)
       s_epol[lane] = gemr::KB_ * Ts[s0 + kg] / v.qs[LSP - 1] *
-                     gemr::dx1_line(v, i1, lm, l0, lp, gemr::hm(v.h1, v, i1, i2, i3));
+                     gemr::dx1_line(v, i1, lm, l0, lp, gemr::x1_div(v, i1, i2, i3));
   }
   __syncthreads();
   if (ok)
@@ -166,6 +167,7 @@ gemr::View rate_view(const gem_grid* g) {
   v.h1 = G.unit ? nullptr : G.h1;
   v.h2 = G.unit ? nullptr : G.h2;
   v.h3 = G.unit ? nullptr : G.h3;
+  v.yh1 = G.unit ? nullptr : G.yh1;
   v.dx1 = G.L[0].dx;
   const double ms[LSP] = {16.0 * AMU, 30.0 * AMU, 28.0 * AMU, 32.0 * AMU, 14.0 * AMU, 1.0 * AMU, 5.485799090e-4 * AMU};
   const double gam[LSP] = {5.0 / 3, 7.0 / 5, 7.0 / 5, 7.0 / 5, 5.0 / 3, 5.0 / 3, 5.0 / 3};

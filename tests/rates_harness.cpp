@@ -24,6 +24,7 @@ static gemr::View mk(const HRView* h) {
   v.ng = v.s3 * (h->lx3 + 4);
   v.c3 = h->c3;
   v.h1 = h->h1;
+  v.yh1 = nullptr;  // read by the device build only
   v.h2 = h->h2;
   v.h3 = h->h3;
   v.dx1 = h->dx1;
