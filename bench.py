@@ -144,14 +144,15 @@ def measured_hbm_peak():
 
 
 class CpuSample:
-    """The oracle (C++ restatement of the reference Fortran) on the host cores, all threads,
-    on an x3 slab of the workload grid sized so one step takes about `step_seconds`."""
+    """The oracle (C++ restatement of the reference Fortran) on the host cores (all threads
+    unless `threads` is given), on an x3 slab of the workload grid sized so one step takes
+    about `step_seconds`."""
 
-    def __init__(self, lx1, lx2, lx3, step_seconds=4.0):
+    def __init__(self, lx1, lx2, lx3, step_seconds=4.0, threads=None):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O  # checker / CPU baseline only
         self.O = O
-        self.threads = os.cpu_count() or 1
+        self.threads = threads or os.cpu_count() or 1
         O.set_num_threads(self.threads)
         self.lx1, self.lx2, self.lx3 = lx1, lx2, lx3
         slab, el = 2, None
@@ -164,6 +165,7 @@ class CpuSample:
         self.g, self.st, self.slab = g, st, slab
 
     def _one(self, g, st):
+        self.O.set_num_threads(self.threads)
         t0 = time.perf_counter()
         dt, _ = self.O.dt_calc(g, st, 0.5)
         self.O.fluid_adv(g, st, dt)
@@ -176,16 +178,22 @@ class CpuSample:
 
     def describe(self, nsteps, seconds):
         return (f"{nsteps} step(s) of dt_calc + fluid advance on a {self.lx1}x{self.lx2}x{self.slab} x3-slab "
-                f"of the {self.lx1}x{self.lx2}x{self.lx3} dipole workload, {self.threads} OpenMP threads, "
+                f"of the {self.lx1}x{self.lx2}x{self.lx3} dipole workload, {self.threads} OpenMP thread{'s' if self.threads > 1 else ''}, "
                 f"{seconds:.1f} s")
 
 
 def cpu_baseline(lx1, lx2, lx3, target_seconds=15.0):
+    """All host threads, then one thread on a smaller slab (about a fifth of the time)."""
     cs = CpuSample(lx1, lx2, lx3, step_seconds=target_seconds / 4)
     t0 = time.perf_counter()
     vals = [cs.step() for _ in range(3)]
     el = time.perf_counter() - t0
-    return float(np.median(vals)), cs.threads, cs.describe(3, el)
+    one = CpuSample(lx1, lx2, lx3, step_seconds=target_seconds / 20, threads=1)
+    t0 = time.perf_counter()
+    vals1 = [one.step() for _ in range(3)]
+    el1 = time.perf_counter() - t0
+    single = {"value": float(np.median(vals1)), "unit": UNIT, "cores": 1, "sample": one.describe(3, el1)}
+    return float(np.median(vals)), cs.threads, cs.describe(3, el), single
 
 
 def dist_setup(n):
@@ -360,8 +368,9 @@ def run_b200(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, threads, sample = cpu_baseline(w["lx1"], w["lx2"], w["lx3"], args.cpu_seconds)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        v, threads, sample, single = cpu_baseline(w["lx1"], w["lx2"], w["lx3"], args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+               "single_thread": single}
 
     launches_per_step = 2 + 3 + 3 + 1 + (1 if g.lnull > 0 else 0) + 1
     line = {
