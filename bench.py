@@ -678,6 +678,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instance measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--no-full-step", action="store_true", help="skip the full fluid_adv measurement")
+    ap.add_argument("--full-step", action="store_true",
+                    help="run the full fluid_adv measurement on the --lx grid too (profiling a small case)")
     ap.add_argument("--no-batched-adjoint", action="store_true",
                     help="skip the batched adjoint workload (32 instances x 200 steps, about a minute)")
     ap.add_argument("--lx", type=int, nargs=3, default=None, metavar=("LX1", "LX2", "LX3"),
@@ -710,7 +712,7 @@ def main():
         import torch
         torch.cuda.empty_cache()
         line["adjoint"] = run_adjoint(args)
-    if not args.no_full_step and not args.lx and world == 1:  # single-GPU figures, taken at N = 1
+    if not args.no_full_step and (not args.lx or args.full_step) and world == 1:  # single-GPU, N = 1
         import torch
         torch.cuda.empty_cache()
         line["full_step"] = run_full_step(args)
