@@ -106,7 +106,10 @@ struct SharedX1 {
 // are the adjacent lanes (c +- 1), except across the block's edges (lanes 0 and 31), which
 // form that one neighbour's log themselves.  At the line ends the missing side is the cell
 // itself, as the direct form's clamped neighbour index gives.
-__global__ void __launch_bounds__(kRateThreads) kr_momentum(gemr::View v, RateIn in, const double* __restrict__ fv,
+// 72 registers (four blocks per SM): each SM sub-partition holds a quarter of the register
+// file, so at its natural 93 registers (96 allocated) only 5 warps fit per sub-partition and
+// two 7-warp blocks per SM; the cap costs 36 bytes of spills.
+__global__ void __launch_bounds__(kRateThreads, 4) kr_momentum(gemr::View v, RateIn in, const double* __restrict__ fv,
                                                             const double* __restrict__ E1,
                                                             const double* __restrict__ Q,
                                                             const double* __restrict__ alt,
