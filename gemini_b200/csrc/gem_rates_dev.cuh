@@ -68,7 +68,7 @@ __device__ __forceinline__ void fill_pairs(const gemr::View& v, int isp, int lan
   }
 }
 
-// Five 7-warp blocks per SM (56 registers, 132 bytes spilled): 11.2 -> 10.3 ms at config 1
+// Five 7-warp blocks per SM (56 registers, 112 bytes spilled): 11.2 -> 10.3 ms at config 1
 // against its natural 72 registers and four blocks.
 __global__ void __launch_bounds__(kRateThreads, 5) kr_energy(gemr::View v, RateIn in, const double* __restrict__ fv,
                                                           double* __restrict__ Pr, double* __restrict__ Lo) {
@@ -108,7 +108,7 @@ struct SharedX1 {
 // are the adjacent lanes (c +- 1), except across the block's edges (lanes 0 and 31), which
 // form that one neighbour's log themselves.  At the line ends the missing side is the cell
 // itself, as the direct form's clamped neighbour index gives.
-// Five 7-warp blocks per SM (56 registers, 112 bytes spilled): each SM sub-partition holds a
+// Five 7-warp blocks per SM (56 registers, 132 bytes spilled): each SM sub-partition holds a
 // quarter of the register file, so at its natural 93 registers (96 allocated) only 5 warps
 // fit per sub-partition and two blocks per SM (16.2 ms at config 1; 72 registers, four
 // blocks: 10.1 ms; 56: 9.95 ms).
