@@ -64,4 +64,14 @@ void hr_momentum(const HRView* hv, const double* nn, const double* vn1, const do
                         Q, alt, g1, Pr, Lo);
 }
 
+// the symmetric part of one Coulomb pair (Teff**1.5, Phi, Psi): the device kernels evaluate
+// it once per unordered pair and give both species the same bits
+void hr_coulomb_pair(const HRView* hv, int isp, int isp2, double ts1, double ts2, double v1, double v2, double* out) {
+  const gemr::View v = mk(hv);
+  const gemr::CoulPair q = gemr::coulomb_pair(v, isp, isp2, ts1, ts2, v1, v2);
+  out[0] = q.P;
+  out[1] = q.Phi;
+  out[2] = q.Psi;
+}
+
 }  // extern "C"

@@ -41,6 +41,7 @@ def harness(tmp_path_factory):
     L.hr_continuity.argtypes = [P] + [_D] * 8
     L.hr_energy.argtypes = [P] + [_D] * 8
     L.hr_momentum.argtypes = [P] + [_D] * 10
+    L.hr_coulomb_pair.argtypes = [P, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 4 + [_D]
     return L
 
 
@@ -95,3 +96,27 @@ def test_rate_bodies_equal_the_oracle_on_the_host(harness, name, mk):
                                 _p(Pr), _p(Lo))
         assert np.array_equal(Lo, La), which
         assert np.array_equal(Pr, Pa), which
+
+
+def test_coulomb_pair_is_symmetric_to_the_bit(harness):
+    """The device rate kernels evaluate each unordered charged pair's Teff**1.5, Phi and Psi
+    once and hand both species the same bits; that is exact because, with no contraction,
+    swapping the species (and their temperatures and drifts) gives the same bits.  Checked on
+    every pair over temperatures of 100..40000 K and drifts of up to 3 km/s (both branches
+    of Phi, W below and above 0.1)."""
+    g = G.cartesian_grid(6, 2, 2)
+    keep = []
+    v = _view(g, keep)
+    rng = np.random.default_rng(17)
+    a, b = np.zeros(3), np.zeros(3)
+    branches = set()
+    for _ in range(400):
+        i, j = (int(x) for x in rng.choice(LSP, 2, replace=False))
+        t1, t2 = rng.uniform(100, 40000, 2)
+        u1, u2 = rng.uniform(-3000, 3000, 2) * rng.choice([1e-3, 1.0])
+        harness.hr_coulomb_pair(ctypes.byref(v), i, j, t1, t2, u1, u2, _p(a))
+        harness.hr_coulomb_pair(ctypes.byref(v), j, i, t2, t1, u2, u1, _p(b))
+        assert a.tobytes() == b.tobytes(), (i, j, t1, t2, u1, u2, a, b)
+        branches.add(a[1] == 1.0)
+    assert branches == {True, False}
+
