@@ -399,7 +399,7 @@ def run_b200(args, world, rank, local):
 
 
 def run_full_step(args):
-    """fluid_adv in full (app/main.f90:280-381) on the config-1 grid: dt_calc, the step with
+    """fluid_adv in full (app/main.f90:280-381) on the workload grid: dt_calc, the step with
     compression (VNRicht_artvisc, RK2 boundary, compression), the diffusion, and the
     source/loss sub-step (rates and ETD solves of energy, momentum, mass), through
     gem_fluid_adv_full_dev.  The neutral atmosphere and ionization rates are seeded
@@ -448,7 +448,8 @@ def run_full_step(args):
     nonfinite = F.check_finite(ds)
     ds.close()
     dg.close()
-    return {"workload": "fluid_adv in full on the config-1 grid: dt_calc, advection, compression, diffusion, "
+    return {"workload": f"fluid_adv in full on the {g.lx1}x{g.lx2}x{g.lx3} dipole grid: dt_calc, advection, "
+                        "compression, diffusion, "
                         "source/loss (seeded synthetic exponential neutral atmosphere and ionization layer)",
             "ms_per_step": ms, "value": nc * LSP / (ms / 1e3) / 1e9, "unit": UNIT, "steps": K,
             "nonfinite": nonfinite,

@@ -22,8 +22,7 @@ __global__ void kr_continuity(gemr::View v, RateIn in, const double* __restrict_
 }
 
 // The energy and momentum exchange run one block per 32 interior cells, one warp per
-// species (thread = (cell, species) as before, 32 consecutive cells of one species per
-// warp).  Each of the 21 unordered charged pairs of a cell has its symmetric part (Teff**1.5,
+// species (a thread per (cell, species), 32 consecutive cells of one species per warp).  Each of the 21 unordered charged pairs of a cell has its symmetric part (Teff**1.5,
 // Phi, Psi) evaluated once, by warp i for the pairs (i, i+1), (i, i+2), (i, i+3) mod 7, and
 // shared through shared memory: the bits are those of evaluating it in both threads.
 constexpr int kRateCells = 32;
@@ -68,8 +67,8 @@ __device__ __forceinline__ void fill_pairs(const gemr::View& v, int isp, int lan
   }
 }
 
-// Five 7-warp blocks per SM (56 registers, 112 bytes spilled): 11.2 -> 10.3 ms at config 1
-// against its natural 72 registers and four blocks.
+// Five 7-warp blocks per SM (56 registers, 112 bytes spilled): 11.2 -> 10.3 ms on the
+// 384x192x192 dipole grid against its natural 72 registers and four blocks.
 __global__ void __launch_bounds__(kRateThreads, 5) kr_energy(gemr::View v, RateIn in, const double* __restrict__ fv,
                                                           double* __restrict__ Pr, double* __restrict__ Lo) {
   __shared__ PairTab tab;
@@ -110,8 +109,8 @@ struct SharedX1 {
 // itself, as the direct form's clamped neighbour index gives.
 // Five 7-warp blocks per SM (56 registers, 132 bytes spilled): each SM sub-partition holds a
 // quarter of the register file, so at its natural 93 registers (96 allocated) only 5 warps
-// fit per sub-partition and two blocks per SM (16.2 ms at config 1; 72 registers, four
-// blocks: 10.1 ms; 56: 9.95 ms).
+// fit per sub-partition and two blocks per SM (16.2 ms on the 384x192x192 dipole grid;
+// 72 registers, four blocks: 10.1 ms; 56: 9.95 ms).
 __global__ void __launch_bounds__(kRateThreads, 5) kr_momentum(gemr::View v, RateIn in, const double* __restrict__ fv,
                                                             const double* __restrict__ E1,
                                                             const double* __restrict__ Q,
